@@ -1,0 +1,470 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 face-loop path (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--n 256] [--impl ours|reference]
+
+Workload: MeshStructGenSource-equivalent structured hex mesh n^3 on the unit
+cube (default 256^3: 16.8M cells, 50.1M interior + 393K boundary faces),
+seeded synthetic fields. One step = the FP32-compensated forward
+(GradientPhiGaussDolfyn with nGradient = 1 fused with the plain
+FluxMassDolfynFaceLoop m_f = rho_f (u_f . S_f)) plus the hand-written adjoint
+of L = sum_c V_c |grad_c|^2 + sum_f g_f m_f, on device-resident inputs.
+Metric: Gfaces/s = (interior + boundary faces) / step time, summed over GPUs
+(each GPU runs its own mesh: weak scaling, no data-path collective).
+
+Also reported: the plain FP64 forward on the same mesh, the FP32-compensated
+error against the FP64 path, the end-to-end host-buffer call (H2D + D2H
+inside the timed region), the CPU baseline (the reference's own kernels)
+and the HBM roofline of the dominant kernel.
+
+--impl reference: the reference's own CPU kernels (compiled unchanged into
+oracle/_ref, else the oracle restatement), all host cores as independent
+processes on z-slabs of the mesh (what mpirun -n P with the naive
+partitioner runs: the kernels have no communication).
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+METRIC = "Gfaces/s and HBM GB/s, FP32-comp+adjoint vs FP64 plain on 1 B200, err vs FP64"
+SEED = 20261203
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def load_cupcfd():
+    name = "cupcfd_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    path = os.path.join(ROOT, "cup-cfd_b200", "__init__.py")
+    spec = importlib.util.spec_from_file_location(name, path, submodule_search_locations=[os.path.dirname(path)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def face_counts(n):
+    nC = n ** 3
+    nFi = 3 * n * n * (n - 1)
+    nB = 6 * n * n
+    return nC, nFi + nB, nFi, nB
+
+
+def bytes_model(nC, nF, nFi, nB):
+    """Algorithmic (compulsory) bytes: each distinct input read once, each
+    output written once; int32 indices; FP64 volumes in both precisions."""
+    return {
+        # fused forward, FP32: phi 4 + rho,u,v,w 16 + V 8 + grad 12 per cell;
+        # S 12 + lambda 4 + cell1 4 per face; cell2 4 + m_f 4 per interior face; phiB 4 per boundary face
+        "fwd_f32": 40 * nC + 20 * nF + 8 * nFi + 4 * nB,
+        # adjoint, FP32: grad 12 + state 16 + phibar 4 + statebar 16 per cell; face geometry and
+        # connectivity as above; g_f 4 per interior face; phibBar 4 per boundary face
+        "adj_f32": 48 * nC + 20 * nF + 8 * nFi + 4 * nB,
+        # whole forward+adjoint pipeline: face data and inputs counted once, grad written once and read once
+        "pipeline_f32": 72 * nC + 20 * nF + 12 * nFi + 8 * nB,
+        # fused forward, FP64: 8-byte reals
+        "fwd_f64": 72 * nC + 32 * nF + 16 * nFi + 8 * nB,
+    }
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            p = json.load(fh)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM traffic per launch from the committed ncu summary, if present."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as fh:
+            return json.load(fh)
+    except Exception:
+        return {}
+
+
+class Clocks:
+    """nvidia-smi sampler for the timed region (SM clock, throttle reasons)."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as fh:
+            for line in fh:
+                p = [x.strip() for x in line.split(",")]
+                if len(p) < 9:
+                    continue
+                try:
+                    sm.append(float(p[1]))
+                    mx = float(p[2])
+                except ValueError:
+                    continue
+                for nm, v in zip(names, p[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference's own kernels on a bounded sample
+# ---------------------------------------------------------------------------
+def _cpu_worker(args):
+    n, nz_local, z0, reps = args
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import oracle as O
+    h = 1.0 / n
+    # one z-slab of the n^3 mesh plus one ghost layer below and above (when present)
+    lo = max(z0 - 1, 0)
+    hi = min(z0 + nz_local + 1, n)
+    m = O.structgen(n, n, hi - lo, bounds=(0.0, 1.0, 0.0, 1.0, lo * h, hi * h))
+    f = O.fields(m, SEED)
+    kind = "reference"
+    if O.load_ref() is not None:
+        R = O.RefKernels(m)
+        _, _, _, sg = R.gradient(f["phi"], f["phiB"], 1, reps=reps)
+        _, _, sm = R.flux_mass(f, reps=reps)
+        t = [a + b for a, b in zip(sg, sm)]
+    else:
+        kind = "port"
+        t = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            O.gradient(m, f["phi"], f["phiB"], 1)
+            O.flux_mass_face_loop(m, f)
+            t.append(time.perf_counter() - t0)
+    return kind, m["nFaces"], t
+
+
+def cpu_baseline(n, procs, reps):
+    """Gfaces/s of the reference's forward face loops (GradientPhiGaussDolfyn +
+    FluxMassDolfynFaceLoop, FP64; the reference has no adjoint) on `procs`
+    independent processes over z-slabs of an n^3 mesh."""
+    import multiprocessing as mp
+    nC, nF, nFi, nB = face_counts(n)
+    slabs = [(n, n // procs + (1 if r < n % procs else 0)) for r in range(procs)]
+    z, jobs = 0, []
+    for _, nzl in slabs:
+        jobs.append((n, nzl, z, reps))
+        z += nzl
+    if procs == 1:
+        res = [_cpu_worker(jobs[0])]
+    else:
+        with mp.get_context("spawn").Pool(procs) as pool:
+            res = pool.map(_cpu_worker, jobs)
+    kind = res[0][0]
+    # per repetition, the slowest process bounds the step (all ranks run in lock step)
+    per_rep = [max(r[2][i] for r in res) for i in range(reps)]
+    t = statistics.median(per_rep)
+    return {"value": nF / t / 1e9, "unit": "Gfaces/s", "cores": procs, "kind": kind,
+            "sample": f"{n}^3 structured mesh ({nF} faces) in {procs} z-slab(s) with one ghost layer; "
+                      f"reference GradientPhiGaussDolfyn + FluxMassDolfynFaceLoop (FP64 forward; the "
+                      f"reference has no adjoint); median of {reps} repetitions; unique faces / slowest slab",
+            "ms_per_step": t * 1e3}
+
+
+# ---------------------------------------------------------------------------
+# reference arm
+# ---------------------------------------------------------------------------
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    procs = os.cpu_count() or 1
+    n = a.cpu_n
+    reps = max(3, min(a.steps, 20))
+    t0 = time.time()
+    cb = cpu_baseline(n, procs, reps)
+    nC, nF, nFi, nB = face_counts(a.n)
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "Gfaces/s", "n_gpus": a.gpus,
+            "steps": reps, "warmup": 0, "ms_per_step": cb["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": f"reference CPU face loops, bounded sample of the {a.n}^3 workload", "mesh": f"{n}^3",
+                       "cells": n ** 3},
+            "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "Gfaces/s", "h2d_bytes_per_step": 0,
+                                        "d2h_bytes_per_step": 0},
+            "wall_s": round(time.time() - t0, 1)}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def run_gpu(a):
+    import numpy as np
+    import torch
+    cg = load_cupcfd()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n = a.n
+    t_build = time.time()
+    mesh = cg.Mesh.structgen(n, n, n, order=a.order, device=local)
+    torch.cuda.synchronize()
+    t_build = time.time() - t_build
+    nC, nF, nFi, nB = mesh.nCells, mesh.nFaces, mesh.nInteriorFaces, mesh.nBoundaries
+    log(f"[rank {rank}] mesh {n}^3: {nC} cells, {nF} faces ({nFi} interior), built in {t_build:.2f} s, "
+        f"{mesh.deviceBytes / 1e9:.2f} GB")
+    g = torch.Generator(device=dev)
+    g.manual_seed(SEED + rank)
+    # fields (internal numbering; i.i.d. so numbering does not change the distribution)
+    phi = torch.rand(nC, generator=g, device=dev) * 2 - 1
+    phiB = torch.rand(nB, generator=g, device=dev) * 2 - 1
+    rho = torch.rand(nC, generator=g, device=dev) * 0.2 + 0.9
+    uvw = torch.randn(3, nC, generator=g, device=dev)
+    state = torch.stack([rho, uvw[0], uvw[1], uvw[2]], 1).contiguous()           # float4 per cell
+    gface = torch.randn(nF, generator=g, device=dev)
+    grad = torch.empty(3, nC, device=dev)
+    mflux = torch.zeros(nF, device=dev)
+    pbar = torch.empty(nC, device=dev)
+    pbbar = torch.empty(nB, device=dev)
+    sbar = torch.empty(nC, 4, device=dev)
+    loss = torch.zeros(1, dtype=torch.float64, device=dev)
+    st = torch.cuda.current_stream()
+    F32 = cg.PREC_F32C
+
+    def step():
+        cg.dev_forward(mesh, F32, phi, phiB, state, grad, mflux, gface=gface, loss=loss, stream=st)
+        cg.dev_adjoint(mesh, F32, grad, state, gface, pbar, pbbar, sbar, stream=st)
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+    K = a.steps
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    vis = [v for v in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if v.strip()]
+    clocks = Clocks(vis[local] if local < len(vis) else local)
+    clocks.start()
+    time.sleep(0.3)
+    launches0 = cg.launch_count()
+    t_start.record(st)
+    for k in range(K):
+        ev[k][0].record(st)
+        cg.dev_forward(mesh, F32, phi, phiB, state, grad, mflux, gface=gface, loss=loss, stream=st)
+        ev[k][1].record(st)
+        cg.dev_adjoint(mesh, F32, grad, state, gface, pbar, pbbar, sbar, stream=st)
+        ev[k][2].record(st)
+    t_end.record(st)
+    torch.cuda.synchronize()
+    launches = cg.launch_count() - launches0
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    total_ms = t_start.elapsed_time(t_end)
+    fwd_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in ev)
+    adj_ms = statistics.mean(e[1].elapsed_time(e[2]) for e in ev)
+    tmax = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    total_ms = float(tmax.item())
+    ms_step = total_ms / K
+    value = world * nF / (ms_step * 1e-3) / 1e9
+
+    # ---- plain FP64 forward on the same mesh
+    phi64, phiB64 = phi.double(), phiB.double()
+    st64 = state.double().t().contiguous()                                        # [4][nC] blocks
+    grad64 = torch.empty(3, nC, dtype=torch.float64, device=dev)
+    mf64 = torch.zeros(nF, dtype=torch.float64, device=dev)
+    for _ in range(a.warmup):
+        cg.dev_forward(mesh, cg.PREC_F64, phi64, phiB64, st64, grad64, mf64, stream=st)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    K64 = max(1, K // 2)
+    e0.record(st)
+    for _ in range(K64):
+        cg.dev_forward(mesh, cg.PREC_F64, phi64, phiB64, st64, grad64, mf64, stream=st)
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms64 = e0.elapsed_time(e1) / K64
+
+    # ---- FP32-compensated vs FP64 on the same inputs (forward + adjoint)
+    gf64 = gface.double()
+    pbar64 = torch.empty(nC, dtype=torch.float64, device=dev)
+    pbbar64 = torch.empty(nB, dtype=torch.float64, device=dev)
+    sbar64 = torch.empty(4, nC, dtype=torch.float64, device=dev)
+    loss64 = torch.zeros(1, dtype=torch.float64, device=dev)
+    cg.dev_forward(mesh, cg.PREC_F64, phi64, phiB64, st64, grad64, mf64, gface=gf64, loss=loss64, stream=st)
+    cg.dev_adjoint(mesh, cg.PREC_F64, grad64, st64, gf64, pbar64, pbbar64, sbar64, stream=st)
+    step()
+    torch.cuda.synchronize()
+
+    def err(x32, x64):
+        rms_ref = float(torch.sqrt(torch.mean(x64 * x64)).item()) if x64.numel() else 0.0
+        e = cg.error_norms(x32, x64, 1e-2 * rms_ref)
+        return {"max_rel_normwise": e["max_rel_norm"], "rms_rel": e["rms_rel"], "max_rel_floor1e-2rms": e["max_rel_floor"]}
+
+    errors = {
+        "grad": err(grad.contiguous(), grad64),
+        "massFlux": err(mflux.contiguous(), mf64),
+        "phiBar": err(pbar, pbar64),
+        "stateBar": err(sbar.t().contiguous(), sbar64),
+        "loss_rel": abs(float(loss.item()) - float(loss64.item())) / abs(float(loss64.item())),
+    }
+
+    # ---- end to end through the reference-facing host-buffer call
+    e2e = None
+    K2 = max(1, min(K, a.e2e_steps))
+    hb = {}
+    for nm, cnt in (("phi", nC), ("phiB", nB), ("den", nC), ("u", nC), ("v", nC), ("w", nC), ("gface", nF)):
+        hb[nm] = torch.empty(cnt, dtype=torch.float64, pin_memory=True)
+    hb["phi"].copy_(phi64.cpu()); hb["phiB"].copy_(phiB64.cpu())
+    hb["den"].copy_(rho.double().cpu()); hb["u"].copy_(uvw[0].double().cpu())
+    hb["v"].copy_(uvw[1].double().cpu()); hb["w"].copy_(uvw[2].double().cpu()); hb["gface"].copy_(gf64.cpu())
+    out = {"grad": torch.empty(nC, 3, dtype=torch.float64, pin_memory=True),
+           "massFlux": torch.empty(nF, dtype=torch.float64, pin_memory=True),
+           "phiBar": torch.empty(nC, dtype=torch.float64, pin_memory=True),
+           "phiBBar": torch.empty(nB, dtype=torch.float64, pin_memory=True),
+           "denBar": torch.empty(nC, dtype=torch.float64, pin_memory=True),
+           "uBar": torch.empty(nC, dtype=torch.float64, pin_memory=True),
+           "vBar": torch.empty(nC, dtype=torch.float64, pin_memory=True),
+           "wBar": torch.empty(nC, dtype=torch.float64, pin_memory=True),
+           "loss": torch.empty(1, dtype=torch.float64, pin_memory=True)}
+    hn = {k: v.numpy() for k, v in hb.items()}
+    on = {k: v.numpy() for k, v in out.items()}
+    args_e2e = (mesh, F32, hn["phi"], hn["phiB"], hn["den"], hn["u"], hn["v"], hn["w"], hn["gface"])
+    cg.forward_adjoint(*args_e2e, out=on)   # warm (allocates the mesh's scratch buffers)
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(K2):
+        cg.forward_adjoint(*args_e2e, out=on)
+    te = (time.perf_counter() - t0) / K2
+    temax = torch.tensor([te], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(temax, op=dist.ReduceOp.MAX)
+    te = float(temax.item())
+    h2d = 8 * (5 * nC + nB + nF)
+    d2h = 8 * (3 * nC + nF + 5 * nC + nB + 1)
+    e2e = {"value": world * nF / te / 1e9, "unit": "Gfaces/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+           "ms_per_step": te * 1e3, "steps": K2,
+           "call": "cupcfd_gpu_forward_adjoint (host FP64 buffers in reference numbering, pinned)"}
+
+    # ---- roofline of the dominant kernel
+    bm = bytes_model(nC, nF, nFi, nB)
+    peak, peak_src = measured_peaks()
+    dom = "fwd" if fwd_ms >= adj_ms else "adj"
+    dom_ms = fwd_ms if dom == "fwd" else adj_ms
+    dom_bytes = bm["fwd_f32" if dom == "fwd" else "adj_f32"]
+    achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
+    tr = profile_traffic().get(f"{'k_fwd_f32' if dom == 'fwd' else 'k_adj_f32'}@{n}")
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": tr, "kernel": "k_fwd_f32" if dom == "fwd" else "k_adj_f32", "peak_source": peak_src,
+            "algorithmic_bytes_per_launch": dom_bytes, "ms_per_launch": dom_ms}
+    pipe_gbs = bm["pipeline_f32"] / (ms_step * 1e-3) / 1e9
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu:
+        try:
+            cpu = cpu_baseline(a.cpu_n, 1, a.cpu_reps)
+        except Exception as ex:  # the baseline never blocks the GPU line
+            cpu = {"value": None, "unit": "Gfaces/s", "cores": 1, "kind": "reference", "sample": f"failed: {ex}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "Gfaces/s", "n_gpus": world, "steps": K, "warmup": a.warmup,
+            "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic, seeded: phi~U[-1,1], u,v,w~N(0,1), rho~U[0.9,1.1], phiB~U[-1,1], g_f~N(0,1)",
+            "config": {"workload": f"structgen {n}^3 unit cube, FP32-compensated forward+adjoint of "
+                                   f"GradientPhiGaussDolfyn + FluxMassDolfynFaceLoop",
+                       "mesh": f"{n}^3", "cells": nC, "faces": nF, "interior_faces": nFi, "boundary_faces": nB,
+                       "order": ["native", "morton", "owner"][a.order], "parallelism": f"replicas x{world}",
+                       "l2": f"inputs larger than L2 ({bm['pipeline_f32'] / 1e9:.2f} GB compulsory traffic per step)"},
+            "roofline": roof,
+            "pipeline": {"gbs": pipe_gbs, "frac": pipe_gbs / peak, "algorithmic_bytes": bm["pipeline_f32"],
+                         "fwd_ms": fwd_ms, "adj_ms": adj_ms},
+            "fp64_plain_forward": {"value": world * nF / (ms64 * 1e-3) / 1e9, "unit": "Gfaces/s", "ms_per_step": ms64,
+                                   "gbs": bm["fwd_f64"] / (ms64 * 1e-3) / 1e9,
+                                   "frac": bm["fwd_f64"] / (ms64 * 1e-3) / 1e9 / peak},
+            "error_vs_fp64": errors,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "gpu_launches": launches,
+            "clocks": clk,
+            "mesh_build_s": t_build,
+        }
+        print(json.dumps(line), flush=True)
+    mesh.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--n", type=int, default=256, help="mesh is n^3 cells")
+    ap.add_argument("--order", type=int, default=1, help="0 native, 1 morton, 2 owner")
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--cpu-n", type=int, default=64, help="CPU baseline sample: cpu_n^3 mesh")
+    ap.add_argument("--cpu-reps", type=int, default=20)
+    ap.add_argument("--no-cpu", action="store_true")
+    a = ap.parse_args()
+    if a.warmup < 3:
+        a.warmup = 3
+    if a.impl == "reference":
+        sys.exit(run_reference(a))
+    sys.exit(run_gpu(a))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,389 @@
+"""cupcfd_b200 -- Python front end of libcupcfd_gpu (the C-ABI CUDA library).
+
+The library implements CUP-CFD's finite-volume face-loop path on B200:
+``GradientPhiGaussDolfyn`` (include/fvm/implementation/component/GradientKernels.ipp)
+and ``FluxMassDolfynFaceLoop`` (include/fvm/implementation/component/MassKernels.ipp)
+over the MiniSoA mesh. This module is a thin ctypes layer over
+``include/cupcfd_gpu.h``: host calls take numpy arrays in the reference's
+numbering and layout and return the reference's eCodes integers; device calls
+take torch CUDA tensors in the mesh's internal numbering. torch is used only
+for device memory and streams.
+
+There is no CPU fallback: every call runs the CUDA library, and importing
+fails loudly when the library cannot be loaded.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcupcfd_gpu.so")
+
+# eCodes values (include/error/Error.h)
+E_ARRAY_SIZE_MISMATCH = 25
+E_INVALID_INDEX = 68
+E_CONFIG_INVALID_VALUE = 90
+E_SUCCESS = 95
+E_ERROR = 98
+E_NULL_PTR = 99
+E_NOT_IMPLEMENTED = 109
+
+RTYPE_DEFAULT, RTYPE_INLET, RTYPE_OUTLET, RTYPE_SYMP, RTYPE_WALL = range(5)
+PREC_F64, PREC_F32C = 0, 1
+ORDER_NATIVE, ORDER_MORTON, ORDER_OWNER = 0, 1, 2
+SIGN_REFERENCE, SIGN_SIGNED = 0, 1
+
+_lock = threading.Lock()
+_lib = None
+
+
+class CupcfdError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"cupcfd_gpu error {code}: {msg}")
+        self.code = code
+
+
+class Vec3View(C.Structure):
+    _fields_ = [("base", C.c_void_p), ("stride", C.c_int32), ("offset", C.c_int32)]
+
+
+class MeshView(C.Structure):
+    _fields_ = [("nCells", C.c_int32), ("nFaces", C.c_int32), ("nBoundaries", C.c_int32), ("real_size", C.c_int32),
+                ("faceCell1", C.c_void_p), ("faceCell2", C.c_void_p), ("faceBnd", C.c_void_p),
+                ("faceLambda", C.c_void_p), ("faceArea", C.c_void_p),
+                ("faceNorm", Vec3View), ("faceCenter", Vec3View), ("faceXpac", Vec3View), ("faceXnac", Vec3View),
+                ("cellCenter", Vec3View), ("cellVolume", C.c_void_p)]
+
+
+class MeshOptions(C.Structure):
+    _fields_ = [("order", C.c_int32), ("precisions", C.c_int32), ("device", C.c_int32)]
+
+
+class MeshInfo(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in ("nCells", "nFaces", "nInteriorFaces", "nBoundaries", "nRegions",
+                                         "nIncidences", "maxCellFaces", "order", "precisions")] + [
+        ("deviceBytes", C.c_int64)]
+
+
+# exported symbols of include/cupcfd_gpu.h with their ctypes signatures
+_VP, _I, _I64, _D = C.c_void_p, C.c_int32, C.c_int64, C.c_double
+SIGNATURES = {
+    "cupcfd_gpu_last_error": ([], C.c_char_p),
+    "cupcfd_gpu_version": ([], C.c_char_p),
+    "cupcfd_gpu_launch_count": ([], C.c_int64),
+    "cupcfd_gpu_mesh_create": ([_VP, _VP, _VP], _I),
+    "cupcfd_gpu_mesh_create_structgen": ([_I, _I, _I, _VP, _VP, _VP], _I),
+    "cupcfd_gpu_mesh_create_jittered": ([_I, _I, _I, _D, C.c_uint64, _I, _VP, _VP], _I),
+    "cupcfd_gpu_mesh_destroy": ([_VP], _I),
+    "cupcfd_gpu_mesh_get_info": ([_VP, _VP], _I),
+    "cupcfd_gpu_mesh_set_regions": ([_VP, _I, _VP, _VP, _VP, _VP, _I], _I),
+    "cupcfd_gpu_mesh_get_cell_face_csr": ([_VP, _VP, _I, _VP, _I], _I),
+    "cupcfd_gpu_mesh_get_geometry": ([_VP] * 10, _I),
+    "cupcfd_gpu_mesh_get_numbering": ([_VP, _VP, _VP], _I),
+    "cupcfd_gpu_gradient_phi_gauss_dolfyn": ([_VP, _I, _VP, _I, _VP, _I, _VP, _I, _I, _I, _VP, _I, _I, _I, _I, _I, _I], _I),
+    "cupcfd_gpu_flux_mass_dolfyn_face_loop": ([_VP, Vec3View, _I, Vec3View, _I, Vec3View, _I, Vec3View, _I]
+                                              + [_VP, _I] * 14 + [_D] + [_VP] * 4 + [_I] * 4 + [_VP, _I] * 8, _I),
+    "cupcfd_gpu_forward_adjoint": ([_VP, _I] + [_VP] * 16, _I),
+    "cupcfd_gpu_dev_permute_cells": ([_VP, _I, _I, _VP, _I, _I64, _VP, _I, _I64, _VP], _I),
+    "cupcfd_gpu_dev_permute_faces": ([_VP, _I, _VP, _I, _VP, _I, _VP], _I),
+    "cupcfd_gpu_dev_gradient": ([_VP, _I, _I, _I, _VP, _VP, _VP, _VP, _VP], _I),
+    "cupcfd_gpu_dev_mass_plain": ([_VP, _I, _VP, _VP, _VP], _I),
+    "cupcfd_gpu_dev_gradient_adjoint": ([_VP, _I, _I, _VP, _VP, _VP, _VP], _I),
+    "cupcfd_gpu_dev_mass_plain_adjoint": ([_VP, _I, _VP, _VP, _VP, _VP], _I),
+    "cupcfd_gpu_dev_forward": ([_VP, _I] + [_VP] * 8, _I),
+    "cupcfd_gpu_dev_adjoint": ([_VP, _I] + [_VP] * 7, _I),
+    "cupcfd_gpu_dev_forward_adjoint": ([_VP, _I] + [_VP] * 11, _I),
+    "cupcfd_gpu_dev_error_norms": ([_VP, _I, _VP, _I, _I64, _D, _VP, _VP], _I),
+}
+
+
+def lib():
+    """The loaded library (built from csrc/ with nvcc if the .so is missing)."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                import importlib.util
+                spec = importlib.util.spec_from_file_location("_cupcfd_build", os.path.join(HERE, "build.py"))
+                b = importlib.util.module_from_spec(spec)
+                spec.loader.exec_module(b)
+                b.build()
+            L = C.CDLL(LIB_PATH)
+            for name, (args, res) in SIGNATURES.items():
+                fn = getattr(L, name)
+                fn.argtypes = args
+                fn.restype = res
+            _lib = L
+        return _lib
+
+
+def last_error() -> str:
+    return lib().cupcfd_gpu_last_error().decode()
+
+
+def launch_count() -> int:
+    return int(lib().cupcfd_gpu_launch_count())
+
+
+def check(rc):
+    if rc != E_SUCCESS:
+        raise CupcfdError(rc, last_error())
+    return rc
+
+
+def _p(a):
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return C.c_void_p(a.data_ptr())
+    assert a.flags["C_CONTIGUOUS"], "host arrays must be C-contiguous"
+    return C.c_void_p(a.ctypes.data)
+
+
+def _vec(a, real_size=8):
+    """Vec3View of a host array: (n,3) packed, or an (n, k) array whose
+    components sit at columns 1..3 (emulating the vptr-carrying
+    EuclideanVector layout: k = 4 for double gives a 32-byte stride)."""
+    if a is None:
+        return Vec3View(None, 3 * real_size, 0)
+    assert a.flags["C_CONTIGUOUS"]
+    if a.ndim == 2 and a.shape[1] == 3:
+        return Vec3View(a.ctypes.data, 3 * real_size, 0)
+    if a.ndim == 2 and a.shape[1] == 4:
+        return Vec3View(a.ctypes.data, 4 * real_size, real_size)
+    raise ValueError("vector arrays must be (n,3) packed or (n,4) with a leading pad slot")
+
+
+def _stream(s):
+    if s is None:
+        return None
+    if hasattr(s, "cuda_stream"):
+        return C.c_void_p(s.cuda_stream)
+    return C.c_void_p(int(s))
+
+
+# ---------------------------------------------------------------------------
+# mesh
+# ---------------------------------------------------------------------------
+class Mesh:
+    """A device mesh (cupcfd_gpu_mesh). Build with ``structgen``, ``jittered``
+    or ``from_arrays``; free with ``close`` (or garbage collection)."""
+
+    def __init__(self, handle):
+        self.h = handle
+        info = MeshInfo()
+        check(lib().cupcfd_gpu_mesh_get_info(self.h, C.byref(info)))
+        self.nCells, self.nFaces, self.nInteriorFaces = info.nCells, info.nFaces, info.nInteriorFaces
+        self.nBoundaries, self.nIncidences, self.maxCellFaces = info.nBoundaries, info.nIncidences, info.maxCellFaces
+        self.order, self.precisions, self.deviceBytes = info.order, info.precisions, info.deviceBytes
+
+    @staticmethod
+    def _opts(order, precisions, device):
+        return MeshOptions(order, precisions, device)
+
+    @classmethod
+    def structgen(cls, nx, ny, nz, bounds=(0.0, 1.0, 0.0, 1.0, 0.0, 1.0), order=ORDER_MORTON,
+                  precisions=(1 << PREC_F64) | (1 << PREC_F32C), device=-1):
+        h = C.c_void_p()
+        b = (C.c_double * 6)(*bounds)
+        o = cls._opts(order, precisions, device)
+        check(lib().cupcfd_gpu_mesh_create_structgen(nx, ny, nz, b, C.byref(o), C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def jittered(cls, nx, ny, nz, jitter=0.25, seed=1, permute=True, order=ORDER_MORTON,
+                 precisions=(1 << PREC_F64) | (1 << PREC_F32C), device=-1):
+        h = C.c_void_p()
+        o = cls._opts(order, precisions, device)
+        check(lib().cupcfd_gpu_mesh_create_jittered(nx, ny, nz, float(jitter), int(seed), int(bool(permute)),
+                                                     C.byref(o), C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_arrays(cls, m, order=ORDER_MORTON, precisions=(1 << PREC_F64) | (1 << PREC_F32C), device=-1,
+                    return_code=False):
+        """Upload a host mesh given as a dict of numpy arrays (keys of a
+        one-rank CupCfdSoAMesh: faceCell1/2, faceBnd, faceLambda, faceArea,
+        faceNorm, faceCenter, faceXpac, faceXnac, cellCenter, cellVolume)."""
+        rs = m["faceLambda"].dtype.itemsize
+        keep = {k: np.ascontiguousarray(v) for k, v in m.items() if isinstance(v, np.ndarray)}
+        v = MeshView()
+        v.nCells, v.nFaces, v.nBoundaries, v.real_size = int(m["nCells"]), int(m["nFaces"]), int(m["nBnd"]), rs
+        v.faceCell1, v.faceCell2, v.faceBnd = _p(keep["faceCell1"]), _p(keep["faceCell2"]), _p(keep["faceBnd"])
+        v.faceLambda, v.faceArea, v.cellVolume = _p(keep["faceLambda"]), _p(keep["faceArea"]), _p(keep["cellVolume"])
+        v.faceNorm, v.faceCenter, v.cellCenter = _vec(keep["faceNorm"], rs), _vec(keep["faceCenter"], rs), _vec(keep["cellCenter"], rs)
+        v.faceXpac = _vec(keep.get("faceXpac"), rs)
+        v.faceXnac = _vec(keep.get("faceXnac"), rs)
+        h = C.c_void_p()
+        o = cls._opts(order, precisions, device)
+        rc = lib().cupcfd_gpu_mesh_create(C.byref(v), C.byref(o), C.byref(h))
+        if return_code:
+            return rc, (cls(h) if rc == E_SUCCESS else None)
+        check(rc)
+        return cls(h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().cupcfd_gpu_mesh_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_regions(self, region_type, region_uvw, region_den, bnd_region):
+        rt = np.ascontiguousarray(region_type, np.int32)
+        uvw = np.ascontiguousarray(region_uvw, np.float64)
+        den = np.ascontiguousarray(region_den, np.float64)
+        br = np.ascontiguousarray(bnd_region, np.int32)
+        return lib().cupcfd_gpu_mesh_set_regions(self.h, len(rt), _p(rt), _p(uvw), _p(den), _p(br), len(br))
+
+    def cell_face_csr(self):
+        xadj = np.empty(self.nCells + 1, np.int32)
+        adj = np.empty(self.nIncidences, np.int32)
+        check(lib().cupcfd_gpu_mesh_get_cell_face_csr(self.h, _p(xadj), len(xadj), _p(adj), len(adj)))
+        return xadj, adj
+
+    def geometry(self):
+        nF, nC = self.nFaces, self.nCells
+        g = dict(faceCell1=np.empty(nF, np.int32), faceCell2=np.empty(nF, np.int32), faceBnd=np.empty(nF, np.int32),
+                 faceLambda=np.empty(nF), faceArea=np.empty(nF), faceNorm=np.empty((nF, 3)),
+                 faceCenter=np.empty((nF, 3)), cellCenter=np.empty((nC, 3)), cellVolume=np.empty(nC))
+        check(lib().cupcfd_gpu_mesh_get_geometry(self.h, *[_p(g[k]) for k in (
+            "faceCell1", "faceCell2", "faceBnd", "faceLambda", "faceArea", "faceNorm", "faceCenter", "cellCenter",
+            "cellVolume")]))
+        return g
+
+    def numbering(self):
+        c = np.empty(self.nCells, np.int32)
+        f = np.empty(self.nFaces, np.int32)
+        check(lib().cupcfd_gpu_mesh_get_numbering(self.h, _p(c), _p(f)))
+        return c, f
+
+
+# ---------------------------------------------------------------------------
+# reference-facing calls (host numpy arrays, reference numbering)
+# ---------------------------------------------------------------------------
+def GradientPhiGaussDolfyn(mesh, nGradient, phiCell, phiBoundary, dPhidxCell, dPhidxoCell,
+                           precision=PREC_F64, sign_mode=SIGN_REFERENCE):
+    """Mirror of cupcfd::fvm::GradientPhiGaussDolfyn (GradientKernels.h:48-54).
+    dPhidxCell / dPhidxoCell are (n,3) or (n,4) (leading pad slot, the
+    EuclideanVector layout) arrays written in place. Returns an eCodes value."""
+    rs = phiCell.dtype.itemsize
+    v, vo = _vec(dPhidxCell, rs), _vec(dPhidxoCell, rs)
+    return lib().cupcfd_gpu_gradient_phi_gauss_dolfyn(
+        mesh.h, int(nGradient), _p(phiCell), len(phiCell), _p(phiBoundary), len(phiBoundary),
+        v.base, len(dPhidxCell), v.stride, v.offset, vo.base, len(dPhidxoCell), vo.stride, vo.offset,
+        rs, precision, sign_mode)
+
+
+def FluxMassDolfynFaceLoop(mesh, dudx, dvdx, dwdx, dpdx, denCell, denBoundary, uCell, vCell, wCell, massFlux, p, ar,
+                           su, rface, small, counters, solveTurbEnergy, solveTurbDiss, solveVisc, solveEnthalpy,
+                           teCell, teBoundary, edCell, edBoundary, viseffCell, viseffBoundary, tCell, tBoundary):
+    """Mirror of cupcfd::fvm::FluxMassDolfynFaceLoop (MassKernels.h:48-81).
+    ``counters`` is an int32 array [icinl, icout, icsym, icwal] updated in
+    place; in/out arrays are updated in place. Returns an eCodes value."""
+    cnt = counters
+    ptrs = [C.c_void_p(cnt.ctypes.data + 4 * k) for k in range(4)]
+
+    def a(x):
+        return (_p(x), 0 if x is None else len(x))
+
+    args = [mesh.h]
+    for vv in (dudx, dvdx, dwdx, dpdx):
+        args += [_vec(vv), len(vv)]
+    for x in (denCell, denBoundary, uCell, vCell, wCell, massFlux, p, ar, su):
+        args += list(a(x))
+    args += [_p(rface), len(rface), float(small)] + ptrs
+    args += [int(bool(solveTurbEnergy)), int(bool(solveTurbDiss)), int(bool(solveVisc)), int(bool(solveEnthalpy))]
+    for x in (teCell, teBoundary, edCell, edBoundary, viseffCell, viseffBoundary, tCell, tBoundary):
+        args += list(a(x))
+    return lib().cupcfd_gpu_flux_mass_dolfyn_face_loop(*args)
+
+
+def forward_adjoint(mesh, precision, phi, phiB, den, u, v, w, gface, out=None):
+    """Forward + adjoint of the benchmark loss through host buffers.
+    Returns a dict of host FP64 arrays (grad (n,3), massFlux, phiBar,
+    phiBBar, denBar, uBar, vBar, wBar, loss)."""
+    nC, nF, nB = mesh.nCells, mesh.nFaces, mesh.nBoundaries
+    if out is None:
+        out = dict(grad=np.empty((nC, 3)), massFlux=np.empty(nF), phiBar=np.empty(nC), phiBBar=np.empty(nB),
+                   denBar=np.empty(nC), uBar=np.empty(nC), vBar=np.empty(nC), wBar=np.empty(nC), loss=np.empty(1))
+    check(lib().cupcfd_gpu_forward_adjoint(mesh.h, precision, _p(phi), _p(phiB), _p(den), _p(u), _p(v), _p(w), _p(gface),
+                                           *[_p(out[k]) for k in ("grad", "massFlux", "phiBar", "phiBBar", "denBar",
+                                                                  "uBar", "vBar", "wBar", "loss")]))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# device-resident calls (torch CUDA tensors, internal numbering)
+# ---------------------------------------------------------------------------
+def _es(prec):
+    return 8 if prec == PREC_F64 else 4
+
+
+def permute_cells(mesh, to_internal, src, dst, ncomp=1, stream=None):
+    check(lib().cupcfd_gpu_dev_permute_cells(mesh.h, int(bool(to_internal)), ncomp, _p(src), src.element_size(), 0,
+                                             _p(dst), dst.element_size(), 0, _stream(stream)))
+
+
+def permute_faces(mesh, to_internal, src, dst, stream=None):
+    check(lib().cupcfd_gpu_dev_permute_faces(mesh.h, int(bool(to_internal)), _p(src), src.element_size(), _p(dst),
+                                             dst.element_size(), _stream(stream)))
+
+
+def dev_gradient(mesh, precision, phi, phiB, grad, grad_o=None, nGradient=1, sign_mode=SIGN_REFERENCE, stream=None):
+    check(lib().cupcfd_gpu_dev_gradient(mesh.h, precision, nGradient, sign_mode, _p(phi), _p(phiB), _p(grad),
+                                        _p(grad_o), _stream(stream)))
+
+
+def dev_mass_plain(mesh, precision, state, mflux, stream=None):
+    check(lib().cupcfd_gpu_dev_mass_plain(mesh.h, precision, _p(state), _p(mflux), _stream(stream)))
+
+
+def dev_gradient_adjoint(mesh, precision, gbar, phiBar, phiBBar, sign_mode=SIGN_REFERENCE, stream=None):
+    check(lib().cupcfd_gpu_dev_gradient_adjoint(mesh.h, precision, sign_mode, _p(gbar), _p(phiBar), _p(phiBBar),
+                                                _stream(stream)))
+
+
+def dev_mass_plain_adjoint(mesh, precision, state, mbar, stateBar, stream=None):
+    check(lib().cupcfd_gpu_dev_mass_plain_adjoint(mesh.h, precision, _p(state), _p(mbar), _p(stateBar), _stream(stream)))
+
+
+def dev_forward(mesh, precision, phi, phiB, state, grad, mflux, gface=None, loss=None, stream=None):
+    check(lib().cupcfd_gpu_dev_forward(mesh.h, precision, _p(phi), _p(phiB), _p(state), _p(gface), _p(grad), _p(mflux),
+                                       _p(loss), _stream(stream)))
+
+
+def dev_adjoint(mesh, precision, grad, state, gface, phiBar, phiBBar, stateBar, stream=None):
+    check(lib().cupcfd_gpu_dev_adjoint(mesh.h, precision, _p(grad), _p(state), _p(gface), _p(phiBar), _p(phiBBar),
+                                       _p(stateBar), _stream(stream)))
+
+
+def dev_forward_adjoint(mesh, precision, phi, phiB, state, gface, grad, mflux, phiBar, phiBBar, stateBar, loss=None,
+                        stream=None):
+    check(lib().cupcfd_gpu_dev_forward_adjoint(mesh.h, precision, _p(phi), _p(phiB), _p(state), _p(gface), _p(grad),
+                                               _p(mflux), _p(phiBar), _p(phiBBar), _p(stateBar), _p(loss),
+                                               _stream(stream)))
+
+
+def error_norms(a, b, floor=0.0, stream=None):
+    """FP64 norms of device tensors a vs b: dict(max_abs, max_ref, rms_rel, max_rel_floor)."""
+    out = (C.c_double * 5)()
+    check(lib().cupcfd_gpu_dev_error_norms(_p(a), a.element_size(), _p(b), b.element_size(), a.numel(), float(floor),
+                                           out, _stream(stream)))
+    mx, mb, s2, b2, mr = list(out)
+    return dict(max_abs=mx, max_ref=mb, max_rel_norm=mx / mb if mb else 0.0,
+                rms_rel=(s2 / b2) ** 0.5 if b2 else 0.0, max_rel_floor=mr)

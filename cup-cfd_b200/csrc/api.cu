@@ -1,0 +1,693 @@
+// C ABI: reference-facing host-buffer calls and device-resident calls.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "kernels_adj.cuh"
+
+using namespace cupcfd_gpu;
+
+namespace {
+
+constexpr int BLK = 256;
+
+// scratch slots of a mesh (each grows on demand and is reused across calls)
+enum Slot {
+    S_ERR = 0, S_GEOM = 1, S_IN0, S_IN1, S_IN2, S_IN3, S_IN4, S_IN5, S_IN6, S_IN7,
+    S_OUT0, S_OUT1, S_OUT2, S_OUT3, S_OUT4, S_GO, S_LOSS, S_CNT, S_NORM
+};
+
+template <class T>
+int scratch(cupcfd_gpu_mesh *m, int slot, size_t n, T **p) {
+    void *v;
+    CG_TRY(m->scratchBuf(slot, n * sizeof(T), &v));
+    *p = (T *) v;
+    return CUPCFD_E_SUCCESS;
+}
+
+inline cudaStream_t as_stream(void *s) { return (cudaStream_t) s; }
+inline SellView sell(const cupcfd_gpu_mesh *m) { return SellView{m->sell.slicePtr, m->sell.inc}; }
+
+// ---------------------------------------------------------------------------
+// permutation kernels (gathers): dst[c][i] = src[c][map[i]]
+// ---------------------------------------------------------------------------
+template <class TS, class TD>
+__global__ void k_gather(int n, int ncomp, const int *__restrict__ map, const TS *__restrict__ src, int64_t ss,
+                         TD *__restrict__ dst, int64_t dsd) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int j = map ? map[i] : i;
+    for (int c = 0; c < ncomp; c++) dst[c * dsd + i] = (TD) src[c * ss + j];
+}
+
+// reference-order AoS [n][ncomp] (packed) -> internal component blocks
+template <class TS, class TD>
+__global__ void k_aos_to_blocks(int n, int ncomp, const int *__restrict__ n2o, const TS *__restrict__ src,
+                                TD *__restrict__ dst, int64_t ld) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int o = n2o[i];
+    for (int c = 0; c < ncomp; c++) dst[c * ld + i] = (TD) src[(int64_t) o * ncomp + c];
+}
+
+// internal component blocks -> reference-order AoS [n][ncomp]
+template <class TS, class TD>
+__global__ void k_blocks_to_aos(int n, int ncomp, const int *__restrict__ o2n, const TS *__restrict__ src, int64_t ld,
+                                TD *__restrict__ dst) {
+    int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= n) return;
+    int i = o2n[o];
+    for (int c = 0; c < ncomp; c++) dst[(int64_t) o * ncomp + c] = (TD) src[c * ld + i];
+}
+
+// float4 state <-> blocks
+__global__ void k_state_to_f4(int n, const int *__restrict__ n2o, const double *__restrict__ r, const double *__restrict__ u,
+                              const double *__restrict__ v, const double *__restrict__ w, float4 *__restrict__ out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int o = n2o[i];
+    out[i] = make_float4((float) r[o], (float) u[o], (float) v[o], (float) w[o]);
+}
+
+__global__ void k_f4_to_ref(int n, const int *__restrict__ o2n, const float4 *__restrict__ in, double *__restrict__ r,
+                            double *__restrict__ u, double *__restrict__ v, double *__restrict__ w) {
+    int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= n) return;
+    float4 s = in[o2n[o]];
+    r[o] = s.x; u[o] = s.y; v[o] = s.z; w[o] = s.w;
+}
+
+// face data internal -> reference (boundary entries zero when zeroBnd)
+template <class TS>
+__global__ void k_faces_to_ref(int nF, const int *__restrict__ o2n, const int2 *__restrict__ fcells, const TS *__restrict__ src,
+                               double *__restrict__ dst, int zeroBnd) {
+    int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= nF) return;
+    int i = o2n[o];
+    dst[o] = (zeroBnd && fcells[i].y < 0) ? 0.0 : (double) src[i];
+}
+
+template <class TS, class TD>
+__global__ void k_convert(int64_t n, const TS *__restrict__ a, TD *__restrict__ b) {
+    int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = (TD) a[i];
+}
+
+// rface pairs: dst[2i], dst[2i+1] = src[2 map[i]], src[2 map[i]+1]
+__global__ void k_gather_pairs(int n, const int *__restrict__ map, const double *__restrict__ src, double *__restrict__ dst) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int j = map[i];
+    dst[2 * (int64_t) i] = src[2 * (int64_t) j];
+    dst[2 * (int64_t) i + 1] = src[2 * (int64_t) j + 1];
+}
+
+int check_prec(const cupcfd_gpu_mesh *m, int precision) {
+    CG_RETURN_IF(precision != CUPCFD_PREC_F64 && precision != CUPCFD_PREC_F32C, CUPCFD_E_CONFIG_INVALID_VALUE,
+                 "unknown precision");
+    CG_RETURN_IF(!(m->precisions & (1 << precision)), CUPCFD_E_CONFIG_INVALID_VALUE,
+                 "the mesh was created without this precision's geometry");
+    return CUPCFD_E_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// one gradient iteration (device, internal numbering). corr: add the
+// non-orthogonal correction of the previous iterate `prev` (which must not
+// alias `grad`); gcopy (optional) receives a copy of the result.
+// ---------------------------------------------------------------------------
+int launch_grad_once(cupcfd_gpu_mesh *m, int precision, bool corr, bool sgn, const void *phi, const void *phiB,
+                     const void *prev, void *grad, void *gcopy, cudaStream_t st) {
+    int64_t ldc = m->nC;
+    unsigned grid = grid_for(m->nC, BLK);
+    if (precision == CUPCFD_PREC_F64) {
+        const double *pp = (const double *) phi, *pb = (const double *) phiB, *go = (const double *) prev;
+        double *g = (double *) grad, *gc = (double *) gcopy;
+        if (!corr && !sgn) k_grad_f64<false, false><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->faceCells, m->fg64, m->fc64, m->cc64, pp, pb, m->vol, go, g, gc, ldc);
+        else if (!corr && sgn) k_grad_f64<false, true><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->faceCells, m->fg64, m->fc64, m->cc64, pp, pb, m->vol, go, g, gc, ldc);
+        else if (corr && !sgn) k_grad_f64<true, false><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->faceCells, m->fg64, m->fc64, m->cc64, pp, pb, m->vol, go, g, gc, ldc);
+        else k_grad_f64<true, true><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->faceCells, m->fg64, m->fc64, m->cc64, pp, pb, m->vol, go, g, gc, ldc);
+    } else {
+        const float *pp = (const float *) phi, *pb = (const float *) phiB, *go = (const float *) prev;
+        float *g = (float *) grad, *gc = (float *) gcopy;
+        if (!corr && !sgn) k_grad_f32<false, false><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->faceCells, m->fg32, m->fc32, m->cc32, pp, pb, m->vol, go, g, gc, ldc);
+        else if (!corr && sgn) k_grad_f32<false, true><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->faceCells, m->fg32, m->fc32, m->cc32, pp, pb, m->vol, go, g, gc, ldc);
+        else if (corr && !sgn) k_grad_f32<true, false><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->faceCells, m->fg32, m->fc32, m->cc32, pp, pb, m->vol, go, g, gc, ldc);
+        else k_grad_f32<true, true><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->faceCells, m->fg32, m->fc32, m->cc32, pp, pb, m->vol, go, g, gc, ldc);
+    }
+    CG_LAUNCHED();
+    return CUPCFD_E_SUCCESS;
+}
+
+}  // namespace
+
+// ===========================================================================
+// device-resident calls
+// ===========================================================================
+extern "C" int cupcfd_gpu_dev_permute_cells(const cupcfd_gpu_mesh *m, int32_t to_internal, int32_t ncomp, const void *src,
+                                            int32_t src_size, int64_t src_cs, void *dst, int32_t dst_size, int64_t dst_cs,
+                                            void *stream) {
+    clear_error();
+    CG_RETURN_IF(!m || !src || !dst, CUPCFD_E_NULL_PTR, "permute_cells: null argument");
+    CG_RETURN_IF((src_size != 4 && src_size != 8) || (dst_size != 4 && dst_size != 8) || ncomp <= 0,
+                 CUPCFD_E_CONFIG_INVALID_VALUE, "permute_cells: element size must be 4 or 8");
+    CG_RETURN_IF(src == dst, CUPCFD_E_CONFIG_INVALID_VALUE, "permute_cells: in-place permutation is not supported");
+    int64_t ss = src_cs ? src_cs / src_size : m->nC, dsd = dst_cs ? dst_cs / dst_size : m->nC;
+    const int *map = to_internal ? m->cellN2O : m->cellO2N;
+    cudaStream_t st = as_stream(stream);
+    unsigned grid = grid_for(m->nC, BLK);
+    if (src_size == 8 && dst_size == 8) k_gather<double, double><<<grid, BLK, 0, st>>>(m->nC, ncomp, map, (const double *) src, ss, (double *) dst, dsd);
+    else if (src_size == 8) k_gather<double, float><<<grid, BLK, 0, st>>>(m->nC, ncomp, map, (const double *) src, ss, (float *) dst, dsd);
+    else if (dst_size == 8) k_gather<float, double><<<grid, BLK, 0, st>>>(m->nC, ncomp, map, (const float *) src, ss, (double *) dst, dsd);
+    else k_gather<float, float><<<grid, BLK, 0, st>>>(m->nC, ncomp, map, (const float *) src, ss, (float *) dst, dsd);
+    CG_LAUNCHED();
+    return CUPCFD_E_SUCCESS;
+}
+
+extern "C" int cupcfd_gpu_dev_permute_faces(const cupcfd_gpu_mesh *m, int32_t to_internal, const void *src, int32_t src_size,
+                                            void *dst, int32_t dst_size, void *stream) {
+    clear_error();
+    CG_RETURN_IF(!m || !src || !dst, CUPCFD_E_NULL_PTR, "permute_faces: null argument");
+    CG_RETURN_IF((src_size != 4 && src_size != 8) || (dst_size != 4 && dst_size != 8), CUPCFD_E_CONFIG_INVALID_VALUE,
+                 "permute_faces: element size must be 4 or 8");
+    CG_RETURN_IF(src == dst, CUPCFD_E_CONFIG_INVALID_VALUE, "permute_faces: in-place permutation is not supported");
+    const int *map = to_internal ? m->faceN2O : m->faceO2N;
+    cudaStream_t st = as_stream(stream);
+    unsigned grid = grid_for(m->nF, BLK);
+    if (src_size == 8 && dst_size == 8) k_gather<double, double><<<grid, BLK, 0, st>>>(m->nF, 1, map, (const double *) src, 0, (double *) dst, 0);
+    else if (src_size == 8) k_gather<double, float><<<grid, BLK, 0, st>>>(m->nF, 1, map, (const double *) src, 0, (float *) dst, 0);
+    else if (dst_size == 8) k_gather<float, double><<<grid, BLK, 0, st>>>(m->nF, 1, map, (const float *) src, 0, (double *) dst, 0);
+    else k_gather<float, float><<<grid, BLK, 0, st>>>(m->nF, 1, map, (const float *) src, 0, (float *) dst, 0);
+    CG_LAUNCHED();
+    return CUPCFD_E_SUCCESS;
+}
+
+extern "C" int cupcfd_gpu_dev_gradient(cupcfd_gpu_mesh *m, int32_t precision, int32_t nGradient, int32_t sign_mode,
+                                       const void *phi, const void *phiB, void *grad, void *grad_o, void *stream) {
+    clear_error();
+    CG_RETURN_IF(!m, CUPCFD_E_NULL_PTR, "dev_gradient: null mesh");
+    CG_TRY(check_prec(m, precision));
+    CG_RETURN_IF(sign_mode != CUPCFD_SIGN_REFERENCE && sign_mode != CUPCFD_SIGN_SIGNED, CUPCFD_E_CONFIG_INVALID_VALUE,
+                 "unknown sign_mode");
+    CG_RETURN_IF(!phi || !grad || (m->nB > 0 && !phiB), CUPCFD_E_NULL_PTR, "dev_gradient: null device pointer");
+    cudaStream_t st = as_stream(stream);
+    size_t es = precision == CUPCFD_PREC_F64 ? 8 : 4;
+    size_t bytes = 3 * (size_t) m->nC * es;
+    bool sgn = sign_mode == CUPCFD_SIGN_SIGNED;
+    if (nGradient <= 0) {
+        // GradientKernels.ipp:57-61: the previous-iterate array is zeroed, the gradient untouched
+        if (grad_o) CG_CHECK_CUDA(cudaMemsetAsync(grad_o, 0, bytes, st));
+        return CUPCFD_E_SUCCESS;
+    }
+    // first iteration: the previous iterate is zero, so the correction is exactly +0 and skipped
+    CG_TRY(launch_grad_once(m, precision, false, sgn, phi, phiB, nullptr, grad, nGradient == 1 ? grad_o : nullptr, st));
+    if (nGradient > 1) {
+        // later iterations read the previous iterate from a separate copy so
+        // no launch reads the buffer it writes
+        char *prev;
+        CG_TRY(scratch(m, S_GO, bytes, &prev));
+        for (int it = 1; it < nGradient; it++) {
+            CG_CHECK_CUDA(cudaMemcpyAsync(prev, grad, bytes, cudaMemcpyDeviceToDevice, st));
+            CG_TRY(launch_grad_once(m, precision, true, sgn, phi, phiB, prev, grad, nullptr, st));
+        }
+        if (grad_o) CG_CHECK_CUDA(cudaMemcpyAsync(grad_o, grad, bytes, cudaMemcpyDeviceToDevice, st));
+    }
+    return CUPCFD_E_SUCCESS;
+}
+
+extern "C" int cupcfd_gpu_dev_mass_plain(cupcfd_gpu_mesh *m, int32_t precision, const void *state, void *massFlux, void *stream) {
+    clear_error();
+    CG_RETURN_IF(!m || !state || !massFlux, CUPCFD_E_NULL_PTR, "dev_mass_plain: null argument");
+    CG_TRY(check_prec(m, precision));
+    cudaStream_t st = as_stream(stream);
+    if (precision == CUPCFD_PREC_F64)
+        k_mass_plain_f64<<<grid_for(m->nF, BLK), BLK, 0, st>>>(m->nF, m->faceCells, m->fg64, (const double *) state, m->nC, (double *) massFlux);
+    else
+        k_mass_plain_f32<<<grid_for(m->nF, BLK), BLK, 0, st>>>(m->nF, m->faceCells, m->fg32, (const float4 *) state, (float *) massFlux);
+    CG_LAUNCHED();
+    return CUPCFD_E_SUCCESS;
+}
+
+extern "C" int cupcfd_gpu_dev_gradient_adjoint(cupcfd_gpu_mesh *m, int32_t precision, int32_t sign_mode, const void *gbar,
+                                               void *phiBar, void *phiBBar, void *stream) {
+    clear_error();
+    CG_RETURN_IF(!m || !gbar || !phiBar || (m->nB > 0 && !phiBBar), CUPCFD_E_NULL_PTR, "dev_gradient_adjoint: null argument");
+    CG_TRY(check_prec(m, precision));
+    CG_RETURN_IF(sign_mode != CUPCFD_SIGN_REFERENCE && sign_mode != CUPCFD_SIGN_SIGNED, CUPCFD_E_CONFIG_INVALID_VALUE,
+                 "unknown sign_mode");
+    cudaStream_t st = as_stream(stream);
+    unsigned grid = grid_for(m->nC, BLK);
+    bool sgn = sign_mode == CUPCFD_SIGN_SIGNED;
+    if (precision == CUPCFD_PREC_F64) {
+        if (sgn) k_grad_adj_general<true, double><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->faceCells, m->fg64, nullptr, m->vol, (const double *) gbar, (double *) phiBar, (double *) phiBBar, m->nC);
+        else k_grad_adj_general<false, double><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->faceCells, m->fg64, nullptr, m->vol, (const double *) gbar, (double *) phiBar, (double *) phiBBar, m->nC);
+    } else {
+        if (sgn) k_grad_adj_general<true, float><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->faceCells, nullptr, m->fg32, m->vol, (const float *) gbar, (float *) phiBar, (float *) phiBBar, m->nC);
+        else k_grad_adj_general<false, float><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->faceCells, nullptr, m->fg32, m->vol, (const float *) gbar, (float *) phiBar, (float *) phiBBar, m->nC);
+    }
+    CG_LAUNCHED();
+    return CUPCFD_E_SUCCESS;
+}
+
+extern "C" int cupcfd_gpu_dev_mass_plain_adjoint(cupcfd_gpu_mesh *m, int32_t precision, const void *state, const void *mbar,
+                                                 void *stateBar, void *stream) {
+    clear_error();
+    CG_RETURN_IF(!m || !state || !mbar || !stateBar, CUPCFD_E_NULL_PTR, "dev_mass_plain_adjoint: null argument");
+    CG_TRY(check_prec(m, precision));
+    cudaStream_t st = as_stream(stream);
+    unsigned grid = grid_for(m->nC, BLK);
+    if (precision == CUPCFD_PREC_F64)
+        k_adj_f64<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->faceCells, m->fg64, nullptr, 0.0, (const double *) state,
+                                        (const double *) mbar, nullptr, nullptr, (double *) stateBar, m->nC);
+    else
+        k_adj_f32<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->faceCells, m->fg32, nullptr, 0.f, (const float4 *) state,
+                                        (const float *) mbar, nullptr, nullptr, (float4 *) stateBar, m->nC);
+    CG_LAUNCHED();
+    return CUPCFD_E_SUCCESS;
+}
+
+extern "C" int cupcfd_gpu_dev_forward(cupcfd_gpu_mesh *m, int32_t precision, const void *phi, const void *phiB,
+                                      const void *state, const void *gface, void *grad, void *massFlux, double *loss,
+                                      void *stream) {
+    clear_error();
+    CG_RETURN_IF(!m || !phi || !state || !grad || !massFlux || (m->nB > 0 && !phiB), CUPCFD_E_NULL_PTR,
+                 "dev_forward: null argument");
+    CG_RETURN_IF((gface == nullptr) != (loss == nullptr), CUPCFD_E_NULL_PTR, "dev_forward: gface and loss go together");
+    CG_TRY(check_prec(m, precision));
+    cudaStream_t st = as_stream(stream);
+    unsigned grid = grid_for(m->nC, BLK);
+    double *part = nullptr;
+    if (loss) CG_TRY(scratch(m, S_LOSS, grid, &part));
+    if (precision == CUPCFD_PREC_F64)
+        k_fwd_f64<BLK><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->faceCells, m->fg64, (const double *) phi, (const double *) phiB,
+                                             m->vol, (const double *) state, (const double *) gface, (double *) grad,
+                                             (double *) massFlux, part, m->nC);
+    else
+        k_fwd_f32<BLK><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->faceCells, m->fg32, (const float *) phi, (const float *) phiB,
+                                             m->vol, (const float4 *) state, (const float *) gface, (float *) grad,
+                                             (float *) massFlux, part, m->nC);
+    CG_LAUNCHED();
+    if (loss) {
+        k_reduce_partials<<<1, 1024, 0, st>>>((int) grid, part, loss);
+        CG_LAUNCHED();
+    }
+    return CUPCFD_E_SUCCESS;
+}
+
+extern "C" int cupcfd_gpu_dev_adjoint(cupcfd_gpu_mesh *m, int32_t precision, const void *grad, const void *state,
+                                      const void *gface, void *phiBar, void *phiBBar, void *stateBar, void *stream) {
+    clear_error();
+    CG_RETURN_IF(!m || !grad || !state || !gface || !phiBar || !stateBar || (m->nB > 0 && !phiBBar), CUPCFD_E_NULL_PTR,
+                 "dev_adjoint: null argument");
+    CG_TRY(check_prec(m, precision));
+    cudaStream_t st = as_stream(stream);
+    unsigned grid = grid_for(m->nC, BLK);
+    if (precision == CUPCFD_PREC_F64)
+        k_adj_f64<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->faceCells, m->fg64, (const double *) grad, 2.0, (const double *) state,
+                                        (const double *) gface, (double *) phiBar, (double *) phiBBar, (double *) stateBar, m->nC);
+    else
+        k_adj_f32<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->faceCells, m->fg32, (const float *) grad, 2.f, (const float4 *) state,
+                                        (const float *) gface, (float *) phiBar, (float *) phiBBar, (float4 *) stateBar, m->nC);
+    CG_LAUNCHED();
+    return CUPCFD_E_SUCCESS;
+}
+
+extern "C" int cupcfd_gpu_dev_forward_adjoint(cupcfd_gpu_mesh *m, int32_t precision, const void *phi, const void *phiB,
+                                              const void *state, const void *gface, void *grad, void *massFlux,
+                                              void *phiBar, void *phiBBar, void *stateBar, double *loss, void *stream) {
+    clear_error();
+    CG_RETURN_IF(!m || !gface, CUPCFD_E_NULL_PTR, "dev_forward_adjoint: null argument");
+    double *lp = loss;
+    if (!lp) CG_TRY(scratch(m, S_NORM, 1, &lp));
+    CG_TRY(cupcfd_gpu_dev_forward(m, precision, phi, phiB, state, gface, grad, massFlux, lp, stream));
+    return cupcfd_gpu_dev_adjoint(m, precision, grad, state, gface, phiBar, phiBBar, stateBar, stream);
+}
+
+// ---------------------------------------------------------------------------
+// error norms (FP64)
+// ---------------------------------------------------------------------------
+namespace {
+template <class TA, class TB>
+__global__ void k_norms(int64_t n, const TA *__restrict__ a, const TB *__restrict__ b, double floor, double *__restrict__ part) {
+    __shared__ double sh[5][256 / 32];
+    double mx = 0, mb = 0, s2 = 0, b2 = 0, mr = 0;
+    for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x) {
+        double x = (double) a[i], y = (double) b[i], d = fabs(x - y);
+        mx = fmax(mx, d);
+        mb = fmax(mb, fabs(y));
+        s2 += d * d;
+        b2 += y * y;
+        mr = fmax(mr, d / fmax(fabs(y), floor));
+    }
+    for (int k = 16; k > 0; k >>= 1) {
+        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, k));
+        mb = fmax(mb, __shfl_xor_sync(0xffffffffu, mb, k));
+        s2 += __shfl_xor_sync(0xffffffffu, s2, k);
+        b2 += __shfl_xor_sync(0xffffffffu, b2, k);
+        mr = fmax(mr, __shfl_xor_sync(0xffffffffu, mr, k));
+    }
+    int wq = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) { sh[0][wq] = mx; sh[1][wq] = mb; sh[2][wq] = s2; sh[3][wq] = b2; sh[4][wq] = mr; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r[5] = {0, 0, 0, 0, 0};
+        for (int i = 0; i < (int) blockDim.x / 32; i++) {
+            r[0] = fmax(r[0], sh[0][i]); r[1] = fmax(r[1], sh[1][i]);
+            r[2] += sh[2][i]; r[3] += sh[3][i]; r[4] = fmax(r[4], sh[4][i]);
+        }
+        for (int k = 0; k < 5; k++) part[5 * blockIdx.x + k] = r[k];
+    }
+}
+}  // namespace
+
+extern "C" int cupcfd_gpu_dev_error_norms(const void *a, int32_t as, const void *b, int32_t bs, int64_t n, double floor,
+                                          double *out, void *stream) {
+    clear_error();
+    CG_RETURN_IF(!a || !b || !out, CUPCFD_E_NULL_PTR, "error_norms: null argument");
+    CG_RETURN_IF((as != 4 && as != 8) || (bs != 4 && bs != 8), CUPCFD_E_CONFIG_INVALID_VALUE, "error_norms: size 4 or 8");
+    cudaStream_t st = as_stream(stream);
+    const int blocks = 592;
+    double *part;
+    CG_CHECK_CUDA(cudaMallocAsync((void **) &part, sizeof(double) * 5 * blocks, st));
+    if (as == 8 && bs == 8) k_norms<double, double><<<blocks, 256, 0, st>>>(n, (const double *) a, (const double *) b, floor, part);
+    else if (as == 8) k_norms<double, float><<<blocks, 256, 0, st>>>(n, (const double *) a, (const float *) b, floor, part);
+    else if (bs == 8) k_norms<float, double><<<blocks, 256, 0, st>>>(n, (const float *) a, (const double *) b, floor, part);
+    else k_norms<float, float><<<blocks, 256, 0, st>>>(n, (const float *) a, (const float *) b, floor, part);
+    CG_LAUNCHED();
+    std::vector<double> h(5 * blocks);
+    CG_CHECK_CUDA(cudaMemcpyAsync(h.data(), part, sizeof(double) * 5 * blocks, cudaMemcpyDeviceToHost, st));
+    CG_CHECK_CUDA(cudaFreeAsync(part, st));
+    CG_CHECK_CUDA(cudaStreamSynchronize(st));
+    double r[5] = {0, 0, 0, 0, 0};
+    for (int i = 0; i < blocks; i++) {
+        r[0] = std::max(r[0], h[5 * i]); r[1] = std::max(r[1], h[5 * i + 1]);
+        r[2] += h[5 * i + 2]; r[3] += h[5 * i + 3]; r[4] = std::max(r[4], h[5 * i + 4]);
+    }
+    for (int k = 0; k < 5; k++) out[k] = r[k];
+    return CUPCFD_E_SUCCESS;
+}
+
+// ===========================================================================
+// reference-facing calls (host buffers)
+// ===========================================================================
+namespace {
+
+int h2d_real(cupcfd_gpu_mesh *m, int slot, const void *h, int64_t n, int rs, void **dptr) {
+    void *d;
+    CG_TRY(m->scratchBuf(slot, (size_t) std::max<int64_t>(n, 1) * rs, &d));
+    if (n > 0) CG_CHECK_CUDA(cudaMemcpyAsync(d, h, (size_t) n * rs, cudaMemcpyHostToDevice, m->stream));
+    *dptr = d;
+    return CUPCFD_E_SUCCESS;
+}
+
+// strided host vec3 view -> packed device [3n] of rs bytes
+int h2d_vec3(cupcfd_gpu_mesh *m, int slot, const cupcfd_vec3_view &v, int64_t n, int rs, void **dptr) {
+    CG_RETURN_IF(!v.base, CUPCFD_E_NULL_PTR, "null vector array");
+    CG_RETURN_IF(v.stride < 3 * rs || v.offset < 0, CUPCFD_E_CONFIG_INVALID_VALUE, "vector view: bad stride/offset");
+    void *d;
+    CG_TRY(m->scratchBuf(slot, (size_t) std::max<int64_t>(n, 1) * 3 * rs, &d));
+    if (n > 0)
+        CG_CHECK_CUDA(cudaMemcpy2DAsync(d, 3 * rs, (const char *) v.base + v.offset, (size_t) v.stride, 3 * rs, (size_t) n,
+                                        cudaMemcpyHostToDevice, m->stream));
+    *dptr = d;
+    return CUPCFD_E_SUCCESS;
+}
+
+// packed device [3n] of rs bytes -> strided host vec3 view
+int d2h_vec3(cupcfd_gpu_mesh *m, const void *d, void *base, int stride, int offset, int64_t n, int rs) {
+    if (n <= 0) return CUPCFD_E_SUCCESS;
+    CG_CHECK_CUDA(cudaMemcpy2DAsync((char *) base + offset, (size_t) stride, d, 3 * rs, 3 * rs, (size_t) n,
+                                    cudaMemcpyDeviceToHost, m->stream));
+    return CUPCFD_E_SUCCESS;
+}
+
+void zero_vec3_tail(void *base, int stride, int offset, int from, int to, int rs) {
+    for (int i = from; i < to; i++) std::memset((char *) base + (size_t) i * stride + offset, 0, 3 * rs);
+}
+
+}  // namespace
+
+extern "C" int cupcfd_gpu_gradient_phi_gauss_dolfyn(cupcfd_gpu_mesh *m, int32_t nGradient, const void *phiCell, int32_t nPhiCell,
+                                                    const void *phiBoundary, int32_t nPhiBoundary, void *dPhidxCell,
+                                                    int32_t nDPhidxCell, int32_t stride, int32_t offset, void *dPhidxoCell,
+                                                    int32_t nDPhidxoCell, int32_t strideo, int32_t offseto,
+                                                    int32_t rs, int32_t precision, int32_t sign_mode) {
+    clear_error();
+    CG_RETURN_IF(!m || !phiCell || !dPhidxCell || !dPhidxoCell || (m->nB > 0 && !phiBoundary), CUPCFD_E_NULL_PTR,
+                 "GradientPhiGaussDolfyn: null argument");
+    CG_RETURN_IF(rs != 4 && rs != 8, CUPCFD_E_CONFIG_INVALID_VALUE, "GradientPhiGaussDolfyn: real_size must be 4 or 8");
+    CG_RETURN_IF(stride < 3 * rs || strideo < 3 * rs || offset < 0 || offseto < 0, CUPCFD_E_CONFIG_INVALID_VALUE,
+                 "GradientPhiGaussDolfyn: bad vector stride/offset");
+    CG_TRY(check_prec(m, precision));
+    // the reference reads phiCell[ip/in], phiBoundary[ib] and updates dPhidxCell[0..lTCells)
+    // (GradientKernels.ipp:90-95,107-111,122-126); short arrays are index errors
+    CG_RETURN_IF(nPhiCell < m->nC || nPhiBoundary < m->nB || nDPhidxCell < m->nC || nDPhidxoCell < 0 ||
+                     nDPhidxoCell > nDPhidxCell,
+                 CUPCFD_E_INVALID_INDEX, "GradientPhiGaussDolfyn: array shorter than the mesh needs");
+    CG_TRY(make_device_current(m->device));
+    cudaStream_t st = m->stream;
+    int nC = m->nC;
+    if (nGradient <= 0) {
+        // dPhidxoCell zeroed, dPhidxCell untouched (GradientKernels.ipp:57-61)
+        zero_vec3_tail(dPhidxoCell, strideo, offseto, 0, nDPhidxoCell, rs);
+        return CUPCFD_E_SUCCESS;
+    }
+    size_t es = precision == CUPCFD_PREC_F64 ? 8 : 4;
+    void *dphiRef, *dphibRef;
+    CG_TRY(h2d_real(m, S_IN0, phiCell, nC, rs, &dphiRef));
+    CG_TRY(h2d_real(m, S_IN1, phiBoundary, m->nB, rs, &dphibRef));
+    void *phi, *phib, *grad, *out;
+    CG_TRY(m->scratchBuf(S_IN2, (size_t) nC * es, &phi));
+    CG_TRY(m->scratchBuf(S_IN3, (size_t) std::max(m->nB, 1) * es, &phib));
+    CG_TRY(m->scratchBuf(S_OUT0, 3 * (size_t) nC * es, &grad));
+    CG_TRY(m->scratchBuf(S_OUT1, 3 * (size_t) nC * rs, &out));
+    CG_TRY(cupcfd_gpu_dev_permute_cells(m, 1, 1, dphiRef, rs, 0, phi, (int) es, 0, st));
+    if (m->nB > 0) {
+        if ((size_t) rs == es) CG_CHECK_CUDA(cudaMemcpyAsync(phib, dphibRef, (size_t) m->nB * es, cudaMemcpyDeviceToDevice, st));
+        else if (rs == 8) { k_convert<double, float><<<grid_for(m->nB, BLK), BLK, 0, st>>>(m->nB, (const double *) dphibRef, (float *) phib); CG_LAUNCHED(); }
+        else { k_convert<float, double><<<grid_for(m->nB, BLK), BLK, 0, st>>>(m->nB, (const float *) dphibRef, (double *) phib); CG_LAUNCHED(); }
+    }
+    CG_TRY(cupcfd_gpu_dev_gradient(m, precision, nGradient, sign_mode, phi, phib, grad, nullptr, st));
+    unsigned grid = grid_for(nC, BLK);
+    if (es == 8 && rs == 8) k_blocks_to_aos<double, double><<<grid, BLK, 0, st>>>(nC, 3, m->cellO2N, (const double *) grad, nC, (double *) out);
+    else if (es == 8) k_blocks_to_aos<double, float><<<grid, BLK, 0, st>>>(nC, 3, m->cellO2N, (const double *) grad, nC, (float *) out);
+    else if (rs == 8) k_blocks_to_aos<float, double><<<grid, BLK, 0, st>>>(nC, 3, m->cellO2N, (const float *) grad, nC, (double *) out);
+    else k_blocks_to_aos<float, float><<<grid, BLK, 0, st>>>(nC, 3, m->cellO2N, (const float *) grad, nC, (float *) out);
+    CG_LAUNCHED();
+    CG_TRY(d2h_vec3(m, out, dPhidxCell, stride, offset, nC, rs));
+    CG_TRY(d2h_vec3(m, out, dPhidxoCell, strideo, offseto, std::min(nC, nDPhidxoCell), rs));
+    CG_CHECK_CUDA(cudaStreamSynchronize(st));
+    // entries past lTCells: zeroed by the reset loop, copied into dPhidxoCell (:66-70, :129-131)
+    zero_vec3_tail(dPhidxCell, stride, offset, nC, nDPhidxCell, rs);
+    zero_vec3_tail(dPhidxoCell, strideo, offseto, nC, nDPhidxoCell, rs);
+    return CUPCFD_E_SUCCESS;
+}
+
+extern "C" int cupcfd_gpu_flux_mass_dolfyn_face_loop(
+    cupcfd_gpu_mesh *m, cupcfd_vec3_view dudx, int32_t nDudx, cupcfd_vec3_view dvdx, int32_t nDvdx, cupcfd_vec3_view dwdx,
+    int32_t nDwdx, cupcfd_vec3_view dpdx, int32_t nDpdx, const double *den, int32_t nDen, double *denB, int32_t nDenB,
+    const double *u, int32_t nU, const double *v, int32_t nV, const double *w, int32_t nW, double *massFlux,
+    int32_t nMassFlux, const double *p, int32_t nP, const double *ar, int32_t nAr, double *su, int32_t nSu, double *rface,
+    int32_t nRFace, double small, int32_t *icinl, int32_t *icout, int32_t *icsym, int32_t *icwal, int32_t solveTurbEnergy,
+    int32_t solveTurbDiss, int32_t solveVisc, int32_t solveEnthalpy, const double *teC, int32_t nTeC, double *teB,
+    int32_t nTeB, const double *edC, int32_t nEdC, double *edB, int32_t nEdB, const double *visC, int32_t nVisC,
+    double *visB, int32_t nVisB, const double *tC, int32_t nTC, double *tB, int32_t nTB) {
+    clear_error();
+    CG_RETURN_IF(!m || !den || !u || !v || !w || !massFlux || !p || !ar || !su || !rface || !icinl || !icout || !icsym ||
+                     !icwal,
+                 CUPCFD_E_NULL_PTR, "FluxMassDolfynFaceLoop: null argument");
+    CG_TRY(check_prec(m, CUPCFD_PREC_F64));
+    int nC = m->nC, nF = m->nF, nB = m->nB;
+    // index checks of the reference's DEBUG build (MassKernels.ipp:101-138, 203-245)
+    CG_RETURN_IF(nDudx < nC || nDvdx < nC || nDwdx < nC || nDpdx < nC || nDen < nC || nU < nC || nV < nC || nW < nC ||
+                     nP < nC || nAr < nC || nSu < nC || nMassFlux < nF || nRFace < 2 * nF || nDenB < nB,
+                 CUPCFD_E_INVALID_INDEX, "FluxMassDolfynFaceLoop: array shorter than the mesh needs");
+    bool anyOutlet = false, anyInlet = false;
+    for (int t : m->hRegionType) { anyOutlet |= t == CUPCFD_RTYPE_OUTLET; anyInlet |= t == CUPCFD_RTYPE_INLET; }
+    const double *bcI[4] = {teC, edC, visC, tC};
+    double *bcO[4] = {teB, edB, visB, tB};
+    int nbcI[4] = {nTeC, nEdC, nVisC, nTC}, nbcO[4] = {nTeB, nEdB, nVisB, nTB};
+    int flags = (solveTurbEnergy ? 1 : 0) | (solveTurbDiss ? 2 : 0) | (solveVisc ? 4 : 0) | (solveEnthalpy ? 8 : 0);
+    if (anyOutlet)
+        for (int q = 0; q < 4; q++)
+            if (flags & (1 << q)) {
+                CG_RETURN_IF(!bcI[q] || !bcO[q], CUPCFD_E_NULL_PTR, "FluxMassDolfynFaceLoop: null boundary-copy array");
+                CG_RETURN_IF(nbcI[q] < nC || nbcO[q] < nB, CUPCFD_E_INVALID_INDEX, "FluxMassDolfynFaceLoop: boundary-copy array too short");
+            }
+    CG_TRY(make_device_current(m->device));
+    cudaStream_t st = m->stream;
+    int64_t ldc = nC;
+    unsigned gC = grid_for(nC, BLK), gF = grid_for(nF, BLK);
+    // gradients: four packed [3nC] reference arrays -> 12 internal blocks
+    double *grads, *cs, *mf, *rf, *suD, *tmp, *bcIn = nullptr, *bcOut = nullptr, *denBD;
+    int *cnt;
+    CG_TRY(scratch(m, S_IN0, 12 * (size_t) nC, &grads));
+    CG_TRY(scratch(m, S_IN1, 6 * (size_t) nC, &cs));
+    CG_TRY(scratch(m, S_IN2, 3 * (size_t) std::max(nC, 2 * nF), &tmp));
+    CG_TRY(scratch(m, S_OUT0, (size_t) nF, &mf));
+    CG_TRY(scratch(m, S_OUT1, 2 * (size_t) nF, &rf));
+    CG_TRY(scratch(m, S_OUT2, (size_t) nC, &suD));
+    CG_TRY(scratch(m, S_OUT3, (size_t) std::max(nB, 1), &denBD));
+    CG_TRY(scratch(m, S_CNT, 4, &cnt));
+    cupcfd_vec3_view vv[4] = {dudx, dvdx, dwdx, dpdx};
+    for (int q = 0; q < 4; q++) {
+        void *d;
+        CG_TRY(h2d_vec3(m, S_IN3, vv[q], nC, 8, &d));
+        k_aos_to_blocks<double, double><<<gC, BLK, 0, st>>>(nC, 3, m->cellN2O, (const double *) d, grads + 3 * q * ldc, ldc);
+        CG_LAUNCHED();
+    }
+    const double *cin[6] = {den, u, v, w, p, ar};
+    for (int q = 0; q < 6; q++) {
+        CG_CHECK_CUDA(cudaMemcpyAsync(tmp, cin[q], sizeof(double) * nC, cudaMemcpyHostToDevice, st));
+        k_gather<double, double><<<gC, BLK, 0, st>>>(nC, 1, m->cellN2O, tmp, 0, cs + q * ldc, 0);
+        CG_LAUNCHED();
+    }
+    // in/out arrays: massFlux, rface (faces), su (cells), denB (boundaries)
+    CG_CHECK_CUDA(cudaMemcpyAsync(tmp, massFlux, sizeof(double) * nF, cudaMemcpyHostToDevice, st));
+    k_gather<double, double><<<gF, BLK, 0, st>>>(nF, 1, m->faceN2O, tmp, 0, mf, 0);
+    CG_LAUNCHED();
+    CG_CHECK_CUDA(cudaMemcpyAsync(tmp, rface, sizeof(double) * 2 * nF, cudaMemcpyHostToDevice, st));
+    k_gather_pairs<<<gF, BLK, 0, st>>>(nF, m->faceN2O, tmp, rf);
+    CG_LAUNCHED();
+    if (anyInlet) {
+        CG_CHECK_CUDA(cudaMemcpyAsync(tmp, su, sizeof(double) * nC, cudaMemcpyHostToDevice, st));
+        k_gather<double, double><<<gC, BLK, 0, st>>>(nC, 1, m->cellN2O, tmp, 0, suD, 0);
+        CG_LAUNCHED();
+    }
+    if (anyOutlet && nB > 0) {
+        CG_CHECK_CUDA(cudaMemcpyAsync(denBD, denB, sizeof(double) * nB, cudaMemcpyHostToDevice, st));
+        if (flags) {
+            CG_TRY(scratch(m, S_IN4, 4 * (size_t) nC, &bcIn));
+            CG_TRY(scratch(m, S_OUT4, 4 * (size_t) nB, &bcOut));
+            for (int q = 0; q < 4; q++) {
+                if (!(flags & (1 << q))) continue;
+                CG_CHECK_CUDA(cudaMemcpyAsync(tmp, bcI[q], sizeof(double) * nC, cudaMemcpyHostToDevice, st));
+                k_gather<double, double><<<gC, BLK, 0, st>>>(nC, 1, m->cellN2O, tmp, 0, bcIn + q * ldc, 0);
+                CG_LAUNCHED();
+                CG_CHECK_CUDA(cudaMemcpyAsync(bcOut + (size_t) q * nB, bcO[q], sizeof(double) * nB, cudaMemcpyHostToDevice, st));
+            }
+        }
+    }
+    CG_CHECK_CUDA(cudaMemsetAsync(cnt, 0, 4 * sizeof(int), st));
+    k_mass_full_f64<<<gF, BLK, 0, st>>>(nF, m->faceCells, m->fg64, m->fc64, m->fxp64, m->fxn64, m->cc64, m->vol, grads, cs, ldc,
+                                        m->bndRegion, m->regionType, m->regionUVW, m->regionDen, small, flags, mf, rf, denBD,
+                                        bcIn, bcOut, nB, cnt);
+    CG_LAUNCHED();
+    if (anyInlet) {
+        k_inlet_su<<<gC, BLK, 0, st>>>(nC, sell(m), m->faceCells, m->bndRegion, m->regionType, mf, suD);
+        CG_LAUNCHED();
+    }
+    // back to reference numbering and to the host
+    double *hmf, *hrf;
+    CG_TRY(scratch(m, S_IN5, (size_t) nF, &hmf));
+    CG_TRY(scratch(m, S_IN6, 2 * (size_t) nF, &hrf));
+    k_gather<double, double><<<gF, BLK, 0, st>>>(nF, 1, m->faceO2N, mf, 0, hmf, 0);
+    CG_LAUNCHED();
+    k_gather_pairs<<<gF, BLK, 0, st>>>(nF, m->faceO2N, rf, hrf);
+    CG_LAUNCHED();
+    CG_CHECK_CUDA(cudaMemcpyAsync(massFlux, hmf, sizeof(double) * nF, cudaMemcpyDeviceToHost, st));
+    CG_CHECK_CUDA(cudaMemcpyAsync(rface, hrf, sizeof(double) * 2 * nF, cudaMemcpyDeviceToHost, st));
+    if (anyInlet) {
+        k_gather<double, double><<<gC, BLK, 0, st>>>(nC, 1, m->cellO2N, suD, 0, tmp, 0);
+        CG_LAUNCHED();
+        CG_CHECK_CUDA(cudaMemcpyAsync(su, tmp, sizeof(double) * nC, cudaMemcpyDeviceToHost, st));
+    }
+    if (anyOutlet && nB > 0) {
+        CG_CHECK_CUDA(cudaMemcpyAsync(denB, denBD, sizeof(double) * nB, cudaMemcpyDeviceToHost, st));
+        for (int q = 0; q < 4; q++)
+            if (flags & (1 << q))
+                CG_CHECK_CUDA(cudaMemcpyAsync(bcO[q], bcOut + (size_t) q * nB, sizeof(double) * nB, cudaMemcpyDeviceToHost, st));
+    }
+    int hc[4];
+    CG_CHECK_CUDA(cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, st));
+    CG_CHECK_CUDA(cudaStreamSynchronize(st));
+    *icinl += hc[0]; *icout += hc[1]; *icsym += hc[2]; *icwal += hc[3];
+    return CUPCFD_E_SUCCESS;
+}
+
+extern "C" int cupcfd_gpu_forward_adjoint(cupcfd_gpu_mesh *m, int32_t precision, const double *phi, const double *phiB,
+                                          const double *den, const double *u, const double *v, const double *w,
+                                          const double *gface, double *grad, double *massFlux, double *phiBar,
+                                          double *phiBBar, double *denBar, double *uBar, double *vBar, double *wBar,
+                                          double *loss) {
+    clear_error();
+    CG_RETURN_IF(!m || !phi || !den || !u || !v || !w || !gface || (m->nB > 0 && !phiB), CUPCFD_E_NULL_PTR,
+                 "forward_adjoint: null input");
+    CG_TRY(check_prec(m, precision));
+    CG_TRY(make_device_current(m->device));
+    cudaStream_t st = m->stream;
+    int nC = m->nC, nF = m->nF, nB = m->nB;
+    int64_t ldc = nC;
+    unsigned gC = grid_for(nC, BLK), gF = grid_for(nF, BLK);
+    bool f64 = precision == CUPCFD_PREC_F64;
+    size_t es = f64 ? 8 : 4;
+    // host -> device (reference numbering, FP64)
+    double *in;
+    void *phiI, *phibI, *stI, *gI, *gradI, *mfI, *pbI, *pbbI, *sbI;
+    CG_TRY(scratch(m, S_IN0, 5 * (size_t) nC + nB + nF, &in));
+    double *hPhi = in, *hR = in + nC, *hU = in + 2 * (size_t) nC, *hV = in + 3 * (size_t) nC, *hW = in + 4 * (size_t) nC;
+    double *hPb = in + 5 * (size_t) nC, *hG = hPb + nB;
+    CG_CHECK_CUDA(cudaMemcpyAsync(hPhi, phi, 8 * (size_t) nC, cudaMemcpyHostToDevice, st));
+    CG_CHECK_CUDA(cudaMemcpyAsync(hR, den, 8 * (size_t) nC, cudaMemcpyHostToDevice, st));
+    CG_CHECK_CUDA(cudaMemcpyAsync(hU, u, 8 * (size_t) nC, cudaMemcpyHostToDevice, st));
+    CG_CHECK_CUDA(cudaMemcpyAsync(hV, v, 8 * (size_t) nC, cudaMemcpyHostToDevice, st));
+    CG_CHECK_CUDA(cudaMemcpyAsync(hW, w, 8 * (size_t) nC, cudaMemcpyHostToDevice, st));
+    if (nB > 0) CG_CHECK_CUDA(cudaMemcpyAsync(hPb, phiB, 8 * (size_t) nB, cudaMemcpyHostToDevice, st));
+    CG_CHECK_CUDA(cudaMemcpyAsync(hG, gface, 8 * (size_t) nF, cudaMemcpyHostToDevice, st));
+    // internal numbering, compute precision
+    CG_TRY(m->scratchBuf(S_IN1, (size_t) nC * es, &phiI));
+    CG_TRY(m->scratchBuf(S_IN2, (size_t) std::max(nB, 1) * es, &phibI));
+    CG_TRY(m->scratchBuf(S_IN3, 4 * (size_t) nC * es, &stI));
+    CG_TRY(m->scratchBuf(S_IN4, (size_t) nF * es, &gI));
+    CG_TRY(m->scratchBuf(S_OUT0, 3 * (size_t) nC * es, &gradI));
+    CG_TRY(m->scratchBuf(S_OUT1, (size_t) nF * es, &mfI));
+    CG_TRY(m->scratchBuf(S_OUT2, (size_t) nC * es, &pbI));
+    CG_TRY(m->scratchBuf(S_OUT3, (size_t) std::max(nB, 1) * es, &pbbI));
+    CG_TRY(m->scratchBuf(S_OUT4, 4 * (size_t) nC * es, &sbI));
+    double *dloss;
+    CG_TRY(scratch(m, S_NORM, 1, &dloss));
+    if (f64) {
+        k_gather<double, double><<<gC, BLK, 0, st>>>(nC, 1, m->cellN2O, hPhi, 0, (double *) phiI, 0);
+        k_gather<double, double><<<gC, BLK, 0, st>>>(nC, 4, m->cellN2O, hR, nC, (double *) stI, ldc);
+        if (nB > 0) CG_CHECK_CUDA(cudaMemcpyAsync(phibI, hPb, 8 * (size_t) nB, cudaMemcpyDeviceToDevice, st));
+        k_gather<double, double><<<gF, BLK, 0, st>>>(nF, 1, m->faceN2O, hG, 0, (double *) gI, 0);
+    } else {
+        k_gather<double, float><<<gC, BLK, 0, st>>>(nC, 1, m->cellN2O, hPhi, 0, (float *) phiI, 0);
+        k_state_to_f4<<<gC, BLK, 0, st>>>(nC, m->cellN2O, hR, hU, hV, hW, (float4 *) stI);
+        if (nB > 0) k_convert<double, float><<<grid_for(nB, BLK), BLK, 0, st>>>(nB, hPb, (float *) phibI);
+        k_gather<double, float><<<gF, BLK, 0, st>>>(nF, 1, m->faceN2O, hG, 0, (float *) gI, 0);
+    }
+    g_launches.fetch_add(4);
+    CG_CHECK_CUDA(cudaGetLastError());
+    CG_TRY(cupcfd_gpu_dev_forward_adjoint(m, precision, phiI, phibI, stI, gI, gradI, mfI, pbI, pbbI, sbI, dloss, st));
+    // back to reference numbering (FP64) and to the host
+    double *out;
+    CG_TRY(scratch(m, S_IN5, 8 * (size_t) nC + nF + nB, &out));
+    double *oG = out, *oMf = out + 3 * (size_t) nC, *oPb = oMf + nF, *oR = oPb + nC, *oU = oR + nC, *oV = oU + nC,
+           *oW = oV + nC, *oPbb = oW + nC;
+    if (f64) {
+        k_blocks_to_aos<double, double><<<gC, BLK, 0, st>>>(nC, 3, m->cellO2N, (const double *) gradI, ldc, oG);
+        k_faces_to_ref<double><<<gF, BLK, 0, st>>>(nF, m->faceO2N, m->faceCells, (const double *) mfI, oMf, 1);
+        k_gather<double, double><<<gC, BLK, 0, st>>>(nC, 1, m->cellO2N, (const double *) pbI, 0, oPb, 0);
+        k_gather<double, double><<<gC, BLK, 0, st>>>(nC, 4, m->cellO2N, (const double *) sbI, ldc, oR, nC);
+        if (nB > 0) CG_CHECK_CUDA(cudaMemcpyAsync(oPbb, pbbI, 8 * (size_t) nB, cudaMemcpyDeviceToDevice, st));
+    } else {
+        k_blocks_to_aos<float, double><<<gC, BLK, 0, st>>>(nC, 3, m->cellO2N, (const float *) gradI, ldc, oG);
+        k_faces_to_ref<float><<<gF, BLK, 0, st>>>(nF, m->faceO2N, m->faceCells, (const float *) mfI, oMf, 1);
+        k_gather<float, double><<<gC, BLK, 0, st>>>(nC, 1, m->cellO2N, (const float *) pbI, 0, oPb, 0);
+        k_f4_to_ref<<<gC, BLK, 0, st>>>(nC, m->cellO2N, (const float4 *) sbI, oR, oU, oV, oW);
+        if (nB > 0) k_convert<float, double><<<grid_for(nB, BLK), BLK, 0, st>>>(nB, (const float *) pbbI, oPbb);
+    }
+    g_launches.fetch_add(5);
+    CG_CHECK_CUDA(cudaGetLastError());
+    if (grad) CG_CHECK_CUDA(cudaMemcpyAsync(grad, oG, 24 * (size_t) nC, cudaMemcpyDeviceToHost, st));
+    if (massFlux) CG_CHECK_CUDA(cudaMemcpyAsync(massFlux, oMf, 8 * (size_t) nF, cudaMemcpyDeviceToHost, st));
+    if (phiBar) CG_CHECK_CUDA(cudaMemcpyAsync(phiBar, oPb, 8 * (size_t) nC, cudaMemcpyDeviceToHost, st));
+    if (denBar) CG_CHECK_CUDA(cudaMemcpyAsync(denBar, oR, 8 * (size_t) nC, cudaMemcpyDeviceToHost, st));
+    if (uBar) CG_CHECK_CUDA(cudaMemcpyAsync(uBar, oU, 8 * (size_t) nC, cudaMemcpyDeviceToHost, st));
+    if (vBar) CG_CHECK_CUDA(cudaMemcpyAsync(vBar, oV, 8 * (size_t) nC, cudaMemcpyDeviceToHost, st));
+    if (wBar) CG_CHECK_CUDA(cudaMemcpyAsync(wBar, oW, 8 * (size_t) nC, cudaMemcpyDeviceToHost, st));
+    if (phiBBar && nB > 0) CG_CHECK_CUDA(cudaMemcpyAsync(phiBBar, oPbb, 8 * (size_t) nB, cudaMemcpyDeviceToHost, st));
+    if (loss) CG_CHECK_CUDA(cudaMemcpyAsync(loss, dloss, 8, cudaMemcpyDeviceToHost, st));
+    CG_CHECK_CUDA(cudaStreamSynchronize(st));
+    return CUPCFD_E_SUCCESS;
+}

@@ -1,0 +1,241 @@
+// Face-loop kernels (device code shared by the ABI translation units).
+//
+// Data layout (internal numbering, see internal.cuh):
+//   faceCells[f] = {P, N} or {P, -1 - boundaryId}
+//   fg64/fg32[f] = {Sx, Sy, Sz, lambda}: one 128-bit load per face in FP32
+//   cell scalars T[nC]; cell vectors as three component blocks T[3][ldc]
+//   SELL-32 incidence lists: one thread per cell, 32 consecutive cells per
+//   warp, entry k of the warp's cells is one coalesced 128-byte load.
+//
+// Determinism: every cell sums its faces in ascending reference face id, one
+// thread per cell, no floating-point atomics anywhere. FP64 kernels use
+// explicit round-to-nearest intrinsics in the reference's operand order
+// (GradientKernels.ipp:73-131, MassKernels.ipp:95-306), so results equal the
+// reference CPU build bit for bit.
+#pragma once
+
+#include "internal.cuh"
+
+namespace cupcfd_gpu {
+
+__device__ __forceinline__ double dm(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double da(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double ds(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double dvd(double a, double b) { return __ddiv_rn(a, b); }
+
+// ---------------------------------------------------------------------------
+// Dot2 compensated accumulation (Ogita, Rump & Oishi, "Accurate sum and dot
+// product", SIAM J. Sci. Comput. 26(6), 2005): each product is split into
+// its rounded value and exact error (TwoProduct via FMA), the sum is kept
+// with Knuth's TwoSum error term, and the errors are accumulated separately.
+// The result is as accurate as if computed in twice the working precision.
+// ---------------------------------------------------------------------------
+struct Acc2 {
+    float s = 0.f, e = 0.f;
+    __device__ __forceinline__ void add_prod(float a, float b) {
+        float p = __fmul_rn(a, b);
+        float ep = __fmaf_rn(a, b, -p);
+        float t = __fadd_rn(s, p);
+        float bp = __fsub_rn(t, s);
+        float es = __fadd_rn(__fsub_rn(s, __fsub_rn(t, bp)), __fsub_rn(p, bp));
+        s = t;
+        e = __fadd_rn(e, __fadd_rn(ep, es));
+    }
+    __device__ __forceinline__ void sub_prod(float a, float b) { add_prod(-a, b); }
+    __device__ __forceinline__ double value() const { return (double) s + (double) e; }
+};
+
+// 32-byte read-only load as two 128-bit loads (no __ldg overload for double4)
+__device__ __forceinline__ double4 ldg4(const double4 *p) {
+    double2 a = __ldg(reinterpret_cast<const double2 *>(p));
+    double2 b = __ldg(reinterpret_cast<const double2 *>(p) + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+
+__device__ __forceinline__ float4 ldg4(const float4 *p) { return __ldg(p); }
+
+struct SellView {
+    const int *slicePtr;
+    const int *inc;
+};
+
+// ---------------------------------------------------------------------------
+// Gradient, FP64, reference arithmetic. CORR adds the non-orthogonal
+// correction of the previous iterate (needed from the second iteration on;
+// with a zero previous iterate the term is exactly +0 and is skipped).
+// ---------------------------------------------------------------------------
+template <bool CORR, bool SIGNED>
+__global__ void __launch_bounds__(256) k_grad_f64(int nC, SellView sv, const int2 *__restrict__ fcells,
+                                                  const double4 *__restrict__ fg, const double4 *__restrict__ fc,
+                                                  const double4 *__restrict__ cc, const double *__restrict__ phi,
+                                                  const double *__restrict__ phiB, const double *__restrict__ vol,
+                                                  const double *__restrict__ go, double *__restrict__ g,
+                                                  double *__restrict__ gcopy, int64_t ldc) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nC) return;
+    int s = c >> 5, lane = c & 31;
+    int p0 = __ldg(sv.slicePtr + s);
+    int w = (__ldg(sv.slicePtr + s + 1) - p0) >> 5;
+    const int *e = sv.inc + p0 + lane;
+    double phic = phi[c];
+    double4 xc;
+    double gc0 = 0, gc1 = 0, gc2 = 0;
+    if (CORR) {
+        xc = cc[c];
+        gc0 = go[c]; gc1 = go[ldc + c]; gc2 = go[2 * ldc + c];
+    }
+    double ax = 0.0, ay = 0.0, az = 0.0;
+    for (int k = 0; k < w; k++) {
+        int ent = __ldg(e + 32 * k);
+        if (ent < 0) break;
+        int f = ent >> 1;
+        bool isN = ent & 1;
+        int2 pn = __ldg(fcells + f);
+        double4 G = ldg4(fg + f);
+        double phif;
+        if (pn.y < 0) {
+            phif = __ldg(phiB + (-1 - pn.y));
+        } else {
+            int o = isN ? pn.x : pn.y;
+            double pho = __ldg(phi + o);
+            double facn = G.w;
+            double facp = ds(1.0, facn);
+            double phN = isN ? phic : pho, phP = isN ? pho : phic;
+            phif = da(dm(phN, facn), dm(phP, facp));
+            if (CORR) {
+                double4 xo = ldg4(cc + o);
+                double4 xf = ldg4(fc + f);
+                double go0 = __ldg(go + o), go1 = __ldg(go + ldc + o), go2 = __ldg(go + 2 * ldc + o);
+                double4 xN = isN ? xc : xo, xP = isN ? xo : xc;
+                double gN0 = isN ? gc0 : go0, gN1 = isN ? gc1 : go1, gN2 = isN ? gc2 : go2;
+                double gP0 = isN ? go0 : gc0, gP1 = isN ? go1 : gc1, gP2 = isN ? go2 : gc2;
+                double xac0 = da(dm(xN.x, facn), dm(xP.x, facp));
+                double xac1 = da(dm(xN.y, facn), dm(xP.y, facp));
+                double xac2 = da(dm(xN.z, facn), dm(xP.z, facp));
+                double ga0 = da(dm(gN0, facn), dm(gP0, facp));
+                double ga1 = da(dm(gN1, facn), dm(gP1, facp));
+                double ga2 = da(dm(gN2, facn), dm(gP2, facp));
+                double d = 0.0;
+                d = da(d, dm(ga0, ds(xf.x, xac0)));
+                d = da(d, dm(ga1, ds(xf.y, xac1)));
+                d = da(d, dm(ga2, ds(xf.z, xac2)));
+                phif = da(phif, d);
+            }
+        }
+        if (SIGNED && isN) {
+            ax = ds(ax, dm(phif, G.x)); ay = ds(ay, dm(phif, G.y)); az = ds(az, dm(phif, G.z));
+        } else {
+            ax = da(ax, dm(phif, G.x)); ay = da(ay, dm(phif, G.y)); az = da(az, dm(phif, G.z));
+        }
+    }
+    double fact = dvd(1.0, vol[c]);
+    ax = dm(ax, fact); ay = dm(ay, fact); az = dm(az, fact);
+    g[c] = ax; g[ldc + c] = ay; g[2 * ldc + c] = az;
+    if (gcopy) { gcopy[c] = ax; gcopy[ldc + c] = ay; gcopy[2 * ldc + c] = az; }
+}
+
+// ---------------------------------------------------------------------------
+// Gradient, FP32 storage and arithmetic, Dot2 accumulation, FP64 1/V.
+// ---------------------------------------------------------------------------
+template <bool CORR, bool SIGNED>
+__global__ void __launch_bounds__(256) k_grad_f32(int nC, SellView sv, const int2 *__restrict__ fcells,
+                                                  const float4 *__restrict__ fg, const float4 *__restrict__ fc,
+                                                  const float4 *__restrict__ cc, const float *__restrict__ phi,
+                                                  const float *__restrict__ phiB, const double *__restrict__ vol,
+                                                  const float *__restrict__ go, float *__restrict__ g,
+                                                  float *__restrict__ gcopy, int64_t ldc) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nC) return;
+    int s = c >> 5, lane = c & 31;
+    int p0 = __ldg(sv.slicePtr + s);
+    int w = (__ldg(sv.slicePtr + s + 1) - p0) >> 5;
+    const int *e = sv.inc + p0 + lane;
+    float phic = phi[c];
+    float4 xc;
+    float gc0 = 0, gc1 = 0, gc2 = 0;
+    if (CORR) {
+        xc = cc[c];
+        gc0 = go[c]; gc1 = go[ldc + c]; gc2 = go[2 * ldc + c];
+    }
+    Acc2 ax, ay, az;
+    for (int k = 0; k < w; k++) {
+        int ent = __ldg(e + 32 * k);
+        if (ent < 0) break;
+        int f = ent >> 1;
+        bool isN = ent & 1;
+        int2 pn = __ldg(fcells + f);
+        float4 G = ldg4(fg + f);
+        float phif;
+        if (pn.y < 0) {
+            phif = __ldg(phiB + (-1 - pn.y));
+        } else {
+            int o = isN ? pn.x : pn.y;
+            float pho = __ldg(phi + o);
+            float facn = G.w, facp = 1.f - facn;
+            float phN = isN ? phic : pho, phP = isN ? pho : phic;
+            phif = fmaf(facn, phN, facp * phP);
+            if (CORR) {
+                float4 xo = ldg4(cc + o), xf = ldg4(fc + f);
+                float go0 = __ldg(go + o), go1 = __ldg(go + ldc + o), go2 = __ldg(go + 2 * ldc + o);
+                float4 xN = isN ? xc : xo, xP = isN ? xo : xc;
+                float gN0 = isN ? gc0 : go0, gN1 = isN ? gc1 : go1, gN2 = isN ? gc2 : go2;
+                float gP0 = isN ? go0 : gc0, gP1 = isN ? go1 : gc1, gP2 = isN ? go2 : gc2;
+                float d0 = xf.x - fmaf(facn, xN.x, facp * xP.x);
+                float d1 = xf.y - fmaf(facn, xN.y, facp * xP.y);
+                float d2 = xf.z - fmaf(facn, xN.z, facp * xP.z);
+                phif += fmaf(facn, gN0, facp * gP0) * d0 + fmaf(facn, gN1, facp * gP1) * d1 +
+                        fmaf(facn, gN2, facp * gP2) * d2;
+            }
+        }
+        if (SIGNED && isN) {
+            ax.sub_prod(phif, G.x); ay.sub_prod(phif, G.y); az.sub_prod(phif, G.z);
+        } else {
+            ax.add_prod(phif, G.x); ay.add_prod(phif, G.y); az.add_prod(phif, G.z);
+        }
+    }
+    double fact = 1.0 / vol[c];
+    float rx = (float) (ax.value() * fact), ry = (float) (ay.value() * fact), rz = (float) (az.value() * fact);
+    g[c] = rx; g[ldc + c] = ry; g[2 * ldc + c] = rz;
+    if (gcopy) { gcopy[c] = rx; gcopy[ldc + c] = ry; gcopy[2 * ldc + c] = rz; }
+}
+
+// ---------------------------------------------------------------------------
+// Plain mass flux m_f = rho_f (u_f . S_f), one thread per face.
+// F64: state as four component blocks [4][ldc] (rho, u, v, w).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_mass_plain_f64(int nF, const int2 *__restrict__ fcells,
+                                                        const double4 *__restrict__ fg, const double *__restrict__ st,
+                                                        int64_t ldc, double *__restrict__ mflux) {
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nF) return;
+    int2 pn = fcells[f];
+    if (pn.y < 0) return;
+    double4 G = fg[f];
+    double facn = G.w, facp = ds(1.0, facn);
+    int P = pn.x, N = pn.y;
+    double denf = da(dm(__ldg(st + N), facn), dm(__ldg(st + P), facp));
+    double uF = da(dm(__ldg(st + ldc + N), facn), dm(__ldg(st + ldc + P), facp));
+    double vF = da(dm(__ldg(st + 2 * ldc + N), facn), dm(__ldg(st + 2 * ldc + P), facp));
+    double wF = da(dm(__ldg(st + 3 * ldc + N), facn), dm(__ldg(st + 3 * ldc + P), facp));
+    mflux[f] = dm(denf, da(da(dm(uF, G.x), dm(vF, G.y)), dm(wF, G.z)));
+}
+
+// F32: state as float4 {rho, u, v, w} per cell.
+__global__ void __launch_bounds__(256) k_mass_plain_f32(int nF, const int2 *__restrict__ fcells,
+                                                        const float4 *__restrict__ fg, const float4 *__restrict__ st,
+                                                        float *__restrict__ mflux) {
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nF) return;
+    int2 pn = fcells[f];
+    if (pn.y < 0) return;
+    float4 G = fg[f];
+    float facn = G.w, facp = 1.f - facn;
+    float4 sP = __ldg(st + pn.x), sN = __ldg(st + pn.y);
+    float denf = fmaf(facn, sN.x, facp * sP.x);
+    float uF = fmaf(facn, sN.y, facp * sP.y);
+    float vF = fmaf(facn, sN.z, facp * sP.z);
+    float wF = fmaf(facn, sN.w, facp * sP.w);
+    mflux[f] = denf * fmaf(uF, G.x, fmaf(vF, G.y, wF * G.z));
+}
+
+}  // namespace cupcfd_gpu

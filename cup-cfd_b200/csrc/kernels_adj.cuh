@@ -1,0 +1,445 @@
+// Adjoint kernels, the fused forward pass and the full-semantics mass flux.
+//
+// Adjoints are the transposed gathers over the same SELL-32 incidence lists:
+// a cell collects, over its faces in ascending reference face id, the
+// sensitivities that the forward face loop spread from that face into both
+// of its cells. One thread per cell, no floating-point atomics.
+#pragma once
+
+#include "kernels.cuh"
+
+namespace cupcfd_gpu {
+
+// ---------------------------------------------------------------------------
+// Fused forward pass of the benchmark pipeline: gradient (nGradient = 1) and
+// the plain mass flux of the faces this cell owns, plus the per-block FP64
+// partial of L = sum_c V_c |g_c|^2 + sum_f gface_f m_f.
+// FP64 version: same arithmetic as k_grad_f64 / k_mass_plain_f64.
+// ---------------------------------------------------------------------------
+template <int BLOCK>
+__device__ __forceinline__ void block_sum_store(double v, double *out) {
+    __shared__ double red[BLOCK / 32];
+    for (int k = 16; k > 0; k >>= 1) v += __shfl_xor_sync(0xffffffffu, v, k);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int i = 0; i < BLOCK / 32; i++) t += red[i];
+        out[blockIdx.x] = t;
+    }
+}
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_fwd_f64(int nC, SellView sv, const int2 *__restrict__ fcells,
+                                                   const double4 *__restrict__ fg, const double *__restrict__ phi,
+                                                   const double *__restrict__ phiB, const double *__restrict__ vol,
+                                                   const double *__restrict__ st, const double *__restrict__ gface,
+                                                   double *__restrict__ g, double *__restrict__ mflux,
+                                                   double *__restrict__ lossPart, int64_t ldc) {
+    int c = blockIdx.x * BLOCK + threadIdx.x;
+    double lsum = 0.0;
+    if (c < nC) {
+        int s = c >> 5, lane = c & 31;
+        int p0 = __ldg(sv.slicePtr + s);
+        int w = (__ldg(sv.slicePtr + s + 1) - p0) >> 5;
+        const int *e = sv.inc + p0 + lane;
+        double phic = phi[c];
+        double r0 = st[c], u0 = st[ldc + c], v0 = st[2 * ldc + c], w0 = st[3 * ldc + c];
+        double ax = 0.0, ay = 0.0, az = 0.0;
+        for (int k = 0; k < w; k++) {
+            int ent = __ldg(e + 32 * k);
+            if (ent < 0) break;
+            int f = ent >> 1;
+            bool isN = ent & 1;
+            int2 pn = __ldg(fcells + f);
+            double4 G = ldg4(fg + f);
+            double phif;
+            if (pn.y < 0) {
+                phif = __ldg(phiB + (-1 - pn.y));
+            } else {
+                int o = isN ? pn.x : pn.y;
+                double facn = G.w, facp = ds(1.0, facn);
+                double pho = __ldg(phi + o);
+                phif = isN ? da(dm(phic, facn), dm(pho, facp)) : da(dm(pho, facn), dm(phic, facp));
+                if (!isN) {  // owner computes m_f: P = c, N = o
+                    double denf = da(dm(__ldg(st + o), facn), dm(r0, facp));
+                    double uF = da(dm(__ldg(st + ldc + o), facn), dm(u0, facp));
+                    double vF = da(dm(__ldg(st + 2 * ldc + o), facn), dm(v0, facp));
+                    double wF = da(dm(__ldg(st + 3 * ldc + o), facn), dm(w0, facp));
+                    double m = dm(denf, da(da(dm(uF, G.x), dm(vF, G.y)), dm(wF, G.z)));
+                    mflux[f] = m;
+                    if (gface) lsum += __ldg(gface + f) * m;
+                }
+            }
+            ax = da(ax, dm(phif, G.x)); ay = da(ay, dm(phif, G.y)); az = da(az, dm(phif, G.z));
+        }
+        double V = vol[c];
+        double fact = dvd(1.0, V);
+        ax = dm(ax, fact); ay = dm(ay, fact); az = dm(az, fact);
+        g[c] = ax; g[ldc + c] = ay; g[2 * ldc + c] = az;
+        lsum += V * (ax * ax + ay * ay + az * az);
+    }
+    if (lossPart) block_sum_store<BLOCK>(lsum, lossPart);
+}
+
+// FP32 version; cell state as float4 {rho, u, v, w}.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_fwd_f32(int nC, SellView sv, const int2 *__restrict__ fcells,
+                                                   const float4 *__restrict__ fg, const float *__restrict__ phi,
+                                                   const float *__restrict__ phiB, const double *__restrict__ vol,
+                                                   const float4 *__restrict__ st, const float *__restrict__ gface,
+                                                   float *__restrict__ g, float *__restrict__ mflux,
+                                                   double *__restrict__ lossPart, int64_t ldc) {
+    int c = blockIdx.x * BLOCK + threadIdx.x;
+    double lsum = 0.0;
+    if (c < nC) {
+        int s = c >> 5, lane = c & 31;
+        int p0 = __ldg(sv.slicePtr + s);
+        int w = (__ldg(sv.slicePtr + s + 1) - p0) >> 5;
+        const int *e = sv.inc + p0 + lane;
+        float phic = phi[c];
+        float4 sc = st[c];
+        Acc2 ax, ay, az;
+        for (int k = 0; k < w; k++) {
+            int ent = __ldg(e + 32 * k);
+            if (ent < 0) break;
+            int f = ent >> 1;
+            bool isN = ent & 1;
+            int2 pn = __ldg(fcells + f);
+            float4 G = __ldg(fg + f);
+            float phif;
+            if (pn.y < 0) {
+                phif = __ldg(phiB + (-1 - pn.y));
+            } else {
+                int o = isN ? pn.x : pn.y;
+                float facn = G.w, facp = 1.f - facn;
+                float pho = __ldg(phi + o);
+                phif = isN ? fmaf(facn, phic, facp * pho) : fmaf(facn, pho, facp * phic);
+                if (!isN) {
+                    float4 so = __ldg(st + o);
+                    float denf = fmaf(facn, so.x, facp * sc.x);
+                    float uF = fmaf(facn, so.y, facp * sc.y);
+                    float vF = fmaf(facn, so.z, facp * sc.z);
+                    float wF = fmaf(facn, so.w, facp * sc.w);
+                    float m = denf * fmaf(uF, G.x, fmaf(vF, G.y, wF * G.z));
+                    mflux[f] = m;
+                    if (gface) lsum += (double) __ldg(gface + f) * (double) m;
+                }
+            }
+            ax.add_prod(phif, G.x); ay.add_prod(phif, G.y); az.add_prod(phif, G.z);
+        }
+        double V = vol[c];
+        double fact = 1.0 / V;
+        double gx = ax.value() * fact, gy = ay.value() * fact, gz = az.value() * fact;
+        float rx = (float) gx, ry = (float) gy, rz = (float) gz;
+        g[c] = rx; g[ldc + c] = ry; g[2 * ldc + c] = rz;
+        lsum += V * ((double) rx * rx + (double) ry * ry + (double) rz * rz);
+    }
+    if (lossPart) block_sum_store<BLOCK>(lsum, lossPart);
+}
+
+// Deterministic final reduction of per-block partials (fixed order).
+__global__ void k_reduce_partials(int n, const double *__restrict__ part, double *__restrict__ out) {
+    __shared__ double red[1024];
+    double t = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) t += part[i];
+    red[threadIdx.x] = t;
+    __syncthreads();
+    for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+        if ((int) threadIdx.x < k) red[threadIdx.x] += red[threadIdx.x + k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = red[0];
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint of the benchmark loss, one pass: with L = sum V|g|^2 + sum gface m,
+// dL/dg_c = 2 V_c g_c, so h_c = dL/dg_c / V_c = 2 g_c and
+//   phibar_c  = sum_{f in c, interior} w_cf (h_P + h_N) . S_f
+//   phibBar_b = h_P . S_f                      (boundary face f of id b)
+//   rhobar_c  = sum_f w_cf gface_f (u_f . S_f)
+//   ubar_c    = sum_f w_cf gface_f rho_f S_f   (and v, w)
+// with w_cf = 1 - lambda_f for the owner, lambda_f for the neighbour.
+// When hscale = 0 the gradient part is skipped (mass-only adjoint) and when
+// gface is null the mass part is skipped.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_adj_f64(int nC, SellView sv, const int2 *__restrict__ fcells,
+                                                 const double4 *__restrict__ fg, const double *__restrict__ g,
+                                                 double hscale, const double *__restrict__ st,
+                                                 const double *__restrict__ gface, double *__restrict__ phibar,
+                                                 double *__restrict__ phibBar, double *__restrict__ stbar, int64_t ldc) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nC) return;
+    int s = c >> 5, lane = c & 31;
+    int p0 = __ldg(sv.slicePtr + s);
+    int w = (__ldg(sv.slicePtr + s + 1) - p0) >> 5;
+    const int *e = sv.inc + p0 + lane;
+    bool doG = hscale != 0.0, doM = gface != nullptr;
+    double hx = 0, hy = 0, hz = 0;
+    if (doG) { hx = hscale * g[c]; hy = hscale * g[ldc + c]; hz = hscale * g[2 * ldc + c]; }
+    double r0 = 0, u0 = 0, v0 = 0, w0 = 0;
+    if (doM) { r0 = st[c]; u0 = st[ldc + c]; v0 = st[2 * ldc + c]; w0 = st[3 * ldc + c]; }
+    double pb = 0.0, rb = 0.0, ub = 0.0, vb = 0.0, wb = 0.0;
+    for (int k = 0; k < w; k++) {
+        int ent = __ldg(e + 32 * k);
+        if (ent < 0) break;
+        int f = ent >> 1;
+        bool isN = ent & 1;
+        int2 pn = __ldg(fcells + f);
+        double4 G = ldg4(fg + f);
+        if (pn.y < 0) {
+            if (doG) phibBar[-1 - pn.y] = hx * G.x + hy * G.y + hz * G.z;
+            continue;
+        }
+        int o = isN ? pn.x : pn.y;
+        double facn = G.w, facp = 1.0 - facn;
+        double wc = isN ? facn : facp, wo = isN ? facp : facn;
+        if (doG) {
+            double ox = hscale * __ldg(g + o), oy = hscale * __ldg(g + ldc + o), oz = hscale * __ldg(g + 2 * ldc + o);
+            pb += wc * ((hx + ox) * G.x + (hy + oy) * G.y + (hz + oz) * G.z);
+        }
+        if (doM) {
+            double gf = __ldg(gface + f);
+            double ro = __ldg(st + o), uo = __ldg(st + ldc + o), vo = __ldg(st + 2 * ldc + o), wo_ = __ldg(st + 3 * ldc + o);
+            double denf = wc * r0 + wo * ro;
+            double uF = wc * u0 + wo * uo, vF = wc * v0 + wo * vo, wF = wc * w0 + wo * wo_;
+            double flux = uF * G.x + vF * G.y + wF * G.z;
+            double a = wc * gf;
+            rb += a * flux;
+            double b = a * denf;
+            ub += b * G.x; vb += b * G.y; wb += b * G.z;
+        }
+    }
+    if (doG) phibar[c] = pb;
+    if (doM) { stbar[c] = rb; stbar[ldc + c] = ub; stbar[2 * ldc + c] = vb; stbar[3 * ldc + c] = wb; }
+}
+
+// FP32 version; Dot2-compensated accumulation of the five sums.
+__global__ void __launch_bounds__(256) k_adj_f32(int nC, SellView sv, const int2 *__restrict__ fcells,
+                                                 const float4 *__restrict__ fg, const float *__restrict__ g, float hscale,
+                                                 const float4 *__restrict__ st, const float *__restrict__ gface,
+                                                 float *__restrict__ phibar, float *__restrict__ phibBar,
+                                                 float4 *__restrict__ stbar, int64_t ldc) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nC) return;
+    int s = c >> 5, lane = c & 31;
+    int p0 = __ldg(sv.slicePtr + s);
+    int w = (__ldg(sv.slicePtr + s + 1) - p0) >> 5;
+    const int *e = sv.inc + p0 + lane;
+    bool doG = hscale != 0.f, doM = gface != nullptr;
+    float hx = 0, hy = 0, hz = 0;
+    if (doG) { hx = hscale * g[c]; hy = hscale * g[ldc + c]; hz = hscale * g[2 * ldc + c]; }
+    float4 sc = make_float4(0, 0, 0, 0);
+    if (doM) sc = st[c];
+    Acc2 pb, rb, ub, vb, wb;
+    for (int k = 0; k < w; k++) {
+        int ent = __ldg(e + 32 * k);
+        if (ent < 0) break;
+        int f = ent >> 1;
+        bool isN = ent & 1;
+        int2 pn = __ldg(fcells + f);
+        float4 G = __ldg(fg + f);
+        if (pn.y < 0) {
+            if (doG) phibBar[-1 - pn.y] = fmaf(hx, G.x, fmaf(hy, G.y, hz * G.z));
+            continue;
+        }
+        int o = isN ? pn.x : pn.y;
+        float facn = G.w, facp = 1.f - facn;
+        float wc = isN ? facn : facp, wo = isN ? facp : facn;
+        if (doG) {
+            float ox = hscale * __ldg(g + o), oy = hscale * __ldg(g + ldc + o), oz = hscale * __ldg(g + 2 * ldc + o);
+            pb.add_prod(wc, fmaf(hx + ox, G.x, fmaf(hy + oy, G.y, (hz + oz) * G.z)));
+        }
+        if (doM) {
+            float gf = __ldg(gface + f);
+            float4 so = __ldg(st + o);
+            float denf = fmaf(wc, sc.x, wo * so.x);
+            float uF = fmaf(wc, sc.y, wo * so.y), vF = fmaf(wc, sc.z, wo * so.z), wF = fmaf(wc, sc.w, wo * so.w);
+            float a = wc * gf;
+            rb.add_prod(a, fmaf(uF, G.x, fmaf(vF, G.y, wF * G.z)));
+            float b = a * denf;
+            ub.add_prod(b, G.x); vb.add_prod(b, G.y); wb.add_prod(b, G.z);
+        }
+    }
+    if (doG) phibar[c] = (float) pb.value();
+    if (doM) stbar[c] = make_float4((float) rb.value(), (float) ub.value(), (float) vb.value(), (float) wb.value());
+}
+
+// General gradient adjoint (input gbar = dL/dg, any loss): h_c = gbar_c / V_c.
+template <bool SIGNED, class T>
+__global__ void __launch_bounds__(256) k_grad_adj_general(int nC, SellView sv, const int2 *__restrict__ fcells,
+                                                          const double4 *__restrict__ fg64, const float4 *__restrict__ fg32,
+                                                          const double *__restrict__ vol, const T *__restrict__ gbar,
+                                                          T *__restrict__ phibar, T *__restrict__ phibBar, int64_t ldc) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nC) return;
+    int s = c >> 5, lane = c & 31;
+    int p0 = __ldg(sv.slicePtr + s);
+    int w = (__ldg(sv.slicePtr + s + 1) - p0) >> 5;
+    const int *e = sv.inc + p0 + lane;
+    double iv = 1.0 / vol[c];
+    double hx = (double) gbar[c] * iv, hy = (double) gbar[ldc + c] * iv, hz = (double) gbar[2 * ldc + c] * iv;
+    double pb = 0.0;
+    for (int k = 0; k < w; k++) {
+        int ent = __ldg(e + 32 * k);
+        if (ent < 0) break;
+        int f = ent >> 1;
+        bool isN = ent & 1;
+        int2 pn = __ldg(fcells + f);
+        double Sx, Sy, Sz, lam;
+        if (fg64) { double4 G = ldg4(fg64 + f); Sx = G.x; Sy = G.y; Sz = G.z; lam = G.w; }
+        else { float4 G = __ldg(fg32 + f); Sx = G.x; Sy = G.y; Sz = G.z; lam = G.w; }
+        double own = hx * Sx + hy * Sy + hz * Sz;
+        if (pn.y < 0) {
+            phibBar[-1 - pn.y] = (T) own;
+            continue;
+        }
+        int o = isN ? pn.x : pn.y;
+        double ivo = 1.0 / __ldg(vol + o);
+        double oth = ((double) gbar[o] * Sx + (double) gbar[ldc + o] * Sy + (double) gbar[2 * ldc + o] * Sz) * ivo;
+        // d g_P / d phi_f = +S/V_P; d g_N / d phi_f = +S/V_N (reference) or -S/V_N (signed)
+        double sOwn = (SIGNED && isN) ? -1.0 : 1.0, sOth = (SIGNED && !isN) ? -1.0 : 1.0;
+        double pf = sOwn * own + sOth * oth;
+        pb += (isN ? lam : 1.0 - lam) * pf;
+    }
+    phibar[c] = (T) pb;
+}
+
+// ---------------------------------------------------------------------------
+// FluxMassDolfynFaceLoop, full semantics, FP64, one thread per face
+// (MassKernels.ipp:95-306). Cell inputs are component blocks over ldc:
+// grads = [dudx(3) dvdx(3) dwdx(3) dpdx(3)] (12 blocks), cs = [den u v w p ar]
+// (6 blocks). rface is [2][nF] pairs in internal face order. Boundary
+// branches per region type; the inlet su[ip] update is done afterwards by
+// k_inlet_su in the reference's face order. cnt[4] counts the branches.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_mass_full_f64(
+    int nF, const int2 *__restrict__ fcells, const double4 *__restrict__ fg, const double4 *__restrict__ fc,
+    const double4 *__restrict__ fxp, const double4 *__restrict__ fxn, const double4 *__restrict__ cc,
+    const double *__restrict__ vol, const double *__restrict__ grads, const double *__restrict__ cs, int64_t ldc,
+    const int *__restrict__ bndRegion, const int *__restrict__ regionType, const double *__restrict__ regionUVW,
+    const double *__restrict__ regionDen, double small, int flags, double *__restrict__ mflux,
+    double *__restrict__ rface, double *__restrict__ denB, const double *__restrict__ bcIn, double *__restrict__ bcOut,
+    int nB, int *__restrict__ cnt) {
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nF) return;
+    int2 pn = fcells[f];
+    double4 G = fg[f];
+    int ip = pn.x;
+    if (pn.y >= 0) {
+        int in = pn.y;
+        double4 xP = cc[ip], xN = cc[in];
+        double4 X = fc[f];
+        double facn = G.w, facp = ds(1.0, facn);
+        const double *du = grads, *dvv = grads + 3 * ldc, *dw = grads + 6 * ldc, *dp = grads + 9 * ldc;
+        double duac[3], dvac[3], dwac[3];
+        for (int d = 0; d < 3; d++) {
+            duac[d] = da(dm(du[d * ldc + in], facn), dm(du[d * ldc + ip], facp));
+            dvac[d] = da(dm(dvv[d * ldc + in], facn), dm(dvv[d * ldc + ip], facp));
+            dwac[d] = da(dm(dw[d * ldc + in], facn), dm(dw[d * ldc + ip], facp));
+        }
+        const double *den = cs, *u = cs + ldc, *v = cs + 2 * ldc, *w = cs + 3 * ldc, *p = cs + 4 * ldc, *ar = cs + 5 * ldc;
+        double denf = da(dm(den[in], facn), dm(den[ip], facp));
+        double xac0 = da(dm(xN.x, facn), dm(xP.x, facp));
+        double xac1 = da(dm(xN.y, facn), dm(xP.y, facp));
+        double xac2 = da(dm(xN.z, facn), dm(xP.z, facp));
+        double de0 = ds(X.x, xac0), de1 = ds(X.y, xac1), de2 = ds(X.z, xac2);
+        auto dot3 = [](double a0, double a1, double a2, double b0, double b1, double b2) {
+            double d = 0.0;
+            d = da(d, dm(a0, b0));
+            d = da(d, dm(a1, b1));
+            d = da(d, dm(a2, b2));
+            return d;
+        };
+        double uF = da(da(dm(u[in], facn), dm(u[ip], facp)), dot3(duac[0], duac[1], duac[2], de0, de1, de2));
+        double vF = da(da(dm(v[in], facn), dm(v[ip], facp)), dot3(dvac[0], dvac[1], dvac[2], de0, de1, de2));
+        double wF = da(da(dm(w[in], facn), dm(w[ip], facp)), dot3(dwac[0], dwac[1], dwac[2], de0, de1, de2));
+        double m = dm(denf, da(da(dm(uF, G.x), dm(vF, G.y)), dm(wF, G.z)));
+        // xnorm = S / |S| (EuclideanVector::normalise, EuclideanVector.cpp:100-109)
+        double n0 = G.x, n1 = G.y, n2 = G.z;
+        double L = __dsqrt_rn(dot3(n0, n1, n2, n0, n1, n2));
+        if (L != 0.0) {
+            double sc = dvd(1.0, L);
+            n0 = dm(n0, sc); n1 = dm(n1, sc); n2 = dm(n2, sc);
+        }
+        double xa0 = 0, xa1 = 0, xa2 = 0, xb0 = 0, xb1 = 0, xb2 = 0;
+        if (fxp) {
+            double4 a = fxp[f], b = fxn[f];
+            xa0 = a.x; xa1 = a.y; xa2 = a.z; xb0 = b.x; xb1 = b.y; xb2 = b.z;
+        }
+        double dpP0 = dp[ip], dpP1 = dp[ldc + ip], dpP2 = dp[2 * ldc + ip];
+        double pip = da(p[ip], dot3(dpP0, dpP1, dpP2, ds(xa0, xP.x), ds(xa1, xP.y), ds(xa2, xP.z)));
+        double pin = da(p[in], dot3(dpP0, dpP1, dpP2, ds(xa0, xN.x), ds(xa1, xN.y), ds(xa2, xN.z)));  // dpdx[ip] (MassKernels.ipp:169)
+        double xpn0 = ds(xb0, xa0), xpn1 = ds(xb1, xa1), xpn2 = ds(xb2, xa2);
+        double apv1 = dm(den[ip], ar[ip]);
+        double apv2 = dm(den[in], ar[in]);
+        double apv = da(dm(apv2, facn), dm(apv1, facp));
+        double factv = da(dm(vol[in], facn), dm(vol[ip], facp));
+        apv = dm(apv, dvd(dm(X.w, factv), dot3(ds(xN.x, xP.x), ds(xN.y, xP.y), ds(xN.z, xP.z), n0, n1, n2)));
+        double dpx = dm(da(dm(dp[in], facn), dm(dpP0, facp)), xpn0);
+        double dpy = dm(da(dm(dp[ldc + in], facn), dm(dpP1, facp)), xpn1);
+        double dpz = dm(da(dm(dp[2 * ldc + in], facn), dm(dpP2, facp)), xpn2);
+        rface[2 * (int64_t) f] = -apv;
+        rface[2 * (int64_t) f + 1] = -apv;
+        mflux[f] = ds(m, dm(apv, ds(ds(ds(ds(pin, pip), dpx), dpy), dpz)));
+        return;
+    }
+    int ib = -1 - pn.y;
+    int ir = bndRegion[ib];
+    int it = regionType[ir];
+    if (it == CUPCFD_RTYPE_INLET) {
+        atomicAdd(&cnt[0], 1);
+        double d = 0.0;
+        d = da(d, dm(regionUVW[3 * ir], G.x));
+        d = da(d, dm(regionUVW[3 * ir + 1], G.y));
+        d = da(d, dm(regionUVW[3 * ir + 2], G.z));
+        mflux[f] = dm(regionDen[ir], d);
+    } else if (it == CUPCFD_RTYPE_OUTLET) {
+        atomicAdd(&cnt[1], 1);
+        const double *den = cs, *u = cs + ldc, *v = cs + 2 * ldc, *w = cs + 3 * ldc;
+        double denf = den[ip];
+        denB[ib] = denf;
+        double m = dm(denf, da(da(dm(u[ip], G.x), dm(v[ip], G.y)), dm(w[ip], G.z)));
+        if (m < 0.0) {
+            m = small;
+            // bcIn = [te ed vis t] cell blocks, bcOut = [te ed vis t] boundary blocks
+            for (int q = 0; q < 4; q++)
+                if (flags & (1 << q)) bcOut[(int64_t) q * nB + ib] = bcIn[q * ldc + ip];
+        }
+        mflux[f] = m;
+    } else if (it == CUPCFD_RTYPE_SYMP) {
+        atomicAdd(&cnt[2], 1);
+        mflux[f] = 0.0;
+    } else if (it == CUPCFD_RTYPE_WALL) {
+        atomicAdd(&cnt[3], 1);
+        mflux[f] = 0.0;
+    }
+}
+
+// su[ip] -= massFlux over the cell's inlet faces in ascending reference face
+// id (MassKernels.ipp:258), one thread per cell.
+__global__ void __launch_bounds__(256) k_inlet_su(int nC, SellView sv, const int2 *__restrict__ fcells,
+                                                  const int *__restrict__ bndRegion, const int *__restrict__ regionType,
+                                                  const double *__restrict__ mflux, double *__restrict__ su) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nC) return;
+    int s = c >> 5, lane = c & 31;
+    int p0 = sv.slicePtr[s];
+    int w = (sv.slicePtr[s + 1] - p0) >> 5;
+    const int *e = sv.inc + p0 + lane;
+    double v = su[c];
+    bool touched = false;
+    for (int k = 0; k < w; k++) {
+        int ent = e[32 * k];
+        if (ent < 0) break;
+        int f = ent >> 1;
+        int2 pn = fcells[f];
+        if (pn.y >= 0) continue;
+        if (regionType[bndRegion[-1 - pn.y]] != CUPCFD_RTYPE_INLET) continue;
+        v = ds(v, mflux[f]);
+        touched = true;
+    }
+    if (touched) su[c] = v;
+}
+
+}  // namespace cupcfd_gpu

@@ -1,0 +1,304 @@
+/*
+ * cupcfd_gpu.h - C ABI of the B200 (sm_100a) implementation of CUP-CFD's
+ * finite-volume face-loop path: the Gauss-Green cell gradient
+ * (GradientPhiGaussDolfyn) and the face mass-flux loop
+ * (FluxMassDolfynFaceLoop) over the reference's MiniSoA mesh.
+ *
+ * Plain C: pointers, sizes and int status codes only. Status codes are the
+ * reference's eCodes values (include/error/Error.h:32-144): CUPCFD_E_SUCCESS
+ * is E_SUCCESS, and so on. No call aborts; CUDA failures map to
+ * CUPCFD_E_ERROR and the message is available from cupcfd_gpu_last_error().
+ *
+ * Two layers:
+ *  1. Reference-facing calls (cupcfd_gpu_gradient_phi_gauss_dolfyn,
+ *     cupcfd_gpu_flux_mass_dolfyn_face_loop): HOST buffers in the
+ *     reference's numbering and layout, including the 32-byte (double) /
+ *     24-byte (float) stride of the vptr-carrying EuclideanVector<T,3>
+ *     arrays. Each call copies inputs to the device, runs, and copies the
+ *     outputs back before returning, exactly like the synchronous CPU call
+ *     it replaces.
+ *  2. Device-resident calls (cupcfd_gpu_dev_*): DEVICE pointers in the
+ *     mesh's internal (renumbered) order, stream-ordered on the stream the
+ *     caller passes, no host synchronisation. Fields are moved between the
+ *     two numberings with cupcfd_gpu_dev_permute_cells / _permute_faces.
+ *
+ * Threading: a mesh handle is not thread-safe (as the reference mesh is
+ * not); calls on one handle must be serialised by the caller.
+ */
+#ifndef CUPCFD_GPU_H
+#define CUPCFD_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes: values of the reference enum cupcfd::error::eCodes ---- */
+#define CUPCFD_E_ARRAY_SIZE_MISMATCH 25 /* E_ARRAY_SIZE_MISMATCH, Error.h:59 */
+#define CUPCFD_E_INVALID_INDEX 68       /* E_INVALID_INDEX, Error.h:102 */
+#define CUPCFD_E_CONFIG_INVALID_VALUE 90 /* E_CONFIG_INVALID_VALUE, Error.h:124 */
+#define CUPCFD_E_SUCCESS 95             /* E_SUCCESS, Error.h:129 */
+#define CUPCFD_E_ERROR 98               /* E_ERROR, Error.h:132 */
+#define CUPCFD_E_NULL_PTR 99            /* E_NULL_PTR, Error.h:133 */
+#define CUPCFD_E_NOT_IMPLEMENTED 109    /* E_NOT_IMPLEMENTED, Error.h:143 */
+
+/* ---- region types: cupcfd::geometry::mesh::RType (UnstructuredMeshInterface.h:58-65) ---- */
+#define CUPCFD_RTYPE_DEFAULT 0
+#define CUPCFD_RTYPE_INLET 1
+#define CUPCFD_RTYPE_OUTLET 2
+#define CUPCFD_RTYPE_SYMP 3
+#define CUPCFD_RTYPE_WALL 4
+
+/* ---- arithmetic of a call ---- */
+#define CUPCFD_PREC_F64 0  /* plain FP64; same operand order as the reference, bit-identical results */
+#define CUPCFD_PREC_F32C 1 /* FP32 storage and arithmetic, compensated (Dot2) cell accumulation,
+                              FP64 volumes and final scaling */
+
+/* ---- internal numbering of a device mesh ---- */
+#define CUPCFD_ORDER_NATIVE 0 /* cells and faces in the reference's local order */
+#define CUPCFD_ORDER_MORTON 1 /* cells by Z-order of their centres, faces by owner cell */
+#define CUPCFD_ORDER_OWNER 2  /* cells in reference order, faces by owner cell */
+
+/* ---- gradient sign convention ---- */
+#define CUPCFD_SIGN_REFERENCE 0 /* phi_f S_f added to BOTH cells with the same sign,
+                                   as GradientKernels.ipp:102-103 does (default) */
+#define CUPCFD_SIGN_SIGNED 1    /* textbook Gauss-Green: the neighbour subtracts */
+
+/* Strided view of an array of 3-vectors: component d (0..2) of element i is
+ * the real at (char*)base + i*stride + offset + d*real_size. For a
+ * std::vector<EuclideanVector<double,3>> stride = 32 and offset = 8 (the
+ * vptr); for a packed xyz array stride = 3*real_size and offset = 0. */
+typedef struct {
+    const void *base;
+    int32_t stride;
+    int32_t offset;
+} cupcfd_vec3_view;
+
+/* Host view of a one-rank CupCfdSoAMesh<int,T,int> (CupCfdSoAMesh.h:59-558):
+ * the arrays its getters read, indexed by local id. real_size is sizeof(T)
+ * (8 or 4) and applies to every real array and vector view. faceCell2 is -1
+ * and faceBnd is the local boundary id on boundary faces; faceBnd is -1 on
+ * interior faces (CupCfdSoAMesh.cpp:309-461). faceXpac/faceXnac may have a
+ * NULL base, meaning all zero (what addData stores, UnstructuredMeshInterface.ipp:1778-1780). */
+typedef struct {
+    int32_t nCells;      /* properties.lTCells */
+    int32_t nFaces;      /* properties.lFaces */
+    int32_t nBoundaries; /* properties.lBoundaries */
+    int32_t real_size;   /* 8 (double) or 4 (float) */
+    const int32_t *faceCell1;
+    const int32_t *faceCell2;
+    const int32_t *faceBnd;
+    const void *faceLambda;
+    const void *faceArea;
+    cupcfd_vec3_view faceNorm;
+    cupcfd_vec3_view faceCenter;
+    cupcfd_vec3_view faceXpac;
+    cupcfd_vec3_view faceXnac;
+    cupcfd_vec3_view cellCenter;
+    const void *cellVolume;
+} cupcfd_mesh_view;
+
+typedef struct {
+    int32_t order;      /* CUPCFD_ORDER_* */
+    int32_t precisions; /* bit mask: 1 << CUPCFD_PREC_F64 | 1 << CUPCFD_PREC_F32C */
+    int32_t device;     /* CUDA device ordinal, -1 = current */
+} cupcfd_mesh_options;
+
+typedef struct {
+    int32_t nCells, nFaces, nInteriorFaces, nBoundaries, nRegions;
+    int32_t nIncidences; /* 2*interior + boundary faces: length of the cell->face CSR */
+    int32_t maxCellFaces;
+    int32_t order, precisions;
+    int64_t deviceBytes; /* device memory held by the mesh */
+} cupcfd_mesh_info;
+
+typedef struct cupcfd_gpu_mesh cupcfd_gpu_mesh;
+
+/* Message of the last failing call on this thread ("" if none). */
+const char *cupcfd_gpu_last_error(void);
+/* Library version string. */
+const char *cupcfd_gpu_version(void);
+
+/* ------------------------------------------------------------------------ */
+/* mesh                                                                      */
+/* ------------------------------------------------------------------------ */
+
+/* Uploads a host mesh, validates its connectivity, builds the cell->face CSR
+ * exactly as CupCfdSoAMesh::updateCellFaceMap does (CupCfdSoAMesh.cpp:549-668),
+ * renumbers, and lays out the device arrays. One region of type
+ * RTYPE_DEFAULT is installed; see cupcfd_gpu_mesh_set_regions.
+ * Replaces: the CupCfdSoAMesh finalize()/addData() result the reference
+ * kernels read (CupCfdSoAMesh.cpp:842-888). */
+int cupcfd_gpu_mesh_create(const cupcfd_mesh_view *view, const cupcfd_mesh_options *opt, cupcfd_gpu_mesh **out);
+
+/* Builds the structured hex mesh of MeshStructGenSource(nx, ny, nz, bounds)
+ * (src/geometry/mesh/implementation/source/MeshStructGenSource.cpp:33-1277)
+ * directly on the GPU in FP64, in the reference's label order, then proceeds
+ * as cupcfd_gpu_mesh_create. bounds = {xmin, xmax, ymin, ymax, zmin, zmax}.
+ * Cell volumes are the box volume; the reference's five-tetrahedron Heron
+ * sum agrees to 2e-14 relative (its own rounding). */
+int cupcfd_gpu_mesh_create_structgen(int32_t nx, int32_t ny, int32_t nz, const double bounds[6],
+                                     const cupcfd_mesh_options *opt, cupcfd_gpu_mesh **out);
+
+/* Unit-cube hex mesh with every interior vertex displaced by
+ * U[-jitter*h, jitter*h] per axis (splitmix64 stream keyed by seed, vertex,
+ * axis) and, if permute != 0, cell and face labels shuffled by seeded
+ * Fisher-Yates permutations. Geometry: S_f = 0.5 (v2-v0) x (v3-v1) oriented
+ * away from cell1, area |S_f|, face centre = vertex mean, cell centre =
+ * vertex mean, volume = sum_f x_f . S_f,out / 3, lambda = ((x_f - x_1) . S) /
+ * ((x_2 - x_1) . S). Used for the irregular-mesh workload; no reference
+ * counterpart (the reference reads such meshes from HDF5, MeshHDF5Source.cpp). */
+int cupcfd_gpu_mesh_create_jittered(int32_t nx, int32_t ny, int32_t nz, double jitter, uint64_t seed, int32_t permute,
+                                    const cupcfd_mesh_options *opt, cupcfd_gpu_mesh **out);
+
+int cupcfd_gpu_mesh_destroy(cupcfd_gpu_mesh *mesh);
+int cupcfd_gpu_mesh_get_info(const cupcfd_gpu_mesh *mesh, cupcfd_mesh_info *info);
+
+/* Boundary regions (CupCfdSoAMesh region/boundary arrays): regionType[nRegions]
+ * (CUPCFD_RTYPE_*), regionUVW[3*nRegions], regionDen[nRegions] (host, real_size
+ * 8) and bndRegion[nBoundaries] (host). Replaces getBoundaryRegionID /
+ * getRegionType / getRegionUVW / getRegionDen (UnstructuredMeshInterface.h:1306-1949). */
+int cupcfd_gpu_mesh_set_regions(cupcfd_gpu_mesh *mesh, int32_t nRegions, const int32_t *regionType,
+                                const double *regionUVW, const double *regionDen,
+                                const int32_t *bndRegion, int32_t nBoundaries);
+
+/* Downloads the cell->face CSR in the reference's numbering (host arrays,
+ * xadj[nCells+1], adj[nIncidences]) for bit-exact comparison with
+ * CupCfdSoAMesh::cellFaceMapCSRXAdj / cellFaceMapCSRAdj. */
+int cupcfd_gpu_mesh_get_cell_face_csr(const cupcfd_gpu_mesh *mesh, int32_t *xadj, int32_t nXAdj, int32_t *adj, int32_t nAdj);
+
+/* Downloads the FP64 source arrays in the reference's numbering (any pointer
+ * may be NULL): faceCell1/2, faceBnd [nFaces], faceLambda, faceArea [nFaces],
+ * faceNorm, faceCenter [3*nFaces], cellCenter [3*nCells], cellVolume [nCells]. */
+int cupcfd_gpu_mesh_get_geometry(const cupcfd_gpu_mesh *mesh, int32_t *faceCell1, int32_t *faceCell2, int32_t *faceBnd,
+                                 double *faceLambda, double *faceArea, double *faceNorm, double *faceCenter,
+                                 double *cellCenter, double *cellVolume);
+
+/* Internal numbering: cellNew2Old[nCells], faceNew2Old[nFaces] (host, may be NULL). */
+int cupcfd_gpu_mesh_get_numbering(const cupcfd_gpu_mesh *mesh, int32_t *cellNew2Old, int32_t *faceNew2Old);
+
+/* ------------------------------------------------------------------------ */
+/* reference-facing calls (host buffers, reference numbering and layout)     */
+/* ------------------------------------------------------------------------ */
+
+/* GradientPhiGaussDolfyn (include/fvm/implementation/component/GradientKernels.h:48-54,
+ * GradientKernels.ipp:38-136). phiCell[nPhiCell], phiBoundary[nPhiBoundary]
+ * are host arrays of real_size (4 or 8) bytes; dPhidxCell / dPhidxoCell are
+ * host EuclideanVector<T,3> arrays seen through strided views (only the three
+ * components are written; the vptr slot is never touched). nGradient
+ * iterations with the non-orthogonal correction of the previous iterate.
+ * precision: CUPCFD_PREC_F64 (bit-identical to the reference for T=double)
+ * or CUPCFD_PREC_F32C. sign_mode: CUPCFD_SIGN_*. */
+int cupcfd_gpu_gradient_phi_gauss_dolfyn(cupcfd_gpu_mesh *mesh, int32_t nGradient,
+                                         const void *phiCell, int32_t nPhiCell,
+                                         const void *phiBoundary, int32_t nPhiBoundary,
+                                         void *dPhidxCell, int32_t nDPhidxCell, int32_t stride, int32_t offset,
+                                         void *dPhidxoCell, int32_t nDPhidxoCell, int32_t strideo, int32_t offseto,
+                                         int32_t real_size, int32_t precision, int32_t sign_mode);
+
+/* FluxMassDolfynFaceLoop (include/fvm/implementation/component/MassKernels.h:48-81,
+ * MassKernels.ipp:36-309), full semantics: gradient-corrected face velocities,
+ * the Rhie-Chow pressure term written to rface[2*nFaces], and the boundary
+ * region branches (inlet: su[ip] -= flux; outlet: denBoundary and, for
+ * backflow, te/ed/viseff/t boundary copies; symmetry/wall: zero flux),
+ * updating the four counters. All arrays are host, FP64, reference layout;
+ * dudx/dvdx/dwdx/dpdx are EuclideanVector<double,3> views. Arrays the
+ * reference would not touch are not written. */
+int cupcfd_gpu_flux_mass_dolfyn_face_loop(cupcfd_gpu_mesh *mesh,
+                                          cupcfd_vec3_view dudx, int32_t nDudx, cupcfd_vec3_view dvdx, int32_t nDvdx,
+                                          cupcfd_vec3_view dwdx, int32_t nDwdx, cupcfd_vec3_view dpdx, int32_t nDpdx,
+                                          const double *denCell, int32_t nDenCell, double *denBoundary, int32_t nDenBoundary,
+                                          const double *uCell, int32_t nUCell, const double *vCell, int32_t nVCell,
+                                          const double *wCell, int32_t nWCell, double *massFlux, int32_t nMassFlux,
+                                          const double *p, int32_t nP, const double *ar, int32_t nAr,
+                                          double *su, int32_t nSu, double *rface, int32_t nRFace, double small,
+                                          int32_t *icinl, int32_t *icout, int32_t *icsym, int32_t *icwal,
+                                          int32_t solveTurbEnergy, int32_t solveTurbDiss, int32_t solveVisc, int32_t solveEnthalpy,
+                                          const double *teCell, int32_t nTeCell, double *teBoundary, int32_t nTeBoundary,
+                                          const double *edCell, int32_t nEdCell, double *edBoundary, int32_t nEdBoundary,
+                                          const double *viseffCell, int32_t nViseffCell, double *viseffBoundary, int32_t nViseffBoundary,
+                                          const double *tCell, int32_t nTCell, double *tBoundary, int32_t nTBoundary);
+
+/* Forward + adjoint of the plain face loops through host buffers (the
+ * benchmark's end-to-end call). Inputs (host, reference numbering, FP64):
+ * phi[nCells], phiB[nBoundaries], den/u/v/w[nCells], gface[nFaces] (loss
+ * weights). Loss L = sum_c V_c |dPhidx_c|^2 + sum_{interior f} gface_f m_f,
+ * with m_f = rho_f (u_f . S_f). Outputs (host, FP64, any may be NULL):
+ * grad[3*nCells] (xyz interleaved), massFlux[nFaces] (boundary entries 0),
+ * phiBar[nCells], phiBBar[nBoundaries], denBar/uBar/vBar/wBar[nCells],
+ * loss[1]. nGradient is 1. */
+int cupcfd_gpu_forward_adjoint(cupcfd_gpu_mesh *mesh, int32_t precision,
+                               const double *phi, const double *phiB, const double *den, const double *u,
+                               const double *v, const double *w, const double *gface,
+                               double *grad, double *massFlux, double *phiBar, double *phiBBar,
+                               double *denBar, double *uBar, double *vBar, double *wBar, double *loss);
+
+/* ------------------------------------------------------------------------ */
+/* device-resident calls (device pointers, internal numbering, async)        */
+/* ------------------------------------------------------------------------ */
+/* Layouts (internal numbering; T = double for F64, float for F32C):
+ *   cell scalar     T[nCells]
+ *   cell vector     T[3][nCells]   (x block, then y, then z)
+ *   face scalar     T[nFaces]      (internal face order; boundary entries unused)
+ *   boundary scalar T[nBoundaries] (reference boundary order)
+ *   cell state      T[4][nCells]   (rho, u, v, w blocks) for F64,
+ *                   float4[nCells] (rho, u, v, w interleaved) for F32C
+ * stream: a cudaStream_t (NULL = the legacy default stream). */
+
+/* Reorders n-component cell data (component blocks of nCells, element type
+ * src_size / dst_size bytes = 4 or 8, converting) between numberings.
+ * src_stride/dst_stride are the byte distance between component blocks
+ * (0 = packed). to_internal: reference -> internal, else internal -> reference. */
+int cupcfd_gpu_dev_permute_cells(const cupcfd_gpu_mesh *mesh, int32_t to_internal, int32_t ncomp,
+                                 const void *src, int32_t src_size, int64_t src_comp_stride,
+                                 void *dst, int32_t dst_size, int64_t dst_comp_stride, void *stream);
+int cupcfd_gpu_dev_permute_faces(const cupcfd_gpu_mesh *mesh, int32_t to_internal,
+                                 const void *src, int32_t src_size, void *dst, int32_t dst_size, void *stream);
+
+/* Gradient, nGradient iterations (1 = the benchmark setting). grad_o may be
+ * NULL (then an internal buffer holds the previous iterate). */
+int cupcfd_gpu_dev_gradient(cupcfd_gpu_mesh *mesh, int32_t precision, int32_t nGradient, int32_t sign_mode,
+                            const void *phi, const void *phiB, void *grad, void *grad_o, void *stream);
+/* Plain mass flux m_f = rho_f (u_f . S_f) on interior faces; boundary entries untouched. */
+int cupcfd_gpu_dev_mass_plain(cupcfd_gpu_mesh *mesh, int32_t precision, const void *state, void *massFlux, void *stream);
+/* Adjoints: gradient (nGradient = 1): gbar (cell vector) -> phiBar, phiBBar;
+ * plain mass flux: mbar (face scalar) -> stateBar (cell state layout). */
+int cupcfd_gpu_dev_gradient_adjoint(cupcfd_gpu_mesh *mesh, int32_t precision, int32_t sign_mode, const void *gbar,
+                                    void *phiBar, void *phiBBar, void *stream);
+int cupcfd_gpu_dev_mass_plain_adjoint(cupcfd_gpu_mesh *mesh, int32_t precision, const void *state, const void *mbar,
+                                      void *stateBar, void *stream);
+/* Fused forward of both face loops (nGradient = 1): one launch computes
+ * grad (cell vector) and massFlux (face scalar, interior faces) from phi,
+ * phiB and state. With gface and loss non-NULL it also reduces, in FP64 and
+ * in a fixed order, L = sum_c V_c |grad_c|^2 + sum_{interior f} gface_f m_f
+ * into loss (device double[1]). */
+int cupcfd_gpu_dev_forward(cupcfd_gpu_mesh *mesh, int32_t precision, const void *phi, const void *phiB,
+                           const void *state, const void *gface, void *grad, void *massFlux, double *loss, void *stream);
+/* Adjoint of that loss in one launch (the transposed gather): from grad,
+ * state and gface it writes phiBar (cell scalar), phiBBar (boundary scalar)
+ * and stateBar (cell state layout). */
+int cupcfd_gpu_dev_adjoint(cupcfd_gpu_mesh *mesh, int32_t precision, const void *grad, const void *state,
+                           const void *gface, void *phiBar, void *phiBBar, void *stateBar, void *stream);
+/* Fused forward + adjoint of the benchmark loss (see cupcfd_gpu_forward_adjoint):
+ * two launches over the mesh. Outputs grad, massFlux, phiBar, phiBBar,
+ * stateBar; loss (device double[1], may be NULL) reduced in FP64. */
+int cupcfd_gpu_dev_forward_adjoint(cupcfd_gpu_mesh *mesh, int32_t precision, const void *phi, const void *phiB,
+                                   const void *state, const void *gface, void *grad, void *massFlux,
+                                   void *phiBar, void *phiBBar, void *stateBar, double *loss, void *stream);
+
+/* FP64 error norms of a against b (device arrays of n elements each,
+ * a_size/b_size = 4 or 8 bytes): out[0] = max |a-b|, out[1] = max |b|,
+ * out[2] = sum (a-b)^2, out[3] = sum b^2, out[4] = max |a-b| / max(|b|, floor).
+ * out is a host double[5]; the call synchronises the stream. */
+int cupcfd_gpu_dev_error_norms(const void *a, int32_t a_size, const void *b, int32_t b_size, int64_t n, double floor,
+                               double *out, void *stream);
+
+/* Number of kernels this library launched since load (all threads). */
+int64_t cupcfd_gpu_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

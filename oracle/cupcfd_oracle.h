@@ -1,0 +1,96 @@
+/*
+ * cupcfd_oracle.h - plain-C restatement of the reference's CPU algorithm for
+ * the finite-volume face-loop path (Gauss-Green gradient + face mass flux),
+ * plus the structured mesh generator and the cell->face CSR build it runs on.
+ *
+ * TEST INFRASTRUCTURE ONLY. This is the checker for the CUDA library, never
+ * the thing measured or shipped: only tests/, __graft_entry__.smoke() and the
+ * CPU-baseline leg of bench.py load it. The CUDA library does not link it.
+ *
+ * Pinned against: the reference's own golden vectors in
+ * tests/geometry/mesh/implementation/source/MeshStructGenSourceTests.cpp
+ * (fixtures in tests/golden/), and against the reference's own kernels and
+ * generator compiled unchanged into oracle/_ref/libcupcfd_ref.so.
+ *
+ * Conventions: all arrays are flat; 3-vectors are xyz-interleaved [3*n];
+ * indices are 0-based int32; FP64 throughout. Return values are the
+ * reference's eCodes integers (include/error/Error.h:32-144).
+ */
+#ifndef CUPCFD_ORACLE_H
+#define CUPCFD_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* eCodes values of the reference enum (include/error/Error.h:32-144). */
+#define ORC_E_ARRAY_SIZE_MISMATCH 25
+#define ORC_E_INVALID_INDEX 68
+#define ORC_E_SUCCESS 95
+#define ORC_E_ERROR 98
+
+/* RType (include/geometry/mesh/interface/component/UnstructuredMeshInterface.h:58-65) */
+#define ORC_RTYPE_DEFAULT 0
+#define ORC_RTYPE_INLET 1
+#define ORC_RTYPE_OUTLET 2
+#define ORC_RTYPE_SYMP 3
+#define ORC_RTYPE_WALL 4
+
+/* A one-rank CupCfdSoAMesh as the kernels see it
+ * (src/geometry/mesh/implementation/component/CupCfdSoAMesh.cpp, CupCfdSoAMesh.ipp:41-271). */
+typedef struct {
+    int nCells, nFaces, nBnd, nRegions;
+    const int *faceCell1, *faceCell2, *faceBnd;   /* faceCell2 = -1 / faceBnd = -1 as in addFace */
+    const double *faceLambda, *faceNorm, *faceCenter, *faceArea, *faceXpac, *faceXnac;
+    const double *cellCenter, *cellVolume;
+    const int *bndRegion, *regionType;
+    const double *regionUVW, *regionDen;
+} orc_mesh;
+
+/* ---- structured hex generator (MeshStructGenSource.cpp) ---- */
+void orc_structgen_counts(int nx, int ny, int nz, int *nCells, int *nFaces, int *nBnd, int *nVerts);
+int orc_structgen_build(int nx, int ny, int nz,
+                        double xmin, double xmax, double ymin, double ymax, double zmin, double zmax,
+                        int *faceCell1, int *faceCell2, int *faceBnd,
+                        double *faceLambda, double *faceNorm, double *faceCenter, double *faceArea,
+                        double *cellCenter, double *cellVolume, int *faceVert, double *vertCoords);
+int orc_structgen_cell_face_labels(int nx, int ny, int nz, int *xadj, int *adj);
+
+/* ---- jittered + permuted hex mesh (own geometry definition, see .c) ---- */
+int orc_jitter_build(int nx, int ny, int nz, double jitter, unsigned long long seed, int permute,
+                     int *faceCell1, int *faceCell2, int *faceBnd,
+                     double *faceLambda, double *faceNorm, double *faceCenter, double *faceArea,
+                     double *cellCenter, double *cellVolume, int *cellPerm, int *facePerm);
+
+/* ---- cell->face CSR (CupCfdSoAMesh::updateCellFaceMap, CupCfdSoAMesh.cpp:549-668) ---- */
+int orc_cell_face_csr(int nCells, int nFaces, const int *faceCell1, const int *faceCell2, int *xadj, int *adj);
+
+/* ---- kernels ---- */
+int orc_gradient_phi_gauss(const orc_mesh *m, int nGradient,
+                           const double *phi, int nPhi, const double *phiB, int nPhiB,
+                           double *dPhidx, int nDPhidx, double *dPhidxo, int nDPhidxo);
+
+int orc_flux_mass_face_loop(const orc_mesh *m,
+                            const double *dudx, const double *dvdx, const double *dwdx, const double *dpdx,
+                            const double *den, double *denB, const double *u, const double *v, const double *w,
+                            double *massFlux, const double *p, const double *ar, double *su, double *rface,
+                            double small, int *icinl, int *icout, int *icsym, int *icwal,
+                            int solveTurbEnergy, int solveTurbDiss, int solveVisc, int solveEnthalpy,
+                            const double *teC, double *teB, const double *edC, double *edB,
+                            const double *visC, double *visB, const double *tC, double *tB);
+
+/* Adjoints (new; no reference counterpart). Gradient with nGradient = 1:
+ * given gbar[3*nCells] = dL/d(dPhidx), accumulate dL/dphi into phibar[nCells]
+ * and dL/dphiB into phibBar[nBnd]. Plain mass flux m_f = rho_f (u_f . S_f):
+ * given mbar[nFaces] = dL/dm_f (interior faces), accumulate into
+ * rhobar/ubar/vbar/wbar[nCells]. Outputs are overwritten. */
+int orc_gradient_adjoint(const orc_mesh *m, const double *gbar, double *phibar, double *phibBar);
+int orc_mass_plain_forward(const orc_mesh *m, const double *den, const double *u, const double *v, const double *w,
+                           double *massFlux);
+int orc_mass_plain_adjoint(const orc_mesh *m, const double *den, const double *u, const double *v, const double *w,
+                           const double *mbar, double *denbar, double *ubar, double *vbar, double *wbar);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

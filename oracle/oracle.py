@@ -1,0 +1,339 @@
+"""ctypes front end of the test-only checkers.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+the CPU-baseline leg of bench.py, never by the CUDA library's own code.
+
+* ``liboracle.so`` -- the plain-C restatement in cupcfd_oracle.c (always
+  buildable: ``make -C oracle``).
+* ``_ref/libcupcfd_ref.so`` -- the reference's own sources compiled unchanged
+  (``make -C oracle ref``); present only where it was built from a reference
+  source tree, so everything using it is optional.
+
+Meshes are dicts of numpy arrays in the reference's local numbering
+(faces, cells and boundaries in ascending label order); 3-vectors are
+``(n, 3)`` float64 arrays.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import threading
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_lock = threading.Lock()
+_lib = None
+_ref = None
+_ref_tried = False
+
+E_SUCCESS = 95
+E_INVALID_INDEX = 68
+E_ARRAY_SIZE_MISMATCH = 25
+E_ERROR = 98
+
+
+def _p(a):
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"], "arrays must be C-contiguous"
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def load():
+    """Load (building on first use) the C restatement."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            so = os.path.join(HERE, "liboracle.so")
+            src = os.path.join(HERE, "cupcfd_oracle.c")
+            if not os.path.exists(so) or os.path.getmtime(so) < os.path.getmtime(src):
+                subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
+            _lib = C.CDLL(so)
+            _lib.orc_jitter_build.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_ulonglong, C.c_int] + [C.c_void_p] * 11
+            _lib.orc_structgen_build.argtypes = [C.c_int] * 3 + [C.c_double] * 6 + [C.c_void_p] * 11
+            _lib.orc_flux_mass_face_loop.argtypes = [C.c_void_p] * 15 + [C.c_double] + [C.c_void_p] * 4 + [C.c_int] * 4 + [C.c_void_p] * 8
+        return _lib
+
+
+def load_ref():
+    """Load the reference build if it exists (None otherwise)."""
+    global _ref, _ref_tried
+    with _lock:
+        if not _ref_tried:
+            _ref_tried = True
+            so = os.path.join(HERE, "_ref", "libcupcfd_ref.so")
+            if os.path.exists(so):
+                _ref = C.CDLL(so)
+                _ref.ref_structgen_build.argtypes = [C.c_int] * 3 + [C.c_double] * 6 + [C.c_void_p] * 13
+                _ref.ref_ctx_create.restype = C.c_void_p
+                _ref.ref_ctx_create.argtypes = [C.c_int] * 4 + [C.c_void_p] * 15
+                _ref.ref_ctx_destroy.argtypes = [C.c_void_p]
+                _ref.ref_gradient_phi_gauss.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
+                                                        C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
+                _ref.ref_flux_mass_face_loop.argtypes = ([C.c_void_p] * 15 + [C.c_double] + [C.c_void_p] * 4
+                                                         + [C.c_int] * 4 + [C.c_void_p] * 8 + [C.c_int, C.c_void_p])
+        return _ref
+
+
+# ---------------------------------------------------------------------------
+# meshes
+# ---------------------------------------------------------------------------
+
+def counts(nx, ny, nz):
+    nc = nx * ny * nz
+    nf = ny * nz * (nx + 1) + nx * nz * (ny + 1) + nx * ny * (nz + 1)
+    nb = 2 * (ny * nz + nx * nz + nx * ny)
+    nv = (nx + 1) * (ny + 1) * (nz + 1)
+    return nc, nf, nb, nv
+
+
+def _alloc_mesh(nc, nf, nb):
+    return dict(
+        nCells=nc, nFaces=nf, nBnd=nb,
+        faceCell1=np.empty(nf, np.int32), faceCell2=np.empty(nf, np.int32), faceBnd=np.empty(nf, np.int32),
+        faceLambda=np.empty(nf), faceNorm=np.empty((nf, 3)), faceCenter=np.empty((nf, 3)), faceArea=np.empty(nf),
+        cellCenter=np.empty((nc, 3)), cellVolume=np.empty(nc),
+    )
+
+
+def _finish_mesh(m):
+    nf, nb = m["nFaces"], m["nBnd"]
+    m["faceXpac"] = np.zeros((nf, 3))            # addData passes xpac = xnac = 0 (UnstructuredMeshInterface.ipp:1778-1780)
+    m["faceXnac"] = np.zeros((nf, 3))
+    m["nRegions"] = 1
+    m["bndRegion"] = np.zeros(nb, np.int32)      # one region, label 0
+    m["regionType"] = np.zeros(1, np.int32)      # RTYPE_DEFAULT (CupCfdSoAMesh.cpp:211-221)
+    m["regionUVW"] = np.zeros((1, 3))
+    m["regionDen"] = np.zeros(1)
+    return m
+
+
+def structgen(nx, ny, nz, bounds=(0.0, 1.0, 0.0, 1.0, 0.0, 1.0), with_vertices=False):
+    """Structured hex mesh from the C restatement of MeshStructGenSource."""
+    nc, nf, nb, nv = counts(nx, ny, nz)
+    m = _alloc_mesh(nc, nf, nb)
+    fv = np.empty((nf, 4), np.int32) if with_vertices else None
+    vc = np.empty((nv, 3)) if with_vertices else None
+    rc = load().orc_structgen_build(nx, ny, nz, *[float(b) for b in bounds],
+                                    _p(m["faceCell1"]), _p(m["faceCell2"]), _p(m["faceBnd"]),
+                                    _p(m["faceLambda"]), _p(m["faceNorm"]), _p(m["faceCenter"]), _p(m["faceArea"]),
+                                    _p(m["cellCenter"]), _p(m["cellVolume"]), _p(fv), _p(vc))
+    assert rc == E_SUCCESS, rc
+    if with_vertices:
+        m["faceVert"], m["vertCoords"] = fv, vc
+    return _finish_mesh(m)
+
+
+def structgen_cell_face_labels(nx, ny, nz):
+    nc = nx * ny * nz
+    xadj = np.empty(nc + 1, np.int32)
+    adj = np.empty(6 * nc, np.int32)
+    load().orc_structgen_cell_face_labels(nx, ny, nz, _p(xadj), _p(adj))
+    return xadj, adj
+
+
+def jitter(nx, ny, nz, amount=0.25, seed=1, permute=True):
+    """Jittered, optionally permuted hex mesh (geometry defined in cupcfd_oracle.c)."""
+    nc, nf, nb, _ = counts(nx, ny, nz)
+    m = _alloc_mesh(nc, nf, nb)
+    cp = np.empty(nc, np.int32)
+    fp = np.empty(nf, np.int32)
+    rc = load().orc_jitter_build(nx, ny, nz, float(amount), int(seed), int(bool(permute)),
+                                 _p(m["faceCell1"]), _p(m["faceCell2"]), _p(m["faceBnd"]),
+                                 _p(m["faceLambda"]), _p(m["faceNorm"]), _p(m["faceCenter"]), _p(m["faceArea"]),
+                                 _p(m["cellCenter"]), _p(m["cellVolume"]), _p(cp), _p(fp))
+    assert rc == E_SUCCESS, rc
+    m["cellPerm"], m["facePerm"] = cp, fp
+    return _finish_mesh(m)
+
+
+def cell_face_csr(m):
+    nc, nf = m["nCells"], m["nFaces"]
+    nnz = int(nf + np.count_nonzero(m["faceCell2"] >= 0))
+    xadj = np.empty(nc + 1, np.int32)
+    adj = np.empty(nnz, np.int32)
+    rc = load().orc_cell_face_csr(nc, nf, _p(m["faceCell1"]), _p(m["faceCell2"]), _p(xadj), _p(adj))
+    assert rc == E_SUCCESS, rc
+    return xadj, adj
+
+
+class _OrcMesh(C.Structure):
+    _fields_ = [("nCells", C.c_int), ("nFaces", C.c_int), ("nBnd", C.c_int), ("nRegions", C.c_int)] + [
+        (n, C.c_void_p) for n in ("faceCell1", "faceCell2", "faceBnd", "faceLambda", "faceNorm", "faceCenter",
+                                  "faceArea", "faceXpac", "faceXnac", "cellCenter", "cellVolume", "bndRegion",
+                                  "regionType", "regionUVW", "regionDen")]
+
+
+def _cmesh(m):
+    s = _OrcMesh()
+    for k in ("nCells", "nFaces", "nBnd", "nRegions"):
+        setattr(s, k, int(m[k]))
+    for k, _ in _OrcMesh._fields_[4:]:
+        setattr(s, k, _p(m[k]).value if m[k] is not None else None)
+    return s
+
+
+# ---------------------------------------------------------------------------
+# kernels (C restatement)
+# ---------------------------------------------------------------------------
+
+def gradient(m, phi, phib, n_gradient=1):
+    nc = m["nCells"]
+    g = np.empty((nc, 3))
+    go = np.empty((nc, 3))
+    s = _cmesh(m)
+    phi = np.ascontiguousarray(phi, np.float64)
+    phib = np.ascontiguousarray(phib, np.float64)
+    rc = load().orc_gradient_phi_gauss(C.byref(s), n_gradient, _p(phi), len(phi), _p(phib), len(phib),
+                                       _p(g), nc, _p(go), nc)
+    return rc, g, go
+
+
+def flux_mass_face_loop(m, f):
+    """Full FluxMassDolfynFaceLoop. ``f`` is a dict of input arrays; the
+    in/out arrays (massFlux, su, rface, denB, teB, edB, visB, tB) are copied
+    and returned with the four counters."""
+    out = {k: np.array(f[k], np.float64, copy=True) for k in ("massFlux", "su", "rface", "denB", "teB", "edB", "visB", "tB")}
+    cnt = [C.c_int(int(f.get(k, 0))) for k in ("icinl", "icout", "icsym", "icwal")]
+    s = _cmesh(m)
+    a = {k: np.ascontiguousarray(f[k], np.float64) for k in ("dudx", "dvdx", "dwdx", "dpdx", "den", "u", "v", "w", "p", "ar",
+                                                             "teC", "edC", "visC", "tC")}
+    rc = load().orc_flux_mass_face_loop(
+        C.byref(s), _p(a["dudx"]), _p(a["dvdx"]), _p(a["dwdx"]), _p(a["dpdx"]), _p(a["den"]), _p(out["denB"]),
+        _p(a["u"]), _p(a["v"]), _p(a["w"]), _p(out["massFlux"]), _p(a["p"]), _p(a["ar"]), _p(out["su"]), _p(out["rface"]),
+        float(f["small"]), *[C.byref(c) for c in cnt],
+        *[int(bool(f.get(k, False))) for k in ("solveTurbEnergy", "solveTurbDiss", "solveVisc", "solveEnthalpy")],
+        _p(a["teC"]), _p(out["teB"]), _p(a["edC"]), _p(out["edB"]), _p(a["visC"]), _p(out["visB"]), _p(a["tC"]), _p(out["tB"]))
+    out.update(icinl=cnt[0].value, icout=cnt[1].value, icsym=cnt[2].value, icwal=cnt[3].value)
+    return rc, out
+
+
+def mass_plain(m, den, u, v, w, massflux_in=None):
+    mf = np.zeros(m["nFaces"]) if massflux_in is None else np.array(massflux_in, np.float64, copy=True)
+    s = _cmesh(m)
+    args = [np.ascontiguousarray(x, np.float64) for x in (den, u, v, w)]
+    rc = load().orc_mass_plain_forward(C.byref(s), *[_p(x) for x in args], _p(mf))
+    assert rc == E_SUCCESS
+    return mf
+
+
+def mass_plain_adjoint(m, den, u, v, w, mbar):
+    nc = m["nCells"]
+    outs = [np.empty(nc) for _ in range(4)]
+    s = _cmesh(m)
+    args = [np.ascontiguousarray(x, np.float64) for x in (den, u, v, w, mbar)]
+    rc = load().orc_mass_plain_adjoint(C.byref(s), *[_p(x) for x in args], *[_p(o) for o in outs])
+    assert rc == E_SUCCESS
+    return outs
+
+
+def gradient_adjoint(m, gbar):
+    phibar = np.empty(m["nCells"])
+    phibbar = np.empty(m["nBnd"])
+    s = _cmesh(m)
+    gbar = np.ascontiguousarray(gbar, np.float64)
+    rc = load().orc_gradient_adjoint(C.byref(s), _p(gbar), _p(phibar), _p(phibbar))
+    assert rc == E_SUCCESS
+    return phibar, phibbar
+
+
+# ---------------------------------------------------------------------------
+# the reference's own code (optional)
+# ---------------------------------------------------------------------------
+
+def ref_structgen(nx, ny, nz, bounds=(0.0, 1.0, 0.0, 1.0, 0.0, 1.0), with_vertices=False):
+    ref = load_ref()
+    if ref is None:
+        return None
+    nc, nf, nb, nv = counts(nx, ny, nz)
+    m = _alloc_mesh(nc, nf, nb)
+    xadj = np.empty(nc + 1, np.int32)
+    adj = np.empty(6 * nc, np.int32)
+    fv = np.empty((nf, 4), np.int32) if with_vertices else None
+    vc = np.empty((nv, 3)) if with_vertices else None
+    rc = ref.ref_structgen_build(nx, ny, nz, *[float(b) for b in bounds],
+                                 _p(m["faceCell1"]), _p(m["faceCell2"]), _p(m["faceBnd"]),
+                                 _p(m["faceLambda"]), _p(m["faceNorm"]), _p(m["faceCenter"]), _p(m["faceArea"]),
+                                 _p(m["cellCenter"]), _p(m["cellVolume"]), _p(xadj), _p(adj), _p(fv), _p(vc))
+    assert rc == E_SUCCESS, rc
+    m["srcCellFaceXAdj"], m["srcCellFaceAdj"] = xadj, adj
+    if with_vertices:
+        m["faceVert"], m["vertCoords"] = fv, vc
+    return _finish_mesh(m)
+
+
+class RefKernels:
+    """The reference's GradientPhiGaussDolfyn / FluxMassDolfynFaceLoop over a
+    mesh dict. Keeps references to the arrays it was given."""
+
+    def __init__(self, m):
+        self.ref = load_ref()
+        if self.ref is None:
+            raise RuntimeError("reference build absent (make -C oracle ref)")
+        self.m = {k: (np.ascontiguousarray(v) if isinstance(v, np.ndarray) else v) for k, v in m.items()}
+        mm = self.m
+        self.h = self.ref.ref_ctx_create(mm["nCells"], mm["nFaces"], mm["nBnd"], mm["nRegions"],
+                                         *[_p(mm[k]) for k in ("faceCell1", "faceCell2", "faceBnd", "faceLambda", "faceNorm",
+                                                                "faceCenter", "faceArea", "faceXpac", "faceXnac",
+                                                                "cellCenter", "cellVolume", "bndRegion", "regionType",
+                                                                "regionUVW", "regionDen")])
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.ref.ref_ctx_destroy(self.h)
+            self.h = None
+
+    def gradient(self, phi, phib, n_gradient=1, reps=1):
+        nc = self.m["nCells"]
+        g = np.empty((nc, 3))
+        go = np.empty((nc, 3))
+        secs = np.empty(reps)
+        self._phi = np.ascontiguousarray(phi, np.float64)
+        self._phib = np.ascontiguousarray(phib, np.float64)
+        rc = self.ref.ref_gradient_phi_gauss(self.h, n_gradient, _p(self._phi), len(self._phi), _p(self._phib),
+                                             len(self._phib), _p(g), _p(go), reps, _p(secs))
+        return rc, g, go, secs
+
+    def flux_mass(self, f, reps=1):
+        out = {k: np.array(f[k], np.float64, copy=True) for k in ("massFlux", "su", "rface", "denB", "teB", "edB", "visB", "tB")}
+        cnt = [C.c_int(int(f.get(k, 0))) for k in ("icinl", "icout", "icsym", "icwal")]
+        a = {k: np.ascontiguousarray(f[k], np.float64) for k in ("dudx", "dvdx", "dwdx", "dpdx", "den", "u", "v", "w", "p",
+                                                                 "ar", "teC", "edC", "visC", "tC")}
+        secs = np.empty(reps)
+        rc = self.ref.ref_flux_mass_face_loop(
+            self.h, _p(a["dudx"]), _p(a["dvdx"]), _p(a["dwdx"]), _p(a["dpdx"]), _p(a["den"]), _p(out["denB"]),
+            _p(a["u"]), _p(a["v"]), _p(a["w"]), _p(out["massFlux"]), _p(a["p"]), _p(a["ar"]), _p(out["su"]),
+            _p(out["rface"]), float(f["small"]), *[C.byref(c) for c in cnt],
+            *[int(bool(f.get(k, False))) for k in ("solveTurbEnergy", "solveTurbDiss", "solveVisc", "solveEnthalpy")],
+            _p(a["teC"]), _p(out["teB"]), _p(a["edC"]), _p(out["edB"]), _p(a["visC"]), _p(out["visB"]), _p(a["tC"]),
+            _p(out["tB"]), reps, _p(secs))
+        out.update(icinl=cnt[0].value, icout=cnt[1].value, icsym=cnt[2].value, icwal=cnt[3].value)
+        return rc, out, secs
+
+
+# ---------------------------------------------------------------------------
+# seeded synthetic fields (Philox4x32-10 via numpy)
+# ---------------------------------------------------------------------------
+
+def fields(m, seed, full=False):
+    """phi ~ U[-1,1], u,v,w ~ N(0,1), rho ~ U[0.9,1.1], phiB ~ U[-1,1] from a
+    Philox4x32-10 stream keyed by ``seed``. With ``full``, also seeds the
+    inputs the plain form holds at zero (velocity/pressure gradients ~ N(0,1),
+    p ~ U[-1,1]) and ar ~ U[0.9,1.1]."""
+    nc, nf, nb = m["nCells"], m["nFaces"], m["nBnd"]
+    r = np.random.Generator(np.random.Philox(key=seed))
+    f = dict(phi=r.uniform(-1, 1, nc), u=r.standard_normal(nc), v=r.standard_normal(nc), w=r.standard_normal(nc),
+             den=r.uniform(0.9, 1.1, nc), phiB=r.uniform(-1, 1, nb))
+    z3 = np.zeros((nc, 3))
+    if full:
+        f.update(dudx=r.standard_normal((nc, 3)), dvdx=r.standard_normal((nc, 3)), dwdx=r.standard_normal((nc, 3)),
+                 dpdx=r.standard_normal((nc, 3)), p=r.uniform(-1, 1, nc), ar=r.uniform(0.9, 1.1, nc))
+    else:
+        f.update(dudx=z3, dvdx=z3.copy(), dwdx=z3.copy(), dpdx=z3.copy(), p=np.zeros(nc), ar=r.uniform(0.9, 1.1, nc))
+    f.update(massFlux=np.zeros(nf), su=np.zeros(nc), rface=np.zeros(2 * nf), denB=np.zeros(nb),
+             teC=r.uniform(size=nc), edC=r.uniform(size=nc), visC=r.uniform(size=nc), tC=r.uniform(size=nc),
+             teB=np.zeros(nb), edB=np.zeros(nb), visB=np.zeros(nb), tB=np.zeros(nb), small=1e-18,
+             solveTurbEnergy=False, solveTurbDiss=False, solveVisc=True, solveEnthalpy=False)
+    return f

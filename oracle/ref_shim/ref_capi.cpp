@@ -1,0 +1,260 @@
+/*
+ * C entry points over the reference's OWN CPU code, compiled unchanged from
+ * the reference source tree into oracle/_ref/libcupcfd_ref.so by
+ * oracle/Makefile (target "ref").
+ *
+ * TEST INFRASTRUCTURE ONLY. Nothing in the shipped library links this. It is
+ * used (a) in this container to validate the plain-C restatement in
+ * oracle/cupcfd_oracle.c, and (b) as the timed CPU reference arm.
+ *
+ * Wrapped reference code:
+ *   - cupcfd::fvm::GradientPhiGaussDolfyn   include/fvm/implementation/component/GradientKernels.ipp:38-136
+ *   - cupcfd::fvm::FluxMassDolfynFaceLoop   include/fvm/implementation/component/MassKernels.ipp:36-309
+ *   - MeshStructGenSource<int,double>       src/geometry/mesh/implementation/source/MeshStructGenSource.cpp:33-1277
+ * The mesh the kernels see is the one-rank CupCfdSoAMesh that addData
+ * (include/geometry/mesh/interface/component/UnstructuredMeshInterface.ipp:1464-1862)
+ * builds from the generator: faces, boundaries and cells in ascending label
+ * order, xpac = xnac = 0, every region RTYPE_DEFAULT.
+ */
+#include <chrono>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+#include <algorithm>
+
+#include "Error.h"
+#include "EuclideanVector.h"
+#include "EuclideanPoint.h"
+#include "GradientKernels.h"
+#include "MassKernels.h"
+#include "MeshStructGenSource.h"
+
+namespace euc = cupcfd::geometry::euclidean;
+namespace msh = cupcfd::geometry::mesh;
+
+typedef msh::UnstructuredMeshInterface<int, int, double, int> RefMesh;
+
+/* Error code values, exported so the tests can pin the C ABI's constants. */
+extern "C" int ref_ecode_success() { return (int) cupcfd::error::E_SUCCESS; }
+extern "C" int ref_ecode_invalid_index() { return (int) cupcfd::error::E_INVALID_INDEX; }
+extern "C" int ref_ecode_array_size_mismatch() { return (int) cupcfd::error::E_ARRAY_SIZE_MISMATCH; }
+extern "C" int ref_ecode_error() { return (int) cupcfd::error::E_ERROR; }
+extern "C" int ref_ecode_null_ptr() { return (int) cupcfd::error::E_NULL_PTR; }
+extern "C" int ref_ecode_not_implemented() { return (int) cupcfd::error::E_NOT_IMPLEMENTED; }
+extern "C" int ref_sizeof_euclidean_vector_f64() { return (int) sizeof(euc::EuclideanVector<double,3>); }
+extern "C" int ref_sizeof_euclidean_vector_f32() { return (int) sizeof(euc::EuclideanVector<float,3>); }
+extern "C" int ref_offsetof_cmp_f64() {
+	euc::EuclideanVector<double,3> v;
+	return (int) ((char *) &v.cmp[0] - (char *) &v);
+}
+
+/* ---- structured generator ------------------------------------------------ */
+
+extern "C" void ref_structgen_counts(int nx, int ny, int nz, int * nCells, int * nFaces, int * nBnd, int * nVerts) {
+	msh::MeshStructGenSource<int, double> src(nx, ny, nz, 0.0, 1.0, 0.0, 1.0, 0.0, 1.0);
+	src.getCellCount(nCells);
+	src.getFaceCount(nFaces);
+	src.getBoundaryCount(nBnd);
+	src.getVertexCount(nVerts);
+}
+
+/* Build every array the face loops read, for all labels in ascending order.
+ * faceBnd[f] is the boundary label of f, or -1 for an interior face. */
+extern "C" int ref_structgen_build(int nx, int ny, int nz,
+                                   double xmin, double xmax, double ymin, double ymax, double zmin, double zmax,
+                                   int * faceCell1, int * faceCell2, int * faceBnd,
+                                   double * faceLambda, double * faceNorm, double * faceCenter, double * faceArea,
+                                   double * cellCenter, double * cellVolume,
+                                   int * cellFaceXAdj, int * cellFaceAdj,
+                                   int * faceVert, double * vertCoords) {
+	msh::MeshStructGenSource<int, double> src(nx, ny, nz, xmin, xmax, ymin, ymax, zmin, zmax);
+	int nC, nF, nB, nV;
+	src.getCellCount(&nC);
+	src.getFaceCount(&nF);
+	src.getBoundaryCount(&nB);
+	src.getVertexCount(&nV);
+	cupcfd::error::eCodes st;
+
+	std::vector<int> cl(nC), fl(nF), vl(nV);
+	for (int i = 0; i < nC; i++) cl[i] = i;
+	for (int i = 0; i < nF; i++) fl[i] = i;
+	for (int i = 0; i < nV; i++) vl[i] = i;
+
+	bool * isB = (bool *) malloc(sizeof(bool) * nF);
+	st = src.getFaceIsBoundary(isB, nF, fl.data(), nF);
+	if (st != cupcfd::error::E_SUCCESS) return (int) st;
+	st = src.getFaceCell1Labels(faceCell1, nF, fl.data(), nF);
+	if (st != cupcfd::error::E_SUCCESS) return (int) st;
+
+	std::vector<int> interior, boundary;
+	for (int f = 0; f < nF; f++) (isB[f] ? boundary : interior).push_back(f);
+	std::vector<int> c2(interior.size()), bl(boundary.size());
+	if (!interior.empty()) {
+		st = src.getFaceCell2Labels(c2.data(), (int) interior.size(), interior.data(), (int) interior.size());
+		if (st != cupcfd::error::E_SUCCESS) return (int) st;
+	}
+	if (!boundary.empty()) {
+		st = src.getFaceBoundaryLabels(bl.data(), (int) boundary.size(), boundary.data(), (int) boundary.size());
+		if (st != cupcfd::error::E_SUCCESS) return (int) st;
+	}
+	for (int f = 0; f < nF; f++) { faceCell2[f] = -1; faceBnd[f] = -1; }
+	for (size_t k = 0; k < interior.size(); k++) faceCell2[interior[k]] = c2[k];
+	for (size_t k = 0; k < boundary.size(); k++) faceBnd[boundary[k]] = bl[k];
+	free(isB);
+
+	st = src.getFaceLambda(faceLambda, nF, fl.data(), nF);
+	if (st != cupcfd::error::E_SUCCESS) return (int) st;
+	st = src.getFaceArea(faceArea, nF, fl.data(), nF);
+	if (st != cupcfd::error::E_SUCCESS) return (int) st;
+
+	std::vector<euc::EuclideanVector<double,3>> nrm(nF);
+	st = src.getFaceNormal(nrm.data(), nF, fl.data(), nF);
+	if (st != cupcfd::error::E_SUCCESS) return (int) st;
+	std::vector<euc::EuclideanPoint<double,3>> fc(nF);
+	st = src.getFaceCenter(fc.data(), nF, fl.data(), nF);
+	if (st != cupcfd::error::E_SUCCESS) return (int) st;
+	for (int f = 0; f < nF; f++) {
+		for (int d = 0; d < 3; d++) {
+			faceNorm[3*f+d] = nrm[f].cmp[d];
+			faceCenter[3*f+d] = fc[f].cmp[d];
+		}
+	}
+
+	std::vector<euc::EuclideanPoint<double,3>> cc(nC);
+	st = src.getCellCenter(cc.data(), nC, cl.data(), nC);
+	if (st != cupcfd::error::E_SUCCESS) return (int) st;
+	st = src.getCellVolume(cellVolume, nC, cl.data(), nC);
+	if (st != cupcfd::error::E_SUCCESS) return (int) st;
+	for (int c = 0; c < nC; c++)
+		for (int d = 0; d < 3; d++) cellCenter[3*c+d] = cc[c].cmp[d];
+
+	if (cellFaceXAdj && cellFaceAdj) {
+		st = src.getCellFaceLabels(cellFaceXAdj, nC + 1, cellFaceAdj, 6 * nC, cl.data(), nC);
+		if (st != cupcfd::error::E_SUCCESS) return (int) st;
+	}
+	if (faceVert) {
+		std::vector<int> xadj(nF + 1);
+		st = src.getFaceVerticesLabelsCSR(xadj.data(), nF + 1, faceVert, 4 * nF, fl.data(), nF);
+		if (st != cupcfd::error::E_SUCCESS) return (int) st;
+	}
+	if (vertCoords) {
+		std::vector<euc::EuclideanPoint<double,3>> vc(nV);
+		st = src.getVertexCoords(vc.data(), nV, vl.data(), nV);
+		if (st != cupcfd::error::E_SUCCESS) return (int) st;
+		for (int v = 0; v < nV; v++)
+			for (int d = 0; d < 3; d++) vertCoords[3*v+d] = vc[v].cmp[d];
+	}
+	return (int) cupcfd::error::E_SUCCESS;
+}
+
+/* ---- kernel context --------------------------------------------------------
+ * Holds a shim mesh over caller-owned arrays plus the reference's vptr'd
+ * EuclideanVector field arrays, so that timing covers only the kernel call,
+ * as the reference's TreeTimer block does (src/benchmarks/.../BenchmarkKernels.cpp:166-186). */
+struct RefCtx {
+	RefMesh mesh;
+	int nC, nF, nB, nR;
+	std::vector<euc::EuclideanVector<double,3>> g, go;
+	std::vector<euc::EuclideanVector<double,3>> dudx, dvdx, dwdx, dpdx;
+};
+
+extern "C" void * ref_ctx_create(int nCells, int nFaces, int nBnd, int nRegions,
+                                 const int * faceCell1, const int * faceCell2, const int * faceBnd,
+                                 const double * faceLambda, const double * faceNorm, const double * faceCenter,
+                                 const double * faceArea, const double * faceXpac, const double * faceXnac,
+                                 const double * cellCenter, const double * cellVolume,
+                                 const int * boundaryRegion, const int * regionType,
+                                 const double * regionUVW, const double * regionDen) {
+	RefCtx * c = new RefCtx();
+	c->nC = nCells; c->nF = nFaces; c->nB = nBnd; c->nR = nRegions;
+	c->mesh.properties.lOCells = nCells;
+	c->mesh.properties.lGhCells = 0;
+	c->mesh.properties.lTCells = nCells;
+	c->mesh.properties.lFaces = nFaces;
+	c->mesh.properties.lBoundaries = nBnd;
+	c->mesh.properties.lRegions = nRegions;
+	c->mesh.a.faceCell1 = faceCell1;
+	c->mesh.a.faceCell2 = faceCell2;
+	c->mesh.a.faceBoundary = faceBnd;
+	c->mesh.a.faceLambda = faceLambda;
+	c->mesh.a.faceNorm = faceNorm;
+	c->mesh.a.faceCenter = faceCenter;
+	c->mesh.a.faceArea = faceArea;
+	c->mesh.a.faceXpac = faceXpac;
+	c->mesh.a.faceXnac = faceXnac;
+	c->mesh.a.cellCenter = cellCenter;
+	c->mesh.a.cellVolume = cellVolume;
+	c->mesh.a.boundaryRegion = boundaryRegion;
+	c->mesh.a.regionType = regionType;
+	c->mesh.a.regionUVW = regionUVW;
+	c->mesh.a.regionDen = regionDen;
+	c->g.resize(nCells);
+	c->go.resize(nCells);
+	return c;
+}
+
+extern "C" void ref_ctx_destroy(void * p) { delete (RefCtx *) p; }
+
+static void unpackVec(const std::vector<euc::EuclideanVector<double,3>> & v, double * out) {
+	for (size_t i = 0; i < v.size(); i++)
+		for (int d = 0; d < 3; d++) out[3*i+d] = v[i].cmp[d];
+}
+static void packVec(std::vector<euc::EuclideanVector<double,3>> & v, const double * in, int n) {
+	v.resize(n);
+	for (int i = 0; i < n; i++)
+		for (int d = 0; d < 3; d++) v[i].cmp[d] = in[3*i+d];
+}
+
+/* Runs GradientPhiGaussDolfyn `reps` times; per-call seconds go to secs[reps]
+ * (may be NULL). Outputs are the last call's dPhidxCell / dPhidxoCell. */
+extern "C" int ref_gradient_phi_gauss(void * p, int nGradient, double * phi, int nPhi, double * phiB, int nPhiB,
+                                      double * dPhidx, double * dPhidxo, int reps, double * secs) {
+	RefCtx * c = (RefCtx *) p;
+	cupcfd::error::eCodes st = cupcfd::error::E_SUCCESS;
+	for (int r = 0; r < reps; r++) {
+		auto t0 = std::chrono::steady_clock::now();
+		st = cupcfd::fvm::GradientPhiGaussDolfyn(c->mesh, nGradient, phi, nPhi, phiB, nPhiB,
+		                                         c->g.data(), c->nC, c->go.data(), c->nC);
+		auto t1 = std::chrono::steady_clock::now();
+		if (secs) secs[r] = std::chrono::duration<double>(t1 - t0).count();
+		if (st != cupcfd::error::E_SUCCESS) return (int) st;
+	}
+	if (dPhidx) unpackVec(c->g, dPhidx);
+	if (dPhidxo) unpackVec(c->go, dPhidxo);
+	return (int) st;
+}
+
+/* Runs FluxMassDolfynFaceLoop `reps` times with the reference's full
+ * argument list. Vector fields are xyz-interleaved [3*nCells]. The arrays
+ * massFlux, su, rface, denB and the te/ed/viseff/t boundary arrays are
+ * updated in place exactly as the reference does. */
+extern "C" int ref_flux_mass_face_loop(void * p,
+                                       const double * dudx, const double * dvdx, const double * dwdx, const double * dpdx,
+                                       double * den, double * denB, double * u, double * v, double * w,
+                                       double * massFlux, double * pr, double * ar, double * su, double * rface,
+                                       double small, int * icinl, int * icout, int * icsym, int * icwal,
+                                       int solveTurbEnergy, int solveTurbDiss, int solveVisc, int solveEnthalpy,
+                                       double * teC, double * teB, double * edC, double * edB,
+                                       double * visC, double * visB, double * tC, double * tB,
+                                       int reps, double * secs) {
+	RefCtx * c = (RefCtx *) p;
+	int nC = c->nC, nF = c->nF, nB = c->nB;
+	packVec(c->dudx, dudx, nC);
+	packVec(c->dvdx, dvdx, nC);
+	packVec(c->dwdx, dwdx, nC);
+	packVec(c->dpdx, dpdx, nC);
+	cupcfd::error::eCodes st = cupcfd::error::E_SUCCESS;
+	for (int r = 0; r < reps; r++) {
+		auto t0 = std::chrono::steady_clock::now();
+		st = cupcfd::fvm::FluxMassDolfynFaceLoop(c->mesh,
+			c->dudx.data(), nC, c->dvdx.data(), nC, c->dwdx.data(), nC, c->dpdx.data(), nC,
+			den, nC, denB, nB, u, nC, v, nC, w, nC, massFlux, nF, pr, nC, ar, nC, su, nC, rface, 2 * nF,
+			small, icinl, icout, icsym, icwal,
+			solveTurbEnergy != 0, solveTurbDiss != 0, solveVisc != 0, solveEnthalpy != 0,
+			teC, nC, teB, nB, edC, nC, edB, nB, visC, nC, visB, nB, tC, nC, tB, nB);
+		auto t1 = std::chrono::steady_clock::now();
+		if (secs) secs[r] = std::chrono::duration<double>(t1 - t0).count();
+		if (st != cupcfd::error::E_SUCCESS) return (int) st;
+	}
+	return (int) st;
+}

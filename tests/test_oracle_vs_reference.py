@@ -1,0 +1,102 @@
+"""Validates the plain-C oracle against the reference's own code, compiled
+unchanged from its sources into oracle/_ref/libcupcfd_ref.so (make -C oracle
+ref). Skipped where that build is absent. CPU only."""
+import numpy as np
+import pytest
+
+import oracle as O
+
+pytestmark = pytest.mark.skipif(O.load_ref() is None, reason="reference build absent (make -C oracle ref)")
+
+DIMS = [(2, 3, 4), (5, 4, 3), (16, 16, 16), (1, 1, 1), (9, 2, 5)]
+BOUNDS = [(0.0, 1.0, 0.0, 1.0, 0.0, 1.0), (-1.0, 1.0, -1.0, 2.0, 0.0, 2.0), (0.0, 3.0, -0.5, 0.25, 1.0, 1.7)]
+
+
+@pytest.mark.parametrize("dims", DIMS)
+@pytest.mark.parametrize("bounds", BOUNDS)
+def test_structgen_geometry_bit_exact(dims, bounds):
+    a = O.structgen(*dims, bounds=bounds, with_vertices=True)
+    b = O.ref_structgen(*dims, bounds=bounds, with_vertices=True)
+    for k in ("faceCell1", "faceCell2", "faceBnd", "faceLambda", "faceNorm", "faceCenter", "faceArea", "cellCenter",
+              "faceVert", "vertCoords"):
+        assert np.array_equal(a[k], b[k]), k
+    # volume: exact box volume vs the reference's five-tetrahedron Heron sum,
+    # whose own rounding reaches ~1e-14 relative on stretched cells
+    rel = np.abs(a["cellVolume"] - b["cellVolume"]) / np.abs(b["cellVolume"])
+    assert rel.max() <= 2e-14
+
+
+@pytest.mark.parametrize("dims", DIMS[:3])
+def test_csr_matches_source(dims):
+    b = O.ref_structgen(*dims)
+    xadj, adj = O.cell_face_csr(b)
+    sx, sa = b["srcCellFaceXAdj"], b["srcCellFaceAdj"]
+    assert np.array_equal(xadj, sx)
+    for c in range(len(sx) - 1):
+        assert np.array_equal(adj[sx[c]:sx[c + 1]], np.sort(sa[sx[c]:sx[c + 1]]))
+
+
+@pytest.mark.parametrize("dims", [(2, 3, 4), (8, 8, 8), (5, 4, 3)])
+@pytest.mark.parametrize("ngrad", [0, 1, 2, 3])
+def test_gradient_bit_exact(dims, ngrad):
+    m = O.ref_structgen(*dims)
+    f = O.fields(m, 11, full=True)
+    rc, g, go = O.gradient(m, f["phi"], f["phiB"], ngrad)
+    R = O.RefKernels(m)
+    rc2, g2, go2, _ = R.gradient(f["phi"], f["phiB"], ngrad)
+    assert rc == rc2 == O.E_SUCCESS
+    if ngrad > 0:
+        assert np.array_equal(g, g2)
+    assert np.array_equal(go, go2)
+
+
+@pytest.mark.parametrize("full", [False, True])
+@pytest.mark.parametrize("regions", [False, True])
+def test_mass_flux_bit_exact(full, regions):
+    m = O.ref_structgen(6, 5, 4)
+    if regions:
+        m = dict(m)
+        m["nRegions"] = 5
+        m["regionType"] = np.array([0, 1, 2, 3, 4], np.int32)
+        rng = np.random.default_rng(3)
+        m["regionUVW"] = rng.standard_normal((5, 3))
+        m["regionDen"] = rng.uniform(0.5, 1.5, 5)
+        m["bndRegion"] = rng.integers(0, 5, m["nBnd"]).astype(np.int32)
+    f = O.fields(m, 5, full=full)
+    f["solveTurbEnergy"] = f["solveTurbDiss"] = f["solveEnthalpy"] = True
+    rc, out = O.flux_mass_face_loop(m, f)
+    R = O.RefKernels(m)
+    rc2, out2, _ = R.flux_mass(f)
+    assert rc == rc2 == O.E_SUCCESS
+    for k in ("massFlux", "su", "rface", "denB", "teB", "edB", "visB", "tB"):
+        assert np.array_equal(out[k], out2[k]), k
+    for k in ("icinl", "icout", "icsym", "icwal"):
+        assert out[k] == out2[k]
+
+
+def test_jittered_mesh_through_reference_kernels():
+    """The reference kernels accept the jittered + permuted mesh arrays
+    (as they would from MeshHDF5Source) and agree with the oracle bit for bit."""
+    m = O.jitter(6, 5, 7, 0.25, seed=4, permute=True)
+    f = O.fields(m, 9, full=True)
+    rc, g, go = O.gradient(m, f["phi"], f["phiB"], 2)
+    R = O.RefKernels(m)
+    rc2, g2, go2, _ = R.gradient(f["phi"], f["phiB"], 2)
+    assert rc == rc2 == O.E_SUCCESS and np.array_equal(g, g2)
+    rc, out = O.flux_mass_face_loop(m, f)
+    rc2, out2, _ = R.flux_mass(f)
+    assert np.array_equal(out["massFlux"], out2["massFlux"]) and np.array_equal(out["rface"], out2["rface"])
+
+
+def test_error_codes_match_reference_enum():
+    ref = O.load_ref()
+    assert ref.ref_ecode_success() == O.E_SUCCESS == 95
+    assert ref.ref_ecode_invalid_index() == O.E_INVALID_INDEX == 68
+    assert ref.ref_ecode_array_size_mismatch() == O.E_ARRAY_SIZE_MISMATCH == 25
+    assert ref.ref_ecode_error() == O.E_ERROR == 98
+    assert ref.ref_ecode_null_ptr() == 99
+    assert ref.ref_ecode_not_implemented() == 109
+    # EuclideanVector<T,3> carries a vptr: 32-byte (double) / 24-byte (float) stride, components at +8
+    assert ref.ref_sizeof_euclidean_vector_f64() == 32
+    assert ref.ref_sizeof_euclidean_vector_f32() == 24
+    assert ref.ref_offsetof_cmp_f64() == 8
