@@ -21,7 +21,9 @@ import threading
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libcupcfd_gpu.so")
+# CUPCFD_GPU_LIB selects another build of the same library (e.g. a variant
+# built with different CUPCFD_* tuning macros); default: the in-tree build.
+LIB_PATH = os.environ.get("CUPCFD_GPU_LIB") or os.path.join(HERE, "libcupcfd_gpu.so")
 
 # eCodes values (include/error/Error.h)
 E_ARRAY_SIZE_MISMATCH = 25
@@ -34,7 +36,7 @@ E_NOT_IMPLEMENTED = 109
 
 RTYPE_DEFAULT, RTYPE_INLET, RTYPE_OUTLET, RTYPE_SYMP, RTYPE_WALL = range(5)
 PREC_F64, PREC_F32C = 0, 1
-ORDER_NATIVE, ORDER_MORTON, ORDER_OWNER = 0, 1, 2
+ORDER_NATIVE, ORDER_MORTON, ORDER_OWNER, ORDER_RCM = 0, 1, 2, 3
 SIGN_REFERENCE, SIGN_SIGNED = 0, 1
 
 _lock = threading.Lock()
@@ -65,7 +67,7 @@ class MeshOptions(C.Structure):
 
 class MeshInfo(C.Structure):
     _fields_ = [(n, C.c_int32) for n in ("nCells", "nFaces", "nInteriorFaces", "nBoundaries", "nRegions",
-                                         "nIncidences", "maxCellFaces", "order", "precisions")] + [
+                                         "nIncidences", "maxCellFaces", "order", "precisions", "bandwidth")] + [
         ("deviceBytes", C.c_int64)]
 
 
@@ -81,12 +83,14 @@ SIGNATURES = {
     "cupcfd_gpu_mesh_destroy": ([_VP], _I),
     "cupcfd_gpu_mesh_get_info": ([_VP, _VP], _I),
     "cupcfd_gpu_mesh_set_regions": ([_VP, _I, _VP, _VP, _VP, _VP, _I], _I),
+    "cupcfd_gpu_mesh_set_fusion": ([_VP, _I], _I),
+    "cupcfd_gpu_mesh_check_status": ([_VP, _VP], _I),
     "cupcfd_gpu_mesh_get_cell_face_csr": ([_VP, _VP, _I, _VP, _I], _I),
     "cupcfd_gpu_mesh_get_geometry": ([_VP] * 10, _I),
     "cupcfd_gpu_mesh_get_numbering": ([_VP, _VP, _VP], _I),
     "cupcfd_gpu_gradient_phi_gauss_dolfyn": ([_VP, _I, _VP, _I, _VP, _I, _VP, _I, _I, _I, _VP, _I, _I, _I, _I, _I, _I], _I),
     "cupcfd_gpu_flux_mass_dolfyn_face_loop": ([_VP, Vec3View, _I, Vec3View, _I, Vec3View, _I, Vec3View, _I]
-                                              + [_VP, _I] * 14 + [_D] + [_VP] * 4 + [_I] * 4 + [_VP, _I] * 8, _I),
+                                              + [_VP, _I] * 10 + [_D] + [_VP] * 4 + [_I] * 4 + [_VP, _I] * 8, _I),
     "cupcfd_gpu_forward_adjoint": ([_VP, _I] + [_VP] * 16, _I),
     "cupcfd_gpu_dev_permute_cells": ([_VP, _I, _I, _VP, _I, _I64, _VP, _I, _I64, _VP], _I),
     "cupcfd_gpu_dev_permute_faces": ([_VP, _I, _VP, _I, _VP, _I, _VP], _I),
@@ -180,6 +184,7 @@ class Mesh:
         self.nCells, self.nFaces, self.nInteriorFaces = info.nCells, info.nFaces, info.nInteriorFaces
         self.nBoundaries, self.nIncidences, self.maxCellFaces = info.nBoundaries, info.nIncidences, info.maxCellFaces
         self.order, self.precisions, self.deviceBytes = info.order, info.precisions, info.deviceBytes
+        self.bandwidth = info.bandwidth
 
     @staticmethod
     def _opts(order, precisions, device):
@@ -249,6 +254,13 @@ class Mesh:
         den = np.ascontiguousarray(region_den, np.float64)
         br = np.ascontiguousarray(bnd_region, np.int32)
         return lib().cupcfd_gpu_mesh_set_regions(self.h, len(rt), _p(rt), _p(uvw), _p(den), _p(br), len(br))
+
+    def set_fusion(self, mode):
+        """0 auto, 1 always fused, 2 never fused (forward+adjoint)."""
+        check(lib().cupcfd_gpu_mesh_set_fusion(self.h, int(mode)))
+
+    def check_status(self, stream=None):
+        return lib().cupcfd_gpu_mesh_check_status(self.h, _stream(stream))
 
     def cell_face_csr(self):
         xadj = np.empty(self.nCells + 1, np.int32)

@@ -2,8 +2,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <cstdlib>
 
-#include "kernels_adj.cuh"
+#include "kernels_fused.cuh"
 
 using namespace cupcfd_gpu;
 
@@ -122,23 +123,141 @@ int launch_grad_once(cupcfd_gpu_mesh *m, int precision, bool corr, bool sgn, con
     if (precision == CUPCFD_PREC_F64) {
         const double *pp = (const double *) phi, *pb = (const double *) phiB, *go = (const double *) prev;
         double *g = (double *) grad, *gc = (double *) gcopy;
-        if (!corr && !sgn) k_grad_f64<false, false><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->faceCells, m->fg64, m->fc64, m->cc64, pp, pb, m->vol, go, g, gc, ldc);
-        else if (!corr && sgn) k_grad_f64<false, true><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->faceCells, m->fg64, m->fc64, m->cc64, pp, pb, m->vol, go, g, gc, ldc);
-        else if (corr && !sgn) k_grad_f64<true, false><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->faceCells, m->fg64, m->fc64, m->cc64, pp, pb, m->vol, go, g, gc, ldc);
-        else k_grad_f64<true, true><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->faceCells, m->fg64, m->fc64, m->cc64, pp, pb, m->vol, go, g, gc, ldc);
+        if (!corr && !sgn) k_grad_f64<false, false><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg64, m->fc64, m->cc64, pp, pb, m->vol, go, g, gc, ldc);
+        else if (!corr && sgn) k_grad_f64<false, true><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg64, m->fc64, m->cc64, pp, pb, m->vol, go, g, gc, ldc);
+        else if (corr && !sgn) k_grad_f64<true, false><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg64, m->fc64, m->cc64, pp, pb, m->vol, go, g, gc, ldc);
+        else k_grad_f64<true, true><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg64, m->fc64, m->cc64, pp, pb, m->vol, go, g, gc, ldc);
     } else {
         const float *pp = (const float *) phi, *pb = (const float *) phiB, *go = (const float *) prev;
         float *g = (float *) grad, *gc = (float *) gcopy;
-        if (!corr && !sgn) k_grad_f32<false, false><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->faceCells, m->fg32, m->fc32, m->cc32, pp, pb, m->vol, go, g, gc, ldc);
-        else if (!corr && sgn) k_grad_f32<false, true><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->faceCells, m->fg32, m->fc32, m->cc32, pp, pb, m->vol, go, g, gc, ldc);
-        else if (corr && !sgn) k_grad_f32<true, false><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->faceCells, m->fg32, m->fc32, m->cc32, pp, pb, m->vol, go, g, gc, ldc);
-        else k_grad_f32<true, true><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->faceCells, m->fg32, m->fc32, m->cc32, pp, pb, m->vol, go, g, gc, ldc);
+        if (!corr && !sgn) k_grad_f32<false, false><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg32, m->fc32, m->cc32, pp, pb, m->vol, go, g, gc, ldc);
+        else if (!corr && sgn) k_grad_f32<false, true><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg32, m->fc32, m->cc32, pp, pb, m->vol, go, g, gc, ldc);
+        else if (corr && !sgn) k_grad_f32<true, false><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg32, m->fc32, m->cc32, pp, pb, m->vol, go, g, gc, ldc);
+        else k_grad_f32<true, true><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg32, m->fc32, m->cc32, pp, pb, m->vol, go, g, gc, ldc);
     }
     CG_LAUNCHED();
     return CUPCFD_E_SUCCESS;
 }
 
 }  // namespace
+
+namespace cupcfd_gpu {
+int mesh_post_build(cupcfd_gpu_mesh *m, cudaStream_t st) {
+    int nC = m->nC;
+    int *bw;
+    CG_TRY(scratch(m, S_ERR, 1, &bw));
+    CG_CHECK_CUDA(cudaMemsetAsync(bw, 0, sizeof(int), st));
+    k_bandwidth<<<grid_for(nC, BLK), BLK, 0, st>>>(nC, sell(m), bw);
+    CG_LAUNCHED();
+    CG_CHECK_CUDA(cudaMemcpyAsync(&m->bandwidth, bw, sizeof(int), cudaMemcpyDeviceToHost, st));
+    int dev = 0, sms = 0, b32 = 0, b64 = 0;
+    CG_CHECK_CUDA(cudaGetDevice(&dev));
+    CG_CHECK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    CG_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b32, k_fused_f32, FUSED_TILE, 0));
+    CG_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b64, k_fused_f64, FUSED_TILE, 0));
+    m->fusedGrid[0] = sms * b32;
+    m->fusedGrid[1] = sms * b64;
+    // per-CTA progress counters (zeroed before each launch) and the error word
+    CG_TRY(m->alloc(&m->tileFlags, (size_t) std::max(1, std::max(m->fusedGrid[0], m->fusedGrid[1]))));
+    CG_TRY(m->alloc(&m->fusedCtl, 2));
+    CG_CHECK_CUDA(cudaMemsetAsync(m->fusedCtl, 0, 2 * sizeof(int), st));
+    CG_CHECK_CUDA(cudaStreamSynchronize(st));
+    return CUPCFD_E_SUCCESS;
+}
+}  // namespace cupcfd_gpu
+
+namespace {
+// Forward tiles beyond j the adjoint of tile j needs (bandwidth in tiles).
+int fused_lag_need(const cupcfd_gpu_mesh *m) { return (m->bandwidth + FUSED_TILE - 1) / FUSED_TILE + 1; }
+
+// Extra lag beyond that, in tiles: three rounds of the launch's CTAs, so the
+// adjoint of a round needs only rounds well behind it. CUPCFD_FUSED_SLACK (a
+// tile count) overrides it, for tuning.
+int fused_slack(const cupcfd_gpu_mesh *m, int precision) {
+    const char *env = std::getenv("CUPCFD_FUSED_SLACK");
+    if (env && *env) return std::max(0, std::atoi(env));
+    return 3 * m->fusedGrid[precision == CUPCFD_PREC_F64];
+}
+
+// Whether the auto mode fuses: the data the forward read between a tile's
+// forward and its adjoint (about 150 bytes per cell in FP32, 300 in FP64)
+// must stay well inside the 126 MB L2.
+bool use_fused(const cupcfd_gpu_mesh *m, int precision) {
+    if (m->fusedGrid[precision == CUPCFD_PREC_F64] <= 0) return false;
+    if (m->fusion == 1) return true;
+    if (m->fusion == 2) return false;
+    double perCell = precision == CUPCFD_PREC_F64 ? 300.0 : 150.0;
+    double window = (2.0 * fused_lag_need(m) + fused_slack(m, precision)) * FUSED_TILE * perCell;
+    return window < 64e6;
+}
+
+int launch_fused(cupcfd_gpu_mesh *m, int precision, const void *phi, const void *phiB, const void *state,
+                 const void *gface, void *grad, void *massFlux, void *phiBar, void *phiBBar, void *stateBar,
+                 double *loss, cudaStream_t st) {
+    int nTiles = (m->nC + FUSED_TILE - 1) / FUSED_TILE;
+    int nPart = nTiles * (FUSED_TILE / 32);
+    double *part;
+    CG_TRY(scratch(m, S_LOSS, (size_t) nPart, &part));
+    int grid = m->fusedGrid[precision == CUPCFD_PREC_F64];
+    FusedCtl k;
+    k.prog = m->tileFlags;
+    k.err = m->fusedCtl + 1;
+    k.nTiles = nTiles;
+    k.lagNeed = fused_lag_need(m);
+    k.lag = k.lagNeed + fused_slack(m, precision);
+    k.spinLimit = 1 << 20;
+    CG_CHECK_CUDA(cudaMemsetAsync(m->tileFlags, 0, sizeof(unsigned) * (size_t) grid, st));
+    int nC = m->nC;
+    SellView sv = sell(m);
+    int64_t ldc = m->nC;
+    // cooperative launch: every CTA co-resident, which the round-robin tile
+    // assignment needs to be deadlock-free
+    if (precision == CUPCFD_PREC_F64) {
+        const double4 *fg = m->fg64;
+        const double *vol = m->vol;
+        void *args[] = {&nC, &k, &sv, (void *) &fg, (void *) &phi, (void *) &phiB, (void *) &vol, (void *) &state,
+                        (void *) &gface, &grad, &massFlux, &phiBar, &phiBBar, &stateBar, &part, &ldc};
+        CG_CHECK_CUDA(cudaLaunchCooperativeKernel((const void *) k_fused_f64, grid, FUSED_TILE, args, 0, st));
+    } else {
+        const float4 *fg = m->fg32;
+        const double *vol = m->vol;
+        void *args[] = {&nC, &k, &sv, (void *) &fg, (void *) &phi, (void *) &phiB, (void *) &vol, (void *) &state,
+                        (void *) &gface, &grad, &massFlux, &phiBar, &phiBBar, &stateBar, &part, &ldc};
+        CG_CHECK_CUDA(cudaLaunchCooperativeKernel((const void *) k_fused_f32, grid, FUSED_TILE, args, 0, st));
+    }
+    CG_LAUNCHED();
+    if (loss) {
+        k_reduce_partials<<<1, 1024, 0, st>>>(nPart, part, loss);
+        CG_LAUNCHED();
+    }
+    return CUPCFD_E_SUCCESS;
+}
+}  // namespace
+
+extern "C" int cupcfd_gpu_mesh_set_fusion(cupcfd_gpu_mesh *m, int32_t mode) {
+    clear_error();
+    CG_RETURN_IF(!m, CUPCFD_E_NULL_PTR, "set_fusion: null mesh");
+    CG_RETURN_IF(mode < 0 || mode > 2, CUPCFD_E_CONFIG_INVALID_VALUE, "set_fusion: mode must be 0, 1 or 2");
+    m->fusion = mode;
+    return CUPCFD_E_SUCCESS;
+}
+
+extern "C" int cupcfd_gpu_mesh_check_status(cupcfd_gpu_mesh *m, void *stream) {
+    clear_error();
+    CG_RETURN_IF(!m, CUPCFD_E_NULL_PTR, "check_status: null mesh");
+    CG_TRY(make_device_current(m->device));
+    cudaStream_t st = as_stream(stream);
+    int h = 0;
+    CG_CHECK_CUDA(cudaMemcpyAsync(&h, m->fusedCtl + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CG_CHECK_CUDA(cudaStreamSynchronize(st));
+    if (h) {
+        CG_CHECK_CUDA(cudaMemsetAsync(m->fusedCtl + 1, 0, sizeof(int), st));
+        CG_CHECK_CUDA(cudaStreamSynchronize(st));
+        set_error("a device-side wait of the fused forward+adjoint expired; its outputs are invalid");
+        return CUPCFD_E_ERROR;
+    }
+    return CUPCFD_E_SUCCESS;
+}
 
 // ===========================================================================
 // device-resident calls
@@ -238,11 +357,11 @@ extern "C" int cupcfd_gpu_dev_gradient_adjoint(cupcfd_gpu_mesh *m, int32_t preci
     unsigned grid = grid_for(m->nC, BLK);
     bool sgn = sign_mode == CUPCFD_SIGN_SIGNED;
     if (precision == CUPCFD_PREC_F64) {
-        if (sgn) k_grad_adj_general<true, double><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->faceCells, m->fg64, nullptr, m->vol, (const double *) gbar, (double *) phiBar, (double *) phiBBar, m->nC);
-        else k_grad_adj_general<false, double><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->faceCells, m->fg64, nullptr, m->vol, (const double *) gbar, (double *) phiBar, (double *) phiBBar, m->nC);
+        if (sgn) k_grad_adj_general<true, double><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg64, nullptr, m->vol, (const double *) gbar, (double *) phiBar, (double *) phiBBar, m->nC);
+        else k_grad_adj_general<false, double><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg64, nullptr, m->vol, (const double *) gbar, (double *) phiBar, (double *) phiBBar, m->nC);
     } else {
-        if (sgn) k_grad_adj_general<true, float><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->faceCells, nullptr, m->fg32, m->vol, (const float *) gbar, (float *) phiBar, (float *) phiBBar, m->nC);
-        else k_grad_adj_general<false, float><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->faceCells, nullptr, m->fg32, m->vol, (const float *) gbar, (float *) phiBar, (float *) phiBBar, m->nC);
+        if (sgn) k_grad_adj_general<true, float><<<grid, BLK, 0, st>>>(m->nC, sell(m), nullptr, m->fg32, m->vol, (const float *) gbar, (float *) phiBar, (float *) phiBBar, m->nC);
+        else k_grad_adj_general<false, float><<<grid, BLK, 0, st>>>(m->nC, sell(m), nullptr, m->fg32, m->vol, (const float *) gbar, (float *) phiBar, (float *) phiBBar, m->nC);
     }
     CG_LAUNCHED();
     return CUPCFD_E_SUCCESS;
@@ -256,10 +375,10 @@ extern "C" int cupcfd_gpu_dev_mass_plain_adjoint(cupcfd_gpu_mesh *m, int32_t pre
     cudaStream_t st = as_stream(stream);
     unsigned grid = grid_for(m->nC, BLK);
     if (precision == CUPCFD_PREC_F64)
-        k_adj_f64<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->faceCells, m->fg64, nullptr, 0.0, (const double *) state,
+        k_adj_f64<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg64, nullptr, 0.0, (const double *) state,
                                         (const double *) mbar, nullptr, nullptr, (double *) stateBar, m->nC);
     else
-        k_adj_f32<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->faceCells, m->fg32, nullptr, 0.f, (const float4 *) state,
+        k_adj_f32<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg32, nullptr, 0.f, (const float4 *) state,
                                         (const float *) mbar, nullptr, nullptr, (float4 *) stateBar, m->nC);
     CG_LAUNCHED();
     return CUPCFD_E_SUCCESS;
@@ -278,11 +397,11 @@ extern "C" int cupcfd_gpu_dev_forward(cupcfd_gpu_mesh *m, int32_t precision, con
     double *part = nullptr;
     if (loss) CG_TRY(scratch(m, S_LOSS, grid, &part));
     if (precision == CUPCFD_PREC_F64)
-        k_fwd_f64<BLK><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->faceCells, m->fg64, (const double *) phi, (const double *) phiB,
+        k_fwd_f64<BLK><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg64, (const double *) phi, (const double *) phiB,
                                              m->vol, (const double *) state, (const double *) gface, (double *) grad,
                                              (double *) massFlux, part, m->nC);
     else
-        k_fwd_f32<BLK><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->faceCells, m->fg32, (const float *) phi, (const float *) phiB,
+        k_fwd_f32<BLK><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg32, (const float *) phi, (const float *) phiB,
                                              m->vol, (const float4 *) state, (const float *) gface, (float *) grad,
                                              (float *) massFlux, part, m->nC);
     CG_LAUNCHED();
@@ -302,10 +421,10 @@ extern "C" int cupcfd_gpu_dev_adjoint(cupcfd_gpu_mesh *m, int32_t precision, con
     cudaStream_t st = as_stream(stream);
     unsigned grid = grid_for(m->nC, BLK);
     if (precision == CUPCFD_PREC_F64)
-        k_adj_f64<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->faceCells, m->fg64, (const double *) grad, 2.0, (const double *) state,
+        k_adj_f64<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg64, (const double *) grad, 2.0, (const double *) state,
                                         (const double *) gface, (double *) phiBar, (double *) phiBBar, (double *) stateBar, m->nC);
     else
-        k_adj_f32<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->faceCells, m->fg32, (const float *) grad, 2.f, (const float4 *) state,
+        k_adj_f32<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg32, (const float *) grad, 2.f, (const float4 *) state,
                                         (const float *) gface, (float *) phiBar, (float *) phiBBar, (float4 *) stateBar, m->nC);
     CG_LAUNCHED();
     return CUPCFD_E_SUCCESS;
@@ -318,6 +437,13 @@ extern "C" int cupcfd_gpu_dev_forward_adjoint(cupcfd_gpu_mesh *m, int32_t precis
     CG_RETURN_IF(!m || !gface, CUPCFD_E_NULL_PTR, "dev_forward_adjoint: null argument");
     double *lp = loss;
     if (!lp) CG_TRY(scratch(m, S_NORM, 1, &lp));
+    CG_TRY(check_prec(m, precision));
+    if (use_fused(m, precision)) {
+        CG_RETURN_IF(!phi || !state || !grad || !massFlux || !phiBar || !stateBar || (m->nB > 0 && (!phiB || !phiBBar)),
+                     CUPCFD_E_NULL_PTR, "dev_forward_adjoint: null argument");
+        return launch_fused(m, precision, phi, phiB, state, gface, grad, massFlux, phiBar, phiBBar, stateBar, lp,
+                            as_stream(stream));
+    }
     CG_TRY(cupcfd_gpu_dev_forward(m, precision, phi, phiB, state, gface, grad, massFlux, lp, stream));
     return cupcfd_gpu_dev_adjoint(m, precision, grad, state, gface, phiBar, phiBBar, stateBar, stream);
 }
@@ -573,7 +699,7 @@ extern "C" int cupcfd_gpu_flux_mass_dolfyn_face_loop(
                                         bcIn, bcOut, nB, cnt);
     CG_LAUNCHED();
     if (anyInlet) {
-        k_inlet_su<<<gC, BLK, 0, st>>>(nC, sell(m), m->faceCells, m->bndRegion, m->regionType, mf, suD);
+        k_inlet_su<<<gC, BLK, 0, st>>>(nC, sell(m), m->bndRegion, m->regionType, mf, suD);
         CG_LAUNCHED();
     }
     // back to reference numbering and to the host
@@ -689,5 +815,5 @@ extern "C" int cupcfd_gpu_forward_adjoint(cupcfd_gpu_mesh *m, int32_t precision,
     if (phiBBar && nB > 0) CG_CHECK_CUDA(cudaMemcpyAsync(phiBBar, oPbb, 8 * (size_t) nB, cudaMemcpyDeviceToHost, st));
     if (loss) CG_CHECK_CUDA(cudaMemcpyAsync(loss, dloss, 8, cudaMemcpyDeviceToHost, st));
     CG_CHECK_CUDA(cudaStreamSynchronize(st));
-    return CUPCFD_E_SUCCESS;
+    return cupcfd_gpu_mesh_check_status(m, st);
 }

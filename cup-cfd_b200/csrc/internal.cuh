@@ -20,11 +20,6 @@ void set_error(const std::string &msg);
 void clear_error();
 extern std::atomic<int64_t> g_launches;
 
-struct Status {
-    int code = CUPCFD_E_SUCCESS;
-    bool ok() const { return code == CUPCFD_E_SUCCESS; }
-};
-
 #define CG_CHECK_CUDA(expr)                                                                         \
     do {                                                                                            \
         cudaError_t e_ = (expr);                                                                    \
@@ -68,15 +63,18 @@ struct DevBuf {
 
 // Cell-incidence lists in SELL-32 layout: the cells of slice s (internal ids
 // 32s .. 32s+31) own entries [slicePtr[s], slicePtr[s+1]); entry k of lane l
-// sits at slicePtr[s] + 32k + l. An entry is (internal face id << 1) | role,
-// role 0 when the cell is the face's cell1 (owner, P), 1 when it is cell2
-// (neighbour, N); padding entries are -1 and come after a cell's real ones.
-// Within a cell, entries are in ascending REFERENCE face id, which is the
-// order the reference's face loop adds contributions into that cell.
+// sits at slicePtr[s] + 32k + l, so entry k of a warp's 32 cells is one
+// coalesced 256-byte load. An entry is {code, other}: code = (internal face
+// id << 1) | role, role 0 when the cell is the face's cell1 (owner, P) and 1
+// when it is cell2 (neighbour, N); other = the face's other cell, or
+// -1 - boundaryId on a boundary face. Padding entries are {-1, -1} and come
+// after a cell's real ones. Within a cell, entries are in ascending
+// REFERENCE face id: the order the reference's face loop adds contributions
+// into that cell (GradientKernels.ipp:73-116).
 struct Sell {
     int nSlices = 0;
     int *slicePtr = nullptr;
-    int *inc = nullptr;
+    int2 *inc = nullptr;
     int64_t nEntries = 0;
 };
 
@@ -115,10 +113,13 @@ struct cupcfd_gpu_mesh {
     int *bndRegion = nullptr, *regionType = nullptr;
     double *regionUVW = nullptr, *regionDen = nullptr;
     std::vector<int> hRegionType;
-    // cells owning boundary faces, with those faces (internal ids) in
-    // ascending reference face id: the deterministic order for su[ip] updates
-    int nBC = 0;
-    int *bcPtr = nullptr, *bcCell = nullptr, *bcFace = nullptr;
+    // wavefront-fused forward+adjoint: numbering bandwidth (largest
+    // |c - neighbour|), per-tile publication flags, work counter + error word
+    int bandwidth = 0;
+    int fusion = 0;               // 0 auto, 1 always, 2 never
+    unsigned *tileFlags = nullptr; // per-CTA progress counters of the fused launch
+    int *fusedCtl = nullptr;      // [1] error bits ([0] unused)
+    int fusedGrid[2] = {0, 0};    // resident CTAs of the FP32 / FP64 fused kernels
 
     std::vector<cupcfd_gpu::DevBuf> owned;  // everything above, freed by destroy
     std::vector<cupcfd_gpu::DevBuf> scratch; // reusable buffers for host-buffer calls
@@ -153,5 +154,7 @@ struct Source {
     double *cc, *vol;                   // [3*nC], [nC]
 };
 int build_mesh_from_source(cupcfd_gpu_mesh *m, const Source &src, const cupcfd_mesh_options *opt);
+// bandwidth of the numbering and the fused pipeline's device state (api.cu)
+int mesh_post_build(cupcfd_gpu_mesh *m, cudaStream_t st);
 int make_device_current(int device);
 }  // namespace cupcfd_gpu

@@ -4,8 +4,14 @@
 //   faceCells[f] = {P, N} or {P, -1 - boundaryId}
 //   fg64/fg32[f] = {Sx, Sy, Sz, lambda}: one 128-bit load per face in FP32
 //   cell scalars T[nC]; cell vectors as three component blocks T[3][ldc]
-//   SELL-32 incidence lists: one thread per cell, 32 consecutive cells per
-//   warp, entry k of the warp's cells is one coalesced 128-byte load.
+//   SELL-32 incidence lists of int2 {face << 1 | role, other cell}: one
+//   thread per cell, 32 consecutive cells per warp, entry k of the warp's
+//   cells is one coalesced 256-byte load.
+//
+// Memory-level parallelism: a thread loads a chunk of incidence entries,
+// then every face record and neighbour value of the chunk, and only then
+// computes, so each thread keeps several independent gathers in flight
+// instead of one dependent chain per face.
 //
 // Determinism: every cell sums its faces in ascending reference face id, one
 // thread per cell, no floating-point atomics anywhere. FP64 kernels use
@@ -51,13 +57,73 @@ __device__ __forceinline__ double4 ldg4(const double4 *p) {
     double2 b = __ldg(reinterpret_cast<const double2 *>(p) + 1);
     return make_double4(a.x, a.y, b.x, b.y);
 }
-
 __device__ __forceinline__ float4 ldg4(const float4 *p) { return __ldg(p); }
 
 struct SellView {
     const int *slicePtr;
-    const int *inc;
+    const int2 *inc;
 };
+
+// The cell's first incidence entry and its slice width (entries per lane).
+__device__ __forceinline__ const int2 *cell_entries(const SellView &sv, int c, int &w) {
+    int s = c >> 5;
+    int p0 = __ldg(sv.slicePtr + s);
+    w = (__ldg(sv.slicePtr + s + 1) - p0) >> 5;
+    return sv.inc + p0 + (c & 31);
+}
+
+// Read-only 8-byte load of an incidence entry. With CUPCFD_L2_PREFETCH the
+// load asks L2 to fetch 256-byte blocks from DRAM (the incidence stream is
+// read sequentially slice by slice).
+__device__ __forceinline__ int2 ld_entry(const int2 *p) {
+#ifdef CUPCFD_L2_PREFETCH
+    int2 v;
+    asm("ld.global.nc.L2::256B.v2.s32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "l"(p));
+    return v;
+#else
+    return __ldg(p);
+#endif
+}
+
+// Entries k0 .. k0+W-1 of the cell (padding {-1,-1} past its slice width).
+template <int W>
+__device__ __forceinline__ void load_entries(const int2 *e, int k0, int w, int2 (&en)[W]) {
+#pragma unroll
+    for (int j = 0; j < W; j++) en[j] = (k0 + j < w) ? ld_entry(e + 32 * (k0 + j)) : make_int2(-1, -1);
+}
+
+// Entries per chunk in the unrolled kernels (six covers a hex cell in one
+// chunk; wider cells take more chunks) and the minimum resident blocks per
+// SM the register allocation must allow, per kernel family. Chosen by
+// measurement on B200; overridable at build time.
+#ifndef CUPCFD_GRAD_CHUNK
+#define CUPCFD_GRAD_CHUNK 6
+#endif
+#ifndef CUPCFD_FWD_CHUNK
+#define CUPCFD_FWD_CHUNK 3
+#endif
+#ifndef CUPCFD_ADJ_CHUNK
+#define CUPCFD_ADJ_CHUNK 2
+#endif
+#ifndef CUPCFD_MINB_F32
+#define CUPCFD_MINB_F32 4
+#endif
+#ifndef CUPCFD_MINB_F64
+#define CUPCFD_MINB_F64 2
+#endif
+#ifndef CUPCFD_FWD_CHUNK_F64
+#define CUPCFD_FWD_CHUNK_F64 2
+#endif
+#ifndef CUPCFD_MINB_FWD_F64
+#define CUPCFD_MINB_FWD_F64 3
+#endif
+#ifndef CUPCFD_MINB_FUSED_F32
+#define CUPCFD_MINB_FUSED_F32 3
+#endif
+#ifndef CUPCFD_MINB_FUSED_F64
+#define CUPCFD_MINB_FUSED_F64 2
+#endif
+constexpr int CHUNK = CUPCFD_GRAD_CHUNK;
 
 // ---------------------------------------------------------------------------
 // Gradient, FP64, reference arithmetic. CORR adds the non-orthogonal
@@ -65,67 +131,74 @@ struct SellView {
 // with a zero previous iterate the term is exactly +0 and is skipped).
 // ---------------------------------------------------------------------------
 template <bool CORR, bool SIGNED>
-__global__ void __launch_bounds__(256) k_grad_f64(int nC, SellView sv, const int2 *__restrict__ fcells,
-                                                  const double4 *__restrict__ fg, const double4 *__restrict__ fc,
-                                                  const double4 *__restrict__ cc, const double *__restrict__ phi,
-                                                  const double *__restrict__ phiB, const double *__restrict__ vol,
-                                                  const double *__restrict__ go, double *__restrict__ g,
-                                                  double *__restrict__ gcopy, int64_t ldc) {
+__global__ void __launch_bounds__(256, CUPCFD_MINB_F64) k_grad_f64(int nC, SellView sv, const double4 *__restrict__ fg,
+                                                  const double4 *__restrict__ fc, const double4 *__restrict__ cc,
+                                                  const double *__restrict__ phi, const double *__restrict__ phiB,
+                                                  const double *__restrict__ vol, const double *__restrict__ go,
+                                                  double *__restrict__ g, double *__restrict__ gcopy, int64_t ldc) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nC) return;
-    int s = c >> 5, lane = c & 31;
-    int p0 = __ldg(sv.slicePtr + s);
-    int w = (__ldg(sv.slicePtr + s + 1) - p0) >> 5;
-    const int *e = sv.inc + p0 + lane;
+    int w;
+    const int2 *e = cell_entries(sv, c, w);
     double phic = phi[c];
-    double4 xc;
+    double4 xc = make_double4(0, 0, 0, 0);
     double gc0 = 0, gc1 = 0, gc2 = 0;
     if (CORR) {
         xc = cc[c];
         gc0 = go[c]; gc1 = go[ldc + c]; gc2 = go[2 * ldc + c];
     }
     double ax = 0.0, ay = 0.0, az = 0.0;
-    for (int k = 0; k < w; k++) {
-        int ent = __ldg(e + 32 * k);
-        if (ent < 0) break;
-        int f = ent >> 1;
-        bool isN = ent & 1;
-        int2 pn = __ldg(fcells + f);
-        double4 G = ldg4(fg + f);
-        double phif;
-        if (pn.y < 0) {
-            phif = __ldg(phiB + (-1 - pn.y));
-        } else {
-            int o = isN ? pn.x : pn.y;
-            double pho = __ldg(phi + o);
-            double facn = G.w;
-            double facp = ds(1.0, facn);
-            double phN = isN ? phic : pho, phP = isN ? pho : phic;
-            phif = da(dm(phN, facn), dm(phP, facp));
-            if (CORR) {
-                double4 xo = ldg4(cc + o);
-                double4 xf = ldg4(fc + f);
-                double go0 = __ldg(go + o), go1 = __ldg(go + ldc + o), go2 = __ldg(go + 2 * ldc + o);
-                double4 xN = isN ? xc : xo, xP = isN ? xo : xc;
-                double gN0 = isN ? gc0 : go0, gN1 = isN ? gc1 : go1, gN2 = isN ? gc2 : go2;
-                double gP0 = isN ? go0 : gc0, gP1 = isN ? go1 : gc1, gP2 = isN ? go2 : gc2;
-                double xac0 = da(dm(xN.x, facn), dm(xP.x, facp));
-                double xac1 = da(dm(xN.y, facn), dm(xP.y, facp));
-                double xac2 = da(dm(xN.z, facn), dm(xP.z, facp));
-                double ga0 = da(dm(gN0, facn), dm(gP0, facp));
-                double ga1 = da(dm(gN1, facn), dm(gP1, facp));
-                double ga2 = da(dm(gN2, facn), dm(gP2, facp));
-                double d = 0.0;
-                d = da(d, dm(ga0, ds(xf.x, xac0)));
-                d = da(d, dm(ga1, ds(xf.y, xac1)));
-                d = da(d, dm(ga2, ds(xf.z, xac2)));
-                phif = da(phif, d);
-            }
+    for (int k0 = 0; k0 < w; k0 += CHUNK) {
+        int2 en[CHUNK];
+        load_entries(e, k0, w, en);
+        double4 G[CHUNK];
+        double pv[CHUNK];
+#pragma unroll
+        for (int j = 0; j < CHUNK; j++) {
+            if (en[j].x < 0) continue;
+            G[j] = ldg4(fg + (en[j].x >> 1));
+            int o = en[j].y;
+            pv[j] = o >= 0 ? __ldg(phi + o) : __ldg(phiB + (-1 - o));
         }
-        if (SIGNED && isN) {
-            ax = ds(ax, dm(phif, G.x)); ay = ds(ay, dm(phif, G.y)); az = ds(az, dm(phif, G.z));
-        } else {
-            ax = da(ax, dm(phif, G.x)); ay = da(ay, dm(phif, G.y)); az = da(az, dm(phif, G.z));
+#pragma unroll
+        for (int j = 0; j < CHUNK; j++) {
+            int code = en[j].x;
+            if (code < 0) continue;
+            bool isN = code & 1;
+            int o = en[j].y;
+            double phif;
+            if (o < 0) {
+                phif = pv[j];
+            } else {
+                double facn = G[j].w;
+                double facp = ds(1.0, facn);
+                double phN = isN ? phic : pv[j], phP = isN ? pv[j] : phic;
+                phif = da(dm(phN, facn), dm(phP, facp));
+                if (CORR) {
+                    double4 xo = ldg4(cc + o);
+                    double4 xf = ldg4(fc + (code >> 1));
+                    double go0 = __ldg(go + o), go1 = __ldg(go + ldc + o), go2 = __ldg(go + 2 * ldc + o);
+                    double4 xN = isN ? xc : xo, xP = isN ? xo : xc;
+                    double gN0 = isN ? gc0 : go0, gN1 = isN ? gc1 : go1, gN2 = isN ? gc2 : go2;
+                    double gP0 = isN ? go0 : gc0, gP1 = isN ? go1 : gc1, gP2 = isN ? go2 : gc2;
+                    double xac0 = da(dm(xN.x, facn), dm(xP.x, facp));
+                    double xac1 = da(dm(xN.y, facn), dm(xP.y, facp));
+                    double xac2 = da(dm(xN.z, facn), dm(xP.z, facp));
+                    double ga0 = da(dm(gN0, facn), dm(gP0, facp));
+                    double ga1 = da(dm(gN1, facn), dm(gP1, facp));
+                    double ga2 = da(dm(gN2, facn), dm(gP2, facp));
+                    double d = 0.0;
+                    d = da(d, dm(ga0, ds(xf.x, xac0)));
+                    d = da(d, dm(ga1, ds(xf.y, xac1)));
+                    d = da(d, dm(ga2, ds(xf.z, xac2)));
+                    phif = da(phif, d);
+                }
+            }
+            if (SIGNED && isN) {
+                ax = ds(ax, dm(phif, G[j].x)); ay = ds(ay, dm(phif, G[j].y)); az = ds(az, dm(phif, G[j].z));
+            } else {
+                ax = da(ax, dm(phif, G[j].x)); ay = da(ay, dm(phif, G[j].y)); az = da(az, dm(phif, G[j].z));
+            }
         }
     }
     double fact = dvd(1.0, vol[c]);
@@ -138,59 +211,66 @@ __global__ void __launch_bounds__(256) k_grad_f64(int nC, SellView sv, const int
 // Gradient, FP32 storage and arithmetic, Dot2 accumulation, FP64 1/V.
 // ---------------------------------------------------------------------------
 template <bool CORR, bool SIGNED>
-__global__ void __launch_bounds__(256) k_grad_f32(int nC, SellView sv, const int2 *__restrict__ fcells,
-                                                  const float4 *__restrict__ fg, const float4 *__restrict__ fc,
-                                                  const float4 *__restrict__ cc, const float *__restrict__ phi,
-                                                  const float *__restrict__ phiB, const double *__restrict__ vol,
-                                                  const float *__restrict__ go, float *__restrict__ g,
-                                                  float *__restrict__ gcopy, int64_t ldc) {
+__global__ void __launch_bounds__(256, CUPCFD_MINB_F32) k_grad_f32(int nC, SellView sv, const float4 *__restrict__ fg,
+                                                  const float4 *__restrict__ fc, const float4 *__restrict__ cc,
+                                                  const float *__restrict__ phi, const float *__restrict__ phiB,
+                                                  const double *__restrict__ vol, const float *__restrict__ go,
+                                                  float *__restrict__ g, float *__restrict__ gcopy, int64_t ldc) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nC) return;
-    int s = c >> 5, lane = c & 31;
-    int p0 = __ldg(sv.slicePtr + s);
-    int w = (__ldg(sv.slicePtr + s + 1) - p0) >> 5;
-    const int *e = sv.inc + p0 + lane;
+    int w;
+    const int2 *e = cell_entries(sv, c, w);
     float phic = phi[c];
-    float4 xc;
+    float4 xc = make_float4(0, 0, 0, 0);
     float gc0 = 0, gc1 = 0, gc2 = 0;
     if (CORR) {
         xc = cc[c];
         gc0 = go[c]; gc1 = go[ldc + c]; gc2 = go[2 * ldc + c];
     }
     Acc2 ax, ay, az;
-    for (int k = 0; k < w; k++) {
-        int ent = __ldg(e + 32 * k);
-        if (ent < 0) break;
-        int f = ent >> 1;
-        bool isN = ent & 1;
-        int2 pn = __ldg(fcells + f);
-        float4 G = ldg4(fg + f);
-        float phif;
-        if (pn.y < 0) {
-            phif = __ldg(phiB + (-1 - pn.y));
-        } else {
-            int o = isN ? pn.x : pn.y;
-            float pho = __ldg(phi + o);
-            float facn = G.w, facp = 1.f - facn;
-            float phN = isN ? phic : pho, phP = isN ? pho : phic;
-            phif = fmaf(facn, phN, facp * phP);
-            if (CORR) {
-                float4 xo = ldg4(cc + o), xf = ldg4(fc + f);
-                float go0 = __ldg(go + o), go1 = __ldg(go + ldc + o), go2 = __ldg(go + 2 * ldc + o);
-                float4 xN = isN ? xc : xo, xP = isN ? xo : xc;
-                float gN0 = isN ? gc0 : go0, gN1 = isN ? gc1 : go1, gN2 = isN ? gc2 : go2;
-                float gP0 = isN ? go0 : gc0, gP1 = isN ? go1 : gc1, gP2 = isN ? go2 : gc2;
-                float d0 = xf.x - fmaf(facn, xN.x, facp * xP.x);
-                float d1 = xf.y - fmaf(facn, xN.y, facp * xP.y);
-                float d2 = xf.z - fmaf(facn, xN.z, facp * xP.z);
-                phif += fmaf(facn, gN0, facp * gP0) * d0 + fmaf(facn, gN1, facp * gP1) * d1 +
-                        fmaf(facn, gN2, facp * gP2) * d2;
-            }
+    for (int k0 = 0; k0 < w; k0 += CHUNK) {
+        int2 en[CHUNK];
+        load_entries(e, k0, w, en);
+        float4 G[CHUNK];
+        float pv[CHUNK];
+#pragma unroll
+        for (int j = 0; j < CHUNK; j++) {
+            if (en[j].x < 0) continue;
+            G[j] = __ldg(fg + (en[j].x >> 1));
+            int o = en[j].y;
+            pv[j] = o >= 0 ? __ldg(phi + o) : __ldg(phiB + (-1 - o));
         }
-        if (SIGNED && isN) {
-            ax.sub_prod(phif, G.x); ay.sub_prod(phif, G.y); az.sub_prod(phif, G.z);
-        } else {
-            ax.add_prod(phif, G.x); ay.add_prod(phif, G.y); az.add_prod(phif, G.z);
+#pragma unroll
+        for (int j = 0; j < CHUNK; j++) {
+            int code = en[j].x;
+            if (code < 0) continue;
+            bool isN = code & 1;
+            int o = en[j].y;
+            float phif;
+            if (o < 0) {
+                phif = pv[j];
+            } else {
+                float facn = G[j].w, facp = 1.f - facn;
+                float phN = isN ? phic : pv[j], phP = isN ? pv[j] : phic;
+                phif = fmaf(facn, phN, facp * phP);
+                if (CORR) {
+                    float4 xo = __ldg(cc + o), xf = __ldg(fc + (code >> 1));
+                    float go0 = __ldg(go + o), go1 = __ldg(go + ldc + o), go2 = __ldg(go + 2 * ldc + o);
+                    float4 xN = isN ? xc : xo, xP = isN ? xo : xc;
+                    float gN0 = isN ? gc0 : go0, gN1 = isN ? gc1 : go1, gN2 = isN ? gc2 : go2;
+                    float gP0 = isN ? go0 : gc0, gP1 = isN ? go1 : gc1, gP2 = isN ? go2 : gc2;
+                    float d0 = xf.x - fmaf(facn, xN.x, facp * xP.x);
+                    float d1 = xf.y - fmaf(facn, xN.y, facp * xP.y);
+                    float d2 = xf.z - fmaf(facn, xN.z, facp * xP.z);
+                    phif += fmaf(facn, gN0, facp * gP0) * d0 + fmaf(facn, gN1, facp * gP1) * d1 +
+                            fmaf(facn, gN2, facp * gP2) * d2;
+                }
+            }
+            if (SIGNED && isN) {
+                ax.sub_prod(phif, G[j].x); ay.sub_prod(phif, G[j].y); az.sub_prod(phif, G[j].z);
+            } else {
+                ax.add_prod(phif, G[j].x); ay.add_prod(phif, G[j].y); az.add_prod(phif, G[j].z);
+            }
         }
     }
     double fact = 1.0 / vol[c];
@@ -210,7 +290,7 @@ __global__ void __launch_bounds__(256) k_mass_plain_f64(int nF, const int2 *__re
     if (f >= nF) return;
     int2 pn = fcells[f];
     if (pn.y < 0) return;
-    double4 G = fg[f];
+    double4 G = ldg4(fg + f);
     double facn = G.w, facp = ds(1.0, facn);
     int P = pn.x, N = pn.y;
     double denf = da(dm(__ldg(st + N), facn), dm(__ldg(st + P), facp));

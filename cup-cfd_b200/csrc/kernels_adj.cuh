@@ -29,113 +29,158 @@ __device__ __forceinline__ void block_sum_store(double v, double *out) {
     }
 }
 
-template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_fwd_f64(int nC, SellView sv, const int2 *__restrict__ fcells,
-                                                   const double4 *__restrict__ fg, const double *__restrict__ phi,
-                                                   const double *__restrict__ phiB, const double *__restrict__ vol,
-                                                   const double *__restrict__ st, const double *__restrict__ gface,
-                                                   double *__restrict__ g, double *__restrict__ mflux,
-                                                   double *__restrict__ lossPart, int64_t ldc) {
-    int c = blockIdx.x * BLOCK + threadIdx.x;
-    double lsum = 0.0;
-    if (c < nC) {
-        int s = c >> 5, lane = c & 31;
-        int p0 = __ldg(sv.slicePtr + s);
-        int w = (__ldg(sv.slicePtr + s + 1) - p0) >> 5;
-        const int *e = sv.inc + p0 + lane;
-        double phic = phi[c];
-        double r0 = st[c], u0 = st[ldc + c], v0 = st[2 * ldc + c], w0 = st[3 * ldc + c];
-        double ax = 0.0, ay = 0.0, az = 0.0;
-        for (int k = 0; k < w; k++) {
-            int ent = __ldg(e + 32 * k);
-            if (ent < 0) break;
-            int f = ent >> 1;
-            bool isN = ent & 1;
-            int2 pn = __ldg(fcells + f);
-            double4 G = ldg4(fg + f);
+// Per-cell body of the FP64 fused forward (exact reference arithmetic).
+// Returns this cell's loss contribution (0 when gface is null).
+template <int CH>
+__device__ __forceinline__ double fwd_cell_f64(int c, const SellView &sv, const double4 *__restrict__ fg,
+                                               const double *__restrict__ phi, const double *__restrict__ phiB,
+                                               const double *__restrict__ vol, const double *__restrict__ st,
+                                               const double *__restrict__ gface, double *__restrict__ g,
+                                               double *__restrict__ mflux, int64_t ldc) {
+    int w;
+    const int2 *e = cell_entries(sv, c, w);
+    double phic = phi[c];
+    double r0 = st[c], u0 = st[ldc + c], v0 = st[2 * ldc + c], w0 = st[3 * ldc + c];
+    double ax = 0.0, ay = 0.0, az = 0.0, lsum = 0.0;
+    for (int k0 = 0; k0 < w; k0 += CH) {
+        int2 en[CH];
+        load_entries(e, k0, w, en);
+        double4 G[CH];
+        double pv[CH], so[CH][4], gf[CH];
+#pragma unroll
+        for (int j = 0; j < CH; j++) {
+            int code = en[j].x;
+            if (code < 0) continue;
+            int f = code >> 1, o = en[j].y;
+            G[j] = ldg4(fg + f);
+            pv[j] = o >= 0 ? __ldg(phi + o) : __ldg(phiB + (-1 - o));
+            if (o >= 0 && !(code & 1)) {
+                so[j][0] = __ldg(st + o); so[j][1] = __ldg(st + ldc + o);
+                so[j][2] = __ldg(st + 2 * ldc + o); so[j][3] = __ldg(st + 3 * ldc + o);
+                gf[j] = gface ? __ldg(gface + f) : 0.0;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < CH; j++) {
+            int code = en[j].x;
+            if (code < 0) continue;
+            bool isN = code & 1;
+            int o = en[j].y;
             double phif;
-            if (pn.y < 0) {
-                phif = __ldg(phiB + (-1 - pn.y));
+            if (o < 0) {
+                phif = pv[j];
             } else {
-                int o = isN ? pn.x : pn.y;
-                double facn = G.w, facp = ds(1.0, facn);
-                double pho = __ldg(phi + o);
-                phif = isN ? da(dm(phic, facn), dm(pho, facp)) : da(dm(pho, facn), dm(phic, facp));
-                if (!isN) {  // owner computes m_f: P = c, N = o
-                    double denf = da(dm(__ldg(st + o), facn), dm(r0, facp));
-                    double uF = da(dm(__ldg(st + ldc + o), facn), dm(u0, facp));
-                    double vF = da(dm(__ldg(st + 2 * ldc + o), facn), dm(v0, facp));
-                    double wF = da(dm(__ldg(st + 3 * ldc + o), facn), dm(w0, facp));
-                    double m = dm(denf, da(da(dm(uF, G.x), dm(vF, G.y)), dm(wF, G.z)));
-                    mflux[f] = m;
-                    if (gface) lsum += __ldg(gface + f) * m;
+                double facn = G[j].w, facp = ds(1.0, facn);
+                phif = isN ? da(dm(phic, facn), dm(pv[j], facp)) : da(dm(pv[j], facn), dm(phic, facp));
+                if (!isN) {  // the owner computes m_f: P = c, N = o
+                    double denf = da(dm(so[j][0], facn), dm(r0, facp));
+                    double uF = da(dm(so[j][1], facn), dm(u0, facp));
+                    double vF = da(dm(so[j][2], facn), dm(v0, facp));
+                    double wF = da(dm(so[j][3], facn), dm(w0, facp));
+                    double m = dm(denf, da(da(dm(uF, G[j].x), dm(vF, G[j].y)), dm(wF, G[j].z)));
+                    mflux[code >> 1] = m;
+                    lsum += gf[j] * m;
                 }
             }
-            ax = da(ax, dm(phif, G.x)); ay = da(ay, dm(phif, G.y)); az = da(az, dm(phif, G.z));
+            ax = da(ax, dm(phif, G[j].x)); ay = da(ay, dm(phif, G[j].y)); az = da(az, dm(phif, G[j].z));
         }
-        double V = vol[c];
-        double fact = dvd(1.0, V);
-        ax = dm(ax, fact); ay = dm(ay, fact); az = dm(az, fact);
-        g[c] = ax; g[ldc + c] = ay; g[2 * ldc + c] = az;
-        lsum += V * (ax * ax + ay * ay + az * az);
     }
-    if (lossPart) block_sum_store<BLOCK>(lsum, lossPart);
+    double V = vol[c];
+    double fact = dvd(1.0, V);
+    ax = dm(ax, fact); ay = dm(ay, fact); az = dm(az, fact);
+    g[c] = ax; g[ldc + c] = ay; g[2 * ldc + c] = az;
+    return lsum + V * (ax * ax + ay * ay + az * az);
 }
 
-// FP32 version; cell state as float4 {rho, u, v, w}.
-template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_fwd_f32(int nC, SellView sv, const int2 *__restrict__ fcells,
-                                                   const float4 *__restrict__ fg, const float *__restrict__ phi,
-                                                   const float *__restrict__ phiB, const double *__restrict__ vol,
-                                                   const float4 *__restrict__ st, const float *__restrict__ gface,
-                                                   float *__restrict__ g, float *__restrict__ mflux,
-                                                   double *__restrict__ lossPart, int64_t ldc) {
-    int c = blockIdx.x * BLOCK + threadIdx.x;
+// Per-cell body of the FP32 fused forward; state as float4 {rho, u, v, w}.
+template <int CH>
+__device__ __forceinline__ double fwd_cell_f32(int c, const SellView &sv, const float4 *__restrict__ fg,
+                                               const float *__restrict__ phi, const float *__restrict__ phiB,
+                                               const double *__restrict__ vol, const float4 *__restrict__ st,
+                                               const float *__restrict__ gface, float *__restrict__ g,
+                                               float *__restrict__ mflux, int64_t ldc) {
+    int w;
+    const int2 *e = cell_entries(sv, c, w);
+    float phic = phi[c];
+    float4 sc = st[c];
+    Acc2 ax, ay, az;
     double lsum = 0.0;
-    if (c < nC) {
-        int s = c >> 5, lane = c & 31;
-        int p0 = __ldg(sv.slicePtr + s);
-        int w = (__ldg(sv.slicePtr + s + 1) - p0) >> 5;
-        const int *e = sv.inc + p0 + lane;
-        float phic = phi[c];
-        float4 sc = st[c];
-        Acc2 ax, ay, az;
-        for (int k = 0; k < w; k++) {
-            int ent = __ldg(e + 32 * k);
-            if (ent < 0) break;
-            int f = ent >> 1;
-            bool isN = ent & 1;
-            int2 pn = __ldg(fcells + f);
-            float4 G = __ldg(fg + f);
+    for (int k0 = 0; k0 < w; k0 += CH) {
+        int2 en[CH];
+        load_entries(e, k0, w, en);
+        float4 G[CH], so[CH];
+        float pv[CH], gf[CH];
+#pragma unroll
+        for (int j = 0; j < CH; j++) {
+            int code = en[j].x;
+            if (code < 0) continue;
+            int f = code >> 1, o = en[j].y;
+            G[j] = __ldg(fg + f);
+            pv[j] = o >= 0 ? __ldg(phi + o) : __ldg(phiB + (-1 - o));
+            if (o >= 0 && !(code & 1)) {
+                so[j] = __ldg(st + o);
+                gf[j] = gface ? __ldg(gface + f) : 0.f;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < CH; j++) {
+            int code = en[j].x;
+            if (code < 0) continue;
+            bool isN = code & 1;
+            int o = en[j].y;
             float phif;
-            if (pn.y < 0) {
-                phif = __ldg(phiB + (-1 - pn.y));
+            if (o < 0) {
+                phif = pv[j];
             } else {
-                int o = isN ? pn.x : pn.y;
-                float facn = G.w, facp = 1.f - facn;
-                float pho = __ldg(phi + o);
-                phif = isN ? fmaf(facn, phic, facp * pho) : fmaf(facn, pho, facp * phic);
+                float facn = G[j].w, facp = 1.f - facn;
+                phif = isN ? fmaf(facn, phic, facp * pv[j]) : fmaf(facn, pv[j], facp * phic);
                 if (!isN) {
-                    float4 so = __ldg(st + o);
-                    float denf = fmaf(facn, so.x, facp * sc.x);
-                    float uF = fmaf(facn, so.y, facp * sc.y);
-                    float vF = fmaf(facn, so.z, facp * sc.z);
-                    float wF = fmaf(facn, so.w, facp * sc.w);
-                    float m = denf * fmaf(uF, G.x, fmaf(vF, G.y, wF * G.z));
-                    mflux[f] = m;
-                    if (gface) lsum += (double) __ldg(gface + f) * (double) m;
+                    float denf = fmaf(facn, so[j].x, facp * sc.x);
+                    float uF = fmaf(facn, so[j].y, facp * sc.y);
+                    float vF = fmaf(facn, so[j].z, facp * sc.z);
+                    float wF = fmaf(facn, so[j].w, facp * sc.w);
+                    float m = denf * fmaf(uF, G[j].x, fmaf(vF, G[j].y, wF * G[j].z));
+                    mflux[code >> 1] = m;
+                    lsum += (double) gf[j] * (double) m;
                 }
             }
-            ax.add_prod(phif, G.x); ay.add_prod(phif, G.y); az.add_prod(phif, G.z);
+            ax.add_prod(phif, G[j].x); ay.add_prod(phif, G[j].y); az.add_prod(phif, G[j].z);
         }
-        double V = vol[c];
-        double fact = 1.0 / V;
-        double gx = ax.value() * fact, gy = ay.value() * fact, gz = az.value() * fact;
-        float rx = (float) gx, ry = (float) gy, rz = (float) gz;
-        g[c] = rx; g[ldc + c] = ry; g[2 * ldc + c] = rz;
-        lsum += V * ((double) rx * rx + (double) ry * ry + (double) rz * rz);
     }
-    if (lossPart) block_sum_store<BLOCK>(lsum, lossPart);
+    double V = vol[c];
+    double fact = 1.0 / V;
+    float rx = (float) (ax.value() * fact), ry = (float) (ay.value() * fact), rz = (float) (az.value() * fact);
+    g[c] = rx; g[ldc + c] = ry; g[2 * ldc + c] = rz;
+    return lsum + V * ((double) rx * rx + (double) ry * ry + (double) rz * rz);
+}
+
+// ---------------------------------------------------------------------------
+// Fused forward of the benchmark pipeline: gradient (nGradient = 1) and the
+// plain mass flux of the faces each cell owns, plus the per-block FP64
+// partial of L = sum_c V_c |g_c|^2 + sum_f gface_f m_f.
+// ---------------------------------------------------------------------------
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK, CUPCFD_MINB_FWD_F64) k_fwd_f64(int nC, SellView sv, const double4 *__restrict__ fg,
+                                                   const double *__restrict__ phi, const double *__restrict__ phiB,
+                                                   const double *__restrict__ vol, const double *__restrict__ st,
+                                                   const double *__restrict__ gface, double *__restrict__ g,
+                                                   double *__restrict__ mflux, double *__restrict__ lossPart, int64_t ldc) {
+    int c = blockIdx.x * BLOCK + threadIdx.x;
+    double l = 0.0;
+    if (c < nC) l = fwd_cell_f64<CUPCFD_FWD_CHUNK_F64>(c, sv, fg, phi, phiB, vol, st, gface, g, mflux, ldc);
+    if (lossPart) block_sum_store<BLOCK>(l, lossPart);
+}
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK, CUPCFD_MINB_F32) k_fwd_f32(int nC, SellView sv, const float4 *__restrict__ fg,
+                                                   const float *__restrict__ phi, const float *__restrict__ phiB,
+                                                   const double *__restrict__ vol, const float4 *__restrict__ st,
+                                                   const float *__restrict__ gface, float *__restrict__ g,
+                                                   float *__restrict__ mflux, double *__restrict__ lossPart, int64_t ldc) {
+    int c = blockIdx.x * BLOCK + threadIdx.x;
+    double l = 0.0;
+    if (c < nC) l = fwd_cell_f32<CUPCFD_FWD_CHUNK>(c, sv, fg, phi, phiB, vol, st, gface, g, mflux, ldc);
+    if (lossPart) block_sum_store<BLOCK>(l, lossPart);
 }
 
 // Deterministic final reduction of per-block partials (fixed order).
@@ -160,147 +205,181 @@ __global__ void k_reduce_partials(int n, const double *__restrict__ part, double
 //   rhobar_c  = sum_f w_cf gface_f (u_f . S_f)
 //   ubar_c    = sum_f w_cf gface_f rho_f S_f   (and v, w)
 // with w_cf = 1 - lambda_f for the owner, lambda_f for the neighbour.
-// When hscale = 0 the gradient part is skipped (mass-only adjoint) and when
-// gface is null the mass part is skipped.
+// hscale = 0 skips the gradient part (mass-only adjoint); a null gface
+// skips the mass part. LDCG reads g with ld.global.cg (L2, coherent) for use
+// inside a kernel that also writes g.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_adj_f64(int nC, SellView sv, const int2 *__restrict__ fcells,
-                                                 const double4 *__restrict__ fg, const double *__restrict__ g,
-                                                 double hscale, const double *__restrict__ st,
-                                                 const double *__restrict__ gface, double *__restrict__ phibar,
-                                                 double *__restrict__ phibBar, double *__restrict__ stbar, int64_t ldc) {
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= nC) return;
-    int s = c >> 5, lane = c & 31;
-    int p0 = __ldg(sv.slicePtr + s);
-    int w = (__ldg(sv.slicePtr + s + 1) - p0) >> 5;
-    const int *e = sv.inc + p0 + lane;
+template <bool LDCG>
+__device__ __forceinline__ float ldg_g(const float *p) { return LDCG ? __ldcg(p) : __ldg(p); }
+template <bool LDCG>
+__device__ __forceinline__ double ldg_g(const double *p) { return LDCG ? __ldcg(p) : __ldg(p); }
+
+template <bool LDCG, int CH = CUPCFD_ADJ_CHUNK>
+__device__ __forceinline__ void adj_cell_f64(int c, const SellView &sv, const double4 *__restrict__ fg,
+                                             const double *g, double hscale, const double *__restrict__ st,
+                                             const double *__restrict__ gface, double *__restrict__ phibar,
+                                             double *__restrict__ phibBar, double *__restrict__ stbar, int64_t ldc) {
+    int w;
+    const int2 *e = cell_entries(sv, c, w);
     bool doG = hscale != 0.0, doM = gface != nullptr;
     double hx = 0, hy = 0, hz = 0;
-    if (doG) { hx = hscale * g[c]; hy = hscale * g[ldc + c]; hz = hscale * g[2 * ldc + c]; }
+    if (doG) { hx = hscale * ldg_g<LDCG>(g + c); hy = hscale * ldg_g<LDCG>(g + ldc + c); hz = hscale * ldg_g<LDCG>(g + 2 * ldc + c); }
     double r0 = 0, u0 = 0, v0 = 0, w0 = 0;
     if (doM) { r0 = st[c]; u0 = st[ldc + c]; v0 = st[2 * ldc + c]; w0 = st[3 * ldc + c]; }
     double pb = 0.0, rb = 0.0, ub = 0.0, vb = 0.0, wb = 0.0;
-    for (int k = 0; k < w; k++) {
-        int ent = __ldg(e + 32 * k);
-        if (ent < 0) break;
-        int f = ent >> 1;
-        bool isN = ent & 1;
-        int2 pn = __ldg(fcells + f);
-        double4 G = ldg4(fg + f);
-        if (pn.y < 0) {
-            if (doG) phibBar[-1 - pn.y] = hx * G.x + hy * G.y + hz * G.z;
-            continue;
+    for (int k0 = 0; k0 < w; k0 += CH) {
+        int2 en[CH];
+        load_entries(e, k0, w, en);
+        double4 G[CH];
+        double go[CH][3], so[CH][4], gf[CH];
+#pragma unroll
+        for (int j = 0; j < CH; j++) {
+            int code = en[j].x;
+            if (code < 0) continue;
+            int f = code >> 1, o = en[j].y;
+            G[j] = ldg4(fg + f);
+            if (o < 0) continue;
+            if (doG) { go[j][0] = ldg_g<LDCG>(g + o); go[j][1] = ldg_g<LDCG>(g + ldc + o); go[j][2] = ldg_g<LDCG>(g + 2 * ldc + o); }
+            if (doM) {
+                so[j][0] = __ldg(st + o); so[j][1] = __ldg(st + ldc + o);
+                so[j][2] = __ldg(st + 2 * ldc + o); so[j][3] = __ldg(st + 3 * ldc + o);
+                gf[j] = __ldg(gface + f);
+            }
         }
-        int o = isN ? pn.x : pn.y;
-        double facn = G.w, facp = 1.0 - facn;
-        double wc = isN ? facn : facp, wo = isN ? facp : facn;
-        if (doG) {
-            double ox = hscale * __ldg(g + o), oy = hscale * __ldg(g + ldc + o), oz = hscale * __ldg(g + 2 * ldc + o);
-            pb += wc * ((hx + ox) * G.x + (hy + oy) * G.y + (hz + oz) * G.z);
-        }
-        if (doM) {
-            double gf = __ldg(gface + f);
-            double ro = __ldg(st + o), uo = __ldg(st + ldc + o), vo = __ldg(st + 2 * ldc + o), wo_ = __ldg(st + 3 * ldc + o);
-            double denf = wc * r0 + wo * ro;
-            double uF = wc * u0 + wo * uo, vF = wc * v0 + wo * vo, wF = wc * w0 + wo * wo_;
-            double flux = uF * G.x + vF * G.y + wF * G.z;
-            double a = wc * gf;
-            rb += a * flux;
-            double b = a * denf;
-            ub += b * G.x; vb += b * G.y; wb += b * G.z;
+#pragma unroll
+        for (int j = 0; j < CH; j++) {
+            int code = en[j].x;
+            if (code < 0) continue;
+            int o = en[j].y;
+            if (o < 0) {
+                if (doG) phibBar[-1 - o] = hx * G[j].x + hy * G[j].y + hz * G[j].z;
+                continue;
+            }
+            bool isN = code & 1;
+            double facn = G[j].w, facp = 1.0 - facn;
+            double wc = isN ? facn : facp, wo = isN ? facp : facn;
+            if (doG)
+                pb += wc * ((hx + hscale * go[j][0]) * G[j].x + (hy + hscale * go[j][1]) * G[j].y +
+                            (hz + hscale * go[j][2]) * G[j].z);
+            if (doM) {
+                double denf = wc * r0 + wo * so[j][0];
+                double uF = wc * u0 + wo * so[j][1], vF = wc * v0 + wo * so[j][2], wF = wc * w0 + wo * so[j][3];
+                double a = wc * gf[j];
+                rb += a * (uF * G[j].x + vF * G[j].y + wF * G[j].z);
+                double b = a * denf;
+                ub += b * G[j].x; vb += b * G[j].y; wb += b * G[j].z;
+            }
         }
     }
     if (doG) phibar[c] = pb;
     if (doM) { stbar[c] = rb; stbar[ldc + c] = ub; stbar[2 * ldc + c] = vb; stbar[3 * ldc + c] = wb; }
 }
 
-// FP32 version; Dot2-compensated accumulation of the five sums.
-__global__ void __launch_bounds__(256) k_adj_f32(int nC, SellView sv, const int2 *__restrict__ fcells,
-                                                 const float4 *__restrict__ fg, const float *__restrict__ g, float hscale,
-                                                 const float4 *__restrict__ st, const float *__restrict__ gface,
-                                                 float *__restrict__ phibar, float *__restrict__ phibBar,
-                                                 float4 *__restrict__ stbar, int64_t ldc) {
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= nC) return;
-    int s = c >> 5, lane = c & 31;
-    int p0 = __ldg(sv.slicePtr + s);
-    int w = (__ldg(sv.slicePtr + s + 1) - p0) >> 5;
-    const int *e = sv.inc + p0 + lane;
+template <bool LDCG, int CH = CUPCFD_ADJ_CHUNK>
+__device__ __forceinline__ void adj_cell_f32(int c, const SellView &sv, const float4 *__restrict__ fg, const float *g,
+                                             float hscale, const float4 *__restrict__ st,
+                                             const float *__restrict__ gface, float *__restrict__ phibar,
+                                             float *__restrict__ phibBar, float4 *__restrict__ stbar, int64_t ldc) {
+    int w;
+    const int2 *e = cell_entries(sv, c, w);
     bool doG = hscale != 0.f, doM = gface != nullptr;
     float hx = 0, hy = 0, hz = 0;
-    if (doG) { hx = hscale * g[c]; hy = hscale * g[ldc + c]; hz = hscale * g[2 * ldc + c]; }
+    if (doG) { hx = hscale * ldg_g<LDCG>(g + c); hy = hscale * ldg_g<LDCG>(g + ldc + c); hz = hscale * ldg_g<LDCG>(g + 2 * ldc + c); }
     float4 sc = make_float4(0, 0, 0, 0);
     if (doM) sc = st[c];
     Acc2 pb, rb, ub, vb, wb;
-    for (int k = 0; k < w; k++) {
-        int ent = __ldg(e + 32 * k);
-        if (ent < 0) break;
-        int f = ent >> 1;
-        bool isN = ent & 1;
-        int2 pn = __ldg(fcells + f);
-        float4 G = __ldg(fg + f);
-        if (pn.y < 0) {
-            if (doG) phibBar[-1 - pn.y] = fmaf(hx, G.x, fmaf(hy, G.y, hz * G.z));
-            continue;
+    for (int k0 = 0; k0 < w; k0 += CH) {
+        int2 en[CH];
+        load_entries(e, k0, w, en);
+        float4 G[CH], so[CH];
+        float go[CH][3], gf[CH];
+#pragma unroll
+        for (int j = 0; j < CH; j++) {
+            int code = en[j].x;
+            if (code < 0) continue;
+            int f = code >> 1, o = en[j].y;
+            G[j] = __ldg(fg + f);
+            if (o < 0) continue;
+            if (doG) { go[j][0] = ldg_g<LDCG>(g + o); go[j][1] = ldg_g<LDCG>(g + ldc + o); go[j][2] = ldg_g<LDCG>(g + 2 * ldc + o); }
+            if (doM) { so[j] = __ldg(st + o); gf[j] = __ldg(gface + f); }
         }
-        int o = isN ? pn.x : pn.y;
-        float facn = G.w, facp = 1.f - facn;
-        float wc = isN ? facn : facp, wo = isN ? facp : facn;
-        if (doG) {
-            float ox = hscale * __ldg(g + o), oy = hscale * __ldg(g + ldc + o), oz = hscale * __ldg(g + 2 * ldc + o);
-            pb.add_prod(wc, fmaf(hx + ox, G.x, fmaf(hy + oy, G.y, (hz + oz) * G.z)));
-        }
-        if (doM) {
-            float gf = __ldg(gface + f);
-            float4 so = __ldg(st + o);
-            float denf = fmaf(wc, sc.x, wo * so.x);
-            float uF = fmaf(wc, sc.y, wo * so.y), vF = fmaf(wc, sc.z, wo * so.z), wF = fmaf(wc, sc.w, wo * so.w);
-            float a = wc * gf;
-            rb.add_prod(a, fmaf(uF, G.x, fmaf(vF, G.y, wF * G.z)));
-            float b = a * denf;
-            ub.add_prod(b, G.x); vb.add_prod(b, G.y); wb.add_prod(b, G.z);
+#pragma unroll
+        for (int j = 0; j < CH; j++) {
+            int code = en[j].x;
+            if (code < 0) continue;
+            int o = en[j].y;
+            if (o < 0) {
+                if (doG) phibBar[-1 - o] = fmaf(hx, G[j].x, fmaf(hy, G[j].y, hz * G[j].z));
+                continue;
+            }
+            bool isN = code & 1;
+            float facn = G[j].w, facp = 1.f - facn;
+            float wc = isN ? facn : facp, wo = isN ? facp : facn;
+            if (doG) {
+                float sx = fmaf(hscale, go[j][0], hx), sy = fmaf(hscale, go[j][1], hy), sz = fmaf(hscale, go[j][2], hz);
+                pb.add_prod(wc, fmaf(sx, G[j].x, fmaf(sy, G[j].y, sz * G[j].z)));
+            }
+            if (doM) {
+                float denf = fmaf(wc, sc.x, wo * so[j].x);
+                float uF = fmaf(wc, sc.y, wo * so[j].y), vF = fmaf(wc, sc.z, wo * so[j].z), wF = fmaf(wc, sc.w, wo * so[j].w);
+                float a = wc * gf[j];
+                rb.add_prod(a, fmaf(uF, G[j].x, fmaf(vF, G[j].y, wF * G[j].z)));
+                float b = a * denf;
+                ub.add_prod(b, G[j].x); vb.add_prod(b, G[j].y); wb.add_prod(b, G[j].z);
+            }
         }
     }
     if (doG) phibar[c] = (float) pb.value();
     if (doM) stbar[c] = make_float4((float) rb.value(), (float) ub.value(), (float) vb.value(), (float) wb.value());
 }
 
+__global__ void __launch_bounds__(256, CUPCFD_MINB_F64) k_adj_f64(int nC, SellView sv, const double4 *__restrict__ fg,
+                                                 const double *__restrict__ g, double hscale, const double *__restrict__ st,
+                                                 const double *__restrict__ gface, double *__restrict__ phibar,
+                                                 double *__restrict__ phibBar, double *__restrict__ stbar, int64_t ldc) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < nC) adj_cell_f64<false>(c, sv, fg, g, hscale, st, gface, phibar, phibBar, stbar, ldc);
+}
+
+__global__ void __launch_bounds__(256, CUPCFD_MINB_F32) k_adj_f32(int nC, SellView sv, const float4 *__restrict__ fg,
+                                                 const float *__restrict__ g, float hscale, const float4 *__restrict__ st,
+                                                 const float *__restrict__ gface, float *__restrict__ phibar,
+                                                 float *__restrict__ phibBar, float4 *__restrict__ stbar, int64_t ldc) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < nC) adj_cell_f32<false>(c, sv, fg, g, hscale, st, gface, phibar, phibBar, stbar, ldc);
+}
+
 // General gradient adjoint (input gbar = dL/dg, any loss): h_c = gbar_c / V_c.
 template <bool SIGNED, class T>
-__global__ void __launch_bounds__(256) k_grad_adj_general(int nC, SellView sv, const int2 *__restrict__ fcells,
-                                                          const double4 *__restrict__ fg64, const float4 *__restrict__ fg32,
-                                                          const double *__restrict__ vol, const T *__restrict__ gbar,
-                                                          T *__restrict__ phibar, T *__restrict__ phibBar, int64_t ldc) {
+__global__ void __launch_bounds__(256) k_grad_adj_general(int nC, SellView sv, const double4 *__restrict__ fg64,
+                                                          const float4 *__restrict__ fg32, const double *__restrict__ vol,
+                                                          const T *__restrict__ gbar, T *__restrict__ phibar,
+                                                          T *__restrict__ phibBar, int64_t ldc) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nC) return;
-    int s = c >> 5, lane = c & 31;
-    int p0 = __ldg(sv.slicePtr + s);
-    int w = (__ldg(sv.slicePtr + s + 1) - p0) >> 5;
-    const int *e = sv.inc + p0 + lane;
+    int w;
+    const int2 *e = cell_entries(sv, c, w);
     double iv = 1.0 / vol[c];
     double hx = (double) gbar[c] * iv, hy = (double) gbar[ldc + c] * iv, hz = (double) gbar[2 * ldc + c] * iv;
     double pb = 0.0;
     for (int k = 0; k < w; k++) {
-        int ent = __ldg(e + 32 * k);
-        if (ent < 0) break;
-        int f = ent >> 1;
-        bool isN = ent & 1;
-        int2 pn = __ldg(fcells + f);
+        int2 en = __ldg(e + 32 * k);
+        if (en.x < 0) break;
+        int f = en.x >> 1, o = en.y;
+        bool isN = en.x & 1;
         double Sx, Sy, Sz, lam;
         if (fg64) { double4 G = ldg4(fg64 + f); Sx = G.x; Sy = G.y; Sz = G.z; lam = G.w; }
         else { float4 G = __ldg(fg32 + f); Sx = G.x; Sy = G.y; Sz = G.z; lam = G.w; }
         double own = hx * Sx + hy * Sy + hz * Sz;
-        if (pn.y < 0) {
-            phibBar[-1 - pn.y] = (T) own;
+        if (o < 0) {
+            phibBar[-1 - o] = (T) own;
             continue;
         }
-        int o = isN ? pn.x : pn.y;
         double ivo = 1.0 / __ldg(vol + o);
         double oth = ((double) gbar[o] * Sx + (double) gbar[ldc + o] * Sy + (double) gbar[2 * ldc + o] * Sz) * ivo;
         // d g_P / d phi_f = +S/V_P; d g_N / d phi_f = +S/V_N (reference) or -S/V_N (signed)
         double sOwn = (SIGNED && isN) ? -1.0 : 1.0, sOth = (SIGNED && !isN) ? -1.0 : 1.0;
-        double pf = sOwn * own + sOth * oth;
-        pb += (isN ? lam : 1.0 - lam) * pf;
+        pb += (isN ? lam : 1.0 - lam) * (sOwn * own + sOth * oth);
     }
     phibar[c] = (T) pb;
 }
@@ -418,25 +497,21 @@ __global__ void __launch_bounds__(256) k_mass_full_f64(
 
 // su[ip] -= massFlux over the cell's inlet faces in ascending reference face
 // id (MassKernels.ipp:258), one thread per cell.
-__global__ void __launch_bounds__(256) k_inlet_su(int nC, SellView sv, const int2 *__restrict__ fcells,
-                                                  const int *__restrict__ bndRegion, const int *__restrict__ regionType,
-                                                  const double *__restrict__ mflux, double *__restrict__ su) {
+__global__ void __launch_bounds__(256) k_inlet_su(int nC, SellView sv, const int *__restrict__ bndRegion,
+                                                  const int *__restrict__ regionType, const double *__restrict__ mflux,
+                                                  double *__restrict__ su) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nC) return;
-    int s = c >> 5, lane = c & 31;
-    int p0 = sv.slicePtr[s];
-    int w = (sv.slicePtr[s + 1] - p0) >> 5;
-    const int *e = sv.inc + p0 + lane;
+    int w;
+    const int2 *e = cell_entries(sv, c, w);
     double v = su[c];
     bool touched = false;
     for (int k = 0; k < w; k++) {
-        int ent = e[32 * k];
-        if (ent < 0) break;
-        int f = ent >> 1;
-        int2 pn = fcells[f];
-        if (pn.y >= 0) continue;
-        if (regionType[bndRegion[-1 - pn.y]] != CUPCFD_RTYPE_INLET) continue;
-        v = ds(v, mflux[f]);
+        int2 en = e[32 * k];
+        if (en.x < 0) break;
+        if (en.y >= 0) continue;
+        if (regionType[bndRegion[-1 - en.y]] != CUPCFD_RTYPE_INLET) continue;
+        v = ds(v, mflux[en.x >> 1]);
         touched = true;
     }
     if (touched) su[c] = v;

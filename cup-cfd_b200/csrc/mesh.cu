@@ -141,6 +141,30 @@ __global__ void k_face_owner_keys(int nF, const int *__restrict__ c1, const int 
     key[f] = ((uint64_t) (uint32_t) cellO2N[c1[f]] << 32) | (uint32_t) f;
 }
 
+// j = rank of face f among its owner's faces (ascending reference face id),
+// for every face (one thread per reference cell). err bit set if j >= 32.
+__global__ void k_owned_rank(int nC, const int *__restrict__ xadj, const int *__restrict__ adj,
+                             const int *__restrict__ c1, int *__restrict__ rank, int *__restrict__ err) {
+    int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= nC) return;
+    int j = 0;
+    for (int k = xadj[o]; k < xadj[o + 1]; k++) {
+        int f = adj[k];
+        if (c1[f] == o) rank[f] = j++;
+    }
+    if (j > 32) atomicOr(err, 1);
+}
+
+// Face key (owner slice, owned-face rank, owner lane): entry k of a warp's 32
+// cells then reads consecutive face records (a SELL layout for faces).
+__global__ void k_face_slice_keys(int nF, const int *__restrict__ c1, const int *__restrict__ cellO2N,
+                                  const int *__restrict__ rank, uint64_t *__restrict__ key) {
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nF) return;
+    uint64_t P = (uint64_t) (uint32_t) cellO2N[c1[f]];
+    key[f] = ((P >> 5) << 10) | ((uint64_t) rank[f] << 5) | (P & 31);
+}
+
 __global__ void k_low32(int n, const uint64_t *__restrict__ key, int *__restrict__ out) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) out[i] = (int) (uint32_t) key[i];
@@ -203,9 +227,10 @@ __global__ void k_slice_width(int nC, int nSlices, const int *__restrict__ cellN
     if (lane == 0) words[s] = 32 * d;
 }
 
-__global__ void k_fill_sell(int nC, const int *__restrict__ cellN2O, const int *__restrict__ xadj,
-                            const int *__restrict__ adj, const int *__restrict__ c1, const int *__restrict__ faceO2N,
-                            const int *__restrict__ slicePtr, int *__restrict__ inc) {
+__global__ void k_fill_sell(int nC, const int *__restrict__ cellN2O, const int *__restrict__ cellO2N,
+                            const int *__restrict__ xadj, const int *__restrict__ adj, const int *__restrict__ c1,
+                            const int *__restrict__ c2, const int *__restrict__ bnd, const int *__restrict__ faceO2N,
+                            const int *__restrict__ slicePtr, int2 *__restrict__ inc) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     int s = c >> 5, lane = c & 31;
     if (s * 32 >= nC) return;
@@ -217,10 +242,11 @@ __global__ void k_fill_sell(int nC, const int *__restrict__ cellN2O, const int *
         for (int j = xadj[o]; j < xadj[o + 1]; j++, k++) {
             int fo = adj[j];
             int role = (c1[fo] == o) ? 0 : 1;
-            inc[base + 32 * k] = (faceO2N[fo] << 1) | role;
+            int other = role ? cellO2N[c1[fo]] : (bnd[fo] > -1 ? -1 - bnd[fo] : cellO2N[c2[fo]]);
+            inc[base + 32 * k] = make_int2((faceO2N[fo] << 1) | role, other);
         }
     }
-    for (; k < width; k++) inc[base + 32 * k] = -1;
+    for (; k < width; k++) inc[base + 32 * k] = make_int2(-1, -1);
 }
 
 __global__ void k_any_nonzero(int64_t n, const double *__restrict__ a, int *__restrict__ flag) {
@@ -312,6 +338,93 @@ int bits_for(uint64_t v) {
 
 namespace cupcfd_gpu {
 
+// Reverse Cuthill-McKee numbering of the cell graph (host). Each connected
+// component starts from a pseudo-peripheral cell (repeated breadth-first
+// search from a minimum-degree cell until the eccentricity stops growing);
+// neighbours are visited in ascending degree, ties by reference id; the
+// final order is reversed. cellN2O[new] = reference id.
+static int rcm_numbering(cupcfd_gpu_mesh *m, const Source &s, cudaStream_t st) {
+    int nC = s.nC, nF = s.nF;
+    std::vector<int> xadj(nC + 1), adj(m->nInc), c1(nF), c2(nF);
+    CG_CHECK_CUDA(cudaMemcpyAsync(xadj.data(), m->refXadj, sizeof(int) * (nC + 1), cudaMemcpyDeviceToHost, st));
+    CG_CHECK_CUDA(cudaMemcpyAsync(adj.data(), m->refAdj, sizeof(int) * (size_t) m->nInc, cudaMemcpyDeviceToHost, st));
+    CG_CHECK_CUDA(cudaMemcpyAsync(c1.data(), s.c1, sizeof(int) * nF, cudaMemcpyDeviceToHost, st));
+    CG_CHECK_CUDA(cudaMemcpyAsync(c2.data(), s.c2, sizeof(int) * nF, cudaMemcpyDeviceToHost, st));
+    CG_CHECK_CUDA(cudaStreamSynchronize(st));
+    // cell adjacency (interior faces only)
+    std::vector<int> nx(nC + 1, 0);
+    for (int c = 0; c < nC; c++) {
+        int d = 0;
+        for (int k = xadj[c]; k < xadj[c + 1]; k++) d += (c2[adj[k]] >= 0);
+        nx[c + 1] = nx[c] + d;
+    }
+    std::vector<int> nb(nx[nC]);
+    for (int c = 0; c < nC; c++) {
+        int p = nx[c];
+        for (int k = xadj[c]; k < xadj[c + 1]; k++) {
+            int f = adj[k];
+            if (c2[f] < 0) continue;
+            nb[p++] = c1[f] == c ? c2[f] : c1[f];
+        }
+    }
+    auto deg = [&](int c) { return nx[c + 1] - nx[c]; };
+    std::vector<int> level(nC, -1), order;
+    order.reserve(nC);
+    std::vector<char> done(nC, 0);
+    std::vector<int> q;
+    q.reserve(nC);
+    auto bfs_last = [&](int start, int &ecc) {
+        // returns a minimum-degree cell of the last level
+        q.clear();
+        q.push_back(start);
+        level[start] = 0;
+        size_t h = 0;
+        int last = start;
+        while (h < q.size()) {
+            int c = q[h++];
+            for (int k = nx[c]; k < nx[c + 1]; k++) {
+                int o = nb[k];
+                if (level[o] < 0) { level[o] = level[c] + 1; q.push_back(o); }
+            }
+        }
+        ecc = level[q.back()];
+        for (int c : q)
+            if (level[c] == ecc && (deg(c) < deg(last) || level[last] != ecc)) last = c;
+        for (int c : q) level[c] = -1;
+        return last;
+    };
+    std::vector<int> byDeg(nC);
+    for (int i = 0; i < nC; i++) byDeg[i] = i;
+    std::stable_sort(byDeg.begin(), byDeg.end(), [&](int a, int b) { return deg(a) < deg(b); });
+    for (int seed : byDeg) {
+        if (done[seed]) continue;
+        int ecc = 0, e2 = 0;
+        int start = bfs_last(seed, ecc);
+        for (int it = 0; it < 4; it++) {
+            int cand = bfs_last(start, e2);
+            if (e2 <= ecc) break;
+            ecc = e2;
+            start = cand;
+        }
+        size_t h = order.size();
+        order.push_back(start);
+        done[start] = 1;
+        std::vector<int> tmp;
+        while (h < order.size()) {
+            int c = order[h++];
+            tmp.clear();
+            for (int k = nx[c]; k < nx[c + 1]; k++)
+                if (!done[nb[k]]) { done[nb[k]] = 1; tmp.push_back(nb[k]); }
+            std::sort(tmp.begin(), tmp.end(), [&](int a, int b) { return deg(a) != deg(b) ? deg(a) < deg(b) : a < b; });
+            order.insert(order.end(), tmp.begin(), tmp.end());
+        }
+    }
+    std::reverse(order.begin(), order.end());
+    CG_CHECK_CUDA(cudaMemcpyAsync(m->cellN2O, order.data(), sizeof(int) * nC, cudaMemcpyHostToDevice, st));
+    CG_CHECK_CUDA(cudaStreamSynchronize(st));
+    return CUPCFD_E_SUCCESS;
+}
+
 int build_mesh_from_source(cupcfd_gpu_mesh *m, const Source &s, const cupcfd_mesh_options *opt) {
     cudaStream_t st = m->stream;
     const int B = 256;
@@ -321,7 +434,7 @@ int build_mesh_from_source(cupcfd_gpu_mesh *m, const Source &s, const cupcfd_mes
     m->nC = nC; m->nF = nF; m->nB = nB;
     m->order = opt ? opt->order : CUPCFD_ORDER_MORTON;
     m->precisions = opt ? opt->precisions : ((1 << CUPCFD_PREC_F64) | (1 << CUPCFD_PREC_F32C));
-    CG_RETURN_IF(m->order < 0 || m->order > 2, CUPCFD_E_CONFIG_INVALID_VALUE, "mesh: unknown order");
+    CG_RETURN_IF(m->order < 0 || m->order > 3, CUPCFD_E_CONFIG_INVALID_VALUE, "mesh: unknown order");
     CG_RETURN_IF((m->precisions & 3) == 0, CUPCFD_E_CONFIG_INVALID_VALUE, "mesh: no precision selected");
 
     // --- validation
@@ -396,6 +509,8 @@ int build_mesh_from_source(cupcfd_gpu_mesh *m, const Source &s, const cupcfd_mes
         // stable LSD radix sort: equal keys keep ascending reference id
         CG_TRY(sort_pairs(keys, keysOut, vals, m->cellN2O, nC, 63, st));
         CG_CHECK_CUDA(cudaStreamSynchronize(st));
+    } else if (m->order == CUPCFD_ORDER_RCM) {
+        CG_TRY(rcm_numbering(m, s, st));
     } else {
         k_iota<<<grid_for(nC, B), B, 0, st>>>(nC, m->cellN2O);
         CG_LAUNCHED();
@@ -410,15 +525,35 @@ int build_mesh_from_source(cupcfd_gpu_mesh *m, const Source &s, const cupcfd_mes
         k_iota<<<grid_for(nF, B), B, 0, st>>>(nF, m->faceN2O);
         CG_LAUNCHED();
     } else {
+        // faces by (owner slice, owned-face rank, owner lane); falls back to
+        // (owner, reference id) if some cell owns more than 32 faces
         uint64_t *keys, *keysOut;
-        Tmp t1, t2;
+        int *rank, *err2, *vals;
+        Tmp t1, t2, t3, t4, t5;
         CG_TRY(t1.get(&keys, (size_t) nF));
         CG_TRY(t2.get(&keysOut, (size_t) nF));
-        k_face_owner_keys<<<grid_for(nF, B), B, 0, st>>>(nF, s.c1, m->cellO2N, keys);
+        CG_TRY(t3.get(&rank, (size_t) nF));
+        CG_TRY(t4.get(&err2, 1));
+        CG_TRY(t5.get(&vals, (size_t) nF));
+        CG_CHECK_CUDA(cudaMemsetAsync(err2, 0, sizeof(int), st));
+        k_owned_rank<<<grid_for(nC, B), B, 0, st>>>(nC, m->refXadj, m->refAdj, s.c1, rank, err2);
         CG_LAUNCHED();
-        CG_TRY(sort_keys(keys, keysOut, nF, 32 + bits_for((uint64_t) nC), st));
-        k_low32<<<grid_for(nF, B), B, 0, st>>>(nF, keysOut, m->faceN2O);
-        CG_LAUNCHED();
+        int herr2 = 0;
+        CG_CHECK_CUDA(cudaMemcpyAsync(&herr2, err2, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CG_CHECK_CUDA(cudaStreamSynchronize(st));
+        if (!herr2) {
+            k_face_slice_keys<<<grid_for(nF, B), B, 0, st>>>(nF, s.c1, m->cellO2N, rank, keys);
+            CG_LAUNCHED();
+            k_iota<<<grid_for(nF, B), B, 0, st>>>(nF, vals);
+            CG_LAUNCHED();
+            CG_TRY(sort_pairs(keys, keysOut, vals, m->faceN2O, nF, 10 + bits_for((uint64_t) (nC >> 5) + 1), st));
+        } else {
+            k_face_owner_keys<<<grid_for(nF, B), B, 0, st>>>(nF, s.c1, m->cellO2N, keys);
+            CG_LAUNCHED();
+            CG_TRY(sort_keys(keys, keysOut, nF, 32 + bits_for((uint64_t) nC), st));
+            k_low32<<<grid_for(nF, B), B, 0, st>>>(nF, keysOut, m->faceN2O);
+            CG_LAUNCHED();
+        }
         CG_CHECK_CUDA(cudaStreamSynchronize(st));
     }
     k_invert<<<grid_for(nF, B), B, 0, st>>>(nF, m->faceN2O, m->faceO2N);
@@ -484,8 +619,9 @@ int build_mesh_from_source(cupcfd_gpu_mesh *m, const Source &s, const cupcfd_mes
         CG_CHECK_CUDA(cudaStreamSynchronize(st));
         m->sell.nEntries = total;
         CG_TRY(m->alloc(&m->sell.inc, (size_t) total));
-        k_fill_sell<<<grid_for((int64_t) nSlices * 32, B), B, 0, st>>>(nC, m->cellN2O, m->refXadj, m->refAdj, s.c1,
-                                                                      m->faceO2N, m->sell.slicePtr, m->sell.inc);
+        k_fill_sell<<<grid_for((int64_t) nSlices * 32, B), B, 0, st>>>(nC, m->cellN2O, m->cellO2N, m->refXadj, m->refAdj,
+                                                                      s.c1, s.c2, s.bnd, m->faceO2N, m->sell.slicePtr,
+                                                                      m->sell.inc);
         CG_LAUNCHED();
     }
     {
@@ -503,6 +639,9 @@ int build_mesh_from_source(cupcfd_gpu_mesh *m, const Source &s, const cupcfd_mes
         CG_CHECK_CUDA(cudaMemcpyAsync(&m->maxDeg, mx, sizeof(int), cudaMemcpyDeviceToHost, st));
         CG_CHECK_CUDA(cudaStreamSynchronize(st));
     }
+
+    // --- numbering bandwidth and the fused pipeline's control words (api.cu)
+    CG_TRY(mesh_post_build(m, st));
 
     // --- one default region
     m->nR = 1;
@@ -675,6 +814,7 @@ extern "C" int cupcfd_gpu_mesh_get_info(const cupcfd_gpu_mesh *m, cupcfd_mesh_in
     info->maxCellFaces = m->maxDeg;
     info->order = m->order;
     info->precisions = m->precisions;
+    info->bandwidth = m->bandwidth;
     info->deviceBytes = m->bytes;
     return CUPCFD_E_SUCCESS;
 }

@@ -58,8 +58,12 @@ extern "C" {
 
 /* ---- internal numbering of a device mesh ---- */
 #define CUPCFD_ORDER_NATIVE 0 /* cells and faces in the reference's local order */
-#define CUPCFD_ORDER_MORTON 1 /* cells by Z-order of their centres, faces by owner cell */
-#define CUPCFD_ORDER_OWNER 2  /* cells in reference order, faces by owner cell */
+#define CUPCFD_ORDER_MORTON 1 /* cells by Z-order of their centres, faces by owner (see below) */
+#define CUPCFD_ORDER_OWNER 2  /* cells in reference order, faces by owner (see below) */
+#define CUPCFD_ORDER_RCM 3    /* cells by reverse Cuthill-McKee, faces by owner (see below) */
+/* "Faces by owner": sorted by (owner's 32-cell slice, rank of the face among
+ * its owner's faces, owner's lane in the slice), so that the k-th face of 32
+ * consecutive cells are consecutive records. */
 
 /* ---- gradient sign convention ---- */
 #define CUPCFD_SIGN_REFERENCE 0 /* phi_f S_f added to BOTH cells with the same sign,
@@ -111,6 +115,7 @@ typedef struct {
     int32_t nIncidences; /* 2*interior + boundary faces: length of the cell->face CSR */
     int32_t maxCellFaces;
     int32_t order, precisions;
+    int32_t bandwidth;   /* largest |c - neighbour| of the internal numbering */
     int64_t deviceBytes; /* device memory held by the mesh */
 } cupcfd_mesh_info;
 
@@ -155,6 +160,16 @@ int cupcfd_gpu_mesh_create_jittered(int32_t nx, int32_t ny, int32_t nz, double j
 
 int cupcfd_gpu_mesh_destroy(cupcfd_gpu_mesh *mesh);
 int cupcfd_gpu_mesh_get_info(const cupcfd_gpu_mesh *mesh, cupcfd_mesh_info *info);
+
+/* Forward+adjoint execution: 0 = auto (one wavefront-fused launch when the
+ * numbering's bandwidth keeps the lag window well inside L2, else two
+ * launches), 1 = always fused, 2 = never fused. */
+int cupcfd_gpu_mesh_set_fusion(cupcfd_gpu_mesh *mesh, int32_t mode);
+
+/* Synchronises the mesh's work and returns CUPCFD_E_ERROR (message in
+ * cupcfd_gpu_last_error) if a device-side wait of an earlier asynchronous
+ * call expired; clears the condition. CUPCFD_E_SUCCESS otherwise. */
+int cupcfd_gpu_mesh_check_status(cupcfd_gpu_mesh *mesh, void *stream);
 
 /* Boundary regions (CupCfdSoAMesh region/boundary arrays): regionType[nRegions]
  * (CUPCFD_RTYPE_*), regionUVW[3*nRegions], regionDen[nRegions] (host, real_size

@@ -1,0 +1,228 @@
+// cupcfd_gpu/fvm.hpp - C++ drop-in for CUP-CFD's face-loop kernels on B200.
+//
+// Same names and parameter lists as the reference's templates
+//   cupcfd::fvm::GradientPhiGaussDolfyn  (include/fvm/implementation/component/GradientKernels.h:48-54)
+//   cupcfd::fvm::FluxMassDolfynFaceLoop  (include/fvm/implementation/component/MassKernels.h:48-81)
+// in namespace cupcfd::fvm::gpu, so a call site switches by namespace only:
+//
+//   status = cupcfd::fvm::gpu::GradientPhiGaussDolfyn(mesh, nGradient, phiCell, nPhiCell,
+//                                                     phiBoundary, nPhiBoundary,
+//                                                     dPhidxCell, nDPhidxCell, dPhidxoCell, nDPhidxoCell);
+//
+// The mesh is any object with the reference mesh getters (a CupCfdSoAMesh,
+// a CupCfdAoSMesh or the UnstructuredMeshInterface<M,I,T,L> they derive
+// from). On the first call for a mesh object its arrays are read through
+// those getters once and uploaded (cupcfd_gpu_mesh_create); later calls
+// reuse the device mesh. Call release(mesh) before the host mesh changes or
+// goes away. Field arrays are the caller's host arrays, as in the
+// reference; the vptr-carrying EuclideanVector<T,3> arrays are passed as
+// strided views and only their components are written.
+//
+// Return type: cupcfd::error::eCodes when the reference's Error.h has been
+// included first, else int with the same values.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <mutex>
+#include <unordered_map>
+#include <vector>
+
+#include "cupcfd_gpu.h"
+
+namespace cupcfd {
+namespace fvm {
+namespace gpu {
+
+#ifdef CUPCFD_ERROR_INCLUDE_H
+using ecode_t = cupcfd::error::eCodes;
+#else
+using ecode_t = int;
+#endif
+
+// Precision and numbering used for meshes attached implicitly. Change before
+// the first call on a mesh (or release it and attach again).
+struct Settings {
+    int precision = CUPCFD_PREC_F64;  // bit-identical to the reference for T = double
+    int sign_mode = CUPCFD_SIGN_REFERENCE;
+    int order = CUPCFD_ORDER_MORTON;
+    int device = -1;
+};
+inline Settings &settings() {
+    static Settings s;
+    return s;
+}
+
+namespace detail {
+
+template <class V>
+inline cupcfd_vec3_view view_of(const V *a) {
+    // component 0 of element 0 relative to the element start: the vptr slot
+    // (8 bytes) for the reference's EuclideanVector/EuclideanPoint
+    cupcfd_vec3_view v;
+    v.base = a;
+    v.stride = (int32_t) sizeof(V);
+    v.offset = a ? (int32_t) ((const char *) &a->cmp[0] - (const char *) a) : 0;
+    return v;
+}
+
+struct Registry {
+    std::mutex mu;
+    std::unordered_map<const void *, cupcfd_gpu_mesh *> meshes;
+    static Registry &get() {
+        static Registry r;
+        return r;
+    }
+};
+
+// Reads a mesh through its getters into packed arrays and uploads it.
+template <class Mesh>
+int upload(Mesh &mesh, cupcfd_gpu_mesh **out) {
+    using T = decltype(mesh.getFaceLambda(0));
+    const int nF = (int) mesh.properties.lFaces;
+    const int nC = (int) mesh.properties.lTCells;
+    const int nB = (int) mesh.properties.lBoundaries;
+    const int nR = (int) mesh.properties.lRegions;
+    std::vector<int32_t> c1(nF), c2(nF), bnd(nF);
+    std::vector<T> lam(nF), area(nF), S(3 * (size_t) nF), xf(3 * (size_t) nF), xp(3 * (size_t) nF),
+        xn(3 * (size_t) nF), cc(3 * (size_t) nC), vol(nC);
+    bool xzero = true;
+    for (int f = 0; f < nF; f++) {
+        c1[f] = (int32_t) mesh.getFaceCell1ID(f);
+        c2[f] = (int32_t) mesh.getFaceCell2ID(f);
+        bool isB = mesh.getFaceIsBoundary(f);
+        bnd[f] = isB ? (int32_t) mesh.getFaceBoundaryID(f) : -1;
+        lam[f] = mesh.getFaceLambda(f);
+        area[f] = mesh.getFaceArea(f);
+        auto n = mesh.getFaceNorm(f);
+        auto x = mesh.getFaceCenter(f);
+        auto a = mesh.getFaceXpac(f);
+        auto b = mesh.getFaceXnac(f);
+        for (int d = 0; d < 3; d++) {
+            S[3 * f + d] = n.cmp[d];
+            xf[3 * f + d] = x.cmp[d];
+            xp[3 * f + d] = a.cmp[d];
+            xn[3 * f + d] = b.cmp[d];
+            xzero = xzero && a.cmp[d] == T(0) && b.cmp[d] == T(0);
+        }
+    }
+    for (int c = 0; c < nC; c++) {
+        auto x = mesh.getCellCenter(c);
+        for (int d = 0; d < 3; d++) cc[3 * c + d] = x.cmp[d];
+        vol[c] = mesh.getCellVolume(c);
+    }
+    cupcfd_mesh_view v;
+    v.nCells = nC;
+    v.nFaces = nF;
+    v.nBoundaries = nB;
+    v.real_size = (int32_t) sizeof(T);
+    v.faceCell1 = c1.data();
+    v.faceCell2 = c2.data();
+    v.faceBnd = bnd.data();
+    v.faceLambda = lam.data();
+    v.faceArea = area.data();
+    v.faceNorm = {S.data(), (int32_t) (3 * sizeof(T)), 0};
+    v.faceCenter = {xf.data(), (int32_t) (3 * sizeof(T)), 0};
+    v.faceXpac = {xzero ? nullptr : xp.data(), (int32_t) (3 * sizeof(T)), 0};
+    v.faceXnac = {xzero ? nullptr : xn.data(), (int32_t) (3 * sizeof(T)), 0};
+    v.cellCenter = {cc.data(), (int32_t) (3 * sizeof(T)), 0};
+    v.cellVolume = vol.data();
+    cupcfd_mesh_options o;
+    o.order = settings().order;
+    o.precisions = (1 << CUPCFD_PREC_F64) | (1 << CUPCFD_PREC_F32C);
+    o.device = settings().device;
+    int rc = cupcfd_gpu_mesh_create(&v, &o, out);
+    if (rc != CUPCFD_E_SUCCESS) return rc;
+    // boundary regions (UnstructuredMeshInterface.h:1306-1949)
+    if (nR > 0) {
+        std::vector<int32_t> rt(nR), br(nB);
+        std::vector<double> uvw(3 * (size_t) nR), den(nR);
+        for (int r = 0; r < nR; r++) {
+            rt[r] = (int32_t) mesh.getRegionType(r);
+            auto u = mesh.getRegionUVW(r);
+            for (int d = 0; d < 3; d++) uvw[3 * r + d] = (double) u.cmp[d];
+            den[r] = (double) mesh.getRegionDen(r);
+        }
+        for (int b = 0; b < nB; b++) br[b] = (int32_t) mesh.getBoundaryRegionID(b);
+        rc = cupcfd_gpu_mesh_set_regions(*out, nR, rt.data(), uvw.data(), den.data(), br.data(), nB);
+        if (rc != CUPCFD_E_SUCCESS) {
+            cupcfd_gpu_mesh_destroy(*out);
+            *out = nullptr;
+        }
+    }
+    return rc;
+}
+
+}  // namespace detail
+
+// Device mesh of a host mesh object (uploaded on first use).
+template <class Mesh>
+int attach(Mesh &mesh, cupcfd_gpu_mesh **out) {
+    auto &r = detail::Registry::get();
+    std::lock_guard<std::mutex> g(r.mu);
+    auto it = r.meshes.find(&mesh);
+    if (it != r.meshes.end()) {
+        *out = it->second;
+        return CUPCFD_E_SUCCESS;
+    }
+    int rc = detail::upload(mesh, out);
+    if (rc == CUPCFD_E_SUCCESS) r.meshes[&mesh] = *out;
+    return rc;
+}
+
+// Frees the device copy of a host mesh (no-op if none).
+template <class Mesh>
+void release(Mesh &mesh) {
+    auto &r = detail::Registry::get();
+    std::lock_guard<std::mutex> g(r.mu);
+    auto it = r.meshes.find(&mesh);
+    if (it != r.meshes.end()) {
+        cupcfd_gpu_mesh_destroy(it->second);
+        r.meshes.erase(it);
+    }
+}
+
+// GradientPhiGaussDolfyn (GradientKernels.h:48-54)
+template <class Mesh, class I, class T, class Vec>
+ecode_t GradientPhiGaussDolfyn(Mesh &mesh, I nGradient, T *phiCell, I nPhiCell, T *phiBoundary, I nPhiBoundary,
+                               Vec *dPhidxCell, I nDPhidxCell, Vec *dPhidxoCell, I nDPhidxoCell) {
+    cupcfd_gpu_mesh *m = nullptr;
+    int rc = attach(mesh, &m);
+    if (rc != CUPCFD_E_SUCCESS) return (ecode_t) rc;
+    cupcfd_vec3_view v = detail::view_of(dPhidxCell), vo = detail::view_of(dPhidxoCell);
+    rc = cupcfd_gpu_gradient_phi_gauss_dolfyn(m, (int32_t) nGradient, phiCell, (int32_t) nPhiCell, phiBoundary,
+                                              (int32_t) nPhiBoundary, dPhidxCell, (int32_t) nDPhidxCell, v.stride,
+                                              v.offset, dPhidxoCell, (int32_t) nDPhidxoCell, vo.stride, vo.offset,
+                                              (int32_t) sizeof(T), settings().precision, settings().sign_mode);
+    return (ecode_t) rc;
+}
+
+// FluxMassDolfynFaceLoop (MassKernels.h:48-81), T = double
+template <class Mesh, class I, class Vec>
+ecode_t FluxMassDolfynFaceLoop(Mesh &mesh, Vec *dudx, I nDudx, Vec *dvdx, I nDvdx, Vec *dwdx, I nDwdx, Vec *dpdx,
+                               I nDpdx, double *denCell, I nDenCell, double *denBoundary, I nDenBoundary,
+                               double *uCell, I nUCell, double *vCell, I nVCell, double *wCell, I nWCell,
+                               double *massFlux, I nMassFlux, double *p, I nP, double *ar, I nAr, double *su, I nSu,
+                               double *rface, I nRFace, double small, I *icinl, I *icout, I *icsym, I *icwal,
+                               bool solveTurbEnergy, bool solveTurbDiss, bool solveVisc, bool solveEnthalpy,
+                               double *teCell, I nTeCell, double *teBoundary, I nTeBoundary, double *edCell,
+                               I nEdCell, double *edBoundary, I nEdBoundary, double *viseffCell, I nViseffCell,
+                               double *viseffBoundary, I nViseffBoundary, double *tCell, I nTCell, double *tBoundary,
+                               I nTBoundary) {
+    static_assert(sizeof(I) == 4, "int32 indices");
+    cupcfd_gpu_mesh *m = nullptr;
+    int rc = attach(mesh, &m);
+    if (rc != CUPCFD_E_SUCCESS) return (ecode_t) rc;
+    rc = cupcfd_gpu_flux_mass_dolfyn_face_loop(
+        m, detail::view_of(dudx), nDudx, detail::view_of(dvdx), nDvdx, detail::view_of(dwdx), nDwdx,
+        detail::view_of(dpdx), nDpdx, denCell, nDenCell, denBoundary, nDenBoundary, uCell, nUCell, vCell, nVCell,
+        wCell, nWCell, massFlux, nMassFlux, p, nP, ar, nAr, su, nSu, rface, nRFace, small, (int32_t *) icinl,
+        (int32_t *) icout, (int32_t *) icsym, (int32_t *) icwal, solveTurbEnergy, solveTurbDiss, solveVisc,
+        solveEnthalpy, teCell, nTeCell, teBoundary, nTeBoundary, edCell, nEdCell, edBoundary, nEdBoundary,
+        viseffCell, nViseffCell, viseffBoundary, nViseffBoundary, tCell, nTCell, tBoundary, nTBoundary);
+    return (ecode_t) rc;
+}
+
+}  // namespace gpu
+}  // namespace fvm
+}  // namespace cupcfd

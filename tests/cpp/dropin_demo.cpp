@@ -1,0 +1,144 @@
+// Drop-in check of include/cupcfd_gpu/fvm.hpp against the reference itself.
+//
+// Builds a structured mesh with the reference's MeshStructGenSource, lays it
+// out as a one-rank mesh behind the getter interface the reference kernels
+// use, then calls, with the SAME argument lists and the reference's own
+// EuclideanVector<double,3> arrays:
+//   cupcfd::fvm::GradientPhiGaussDolfyn        (reference CPU template)
+//   cupcfd::fvm::gpu::GradientPhiGaussDolfyn   (this library, B200)
+// and likewise FluxMassDolfynFaceLoop with inlet/outlet/symmetry/wall
+// regions, and requires bit-identical results. Exit status 0 on success.
+//
+// Built by `make -C oracle dropin` (needs the reference sources); the binary
+// lands in oracle/_ref/ next to the reference build it links.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <random>
+#include <vector>
+
+#include "Error.h"
+#include "EuclideanVector.h"
+#include "GradientKernels.h"
+#include "MassKernels.h"
+#include "MeshStructGenSource.h"
+#include "cupcfd_gpu/fvm.hpp"
+
+namespace euc = cupcfd::geometry::euclidean;
+namespace msh = cupcfd::geometry::mesh;
+typedef msh::UnstructuredMeshInterface<int, int, double, int> Mesh;
+
+static int fail(const char *what) {
+    std::printf("FAIL: %s (%s)\n", what, cupcfd_gpu_last_error());
+    return 1;
+}
+
+static bool same(const std::vector<euc::EuclideanVector<double, 3>> &a, const std::vector<euc::EuclideanVector<double, 3>> &b) {
+    for (size_t i = 0; i < a.size(); i++)
+        for (int d = 0; d < 3; d++)
+            if (!(a[i].cmp[d] == b[i].cmp[d])) return false;
+    return true;
+}
+
+int main(int argc, char **argv) {
+    int n = argc > 1 ? std::atoi(argv[1]) : 12;
+    int nx = n, ny = n - 1, nz = n + 2;
+    msh::MeshStructGenSource<int, double> src(nx, ny, nz, 0.0, 1.0, -1.0, 1.0, 0.0, 2.0);
+    int nC, nF, nB, nV;
+    src.getCellCount(&nC);
+    src.getFaceCount(&nF);
+    src.getBoundaryCount(&nB);
+    src.getVertexCount(&nV);
+    std::vector<int> fl(nF), cl(nC), c1(nF), c2(nF, -1), bnd(nF, -1);
+    for (int i = 0; i < nF; i++) fl[i] = i;
+    for (int i = 0; i < nC; i++) cl[i] = i;
+    std::vector<char> isB(nF);
+    src.getFaceIsBoundary((bool *) isB.data(), nF, fl.data(), nF);
+    src.getFaceCell1Labels(c1.data(), nF, fl.data(), nF);
+    std::vector<int> inner, outer;
+    for (int f = 0; f < nF; f++) (isB[f] ? outer : inner).push_back(f);
+    std::vector<int> tmp(inner.size()), bl(outer.size());
+    src.getFaceCell2Labels(tmp.data(), (int) inner.size(), inner.data(), (int) inner.size());
+    for (size_t k = 0; k < inner.size(); k++) c2[inner[k]] = tmp[k];
+    src.getFaceBoundaryLabels(bl.data(), (int) outer.size(), outer.data(), (int) outer.size());
+    for (size_t k = 0; k < outer.size(); k++) bnd[outer[k]] = bl[k];
+    std::vector<double> lam(nF), area(nF), vol(nC);
+    src.getFaceLambda(lam.data(), nF, fl.data(), nF);
+    src.getFaceArea(area.data(), nF, fl.data(), nF);
+    src.getCellVolume(vol.data(), nC, cl.data(), nC);
+    std::vector<euc::EuclideanVector<double, 3>> nrm(nF);
+    std::vector<euc::EuclideanPoint<double, 3>> fc(nF), cc(nC);
+    src.getFaceNormal(nrm.data(), nF, fl.data(), nF);
+    src.getFaceCenter(fc.data(), nF, fl.data(), nF);
+    src.getCellCenter(cc.data(), nC, cl.data(), nC);
+    std::vector<double> S(3 * nF), X(3 * nF), C(3 * nC), Z(3 * nF, 0.0);
+    for (int f = 0; f < nF; f++)
+        for (int d = 0; d < 3; d++) { S[3 * f + d] = nrm[f].cmp[d]; X[3 * f + d] = fc[f].cmp[d]; }
+    for (int c = 0; c < nC; c++)
+        for (int d = 0; d < 3; d++) C[3 * c + d] = cc[c].cmp[d];
+    // four boundary regions: inlet, outlet, symmetry, wall
+    int nR = 4;
+    std::vector<int> rtype = {msh::RTYPE_INLET, msh::RTYPE_OUTLET, msh::RTYPE_SYMP, msh::RTYPE_WALL}, breg(nB);
+    std::vector<double> ruvw = {1.0, 0.5, -0.25, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, rden = {1.2, 1, 1, 1};
+    for (int b = 0; b < nB; b++) breg[b] = b % nR;
+
+    Mesh mesh;
+    mesh.properties = {nC, 0, nC, nF, nB, nR};
+    mesh.a = {c1.data(), c2.data(), bnd.data(), lam.data(), S.data(), X.data(), area.data(), Z.data(), Z.data(),
+              C.data(), vol.data(), breg.data(), rtype.data(), ruvw.data(), rden.data()};
+
+    std::mt19937_64 rng(20261203);
+    std::uniform_real_distribution<double> U(-1.0, 1.0);
+    std::normal_distribution<double> N01(0.0, 1.0);
+    std::vector<double> phi(nC), phiB(nB);
+    for (auto &x : phi) x = U(rng);
+    for (auto &x : phiB) x = U(rng);
+
+    // ---- GradientPhiGaussDolfyn: identical call sites, two namespaces
+    for (int nGrad = 1; nGrad <= 3; nGrad++) {
+        std::vector<euc::EuclideanVector<double, 3>> g1(nC), go1(nC), g2(nC), go2(nC);
+        cupcfd::error::eCodes s1 = cupcfd::fvm::GradientPhiGaussDolfyn(mesh, nGrad, phi.data(), nC, phiB.data(), nB,
+                                                                        g1.data(), nC, go1.data(), nC);
+        cupcfd::error::eCodes s2 = cupcfd::fvm::gpu::GradientPhiGaussDolfyn(mesh, nGrad, phi.data(), nC, phiB.data(), nB,
+                                                                             g2.data(), nC, go2.data(), nC);
+        if (s1 != cupcfd::error::E_SUCCESS || s2 != cupcfd::error::E_SUCCESS) return fail("gradient status");
+        if (!same(g1, g2) || !same(go1, go2)) return fail("gradient differs from the reference");
+    }
+
+    // ---- FluxMassDolfynFaceLoop with all region types
+    std::vector<euc::EuclideanVector<double, 3>> du(nC), dv(nC), dw(nC), dp(nC);
+    for (int c = 0; c < nC; c++)
+        for (int d = 0; d < 3; d++) { du[c].cmp[d] = N01(rng); dv[c].cmp[d] = N01(rng); dw[c].cmp[d] = N01(rng); dp[c].cmp[d] = N01(rng); }
+    std::vector<double> den(nC), u(nC), v(nC), w(nC), p(nC), ar(nC), te(nC), ed(nC), vis(nC), t(nC);
+    for (int c = 0; c < nC; c++) {
+        den[c] = 0.9 + 0.2 * (U(rng) + 1) / 2; u[c] = N01(rng); v[c] = N01(rng); w[c] = N01(rng);
+        p[c] = U(rng); ar[c] = 0.9 + 0.2 * (U(rng) + 1) / 2; te[c] = U(rng); ed[c] = U(rng); vis[c] = U(rng); t[c] = U(rng);
+    }
+    struct Out {
+        std::vector<double> mf, su, rf, denB, teB, edB, visB, tB;
+        int c[4];
+    } o[2];
+    for (int r = 0; r < 2; r++) {
+        o[r].mf.assign(nF, 0.125); o[r].su.assign(nC, 0.5); o[r].rf.assign(2 * nF, -3.0); o[r].denB.assign(nB, 0.0);
+        o[r].teB.assign(nB, 0.0); o[r].edB.assign(nB, 0.0); o[r].visB.assign(nB, 0.0); o[r].tB.assign(nB, 0.0);
+        o[r].c[0] = 1; o[r].c[1] = o[r].c[2] = o[r].c[3] = 0;
+    }
+#define MASS_ARGS(O)                                                                                                  \
+    mesh, du.data(), nC, dv.data(), nC, dw.data(), nC, dp.data(), nC, den.data(), nC, O.denB.data(), nB, u.data(), nC, \
+        v.data(), nC, w.data(), nC, O.mf.data(), nF, p.data(), nC, ar.data(), nC, O.su.data(), nC, O.rf.data(), 2 * nF,  \
+        1e-18, &O.c[0], &O.c[1], &O.c[2], &O.c[3], true, true, true, true, te.data(), nC, O.teB.data(), nB, ed.data(),  \
+        nC, O.edB.data(), nB, vis.data(), nC, O.visB.data(), nB, t.data(), nC, O.tB.data(), nB
+    cupcfd::error::eCodes m1 = cupcfd::fvm::FluxMassDolfynFaceLoop(MASS_ARGS(o[0]));
+    cupcfd::error::eCodes m2 = cupcfd::fvm::gpu::FluxMassDolfynFaceLoop(MASS_ARGS(o[1]));
+    if (m1 != cupcfd::error::E_SUCCESS || m2 != cupcfd::error::E_SUCCESS) return fail("mass flux status");
+    if (o[0].mf != o[1].mf || o[0].su != o[1].su || o[0].rf != o[1].rf || o[0].denB != o[1].denB ||
+        o[0].teB != o[1].teB || o[0].edB != o[1].edB || o[0].visB != o[1].visB || o[0].tB != o[1].tB)
+        return fail("mass flux differs from the reference");
+    for (int k = 0; k < 4; k++)
+        if (o[0].c[k] != o[1].c[k]) return fail("region counters differ");
+    cupcfd::fvm::gpu::release(mesh);
+    std::printf("OK dropin %dx%dx%d: %d cells, %d faces; gradient (nGradient 1-3) and mass flux bit-identical\n", nx,
+                ny, nz, nC, nF);
+    return 0;
+}

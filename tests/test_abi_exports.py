@@ -69,3 +69,21 @@ def test_null_arguments_rejected_without_touching_the_gpu(cg):
     assert L.cupcfd_gpu_mesh_create_structgen(0, 4, 4, None, None, C.byref(h)) == cg.E_CONFIG_INVALID_VALUE
     assert L.cupcfd_gpu_mesh_create_jittered(4, 4, 4, 0.7, 1, 1, None, C.byref(h)) == cg.E_CONFIG_INVALID_VALUE
     assert L.cupcfd_gpu_mesh_create_structgen(2048, 2048, 2048, None, None, C.byref(h)) == cg.E_NOT_IMPLEMENTED
+
+
+def declared_arity():
+    """Parameter count of every function declared in include/*.h."""
+    out = {}
+    for h in HEADERS:
+        text = re.sub(r"/\*.*?\*/", "", open(h).read(), flags=re.S)
+        for m in re.finditer(r"\b(cupcfd_gpu_\w+)\s*\(([^)]*)\)\s*;", text):
+            params = [p for p in m.group(2).split(",") if p.strip() and p.strip() != "void"]
+            out[m.group(1)] = len(params)
+    return out
+
+
+def test_binding_arity_matches_header(cg):
+    ar = declared_arity()
+    assert set(ar) == set(cg.SIGNATURES)
+    bad = {n: (len(cg.SIGNATURES[n][0]), k) for n, k in ar.items() if len(cg.SIGNATURES[n][0]) != k}
+    assert not bad, bad
