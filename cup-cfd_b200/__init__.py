@@ -100,6 +100,7 @@ SIGNATURES = {
     "cupcfd_gpu_dev_mass_plain_adjoint": ([_VP, _I, _VP, _VP, _VP, _VP], _I),
     "cupcfd_gpu_dev_forward": ([_VP, _I] + [_VP] * 8, _I),
     "cupcfd_gpu_dev_adjoint": ([_VP, _I] + [_VP] * 7, _I),
+    "cupcfd_gpu_dev_forward_noalloc": ([_VP, _I] + [_VP] * 8, _I),
     "cupcfd_gpu_dev_forward_adjoint": ([_VP, _I] + [_VP] * 11, _I),
     "cupcfd_gpu_dev_error_norms": ([_VP, _I, _VP, _I, _I64, _D, _VP, _VP], _I),
 }
@@ -377,6 +378,12 @@ def dev_mass_plain_adjoint(mesh, precision, state, mbar, stateBar, stream=None):
 def dev_forward(mesh, precision, phi, phiB, state, grad, mflux, gface=None, loss=None, stream=None):
     check(lib().cupcfd_gpu_dev_forward(mesh.h, precision, _p(phi), _p(phiB), _p(state), _p(gface), _p(grad), _p(mflux),
                                        _p(loss), _stream(stream)))
+
+
+def dev_forward_noalloc(mesh, precision, phi, phiB, state, grad, mflux, gface=None, loss=None, stream=None):
+    """cupcfd_gpu_dev_forward without allocation; returns the status code."""
+    return lib().cupcfd_gpu_dev_forward_noalloc(mesh.h, precision, _p(phi), _p(phiB), _p(state), _p(gface), _p(grad),
+                                                _p(mflux), _p(loss), _stream(stream))
 
 
 def dev_adjoint(mesh, precision, grad, state, gface, phiBar, phiBBar, stateBar, stream=None):

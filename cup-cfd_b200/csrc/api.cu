@@ -817,3 +817,76 @@ extern "C" int cupcfd_gpu_forward_adjoint(cupcfd_gpu_mesh *m, int32_t precision,
     CG_CHECK_CUDA(cudaStreamSynchronize(st));
     return cupcfd_gpu_mesh_check_status(m, st);
 }
+
+// ===========================================================================
+// Forward without any allocation (no counterpart in the reference)
+// ===========================================================================
+// cupcfd_gpu_dev_forward takes the per-block loss partials from the mesh's
+// scratch pool, which grows with cudaMalloc on first use. Some callers
+// cannot allocate at the point where they run the forward: a solver that
+// reserves its whole device-memory budget at start-up and treats any later
+// allocation as a failure, or a caller running inside another runtime that
+// owns the device's allocator and must not see a foreign cudaMalloc/cudaFree
+// (which also synchronises the device). This variant runs the same kernels
+// with the partials in a fixed array compiled into the library instead.
+//
+// Limits: the array holds NOALLOC_MAX_PARTIALS doubles (512 KiB, one per
+// 256-cell block), so a loss can be reduced for meshes of up to 16,777,216
+// cells; larger meshes are rejected with CUPCFD_E_ARRAY_SIZE_MISMATCH before
+// anything runs. Every GPU that loads the library holds the array until the
+// process exits. All calls share it: each call writes every slot it reads
+// before reading it (nothing needs clearing), but calls whose kernels
+// overlap on the GPU (different streams, no ordering between them) race on
+// it. The first call on a device looks up the array's device address
+// (cudaGetSymbolAddress) with that device current; make that first call
+// before any stream capture. No error message is recorded (recording one
+// allocates host memory); the status code says what failed.
+namespace {
+constexpr int NOALLOC_MAX_PARTIALS = 65536;
+constexpr int NOALLOC_MAX_DEVICES = 64;
+static __device__ __align__(256) double g_noalloc_partials[NOALLOC_MAX_PARTIALS];
+static double *g_noalloc_ptr[NOALLOC_MAX_DEVICES];
+static std::atomic<int> g_noalloc_ready[NOALLOC_MAX_DEVICES];
+}  // namespace
+
+extern "C" int cupcfd_gpu_dev_forward_noalloc(cupcfd_gpu_mesh *m, int32_t precision, const void *phi,
+                                              const void *phiB, const void *state, const void *gface, void *grad,
+                                              void *massFlux, double *loss, void *stream) {
+    if (!m || !phi || !state || !grad || !massFlux || (m->nB > 0 && !phiB)) return CUPCFD_E_NULL_PTR;
+    if ((gface == nullptr) != (loss == nullptr)) return CUPCFD_E_NULL_PTR;
+    if ((precision != CUPCFD_PREC_F64 && precision != CUPCFD_PREC_F32C) || !(m->precisions & (1 << precision)))
+        return CUPCFD_E_CONFIG_INVALID_VALUE;
+    unsigned grid = grid_for(m->nC, BLK);
+    if (loss && grid > (unsigned) NOALLOC_MAX_PARTIALS) return CUPCFD_E_ARRAY_SIZE_MISMATCH;
+    int dev = m->device;
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return CUPCFD_E_NOT_IMPLEMENTED;
+    if (cudaSetDevice(dev) != cudaSuccess) return CUPCFD_E_ERROR;
+    double *part = nullptr;
+    if (loss) {
+        // one-time set-up per device, with that device current
+        if (g_noalloc_ready[dev].load(std::memory_order_acquire) == 0) {
+            void *p = nullptr;
+            if (cudaGetSymbolAddress(&p, g_noalloc_partials) != cudaSuccess) return CUPCFD_E_ERROR;
+            g_noalloc_ptr[dev] = (double *) p;
+            g_noalloc_ready[dev].store(1, std::memory_order_release);
+        }
+        part = g_noalloc_ptr[dev];
+    }
+    cudaStream_t st = as_stream(stream);
+    if (precision == CUPCFD_PREC_F64)
+        k_fwd_f64<BLK><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg64, (const double *) phi, (const double *) phiB,
+                                             m->vol, (const double *) state, (const double *) gface, (double *) grad,
+                                             (double *) massFlux, part, m->nC);
+    else
+        k_fwd_f32<BLK><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg32, (const float *) phi, (const float *) phiB,
+                                             m->vol, (const float4 *) state, (const float *) gface, (float *) grad,
+                                             (float *) massFlux, part, m->nC);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    if (cudaGetLastError() != cudaSuccess) return CUPCFD_E_ERROR;
+    if (loss) {
+        k_reduce_partials<<<1, 1024, 0, st>>>((int) grid, part, loss);
+        g_launches.fetch_add(1, std::memory_order_relaxed);
+        if (cudaGetLastError() != cudaSuccess) return CUPCFD_E_ERROR;
+    }
+    return CUPCFD_E_SUCCESS;
+}

@@ -296,6 +296,23 @@ int cupcfd_gpu_dev_forward(cupcfd_gpu_mesh *mesh, int32_t precision, const void 
  * and stateBar (cell state layout). */
 int cupcfd_gpu_dev_adjoint(cupcfd_gpu_mesh *mesh, int32_t precision, const void *grad, const void *state,
                            const void *gface, void *phiBar, void *phiBBar, void *stateBar, void *stream);
+/* The forward above without any allocation. No counterpart in the
+ * reference. For callers that cannot allocate device memory when they run
+ * the forward (a solver that reserves its whole memory budget at start-up,
+ * or code running inside another runtime that owns the device allocator):
+ * the loss partials live in a fixed array inside the library instead of the
+ * mesh's scratch pool, and the call makes no cudaMalloc/cudaFree or other
+ * allocating call. Same arguments and results as cupcfd_gpu_dev_forward.
+ * Limits: the array holds 65,536 partials (512 KiB per GPU that loads the
+ * library, held until exit), so with a loss the mesh may have at most
+ * 16,777,216 cells; larger meshes return CUPCFD_E_ARRAY_SIZE_MISMATCH. All
+ * calls share the array: calls whose kernels overlap on the GPU race. The
+ * first call on a device sets up the array's address with that device
+ * current; make it before any stream capture. Errors are reported by status
+ * code only (cupcfd_gpu_last_error is not updated). */
+int cupcfd_gpu_dev_forward_noalloc(cupcfd_gpu_mesh *mesh, int32_t precision, const void *phi, const void *phiB,
+                                   const void *state, const void *gface, void *grad, void *massFlux, double *loss,
+                                   void *stream);
 /* Fused forward + adjoint of the benchmark loss (see cupcfd_gpu_forward_adjoint):
  * two launches over the mesh. Outputs grad, massFlux, phiBar, phiBBar,
  * stateBar; loss (device double[1], may be NULL) reduced in FP64. */
