@@ -68,7 +68,7 @@ class MeshOptions(C.Structure):
 class MeshInfo(C.Structure):
     _fields_ = [(n, C.c_int32) for n in ("nCells", "nFaces", "nInteriorFaces", "nBoundaries", "nRegions",
                                          "nIncidences", "maxCellFaces", "order", "precisions", "bandwidth")] + [
-        ("deviceBytes", C.c_int64)]
+        ("deviceBytes", C.c_int64), ("stagedCtas", C.c_int32), ("stagedSmem", C.c_int32)]
 
 
 # exported symbols of include/cupcfd_gpu.h with their ctypes signatures
@@ -186,6 +186,7 @@ class Mesh:
         self.nBoundaries, self.nIncidences, self.maxCellFaces = info.nBoundaries, info.nIncidences, info.maxCellFaces
         self.order, self.precisions, self.deviceBytes = info.order, info.precisions, info.deviceBytes
         self.bandwidth = info.bandwidth
+        self.stagedCtas, self.stagedSmem = info.stagedCtas, info.stagedSmem
 
     @staticmethod
     def _opts(order, precisions, device):

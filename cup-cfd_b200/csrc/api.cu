@@ -3,6 +3,7 @@
 #include <cmath>
 #include <cstring>
 #include <cstdlib>
+#include <initializer_list>
 
 #include "kernels_fused.cuh"
 
@@ -27,7 +28,141 @@ int scratch(cupcfd_gpu_mesh *m, int slot, size_t n, T **p) {
 }
 
 inline cudaStream_t as_stream(void *s) { return (cudaStream_t) s; }
-inline SellView sell(const cupcfd_gpu_mesh *m) { return SellView{m->sell.slicePtr, m->sell.inc}; }
+inline SellView sell(const cupcfd_gpu_mesh *m) { return SellView{m->sell.slicePtr, m->sell.inc, m->sell.width}; }
+
+// ---------------------------------------------------------------------------
+// staged face loops (kernels_staged.cuh): stage-ring depth, stage
+// capacities, shared-memory layout and the launch conditions
+// ---------------------------------------------------------------------------
+#ifndef CUPCFD_STAGES
+#define CUPCFD_STAGES 3
+#endif
+// stage capacities per cell of a tile: incidence entries, and owned faces
+// in halves (7 -> 3.5 faces per cell; a hexahedral cell owns about 3)
+#ifndef CUPCFD_STAGED_ENT_PER_CELL
+#define CUPCFD_STAGED_ENT_PER_CELL 6
+#endif
+#ifndef CUPCFD_STAGED_FACE_HALVES
+#define CUPCFD_STAGED_FACE_HALVES 7
+#endif
+constexpr int STAGES = CUPCFD_STAGES;
+static_assert(STAGES >= 2 && STAGES <= 8, "stage ring of 2 to 8 stages");
+
+inline int round_up(int x, int k) { return (x + k - 1) / k * k; }
+
+StageLayout staged_layout(const cupcfd_gpu_mesh *m, bool forward) {
+    constexpr int T = STAGED_TILE;
+    StageLayout L{};
+    L.entCap = m->stagedEntCap;
+    L.faceCap = m->stagedFaceCap;
+    L.gfCap = L.faceCap + 8;
+    int o = 0;
+    L.ent = o; o += L.entCap * 8;
+    L.fg = o; o += L.faceCap * 16;
+    L.gf = o; o += L.gfCap * 4;
+    if (forward) {  // phi, state, vol
+        L.c0 = o; o += T * 4;
+        L.c1 = o; o += T * 16;
+        L.c2 = o; o += T * 8;
+        L.c3 = o;
+    } else {        // g (three component blocks), state
+        L.c0 = o; o += T * 4;
+        L.c1 = o; o += T * 4;
+        L.c2 = o; o += T * 4;
+        L.c3 = o; o += T * 16;
+    }
+    L.bytes = round_up(o, 128);
+    L.base = round_up(64 + 64 * STAGES, 128);
+    return L;
+}
+inline int staged_smem(const StageLayout &L) { return L.base + STAGES * L.bytes; }
+
+inline bool aligned16(const void *p) { return ((uintptr_t) p & 15u) == 0; }
+
+StagedArgs staged_args(const cupcfd_gpu_mesh *m, bool forward) {
+    StagedArgs a;
+    a.nC = m->nC;
+    a.nF = m->nF;
+    a.nTiles = m->nTiles;
+    a.desc = (const TileDesc *) m->tileDesc;
+    a.inc = m->sell.inc;
+    a.L = staged_layout(m, forward);
+    a.spinLimit = 1 << 20;
+    a.err = m->fusedCtl + 1;
+    return a;
+}
+
+// Builds the per-tile ranges and sizes the staged launches; leaves
+// m->staged false (unstaged kernels only) when the mesh does not allow it.
+int staged_setup(cupcfd_gpu_mesh *m, cudaStream_t st) {
+    m->staged = false;
+    if (!(m->precisions & (1 << CUPCFD_PREC_F32C)) || m->nF < 1 || m->nC < 1) return CUPCFD_E_SUCCESS;
+    const char *env = std::getenv("CUPCFD_STAGED");
+    if (env && std::strcmp(env, "0") == 0) return CUPCFD_E_SUCCESS;
+    m->nTiles = (int) grid_for(m->nC, STAGED_TILE);
+    TileDesc *desc;
+    CG_TRY(m->alloc(&desc, (size_t) m->nTiles));
+    m->tileDesc = desc;
+    int *start, *aux;  // aux: [0..2] maxima, [3] order flag
+    CG_TRY(m->alloc(&start, (size_t) m->nTiles + 1));
+    CG_TRY(m->alloc(&aux, 4));
+    CG_CHECK_CUDA(cudaMemsetAsync(aux, 0, 4 * sizeof(int), st));
+    k_tile_face_start<<<grid_for(m->nF, BLK), BLK, 0, st>>>(m->nF, m->nTiles, m->faceCells, start, aux + 3);
+    CG_LAUNCHED();
+    k_tile_desc<<<grid_for(m->nTiles, BLK), BLK, 0, st>>>(m->nTiles, m->sell.nSlices, m->sell.slicePtr, start, desc, aux);
+    CG_LAUNCHED();
+    int h[4];
+    CG_CHECK_CUDA(cudaMemcpyAsync(h, aux, sizeof(h), cudaMemcpyDeviceToHost, st));
+    CG_CHECK_CUDA(cudaStreamSynchronize(st));
+    if (h[3] != 0 || h[2] > 255) return CUPCFD_E_SUCCESS;  // faces not by owner tile, or too wide a slice
+    // capacities: the largest tile's counts, at most the compile-time limits;
+    // CUPCFD_STAGED_ENT_CAP / CUPCFD_STAGED_FACE_CAP (per tile) lower them,
+    // which sends the overflow through the global-memory path
+    int entLim = STAGED_TILE * CUPCFD_STAGED_ENT_PER_CELL, faceLim = STAGED_TILE * CUPCFD_STAGED_FACE_HALVES / 2;
+    if (const char *e = std::getenv("CUPCFD_STAGED_ENT_CAP")) if (*e) entLim = std::min(entLim, std::atoi(e));
+    if (const char *e = std::getenv("CUPCFD_STAGED_FACE_CAP")) if (*e) faceLim = std::min(faceLim, std::atoi(e));
+    m->stagedEntCap = std::max(32, round_up(std::min(h[0], entLim), 32));
+    m->stagedFaceCap = std::max(4, round_up(std::min(h[1], faceLim), 4));
+    int dev = 0, sms = 0, optin = 0;
+    CG_CHECK_CUDA(cudaGetDevice(&dev));
+    CG_CHECK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    CG_CHECK_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    const void *kern[2] = {(const void *) k_fwd_f32_staged<STAGES>, (const void *) k_adj_f32_staged<STAGES>};
+    for (int i = 0; i < 2; i++) {
+        int smem = staged_smem(staged_layout(m, i == 0));
+        cudaFuncAttributes fa;
+        CG_CHECK_CUDA(cudaFuncGetAttributes(&fa, kern[i]));
+        if (smem + (int) fa.sharedSizeBytes > optin) return CUPCFD_E_SUCCESS;
+        CG_CHECK_CUDA(cudaFuncSetAttribute(kern[i], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           optin - (int) fa.sharedSizeBytes));
+        int nb = 0;
+        CG_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern[i], STAGED_TILE, smem));
+        if (nb < 1) return CUPCFD_E_SUCCESS;
+        m->stagedGrid[i] = std::min(m->nTiles, sms * nb);
+        m->stagedSmem[i] = smem;
+    }
+    // L2-prefetch variant: prefetch one wave of resident blocks ahead (the
+    // block that will take this block's place), the best distance measured
+    int nbPf = 0;
+    CG_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nbPf, k_fwd_f32_pf, STAGED_TILE, 0));
+    m->prefetchDist = sms * std::max(1, nbPf);
+    if (const char *e = std::getenv("CUPCFD_PREFETCH_DIST")) if (*e) m->prefetchDist = std::max(1, std::atoi(e));
+    m->tileMode = 1;
+    if (const char *e = std::getenv("CUPCFD_TILE_MODE")) if (*e) m->tileMode = std::atoi(e);
+    m->staged = m->tileMode != 0;
+    return CUPCFD_E_SUCCESS;
+}
+
+PrefetchArgs prefetch_args(const cupcfd_gpu_mesh *m) {
+    PrefetchArgs p;
+    p.desc = (const TileDesc *) m->tileDesc;
+    p.inc = m->sell.inc;
+    p.nC = m->nC;
+    p.nF = m->nF;
+    p.nTiles = m->nTiles;
+    p.dist = m->prefetchDist;
+    return p;
+}
 
 // ---------------------------------------------------------------------------
 // permutation kernels (gathers): dst[c][i] = src[c][map[i]]
@@ -111,6 +246,20 @@ int check_prec(const cupcfd_gpu_mesh *m, int precision) {
     return CUPCFD_E_SUCCESS;
 }
 
+// Device arrays must be aligned to their element: T for scalars and vector
+// blocks, 16 bytes for the F32C float4 state (8 for the F64 state blocks).
+int check_align(int precision, std::initializer_list<const void *> arrays, std::initializer_list<const void *> states) {
+    uintptr_t a = precision == CUPCFD_PREC_F64 ? 8 : 4, sa = precision == CUPCFD_PREC_F64 ? 8 : 16;
+    for (const void *p : arrays)
+        CG_RETURN_IF(((uintptr_t) p) % a != 0, CUPCFD_E_CONFIG_INVALID_VALUE,
+                     "device array not aligned to its element size");
+    for (const void *p : states)
+        CG_RETURN_IF(((uintptr_t) p) % sa != 0, CUPCFD_E_CONFIG_INVALID_VALUE,
+                     precision == CUPCFD_PREC_F64 ? "state array not 8-byte aligned"
+                                                  : "F32C state (float4 records) not 16-byte aligned");
+    return CUPCFD_E_SUCCESS;
+}
+
 // ---------------------------------------------------------------------------
 // one gradient iteration (device, internal numbering). corr: add the
 // non-orthogonal correction of the previous iterate `prev` (which must not
@@ -157,61 +306,62 @@ int mesh_post_build(cupcfd_gpu_mesh *m, cudaStream_t st) {
     CG_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b64, k_fused_f64, FUSED_TILE, 0));
     m->fusedGrid[0] = sms * b32;
     m->fusedGrid[1] = sms * b64;
-    // per-CTA progress counters (zeroed before each launch) and the error word
-    CG_TRY(m->alloc(&m->tileFlags, (size_t) std::max(1, std::max(m->fusedGrid[0], m->fusedGrid[1]))));
+    // per-round completion counters of the fused launch (zeroed before each
+    // launch; at most one round per tile) and the error word
+    CG_TRY(m->alloc(&m->tileFlags, (size_t) grid_for(nC, FUSED_TILE) + 1));
     CG_TRY(m->alloc(&m->fusedCtl, 2));
     CG_CHECK_CUDA(cudaMemsetAsync(m->fusedCtl, 0, 2 * sizeof(int), st));
+    CG_TRY(staged_setup(m, st));
     CG_CHECK_CUDA(cudaStreamSynchronize(st));
     return CUPCFD_E_SUCCESS;
 }
 }  // namespace cupcfd_gpu
 
 namespace {
-// Forward tiles beyond j the adjoint of tile j needs (bandwidth in tiles).
-int fused_lag_need(const cupcfd_gpu_mesh *m) { return (m->bandwidth + FUSED_TILE - 1) / FUSED_TILE + 1; }
+// Tiles beyond j whose gradients the adjoint of tile j reads.
+int fused_ahead_tiles(const cupcfd_gpu_mesh *m) { return (m->bandwidth + FUSED_TILE - 1) / FUSED_TILE + 1; }
 
-// Extra lag beyond that, in tiles: three rounds of the launch's CTAs, so the
-// adjoint of a round needs only rounds well behind it. CUPCFD_FUSED_SLACK (a
-// tile count) overrides it, for tuning.
-int fused_slack(const cupcfd_gpu_mesh *m, int precision) {
-    const char *env = std::getenv("CUPCFD_FUSED_SLACK");
-    if (env && *env) return std::max(0, std::atoi(env));
-    return 3 * m->fusedGrid[precision == CUPCFD_PREC_F64];
+// Rounds between a tile's forward and its adjoint: the adjoint of round r
+// then needs forward rounds < r only.
+int fused_lag_rounds(const cupcfd_gpu_mesh *m, int grid) {
+    return 1 + (fused_ahead_tiles(m) + grid - 1) / grid;
 }
 
-// Whether the auto mode fuses: the data the forward read between a tile's
-// forward and its adjoint (about 150 bytes per cell in FP32, 300 in FP64)
-// must stay well inside the 126 MB L2.
+// The fused launch runs only on request (mode 1): measured on B200 at 256^3
+// it is slower than the two launches (its tile body runs about 40% slower
+// even with every wait removed, and the L2 hits it is built for did not
+// materialise), so the auto mode takes the two launches.
 bool use_fused(const cupcfd_gpu_mesh *m, int precision) {
-    if (m->fusedGrid[precision == CUPCFD_PREC_F64] <= 0) return false;
-    if (m->fusion == 1) return true;
-    if (m->fusion == 2) return false;
-    double perCell = precision == CUPCFD_PREC_F64 ? 300.0 : 150.0;
-    double window = (2.0 * fused_lag_need(m) + fused_slack(m, precision)) * FUSED_TILE * perCell;
-    return window < 64e6;
+    return m->fusion == 1 && m->fusedGrid[precision == CUPCFD_PREC_F64] > 0;
 }
 
 int launch_fused(cupcfd_gpu_mesh *m, int precision, const void *phi, const void *phiB, const void *state,
                  const void *gface, void *grad, void *massFlux, void *phiBar, void *phiBBar, void *stateBar,
                  double *loss, cudaStream_t st) {
-    int nTiles = (m->nC + FUSED_TILE - 1) / FUSED_TILE;
-    int nPart = nTiles * (FUSED_TILE / 32);
+    int nTiles = (int) grid_for(m->nC, FUSED_TILE);
     double *part;
-    CG_TRY(scratch(m, S_LOSS, (size_t) nPart, &part));
-    int grid = m->fusedGrid[precision == CUPCFD_PREC_F64];
+    CG_TRY(scratch(m, S_LOSS, (size_t) nTiles, &part));
+    int grid = std::min(nTiles, m->fusedGrid[precision == CUPCFD_PREC_F64]);
     FusedCtl k;
-    k.prog = m->tileFlags;
+    k.done = m->tileFlags;
     k.err = m->fusedCtl + 1;
     k.nTiles = nTiles;
-    k.lagNeed = fused_lag_need(m);
-    k.lag = k.lagNeed + fused_slack(m, precision);
-    k.spinLimit = 1 << 20;
-    CG_CHECK_CUDA(cudaMemsetAsync(m->tileFlags, 0, sizeof(unsigned) * (size_t) grid, st));
+    k.nRounds = (nTiles + grid - 1) / grid;
+    k.aheadTiles = fused_ahead_tiles(m);
+    k.lagRounds = fused_lag_rounds(m, grid);
+    k.spinLimit = 1 << 22;
+    k.pf = prefetch_args(m);
+    k.pf.dist = grid;
+    // the prefetch reads whole 16-byte-aligned ranges of the user arrays
+    // (the gradient's component blocks too)
+    if (precision != CUPCFD_PREC_F32C || !m->staged || !aligned16(phi) || !aligned16(state) || !aligned16(gface) ||
+        !aligned16(grad) || m->nC % 4 != 0)
+        k.pf.desc = nullptr;
+    CG_CHECK_CUDA(cudaMemsetAsync(m->tileFlags, 0, sizeof(unsigned) * (size_t) k.nRounds, st));
     int nC = m->nC;
     SellView sv = sell(m);
     int64_t ldc = m->nC;
-    // cooperative launch: every CTA co-resident, which the round-robin tile
-    // assignment needs to be deadlock-free
+    // cooperative launch: every CTA co-resident, which the waits need
     if (precision == CUPCFD_PREC_F64) {
         const double4 *fg = m->fg64;
         const double *vol = m->vol;
@@ -227,7 +377,7 @@ int launch_fused(cupcfd_gpu_mesh *m, int precision, const void *phi, const void 
     }
     CG_LAUNCHED();
     if (loss) {
-        k_reduce_partials<<<1, 1024, 0, st>>>(nPart, part, loss);
+        k_reduce_partials<<<1, 1024, 0, st>>>(nTiles, part, loss);
         CG_LAUNCHED();
     }
     return CUPCFD_E_SUCCESS;
@@ -253,7 +403,7 @@ extern "C" int cupcfd_gpu_mesh_check_status(cupcfd_gpu_mesh *m, void *stream) {
     if (h) {
         CG_CHECK_CUDA(cudaMemsetAsync(m->fusedCtl + 1, 0, sizeof(int), st));
         CG_CHECK_CUDA(cudaStreamSynchronize(st));
-        set_error("a device-side wait of the fused forward+adjoint expired; its outputs are invalid");
+        set_error("a device-side wait (fused forward+adjoint or staged face loop) expired; its outputs are invalid");
         return CUPCFD_E_ERROR;
     }
     return CUPCFD_E_SUCCESS;
@@ -308,6 +458,7 @@ extern "C" int cupcfd_gpu_dev_gradient(cupcfd_gpu_mesh *m, int32_t precision, in
     CG_RETURN_IF(sign_mode != CUPCFD_SIGN_REFERENCE && sign_mode != CUPCFD_SIGN_SIGNED, CUPCFD_E_CONFIG_INVALID_VALUE,
                  "unknown sign_mode");
     CG_RETURN_IF(!phi || !grad || (m->nB > 0 && !phiB), CUPCFD_E_NULL_PTR, "dev_gradient: null device pointer");
+    CG_TRY(check_align(precision, {phi, phiB, grad, grad_o}, {}));
     cudaStream_t st = as_stream(stream);
     size_t es = precision == CUPCFD_PREC_F64 ? 8 : 4;
     size_t bytes = 3 * (size_t) m->nC * es;
@@ -337,6 +488,7 @@ extern "C" int cupcfd_gpu_dev_mass_plain(cupcfd_gpu_mesh *m, int32_t precision, 
     clear_error();
     CG_RETURN_IF(!m || !state || !massFlux, CUPCFD_E_NULL_PTR, "dev_mass_plain: null argument");
     CG_TRY(check_prec(m, precision));
+    CG_TRY(check_align(precision, {massFlux}, {state}));
     cudaStream_t st = as_stream(stream);
     if (precision == CUPCFD_PREC_F64)
         k_mass_plain_f64<<<grid_for(m->nF, BLK), BLK, 0, st>>>(m->nF, m->faceCells, m->fg64, (const double *) state, m->nC, (double *) massFlux);
@@ -351,6 +503,7 @@ extern "C" int cupcfd_gpu_dev_gradient_adjoint(cupcfd_gpu_mesh *m, int32_t preci
     clear_error();
     CG_RETURN_IF(!m || !gbar || !phiBar || (m->nB > 0 && !phiBBar), CUPCFD_E_NULL_PTR, "dev_gradient_adjoint: null argument");
     CG_TRY(check_prec(m, precision));
+    CG_TRY(check_align(precision, {gbar, phiBar, phiBBar}, {}));
     CG_RETURN_IF(sign_mode != CUPCFD_SIGN_REFERENCE && sign_mode != CUPCFD_SIGN_SIGNED, CUPCFD_E_CONFIG_INVALID_VALUE,
                  "unknown sign_mode");
     cudaStream_t st = as_stream(stream);
@@ -372,6 +525,7 @@ extern "C" int cupcfd_gpu_dev_mass_plain_adjoint(cupcfd_gpu_mesh *m, int32_t pre
     clear_error();
     CG_RETURN_IF(!m || !state || !mbar || !stateBar, CUPCFD_E_NULL_PTR, "dev_mass_plain_adjoint: null argument");
     CG_TRY(check_prec(m, precision));
+    CG_TRY(check_align(precision, {mbar}, {state, stateBar}));
     cudaStream_t st = as_stream(stream);
     unsigned grid = grid_for(m->nC, BLK);
     if (precision == CUPCFD_PREC_F64)
@@ -384,6 +538,30 @@ extern "C" int cupcfd_gpu_dev_mass_plain_adjoint(cupcfd_gpu_mesh *m, int32_t pre
     return CUPCFD_E_SUCCESS;
 }
 
+namespace {
+// FP32 forward: the staged kernel when the mesh and the pointers allow it
+// (identical results), else the unstaged one. One launch either way; the
+// caller checks it. part: per-256-cell loss partials, or null.
+void launch_fwd_f32(const cupcfd_gpu_mesh *m, const void *phi, const void *phiB, const void *state, const void *gface,
+                    void *grad, void *massFlux, double *part, cudaStream_t st) {
+    bool tiles = m->staged && aligned16(phi) && aligned16(state) && (!gface || aligned16(gface));
+    if (tiles && m->tileMode == 1)
+        k_fwd_f32_pf<<<grid_for(m->nC, BLK), BLK, 0, st>>>(m->nC, sell(m), m->fg32, (const float *) phi,
+                                                          (const float *) phiB, m->vol, (const float4 *) state,
+                                                          (const float *) gface, (float *) grad, (float *) massFlux,
+                                                          part, m->nC, prefetch_args(m));
+    else if (tiles)
+        k_fwd_f32_staged<STAGES><<<m->stagedGrid[0], STAGED_TILE, m->stagedSmem[0], st>>>(
+            staged_args(m, true), m->fg32, (const float *) phi, (const float *) phiB, m->vol, (const float4 *) state,
+            (const float *) gface, (float *) grad, (float *) massFlux, part, m->nC);
+    else
+        k_fwd_f32<BLK><<<grid_for(m->nC, BLK), BLK, 0, st>>>(m->nC, sell(m), m->fg32, (const float *) phi,
+                                                             (const float *) phiB, m->vol, (const float4 *) state,
+                                                             (const float *) gface, (float *) grad, (float *) massFlux,
+                                                             part, m->nC);
+}
+}  // namespace
+
 extern "C" int cupcfd_gpu_dev_forward(cupcfd_gpu_mesh *m, int32_t precision, const void *phi, const void *phiB,
                                       const void *state, const void *gface, void *grad, void *massFlux, double *loss,
                                       void *stream) {
@@ -392,6 +570,8 @@ extern "C" int cupcfd_gpu_dev_forward(cupcfd_gpu_mesh *m, int32_t precision, con
                  "dev_forward: null argument");
     CG_RETURN_IF((gface == nullptr) != (loss == nullptr), CUPCFD_E_NULL_PTR, "dev_forward: gface and loss go together");
     CG_TRY(check_prec(m, precision));
+    CG_TRY(check_align(precision, {phi, phiB, gface, grad, massFlux}, {state}));
+    CG_RETURN_IF(((uintptr_t) loss) % 8 != 0, CUPCFD_E_CONFIG_INVALID_VALUE, "dev_forward: loss not 8-byte aligned");
     cudaStream_t st = as_stream(stream);
     unsigned grid = grid_for(m->nC, BLK);
     double *part = nullptr;
@@ -401,9 +581,7 @@ extern "C" int cupcfd_gpu_dev_forward(cupcfd_gpu_mesh *m, int32_t precision, con
                                              m->vol, (const double *) state, (const double *) gface, (double *) grad,
                                              (double *) massFlux, part, m->nC);
     else
-        k_fwd_f32<BLK><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg32, (const float *) phi, (const float *) phiB,
-                                             m->vol, (const float4 *) state, (const float *) gface, (float *) grad,
-                                             (float *) massFlux, part, m->nC);
+        launch_fwd_f32(m, phi, phiB, state, gface, grad, massFlux, part, st);
     CG_LAUNCHED();
     if (loss) {
         k_reduce_partials<<<1, 1024, 0, st>>>((int) grid, part, loss);
@@ -418,11 +596,20 @@ extern "C" int cupcfd_gpu_dev_adjoint(cupcfd_gpu_mesh *m, int32_t precision, con
     CG_RETURN_IF(!m || !grad || !state || !gface || !phiBar || !stateBar || (m->nB > 0 && !phiBBar), CUPCFD_E_NULL_PTR,
                  "dev_adjoint: null argument");
     CG_TRY(check_prec(m, precision));
+    CG_TRY(check_align(precision, {grad, gface, phiBar, phiBBar}, {state, stateBar}));
     cudaStream_t st = as_stream(stream);
     unsigned grid = grid_for(m->nC, BLK);
     if (precision == CUPCFD_PREC_F64)
         k_adj_f64<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg64, (const double *) grad, 2.0, (const double *) state,
                                         (const double *) gface, (double *) phiBar, (double *) phiBBar, (double *) stateBar, m->nC);
+    else if (m->staged && m->tileMode == 1 && aligned16(grad) && aligned16(state) && aligned16(gface) && m->nC % 4 == 0)
+        k_adj_f32_pf<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg32, (const float *) grad, 2.f, (const float4 *) state,
+                                           (const float *) gface, (float *) phiBar, (float *) phiBBar,
+                                           (float4 *) stateBar, m->nC, prefetch_args(m));
+    else if (m->staged && aligned16(grad) && aligned16(state) && aligned16(gface) && m->nC % 4 == 0)
+        k_adj_f32_staged<STAGES><<<m->stagedGrid[1], STAGED_TILE, m->stagedSmem[1], st>>>(
+            staged_args(m, false), m->fg32, (const float *) grad, 2.f, (const float4 *) state, (const float *) gface,
+            (float *) phiBar, (float *) phiBBar, (float4 *) stateBar, m->nC);
     else
         k_adj_f32<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg32, (const float *) grad, 2.f, (const float4 *) state,
                                         (const float *) gface, (float *) phiBar, (float *) phiBBar, (float4 *) stateBar, m->nC);
@@ -441,8 +628,34 @@ extern "C" int cupcfd_gpu_dev_forward_adjoint(cupcfd_gpu_mesh *m, int32_t precis
     if (use_fused(m, precision)) {
         CG_RETURN_IF(!phi || !state || !grad || !massFlux || !phiBar || !stateBar || (m->nB > 0 && (!phiB || !phiBBar)),
                      CUPCFD_E_NULL_PTR, "dev_forward_adjoint: null argument");
+        CG_TRY(check_align(precision, {phi, phiB, gface, grad, massFlux, phiBar, phiBBar}, {state, stateBar}));
+        CG_RETURN_IF(((uintptr_t) lp) % 8 != 0, CUPCFD_E_CONFIG_INVALID_VALUE, "dev_forward_adjoint: loss not 8-byte aligned");
         return launch_fused(m, precision, phi, phiB, state, gface, grad, massFlux, phiBar, phiBBar, stateBar, lp,
                             as_stream(stream));
+    }
+    if (precision == CUPCFD_PREC_F32C && m->staged && m->tileMode == 1 && aligned16(phi) && aligned16(state) &&
+        aligned16(gface) && aligned16(grad) && aligned16(stateBar) && m->nC % 4 == 0) {
+        // forward with the mass-flux adjoint, then the gradient adjoint: the
+        // state and gface stream through one pass only
+        CG_RETURN_IF(!phi || !state || !grad || !massFlux || !phiBar || !stateBar || (m->nB > 0 && (!phiB || !phiBBar)),
+                     CUPCFD_E_NULL_PTR, "dev_forward_adjoint: null argument");
+        CG_TRY(check_align(precision, {phi, phiB, gface, grad, massFlux, phiBar, phiBBar}, {state, stateBar}));
+        CG_RETURN_IF(((uintptr_t) lp) % 8 != 0, CUPCFD_E_CONFIG_INVALID_VALUE, "dev_forward_adjoint: loss not 8-byte aligned");
+        cudaStream_t st = as_stream(stream);
+        unsigned grid = grid_for(m->nC, BLK);
+        double *part;
+        CG_TRY(scratch(m, S_LOSS, grid, &part));
+        PrefetchArgs pf = prefetch_args(m);
+        k_fwd_madj_f32_pf<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg32, (const float *) phi, (const float *) phiB,
+                                                m->vol, (const float4 *) state, (const float *) gface, (float *) grad,
+                                                (float *) massFlux, (float4 *) stateBar, part, m->nC, pf);
+        CG_LAUNCHED();
+        k_reduce_partials<<<1, 1024, 0, st>>>((int) grid, part, lp);
+        CG_LAUNCHED();
+        k_gadj_f32_pf<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg32, (const float *) grad, 2.f, (float *) phiBar,
+                                            (float *) phiBBar, m->nC, pf);
+        CG_LAUNCHED();
+        return CUPCFD_E_SUCCESS;
     }
     CG_TRY(cupcfd_gpu_dev_forward(m, precision, phi, phiB, state, gface, grad, massFlux, lp, stream));
     return cupcfd_gpu_dev_adjoint(m, precision, grad, state, gface, phiBar, phiBBar, stateBar, stream);
@@ -856,6 +1069,12 @@ extern "C" int cupcfd_gpu_dev_forward_noalloc(cupcfd_gpu_mesh *m, int32_t precis
     if ((gface == nullptr) != (loss == nullptr)) return CUPCFD_E_NULL_PTR;
     if ((precision != CUPCFD_PREC_F64 && precision != CUPCFD_PREC_F32C) || !(m->precisions & (1 << precision)))
         return CUPCFD_E_CONFIG_INVALID_VALUE;
+    {
+        uintptr_t a = precision == CUPCFD_PREC_F64 ? 8 : 4, sa = precision == CUPCFD_PREC_F64 ? 8 : 16;
+        for (const void *p : {phi, phiB, gface, (const void *) grad, (const void *) massFlux})
+            if (((uintptr_t) p) % a != 0) return CUPCFD_E_CONFIG_INVALID_VALUE;
+        if (((uintptr_t) state) % sa != 0 || ((uintptr_t) loss) % 8 != 0) return CUPCFD_E_CONFIG_INVALID_VALUE;
+    }
     unsigned grid = grid_for(m->nC, BLK);
     if (loss && grid > (unsigned) NOALLOC_MAX_PARTIALS) return CUPCFD_E_ARRAY_SIZE_MISMATCH;
     int dev = m->device;
@@ -878,9 +1097,7 @@ extern "C" int cupcfd_gpu_dev_forward_noalloc(cupcfd_gpu_mesh *m, int32_t precis
                                              m->vol, (const double *) state, (const double *) gface, (double *) grad,
                                              (double *) massFlux, part, m->nC);
     else
-        k_fwd_f32<BLK><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg32, (const float *) phi, (const float *) phiB,
-                                             m->vol, (const float4 *) state, (const float *) gface, (float *) grad,
-                                             (float *) massFlux, part, m->nC);
+        launch_fwd_f32(m, phi, phiB, state, gface, grad, massFlux, part, st);
     g_launches.fetch_add(1, std::memory_order_relaxed);
     if (cudaGetLastError() != cudaSuccess) return CUPCFD_E_ERROR;
     if (loss) {

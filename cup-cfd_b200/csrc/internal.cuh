@@ -76,6 +76,7 @@ struct Sell {
     int *slicePtr = nullptr;
     int2 *inc = nullptr;
     int64_t nEntries = 0;
+    int width = 0;  // the common width when every slice has it (then slice s starts at 32 * width * s), else 0
 };
 
 }  // namespace cupcfd_gpu
@@ -120,6 +121,17 @@ struct cupcfd_gpu_mesh {
     unsigned *tileFlags = nullptr; // per-CTA progress counters of the fused launch
     int *fusedCtl = nullptr;      // [1] error bits ([0] unused)
     int fusedGrid[2] = {0, 0};    // resident CTAs of the FP32 / FP64 fused kernels
+    // staged face loops: per-tile ranges (TileDesc[nTiles], 256-cell tiles),
+    // the largest tile's entry and owned-face counts, resident CTAs of the
+    // FP32 staged forward / adjoint and their dynamic shared memory
+    void *tileDesc = nullptr;
+    int nTiles = 0;
+    bool staged = false;
+    int stagedEntCap = 0, stagedFaceCap = 0;  // stage capacities (entries, faces per tile)
+    int stagedGrid[2] = {0, 0};
+    int stagedSmem[2] = {0, 0};
+    int tileMode = 0;             // 0 unstaged, 1 L2 prefetch, 2 shared-memory stages
+    int prefetchDist = 0;         // tiles ahead for the L2 prefetch variant
 
     std::vector<cupcfd_gpu::DevBuf> owned;  // everything above, freed by destroy
     std::vector<cupcfd_gpu::DevBuf> scratch; // reusable buffers for host-buffer calls

@@ -154,6 +154,82 @@ __device__ __forceinline__ double fwd_cell_f32(int c, const SellView &sv, const 
     return lsum + V * ((double) rx * rx + (double) ry * ry + (double) rz * rz);
 }
 
+// Per-cell body of the FP32 forward that also runs the mass-flux part of
+// the adjoint (which needs only inputs: state, gface and geometry): the
+// forward of fwd_cell_f32 plus, over every interior face, the rhobar / ubar
+// accumulation of adj_cell_f32, with the same arithmetic in the same face
+// order, so stbar equals the one the full adjoint writes bit for bit.
+template <int CH>
+__device__ __forceinline__ double fwd_madj_cell_f32(int c, const SellView &sv, const float4 *__restrict__ fg,
+                                                    const float *__restrict__ phi, const float *__restrict__ phiB,
+                                                    const double *__restrict__ vol, const float4 *__restrict__ st,
+                                                    const float *__restrict__ gface, float *__restrict__ g,
+                                                    float *__restrict__ mflux, float4 *__restrict__ stbar,
+                                                    int64_t ldc) {
+    int w;
+    const int2 *e = cell_entries(sv, c, w);
+    float phic = phi[c];
+    float4 sc = st[c];
+    Acc2 ax, ay, az, rb, ub, vb, wb;
+    double lsum = 0.0;
+    for (int k0 = 0; k0 < w; k0 += CH) {
+        int2 en[CH];
+        load_entries(e, k0, w, en);
+        float4 G[CH], so[CH];
+        float pv[CH], gf[CH];
+#pragma unroll
+        for (int j = 0; j < CH; j++) {
+            int code = en[j].x;
+            if (code < 0) continue;
+            int f = code >> 1, o = en[j].y;
+            G[j] = __ldg(fg + f);
+            pv[j] = o >= 0 ? __ldg(phi + o) : __ldg(phiB + (-1 - o));
+            if (o >= 0) {
+                so[j] = __ldg(st + o);
+                gf[j] = __ldg(gface + f);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < CH; j++) {
+            int code = en[j].x;
+            if (code < 0) continue;
+            bool isN = code & 1;
+            int o = en[j].y;
+            float phif;
+            if (o < 0) {
+                phif = pv[j];
+            } else {
+                float facn = G[j].w, facp = 1.f - facn;
+                phif = isN ? fmaf(facn, phic, facp * pv[j]) : fmaf(facn, pv[j], facp * phic);
+                if (!isN) {
+                    float denf = fmaf(facn, so[j].x, facp * sc.x);
+                    float uF = fmaf(facn, so[j].y, facp * sc.y);
+                    float vF = fmaf(facn, so[j].z, facp * sc.z);
+                    float wF = fmaf(facn, so[j].w, facp * sc.w);
+                    float m = denf * fmaf(uF, G[j].x, fmaf(vF, G[j].y, wF * G[j].z));
+                    mflux[code >> 1] = m;
+                    lsum += (double) gf[j] * (double) m;
+                }
+                // mass part of the adjoint (adj_cell_f32)
+                float wc = isN ? facn : facp, wo = isN ? facp : facn;
+                float denA = fmaf(wc, sc.x, wo * so[j].x);
+                float uA = fmaf(wc, sc.y, wo * so[j].y), vA = fmaf(wc, sc.z, wo * so[j].z), wA = fmaf(wc, sc.w, wo * so[j].w);
+                float a = wc * gf[j];
+                rb.add_prod(a, fmaf(uA, G[j].x, fmaf(vA, G[j].y, wA * G[j].z)));
+                float b = a * denA;
+                ub.add_prod(b, G[j].x); vb.add_prod(b, G[j].y); wb.add_prod(b, G[j].z);
+            }
+            ax.add_prod(phif, G[j].x); ay.add_prod(phif, G[j].y); az.add_prod(phif, G[j].z);
+        }
+    }
+    double V = vol[c];
+    double fact = 1.0 / V;
+    float rx = (float) (ax.value() * fact), ry = (float) (ay.value() * fact), rz = (float) (az.value() * fact);
+    g[c] = rx; g[ldc + c] = ry; g[2 * ldc + c] = rz;
+    stbar[c] = make_float4((float) rb.value(), (float) ub.value(), (float) vb.value(), (float) wb.value());
+    return lsum + V * ((double) rx * rx + (double) ry * ry + (double) rz * rz);
+}
+
 // ---------------------------------------------------------------------------
 // Fused forward of the benchmark pipeline: gradient (nGradient = 1) and the
 // plain mass flux of the faces each cell owns, plus the per-block FP64

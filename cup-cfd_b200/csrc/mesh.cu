@@ -6,6 +6,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 
@@ -638,6 +639,11 @@ int build_mesh_from_source(cupcfd_gpu_mesh *m, const Source &s, const cupcfd_mes
         g_launches.fetch_add(1);
         CG_CHECK_CUDA(cudaMemcpyAsync(&m->maxDeg, mx, sizeof(int), cudaMemcpyDeviceToHost, st));
         CG_CHECK_CUDA(cudaStreamSynchronize(st));
+        // every slice is maxDeg wide exactly when the entries fill 32 * maxDeg per slice
+        // (CUPCFD_UNIFORM_SELL=0 keeps the slice-pointer lookup, for comparisons)
+        const char *e = std::getenv("CUPCFD_UNIFORM_SELL");
+        bool allow = !(e && std::strcmp(e, "0") == 0);
+        m->sell.width = (allow && m->sell.nEntries == (int64_t) 32 * nSlices * m->maxDeg) ? m->maxDeg : 0;
     }
 
     // --- numbering bandwidth and the fused pipeline's control words (api.cu)
@@ -816,6 +822,8 @@ extern "C" int cupcfd_gpu_mesh_get_info(const cupcfd_gpu_mesh *m, cupcfd_mesh_in
     info->precisions = m->precisions;
     info->bandwidth = m->bandwidth;
     info->deviceBytes = m->bytes;
+    info->stagedCtas = m->staged ? m->stagedGrid[0] : 0;
+    info->stagedSmem = m->staged ? m->stagedSmem[0] : 0;
     return CUPCFD_E_SUCCESS;
 }
 

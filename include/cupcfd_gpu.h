@@ -117,6 +117,8 @@ typedef struct {
     int32_t order, precisions;
     int32_t bandwidth;   /* largest |c - neighbour| of the internal numbering */
     int64_t deviceBytes; /* device memory held by the mesh */
+    int32_t stagedCtas;  /* CTAs of a staged FP32 forward launch; 0 when this mesh runs the unstaged kernels only */
+    int32_t stagedSmem;  /* its dynamic shared memory per CTA, bytes */
 } cupcfd_mesh_info;
 
 typedef struct cupcfd_gpu_mesh cupcfd_gpu_mesh;
@@ -161,9 +163,11 @@ int cupcfd_gpu_mesh_create_jittered(int32_t nx, int32_t ny, int32_t nz, double j
 int cupcfd_gpu_mesh_destroy(cupcfd_gpu_mesh *mesh);
 int cupcfd_gpu_mesh_get_info(const cupcfd_gpu_mesh *mesh, cupcfd_mesh_info *info);
 
-/* Forward+adjoint execution: 0 = auto (one wavefront-fused launch when the
- * numbering's bandwidth keeps the lag window well inside L2, else two
- * launches), 1 = always fused, 2 = never fused. */
+/* Forward+adjoint execution: 1 = one wavefront-fused cooperative launch
+ * (forward and adjoint tiles interleaved, the adjoint of a tile a few rounds
+ * behind its forward); 0 (auto) and 2 = two launches, the faster on B200 at
+ * every size measured: a forward that also runs the mass-flux adjoint, then
+ * the gradient adjoint. All modes give bit-identical results. */
 int cupcfd_gpu_mesh_set_fusion(cupcfd_gpu_mesh *mesh, int32_t mode);
 
 /* Synchronises the mesh's work and returns CUPCFD_E_ERROR (message in
@@ -260,7 +264,14 @@ int cupcfd_gpu_forward_adjoint(cupcfd_gpu_mesh *mesh, int32_t precision,
  *   boundary scalar T[nBoundaries] (reference boundary order)
  *   cell state      T[4][nCells]   (rho, u, v, w blocks) for F64,
  *                   float4[nCells] (rho, u, v, w interleaved) for F32C
- * stream: a cudaStream_t (NULL = the legacy default stream). */
+ * stream: a cudaStream_t (NULL = the legacy default stream).
+ * Every array is aligned to its element (the F32C state to 16 bytes);
+ * misaligned pointers are rejected with CUPCFD_E_CONFIG_INVALID_VALUE.
+ * F32C forward/adjoint calls whose arrays start on 16-byte boundaries (and,
+ * for the adjoint, nCells a multiple of 4) run the staged kernels, which
+ * fetch each 256-cell tile's contiguous ranges into shared memory with bulk
+ * async copies; other pointers take the unstaged kernels. Results are
+ * bit-identical either way. */
 
 /* Reorders n-component cell data (component blocks of nCells, element type
  * src_size / dst_size bytes = 4 or 8, converting) between numberings.

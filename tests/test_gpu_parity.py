@@ -410,11 +410,13 @@ def test_rcm_bounds_bandwidth_of_permuted_mesh(cg, gpu):
 
 
 @pytest.mark.parametrize("order", [2, 3])
-def test_fused_host_call_matches_oracle(cg, gpu, order):
-    """The host-buffer forward+adjoint (fused in auto mode for these
-    numberings) against the FP64 oracle."""
+@pytest.mark.parametrize("fusion", [0, 1])
+def test_fused_host_call_matches_oracle(cg, gpu, order, fusion):
+    """The host-buffer forward+adjoint (two launches in auto mode, one fused
+    launch in mode 1) against the FP64 oracle."""
     ref = O.jitter(14, 12, 11, 0.25, seed=16, permute=True)
     mesh = cg.Mesh.from_arrays(ref, order=order)
+    mesh.set_fusion(fusion)
     f = O.fields(ref, 17)
     gface = np.random.Generator(np.random.Philox(key=18)).standard_normal(ref["nFaces"])
     out = cg.forward_adjoint(mesh, cg.PREC_F64, f["phi"], f["phiB"], f["den"], f["u"], f["v"], f["w"], gface)

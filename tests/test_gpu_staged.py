@@ -1,0 +1,180 @@
+"""Tile-path FP32 kernels against the plain ones: the shared-memory staged
+and the L2-prefetch forward/adjoint, and the two-launch forward+adjoint
+(forward with the mass-flux adjoint, then the gradient adjoint).
+
+The staged kernels fetch each 256-cell tile's contiguous ranges (incidence
+entries, the tile's owned faces, cell arrays) into shared memory with bulk
+async copies and otherwise run the same per-cell arithmetic in the same face
+order, so results must be bit-identical. The library picks the staged kernels
+when the user arrays start on 16-byte boundaries; passing views offset by one
+float (4 bytes) makes it take the unstaged kernels on the same mesh and data.
+
+Cases: the Morton, owner and RCM numberings (the native one keeps the
+reference's face order, which is not by owner, and is never staged), a
+ragged last tile, an odd cell count (the
+adjoint's gradient blocks are then not 16-byte aligned, so only the forward
+is staged), a jittered mesh, and stage capacities lowered far below the
+tiles' needs so entries and faces overflow to the global-memory path.
+"""
+import os
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _fields(torch, mesh, seed):
+    dev = torch.device("cuda:0")
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    nC, nF, nB = mesh.nCells, mesh.nFaces, mesh.nBoundaries
+    phi = (torch.rand(nC, generator=g, device=dev, dtype=torch.float64) * 2 - 1).float()
+    phiB = (torch.rand(max(nB, 1), generator=g, device=dev, dtype=torch.float64) * 2 - 1).float()
+    st = torch.randn(nC, 4, generator=g, device=dev, dtype=torch.float64).float()
+    st[:, 0] = 0.9 + 0.2 * torch.rand(nC, generator=g, device=dev, dtype=torch.float64).float()
+    gface = torch.randn(nF, generator=g, device=dev, dtype=torch.float64).float()
+    return phi, phiB, st.contiguous(), gface
+
+
+def _offset_copy(torch, t):
+    """Same values in a buffer that starts 4 bytes past a 16-byte boundary."""
+    buf = torch.empty(t.numel() + 4, dtype=t.dtype, device=t.device)
+    v = buf[1:1 + t.numel()].view(t.shape)
+    v.copy_(t)
+    assert v.data_ptr() % 16 == 4
+    return v
+
+
+def _run(cg, torch, mesh, phi, phiB, st, gface, offset):
+    dev = torch.device("cuda:0")
+    nC, nF, nB = mesh.nCells, mesh.nFaces, mesh.nBoundaries
+    if offset:
+        phi, gface = _offset_copy(torch, phi), _offset_copy(torch, gface)
+        grad = _offset_copy(torch, torch.full((3, nC), float("nan"), device=dev))
+    else:
+        grad = torch.full((3, nC), float("nan"), device=dev)
+    mf = torch.full((nF,), -7.0, device=dev)
+    loss = torch.full((1,), float("nan"), dtype=torch.float64, device=dev)
+    pb = torch.full((nC,), float("nan"), device=dev)
+    pbb = torch.full((max(nB, 1),), float("nan"), device=dev)
+    sb = torch.full((nC, 4), float("nan"), device=dev)
+    s = torch.cuda.current_stream()
+    cg.dev_forward(mesh, cg.PREC_F32C, phi, phiB, st, grad, mf, gface=gface, loss=loss, stream=s)
+    cg.dev_adjoint(mesh, cg.PREC_F32C, grad, st, gface, pb, pbb, sb, stream=s)
+    mesh.check_status()
+    torch.cuda.synchronize()
+    return [grad.clone(), mf, loss, pb, pbb, sb]
+
+
+def _assert_same(a, b):
+    import torch
+    names = ["grad", "massFlux", "loss", "phiBar", "phiBBar", "stateBar"]
+    for n, x, y in zip(names, a, b):
+        assert torch.equal(x, y), n
+        assert torch.isfinite(x).all(), n
+
+
+CASES = [
+    ("structgen", (12, 10, 8), "ORDER_OWNER"),     # 960 cells: ragged last tile
+    ("structgen", (33, 17, 9), "ORDER_MORTON"),    # 5049 cells: odd count
+    ("structgen", (40, 32, 24), "ORDER_RCM"),
+    ("structgen", (64, 64, 64), "ORDER_OWNER"),    # whole tiles only
+    ("jittered", (20, 18, 16), "ORDER_OWNER"),
+]
+
+
+@pytest.mark.parametrize("kind,dims,order", CASES)
+def test_staged_equals_unstaged(cg, gpu, kind, dims, order):
+    import torch
+    make = cg.Mesh.structgen if kind == "structgen" else cg.Mesh.jittered
+    mesh = make(*dims, order=getattr(cg, order))
+    assert mesh.stagedCtas > 0 and mesh.stagedSmem > 0
+    fields = _fields(torch, mesh, 5)
+    _assert_same(_run(cg, torch, mesh, *fields, offset=False), _run(cg, torch, mesh, *fields, offset=True))
+
+
+def test_native_numbering_is_unstaged(cg, gpu):
+    """ORDER_NATIVE keeps the reference's face numbering, which is not sorted
+    by owner tile, so the tile ranges do not exist and the mesh runs the
+    unstaged kernels."""
+    assert cg.Mesh.structgen(16, 12, 8, order=cg.ORDER_NATIVE).stagedCtas == 0
+
+
+def test_staged_overflow_to_global(cg, gpu, monkeypatch):
+    """Stage buffers far smaller than a tile's ranges: the entries and faces
+    beyond them are read from global memory, results unchanged."""
+    import torch
+    monkeypatch.setenv("CUPCFD_STAGED_ENT_CAP", "64")
+    monkeypatch.setenv("CUPCFD_STAGED_FACE_CAP", "8")
+    small = cg.Mesh.structgen(30, 20, 10, order=cg.ORDER_MORTON)
+    monkeypatch.delenv("CUPCFD_STAGED_ENT_CAP")
+    monkeypatch.delenv("CUPCFD_STAGED_FACE_CAP")
+    full = cg.Mesh.structgen(30, 20, 10, order=cg.ORDER_MORTON)
+    assert 0 < small.stagedSmem < full.stagedSmem
+    fields = _fields(torch, small, 9)
+    ref = _run(cg, torch, full, *fields, offset=True)
+    _assert_same(_run(cg, torch, small, *fields, offset=False), ref)
+    _assert_same(_run(cg, torch, full, *fields, offset=False), ref)
+
+
+def test_staging_can_be_disabled(cg, gpu, monkeypatch):
+    import torch
+    monkeypatch.setenv("CUPCFD_STAGED", "0")
+    off = cg.Mesh.structgen(16, 16, 16, order=cg.ORDER_OWNER)
+    monkeypatch.delenv("CUPCFD_STAGED")
+    on = cg.Mesh.structgen(16, 16, 16, order=cg.ORDER_OWNER)
+    assert off.stagedCtas == 0 and on.stagedCtas > 0
+    fields = _fields(torch, on, 3)
+    _assert_same(_run(cg, torch, off, *fields, offset=False), _run(cg, torch, on, *fields, offset=False))
+
+
+def test_misaligned_state_is_rejected(cg, gpu):
+    """float4 state records must start on 16-byte boundaries; a misaligned
+    pointer is refused before anything is launched."""
+    import torch
+    mesh = cg.Mesh.structgen(8, 8, 8, order=cg.ORDER_OWNER)
+    phi, phiB, st, gface = _fields(torch, mesh, 1)
+    bad = _offset_copy(torch, st)
+    grad = torch.zeros(3, mesh.nCells, device="cuda:0")
+    mf = torch.zeros(mesh.nFaces, device="cuda:0")
+    before = cg.launch_count()
+    rc = cg.lib().cupcfd_gpu_dev_forward(mesh.h, cg.PREC_F32C, cg._p(phi), cg._p(phiB), cg._p(bad), None,
+                                         cg._p(grad), cg._p(mf), None, None)
+    assert rc == cg.E_CONFIG_INVALID_VALUE
+    assert "16-byte" in cg.last_error()
+    assert cg.launch_count() == before
+
+
+def _run_pipeline(cg, torch, mesh, phi, phiB, st, gface, offset):
+    """dev_forward_adjoint; offset views of phi/gface/grad force the plain kernels."""
+    dev = torch.device("cuda:0")
+    nC, nF, nB = mesh.nCells, mesh.nFaces, mesh.nBoundaries
+    if offset:
+        phi, gface = _offset_copy(torch, phi), _offset_copy(torch, gface)
+        grad = _offset_copy(torch, torch.full((3, nC), float("nan"), device=dev))
+    else:
+        grad = torch.full((3, nC), float("nan"), device=dev)
+    mf = torch.full((nF,), -7.0, device=dev)
+    loss = torch.full((1,), float("nan"), dtype=torch.float64, device=dev)
+    pb = torch.full((nC,), float("nan"), device=dev)
+    pbb = torch.full((max(nB, 1),), float("nan"), device=dev)
+    sb = torch.full((nC, 4), float("nan"), device=dev)
+    s = torch.cuda.current_stream()
+    cg.dev_forward_adjoint(mesh, cg.PREC_F32C, phi, phiB, st, gface, grad, mf, pb, pbb, sb, loss, stream=s)
+    mesh.check_status()
+    torch.cuda.synchronize()
+    return [grad.clone(), mf, loss, pb, pbb, sb]
+
+
+@pytest.mark.parametrize("kind,dims,order", CASES)
+def test_forward_adjoint_pipeline_equals_separate_calls(cg, gpu, kind, dims, order):
+    """The two-launch forward+adjoint (mass-flux adjoint moved into the
+    forward) equals dev_forward followed by dev_adjoint, bit for bit, and
+    so does the same call on offset pointers (plain kernels)."""
+    import torch
+    make = cg.Mesh.structgen if kind == "structgen" else cg.Mesh.jittered
+    mesh = make(*dims, order=getattr(cg, order))
+    fields = _fields(torch, mesh, 7)
+    ref = _run(cg, torch, mesh, *fields, offset=False)
+    _assert_same(_run_pipeline(cg, torch, mesh, *fields, offset=False), ref)
+    _assert_same(_run_pipeline(cg, torch, mesh, *fields, offset=True), ref)
