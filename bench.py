@@ -66,6 +66,13 @@ def bytes_model(nC, nF, nFi, nB):
     """Algorithmic (compulsory) bytes: each distinct input read once, each
     output written once; int32 indices; FP64 volumes in both precisions."""
     return {
+        # forward with the mass-flux adjoint (k_fwd_madj_f32_pf): phi 4 + rho,u,v,w 16 + V 8 + grad 12 +
+        # statebar 16 per cell; S 12 + lambda 4 + cell1 4 per face; cell2 4 + g_f 4 + m_f 4 per interior
+        # face; phiB 4 per boundary face
+        "fwd_madj_f32": 56 * nC + 20 * nF + 12 * nFi + 4 * nB,
+        # gradient adjoint (k_gadj_f32_pf): grad 12 + phibar 4 per cell; face geometry and connectivity
+        # as above; phibBar 4 per boundary face
+        "gadj_f32": 16 * nC + 20 * nF + 4 * nFi + 4 * nB,
         # fused forward, FP32: phi 4 + rho,u,v,w 16 + V 8 + grad 12 per cell;
         # S 12 + lambda 4 + cell1 4 per face; cell2 4 + m_f 4 per interior face; phiB 4 per boundary face
         "fwd_f32": 40 * nC + 20 * nF + 8 * nFi + 4 * nB,
@@ -290,6 +297,8 @@ def run_gpu(a):
     clocks.start()
     time.sleep(0.3)
     launches0 = cg.launch_count()
+    cg.timing_read()
+    cg.timing_enable(True)        # per-kernel CUDA events on the launching stream, over the timed region
     t_start.record(st)
     for k in range(K):
         ev[k][0].record(st)
@@ -298,15 +307,16 @@ def run_gpu(a):
     t_end.record(st)
     torch.cuda.synchronize()
     launches = cg.launch_count() - launches0
+    cg.timing_enable(False)
+    ktimes = cg.timing_read()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     clk = clocks.stop()
     status = mesh.check_status(st)
     if status != cg.E_SUCCESS:
-        raise RuntimeError(f"fused pipeline reported an error: {cg.last_error()}")
+        raise RuntimeError(f"forward+adjoint reported an error: {cg.last_error()}")
     total_ms = t_start.elapsed_time(t_end)
-    launch_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in ev)
     tmax = torch.tensor([total_ms], dtype=torch.float64, device=dev)
     if dist:
         dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
@@ -314,7 +324,7 @@ def run_gpu(a):
     ms_step = total_ms / K
     value = world * nF / (ms_step * 1e-3) / 1e9
 
-    # ---- the same pipeline as two launches (forward, then adjoint), for comparison
+    # ---- the same work as the separate dev_forward and dev_adjoint calls, for comparison
     e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
     K2p = max(1, K // 4)
     for _ in range(2):
@@ -413,18 +423,27 @@ def run_gpu(a):
            "ms_per_step": te * 1e3, "steps": K2,
            "call": "cupcfd_gpu_forward_adjoint (host FP64 buffers in reference numbering, pinned)"}
 
-    # ---- roofline of the dominant kernel (the fused forward+adjoint launch)
+    # ---- roofline of the dominant kernel, from the device timers of the timed region
     bm = bytes_model(nC, nF, nFi, nB)
     peak, peak_src = measured_peaks()
-    fused = mesh.bandwidth is not None and launches == 2 * K  # one fused launch + one loss reduction per step
-    kname = "k_fused_f32" if fused else "k_fwd_f32+k_adj_f32"
-    achieved = bm["pipeline_f32"] / (launch_ms * 1e-3) / 1e9
+    kbytes = {"k_fwd_madj_f32_pf": bm["fwd_madj_f32"], "k_gadj_f32_pf": bm["gadj_f32"], "k_fused_f32": bm["pipeline_f32"],
+              "k_fwd_f32_pf": bm["fwd_f32"], "k_fwd_f32": bm["fwd_f32"], "k_adj_f32_pf": bm["adj_f32"],
+              "k_adj_f32": bm["adj_f32"]}
+    tot_ms = sum(v[1] for v in ktimes.values()) or 1.0
+    kernels = {k: {"launches": v[0], "avg_ms": v[1] / max(v[0], 1), "share": v[1] / tot_ms,
+                   "algorithmic_bytes": kbytes.get(k)} for k, v in ktimes.items()}
+    kname = max(ktimes, key=lambda k: ktimes[k][1]) if ktimes else None
+    kms = kernels[kname]["avg_ms"] if kname else float("nan")
+    kb = kbytes.get(kname, 0)
+    achieved = kb / (kms * 1e-3) / 1e9
     tr = profile_traffic().get(f"{kname}@{n}")
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": tr, "kernel": kname, "peak_source": peak_src,
-            "algorithmic_bytes_per_launch": bm["pipeline_f32"], "ms_per_launch": launch_ms,
-            "note": "ms_per_launch brackets the fused launch plus the loss reduction (1 block) and a 4-byte memset"}
-    two_pass = {"fwd_ms": fwd_ms, "adj_ms": adj_ms, "value": world * nF / ((fwd_ms + adj_ms) * 1e-3) / 1e9,
+            "traffic": tr, "kernel": kname, "peak_source": peak_src, "algorithmic_bytes_per_launch": kb,
+            "ms_per_launch": kms,
+            "pipeline": {"algorithmic_bytes": bm["pipeline_f32"], "ms_per_step": ms_step,
+                         "achieved": bm["pipeline_f32"] / (ms_step * 1e-3) / 1e9,
+                         "frac": bm["pipeline_f32"] / (ms_step * 1e-3) / 1e9 / peak}}
+    separate = {"fwd_ms": fwd_ms, "adj_ms": adj_ms, "value": world * nF / ((fwd_ms + adj_ms) * 1e-3) / 1e9,
                 "fwd_gbs": bm["fwd_f32"] / (fwd_ms * 1e-3) / 1e9, "adj_gbs": bm["adj_f32"] / (adj_ms * 1e-3) / 1e9}
 
     cpu = None
@@ -445,9 +464,10 @@ def run_gpu(a):
                        "order": ["native", "morton", "owner", "rcm"][a.order], "parallelism": f"replicas x{world}",
                        "l2": f"inputs larger than L2 ({bm['pipeline_f32'] / 1e9:.2f} GB compulsory traffic per step)"},
             "roofline": roof,
-            "two_pass": two_pass,
+            "kernels": kernels,
+            "separate_calls": separate,
             "mesh": {"order": ["native", "morton", "owner", "rcm"][a.order], "bandwidth": mesh.bandwidth,
-                     "fused": fused},
+                     "forward_adjoint": "two launches: forward with the mass-flux adjoint, then the gradient adjoint"},
             "fp64_plain_forward": {"value": world * nF / (ms64 * 1e-3) / 1e9, "unit": "Gfaces/s", "ms_per_step": ms64,
                                    "gbs": bm["fwd_f64"] / (ms64 * 1e-3) / 1e9,
                                    "frac": bm["fwd_f64"] / (ms64 * 1e-3) / 1e9 / peak},

@@ -77,6 +77,8 @@ SIGNATURES = {
     "cupcfd_gpu_last_error": ([], C.c_char_p),
     "cupcfd_gpu_version": ([], C.c_char_p),
     "cupcfd_gpu_launch_count": ([], C.c_int64),
+    "cupcfd_gpu_timing_enable": ([_I], _I),
+    "cupcfd_gpu_timing_read": ([_I, _VP, _VP, _VP, _VP], _I),
     "cupcfd_gpu_mesh_create": ([_VP, _VP, _VP], _I),
     "cupcfd_gpu_mesh_create_structgen": ([_I, _I, _I, _VP, _VP, _VP], _I),
     "cupcfd_gpu_mesh_create_jittered": ([_I, _I, _I, _D, C.c_uint64, _I, _VP, _VP], _I),
@@ -132,6 +134,25 @@ def last_error() -> str:
 
 def launch_count() -> int:
     return int(lib().cupcfd_gpu_launch_count())
+
+
+def timing_enable(on: bool = True):
+    """Bracket this library's forward/adjoint kernel launches with CUDA events."""
+    check(lib().cupcfd_gpu_timing_enable(1 if on else 0))
+
+
+def timing_read(capacity: int = 32) -> dict:
+    """{kernel name: (launches, device ms)} since the previous read (waits for the events)."""
+    names = C.create_string_buffer(64 * capacity)
+    launches = (C.c_int64 * capacity)()
+    ms = (C.c_double * capacity)()
+    count = C.c_int32()
+    check(lib().cupcfd_gpu_timing_read(capacity, names, launches, ms, C.byref(count)))
+    out = {}
+    for i in range(min(count.value, capacity)):
+        nm = names.raw[64 * i:64 * (i + 1)].split(b"\0", 1)[0].decode()
+        out[nm] = (int(launches[i]), float(ms[i]))
+    return out
 
 
 def check(rc):

@@ -4,6 +4,8 @@
 #include <cstring>
 #include <cstdlib>
 #include <initializer_list>
+#include <map>
+#include <mutex>
 
 #include "kernels_fused.cuh"
 
@@ -29,6 +31,46 @@ int scratch(cupcfd_gpu_mesh *m, int slot, size_t n, T **p) {
 
 inline cudaStream_t as_stream(void *s) { return (cudaStream_t) s; }
 inline SellView sell(const cupcfd_gpu_mesh *m) { return SellView{m->sell.slicePtr, m->sell.inc, m->sell.width}; }
+
+// ---------------------------------------------------------------------------
+// device timers (cupcfd_gpu_timing_*): a KTIMER scope records one event
+// before and one after the launch it encloses, on the launch's stream
+// ---------------------------------------------------------------------------
+struct TimerRec {
+    const char *name;
+    int device;
+    cudaEvent_t a, b;
+};
+std::mutex g_timer_mu;
+std::atomic<bool> g_timer_on{false};
+std::vector<TimerRec> g_timer_recs;
+
+class KernelTimer {
+  public:
+    KernelTimer(const char *name, cudaStream_t st) : name_(name), st_(st) {
+        if (!g_timer_on.load(std::memory_order_relaxed)) return;
+        if (cudaEventCreate(&a_) != cudaSuccess || cudaEventRecord(a_, st_) != cudaSuccess) a_ = nullptr;
+    }
+    void set_name(const char *name) { name_ = name; }
+    ~KernelTimer() {
+        if (!a_) return;
+        cudaEvent_t b = nullptr;
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaEventCreate(&b) != cudaSuccess || cudaEventRecord(b, st_) != cudaSuccess) {
+            cudaEventDestroy(a_);
+            if (b) cudaEventDestroy(b);
+            return;
+        }
+        std::lock_guard<std::mutex> lk(g_timer_mu);
+        g_timer_recs.push_back({name_, dev, a_, b});
+    }
+  private:
+    const char *name_;
+    cudaStream_t st_;
+    cudaEvent_t a_ = nullptr;
+};
+#define KTIMER(name, stream) KernelTimer ktimer_(name, stream)
 
 // ---------------------------------------------------------------------------
 // staged face loops (kernels_staged.cuh): stage-ring depth, stage
@@ -92,11 +134,12 @@ StagedArgs staged_args(const cupcfd_gpu_mesh *m, bool forward) {
     return a;
 }
 
-// Builds the per-tile ranges and sizes the staged launches; leaves
-// m->staged false (unstaged kernels only) when the mesh does not allow it.
+// Builds the per-tile ranges (used by the L2-prefetch kernels of both
+// precisions) and sizes the FP32 shared-memory staged launches; leaves
+// m->staged false (plain kernels only) when the mesh does not allow it.
 int staged_setup(cupcfd_gpu_mesh *m, cudaStream_t st) {
     m->staged = false;
-    if (!(m->precisions & (1 << CUPCFD_PREC_F32C)) || m->nF < 1 || m->nC < 1) return CUPCFD_E_SUCCESS;
+    if (m->nF < 1 || m->nC < 1) return CUPCFD_E_SUCCESS;
     const char *env = std::getenv("CUPCFD_STAGED");
     if (env && std::strcmp(env, "0") == 0) return CUPCFD_E_SUCCESS;
     m->nTiles = (int) grid_for(m->nC, STAGED_TILE);
@@ -128,27 +171,33 @@ int staged_setup(cupcfd_gpu_mesh *m, cudaStream_t st) {
     CG_CHECK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     CG_CHECK_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     const void *kern[2] = {(const void *) k_fwd_f32_staged<STAGES>, (const void *) k_adj_f32_staged<STAGES>};
-    for (int i = 0; i < 2; i++) {
+    bool smemOk = (m->precisions & (1 << CUPCFD_PREC_F32C)) != 0;
+    for (int i = 0; i < 2 && smemOk; i++) {
         int smem = staged_smem(staged_layout(m, i == 0));
         cudaFuncAttributes fa;
         CG_CHECK_CUDA(cudaFuncGetAttributes(&fa, kern[i]));
-        if (smem + (int) fa.sharedSizeBytes > optin) return CUPCFD_E_SUCCESS;
-        CG_CHECK_CUDA(cudaFuncSetAttribute(kern[i], cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           optin - (int) fa.sharedSizeBytes));
         int nb = 0;
-        CG_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern[i], STAGED_TILE, smem));
-        if (nb < 1) return CUPCFD_E_SUCCESS;
-        m->stagedGrid[i] = std::min(m->nTiles, sms * nb);
-        m->stagedSmem[i] = smem;
+        if (smem + (int) fa.sharedSizeBytes <= optin) {
+            CG_CHECK_CUDA(cudaFuncSetAttribute(kern[i], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               optin - (int) fa.sharedSizeBytes));
+            CG_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern[i], STAGED_TILE, smem));
+        }
+        smemOk = nb >= 1;
+        m->stagedGrid[i] = smemOk ? std::min(m->nTiles, sms * nb) : 0;
+        m->stagedSmem[i] = smemOk ? smem : 0;
     }
+    if (!smemOk) m->stagedGrid[0] = m->stagedGrid[1] = m->stagedSmem[0] = m->stagedSmem[1] = 0;
     // L2-prefetch variant: prefetch one wave of resident blocks ahead (the
     // block that will take this block's place), the best distance measured
     int nbPf = 0;
     CG_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nbPf, k_fwd_f32_pf, STAGED_TILE, 0));
     m->prefetchDist = sms * std::max(1, nbPf);
     if (const char *e = std::getenv("CUPCFD_PREFETCH_DIST")) if (*e) m->prefetchDist = std::max(1, std::atoi(e));
+    // 1: L2 prefetch (the default, fastest measured); 2: shared-memory stages
+    // (FP32 forward/adjoint, when they fit); CUPCFD_TILE_MODE overrides
     m->tileMode = 1;
     if (const char *e = std::getenv("CUPCFD_TILE_MODE")) if (*e) m->tileMode = std::atoi(e);
+    if (m->tileMode == 2 && m->stagedGrid[0] == 0) m->tileMode = 1;
     m->staged = m->tileMode != 0;
     return CUPCFD_E_SUCCESS;
 }
@@ -367,12 +416,14 @@ int launch_fused(cupcfd_gpu_mesh *m, int precision, const void *phi, const void 
         const double *vol = m->vol;
         void *args[] = {&nC, &k, &sv, (void *) &fg, (void *) &phi, (void *) &phiB, (void *) &vol, (void *) &state,
                         (void *) &gface, &grad, &massFlux, &phiBar, &phiBBar, &stateBar, &part, &ldc};
+        KTIMER("k_fused_f64", st);
         CG_CHECK_CUDA(cudaLaunchCooperativeKernel((const void *) k_fused_f64, grid, FUSED_TILE, args, 0, st));
     } else {
         const float4 *fg = m->fg32;
         const double *vol = m->vol;
         void *args[] = {&nC, &k, &sv, (void *) &fg, (void *) &phi, (void *) &phiB, (void *) &vol, (void *) &state,
                         (void *) &gface, &grad, &massFlux, &phiBar, &phiBBar, &stateBar, &part, &ldc};
+        KTIMER("k_fused_f32", st);
         CG_CHECK_CUDA(cudaLaunchCooperativeKernel((const void *) k_fused_f32, grid, FUSED_TILE, args, 0, st));
     }
     CG_LAUNCHED();
@@ -542,23 +593,47 @@ namespace {
 // FP32 forward: the staged kernel when the mesh and the pointers allow it
 // (identical results), else the unstaged one. One launch either way; the
 // caller checks it. part: per-256-cell loss partials, or null.
-void launch_fwd_f32(const cupcfd_gpu_mesh *m, const void *phi, const void *phiB, const void *state, const void *gface,
-                    void *grad, void *massFlux, double *part, cudaStream_t st) {
+const char *launch_fwd_f32(const cupcfd_gpu_mesh *m, const void *phi, const void *phiB, const void *state,
+                           const void *gface, void *grad, void *massFlux, double *part, cudaStream_t st) {
     bool tiles = m->staged && aligned16(phi) && aligned16(state) && (!gface || aligned16(gface));
-    if (tiles && m->tileMode == 1)
+    if (tiles && m->tileMode == 1) {
         k_fwd_f32_pf<<<grid_for(m->nC, BLK), BLK, 0, st>>>(m->nC, sell(m), m->fg32, (const float *) phi,
                                                           (const float *) phiB, m->vol, (const float4 *) state,
                                                           (const float *) gface, (float *) grad, (float *) massFlux,
                                                           part, m->nC, prefetch_args(m));
-    else if (tiles)
+        return "k_fwd_f32_pf";
+    }
+    if (tiles && m->stagedGrid[0] > 0) {
         k_fwd_f32_staged<STAGES><<<m->stagedGrid[0], STAGED_TILE, m->stagedSmem[0], st>>>(
             staged_args(m, true), m->fg32, (const float *) phi, (const float *) phiB, m->vol, (const float4 *) state,
             (const float *) gface, (float *) grad, (float *) massFlux, part, m->nC);
-    else
-        k_fwd_f32<BLK><<<grid_for(m->nC, BLK), BLK, 0, st>>>(m->nC, sell(m), m->fg32, (const float *) phi,
-                                                             (const float *) phiB, m->vol, (const float4 *) state,
-                                                             (const float *) gface, (float *) grad, (float *) massFlux,
-                                                             part, m->nC);
+        return "k_fwd_f32_staged";
+    }
+    k_fwd_f32<BLK><<<grid_for(m->nC, BLK), BLK, 0, st>>>(m->nC, sell(m), m->fg32, (const float *) phi,
+                                                         (const float *) phiB, m->vol, (const float4 *) state,
+                                                         (const float *) gface, (float *) grad, (float *) massFlux,
+                                                         part, m->nC);
+    return "k_fwd_f32";
+}
+
+// FP64 forward: the L2-prefetch kernel when the tile ranges exist and the
+// arrays allow whole 16-byte ranges (state blocks of an even cell count),
+// else the plain one. Identical results.
+const char *launch_fwd_f64(const cupcfd_gpu_mesh *m, const void *phi, const void *phiB, const void *state,
+                           const void *gface, void *grad, void *massFlux, double *part, cudaStream_t st) {
+    if (m->staged && m->tileMode == 1 && aligned16(phi) && aligned16(state) && (!gface || aligned16(gface)) &&
+        m->nC % 2 == 0) {
+        k_fwd_f64_pf<<<grid_for(m->nC, BLK), BLK, 0, st>>>(m->nC, sell(m), m->fg64, (const double *) phi,
+                                                          (const double *) phiB, m->vol, (const double *) state,
+                                                          (const double *) gface, (double *) grad, (double *) massFlux,
+                                                          part, m->nC, prefetch_args(m));
+        return "k_fwd_f64_pf";
+    }
+    k_fwd_f64<BLK><<<grid_for(m->nC, BLK), BLK, 0, st>>>(m->nC, sell(m), m->fg64, (const double *) phi,
+                                                         (const double *) phiB, m->vol, (const double *) state,
+                                                         (const double *) gface, (double *) grad, (double *) massFlux,
+                                                         part, m->nC);
+    return "k_fwd_f64";
 }
 }  // namespace
 
@@ -576,14 +651,14 @@ extern "C" int cupcfd_gpu_dev_forward(cupcfd_gpu_mesh *m, int32_t precision, con
     unsigned grid = grid_for(m->nC, BLK);
     double *part = nullptr;
     if (loss) CG_TRY(scratch(m, S_LOSS, grid, &part));
-    if (precision == CUPCFD_PREC_F64)
-        k_fwd_f64<BLK><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg64, (const double *) phi, (const double *) phiB,
-                                             m->vol, (const double *) state, (const double *) gface, (double *) grad,
-                                             (double *) massFlux, part, m->nC);
-    else
-        launch_fwd_f32(m, phi, phiB, state, gface, grad, massFlux, part, st);
-    CG_LAUNCHED();
+    {
+        KernelTimer kt(nullptr, st);
+        kt.set_name(precision == CUPCFD_PREC_F64 ? launch_fwd_f64(m, phi, phiB, state, gface, grad, massFlux, part, st)
+                                                 : launch_fwd_f32(m, phi, phiB, state, gface, grad, massFlux, part, st));
+        CG_LAUNCHED();
+    }
     if (loss) {
+        KTIMER("k_reduce_partials", st);
         k_reduce_partials<<<1, 1024, 0, st>>>((int) grid, part, loss);
         CG_LAUNCHED();
     }
@@ -599,20 +674,27 @@ extern "C" int cupcfd_gpu_dev_adjoint(cupcfd_gpu_mesh *m, int32_t precision, con
     CG_TRY(check_align(precision, {grad, gface, phiBar, phiBBar}, {state, stateBar}));
     cudaStream_t st = as_stream(stream);
     unsigned grid = grid_for(m->nC, BLK);
-    if (precision == CUPCFD_PREC_F64)
+    KernelTimer kt(nullptr, st);
+    if (precision == CUPCFD_PREC_F64) {
+        kt.set_name("k_adj_f64");
         k_adj_f64<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg64, (const double *) grad, 2.0, (const double *) state,
                                         (const double *) gface, (double *) phiBar, (double *) phiBBar, (double *) stateBar, m->nC);
-    else if (m->staged && m->tileMode == 1 && aligned16(grad) && aligned16(state) && aligned16(gface) && m->nC % 4 == 0)
+    } else if (m->staged && m->tileMode == 1 && aligned16(grad) && aligned16(state) && aligned16(gface) && m->nC % 4 == 0) {
+        kt.set_name("k_adj_f32_pf");
         k_adj_f32_pf<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg32, (const float *) grad, 2.f, (const float4 *) state,
                                            (const float *) gface, (float *) phiBar, (float *) phiBBar,
                                            (float4 *) stateBar, m->nC, prefetch_args(m));
-    else if (m->staged && aligned16(grad) && aligned16(state) && aligned16(gface) && m->nC % 4 == 0)
+    } else if (m->staged && m->stagedGrid[1] > 0 && aligned16(grad) && aligned16(state) && aligned16(gface) &&
+               m->nC % 4 == 0) {
+        kt.set_name("k_adj_f32_staged");
         k_adj_f32_staged<STAGES><<<m->stagedGrid[1], STAGED_TILE, m->stagedSmem[1], st>>>(
             staged_args(m, false), m->fg32, (const float *) grad, 2.f, (const float4 *) state, (const float *) gface,
             (float *) phiBar, (float *) phiBBar, (float4 *) stateBar, m->nC);
-    else
+    } else {
+        kt.set_name("k_adj_f32");
         k_adj_f32<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg32, (const float *) grad, 2.f, (const float4 *) state,
                                         (const float *) gface, (float *) phiBar, (float *) phiBBar, (float4 *) stateBar, m->nC);
+    }
     CG_LAUNCHED();
     return CUPCFD_E_SUCCESS;
 }
@@ -646,15 +728,24 @@ extern "C" int cupcfd_gpu_dev_forward_adjoint(cupcfd_gpu_mesh *m, int32_t precis
         double *part;
         CG_TRY(scratch(m, S_LOSS, grid, &part));
         PrefetchArgs pf = prefetch_args(m);
-        k_fwd_madj_f32_pf<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg32, (const float *) phi, (const float *) phiB,
+        {
+            KTIMER("k_fwd_madj_f32_pf", st);
+            k_fwd_madj_f32_pf<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg32, (const float *) phi, (const float *) phiB,
                                                 m->vol, (const float4 *) state, (const float *) gface, (float *) grad,
                                                 (float *) massFlux, (float4 *) stateBar, part, m->nC, pf);
-        CG_LAUNCHED();
-        k_reduce_partials<<<1, 1024, 0, st>>>((int) grid, part, lp);
-        CG_LAUNCHED();
-        k_gadj_f32_pf<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg32, (const float *) grad, 2.f, (float *) phiBar,
-                                            (float *) phiBBar, m->nC, pf);
-        CG_LAUNCHED();
+            CG_LAUNCHED();
+        }
+        {
+            KTIMER("k_reduce_partials", st);
+            k_reduce_partials<<<1, 1024, 0, st>>>((int) grid, part, lp);
+            CG_LAUNCHED();
+        }
+        {
+            KTIMER("k_gadj_f32_pf", st);
+            k_gadj_f32_pf<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg32, (const float *) grad, 2.f, (float *) phiBar,
+                                                (float *) phiBBar, m->nC, pf);
+            CG_LAUNCHED();
+        }
         return CUPCFD_E_SUCCESS;
     }
     CG_TRY(cupcfd_gpu_dev_forward(m, precision, phi, phiB, state, gface, grad, massFlux, lp, stream));
@@ -1093,9 +1184,7 @@ extern "C" int cupcfd_gpu_dev_forward_noalloc(cupcfd_gpu_mesh *m, int32_t precis
     }
     cudaStream_t st = as_stream(stream);
     if (precision == CUPCFD_PREC_F64)
-        k_fwd_f64<BLK><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg64, (const double *) phi, (const double *) phiB,
-                                             m->vol, (const double *) state, (const double *) gface, (double *) grad,
-                                             (double *) massFlux, part, m->nC);
+        launch_fwd_f64(m, phi, phiB, state, gface, grad, massFlux, part, st);
     else
         launch_fwd_f32(m, phi, phiB, state, gface, grad, massFlux, part, st);
     g_launches.fetch_add(1, std::memory_order_relaxed);
@@ -1105,5 +1194,53 @@ extern "C" int cupcfd_gpu_dev_forward_noalloc(cupcfd_gpu_mesh *m, int32_t precis
         g_launches.fetch_add(1, std::memory_order_relaxed);
         if (cudaGetLastError() != cudaSuccess) return CUPCFD_E_ERROR;
     }
+    return CUPCFD_E_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// device timers
+// ---------------------------------------------------------------------------
+extern "C" int cupcfd_gpu_timing_enable(int32_t on) {
+    clear_error();
+    g_timer_on.store(on != 0);
+    return CUPCFD_E_SUCCESS;
+}
+
+extern "C" int cupcfd_gpu_timing_read(int32_t capacity, char *names, int64_t *launches, double *ms, int32_t *count) {
+    clear_error();
+    CG_RETURN_IF(!count || (capacity > 0 && (!names || !launches || !ms)), CUPCFD_E_NULL_PTR, "timing_read: null argument");
+    std::vector<TimerRec> recs;
+    {
+        std::lock_guard<std::mutex> lk(g_timer_mu);
+        recs.swap(g_timer_recs);
+    }
+    std::map<std::string, std::pair<int64_t, double>> acc;
+    std::vector<std::string> order;
+    int dev0 = 0;
+    cudaGetDevice(&dev0);
+    int failed = 0;
+    for (const TimerRec &r : recs) {
+        float t = 0.f;
+        cudaSetDevice(r.device);
+        if (cudaEventSynchronize(r.b) != cudaSuccess || cudaEventElapsedTime(&t, r.a, r.b) != cudaSuccess) failed++;
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+        std::string nm = r.name ? r.name : "?";
+        if (!acc.count(nm)) order.push_back(nm);
+        acc[nm].first += 1;
+        acc[nm].second += t;
+    }
+    cudaSetDevice(dev0);
+    CG_RETURN_IF(failed, CUPCFD_E_ERROR, "timing_read: a recorded event could not be timed");
+    int n = 0;
+    for (const std::string &nm : order) {
+        if (n < capacity) {
+            std::snprintf(names + 64 * (size_t) n, 64, "%s", nm.c_str());
+            launches[n] = acc[nm].first;
+            ms[n] = acc[nm].second;
+        }
+        n++;
+    }
+    *count = n;
     return CUPCFD_E_SUCCESS;
 }

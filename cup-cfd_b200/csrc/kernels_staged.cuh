@@ -466,18 +466,22 @@ __device__ __forceinline__ int4 ranges_ready(const int4 *src) {
     return *src;
 }
 
-template <int NCELL>
+// Prefetches a tile's ranges: its entries, its owned faces' records (fgSize
+// bytes each) and gface values (widened to whole 16-byte units inside the
+// array), and, when the tile is whole, the cell arrays (cellBytes per tile).
+template <int NCELL, class TG>
 __device__ __forceinline__ void prefetch_tile(const PrefetchArgs &p, int t, const int4 &d, const void *fg,
-                                              int fgSize, const float *gface, const void *const (&cellSrc)[NCELL],
+                                              int fgSize, const TG *gface, const void *const (&cellSrc)[NCELL],
                                               const int (&cellBytes)[NCELL]) {
+    constexpr int PER16 = 16 / (int) sizeof(TG);
     const int entStart = d.x, entEnd = d.y, fs = d.z, fe = d.w;
     if (entEnd > entStart) bulk_prefetch_l2(p.inc + entStart, (unsigned) (entEnd - entStart) * 8u);
     if (fe > fs)
         bulk_prefetch_l2(static_cast<const unsigned char *>(fg) + (size_t) fs * fgSize, (unsigned) (fe - fs) * (unsigned) fgSize);
     if (gface) {
-        int gfA = fs & ~3, gfB = (fe + 3) & ~3;
-        if (gfB > p.nF) gfB = fe & ~3;
-        if (gfB > gfA) bulk_prefetch_l2(gface + gfA, (unsigned) (gfB - gfA) * 4u);
+        int gfA = fs & ~(PER16 - 1), gfB = (fe + PER16 - 1) & ~(PER16 - 1);
+        if (gfB > p.nF) gfB = fe & ~(PER16 - 1);
+        if (gfB > gfA) bulk_prefetch_l2(gface + gfA, (unsigned) (gfB - gfA) * (unsigned) sizeof(TG));
     }
     if ((long long) (t + 1) * STAGED_TILE <= (long long) p.nC)
         for (int i = 0; i < NCELL; i++)
@@ -518,6 +522,27 @@ __global__ void __launch_bounds__(STAGED_TILE, CUPCFD_MINB_F32)
     if (lead) fetch_ranges_async(&s_rng, pf.desc + tp);
     if (c < nC) adj_cell_f32<false>(c, sv, fg, g, hscale, st, gface, phibar, phibBar, stbar, ldc);
     if (lead) prefetch_tile<4>(pf, tp, ranges_ready(&s_rng), fg, 16, gface, cellSrc, cellBytes);
+}
+
+// FP64 forward (fwd_cell_f64, exact reference arithmetic) with the same L2
+// prefetch; the state's four component blocks are prefetched one by one.
+__global__ void __launch_bounds__(STAGED_TILE, CUPCFD_MINB_FWD_F64)
+    k_fwd_f64_pf(int nC, SellView sv, const double4 *__restrict__ fg, const double *__restrict__ phi,
+                 const double *__restrict__ phiB, const double *__restrict__ vol, const double *__restrict__ st,
+                 const double *__restrict__ gface, double *__restrict__ g, double *__restrict__ mflux,
+                 double *__restrict__ lossPart, int64_t ldc, PrefetchArgs pf) {
+    constexpr int T = STAGED_TILE;
+    int c = blockIdx.x * T + threadIdx.x;
+    const int tp = blockIdx.x + pf.dist;
+    const bool lead = threadIdx.x == T - 32 && tp < pf.nTiles;
+    __shared__ int4 s_rng;
+    const void *const cellSrc[6] = {phi, vol, st, st + ldc, st + 2 * ldc, st + 3 * ldc};
+    const int cellBytes[6] = {T * 8, T * 8, T * 8, T * 8, T * 8, T * 8};
+    if (lead) fetch_ranges_async(&s_rng, pf.desc + tp);
+    double l = 0.0;
+    if (c < nC) l = fwd_cell_f64<CUPCFD_FWD_CHUNK_F64>(c, sv, fg, phi, phiB, vol, st, gface, g, mflux, ldc);
+    if (lead) prefetch_tile<6>(pf, tp, ranges_ready(&s_rng), fg, 32, gface, cellSrc, cellBytes);
+    if (lossPart) block_sum_store<T>(l, lossPart);
 }
 
 // Forward with the mass-flux adjoint (fwd_madj_cell_f32), L2 prefetch as
@@ -562,7 +587,7 @@ __global__ void __launch_bounds__(STAGED_TILE, CUPCFD_MINB_F32)
     const int cellBytes[3] = {T * 4, T * 4, T * 4};
     if (lead) fetch_ranges_async(&s_rng, pf.desc + tp);
     if (c < nC) adj_cell_f32<false>(c, sv, fg, g, hscale, nullptr, nullptr, phibar, phibBar, nullptr, ldc);
-    if (lead) prefetch_tile<3>(pf, tp, ranges_ready(&s_rng), fg, 16, nullptr, cellSrc, cellBytes);
+    if (lead) prefetch_tile<3>(pf, tp, ranges_ready(&s_rng), fg, 16, (const float *) nullptr, cellSrc, cellBytes);
 }
 
 // ---------------------------------------------------------------------------

@@ -341,6 +341,18 @@ int cupcfd_gpu_dev_error_norms(const void *a, int32_t a_size, const void *b, int
 /* Number of kernels this library launched since load (all threads). */
 int64_t cupcfd_gpu_launch_count(void);
 
+/* Device timers for measurement (no counterpart in the reference, whose
+ * benchmarks time whole calls on the host): while enabled, every kernel
+ * launch of the cupcfd_gpu_dev_forward / _adjoint / _forward_adjoint calls
+ * is bracketed by two CUDA events on the stream it is launched on.
+ * cupcfd_gpu_timing_read waits for the recorded events and returns, for up
+ * to `capacity` kernels, the kernel name (NUL-terminated, at most 63
+ * characters, in names[64 * i]), its launch count and its summed device
+ * milliseconds since the previous read; *count receives the number of
+ * kernels. Reading clears the record. Disabled by default. */
+int cupcfd_gpu_timing_enable(int32_t on);
+int cupcfd_gpu_timing_read(int32_t capacity, char *names, int64_t *launches, double *ms, int32_t *count);
+
 #ifdef __cplusplus
 }
 #endif

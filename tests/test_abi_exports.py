@@ -87,3 +87,16 @@ def test_binding_arity_matches_header(cg):
     assert set(ar) == set(cg.SIGNATURES)
     bad = {n: (len(cg.SIGNATURES[n][0]), k) for n, k in ar.items() if len(cg.SIGNATURES[n][0]) != k}
     assert not bad, bad
+
+
+def test_device_timers_without_gpu(cg):
+    """Timers off by default; enabling and reading with nothing recorded
+    needs no GPU and reports no kernels."""
+    import ctypes as C
+    L = cg.lib()
+    assert L.cupcfd_gpu_timing_read(0, None, None, None, None) == cg.E_NULL_PTR
+    cg.timing_enable(True)
+    assert cg.timing_read() == {}
+    cg.timing_enable(False)
+    n = C.c_int32(-1)
+    assert L.cupcfd_gpu_timing_read(0, None, None, None, C.byref(n)) == cg.E_SUCCESS and n.value == 0

@@ -178,3 +178,57 @@ def test_forward_adjoint_pipeline_equals_separate_calls(cg, gpu, kind, dims, ord
     ref = _run(cg, torch, mesh, *fields, offset=False)
     _assert_same(_run_pipeline(cg, torch, mesh, *fields, offset=False), ref)
     _assert_same(_run_pipeline(cg, torch, mesh, *fields, offset=True), ref)
+
+
+def test_device_timers_name_the_pipeline_kernels(cg, gpu):
+    """cupcfd_gpu_timing_*: the forward+adjoint call's three launches, each
+    timed on its stream, counted per kernel, and cleared by the read."""
+    import torch
+    mesh = cg.Mesh.structgen(32, 32, 32, order=cg.ORDER_OWNER)
+    fields = _fields(torch, mesh, 2)
+    cg.timing_read()
+    cg.timing_enable(True)
+    try:
+        for _ in range(3):
+            _run_pipeline(cg, torch, mesh, *fields, offset=False)
+        t = cg.timing_read()
+    finally:
+        cg.timing_enable(False)
+    assert {k: v[0] for k, v in t.items()} == {"k_fwd_madj_f32_pf": 3, "k_reduce_partials": 3, "k_gadj_f32_pf": 3}
+    assert all(v[1] > 0 for v in t.values())
+    assert cg.timing_read() == {}
+
+
+def test_fp64_forward_prefetch_equals_plain(cg, gpu):
+    """The FP64 forward with the L2 prefetch (16-byte-aligned arrays) and the
+    plain one (phi offset by one double) give bit-identical results."""
+    import torch
+    mesh = cg.Mesh.structgen(24, 20, 18, order=cg.ORDER_OWNER)
+    dev = torch.device("cuda:0")
+    g = torch.Generator(device=dev)
+    g.manual_seed(4)
+    nC, nF, nB = mesh.nCells, mesh.nFaces, mesh.nBoundaries
+    phi = torch.rand(nC, generator=g, device=dev, dtype=torch.float64) * 2 - 1
+    phiB = torch.rand(nB, generator=g, device=dev, dtype=torch.float64) * 2 - 1
+    st = torch.randn(4, nC, generator=g, device=dev, dtype=torch.float64)
+    gface = torch.randn(nF, generator=g, device=dev, dtype=torch.float64)
+    buf = torch.empty(nC + 2, dtype=torch.float64, device=dev)
+    phi_off = buf[1:1 + nC]
+    phi_off.copy_(phi)
+    assert phi_off.data_ptr() % 16 == 8
+    out = []
+    for p in (phi, phi_off):
+        gr = torch.full((3, nC), float("nan"), dtype=torch.float64, device=dev)
+        mf = torch.zeros(nF, dtype=torch.float64, device=dev)
+        loss = torch.zeros(1, dtype=torch.float64, device=dev)
+        cg.timing_enable(True)
+        try:
+            cg.dev_forward(mesh, cg.PREC_F64, p, phiB, st, gr, mf, gface=gface, loss=loss,
+                           stream=torch.cuda.current_stream())
+            names = set(cg.timing_read())
+        finally:
+            cg.timing_enable(False)
+        out.append((gr, mf, loss, names))
+    assert "k_fwd_f64_pf" in out[0][3] and "k_fwd_f64" in out[1][3]
+    for a, b in zip(out[0][:3], out[1][:3]):
+        assert torch.equal(a, b)
