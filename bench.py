@@ -361,12 +361,27 @@ def run_gpu(a):
     torch.cuda.synchronize()
     ms64 = e0.elapsed_time(e1) / K64
 
-    # ---- FP32-compensated vs FP64 on the same inputs (forward + adjoint)
+    # ---- the same forward + adjoint in FP64 (same work as the FP32 step)
     gf64 = gface.double()
     pbar64 = torch.empty(nC, dtype=torch.float64, device=dev)
     pbbar64 = torch.empty(nB, dtype=torch.float64, device=dev)
     sbar64 = torch.empty(4, nC, dtype=torch.float64, device=dev)
     loss64 = torch.zeros(1, dtype=torch.float64, device=dev)
+
+    def step64():
+        cg.dev_forward_adjoint(mesh, cg.PREC_F64, phi64, phiB64, st64, gf64, grad64, mf64, pbar64, pbbar64, sbar64,
+                               loss64, stream=st)
+
+    for _ in range(3):
+        step64()
+    e0.record(st)
+    for _ in range(K64):
+        step64()
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms64fa = e0.elapsed_time(e1) / K64
+
+    # ---- FP32-compensated vs FP64 on the same inputs (forward + adjoint)
     cg.dev_forward(mesh, cg.PREC_F64, phi64, phiB64, st64, grad64, mf64, gface=gf64, loss=loss64, stream=st)
     cg.dev_adjoint(mesh, cg.PREC_F64, grad64, st64, gf64, pbar64, pbbar64, sbar64, stream=st)
     step()
@@ -471,6 +486,8 @@ def run_gpu(a):
             "fp64_plain_forward": {"value": world * nF / (ms64 * 1e-3) / 1e9, "unit": "Gfaces/s", "ms_per_step": ms64,
                                    "gbs": bm["fwd_f64"] / (ms64 * 1e-3) / 1e9,
                                    "frac": bm["fwd_f64"] / (ms64 * 1e-3) / 1e9 / peak},
+            "fp64_forward_adjoint": {"value": world * nF / (ms64fa * 1e-3) / 1e9, "unit": "Gfaces/s",
+                                     "ms_per_step": ms64fa},
             "error_vs_fp64": errors,
             "e2e": e2e,
             "cpu_baseline": cpu,

@@ -675,7 +675,13 @@ extern "C" int cupcfd_gpu_dev_adjoint(cupcfd_gpu_mesh *m, int32_t precision, con
     cudaStream_t st = as_stream(stream);
     unsigned grid = grid_for(m->nC, BLK);
     KernelTimer kt(nullptr, st);
-    if (precision == CUPCFD_PREC_F64) {
+    if (precision == CUPCFD_PREC_F64 && m->staged && m->tileMode == 1 && aligned16(grad) && aligned16(state) &&
+        aligned16(gface) && m->nC % 2 == 0) {
+        kt.set_name("k_adj_f64_pf");
+        k_adj_f64_pf<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg64, (const double *) grad, 2.0, (const double *) state,
+                                           (const double *) gface, (double *) phiBar, (double *) phiBBar,
+                                           (double *) stateBar, m->nC, prefetch_args(m));
+    } else if (precision == CUPCFD_PREC_F64) {
         kt.set_name("k_adj_f64");
         k_adj_f64<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg64, (const double *) grad, 2.0, (const double *) state,
                                         (const double *) gface, (double *) phiBar, (double *) phiBBar, (double *) stateBar, m->nC);

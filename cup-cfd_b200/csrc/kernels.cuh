@@ -124,6 +124,12 @@ __device__ __forceinline__ void load_entries(const int2 *e, int k0, int w, int2 
 #ifndef CUPCFD_MINB_FWD_F64
 #define CUPCFD_MINB_FWD_F64 3
 #endif
+#ifndef CUPCFD_ADJ_CHUNK_F64
+#define CUPCFD_ADJ_CHUNK_F64 1
+#endif
+#ifndef CUPCFD_MINB_ADJ_F64
+#define CUPCFD_MINB_ADJ_F64 4
+#endif
 #ifndef CUPCFD_MINB_FUSED_F32
 #define CUPCFD_MINB_FUSED_F32 4
 #endif

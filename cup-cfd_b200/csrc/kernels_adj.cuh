@@ -79,7 +79,7 @@ __device__ __forceinline__ double fwd_cell_f64(int c, const SellView &sv, const 
                     double wF = da(dm(so[j][3], facn), dm(w0, facp));
                     double m = dm(denf, da(da(dm(uF, G[j].x), dm(vF, G[j].y)), dm(wF, G[j].z)));
                     mflux[code >> 1] = m;
-                    lsum += gf[j] * m;
+                    lsum = __fma_rn(gf[j], m, lsum);
                 }
             }
             ax = da(ax, dm(phif, G[j].x)); ay = da(ay, dm(phif, G[j].y)); az = da(az, dm(phif, G[j].z));
@@ -89,7 +89,7 @@ __device__ __forceinline__ double fwd_cell_f64(int c, const SellView &sv, const 
     double fact = dvd(1.0, V);
     ax = dm(ax, fact); ay = dm(ay, fact); az = dm(az, fact);
     g[c] = ax; g[ldc + c] = ay; g[2 * ldc + c] = az;
-    return lsum + V * (ax * ax + ay * ay + az * az);
+    return __fma_rn(V, __fma_rn(ax, ax, __fma_rn(ay, ay, __dmul_rn(az, az))), lsum);
 }
 
 // Per-cell body of the FP32 fused forward; state as float4 {rho, u, v, w}.
@@ -141,7 +141,7 @@ __device__ __forceinline__ double fwd_cell_f32(int c, const SellView &sv, const 
                     float wF = fmaf(facn, so[j].w, facp * sc.w);
                     float m = denf * fmaf(uF, G[j].x, fmaf(vF, G[j].y, wF * G[j].z));
                     mflux[code >> 1] = m;
-                    lsum += (double) gf[j] * (double) m;
+                    lsum = __fma_rn((double) gf[j], (double) m, lsum);
                 }
             }
             ax.add_prod(phif, G[j].x); ay.add_prod(phif, G[j].y); az.add_prod(phif, G[j].z);
@@ -151,7 +151,8 @@ __device__ __forceinline__ double fwd_cell_f32(int c, const SellView &sv, const 
     double fact = 1.0 / V;
     float rx = (float) (ax.value() * fact), ry = (float) (ay.value() * fact), rz = (float) (az.value() * fact);
     g[c] = rx; g[ldc + c] = ry; g[2 * ldc + c] = rz;
-    return lsum + V * ((double) rx * rx + (double) ry * ry + (double) rz * rz);
+    return __fma_rn(V, __fma_rn((double) rx, (double) rx, __fma_rn((double) ry, (double) ry, __dmul_rn((double) rz, (double) rz))),
+                    lsum);
 }
 
 // Per-cell body of the FP32 forward that also runs the mass-flux part of
@@ -208,7 +209,7 @@ __device__ __forceinline__ double fwd_madj_cell_f32(int c, const SellView &sv, c
                     float wF = fmaf(facn, so[j].w, facp * sc.w);
                     float m = denf * fmaf(uF, G[j].x, fmaf(vF, G[j].y, wF * G[j].z));
                     mflux[code >> 1] = m;
-                    lsum += (double) gf[j] * (double) m;
+                    lsum = __fma_rn((double) gf[j], (double) m, lsum);
                 }
                 // mass part of the adjoint (adj_cell_f32)
                 float wc = isN ? facn : facp, wo = isN ? facp : facn;
@@ -227,7 +228,8 @@ __device__ __forceinline__ double fwd_madj_cell_f32(int c, const SellView &sv, c
     float rx = (float) (ax.value() * fact), ry = (float) (ay.value() * fact), rz = (float) (az.value() * fact);
     g[c] = rx; g[ldc + c] = ry; g[2 * ldc + c] = rz;
     stbar[c] = make_float4((float) rb.value(), (float) ub.value(), (float) vb.value(), (float) wb.value());
-    return lsum + V * ((double) rx * rx + (double) ry * ry + (double) rz * rz);
+    return __fma_rn(V, __fma_rn((double) rx, (double) rx, __fma_rn((double) ry, (double) ry, __dmul_rn((double) rz, (double) rz))),
+                    lsum);
 }
 
 // ---------------------------------------------------------------------------
@@ -290,7 +292,7 @@ __device__ __forceinline__ float ldg_g(const float *p) { return LDCG ? __ldcg(p)
 template <bool LDCG>
 __device__ __forceinline__ double ldg_g(const double *p) { return LDCG ? __ldcg(p) : __ldg(p); }
 
-template <bool LDCG, int CH = CUPCFD_ADJ_CHUNK>
+template <bool LDCG, int CH = CUPCFD_ADJ_CHUNK_F64>
 __device__ __forceinline__ void adj_cell_f64(int c, const SellView &sv, const double4 *__restrict__ fg,
                                              const double *g, double hscale, const double *__restrict__ st,
                                              const double *__restrict__ gface, double *__restrict__ phibar,
@@ -328,22 +330,26 @@ __device__ __forceinline__ void adj_cell_f64(int c, const SellView &sv, const do
             if (code < 0) continue;
             int o = en[j].y;
             if (o < 0) {
-                if (doG) phibBar[-1 - o] = hx * G[j].x + hy * G[j].y + hz * G[j].z;
+                if (doG) phibBar[-1 - o] = __fma_rn(hx, G[j].x, __fma_rn(hy, G[j].y, __dmul_rn(hz, G[j].z)));
                 continue;
             }
             bool isN = code & 1;
             double facn = G[j].w, facp = 1.0 - facn;
             double wc = isN ? facn : facp, wo = isN ? facp : facn;
             if (doG)
-                pb += wc * ((hx + hscale * go[j][0]) * G[j].x + (hy + hscale * go[j][1]) * G[j].y +
-                            (hz + hscale * go[j][2]) * G[j].z);
+                pb = __fma_rn(wc, __fma_rn(__fma_rn(hscale, go[j][0], hx), G[j].x,
+                                           __fma_rn(__fma_rn(hscale, go[j][1], hy), G[j].y,
+                                                    __dmul_rn(__fma_rn(hscale, go[j][2], hz), G[j].z))),
+                              pb);
             if (doM) {
-                double denf = wc * r0 + wo * so[j][0];
-                double uF = wc * u0 + wo * so[j][1], vF = wc * v0 + wo * so[j][2], wF = wc * w0 + wo * so[j][3];
-                double a = wc * gf[j];
-                rb += a * (uF * G[j].x + vF * G[j].y + wF * G[j].z);
-                double b = a * denf;
-                ub += b * G[j].x; vb += b * G[j].y; wb += b * G[j].z;
+                double denf = __fma_rn(wc, r0, __dmul_rn(wo, so[j][0]));
+                double uF = __fma_rn(wc, u0, __dmul_rn(wo, so[j][1]));
+                double vF = __fma_rn(wc, v0, __dmul_rn(wo, so[j][2]));
+                double wF = __fma_rn(wc, w0, __dmul_rn(wo, so[j][3]));
+                double a = __dmul_rn(wc, gf[j]);
+                rb = __fma_rn(a, __fma_rn(uF, G[j].x, __fma_rn(vF, G[j].y, __dmul_rn(wF, G[j].z))), rb);
+                double b = __dmul_rn(a, denf);
+                ub = __fma_rn(b, G[j].x, ub); vb = __fma_rn(b, G[j].y, vb); wb = __fma_rn(b, G[j].z, wb);
             }
         }
     }
@@ -409,7 +415,7 @@ __device__ __forceinline__ void adj_cell_f32(int c, const SellView &sv, const fl
     if (doM) stbar[c] = make_float4((float) rb.value(), (float) ub.value(), (float) vb.value(), (float) wb.value());
 }
 
-__global__ void __launch_bounds__(256, CUPCFD_MINB_F64) k_adj_f64(int nC, SellView sv, const double4 *__restrict__ fg,
+__global__ void __launch_bounds__(256, CUPCFD_MINB_ADJ_F64) k_adj_f64(int nC, SellView sv, const double4 *__restrict__ fg,
                                                  const double *__restrict__ g, double hscale, const double *__restrict__ st,
                                                  const double *__restrict__ gface, double *__restrict__ phibar,
                                                  double *__restrict__ phibBar, double *__restrict__ stbar, int64_t ldc) {

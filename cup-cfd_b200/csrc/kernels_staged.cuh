@@ -545,6 +545,23 @@ __global__ void __launch_bounds__(STAGED_TILE, CUPCFD_MINB_FWD_F64)
     if (lossPart) block_sum_store<T>(l, lossPart);
 }
 
+// FP64 adjoint (adj_cell_f64) with the same L2 prefetch.
+__global__ void __launch_bounds__(STAGED_TILE, CUPCFD_MINB_ADJ_F64)
+    k_adj_f64_pf(int nC, SellView sv, const double4 *__restrict__ fg, const double *__restrict__ g, double hscale,
+                 const double *__restrict__ st, const double *__restrict__ gface, double *__restrict__ phibar,
+                 double *__restrict__ phibBar, double *__restrict__ stbar, int64_t ldc, PrefetchArgs pf) {
+    constexpr int T = STAGED_TILE;
+    int c = blockIdx.x * T + threadIdx.x;
+    const int tp = blockIdx.x + pf.dist;
+    const bool lead = threadIdx.x == T - 32 && tp < pf.nTiles;
+    __shared__ int4 s_rng;
+    const void *const cellSrc[7] = {g, g + ldc, g + 2 * ldc, st, st + ldc, st + 2 * ldc, st + 3 * ldc};
+    const int cellBytes[7] = {T * 8, T * 8, T * 8, T * 8, T * 8, T * 8, T * 8};
+    if (lead) fetch_ranges_async(&s_rng, pf.desc + tp);
+    if (c < nC) adj_cell_f64<false>(c, sv, fg, g, hscale, st, gface, phibar, phibBar, stbar, ldc);
+    if (lead) prefetch_tile<7>(pf, tp, ranges_ready(&s_rng), fg, 32, gface, cellSrc, cellBytes);
+}
+
 // Forward with the mass-flux adjoint (fwd_madj_cell_f32), L2 prefetch as
 // k_fwd_f32_pf. With k_gadj_f32_pf it forms the two-launch forward+adjoint:
 // the state and gface are then read by one pass only.

@@ -200,8 +200,9 @@ def test_device_timers_name_the_pipeline_kernels(cg, gpu):
 
 
 def test_fp64_forward_prefetch_equals_plain(cg, gpu):
-    """The FP64 forward with the L2 prefetch (16-byte-aligned arrays) and the
-    plain one (phi offset by one double) give bit-identical results."""
+    """The FP64 forward and adjoint with the L2 prefetch (16-byte-aligned
+    arrays) and the plain ones (phi and the gradient offset by one double)
+    give bit-identical results."""
     import torch
     mesh = cg.Mesh.structgen(24, 20, 18, order=cg.ORDER_OWNER)
     dev = torch.device("cuda:0")
@@ -216,19 +217,24 @@ def test_fp64_forward_prefetch_equals_plain(cg, gpu):
     phi_off = buf[1:1 + nC]
     phi_off.copy_(phi)
     assert phi_off.data_ptr() % 16 == 8
+    gbuf = torch.empty(3 * nC + 2, dtype=torch.float64, device=dev)
     out = []
-    for p in (phi, phi_off):
-        gr = torch.full((3, nC), float("nan"), dtype=torch.float64, device=dev)
+    for p, gr in ((phi, torch.empty(3, nC, dtype=torch.float64, device=dev)), (phi_off, gbuf[1:1 + 3 * nC].view(3, nC))):
+        gr.fill_(float("nan"))
         mf = torch.zeros(nF, dtype=torch.float64, device=dev)
         loss = torch.zeros(1, dtype=torch.float64, device=dev)
+        pb = torch.empty(nC, dtype=torch.float64, device=dev)
+        pbb = torch.empty(nB, dtype=torch.float64, device=dev)
+        sb = torch.empty(4, nC, dtype=torch.float64, device=dev)
         cg.timing_enable(True)
         try:
-            cg.dev_forward(mesh, cg.PREC_F64, p, phiB, st, gr, mf, gface=gface, loss=loss,
-                           stream=torch.cuda.current_stream())
+            s = torch.cuda.current_stream()
+            cg.dev_forward(mesh, cg.PREC_F64, p, phiB, st, gr, mf, gface=gface, loss=loss, stream=s)
+            cg.dev_adjoint(mesh, cg.PREC_F64, gr, st, gface, pb, pbb, sb, stream=s)
             names = set(cg.timing_read())
         finally:
             cg.timing_enable(False)
-        out.append((gr, mf, loss, names))
-    assert "k_fwd_f64_pf" in out[0][3] and "k_fwd_f64" in out[1][3]
-    for a, b in zip(out[0][:3], out[1][:3]):
+        out.append((gr.clone(), mf, loss, pb, pbb, sb, names))
+    assert {"k_fwd_f64_pf", "k_adj_f64_pf"} <= out[0][-1] and {"k_fwd_f64", "k_adj_f64"} <= out[1][-1]
+    for a, b in zip(out[0][:-1], out[1][:-1]):
         assert torch.equal(a, b)
