@@ -1,20 +1,23 @@
-"""Tile-path FP32 kernels against the plain ones: the shared-memory staged
-and the L2-prefetch forward/adjoint, and the two-launch forward+adjoint
-(forward with the mass-flux adjoint, then the gradient adjoint).
+"""The tile-path kernels against the plain ones, and the two incidence layouts.
 
-The staged kernels fetch each 256-cell tile's contiguous ranges (incidence
-entries, the tile's owned faces, cell arrays) into shared memory with bulk
-async copies and otherwise run the same per-cell arithmetic in the same face
-order, so results must be bit-identical. The library picks the staged kernels
-when the user arrays start on 16-byte boundaries; passing views offset by one
-float (4 bytes) makes it take the unstaged kernels on the same mesh and data.
+Every variant runs the same per-cell arithmetic in the same face order, so
+results must be bit-identical:
+  - the L2-prefetch kernels (the default when the user arrays start on
+    16-byte boundaries) against the plain kernels, which the same call runs
+    when phi, gface and the gradient are passed as views offset by one float;
+  - the shared-memory staged kernels (CUPCFD_TILE_MODE=2 at mesh creation),
+    including stage capacities lowered far below the tiles' needs so entries
+    and faces overflow to the global-memory path;
+  - the two-launch forward+adjoint (forward with the mass-flux adjoint, then
+    the gradient adjoint) against dev_forward + dev_adjoint.
+The device timers name the kernels each call ran, so every test checks that
+the variant it means to test is the one that ran.
 
 Cases: the Morton, owner and RCM numberings (the native one keeps the
-reference's face order, which is not by owner, and is never staged), a
-ragged last tile, an odd cell count (the
-adjoint's gradient blocks are then not 16-byte aligned, so only the forward
-is staged), a jittered mesh, and stage capacities lowered far below the
-tiles' needs so entries and faces overflow to the global-memory path.
+reference's face order, which is not by owner, and has no tile ranges), a
+ragged last tile, an odd cell count (the adjoint's gradient blocks are then
+not 16-byte aligned, so only the forward takes the tile path), a jittered
+mesh.
 """
 import os
 
@@ -59,10 +62,17 @@ def _run(cg, torch, mesh, phi, phiB, st, gface, offset):
     pbb = torch.full((max(nB, 1),), float("nan"), device=dev)
     sb = torch.full((nC, 4), float("nan"), device=dev)
     s = torch.cuda.current_stream()
-    cg.dev_forward(mesh, cg.PREC_F32C, phi, phiB, st, grad, mf, gface=gface, loss=loss, stream=s)
-    cg.dev_adjoint(mesh, cg.PREC_F32C, grad, st, gface, pb, pbb, sb, stream=s)
+    cg.timing_read()
+    cg.timing_enable(True)
+    try:
+        cg.dev_forward(mesh, cg.PREC_F32C, phi, phiB, st, grad, mf, gface=gface, loss=loss, stream=s)
+        cg.dev_adjoint(mesh, cg.PREC_F32C, grad, st, gface, pb, pbb, sb, stream=s)
+        ran = set(cg.timing_read())
+    finally:
+        cg.timing_enable(False)
     mesh.check_status()
     torch.cuda.synchronize()
+    _run.kernels = ran
     return [grad.clone(), mf, loss, pb, pbb, sb]
 
 
@@ -83,27 +93,57 @@ CASES = [
 ]
 
 
-@pytest.mark.parametrize("kind,dims,order", CASES)
-def test_staged_equals_unstaged(cg, gpu, kind, dims, order):
-    import torch
+def _mesh(cg, kind, dims, order):
     make = cg.Mesh.structgen if kind == "structgen" else cg.Mesh.jittered
-    mesh = make(*dims, order=getattr(cg, order))
+    return make(*dims, order=getattr(cg, order))
+
+
+@pytest.mark.parametrize("kind,dims,order", CASES)
+def test_prefetch_equals_plain(cg, gpu, kind, dims, order):
+    import torch
+    mesh = _mesh(cg, kind, dims, order)
+    fields = _fields(torch, mesh, 5)
+    a = _run(cg, torch, mesh, *fields, offset=False)
+    ka = _run.kernels
+    b = _run(cg, torch, mesh, *fields, offset=True)
+    assert "k_fwd_f32_pf" in ka and "k_fwd_f32" in _run.kernels
+    if mesh.nCells % 4 == 0:
+        assert "k_adj_f32_pf" in ka
+    _assert_same(a, b)
+
+
+@pytest.mark.parametrize("kind,dims,order", CASES)
+def test_staged_smem_equals_plain(cg, gpu, kind, dims, order, monkeypatch):
+    import torch
+    monkeypatch.setenv("CUPCFD_TILE_MODE", "2")
+    mesh = _mesh(cg, kind, dims, order)
     assert mesh.stagedCtas > 0 and mesh.stagedSmem > 0
     fields = _fields(torch, mesh, 5)
-    _assert_same(_run(cg, torch, mesh, *fields, offset=False), _run(cg, torch, mesh, *fields, offset=True))
+    a = _run(cg, torch, mesh, *fields, offset=False)
+    ka = _run.kernels
+    b = _run(cg, torch, mesh, *fields, offset=True)
+    assert "k_fwd_f32_staged" in ka and "k_fwd_f32" in _run.kernels
+    if mesh.nCells % 4 == 0:
+        assert "k_adj_f32_staged" in ka
+    _assert_same(a, b)
 
 
 def test_native_numbering_is_unstaged(cg, gpu):
     """ORDER_NATIVE keeps the reference's face numbering, which is not sorted
-    by owner tile, so the tile ranges do not exist and the mesh runs the
-    unstaged kernels."""
-    assert cg.Mesh.structgen(16, 12, 8, order=cg.ORDER_NATIVE).stagedCtas == 0
+    by owner, so there are no tile ranges and the mesh runs the plain
+    kernels."""
+    import torch
+    mesh = cg.Mesh.structgen(16, 12, 8, order=cg.ORDER_NATIVE)
+    assert mesh.stagedCtas == 0
+    _run(cg, torch, mesh, *_fields(torch, mesh, 1), offset=False)
+    assert _run.kernels == {"k_fwd_f32", "k_reduce_partials", "k_adj_f32"}
 
 
 def test_staged_overflow_to_global(cg, gpu, monkeypatch):
     """Stage buffers far smaller than a tile's ranges: the entries and faces
     beyond them are read from global memory, results unchanged."""
     import torch
+    monkeypatch.setenv("CUPCFD_TILE_MODE", "2")
     monkeypatch.setenv("CUPCFD_STAGED_ENT_CAP", "64")
     monkeypatch.setenv("CUPCFD_STAGED_FACE_CAP", "8")
     small = cg.Mesh.structgen(30, 20, 10, order=cg.ORDER_MORTON)
@@ -114,10 +154,11 @@ def test_staged_overflow_to_global(cg, gpu, monkeypatch):
     fields = _fields(torch, small, 9)
     ref = _run(cg, torch, full, *fields, offset=True)
     _assert_same(_run(cg, torch, small, *fields, offset=False), ref)
+    assert "k_fwd_f32_staged" in _run.kernels
     _assert_same(_run(cg, torch, full, *fields, offset=False), ref)
 
 
-def test_staging_can_be_disabled(cg, gpu, monkeypatch):
+def test_tile_path_can_be_disabled(cg, gpu, monkeypatch):
     import torch
     monkeypatch.setenv("CUPCFD_STAGED", "0")
     off = cg.Mesh.structgen(16, 16, 16, order=cg.ORDER_OWNER)
@@ -125,7 +166,10 @@ def test_staging_can_be_disabled(cg, gpu, monkeypatch):
     on = cg.Mesh.structgen(16, 16, 16, order=cg.ORDER_OWNER)
     assert off.stagedCtas == 0 and on.stagedCtas > 0
     fields = _fields(torch, on, 3)
-    _assert_same(_run(cg, torch, off, *fields, offset=False), _run(cg, torch, on, *fields, offset=False))
+    a = _run(cg, torch, off, *fields, offset=False)
+    assert _run.kernels == {"k_fwd_f32", "k_reduce_partials", "k_adj_f32"}
+    _assert_same(a, _run(cg, torch, on, *fields, offset=False))
+    assert "k_fwd_f32_pf" in _run.kernels
 
 
 def test_misaligned_state_is_rejected(cg, gpu):
