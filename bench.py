@@ -86,6 +86,22 @@ def bytes_model(nC, nF, nFi, nB):
     }
 
 
+def max_over_ranks(x, dist=None, device="cpu"):
+    """The largest x over all ranks (the job's time is its slowest rank's);
+    x itself when there is one rank."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_gfaces(world, faces_per_rank, seconds):
+    """Whole-job throughput: every rank runs its own mesh (weak scaling)."""
+    return world * faces_per_rank / seconds / 1e9
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
@@ -317,12 +333,9 @@ def run_gpu(a):
     if status != cg.E_SUCCESS:
         raise RuntimeError(f"forward+adjoint reported an error: {cg.last_error()}")
     total_ms = t_start.elapsed_time(t_end)
-    tmax = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    if dist:
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-    total_ms = float(tmax.item())
+    total_ms = max_over_ranks(total_ms, dist, dev)
     ms_step = total_ms / K
-    value = world * nF / (ms_step * 1e-3) / 1e9
+    value = job_gfaces(world, nF, ms_step * 1e-3)
 
     # ---- the same work as the separate dev_forward and dev_adjoint calls, for comparison
     e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
@@ -428,13 +441,10 @@ def run_gpu(a):
     for _ in range(K2):
         cg.forward_adjoint(*args_e2e, out=on)
     te = (time.perf_counter() - t0) / K2
-    temax = torch.tensor([te], dtype=torch.float64, device=dev)
-    if dist:
-        dist.all_reduce(temax, op=dist.ReduceOp.MAX)
-    te = float(temax.item())
+    te = max_over_ranks(te, dist, dev)
     h2d = 8 * (5 * nC + nB + nF)
     d2h = 8 * (3 * nC + nF + 5 * nC + nB + 1)
-    e2e = {"value": world * nF / te / 1e9, "unit": "Gfaces/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+    e2e = {"value": job_gfaces(world, nF, te), "unit": "Gfaces/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
            "ms_per_step": te * 1e3, "steps": K2,
            "call": "cupcfd_gpu_forward_adjoint (host FP64 buffers in reference numbering, pinned)"}
 
