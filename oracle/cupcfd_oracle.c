@@ -654,3 +654,132 @@ int orc_gradient_adjoint(const orc_mesh *m, const double *gbar, double *phibar, 
     }
     return ORC_E_SUCCESS;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Boundary / region loops (MassKernels.ipp:311-554).                       */
+/* The reference walks boundaries ib = 0 .. nBnd-1 and reaches each one's   */
+/* face through getBoundaryFaceID; here that map is faceBnd inverted.        */
+/* ------------------------------------------------------------------------ */
+static int *orc_boundary_faces(const orc_mesh *m) {
+    int *bf = (int *) malloc(sizeof(int) * (size_t) (m->nBnd > 0 ? m->nBnd : 1));
+    if (!bf) return NULL;
+    for (int b = 0; b < m->nBnd; b++) bf[b] = -1;
+    for (int f = 0; f < m->nFaces; f++)
+        if (m->faceBnd[f] > -1) bf[m->faceBnd[f]] = f;
+    return bf;
+}
+
+static int orc_btype(const orc_mesh *m, int ib) { return m->regionType[m->bndRegion[ib]]; }
+
+/* FluxMassDolfynBoundaryLoop1 (MassKernels.ipp:311-336): inlet mass inflow. */
+int orc_boundary_loop1(const orc_mesh *m, const double *massFlux, double *flowin) {
+    int *bf = orc_boundary_faces(m);
+    if (!bf) return ORC_E_ERROR;
+    *flowin = 0.0;
+    for (int ib = 0; ib < m->nBnd; ib++)
+        if (orc_btype(m, ib) == ORC_RTYPE_INLET) *flowin = *flowin + massFlux[bf[ib]];
+    free(bf);
+    return ORC_E_SUCCESS;
+}
+
+/* FluxMassDolfynBoundaryLoop2 (MassKernels.ipp:338-368): outlet outflow, in
+ * total and per region (flowRegion accumulates onto its input). */
+int orc_boundary_loop2(const orc_mesh *m, const double *massFlux, double *flowRegion, double *flowout) {
+    int *bf = orc_boundary_faces(m);
+    if (!bf) return ORC_E_ERROR;
+    *flowout = 0.0;
+    for (int ib = 0; ib < m->nBnd; ib++) {
+        int ir = m->bndRegion[ib];
+        if (m->regionType[ir] == ORC_RTYPE_OUTLET) {
+            int i = bf[ib];
+            *flowout = *flowout + massFlux[i];
+            flowRegion[ir] = flowRegion[ir] + massFlux[i];
+        }
+    }
+    free(bf);
+    return ORC_E_SUCCESS;
+}
+
+/* FluxMassDolfynBoundaryLoop3 (MassKernels.ipp:371-393): outlet area and the
+ * area rate -flowin / areaout. */
+int orc_boundary_loop3(const orc_mesh *m, double flowin, double *ratearea) {
+    int *bf = orc_boundary_faces(m);
+    if (!bf) return ORC_E_ERROR;
+    double areaout = 0.0;
+    for (int ib = 0; ib < m->nBnd; ib++)
+        if (orc_btype(m, ib) == ORC_RTYPE_OUTLET) areaout = areaout + m->faceArea[bf[ib]];
+    *ratearea = -flowin / areaout;
+    free(bf);
+    return ORC_E_SUCCESS;
+}
+
+/* FluxMassDolfynBoundaryLoop4 (MassKernels.ipp:395-454): outlet mass flux
+ * from the area rate, and the outlet velocities along the unit normal. */
+int orc_boundary_loop4(const orc_mesh *m, const double *splvl, double *massFlux, double *uB, double *vB, double *wB,
+                       const double *denB, double ratearea, double *flowout) {
+    int *bf = orc_boundary_faces(m);
+    if (!bf) return ORC_E_ERROR;
+    *flowout = 0.0;
+    for (int ib = 0; ib < m->nBnd; ib++) {
+        int ir = m->bndRegion[ib];
+        if (m->regionType[ir] != ORC_RTYPE_OUTLET) continue;
+        int i = bf[ib];
+        double split = splvl[ir];
+        double area = m->faceArea[i];
+        massFlux[i] = ratearea * area * split;
+        double faceFlux = massFlux[i] / denB[ib] / area;
+        /* EuclideanVector::normalise (EuclideanVector.cpp:100-109): length is
+         * sqrt of the dot product accumulated from 0 (EuclideanVector.cpp:83-98) */
+        double x[3] = {m->faceNorm[3 * i], m->faceNorm[3 * i + 1], m->faceNorm[3 * i + 2]};
+        double dot = 0.0;
+        for (int d = 0; d < 3; d++) dot += x[d] * x[d];
+        double scalar = sqrt(dot);
+        if (scalar != 0.0) {
+            scalar = 1.0 / scalar;
+            for (int d = 0; d < 3; d++) x[d] *= scalar;
+        }
+        uB[ib] = faceFlux * x[0];
+        vB[ib] = faceFlux * x[1];
+        wB[ib] = faceFlux * x[2];
+        *flowout = *flowout + massFlux[i];
+    }
+    free(bf);
+    return ORC_E_SUCCESS;
+}
+
+/* FluxMassDolfynBoundaryLoop5 (MassKernels.ipp:457-521): outlet mass flux
+ * scaled by its region's factor, accumulated onto *flowout2 (not reset),
+ * optional velocity scaling, and su[cell1] -= massFlux, boundary by boundary. */
+int orc_boundary_loop5(const orc_mesh *m, double *massFlux, double *su, double *uB, double *vB, double *wB, double fact,
+                       int solveU, int solveV, int solveW, const double *flowFact, double *flowout2) {
+    int *bf = orc_boundary_faces(m);
+    if (!bf) return ORC_E_ERROR;
+    for (int ib = 0; ib < m->nBnd; ib++) {
+        int ir = m->bndRegion[ib];
+        if (m->regionType[ir] != ORC_RTYPE_OUTLET) continue;
+        int i = bf[ib];
+        massFlux[i] = massFlux[i] * flowFact[ir];
+        *flowout2 = *flowout2 + massFlux[i];
+        if (solveU) uB[ib] = uB[ib] * fact;
+        if (solveV) vB[ib] = vB[ib] * fact;
+        if (solveW) wB[ib] = wB[ib] * fact;
+        int ip = m->faceCell1[i];
+        su[ip] = su[ip] - massFlux[i];
+    }
+    free(bf);
+    return ORC_E_SUCCESS;
+}
+
+/* FluxMassDolfynRegionLoop (MassKernels.ipp:523-554): per-region outflow
+ * factor -(split * flowIn) / flowRegion on outlets, 0 elsewhere. */
+int orc_region_loop(const orc_mesh *m, const double *splvl, double *flowFact, const double *flowRegion, double flowIn) {
+    for (int ir = 0; ir < m->nRegions; ir++) {
+        if (m->regionType[ir] == ORC_RTYPE_OUTLET) {
+            double split = splvl[ir];
+            flowFact[ir] = -(split * flowIn) / flowRegion[ir];
+        } else {
+            flowFact[ir] = 0.0;
+        }
+    }
+    return ORC_E_SUCCESS;
+}

@@ -85,6 +85,18 @@ int orc_flux_mass_face_loop(const orc_mesh *m,
  * given mbar[nFaces] = dL/dm_f (interior faces), accumulate into
  * rhobar/ubar/vbar/wbar[nCells]. Outputs are overwritten. */
 int orc_gradient_adjoint(const orc_mesh *m, const double *gbar, double *phibar, double *phibBar);
+
+/* ---- boundary / region loops (MassKernels.ipp:311-554) ----
+ * getBoundaryFaceID is the inverse of faceBnd; splvl[nRegions] stands for
+ * getRegionSplvl. Arguments follow the reference's order. */
+int orc_boundary_loop1(const orc_mesh *m, const double *massFlux, double *flowin);
+int orc_boundary_loop2(const orc_mesh *m, const double *massFlux, double *flowRegion, double *flowout);
+int orc_boundary_loop3(const orc_mesh *m, double flowin, double *ratearea);
+int orc_boundary_loop4(const orc_mesh *m, const double *splvl, double *massFlux, double *uB, double *vB, double *wB,
+                       const double *denB, double ratearea, double *flowout);
+int orc_boundary_loop5(const orc_mesh *m, double *massFlux, double *su, double *uB, double *vB, double *wB, double fact,
+                       int solveU, int solveV, int solveW, const double *flowFact, double *flowout2);
+int orc_region_loop(const orc_mesh *m, const double *splvl, double *flowFact, const double *flowRegion, double flowIn);
 int orc_mass_plain_forward(const orc_mesh *m, const double *den, const double *u, const double *v, const double *w,
                            double *massFlux);
 int orc_mass_plain_adjoint(const orc_mesh *m, const double *den, const double *u, const double *v, const double *w,

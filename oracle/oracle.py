@@ -54,6 +54,10 @@ def load():
             _lib.orc_jitter_build.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_ulonglong, C.c_int] + [C.c_void_p] * 11
             _lib.orc_structgen_build.argtypes = [C.c_int] * 3 + [C.c_double] * 6 + [C.c_void_p] * 11
             _lib.orc_flux_mass_face_loop.argtypes = [C.c_void_p] * 15 + [C.c_double] + [C.c_void_p] * 4 + [C.c_int] * 4 + [C.c_void_p] * 8
+            _lib.orc_boundary_loop3.argtypes = [C.c_void_p, C.c_double, C.c_void_p]
+            _lib.orc_boundary_loop4.argtypes = [C.c_void_p] * 7 + [C.c_double, C.c_void_p]
+            _lib.orc_boundary_loop5.argtypes = [C.c_void_p] * 6 + [C.c_double] + [C.c_int] * 3 + [C.c_void_p] * 2
+            _lib.orc_region_loop.argtypes = [C.c_void_p] * 4 + [C.c_double]
         return _lib
 
 
@@ -74,6 +78,13 @@ def load_ref():
                                                         C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
                 _ref.ref_flux_mass_face_loop.argtypes = ([C.c_void_p] * 15 + [C.c_double] + [C.c_void_p] * 4
                                                          + [C.c_int] * 4 + [C.c_void_p] * 8 + [C.c_int, C.c_void_p])
+                _ref.ref_ctx_set_splvl.argtypes = [C.c_void_p, C.c_void_p]
+                _ref.ref_boundary_loop1.argtypes = [C.c_void_p] * 3
+                _ref.ref_boundary_loop2.argtypes = [C.c_void_p] * 4
+                _ref.ref_boundary_loop3.argtypes = [C.c_void_p, C.c_double, C.c_void_p]
+                _ref.ref_boundary_loop4.argtypes = [C.c_void_p] * 6 + [C.c_double, C.c_void_p]
+                _ref.ref_boundary_loop5.argtypes = [C.c_void_p] * 6 + [C.c_double] + [C.c_int] * 3 + [C.c_void_p] * 2
+                _ref.ref_region_loop.argtypes = [C.c_void_p] * 3 + [C.c_double]
         return _ref
 
 
@@ -240,6 +251,60 @@ def gradient_adjoint(m, gbar):
 
 
 # ---------------------------------------------------------------------------
+# boundary / region loops (C restatement of MassKernels.ipp:311-554). Each
+# takes and returns copies: the in/out arrays of the reference call are
+# returned updated, its scalar outputs as floats.
+# ---------------------------------------------------------------------------
+def _f64(a):
+    return np.array(a, np.float64, copy=True)
+
+
+def boundary_loop1(m, massflux):
+    out = C.c_double(np.nan)
+    mf = np.ascontiguousarray(massflux, np.float64)
+    assert load().orc_boundary_loop1(C.byref(_cmesh(m)), _p(mf), C.byref(out)) == E_SUCCESS
+    return out.value
+
+
+def boundary_loop2(m, massflux, flow_region):
+    out = C.c_double(np.nan)
+    mf, fr = np.ascontiguousarray(massflux, np.float64), _f64(flow_region)
+    assert load().orc_boundary_loop2(C.byref(_cmesh(m)), _p(mf), _p(fr), C.byref(out)) == E_SUCCESS
+    return fr, out.value
+
+
+def boundary_loop3(m, flowin):
+    out = C.c_double(np.nan)
+    assert load().orc_boundary_loop3(C.byref(_cmesh(m)), float(flowin), C.byref(out)) == E_SUCCESS
+    return out.value
+
+
+def boundary_loop4(m, splvl, massflux, ub, vb, wb, denb, ratearea):
+    out = C.c_double(np.nan)
+    mf, u, v, w = _f64(massflux), _f64(ub), _f64(vb), _f64(wb)
+    sp, den = np.ascontiguousarray(splvl, np.float64), np.ascontiguousarray(denb, np.float64)
+    assert load().orc_boundary_loop4(C.byref(_cmesh(m)), _p(sp), _p(mf), _p(u), _p(v), _p(w), _p(den), float(ratearea),
+                                     C.byref(out)) == E_SUCCESS
+    return mf, u, v, w, out.value
+
+
+def boundary_loop5(m, massflux, su, ub, vb, wb, fact, solve, flow_fact, flowout2):
+    out = C.c_double(flowout2)
+    mf, s_, u, v, w = _f64(massflux), _f64(su), _f64(ub), _f64(vb), _f64(wb)
+    ff = np.ascontiguousarray(flow_fact, np.float64)
+    assert load().orc_boundary_loop5(C.byref(_cmesh(m)), _p(mf), _p(s_), _p(u), _p(v), _p(w), float(fact),
+                                     *[int(bool(x)) for x in solve], _p(ff), C.byref(out)) == E_SUCCESS
+    return mf, s_, u, v, w, out.value
+
+
+def region_loop(m, splvl, flow_region, flow_in):
+    ff = np.full(m["nRegions"], np.nan)
+    sp, fr = np.ascontiguousarray(splvl, np.float64), np.ascontiguousarray(flow_region, np.float64)
+    assert load().orc_region_loop(C.byref(_cmesh(m)), _p(sp), _p(ff), _p(fr), float(flow_in)) == E_SUCCESS
+    return ff
+
+
+# ---------------------------------------------------------------------------
 # the reference's own code (optional)
 # ---------------------------------------------------------------------------
 
@@ -311,6 +376,49 @@ class RefKernels:
             _p(out["tB"]), reps, _p(secs))
         out.update(icinl=cnt[0].value, icout=cnt[1].value, icsym=cnt[2].value, icwal=cnt[3].value)
         return rc, out, secs
+
+    # boundary / region loops, the reference templates called unchanged
+    def boundary_loops(self, splvl):
+        self._splvl = np.ascontiguousarray(splvl, np.float64)
+        self.ref.ref_ctx_set_splvl(self.h, _p(self._splvl))
+        return self
+
+    def boundary_loop1(self, massflux):
+        out = C.c_double(np.nan)
+        mf = _f64(massflux)
+        assert self.ref.ref_boundary_loop1(self.h, _p(mf), C.byref(out)) == E_SUCCESS
+        return out.value
+
+    def boundary_loop2(self, massflux, flow_region):
+        out = C.c_double(np.nan)
+        mf, fr = _f64(massflux), _f64(flow_region)
+        assert self.ref.ref_boundary_loop2(self.h, _p(mf), _p(fr), C.byref(out)) == E_SUCCESS
+        return fr, out.value
+
+    def boundary_loop3(self, flowin):
+        out = C.c_double(np.nan)
+        assert self.ref.ref_boundary_loop3(self.h, float(flowin), C.byref(out)) == E_SUCCESS
+        return out.value
+
+    def boundary_loop4(self, massflux, ub, vb, wb, denb, ratearea):
+        out = C.c_double(np.nan)
+        mf, u, v, w, den = _f64(massflux), _f64(ub), _f64(vb), _f64(wb), _f64(denb)
+        assert self.ref.ref_boundary_loop4(self.h, _p(mf), _p(u), _p(v), _p(w), _p(den), float(ratearea),
+                                           C.byref(out)) == E_SUCCESS
+        return mf, u, v, w, out.value
+
+    def boundary_loop5(self, massflux, su, ub, vb, wb, fact, solve, flow_fact, flowout2):
+        out = C.c_double(flowout2)
+        mf, s_, u, v, w, ff = _f64(massflux), _f64(su), _f64(ub), _f64(vb), _f64(wb), _f64(flow_fact)
+        assert self.ref.ref_boundary_loop5(self.h, _p(mf), _p(s_), _p(u), _p(v), _p(w), float(fact),
+                                           *[int(bool(x)) for x in solve], _p(ff), C.byref(out)) == E_SUCCESS
+        return mf, s_, u, v, w, out.value
+
+    def region_loop(self, flow_region, flow_in):
+        ff = np.full(self.m["nRegions"], np.nan)
+        fr = _f64(flow_region)
+        assert self.ref.ref_region_loop(self.h, _p(ff), _p(fr), float(flow_in)) == E_SUCCESS
+        return ff
 
 
 # ---------------------------------------------------------------------------

@@ -1,9 +1,10 @@
 /*
  * Minimal stand-in for the reference's UnstructuredMeshInterface, exposing
  * exactly the getters that the reference kernels GradientPhiGaussDolfyn
- * (include/fvm/implementation/component/GradientKernels.ipp:39-136) and
+ * (include/fvm/implementation/component/GradientKernels.ipp:39-136),
  * FluxMassDolfynFaceLoop (include/fvm/implementation/component/MassKernels.ipp:36-309)
- * call, backed by plain SoA arrays owned by the caller.
+ * and the boundary / region loops (MassKernels.ipp:311-554) call, backed by
+ * plain SoA arrays owned by the caller.
  *
  * TEST INFRASTRUCTURE ONLY: used to compile the reference's own kernel
  * templates, unchanged, into oracle/_ref/libcupcfd_ref.so. Getter names,
@@ -62,6 +63,8 @@ namespace cupcfd
 				const int * regionType;   /* [lRegions] RType values */
 				const T * regionUVW;      /* [3*lRegions] */
 				const T * regionDen;      /* [lRegions] */
+				const I * boundaryFace;   /* [lBoundaries] face of each boundary (getBoundaryFaceID) */
+				const T * regionSplvl;    /* [lRegions] (getRegionSplvl) */
 			};
 
 			template <class M, class I, class T, class L>
@@ -98,6 +101,8 @@ namespace cupcfd
 					inline I getBoundaryRegionID(I b) { return a.boundaryRegion[b]; }
 					inline RType getRegionType(I r) { return (RType) a.regionType[r]; }
 					inline T getRegionDen(I r) { return a.regionDen[r]; }
+					inline I getBoundaryFaceID(I b) { return a.boundaryFace[b]; }
+					inline T getRegionSplvl(I r) { return a.regionSplvl[r]; }
 					inline cupcfd::geometry::euclidean::EuclideanVector<T,3> getRegionUVW(I r) {
 						return cupcfd::geometry::euclidean::EuclideanVector<T,3>(a.regionUVW[3*r], a.regionUVW[3*r+1], a.regionUVW[3*r+2]);
 					}

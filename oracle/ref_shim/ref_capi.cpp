@@ -156,6 +156,8 @@ struct RefCtx {
 	int nC, nF, nB, nR;
 	std::vector<euc::EuclideanVector<double,3>> g, go;
 	std::vector<euc::EuclideanVector<double,3>> dudx, dvdx, dwdx, dpdx;
+	std::vector<int> boundaryFace;   /* getBoundaryFaceID: faceBnd inverted */
+	std::vector<double> splvl;       /* getRegionSplvl (ref_ctx_set_splvl) */
 };
 
 extern "C" void * ref_ctx_create(int nCells, int nFaces, int nBnd, int nRegions,
@@ -188,6 +190,12 @@ extern "C" void * ref_ctx_create(int nCells, int nFaces, int nBnd, int nRegions,
 	c->mesh.a.regionType = regionType;
 	c->mesh.a.regionUVW = regionUVW;
 	c->mesh.a.regionDen = regionDen;
+	c->boundaryFace.assign(nBnd > 0 ? nBnd : 1, -1);
+	for (int f = 0; f < nFaces; f++)
+		if (faceBnd[f] > -1) c->boundaryFace[faceBnd[f]] = f;
+	c->mesh.a.boundaryFace = c->boundaryFace.data();
+	c->splvl.assign(nRegions > 0 ? nRegions : 1, 0.0);
+	c->mesh.a.regionSplvl = c->splvl.data();
 	c->g.resize(nCells);
 	c->go.resize(nCells);
 	return c;
@@ -257,4 +265,45 @@ extern "C" int ref_flux_mass_face_loop(void * p,
 		if (st != cupcfd::error::E_SUCCESS) return (int) st;
 	}
 	return (int) st;
+}
+
+/* ---- boundary / region loops (MassKernels.ipp:311-554), called unchanged ---- */
+extern "C" void ref_ctx_set_splvl(void * p, const double * splvl) {
+	RefCtx * c = (RefCtx *) p;
+	for (int r = 0; r < c->nR; r++) c->splvl[r] = splvl[r];
+}
+
+extern "C" int ref_boundary_loop1(void * p, double * massFlux, double * flowin) {
+	RefCtx * c = (RefCtx *) p;
+	return (int) cupcfd::fvm::FluxMassDolfynBoundaryLoop1(c->mesh, massFlux, c->nF, flowin);
+}
+
+extern "C" int ref_boundary_loop2(void * p, double * massFlux, double * flowRegion, double * flowout) {
+	RefCtx * c = (RefCtx *) p;
+	return (int) cupcfd::fvm::FluxMassDolfynBoundaryLoop2(c->mesh, massFlux, c->nF, flowRegion, c->nR, flowout);
+}
+
+extern "C" int ref_boundary_loop3(void * p, double flowin, double * ratearea) {
+	RefCtx * c = (RefCtx *) p;
+	return (int) cupcfd::fvm::FluxMassDolfynBoundaryLoop3(c->mesh, flowin, ratearea);
+}
+
+extern "C" int ref_boundary_loop4(void * p, double * massFlux, double * uB, double * vB, double * wB, double * denB,
+                                  double ratearea, double * flowout) {
+	RefCtx * c = (RefCtx *) p;
+	return (int) cupcfd::fvm::FluxMassDolfynBoundaryLoop4(c->mesh, massFlux, c->nF, uB, c->nB, vB, c->nB, wB, c->nB,
+	                                                        denB, c->nB, ratearea, flowout);
+}
+
+extern "C" int ref_boundary_loop5(void * p, double * massFlux, double * su, double * uB, double * vB, double * wB,
+                                  double fact, int solveU, int solveV, int solveW, double * flowFact, double * flowout2) {
+	RefCtx * c = (RefCtx *) p;
+	return (int) cupcfd::fvm::FluxMassDolfynBoundaryLoop5(c->mesh, massFlux, c->nF, su, c->nC, uB, c->nB, vB, c->nB,
+	                                                        wB, c->nB, fact, solveU != 0, solveV != 0, solveW != 0,
+	                                                        flowFact, c->nR, flowout2);
+}
+
+extern "C" int ref_region_loop(void * p, double * flowFact, double * flowRegion, double flowIn) {
+	RefCtx * c = (RefCtx *) p;
+	return (int) cupcfd::fvm::FluxMassDolfynRegionLoop(c->mesh, flowFact, c->nR, flowRegion, c->nR, flowIn);
 }

@@ -100,3 +100,54 @@ def test_error_codes_match_reference_enum():
     assert ref.ref_sizeof_euclidean_vector_f64() == 32
     assert ref.ref_sizeof_euclidean_vector_f32() == 24
     assert ref.ref_offsetof_cmp_f64() == 8
+
+
+def _with_regions(m, seed):
+    """Six regions (default, inlet, two outlets, symmetry, wall), boundaries
+    assigned at random, random split levels."""
+    rng = np.random.Generator(np.random.Philox(key=seed))
+    m = dict(m)
+    m["nRegions"] = 6
+    m["regionType"] = np.array([0, 1, 2, 3, 4, 2], np.int32)
+    m["regionUVW"] = rng.standard_normal(18)
+    m["regionDen"] = rng.uniform(0.9, 1.1, 6)
+    m["bndRegion"] = rng.integers(0, 6, m["nBnd"]).astype(np.int32)
+    splvl = rng.uniform(0.2, 0.8, 6)
+    return m, splvl, rng
+
+
+@pytest.mark.parametrize("mk", ["struct", "jitter"])
+def test_boundary_and_region_loops_bit_exact(mk):
+    """FluxMassDolfynBoundaryLoop1-5 and FluxMassDolfynRegionLoop: the C
+    restatement against the reference templates, every output bit for bit."""
+    base = O.structgen(9, 7, 8) if mk == "struct" else O.jitter(9, 8, 7, 0.25, seed=4, permute=True)
+    m, splvl, rng = _with_regions(base, 31 if mk == "struct" else 32)
+    R = O.RefKernels(m).boundary_loops(splvl)
+    nF, nB, nC, nR = m["nFaces"], m["nBnd"], m["nCells"], m["nRegions"]
+    mf = rng.uniform(1e-6, 1e-2, nF) * rng.choice([-1.0, 1.0], nF)
+    assert O.boundary_loop1(m, mf) == R.boundary_loop1(mf)
+    fr0 = rng.uniform(1e-6, 1e-2, nR)
+    fa, oa = O.boundary_loop2(m, mf, fr0)
+    fb, ob = R.boundary_loop2(mf, fr0)
+    assert np.array_equal(fa, fb) and oa == ob
+    assert O.boundary_loop3(m, 1.1) == R.boundary_loop3(1.1)
+    u, v, w, den = (rng.uniform(1e-6, 1e-2, nB) for _ in range(4))
+    a4 = O.boundary_loop4(m, splvl, mf, u, v, w, den, -0.37)
+    b4 = R.boundary_loop4(mf, u, v, w, den, -0.37)
+    for x, y in zip(a4, b4):
+        assert np.array_equal(x, y)
+    su = rng.standard_normal(nC)
+    ff = O.region_loop(m, splvl, fa, 0.7)
+    assert np.array_equal(ff, R.region_loop(fa, 0.7))
+    for solve in ((1, 1, 1), (1, 0, 1)):
+        a5 = O.boundary_loop5(m, a4[0], su, u, v, w, 1.3, solve, ff, 0.25)
+        b5 = R.boundary_loop5(a4[0], su, u, v, w, 1.3, solve, ff, 0.25)
+        for x, y in zip(a5, b5):
+            assert np.array_equal(x, y)
+    # the outlet cells with several boundary faces are where su's order shows
+    bf = np.full(nB, -1)
+    inner = m["faceBnd"] > -1
+    bf[m["faceBnd"][inner]] = np.nonzero(inner)[0]
+    outlet = m["regionType"][m["bndRegion"]] == 2
+    cells = m["faceCell1"][bf[outlet]]
+    assert len(cells) > len(np.unique(cells))
