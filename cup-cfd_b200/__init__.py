@@ -85,6 +85,20 @@ SIGNATURES = {
     "cupcfd_gpu_mesh_destroy": ([_VP], _I),
     "cupcfd_gpu_mesh_get_info": ([_VP, _VP], _I),
     "cupcfd_gpu_mesh_set_regions": ([_VP, _I, _VP, _VP, _VP, _VP, _I], _I),
+    "cupcfd_gpu_mesh_set_region_split": ([_VP, _I, _VP], _I),
+    "cupcfd_gpu_flux_mass_dolfyn_boundary_loop1": ([_VP, _VP, _I, _VP], _I),
+    "cupcfd_gpu_flux_mass_dolfyn_boundary_loop2": ([_VP, _VP, _I, _VP, _I, _VP], _I),
+    "cupcfd_gpu_flux_mass_dolfyn_boundary_loop3": ([_VP, _D, _VP], _I),
+    "cupcfd_gpu_flux_mass_dolfyn_boundary_loop4": ([_VP, _VP, _I, _VP, _I, _VP, _I, _VP, _I, _VP, _I, _D, _VP], _I),
+    "cupcfd_gpu_flux_mass_dolfyn_boundary_loop5": ([_VP, _VP, _I, _VP, _I, _VP, _I, _VP, _I, _VP, _I, _D, _I, _I, _I,
+                                                    _VP, _I, _VP], _I),
+    "cupcfd_gpu_flux_mass_dolfyn_region_loop": ([_VP, _VP, _I, _VP, _I, _D], _I),
+    "cupcfd_gpu_dev_boundary_loop1": ([_VP, _VP, _VP, _VP], _I),
+    "cupcfd_gpu_dev_boundary_loop2": ([_VP, _VP, _VP, _VP, _VP], _I),
+    "cupcfd_gpu_dev_boundary_loop3": ([_VP, _VP, _VP, _VP], _I),
+    "cupcfd_gpu_dev_boundary_loop4": ([_VP] * 9, _I),
+    "cupcfd_gpu_dev_boundary_loop5": ([_VP] * 6 + [_D, _I, _I, _I, _VP, _VP, _VP], _I),
+    "cupcfd_gpu_dev_region_loop": ([_VP] * 5, _I),
     "cupcfd_gpu_mesh_set_fusion": ([_VP, _I], _I),
     "cupcfd_gpu_mesh_check_status": ([_VP, _VP], _I),
     "cupcfd_gpu_mesh_get_cell_face_csr": ([_VP, _VP, _I, _VP, _I], _I),
@@ -278,6 +292,10 @@ class Mesh:
         br = np.ascontiguousarray(bnd_region, np.int32)
         return lib().cupcfd_gpu_mesh_set_regions(self.h, len(rt), _p(rt), _p(uvw), _p(den), _p(br), len(br))
 
+    def set_region_split(self, splvl):
+        sp = np.ascontiguousarray(splvl, np.float64)
+        return lib().cupcfd_gpu_mesh_set_region_split(self.h, len(sp), _p(sp))
+
     def set_fusion(self, mode):
         """0 auto, 1 always fused, 2 never fused (forward+adjoint)."""
         check(lib().cupcfd_gpu_mesh_set_fusion(self.h, int(mode)))
@@ -428,3 +446,81 @@ def error_norms(a, b, floor=0.0, stream=None):
     mx, mb, s2, b2, mr = list(out)
     return dict(max_abs=mx, max_ref=mb, max_rel_norm=mx / mb if mb else 0.0,
                 rms_rel=(s2 / b2) ** 0.5 if b2 else 0.0, max_rel_floor=mr)
+
+
+# ---------------------------------------------------------------------------
+# boundary / region loops of the mass-flux step (MassKernels.ipp:311-554).
+# Host arrays in the reference's numbering; in/out arrays are updated in
+# place, scalar outputs returned. Each returns (status, outputs...).
+# ---------------------------------------------------------------------------
+def _h(a):
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a
+
+
+def FluxMassDolfynBoundaryLoop1(mesh, massFlux):
+    out = C.c_double(np.nan)
+    rc = lib().cupcfd_gpu_flux_mass_dolfyn_boundary_loop1(mesh.h, _p(_h(massFlux)), len(massFlux), C.byref(out))
+    return rc, out.value
+
+
+def FluxMassDolfynBoundaryLoop2(mesh, massFlux, flowRegion):
+    out = C.c_double(np.nan)
+    rc = lib().cupcfd_gpu_flux_mass_dolfyn_boundary_loop2(mesh.h, _p(_h(massFlux)), len(massFlux), _p(_h(flowRegion)),
+                                                          len(flowRegion), C.byref(out))
+    return rc, out.value
+
+
+def FluxMassDolfynBoundaryLoop3(mesh, flowin):
+    out = C.c_double(np.nan)
+    rc = lib().cupcfd_gpu_flux_mass_dolfyn_boundary_loop3(mesh.h, float(flowin), C.byref(out))
+    return rc, out.value
+
+
+def FluxMassDolfynBoundaryLoop4(mesh, massFlux, uB, vB, wB, denB, ratearea):
+    out = C.c_double(np.nan)
+    rc = lib().cupcfd_gpu_flux_mass_dolfyn_boundary_loop4(
+        mesh.h, _p(_h(massFlux)), len(massFlux), _p(_h(uB)), len(uB), _p(_h(vB)), len(vB), _p(_h(wB)), len(wB),
+        _p(_h(denB)), len(denB), float(ratearea), C.byref(out))
+    return rc, out.value
+
+
+def FluxMassDolfynBoundaryLoop5(mesh, massFlux, su, uB, vB, wB, fact, solve, flowFact, flowout2):
+    out = C.c_double(flowout2)
+    rc = lib().cupcfd_gpu_flux_mass_dolfyn_boundary_loop5(
+        mesh.h, _p(_h(massFlux)), len(massFlux), _p(_h(su)), len(su), _p(_h(uB)), len(uB), _p(_h(vB)), len(vB),
+        _p(_h(wB)), len(wB), float(fact), *[int(bool(x)) for x in solve], _p(_h(flowFact)), len(flowFact),
+        C.byref(out))
+    return rc, out.value
+
+
+def FluxMassDolfynRegionLoop(mesh, flowFact, flowRegion, flowIn):
+    return lib().cupcfd_gpu_flux_mass_dolfyn_region_loop(mesh.h, _p(_h(flowFact)), len(flowFact), _p(_h(flowRegion)),
+                                                        len(flowRegion), float(flowIn))
+
+
+def dev_boundary_loop1(mesh, massFlux, flowin, stream=None):
+    check(lib().cupcfd_gpu_dev_boundary_loop1(mesh.h, _p(massFlux), _p(flowin), _stream(stream)))
+
+
+def dev_boundary_loop2(mesh, massFlux, flowRegion, flowout, stream=None):
+    check(lib().cupcfd_gpu_dev_boundary_loop2(mesh.h, _p(massFlux), _p(flowRegion), _p(flowout), _stream(stream)))
+
+
+def dev_boundary_loop3(mesh, flowin, ratearea, stream=None):
+    check(lib().cupcfd_gpu_dev_boundary_loop3(mesh.h, _p(flowin), _p(ratearea), _stream(stream)))
+
+
+def dev_boundary_loop4(mesh, massFlux, uB, vB, wB, denB, ratearea, flowout, stream=None):
+    check(lib().cupcfd_gpu_dev_boundary_loop4(mesh.h, _p(massFlux), _p(uB), _p(vB), _p(wB), _p(denB), _p(ratearea),
+                                              _p(flowout), _stream(stream)))
+
+
+def dev_boundary_loop5(mesh, massFlux, su, uB, vB, wB, fact, solve, flowFact, flowout2, stream=None):
+    check(lib().cupcfd_gpu_dev_boundary_loop5(mesh.h, _p(massFlux), _p(su), _p(uB), _p(vB), _p(wB), float(fact),
+                                              *[int(bool(x)) for x in solve], _p(flowFact), _p(flowout2),
+                                              _stream(stream)))
+
+
+def dev_region_loop(mesh, flowFact, flowRegion, flowIn, stream=None):
+    check(lib().cupcfd_gpu_dev_region_loop(mesh.h, _p(flowFact), _p(flowRegion), _p(flowIn), _stream(stream)))

@@ -1,0 +1,346 @@
+// C ABI of the boundary / region loops of the mass-flux step
+// (FluxMassDolfynBoundaryLoop1-5, FluxMassDolfynRegionLoop;
+// MassKernels.ipp:311-554): reference-facing calls on host buffers in the
+// reference's numbering, and device-resident calls in the mesh's internal
+// numbering. Kernels in kernels_bnd.cuh; FP64 arithmetic of the reference.
+#include <algorithm>
+
+#include "kernels_bnd.cuh"
+
+using namespace cupcfd_gpu;
+
+namespace {
+
+constexpr int BT = 256;
+// scratch slots of the host-buffer calls (kept across calls)
+enum BndSlot { B_MF = 40, B_SU, B_U, B_V, B_W, B_DEN, B_REG, B_REG2, B_SCAL };
+
+// Boundary -> face and sorted-boundary -> cell maps for the caller's numbering.
+struct Maps {
+    const int *face, *cell;
+};
+inline Maps maps_for(const cupcfd_gpu_mesh *m, bool internal) {
+    return internal ? Maps{m->bndFaceInt, m->bndSortedCellInt} : Maps{m->bndFaceRef, m->bndSortedCellRef};
+}
+
+int check_mesh(const cupcfd_gpu_mesh *m, bool needGeometry) {
+    CG_RETURN_IF(!m, CUPCFD_E_NULL_PTR, "boundary loop: null mesh");
+    CG_RETURN_IF(!m->bndMapsOk, CUPCFD_E_INVALID_INDEX,
+                 "boundary loop: the mesh's boundary ids are not a permutation of 0 .. nBoundaries-1");
+    CG_RETURN_IF(needGeometry && !(m->precisions & (1 << CUPCFD_PREC_F64)), CUPCFD_E_CONFIG_INVALID_VALUE,
+                 "boundary loop: the mesh was created without FP64 geometry");
+    return make_device_current(m->device);
+}
+
+template <class T>
+int slot(cupcfd_gpu_mesh *m, int s, size_t n, T **p) {
+    void *v;
+    CG_TRY(m->scratchBuf(s, std::max<size_t>(n, 1) * sizeof(T), &v));
+    *p = (T *) v;
+    return CUPCFD_E_SUCCESS;
+}
+
+int up(void *d, const void *h, size_t bytes, cudaStream_t st) {
+    if (bytes) CG_CHECK_CUDA(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st));
+    return CUPCFD_E_SUCCESS;
+}
+int down(void *h, const void *d, size_t bytes, cudaStream_t st) {
+    if (bytes) CG_CHECK_CUDA(cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, st));
+    return CUPCFD_E_SUCCESS;
+}
+
+// ---- the loops on device arrays (face arrays indexed through mp.face, cell
+// arrays through mp.cell); every scalar in device memory ----
+int run_loop1(cupcfd_gpu_mesh *m, Maps mp, const double *mf, double *flowin, cudaStream_t st) {
+    k_bl_sum<<<1, 1024, 0, st>>>(m->nB, m->bndRegion, m->regionType, CUPCFD_RTYPE_INLET, mf, 1, 0, mp.face, nullptr,
+                                 0.0, flowin, nullptr, 0);
+    CG_LAUNCHED();
+    return CUPCFD_E_SUCCESS;
+}
+
+int run_loop2(cupcfd_gpu_mesh *m, Maps mp, const double *mf, double *flowRegion, double *flowout, cudaStream_t st) {
+    k_bl_sum<<<1, 1024, 0, st>>>(m->nB, m->bndRegion, m->regionType, CUPCFD_RTYPE_OUTLET, mf, 1, 0, mp.face, nullptr,
+                                 0.0, flowout, flowRegion, m->nR);
+    CG_LAUNCHED();
+    return CUPCFD_E_SUCCESS;
+}
+
+int run_loop3(cupcfd_gpu_mesh *m, const double *flowin, double *ratearea, double *areaout, cudaStream_t st) {
+    // face areas from the internal {xf, yf, zf, area} records
+    k_bl_sum<<<1, 1024, 0, st>>>(m->nB, m->bndRegion, m->regionType, CUPCFD_RTYPE_OUTLET, (const double *) m->fc64, 4,
+                                 3, m->bndFaceInt, nullptr, 0.0, areaout, nullptr, 0);
+    CG_LAUNCHED();
+    k_bl_ratearea<<<1, 1, 0, st>>>(flowin, areaout, ratearea);
+    CG_LAUNCHED();
+    return CUPCFD_E_SUCCESS;
+}
+
+int run_loop4(cupcfd_gpu_mesh *m, Maps mp, double *mf, double *uB, double *vB, double *wB, const double *denB,
+              const double *ratearea, double *flowout, cudaStream_t st) {
+    if (m->nB > 0) {
+        k_bl4_update<<<grid_for(m->nB, BT), BT, 0, st>>>(m->nB, m->bndRegion, m->regionType, m->regionSplvl, mp.face,
+                                                         m->bndFaceInt, m->fg64, m->fc64, mf, uB, vB, wB, denB, ratearea);
+        CG_LAUNCHED();
+    }
+    k_bl_sum<<<1, 1024, 0, st>>>(m->nB, m->bndRegion, m->regionType, CUPCFD_RTYPE_OUTLET, mf, 1, 0, mp.face, nullptr,
+                                 0.0, flowout, nullptr, 0);
+    CG_LAUNCHED();
+    return CUPCFD_E_SUCCESS;
+}
+
+int run_loop5(cupcfd_gpu_mesh *m, Maps mp, double *mf, double *su, double *uB, double *vB, double *wB, double fact,
+              int solveU, int solveV, int solveW, const double *flowFact, double *flowout2, cudaStream_t st) {
+    if (m->nB > 0) {
+        k_bl5_update<<<grid_for(m->nB, BT), BT, 0, st>>>(m->nB, m->bndRegion, m->regionType, mp.face, mf, flowFact, uB,
+                                                         vB, wB, fact, solveU, solveV, solveW);
+        CG_LAUNCHED();
+        k_bl5_su<<<grid_for(m->nB, BT), BT, 0, st>>>(m->nB, m->bndSorted, mp.cell, m->bndRegion, m->regionType, mp.face,
+                                                     mf, su);
+        CG_LAUNCHED();
+    }
+    // *flowout2 is not reset (MassKernels.ipp:457-521): the sum starts from its value
+    k_bl_sum<<<1, 1024, 0, st>>>(m->nB, m->bndRegion, m->regionType, CUPCFD_RTYPE_OUTLET, mf, 1, 0, mp.face, flowout2,
+                                 0.0, flowout2, nullptr, 0);
+    CG_LAUNCHED();
+    return CUPCFD_E_SUCCESS;
+}
+
+int run_region_loop(cupcfd_gpu_mesh *m, double *flowFact, const double *flowRegion, const double *flowIn,
+                    cudaStream_t st) {
+    k_region_loop<<<grid_for(m->nR, BT), BT, 0, st>>>(m->nR, m->regionType, m->regionSplvl, flowRegion, flowIn,
+                                                     flowFact);
+    CG_LAUNCHED();
+    return CUPCFD_E_SUCCESS;
+}
+
+inline cudaStream_t as_stream(void *s) { return (cudaStream_t) s; }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// region split levels
+// ---------------------------------------------------------------------------
+extern "C" int cupcfd_gpu_mesh_set_region_split(cupcfd_gpu_mesh *m, int32_t nRegions, const double *splvl) {
+    clear_error();
+    CG_RETURN_IF(!m || !splvl, CUPCFD_E_NULL_PTR, "set_region_split: null argument");
+    CG_RETURN_IF(nRegions != m->nR, CUPCFD_E_ARRAY_SIZE_MISMATCH, "set_region_split: nRegions differs from the mesh's");
+    CG_TRY(make_device_current(m->device));
+    CG_CHECK_CUDA(cudaMemcpyAsync(m->regionSplvl, splvl, sizeof(double) * nRegions, cudaMemcpyHostToDevice, m->stream));
+    CG_CHECK_CUDA(cudaStreamSynchronize(m->stream));
+    return CUPCFD_E_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// reference-facing calls: host buffers, reference numbering. Arrays shorter
+// than the mesh needs return E_INVALID_INDEX, as the reference's DEBUG build
+// does (MassKernels.ipp:326-330, 354-361, 420-436, 477-493, 511-515, 535-542).
+// ---------------------------------------------------------------------------
+extern "C" int cupcfd_gpu_flux_mass_dolfyn_boundary_loop1(cupcfd_gpu_mesh *m, const double *massFlux,
+                                                          int32_t nMassFlux, double *flowin) {
+    clear_error();
+    CG_TRY(check_mesh(m, false));
+    CG_RETURN_IF(!massFlux || !flowin, CUPCFD_E_NULL_PTR, "boundary_loop1: null argument");
+    CG_RETURN_IF(nMassFlux < m->nF, CUPCFD_E_INVALID_INDEX, "boundary_loop1: massFlux shorter than nFaces");
+    cudaStream_t st = m->stream;
+    double *mf, *sc;
+    CG_TRY(slot(m, B_MF, m->nF, &mf));
+    CG_TRY(slot(m, B_SCAL, 4, &sc));
+    CG_TRY(up(mf, massFlux, sizeof(double) * m->nF, st));
+    CG_TRY(run_loop1(m, maps_for(m, false), mf, sc, st));
+    CG_TRY(down(flowin, sc, sizeof(double), st));
+    CG_CHECK_CUDA(cudaStreamSynchronize(st));
+    return CUPCFD_E_SUCCESS;
+}
+
+extern "C" int cupcfd_gpu_flux_mass_dolfyn_boundary_loop2(cupcfd_gpu_mesh *m, const double *massFlux,
+                                                          int32_t nMassFlux, double *flowRegion, int32_t nFlowRegion,
+                                                          double *flowout) {
+    clear_error();
+    CG_TRY(check_mesh(m, false));
+    CG_RETURN_IF(!massFlux || !flowRegion || !flowout, CUPCFD_E_NULL_PTR, "boundary_loop2: null argument");
+    CG_RETURN_IF(nMassFlux < m->nF || nFlowRegion < m->nR, CUPCFD_E_INVALID_INDEX, "boundary_loop2: array too short");
+    cudaStream_t st = m->stream;
+    double *mf, *fr, *sc;
+    CG_TRY(slot(m, B_MF, m->nF, &mf));
+    CG_TRY(slot(m, B_REG, m->nR, &fr));
+    CG_TRY(slot(m, B_SCAL, 4, &sc));
+    CG_TRY(up(mf, massFlux, sizeof(double) * m->nF, st));
+    CG_TRY(up(fr, flowRegion, sizeof(double) * m->nR, st));
+    CG_TRY(run_loop2(m, maps_for(m, false), mf, fr, sc, st));
+    CG_TRY(down(flowRegion, fr, sizeof(double) * m->nR, st));
+    CG_TRY(down(flowout, sc, sizeof(double), st));
+    CG_CHECK_CUDA(cudaStreamSynchronize(st));
+    return CUPCFD_E_SUCCESS;
+}
+
+extern "C" int cupcfd_gpu_flux_mass_dolfyn_boundary_loop3(cupcfd_gpu_mesh *m, double flowin, double *ratearea) {
+    clear_error();
+    CG_TRY(check_mesh(m, true));
+    CG_RETURN_IF(!ratearea, CUPCFD_E_NULL_PTR, "boundary_loop3: null argument");
+    cudaStream_t st = m->stream;
+    double *sc;
+    CG_TRY(slot(m, B_SCAL, 4, &sc));
+    CG_TRY(up(sc, &flowin, sizeof(double), st));
+    CG_TRY(run_loop3(m, sc, sc + 1, sc + 2, st));
+    CG_TRY(down(ratearea, sc + 1, sizeof(double), st));
+    CG_CHECK_CUDA(cudaStreamSynchronize(st));
+    return CUPCFD_E_SUCCESS;
+}
+
+extern "C" int cupcfd_gpu_flux_mass_dolfyn_boundary_loop4(cupcfd_gpu_mesh *m, double *massFlux, int32_t nMassFlux,
+                                                          double *uBoundary, int32_t nUBoundary, double *vBoundary,
+                                                          int32_t nVBoundary, double *wBoundary, int32_t nWBoundary,
+                                                          const double *denBoundary, int32_t nDenBoundary,
+                                                          double ratearea, double *flowout) {
+    clear_error();
+    CG_TRY(check_mesh(m, true));
+    CG_RETURN_IF(!massFlux || !uBoundary || !vBoundary || !wBoundary || !denBoundary || !flowout, CUPCFD_E_NULL_PTR,
+                 "boundary_loop4: null argument");
+    CG_RETURN_IF(nMassFlux < m->nF || nUBoundary < m->nB || nVBoundary < m->nB || nWBoundary < m->nB ||
+                     nDenBoundary < m->nB,
+                 CUPCFD_E_INVALID_INDEX, "boundary_loop4: array too short");
+    cudaStream_t st = m->stream;
+    size_t nb = sizeof(double) * m->nB;
+    double *mf, *u, *v, *w, *den, *sc;
+    CG_TRY(slot(m, B_MF, m->nF, &mf));
+    CG_TRY(slot(m, B_U, m->nB, &u));
+    CG_TRY(slot(m, B_V, m->nB, &v));
+    CG_TRY(slot(m, B_W, m->nB, &w));
+    CG_TRY(slot(m, B_DEN, m->nB, &den));
+    CG_TRY(slot(m, B_SCAL, 4, &sc));
+    CG_TRY(up(mf, massFlux, sizeof(double) * m->nF, st));
+    CG_TRY(up(u, uBoundary, nb, st));
+    CG_TRY(up(v, vBoundary, nb, st));
+    CG_TRY(up(w, wBoundary, nb, st));
+    CG_TRY(up(den, denBoundary, nb, st));
+    CG_TRY(up(sc, &ratearea, sizeof(double), st));
+    CG_TRY(run_loop4(m, maps_for(m, false), mf, u, v, w, den, sc, sc + 1, st));
+    CG_TRY(down(massFlux, mf, sizeof(double) * m->nF, st));
+    CG_TRY(down(uBoundary, u, nb, st));
+    CG_TRY(down(vBoundary, v, nb, st));
+    CG_TRY(down(wBoundary, w, nb, st));
+    CG_TRY(down(flowout, sc + 1, sizeof(double), st));
+    CG_CHECK_CUDA(cudaStreamSynchronize(st));
+    return CUPCFD_E_SUCCESS;
+}
+
+extern "C" int cupcfd_gpu_flux_mass_dolfyn_boundary_loop5(cupcfd_gpu_mesh *m, double *massFlux, int32_t nMassFlux,
+                                                          double *su, int32_t nSu, double *uBoundary,
+                                                          int32_t nUBoundary, double *vBoundary, int32_t nVBoundary,
+                                                          double *wBoundary, int32_t nWBoundary, double fact,
+                                                          int32_t solveU, int32_t solveV, int32_t solveW,
+                                                          const double *flowFact, int32_t nFlowFact,
+                                                          double *flowout2) {
+    clear_error();
+    CG_TRY(check_mesh(m, false));
+    CG_RETURN_IF(!massFlux || !su || !uBoundary || !vBoundary || !wBoundary || !flowFact || !flowout2,
+                 CUPCFD_E_NULL_PTR, "boundary_loop5: null argument");
+    CG_RETURN_IF(nMassFlux < m->nF || nSu < m->nC || nUBoundary < m->nB || nVBoundary < m->nB || nWBoundary < m->nB ||
+                     nFlowFact < m->nR,
+                 CUPCFD_E_INVALID_INDEX, "boundary_loop5: array too short");
+    cudaStream_t st = m->stream;
+    size_t nb = sizeof(double) * m->nB;
+    double *mf, *suD, *u, *v, *w, *ff, *sc;
+    CG_TRY(slot(m, B_MF, m->nF, &mf));
+    CG_TRY(slot(m, B_SU, m->nC, &suD));
+    CG_TRY(slot(m, B_U, m->nB, &u));
+    CG_TRY(slot(m, B_V, m->nB, &v));
+    CG_TRY(slot(m, B_W, m->nB, &w));
+    CG_TRY(slot(m, B_REG, m->nR, &ff));
+    CG_TRY(slot(m, B_SCAL, 4, &sc));
+    CG_TRY(up(mf, massFlux, sizeof(double) * m->nF, st));
+    CG_TRY(up(suD, su, sizeof(double) * m->nC, st));
+    CG_TRY(up(u, uBoundary, nb, st));
+    CG_TRY(up(v, vBoundary, nb, st));
+    CG_TRY(up(w, wBoundary, nb, st));
+    CG_TRY(up(ff, flowFact, sizeof(double) * m->nR, st));
+    CG_TRY(up(sc, flowout2, sizeof(double), st));
+    CG_TRY(run_loop5(m, maps_for(m, false), mf, suD, u, v, w, fact, solveU != 0, solveV != 0, solveW != 0, ff, sc, st));
+    CG_TRY(down(massFlux, mf, sizeof(double) * m->nF, st));
+    CG_TRY(down(su, suD, sizeof(double) * m->nC, st));
+    CG_TRY(down(uBoundary, u, nb, st));
+    CG_TRY(down(vBoundary, v, nb, st));
+    CG_TRY(down(wBoundary, w, nb, st));
+    CG_TRY(down(flowout2, sc, sizeof(double), st));
+    CG_CHECK_CUDA(cudaStreamSynchronize(st));
+    return CUPCFD_E_SUCCESS;
+}
+
+extern "C" int cupcfd_gpu_flux_mass_dolfyn_region_loop(cupcfd_gpu_mesh *m, double *flowFact, int32_t nFlowFact,
+                                                      const double *flowRegion, int32_t nFlowRegion, double flowIn) {
+    clear_error();
+    CG_TRY(check_mesh(m, false));
+    CG_RETURN_IF(!flowFact || !flowRegion, CUPCFD_E_NULL_PTR, "region_loop: null argument");
+    CG_RETURN_IF(nFlowFact < m->nR || nFlowRegion < m->nR, CUPCFD_E_INVALID_INDEX, "region_loop: array too short");
+    cudaStream_t st = m->stream;
+    double *ff, *fr, *sc;
+    CG_TRY(slot(m, B_REG, m->nR, &ff));
+    CG_TRY(slot(m, B_REG2, m->nR, &fr));
+    CG_TRY(slot(m, B_SCAL, 4, &sc));
+    CG_TRY(up(fr, flowRegion, sizeof(double) * m->nR, st));
+    CG_TRY(up(sc, &flowIn, sizeof(double), st));
+    CG_TRY(run_region_loop(m, ff, fr, sc, st));
+    CG_TRY(down(flowFact, ff, sizeof(double) * m->nR, st));
+    CG_CHECK_CUDA(cudaStreamSynchronize(st));
+    return CUPCFD_E_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// device-resident calls: device pointers, internal face and cell numbering,
+// boundary and region arrays by reference id, scalars in device memory,
+// stream-ordered (no synchronisation)
+// ---------------------------------------------------------------------------
+extern "C" int cupcfd_gpu_dev_boundary_loop1(cupcfd_gpu_mesh *m, const double *massFlux, double *flowin, void *stream) {
+    clear_error();
+    CG_TRY(check_mesh(m, false));
+    CG_RETURN_IF(!massFlux || !flowin, CUPCFD_E_NULL_PTR, "dev_boundary_loop1: null argument");
+    return run_loop1(m, maps_for(m, true), massFlux, flowin, as_stream(stream));
+}
+
+extern "C" int cupcfd_gpu_dev_boundary_loop2(cupcfd_gpu_mesh *m, const double *massFlux, double *flowRegion,
+                                             double *flowout, void *stream) {
+    clear_error();
+    CG_TRY(check_mesh(m, false));
+    CG_RETURN_IF(!massFlux || !flowRegion || !flowout, CUPCFD_E_NULL_PTR, "dev_boundary_loop2: null argument");
+    return run_loop2(m, maps_for(m, true), massFlux, flowRegion, flowout, as_stream(stream));
+}
+
+extern "C" int cupcfd_gpu_dev_boundary_loop3(cupcfd_gpu_mesh *m, const double *flowin, double *ratearea, void *stream) {
+    clear_error();
+    CG_TRY(check_mesh(m, true));
+    CG_RETURN_IF(!flowin || !ratearea, CUPCFD_E_NULL_PTR, "dev_boundary_loop3: null argument");
+    double *sc;
+    CG_TRY(slot(m, B_SCAL + 1, 1, &sc));  // the outlet area
+    return run_loop3(m, flowin, ratearea, sc, as_stream(stream));
+}
+
+extern "C" int cupcfd_gpu_dev_boundary_loop4(cupcfd_gpu_mesh *m, double *massFlux, double *uBoundary,
+                                             double *vBoundary, double *wBoundary, const double *denBoundary,
+                                             const double *ratearea, double *flowout, void *stream) {
+    clear_error();
+    CG_TRY(check_mesh(m, true));
+    CG_RETURN_IF(!massFlux || !uBoundary || !vBoundary || !wBoundary || !denBoundary || !ratearea || !flowout,
+                 CUPCFD_E_NULL_PTR, "dev_boundary_loop4: null argument");
+    return run_loop4(m, maps_for(m, true), massFlux, uBoundary, vBoundary, wBoundary, denBoundary, ratearea, flowout,
+                     as_stream(stream));
+}
+
+extern "C" int cupcfd_gpu_dev_boundary_loop5(cupcfd_gpu_mesh *m, double *massFlux, double *su, double *uBoundary,
+                                             double *vBoundary, double *wBoundary, double fact, int32_t solveU,
+                                             int32_t solveV, int32_t solveW, const double *flowFact, double *flowout2,
+                                             void *stream) {
+    clear_error();
+    CG_TRY(check_mesh(m, false));
+    CG_RETURN_IF(!massFlux || !su || !uBoundary || !vBoundary || !wBoundary || !flowFact || !flowout2,
+                 CUPCFD_E_NULL_PTR, "dev_boundary_loop5: null argument");
+    return run_loop5(m, maps_for(m, true), massFlux, su, uBoundary, vBoundary, wBoundary, fact, solveU != 0,
+                     solveV != 0, solveW != 0, flowFact, flowout2, as_stream(stream));
+}
+
+extern "C" int cupcfd_gpu_dev_region_loop(cupcfd_gpu_mesh *m, double *flowFact, const double *flowRegion,
+                                          const double *flowIn, void *stream) {
+    clear_error();
+    CG_TRY(check_mesh(m, false));
+    CG_RETURN_IF(!flowFact || !flowRegion || !flowIn, CUPCFD_E_NULL_PTR, "dev_region_loop: null argument");
+    return run_region_loop(m, flowFact, flowRegion, flowIn, as_stream(stream));
+}

@@ -113,6 +113,14 @@ struct cupcfd_gpu_mesh {
     // boundary regions (boundary ids in reference numbering)
     int *bndRegion = nullptr, *regionType = nullptr;
     double *regionUVW = nullptr, *regionDen = nullptr;
+    double *regionSplvl = nullptr;  // getRegionSplvl, zeros until cupcfd_gpu_mesh_set_region_split
+    // boundary loops: each boundary's face (reference and internal ids), and
+    // the boundaries sorted by (owner cell, id) with those cells in internal
+    // and reference numbering; bndMapsOk false if the boundary ids were not
+    // a permutation of 0 .. nB-1
+    int *bndFaceRef = nullptr, *bndFaceInt = nullptr;
+    int *bndSorted = nullptr, *bndSortedCellInt = nullptr, *bndSortedCellRef = nullptr;
+    bool bndMapsOk = false;
     std::vector<int> hRegionType;
     // wavefront-fused forward+adjoint: numbering bandwidth (largest
     // |c - neighbour|), per-tile publication flags, work counter + error word

@@ -20,14 +20,11 @@
 // reference CPU build bit for bit.
 #pragma once
 
+#include "arith.cuh"
 #include "internal.cuh"
 
 namespace cupcfd_gpu {
 
-__device__ __forceinline__ double dm(double a, double b) { return __dmul_rn(a, b); }
-__device__ __forceinline__ double da(double a, double b) { return __dadd_rn(a, b); }
-__device__ __forceinline__ double ds(double a, double b) { return __dsub_rn(a, b); }
-__device__ __forceinline__ double dvd(double a, double b) { return __ddiv_rn(a, b); }
 
 // ---------------------------------------------------------------------------
 // Dot2 compensated accumulation (Ogita, Rump & Oishi, "Accurate sum and dot

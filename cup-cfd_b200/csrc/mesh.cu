@@ -250,6 +250,35 @@ __global__ void k_fill_sell(int nC, const int *__restrict__ cellN2O, const int *
     for (; k < width; k++) inc[base + 32 * k] = make_int2(-1, -1);
 }
 
+// Boundary -> face maps and the (owner cell, boundary id) sort keys; a
+// boundary id out of range or met twice sets err.
+__global__ void k_bnd_maps(int nF, int nB, const int *__restrict__ faceN2O, const int *__restrict__ bndRef,
+                           const int2 *__restrict__ fcells, int *__restrict__ bndFaceRef, int *__restrict__ bndFaceInt,
+                           unsigned long long *__restrict__ keys, int *__restrict__ err) {
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nF) return;
+    int fo = faceN2O[f], b = bndRef[fo];
+    if (b < 0) return;
+    if (b >= nB || atomicCAS(bndFaceRef + b, -1, fo) != -1) {
+        atomicOr(err, 1);
+        return;
+    }
+    bndFaceInt[b] = f;
+    keys[b] = ((unsigned long long) (unsigned) fcells[f].x << 32) | (unsigned) b;
+}
+
+__global__ void k_bnd_unkey(int nB, const unsigned long long *__restrict__ keys, const int *__restrict__ cellN2O,
+                            const int *__restrict__ bndFaceRef, int *__restrict__ sorted, int *__restrict__ cellInt,
+                            int *__restrict__ cellRef, int *__restrict__ err) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nB) return;
+    if (bndFaceRef[k] < 0) atomicOr(err, 1);  // a boundary id no face carries
+    int c = (int) (keys[k] >> 32);
+    sorted[k] = (int) (unsigned) keys[k];
+    cellInt[k] = c;
+    cellRef[k] = cellN2O[c];
+}
+
 __global__ void k_any_nonzero(int64_t n, const double *__restrict__ a, int *__restrict__ flag) {
     int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n && a[i] != 0.0) *flag = 1;
@@ -646,6 +675,42 @@ int build_mesh_from_source(cupcfd_gpu_mesh *m, const Source &s, const cupcfd_mes
         m->sell.width = (allow && m->sell.nEntries == (int64_t) 32 * nSlices * m->maxDeg) ? m->maxDeg : 0;
     }
 
+    // --- boundary maps for the boundary loops
+    if (nB > 0) {
+        CG_TRY(m->alloc(&m->bndFaceRef, (size_t) nB));
+        CG_TRY(m->alloc(&m->bndFaceInt, (size_t) nB));
+        CG_TRY(m->alloc(&m->bndSorted, (size_t) nB));
+        CG_TRY(m->alloc(&m->bndSortedCellInt, (size_t) nB));
+        CG_TRY(m->alloc(&m->bndSortedCellRef, (size_t) nB));
+        uint64_t *keys, *keysOut;
+        int *berr;
+        Tmp tk1, tk2, tk3;
+        CG_TRY(tk1.get(&keys, (size_t) nB));
+        CG_TRY(tk2.get(&keysOut, (size_t) nB));
+        CG_TRY(tk3.get(&berr, 1));
+        CG_CHECK_CUDA(cudaMemsetAsync(m->bndFaceRef, 0xFF, sizeof(int) * (size_t) nB, st));
+        CG_CHECK_CUDA(cudaMemsetAsync(keys, 0xFF, sizeof(uint64_t) * (size_t) nB, st));
+        CG_CHECK_CUDA(cudaMemsetAsync(berr, 0, sizeof(int), st));
+        k_bnd_maps<<<grid_for(nF, B), B, 0, st>>>(nF, nB, m->faceN2O, s.bnd, m->faceCells, m->bndFaceRef, m->bndFaceInt,
+                                                  (unsigned long long *) keys, berr);
+        CG_LAUNCHED();
+        int hb = 0;
+        CG_CHECK_CUDA(cudaMemcpyAsync(&hb, berr, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CG_CHECK_CUDA(cudaStreamSynchronize(st));
+        if (hb == 0) {
+            CG_TRY(sort_keys(keys, keysOut, nB, 64, st));
+            k_bnd_unkey<<<grid_for(nB, B), B, 0, st>>>(nB, (const unsigned long long *) keysOut, m->cellN2O,
+                                                       m->bndFaceRef, m->bndSorted, m->bndSortedCellInt,
+                                                       m->bndSortedCellRef, berr);
+            CG_LAUNCHED();
+            CG_CHECK_CUDA(cudaMemcpyAsync(&hb, berr, sizeof(int), cudaMemcpyDeviceToHost, st));
+            CG_CHECK_CUDA(cudaStreamSynchronize(st));
+        }
+        m->bndMapsOk = hb == 0;
+    } else {
+        m->bndMapsOk = true;
+    }
+
     // --- numbering bandwidth and the fused pipeline's control words (api.cu)
     CG_TRY(mesh_post_build(m, st));
 
@@ -655,6 +720,8 @@ int build_mesh_from_source(cupcfd_gpu_mesh *m, const Source &s, const cupcfd_mes
     CG_TRY(m->alloc(&m->regionType, 1));
     CG_TRY(m->alloc(&m->regionUVW, 3));
     CG_TRY(m->alloc(&m->regionDen, 1));
+    CG_TRY(m->alloc(&m->regionSplvl, 1));
+    CG_CHECK_CUDA(cudaMemsetAsync(m->regionSplvl, 0, sizeof(double), st));
     CG_CHECK_CUDA(cudaMemsetAsync(m->bndRegion, 0, sizeof(int) * (size_t) std::max(nB, 1), st));
     CG_CHECK_CUDA(cudaMemsetAsync(m->regionType, 0, sizeof(int), st));
     CG_CHECK_CUDA(cudaMemsetAsync(m->regionUVW, 0, 3 * sizeof(double), st));
@@ -849,7 +916,9 @@ extern "C" int cupcfd_gpu_mesh_set_regions(cupcfd_gpu_mesh *m, int32_t nR, const
         CG_TRY(m->alloc(&m->regionType, (size_t) nR));
         CG_TRY(m->alloc(&m->regionUVW, 3 * (size_t) nR));
         CG_TRY(m->alloc(&m->regionDen, (size_t) nR));
+        CG_TRY(m->alloc(&m->regionSplvl, (size_t) nR));
     }
+    CG_CHECK_CUDA(cudaMemsetAsync(m->regionSplvl, 0, sizeof(double) * nR, st));
     CG_CHECK_CUDA(cudaMemcpyAsync(m->regionType, type, sizeof(int) * nR, cudaMemcpyHostToDevice, st));
     CG_CHECK_CUDA(cudaMemcpyAsync(m->regionUVW, uvw, sizeof(double) * 3 * nR, cudaMemcpyHostToDevice, st));
     CG_CHECK_CUDA(cudaMemcpyAsync(m->regionDen, den, sizeof(double) * nR, cudaMemcpyHostToDevice, st));

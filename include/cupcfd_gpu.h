@@ -183,6 +183,11 @@ int cupcfd_gpu_mesh_set_regions(cupcfd_gpu_mesh *mesh, int32_t nRegions, const i
                                 const double *regionUVW, const double *regionDen,
                                 const int32_t *bndRegion, int32_t nBoundaries);
 
+/* Region split levels splvl[nRegions] (replaces getRegionSplvl,
+ * UnstructuredMeshInterface.h:1855-1868), read by the outlet boundary loops;
+ * zero until set, and reset to zero by cupcfd_gpu_mesh_set_regions. */
+int cupcfd_gpu_mesh_set_region_split(cupcfd_gpu_mesh *mesh, int32_t nRegions, const double *splvl);
+
 /* Downloads the cell->face CSR in the reference's numbering (host arrays,
  * xadj[nCells+1], adj[nIncidences]) for bit-exact comparison with
  * CupCfdSoAMesh::cellFaceMapCSRXAdj / cellFaceMapCSRAdj. */
@@ -253,6 +258,38 @@ int cupcfd_gpu_forward_adjoint(cupcfd_gpu_mesh *mesh, int32_t precision,
                                const double *v, const double *w, const double *gface,
                                double *grad, double *massFlux, double *phiBar, double *phiBBar,
                                double *denBar, double *uBar, double *vBar, double *wBar, double *loss);
+
+/* The boundary / region loops of the mass-flux step, FP64, bit-identical to
+ * the reference (MassKernels.h:90-171, MassKernels.ipp:311-554): host
+ * buffers in the reference's numbering (faces, cells, boundary ids, region
+ * ids). Sums run in the reference's boundary order; array lengths below
+ * the mesh's return E_INVALID_INDEX.
+ *   loop1: flowin = sum of massFlux over inlet boundaries
+ *   loop2: flowout = sum over outlets, flowRegion[region] += the same
+ *   loop3: ratearea = -flowin / (outlet area)
+ *   loop4: outlet massFlux = ratearea * area * splvl, outlet velocities
+ *          along the unit normal, flowout = their sum
+ *   loop5: outlet massFlux *= flowFact[region], *flowout2 += it (not reset),
+ *          u/v/wBoundary *= fact where solveU/V/W, su[cell1] -= massFlux
+ *   region loop: flowFact = -(splvl * flowIn) / flowRegion on outlets, else 0 */
+int cupcfd_gpu_flux_mass_dolfyn_boundary_loop1(cupcfd_gpu_mesh *mesh, const double *massFlux, int32_t nMassFlux,
+                                               double *flowin);
+int cupcfd_gpu_flux_mass_dolfyn_boundary_loop2(cupcfd_gpu_mesh *mesh, const double *massFlux, int32_t nMassFlux,
+                                               double *flowRegion, int32_t nFlowRegion, double *flowout);
+int cupcfd_gpu_flux_mass_dolfyn_boundary_loop3(cupcfd_gpu_mesh *mesh, double flowin, double *ratearea);
+int cupcfd_gpu_flux_mass_dolfyn_boundary_loop4(cupcfd_gpu_mesh *mesh, double *massFlux, int32_t nMassFlux,
+                                               double *uBoundary, int32_t nUBoundary, double *vBoundary,
+                                               int32_t nVBoundary, double *wBoundary, int32_t nWBoundary,
+                                               const double *denBoundary, int32_t nDenBoundary, double ratearea,
+                                               double *flowout);
+int cupcfd_gpu_flux_mass_dolfyn_boundary_loop5(cupcfd_gpu_mesh *mesh, double *massFlux, int32_t nMassFlux,
+                                               double *su, int32_t nSu, double *uBoundary, int32_t nUBoundary,
+                                               double *vBoundary, int32_t nVBoundary, double *wBoundary,
+                                               int32_t nWBoundary, double fact, int32_t solveU, int32_t solveV,
+                                               int32_t solveW, const double *flowFact, int32_t nFlowFact,
+                                               double *flowout2);
+int cupcfd_gpu_flux_mass_dolfyn_region_loop(cupcfd_gpu_mesh *mesh, double *flowFact, int32_t nFlowFact,
+                                           const double *flowRegion, int32_t nFlowRegion, double flowIn);
 
 /* ------------------------------------------------------------------------ */
 /* device-resident calls (device pointers, internal numbering, async)        */
@@ -337,6 +374,24 @@ int cupcfd_gpu_dev_forward_adjoint(cupcfd_gpu_mesh *mesh, int32_t precision, con
  * out is a host double[5]; the call synchronises the stream. */
 int cupcfd_gpu_dev_error_norms(const void *a, int32_t a_size, const void *b, int32_t b_size, int64_t n, double floor,
                                double *out, void *stream);
+
+/* The boundary / region loops on device arrays (same semantics as the
+ * host-buffer calls above): massFlux in internal face order, su in internal
+ * cell order, boundary arrays by boundary id and region arrays by region id;
+ * every scalar (flowin, ratearea, flowout, flowout2, flowIn) is a device
+ * double, so the loops chain without synchronising. */
+int cupcfd_gpu_dev_boundary_loop1(cupcfd_gpu_mesh *mesh, const double *massFlux, double *flowin, void *stream);
+int cupcfd_gpu_dev_boundary_loop2(cupcfd_gpu_mesh *mesh, const double *massFlux, double *flowRegion, double *flowout,
+                                  void *stream);
+int cupcfd_gpu_dev_boundary_loop3(cupcfd_gpu_mesh *mesh, const double *flowin, double *ratearea, void *stream);
+int cupcfd_gpu_dev_boundary_loop4(cupcfd_gpu_mesh *mesh, double *massFlux, double *uBoundary, double *vBoundary,
+                                  double *wBoundary, const double *denBoundary, const double *ratearea,
+                                  double *flowout, void *stream);
+int cupcfd_gpu_dev_boundary_loop5(cupcfd_gpu_mesh *mesh, double *massFlux, double *su, double *uBoundary,
+                                  double *vBoundary, double *wBoundary, double fact, int32_t solveU, int32_t solveV,
+                                  int32_t solveW, const double *flowFact, double *flowout2, void *stream);
+int cupcfd_gpu_dev_region_loop(cupcfd_gpu_mesh *mesh, double *flowFact, const double *flowRegion,
+                               const double *flowIn, void *stream);
 
 /* Number of kernels this library launched since load (all threads). */
 int64_t cupcfd_gpu_launch_count(void);
