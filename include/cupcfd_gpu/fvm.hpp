@@ -3,6 +3,7 @@
 // Same names and parameter lists as the reference's templates
 //   cupcfd::fvm::GradientPhiGaussDolfyn  (include/fvm/implementation/component/GradientKernels.h:48-54)
 //   cupcfd::fvm::FluxMassDolfynFaceLoop  (include/fvm/implementation/component/MassKernels.h:48-81)
+//   cupcfd::fvm::FluxMassDolfynBoundaryLoop1-5, FluxMassDolfynRegionLoop (MassKernels.h:90-171)
 // in namespace cupcfd::fvm::gpu, so a call site switches by namespace only:
 //
 //   status = cupcfd::fvm::gpu::GradientPhiGaussDolfyn(mesh, nGradient, phiCell, nPhiCell,
@@ -145,6 +146,12 @@ int upload(Mesh &mesh, cupcfd_gpu_mesh **out) {
         }
         for (int b = 0; b < nB; b++) br[b] = (int32_t) mesh.getBoundaryRegionID(b);
         rc = cupcfd_gpu_mesh_set_regions(*out, nR, rt.data(), uvw.data(), den.data(), br.data(), nB);
+        if (rc == CUPCFD_E_SUCCESS) {
+            // split levels (getRegionSplvl), read by the outlet boundary loops
+            std::vector<double> sp(nR);
+            for (int r = 0; r < nR; r++) sp[r] = (double) mesh.getRegionSplvl(r);
+            rc = cupcfd_gpu_mesh_set_region_split(*out, nR, sp.data());
+        }
         if (rc != CUPCFD_E_SUCCESS) {
             cupcfd_gpu_mesh_destroy(*out);
             *out = nullptr;
@@ -221,6 +228,70 @@ ecode_t FluxMassDolfynFaceLoop(Mesh &mesh, Vec *dudx, I nDudx, Vec *dvdx, I nDvd
         solveEnthalpy, teCell, nTeCell, teBoundary, nTeBoundary, edCell, nEdCell, edBoundary, nEdBoundary,
         viseffCell, nViseffCell, viseffBoundary, nViseffBoundary, tCell, nTCell, tBoundary, nTBoundary);
     return (ecode_t) rc;
+}
+
+// FluxMassDolfynBoundaryLoop1-5 and FluxMassDolfynRegionLoop (MassKernels.h:90-171), T = double.
+// Region types and split levels are those read when the mesh was attached.
+template <class Mesh, class I>
+ecode_t FluxMassDolfynBoundaryLoop1(Mesh &mesh, double *massFlux, I nMassFlux, double *flowin) {
+    cupcfd_gpu_mesh *m = nullptr;
+    int rc = attach(mesh, &m);
+    if (rc != CUPCFD_E_SUCCESS) return (ecode_t) rc;
+    return (ecode_t) cupcfd_gpu_flux_mass_dolfyn_boundary_loop1(m, massFlux, (int32_t) nMassFlux, flowin);
+}
+
+template <class Mesh, class I>
+ecode_t FluxMassDolfynBoundaryLoop2(Mesh &mesh, double *massFlux, I nMassFlux, double *flowRegion, I nFlowRegion,
+                                    double *flowout) {
+    cupcfd_gpu_mesh *m = nullptr;
+    int rc = attach(mesh, &m);
+    if (rc != CUPCFD_E_SUCCESS) return (ecode_t) rc;
+    return (ecode_t) cupcfd_gpu_flux_mass_dolfyn_boundary_loop2(m, massFlux, (int32_t) nMassFlux, flowRegion,
+                                                                (int32_t) nFlowRegion, flowout);
+}
+
+template <class Mesh>
+ecode_t FluxMassDolfynBoundaryLoop3(Mesh &mesh, double flowin, double *ratearea) {
+    cupcfd_gpu_mesh *m = nullptr;
+    int rc = attach(mesh, &m);
+    if (rc != CUPCFD_E_SUCCESS) return (ecode_t) rc;
+    return (ecode_t) cupcfd_gpu_flux_mass_dolfyn_boundary_loop3(m, flowin, ratearea);
+}
+
+template <class Mesh, class I>
+ecode_t FluxMassDolfynBoundaryLoop4(Mesh &mesh, double *massFlux, I nMassFlux, double *uBoundary, I nUBoundary,
+                                    double *vBoundary, I nVboundary, double *wBoundary, I nWBoundary,
+                                    double *denBoundary, I nDenBoundary, double ratearea, double *flowout) {
+    cupcfd_gpu_mesh *m = nullptr;
+    int rc = attach(mesh, &m);
+    if (rc != CUPCFD_E_SUCCESS) return (ecode_t) rc;
+    return (ecode_t) cupcfd_gpu_flux_mass_dolfyn_boundary_loop4(
+        m, massFlux, (int32_t) nMassFlux, uBoundary, (int32_t) nUBoundary, vBoundary, (int32_t) nVboundary, wBoundary,
+        (int32_t) nWBoundary, denBoundary, (int32_t) nDenBoundary, ratearea, flowout);
+}
+
+template <class Mesh, class I>
+ecode_t FluxMassDolfynBoundaryLoop5(Mesh &mesh, double *massFlux, I nMassFlux, double *su, I nSu, double *uBoundary,
+                                    I nUBoundary, double *vBoundary, I nVBoundary, double *wBoundary, I nWBoundary,
+                                    double fact, bool solveU, bool solveV, bool solveW, double *flowFact,
+                                    I nFlowFact, double *flowout2) {
+    cupcfd_gpu_mesh *m = nullptr;
+    int rc = attach(mesh, &m);
+    if (rc != CUPCFD_E_SUCCESS) return (ecode_t) rc;
+    return (ecode_t) cupcfd_gpu_flux_mass_dolfyn_boundary_loop5(
+        m, massFlux, (int32_t) nMassFlux, su, (int32_t) nSu, uBoundary, (int32_t) nUBoundary, vBoundary,
+        (int32_t) nVBoundary, wBoundary, (int32_t) nWBoundary, fact, solveU, solveV, solveW, flowFact,
+        (int32_t) nFlowFact, flowout2);
+}
+
+template <class Mesh, class I>
+ecode_t FluxMassDolfynRegionLoop(Mesh &mesh, double *flowFact, I nFlowFact, double *flowRegion, I nFlowRegion,
+                                 double flowIn) {
+    cupcfd_gpu_mesh *m = nullptr;
+    int rc = attach(mesh, &m);
+    if (rc != CUPCFD_E_SUCCESS) return (ecode_t) rc;
+    return (ecode_t) cupcfd_gpu_flux_mass_dolfyn_region_loop(m, flowFact, (int32_t) nFlowFact, flowRegion,
+                                                            (int32_t) nFlowRegion, flowIn);
 }
 
 }  // namespace gpu

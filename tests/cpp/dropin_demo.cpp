@@ -87,6 +87,12 @@ int main(int argc, char **argv) {
     mesh.properties = {nC, 0, nC, nF, nB, nR};
     mesh.a = {c1.data(), c2.data(), bnd.data(), lam.data(), S.data(), X.data(), area.data(), Z.data(), Z.data(),
               C.data(), vol.data(), breg.data(), rtype.data(), ruvw.data(), rden.data()};
+    std::vector<int> bface(nB);  // getBoundaryFaceID
+    for (int f = 0; f < nF; f++)
+        if (bnd[f] > -1) bface[bnd[f]] = f;
+    std::vector<double> splvl = {0.5, 0.75, 0.25, 1.0};  // getRegionSplvl
+    mesh.a.boundaryFace = bface.data();
+    mesh.a.regionSplvl = splvl.data();
 
     std::mt19937_64 rng(20261203);
     std::uniform_real_distribution<double> U(-1.0, 1.0);
@@ -137,8 +143,51 @@ int main(int argc, char **argv) {
         return fail("mass flux differs from the reference");
     for (int k = 0; k < 4; k++)
         if (o[0].c[k] != o[1].c[k]) return fail("region counters differ");
+
+    // ---- FluxMassDolfynBoundaryLoop1-5 and FluxMassDolfynRegionLoop (outlet region 1, inlet region 0)
+    {
+        namespace ref = cupcfd::fvm;
+        namespace g = cupcfd::fvm::gpu;
+        std::vector<double> mf0(nF);
+        for (auto &x : mf0) x = U(rng) * 1e-2;
+        double fin[2], rate[2], fo4[2], fo2[2], fo5[2] = {0.125, 0.125};
+        std::vector<double> mf[2] = {mf0, mf0}, ub[2], vb[2], wb[2], fr[2], ff[2], s5[2];
+        std::vector<double> denb(nB);
+        for (auto &x : denb) x = 1.0 + 0.1 * U(rng);
+        for (int r = 0; r < 2; r++) {
+            ub[r].assign(nB, 0.01); vb[r].assign(nB, 0.02); wb[r].assign(nB, 0.03);
+            fr[r].assign(nR, 0.001); ff[r].assign(nR, -1.0); s5[r].assign(nC, 0.5);
+        }
+        cupcfd::error::eCodes st[2][6];
+        st[0][0] = ref::FluxMassDolfynBoundaryLoop1(mesh, mf[0].data(), nF, &fin[0]);
+        st[1][0] = g::FluxMassDolfynBoundaryLoop1(mesh, mf[1].data(), nF, &fin[1]);
+        st[0][1] = ref::FluxMassDolfynBoundaryLoop3(mesh, fin[0], &rate[0]);
+        st[1][1] = g::FluxMassDolfynBoundaryLoop3(mesh, fin[1], &rate[1]);
+        st[0][2] = ref::FluxMassDolfynBoundaryLoop4(mesh, mf[0].data(), nF, ub[0].data(), nB, vb[0].data(), nB,
+                                                    wb[0].data(), nB, denb.data(), nB, rate[0], &fo4[0]);
+        st[1][2] = g::FluxMassDolfynBoundaryLoop4(mesh, mf[1].data(), nF, ub[1].data(), nB, vb[1].data(), nB,
+                                                  wb[1].data(), nB, denb.data(), nB, rate[1], &fo4[1]);
+        st[0][3] = ref::FluxMassDolfynBoundaryLoop2(mesh, mf[0].data(), nF, fr[0].data(), nR, &fo2[0]);
+        st[1][3] = g::FluxMassDolfynBoundaryLoop2(mesh, mf[1].data(), nF, fr[1].data(), nR, &fo2[1]);
+        st[0][4] = ref::FluxMassDolfynRegionLoop(mesh, ff[0].data(), nR, fr[0].data(), nR, fin[0]);
+        st[1][4] = g::FluxMassDolfynRegionLoop(mesh, ff[1].data(), nR, fr[1].data(), nR, fin[1]);
+        st[0][5] = ref::FluxMassDolfynBoundaryLoop5(mesh, mf[0].data(), nF, s5[0].data(), nC, ub[0].data(), nB,
+                                                    vb[0].data(), nB, wb[0].data(), nB, 1.25, true, false, true,
+                                                    ff[0].data(), nR, &fo5[0]);
+        st[1][5] = g::FluxMassDolfynBoundaryLoop5(mesh, mf[1].data(), nF, s5[1].data(), nC, ub[1].data(), nB,
+                                                  vb[1].data(), nB, wb[1].data(), nB, 1.25, true, false, true,
+                                                  ff[1].data(), nR, &fo5[1]);
+        for (int k = 0; k < 6; k++)
+            if (st[0][k] != cupcfd::error::E_SUCCESS || st[1][k] != cupcfd::error::E_SUCCESS)
+                return fail("boundary loop status");
+        if (!(fin[0] == fin[1] && rate[0] == rate[1] && fo4[0] == fo4[1] && fo2[0] == fo2[1] && fo5[0] == fo5[1]))
+            return fail("boundary loop scalars differ from the reference");
+        if (mf[0] != mf[1] || ub[0] != ub[1] || vb[0] != vb[1] || wb[0] != wb[1] || fr[0] != fr[1] || ff[0] != ff[1] ||
+            s5[0] != s5[1])
+            return fail("boundary loop arrays differ from the reference");
+    }
     cupcfd::fvm::gpu::release(mesh);
-    std::printf("OK dropin %dx%dx%d: %d cells, %d faces; gradient (nGradient 1-3) and mass flux bit-identical\n", nx,
-                ny, nz, nC, nF);
+    std::printf("OK dropin %dx%dx%d: %d cells, %d faces; gradient (nGradient 1-3), mass flux and the boundary / "
+                "region loops bit-identical\n", nx, ny, nz, nC, nF);
     return 0;
 }
