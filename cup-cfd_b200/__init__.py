@@ -33,6 +33,8 @@ E_SUCCESS = 95
 E_ERROR = 98
 E_NULL_PTR = 99
 E_NOT_IMPLEMENTED = 109
+E_FILE_MISSING = 10
+E_INVALID_FILE_FORMAT = 105
 
 RTYPE_DEFAULT, RTYPE_INLET, RTYPE_OUTLET, RTYPE_SYMP, RTYPE_WALL = range(5)
 PREC_F64, PREC_F32C = 0, 1
@@ -83,6 +85,8 @@ SIGNATURES = {
     "cupcfd_gpu_mesh_create_structgen": ([_I, _I, _I, _VP, _VP, _VP], _I),
     "cupcfd_gpu_mesh_create_jittered": ([_I, _I, _I, _D, C.c_uint64, _I, _VP, _VP], _I),
     "cupcfd_gpu_mesh_destroy": ([_VP], _I),
+    "cupcfd_gpu_mesh_save": ([_VP, C.c_char_p], _I),
+    "cupcfd_gpu_mesh_load": ([C.c_char_p, _VP, _VP], _I),
     "cupcfd_gpu_mesh_get_info": ([_VP, _VP], _I),
     "cupcfd_gpu_mesh_set_regions": ([_VP, _I, _VP, _VP, _VP, _VP, _I], _I),
     "cupcfd_gpu_mesh_set_region_split": ([_VP, _I, _VP], _I),
@@ -267,6 +271,24 @@ class Mesh:
             return rc, (cls(h) if rc == E_SUCCESS else None)
         check(rc)
         return cls(h)
+
+    @classmethod
+    def load(cls, path, order=ORDER_MORTON, precisions=(1 << PREC_F64) | (1 << PREC_F32C), device=-1,
+             return_code=False):
+        """Rebuild a mesh saved by ``save`` (geometry, regions, split levels)
+        with the given layout options."""
+        h = C.c_void_p()
+        o = cls._opts(order, precisions, device)
+        rc = lib().cupcfd_gpu_mesh_load(os.fsencode(path), C.byref(o), C.byref(h))
+        if return_code:
+            return rc, (cls(h) if rc == E_SUCCESS else None)
+        check(rc)
+        return cls(h)
+
+    def save(self, path):
+        """Write the mesh's source arrays, regions and split levels to a
+        raw-binary mesh file (format in include/cupcfd_gpu.h)."""
+        return lib().cupcfd_gpu_mesh_save(self.h, os.fsencode(path))
 
     def close(self):
         if getattr(self, "h", None):

@@ -43,6 +43,8 @@ extern "C" {
 #define CUPCFD_E_ERROR 98               /* E_ERROR, Error.h:132 */
 #define CUPCFD_E_NULL_PTR 99            /* E_NULL_PTR, Error.h:133 */
 #define CUPCFD_E_NOT_IMPLEMENTED 109    /* E_NOT_IMPLEMENTED, Error.h:143 */
+#define CUPCFD_E_FILE_MISSING 10        /* E_FILE_MISSING, Error.h:44 */
+#define CUPCFD_E_INVALID_FILE_FORMAT 105 /* E_INVALID_FILE_FORMAT, Error.h:139 */
 
 /* ---- region types: cupcfd::geometry::mesh::RType (UnstructuredMeshInterface.h:58-65) ---- */
 #define CUPCFD_RTYPE_DEFAULT 0
@@ -159,6 +161,25 @@ int cupcfd_gpu_mesh_create_structgen(int32_t nx, int32_t ny, int32_t nz, const d
  * counterpart (the reference reads such meshes from HDF5, MeshHDF5Source.cpp). */
 int cupcfd_gpu_mesh_create_jittered(int32_t nx, int32_t ny, int32_t nz, double jitter, uint64_t seed, int32_t permute,
                                     const cupcfd_mesh_options *opt, cupcfd_gpu_mesh **out);
+
+/* Mesh files. The reference ingests meshes through MeshHDF5Source
+ * (src/geometry/mesh/implementation/source/MeshHDF5Source.cpp); HDF5 is not
+ * part of this build, so a device mesh is saved to, and reloaded from, a
+ * raw-binary file holding its source arrays in the reference's numbering:
+ * a 64-byte header (magic "CUPCFDM1", version 1, nCells, nFaces,
+ * nBoundaries, nRegions, flags bit 0 = xpac/xnac present), then faceCell1,
+ * faceCell2, faceBnd (int32), faceLambda, faceArea, faceNorm[3],
+ * faceCenter[3], [faceXpac[3], faceXnac[3]], cellCenter[3], cellVolume
+ * (float64), regionType (int32), regionUVW[3], regionDen, regionSplvl
+ * (float64), bndRegion (int32), and an FNV-1a 64-bit hash of all the bytes
+ * before it. Little-endian. Loading rebuilds the device layout exactly as
+ * cupcfd_gpu_mesh_create with `opt`, then installs the regions and split
+ * levels, so kernels on a loaded mesh give the saved mesh's bits.
+ * Errors: CUPCFD_E_FILE_MISSING (cannot open), CUPCFD_E_INVALID_FILE_FORMAT
+ * (magic, version, header ranges, size, truncation or hash wrong), as the
+ * reference's readers return (Error.h:44, Error.h:139). */
+int cupcfd_gpu_mesh_save(const cupcfd_gpu_mesh *mesh, const char *path);
+int cupcfd_gpu_mesh_load(const char *path, const cupcfd_mesh_options *opt, cupcfd_gpu_mesh **out);
 
 int cupcfd_gpu_mesh_destroy(cupcfd_gpu_mesh *mesh);
 int cupcfd_gpu_mesh_get_info(const cupcfd_gpu_mesh *mesh, cupcfd_mesh_info *info);

@@ -96,6 +96,8 @@ def test_error_codes_match_reference_enum():
     assert ref.ref_ecode_error() == O.E_ERROR == 98
     assert ref.ref_ecode_null_ptr() == 99
     assert ref.ref_ecode_not_implemented() == 109
+    assert ref.ref_ecode_file_missing() == 10
+    assert ref.ref_ecode_invalid_file_format() == 105
     # EuclideanVector<T,3> carries a vptr: 32-byte (double) / 24-byte (float) stride, components at +8
     assert ref.ref_sizeof_euclidean_vector_f64() == 32
     assert ref.ref_sizeof_euclidean_vector_f32() == 24
