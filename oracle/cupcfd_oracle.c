@@ -783,3 +783,172 @@ int orc_region_loop(const orc_mesh *m, const double *splvl, double *flowFact, co
     }
     return ORC_E_SUCCESS;
 }
+
+/* ------------------------------------------------------------------------- */
+/* Momentum face loop (include/fvm/implementation/component/UVWKernels.ipp)  */
+/* ------------------------------------------------------------------------- */
+
+/* std::min / std::max as <algorithm> defines them: min(a,b) = b < a ? b : a,
+ * max(a,b) = a < b ? b : a (the first argument wins ties and NaN compares). */
+static double std_min(double a, double b) { return (b < a) ? b : a; }
+static double std_max(double a, double b) { return (a < b) ? b : a; }
+
+/* EuclideanVector::normalise (EuclideanVector.cpp:100-109) */
+static void normalise3(double *x) {
+    double len = sqrt(dot3(x, x));
+    if (len != 0.0) {
+        double sc = 1.0 / len;
+        x[0] *= sc; x[1] *= sc; x[2] *= sc;
+    }
+}
+
+/* FluxUVWDolfynFaceLoop1 (UVWKernels.ipp:38-515), face by face in label
+ * order. uFace/vFace/wFace and visFace are declared outside the face loop
+ * (UVWKernels.ipp:74-75) and carry from one face to the next: interior faces
+ * read the uFace the last inlet or outlet face set (the interpolation that
+ * would set it is commented out, UVWKernels.ipp:165-168, read at :171), symmetry faces read
+ * the visFace the last interior, inlet or outlet face set. The reference
+ * leaves them uninitialised; here they start at 0. rlencos[nFaces] and
+ * bndDist[nBnd] stand for getFaceRLencos / getBoundaryDistance (NULL reads 0,
+ * as every MeshSource-built mesh holds, UnstructuredMeshInterface.ipp:1809-1810,
+ * MeshStructGenSource.cpp:1251-1258); shear[3*nBnd] receives setBoundaryShear
+ * (wall faces only). Vector fields are xyz-interleaved [3*nCells]. */
+int orc_uvw_face_loop1(const orc_mesh *m, const double *rlencos, const double *bndDist, double gammaBlend, double small,
+                       const double *u, const double *v, const double *w, double *uB, double *vB, double *wB,
+                       const double *visC, const double *visB, double *massFlux,
+                       const double *dudx, const double *dvdx, const double *dwdx, double *rFace,
+                       double *su, double *sv, double *sw, double *au, double *av, double *aw, double *shear) {
+    double uFace = 0.0, vFace = 0.0, wFace = 0.0, visFace = 0.0;
+    for (int i = 0; i < m->nFaces; i++) {
+        int ip = m->faceCell1[i];
+        const double *S = m->faceNorm + 3 * i;
+        double rl = rlencos ? rlencos[i] : 0.0;
+        if (m->faceBnd[i] < 0) {
+            int in = m->faceCell2[i];
+            double facn = m->faceLambda[i];
+            double facp = 1.0 - facn;
+            double du[3], dv[3], dw[3], xpn[3];
+            for (int d = 0; d < 3; d++) {
+                du[d] = dudx[3 * in + d] * facn + dudx[3 * ip + d] * facp;
+                dv[d] = dvdx[3 * in + d] * facn + dvdx[3 * ip + d] * facp;
+                dw[d] = dwdx[3 * in + d] * facn + dwdx[3 * ip + d] * facp;
+            }
+            double visac = visC[in] * facn + visC[ip] * facp;
+            sub3(m->cellCenter + 3 * in, m->cellCenter + 3 * ip, xpn);
+            visFace = visac * rl;
+            double mf = massFlux[i];
+            double fuce = mf * uFace, fvce = mf * vFace, fwce = mf * wFace;
+            double fude1 = (du[0] + du[0]) * S[0] + (du[1] + dv[0]) * S[1] + (du[2] + dw[0]) * S[2];
+            double fvde1 = (du[1] + dv[0]) * S[0] + (dv[1] + dv[1]) * S[1] + (dv[2] + dw[1]) * S[2];
+            double fwde1 = (du[2] + dw[0]) * S[0] + (dw[1] + dv[2]) * S[1] + (dw[2] + dw[2]) * S[2];
+            double fude = visac * fude1, fvde = visac * fvde1, fwde = visac * fwde1;
+            double fmin = std_min(mf, 0.0), fmax = std_max(mf, 0.0);
+            double fuci = fmin * u[in] + fmax * u[ip];
+            double fvci = fmin * v[in] + fmax * v[ip];
+            double fwci = fmin * w[in] + fmax * w[ip];
+            double fudi = visFace * dot3(du, xpn), fvdi = visFace * dot3(dv, xpn), fwdi = visFace * dot3(dw, xpn);
+            rFace[2 * i] = -visFace - std_max(mf, 0.0);
+            rFace[2 * i + 1] = -visFace + std_min(mf, 0.0);
+            double bu = gammaBlend * (fuce - fuci), bv = gammaBlend * (fvce - fvci), bw = gammaBlend * (fwce - fwci);
+            su[ip] = su[ip] - bu + fude - fudi;
+            su[in] = su[in] + bu - fude + fudi;
+            sv[ip] = sv[ip] - bv + fvde - fvdi;
+            sv[in] = sv[in] + bv - fvde + fvdi;
+            sw[ip] = sw[ip] - bw + fwde - fwdi;
+            sw[in] = sw[in] + bw - fwde + fwdi;
+            continue;
+        }
+        int ib = m->faceBnd[i], ir = m->bndRegion[ib], it = m->regionType[ir];
+        const double *X = m->faceCenter + 3 * i;
+        const double *du = dudx + 3 * ip, *dv = dvdx + 3 * ip, *dw = dwdx + 3 * ip;
+        double xpn[3];
+        sub3(X, m->cellCenter + 3 * ip, xpn);
+        if (it == ORC_RTYPE_INLET || it == ORC_RTYPE_OUTLET) {
+            double visac, fvde, fwde;
+            double fude = (du[0] + du[0]) * S[0] + (du[1] + dv[0]) * S[1] + (du[2] + dw[0]) * S[2];
+            if (it == ORC_RTYPE_INLET) {   /* UVWKernels.ipp:259-319 */
+                uFace = m->regionUVW[3 * ir]; vFace = m->regionUVW[3 * ir + 1]; wFace = m->regionUVW[3 * ir + 2];
+                visac = visB[ib];
+                fvde = (du[1] + dv[0]) * S[0] + (dv[1] + dv[1]) * S[1] + (dv[2] + dw[1]) * S[2];
+                fwde = (du[2] + dw[0]) * S[0] + (dw[1] + dv[2]) * S[1] + (dw[2] + dw[2]) * S[2];
+            } else {                       /* UVWKernels.ipp:320-382 */
+                visac = visC[ip];
+                uFace = u[ip]; vFace = v[ip]; wFace = w[ip];
+                fvde = (dv[0] + du[1]) * S[0] + (dv[1] + dv[1]) * S[1] + (dv[2] + dw[1]) * S[2];
+                fwde = (dw[0] + du[2]) * S[0] + (dw[1] + dv[2]) * S[1] + (dw[2] + dw[2]) * S[2];
+            }
+            visFace = visac * rl;
+            fude = visac * fude; fvde = visac * fvde; fwde = visac * fwde;
+            double fudi = visFace * dot3(du, xpn), fvdi = visFace * dot3(dv, xpn), fwdi = visFace * dot3(dw, xpn);
+            if (it == ORC_RTYPE_OUTLET && massFlux[i] < 0.0) massFlux[i] = small;
+            double f = -visFace + std_min(massFlux[i], 0.0);
+            au[ip] = au[ip] - f;
+            su[ip] = su[ip] - f * uFace + fude - fudi;
+            uB[ib] = uFace;
+            av[ip] = av[ip] - f;
+            sv[ip] = sv[ip] - f * vFace + fvde - fvdi;
+            vB[ib] = vFace;
+            aw[ip] = aw[ip] - f;
+            sw[ip] = sw[ip] - f * wFace + fwde - fwdi;
+            wB[ib] = wFace;
+        } else if (it == ORC_RTYPE_SYMP) { /* UVWKernels.ipp:383-436; visFace carried, :424 */
+            double visac = visC[ip];
+            double us[3] = {u[ip] + dot3(du, xpn), v[ip] + dot3(dv, xpn), w[ip] + dot3(dw, xpn)};
+            double xn[3] = {0.0 - S[0], 0.0 - S[1], 0.0 - S[2]};
+            normalise3(xn);
+            double dp = dot3(us, xn);
+            double dn = bndDist ? bndDist[ib] : 0.0;
+            double force[3];
+            for (int d = 0; d < 3; d++) force[d] = (2.0 * visac * (dp * xn[d]) / dn) * m->faceArea[i];
+            au[ip] = au[ip] + visFace;
+            av[ip] = av[ip] + visFace;
+            aw[ip] = aw[ip] + visFace;
+            su[ip] = su[ip] + visFace * u[ip] - force[0];
+            sv[ip] = sv[ip] + visFace * v[ip] - force[1];
+            sw[ip] = sw[ip] + visFace * w[ip] - force[2];
+            uB[ib] = us[0]; vB[ib] = us[1]; wB[ib] = us[2];
+        } else if (it == ORC_RTYPE_WALL) { /* UVWKernels.ipp:437-510 */
+            const double *uw = m->regionUVW + 3 * ir;
+            double visac = visB[ib];
+            double coef = visac * m->faceArea[i] / sqrt(dot3(xpn, xpn));
+            double xn[3] = {S[0], S[1], S[2]};
+            normalise3(xn);
+            double up[3] = {u[ip] - uw[0], v[ip] - uw[1], w[ip] - uw[2]};
+            double dp = dot3(up, xn);
+            double ut[3] = {up[0] - dp * xn[0], up[1] - dp * xn[1], up[2] - dp * xn[2]};
+            double uvel = fabs(ut[0]) + fabs(ut[1]) + fabs(ut[2]);
+            double force[3] = {0.0, 0.0, 0.0};
+            if (uvel > small) {
+                double dn = bndDist ? bndDist[ib] : 0.0;
+                for (int d = 0; d < 3; d++) force[d] = (visac * ut[d] / dn) * m->faceArea[i];
+            }
+            for (int d = 0; d < 3; d++) shear[3 * ib + d] = force[d];
+            au[ip] = au[ip] + coef;
+            av[ip] = av[ip] + coef;
+            aw[ip] = aw[ip] + coef;
+            su[ip] = su[ip] + coef * u[ip] - force[0];
+            sv[ip] = sv[ip] + coef * v[ip] - force[1];
+            sw[ip] = sw[ip] + coef * w[ip] - force[2];
+            uB[ib] = uw[0]; vB[ib] = uw[1]; wB[ib] = uw[2];
+        }
+    }
+    return ORC_E_SUCCESS;
+}
+
+/* FluxUVWDolfynRegionLoop1 (UVWKernels.ipp:517-524): every region's force
+ * tangent set to zero. */
+int orc_uvw_region_loop1(const orc_mesh *m, double *forceTangent) {
+    for (int r = 0; r < 3 * m->nRegions; r++) forceTangent[r] = 0.0;
+    return ORC_E_SUCCESS;
+}
+
+/* FluxUVWDolfynBndsLoop1 (UVWKernels.ipp:527-544): wall boundaries add their
+ * shear onto their region's force tangent, in boundary order. */
+int orc_uvw_bnds_loop1(const orc_mesh *m, const double *shear, double *forceTangent) {
+    for (int ib = 0; ib < m->nBnd; ib++) {
+        int ir = m->bndRegion[ib];
+        if (m->regionType[ir] != ORC_RTYPE_WALL) continue;
+        for (int d = 0; d < 3; d++) forceTangent[3 * ir + d] = forceTangent[3 * ir + d] + shear[3 * ib + d];
+    }
+    return ORC_E_SUCCESS;
+}

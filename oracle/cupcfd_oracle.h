@@ -97,6 +97,19 @@ int orc_boundary_loop4(const orc_mesh *m, const double *splvl, double *massFlux,
 int orc_boundary_loop5(const orc_mesh *m, double *massFlux, double *su, double *uB, double *vB, double *wB, double fact,
                        int solveU, int solveV, int solveW, const double *flowFact, double *flowout2);
 int orc_region_loop(const orc_mesh *m, const double *splvl, double *flowFact, const double *flowRegion, double flowIn);
+/* ---- momentum face loop (UVWKernels.ipp:38-544) ----
+ * rlencos[nFaces] / bndDist[nBnd] stand for getFaceRLencos /
+ * getBoundaryDistance (NULL = all zero, as MeshSource-built meshes hold);
+ * shear[3*nBnd] receives setBoundaryShear; forceTangent[3*nRegions] stands
+ * for the region force tangents. The carried face values the reference
+ * leaves uninitialised start at 0. */
+int orc_uvw_face_loop1(const orc_mesh *m, const double *rlencos, const double *bndDist, double gammaBlend, double small,
+                       const double *u, const double *v, const double *w, double *uB, double *vB, double *wB,
+                       const double *visC, const double *visB, double *massFlux,
+                       const double *dudx, const double *dvdx, const double *dwdx, double *rFace,
+                       double *su, double *sv, double *sw, double *au, double *av, double *aw, double *shear);
+int orc_uvw_region_loop1(const orc_mesh *m, double *forceTangent);
+int orc_uvw_bnds_loop1(const orc_mesh *m, const double *shear, double *forceTangent);
 int orc_mass_plain_forward(const orc_mesh *m, const double *den, const double *u, const double *v, const double *w,
                            double *massFlux);
 int orc_mass_plain_adjoint(const orc_mesh *m, const double *den, const double *u, const double *v, const double *w,

@@ -58,6 +58,7 @@ def load():
             _lib.orc_boundary_loop4.argtypes = [C.c_void_p] * 7 + [C.c_double, C.c_void_p]
             _lib.orc_boundary_loop5.argtypes = [C.c_void_p] * 6 + [C.c_double] + [C.c_int] * 3 + [C.c_void_p] * 2
             _lib.orc_region_loop.argtypes = [C.c_void_p] * 4 + [C.c_double]
+            _lib.orc_uvw_face_loop1.argtypes = [C.c_void_p] * 3 + [C.c_double] * 2 + [C.c_void_p] * 20
         return _lib
 
 
@@ -85,6 +86,11 @@ def load_ref():
                 _ref.ref_boundary_loop4.argtypes = [C.c_void_p] * 6 + [C.c_double, C.c_void_p]
                 _ref.ref_boundary_loop5.argtypes = [C.c_void_p] * 6 + [C.c_double] + [C.c_int] * 3 + [C.c_void_p] * 2
                 _ref.ref_region_loop.argtypes = [C.c_void_p] * 3 + [C.c_double]
+                _ref.ref_ctx_set_uvw_geometry.argtypes = [C.c_void_p] * 3
+                _ref.ref_uvw_state.argtypes = [C.c_void_p] * 5
+                _ref.ref_uvw_face_loop1.argtypes = [C.c_void_p, C.c_double, C.c_double] + [C.c_void_p] * 19 + [C.c_int, C.c_void_p]
+                _ref.ref_uvw_region_loop1.argtypes = [C.c_void_p]
+                _ref.ref_uvw_bnds_loop1.argtypes = [C.c_void_p]
         return _ref
 
 
@@ -377,6 +383,41 @@ class RefKernels:
         out.update(icinl=cnt[0].value, icout=cnt[1].value, icsym=cnt[2].value, icwal=cnt[3].value)
         return rc, out, secs
 
+    # momentum loops, the reference templates called unchanged
+    def uvw_geometry(self, rlencos=None, bnd_dist=None):
+        self._rl = None if rlencos is None else np.ascontiguousarray(rlencos, np.float64)
+        self._bd = None if bnd_dist is None else np.ascontiguousarray(bnd_dist, np.float64)
+        self.ref.ref_ctx_set_uvw_geometry(self.h, _p(self._rl), _p(self._bd))
+        return self
+
+    def uvw_face_loop1(self, f, reps=1):
+        out = {k: _f64(f[k]) for k in UVW_INOUT}
+        a = {k: np.ascontiguousarray(f[k], np.float64) for k in ("u", "v", "w", "visC", "visB", "dudx", "dvdx", "dwdx")}
+        secs = np.empty(reps)
+        rc = self.ref.ref_uvw_face_loop1(
+            self.h, float(f["gammaBlend"]), float(f["small"]), _p(a["u"]), _p(a["v"]), _p(a["w"]), _p(out["uB"]),
+            _p(out["vB"]), _p(out["wB"]), _p(a["visC"]), _p(a["visB"]), _p(out["massFlux"]), _p(a["dudx"]),
+            _p(a["dvdx"]), _p(a["dwdx"]), _p(out["rFace"]), *[_p(out[k]) for k in ("su", "sv", "sw", "au", "av", "aw")],
+            reps, _p(secs))
+        out["shear"] = self.uvw_state()[0]
+        return rc, out, secs
+
+    def uvw_state(self, shear=None, force_tangent=None):
+        """Set (when given) and return (shear [nBnd,3], force tangent [nRegions,3])."""
+        sh_in = None if shear is None else np.ascontiguousarray(shear, np.float64)
+        ft_in = None if force_tangent is None else np.ascontiguousarray(force_tangent, np.float64)
+        sh, ft = np.empty((self.m["nBnd"], 3)), np.empty((self.m["nRegions"], 3))
+        self.ref.ref_uvw_state(self.h, _p(sh_in), _p(ft_in), _p(sh), _p(ft))
+        return sh, ft
+
+    def uvw_region_loop1(self):
+        self.ref.ref_uvw_region_loop1(self.h)
+        return self.uvw_state()[1]
+
+    def uvw_bnds_loop1(self):
+        self.ref.ref_uvw_bnds_loop1(self.h)
+        return self.uvw_state()[1]
+
     # boundary / region loops, the reference templates called unchanged
     def boundary_loops(self, splvl):
         self._splvl = np.ascontiguousarray(splvl, np.float64)
@@ -424,6 +465,56 @@ class RefKernels:
 # ---------------------------------------------------------------------------
 # seeded synthetic fields (Philox4x32-10 via numpy)
 # ---------------------------------------------------------------------------
+
+# momentum face loop: in/out arrays of FluxUVWDolfynFaceLoop1 (UVWKernels.h:45-67)
+UVW_INOUT = ("massFlux", "rFace", "su", "sv", "sw", "au", "av", "aw", "uB", "vB", "wB")
+
+
+def uvw_fields(m, seed):
+    """Inputs of the momentum face loop drawn as the reference's benchmark
+    draws them (U[1e-6, 1e-2], BenchmarkKernels.cpp:751-815), with signed mass
+    fluxes (both upwind branches, the outlet clamp) and seeded velocity
+    gradients ~ 1e-2 N(0,1) (the benchmark leaves them unset). rFace starts
+    random so untouched entries are checked."""
+    nc, nf, nb = m["nCells"], m["nFaces"], m["nBnd"]
+    r = np.random.Generator(np.random.Philox(key=seed))
+    U = lambda n: r.uniform(1e-6, 1e-2, n)
+    f = dict(u=U(nc), v=U(nc), w=U(nc), visC=U(nc), massFlux=U(nf) * r.choice([-1.0, 1.0], nf),
+             su=U(nc), sv=U(nc), sw=U(nc), au=U(nc), av=U(nc), aw=U(nc), uB=U(nb), vB=U(nb), wB=U(nb), visB=U(nb),
+             dudx=1e-2 * r.standard_normal((nc, 3)), dvdx=1e-2 * r.standard_normal((nc, 3)),
+             dwdx=1e-2 * r.standard_normal((nc, 3)), rFace=r.standard_normal(2 * nf), gammaBlend=0.9, small=1e-18)
+    return f
+
+
+def uvw_face_loop1(m, f, rlencos=None, bnd_dist=None):
+    """FluxUVWDolfynFaceLoop1 (C restatement). Returns the in/out arrays after
+    the call plus the boundary shear [nBnd, 3]."""
+    out = {k: _f64(f[k]) for k in UVW_INOUT}
+    out["shear"] = np.zeros((m["nBnd"], 3))
+    a = {k: np.ascontiguousarray(f[k], np.float64) for k in ("u", "v", "w", "visC", "visB", "dudx", "dvdx", "dwdx")}
+    rl = None if rlencos is None else np.ascontiguousarray(rlencos, np.float64)
+    bd = None if bnd_dist is None else np.ascontiguousarray(bnd_dist, np.float64)
+    rc = load().orc_uvw_face_loop1(C.byref(_cmesh(m)), _p(rl), _p(bd), float(f["gammaBlend"]), float(f["small"]),
+                                   _p(a["u"]), _p(a["v"]), _p(a["w"]), _p(out["uB"]), _p(out["vB"]), _p(out["wB"]),
+                                   _p(a["visC"]), _p(a["visB"]), _p(out["massFlux"]), _p(a["dudx"]), _p(a["dvdx"]),
+                                   _p(a["dwdx"]), _p(out["rFace"]), *[_p(out[k]) for k in ("su", "sv", "sw", "au", "av", "aw")],
+                                   _p(out["shear"]))
+    assert rc == E_SUCCESS
+    return out
+
+
+def uvw_region_loop1(m):
+    ft = np.full((m["nRegions"], 3), np.nan)
+    assert load().orc_uvw_region_loop1(C.byref(_cmesh(m)), _p(ft)) == E_SUCCESS
+    return ft
+
+
+def uvw_bnds_loop1(m, shear, force_tangent):
+    ft = _f64(force_tangent)
+    sh = np.ascontiguousarray(shear, np.float64)
+    assert load().orc_uvw_bnds_loop1(C.byref(_cmesh(m)), _p(sh), _p(ft)) == E_SUCCESS
+    return ft
+
 
 def fields(m, seed, full=False):
     """phi ~ U[-1,1], u,v,w ~ N(0,1), rho ~ U[0.9,1.1], phiB ~ U[-1,1] from a

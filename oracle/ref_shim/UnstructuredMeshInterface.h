@@ -2,8 +2,10 @@
  * Minimal stand-in for the reference's UnstructuredMeshInterface, exposing
  * exactly the getters that the reference kernels GradientPhiGaussDolfyn
  * (include/fvm/implementation/component/GradientKernels.ipp:39-136),
- * FluxMassDolfynFaceLoop (include/fvm/implementation/component/MassKernels.ipp:36-309)
- * and the boundary / region loops (MassKernels.ipp:311-554) call, backed by
+ * FluxMassDolfynFaceLoop (include/fvm/implementation/component/MassKernels.ipp:36-309),
+ * the boundary / region loops (MassKernels.ipp:311-554) and the momentum
+ * loops FluxUVWDolfynFaceLoop1 / RegionLoop1 / BndsLoop1
+ * (include/fvm/implementation/component/UVWKernels.ipp:38-544) call, backed by
  * plain SoA arrays owned by the caller.
  *
  * TEST INFRASTRUCTURE ONLY: used to compile the reference's own kernel
@@ -65,6 +67,10 @@ namespace cupcfd
 				const T * regionDen;      /* [lRegions] */
 				const I * boundaryFace;   /* [lBoundaries] face of each boundary (getBoundaryFaceID) */
 				const T * regionSplvl;    /* [lRegions] (getRegionSplvl) */
+				const T * faceRLencos;    /* [lFaces] (getFaceRLencos) */
+				const T * boundaryDistance; /* [lBoundaries] (getBoundaryDistance) */
+				T * boundaryShear;        /* [3*lBoundaries] (get/setBoundaryShear) */
+				T * regionForceTangent;   /* [3*lRegions] (get/setRegionForceTangent) */
 			};
 
 			template <class M, class I, class T, class L>
@@ -83,6 +89,23 @@ namespace cupcfd
 					inline T getFaceArea(I f) { return a.faceArea[f]; }
 					inline cupcfd::geometry::euclidean::EuclideanVector3D<T> getFaceNorm(I f) {
 						return cupcfd::geometry::euclidean::EuclideanVector3D<T>(a.faceNorm[3*f], a.faceNorm[3*f+1], a.faceNorm[3*f+2]);
+					}
+					inline void getFaceNorm(I f, cupcfd::geometry::euclidean::EuclideanVector3D<T>& n) {
+						n.cmp[0] = a.faceNorm[3*f]; n.cmp[1] = a.faceNorm[3*f+1]; n.cmp[2] = a.faceNorm[3*f+2];
+					}
+					inline T getFaceRLencos(I f) { return a.faceRLencos[f]; }
+					inline T getBoundaryDistance(I b) { return a.boundaryDistance[b]; }
+					inline cupcfd::geometry::euclidean::EuclideanVector<T,3> getBoundaryShear(I b) {
+						return cupcfd::geometry::euclidean::EuclideanVector<T,3>(a.boundaryShear[3*b], a.boundaryShear[3*b+1], a.boundaryShear[3*b+2]);
+					}
+					inline void setBoundaryShear(I b, cupcfd::geometry::euclidean::EuclideanVector<T,3>& v) {
+						for (int d = 0; d < 3; d++) a.boundaryShear[3*b+d] = v.cmp[d];
+					}
+					inline cupcfd::geometry::euclidean::EuclideanVector<T,3> getRegionForceTangent(I r) {
+						return cupcfd::geometry::euclidean::EuclideanVector<T,3>(a.regionForceTangent[3*r], a.regionForceTangent[3*r+1], a.regionForceTangent[3*r+2]);
+					}
+					inline void setRegionForceTangent(I r, cupcfd::geometry::euclidean::EuclideanVector<T,3>& v) {
+						for (int d = 0; d < 3; d++) a.regionForceTangent[3*r+d] = v.cmp[d];
 					}
 					inline cupcfd::geometry::euclidean::EuclideanPoint<T,3> getFaceCenter(I f) {
 						return cupcfd::geometry::euclidean::EuclideanPoint<T,3>(a.faceCenter[3*f], a.faceCenter[3*f+1], a.faceCenter[3*f+2]);

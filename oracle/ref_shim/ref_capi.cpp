@@ -10,6 +10,9 @@
  * Wrapped reference code:
  *   - cupcfd::fvm::GradientPhiGaussDolfyn   include/fvm/implementation/component/GradientKernels.ipp:38-136
  *   - cupcfd::fvm::FluxMassDolfynFaceLoop   include/fvm/implementation/component/MassKernels.ipp:36-309
+ *   - the mass boundary / region loops       MassKernels.ipp:311-554
+ *   - cupcfd::fvm::FluxUVWDolfynFaceLoop1 / RegionLoop1 / BndsLoop1
+ *                                            include/fvm/implementation/component/UVWKernels.ipp:38-544
  *   - MeshStructGenSource<int,double>       src/geometry/mesh/implementation/source/MeshStructGenSource.cpp:33-1277
  * The mesh the kernels see is the one-rank CupCfdSoAMesh that addData
  * (include/geometry/mesh/interface/component/UnstructuredMeshInterface.ipp:1464-1862)
@@ -27,6 +30,7 @@
 #include "EuclideanPoint.h"
 #include "GradientKernels.h"
 #include "MassKernels.h"
+#include "UVWKernels.h"
 #include "MeshStructGenSource.h"
 
 namespace euc = cupcfd::geometry::euclidean;
@@ -160,6 +164,7 @@ struct RefCtx {
 	std::vector<euc::EuclideanVector<double,3>> dudx, dvdx, dwdx, dpdx;
 	std::vector<int> boundaryFace;   /* getBoundaryFaceID: faceBnd inverted */
 	std::vector<double> splvl;       /* getRegionSplvl (ref_ctx_set_splvl) */
+	std::vector<double> rlencos, bdist, shear, ftan;   /* momentum-loop mesh state, zero until set */
 };
 
 extern "C" void * ref_ctx_create(int nCells, int nFaces, int nBnd, int nRegions,
@@ -198,6 +203,14 @@ extern "C" void * ref_ctx_create(int nCells, int nFaces, int nBnd, int nRegions,
 	c->mesh.a.boundaryFace = c->boundaryFace.data();
 	c->splvl.assign(nRegions > 0 ? nRegions : 1, 0.0);
 	c->mesh.a.regionSplvl = c->splvl.data();
+	c->rlencos.assign(nFaces > 0 ? nFaces : 1, 0.0);
+	c->bdist.assign(nBnd > 0 ? nBnd : 1, 0.0);
+	c->shear.assign(3 * (nBnd > 0 ? nBnd : 1), 0.0);
+	c->ftan.assign(3 * (nRegions > 0 ? nRegions : 1), 0.0);
+	c->mesh.a.faceRLencos = c->rlencos.data();
+	c->mesh.a.boundaryDistance = c->bdist.data();
+	c->mesh.a.boundaryShear = c->shear.data();
+	c->mesh.a.regionForceTangent = c->ftan.data();
 	c->g.resize(nCells);
 	c->go.resize(nCells);
 	return c;
@@ -309,3 +322,48 @@ extern "C" int ref_region_loop(void * p, double * flowFact, double * flowRegion,
 	RefCtx * c = (RefCtx *) p;
 	return (int) cupcfd::fvm::FluxMassDolfynRegionLoop(c->mesh, flowFact, c->nR, flowRegion, c->nR, flowIn);
 }
+
+/* ---- momentum loops (UVWKernels.ipp:38-544), called unchanged ---- */
+extern "C" void ref_ctx_set_uvw_geometry(void * p, const double * rlencos, const double * bdist) {
+	RefCtx * c = (RefCtx *) p;
+	for (int f = 0; f < c->nF; f++) c->rlencos[f] = rlencos ? rlencos[f] : 0.0;
+	for (int b = 0; b < c->nB; b++) c->bdist[b] = bdist ? bdist[b] : 0.0;
+}
+
+/* shear[3*nBnd] and forceTangent[3*nRegions] in / out (either may be NULL). */
+extern "C" void ref_uvw_state(void * p, const double * shearIn, const double * ftanIn, double * shearOut, double * ftanOut) {
+	RefCtx * c = (RefCtx *) p;
+	if (shearIn) std::copy(shearIn, shearIn + 3 * c->nB, c->shear.begin());
+	if (ftanIn) std::copy(ftanIn, ftanIn + 3 * c->nR, c->ftan.begin());
+	if (shearOut) std::copy(c->shear.begin(), c->shear.begin() + 3 * c->nB, shearOut);
+	if (ftanOut) std::copy(c->ftan.begin(), c->ftan.begin() + 3 * c->nR, ftanOut);
+}
+
+/* Runs FluxUVWDolfynFaceLoop1 `reps` times with the reference's argument
+ * list; in/out arrays are updated in place as the reference does. */
+extern "C" int ref_uvw_face_loop1(void * p, double gammaBlend, double small, double * u, double * v, double * w,
+                                  double * uB, double * vB, double * wB, double * visC, double * visB,
+                                  double * massFlux, const double * dudx, const double * dvdx, const double * dwdx,
+                                  double * rFace, double * su, double * sv, double * sw, double * au, double * av,
+                                  double * aw, int reps, double * secs) {
+	RefCtx * c = (RefCtx *) p;
+	int nC = c->nC, nF = c->nF, nB = c->nB;
+	packVec(c->dudx, dudx, nC);
+	packVec(c->dvdx, dvdx, nC);
+	packVec(c->dwdx, dwdx, nC);
+	cupcfd::error::eCodes st = cupcfd::error::E_SUCCESS;
+	for (int r = 0; r < reps; r++) {
+		auto t0 = std::chrono::steady_clock::now();
+		st = cupcfd::fvm::FluxUVWDolfynFaceLoop1(c->mesh, gammaBlend, small, u, nC, v, nC, w, nC, uB, nB, vB, nB, wB, nB,
+		                                          visC, nC, visB, nB, massFlux, nF, c->dudx.data(), nC, c->dvdx.data(), nC,
+		                                          c->dwdx.data(), nC, rFace, 2 * nF, su, nC, sv, nC, sw, nC, au, nC,
+		                                          av, nC, aw, nC);
+		auto t1 = std::chrono::steady_clock::now();
+		if (secs) secs[r] = std::chrono::duration<double>(t1 - t0).count();
+		if (st != cupcfd::error::E_SUCCESS) return (int) st;
+	}
+	return (int) st;
+}
+
+extern "C" void ref_uvw_region_loop1(void * p) { cupcfd::fvm::FluxUVWDolfynRegionLoop1(((RefCtx *) p)->mesh); }
+extern "C" void ref_uvw_bnds_loop1(void * p) { cupcfd::fvm::FluxUVWDolfynBndsLoop1(((RefCtx *) p)->mesh); }

@@ -153,3 +153,59 @@ def test_boundary_and_region_loops_bit_exact(mk):
     outlet = m["regionType"][m["bndRegion"]] == 2
     cells = m["faceCell1"][bf[outlet]]
     assert len(cells) > len(np.unique(cells))
+
+
+def uvw_case(mk, seed, first="outlet"):
+    """A mesh whose face 0 is a boundary face, regions at random with that
+    face's boundary set to an inlet or outlet: the carried uFace / visFace the
+    reference reads (UVWKernels.ipp:74-75) are then defined from face 0 on."""
+    base = O.structgen(9, 7, 8) if mk == "struct" else O.jitter(9, 8, 7, 0.25, seed=5, permute=True)
+    m, _, rng = _with_regions(base, seed)
+    assert m["faceBnd"][0] >= 0
+    m["bndRegion"][m["faceBnd"][0]] = 2 if first == "outlet" else 1
+    return m, rng
+
+
+def assert_same_bits(got, want, keys):
+    for k in keys:
+        a, b = np.asarray(got[k]), np.asarray(want[k])
+        assert a.shape == b.shape, k
+        assert np.array_equal(a.view(np.int64) if a.dtype == np.float64 else a,
+                              b.view(np.int64) if b.dtype == np.float64 else b), k
+
+
+@pytest.mark.parametrize("mk", ["struct", "jitter"])
+@pytest.mark.parametrize("first", ["outlet", "inlet"])
+@pytest.mark.parametrize("geom", ["zero", "set"])
+def test_uvw_face_loop1_bit_exact(mk, first, geom):
+    """FluxUVWDolfynFaceLoop1, RegionLoop1 and BndsLoop1: the C restatement
+    against the reference templates, every output bit for bit. With zero
+    boundary distances (what MeshSource-built meshes hold) the symmetry and
+    wall branches divide by zero, and the infinities and NaNs must agree too."""
+    m, rng = uvw_case(mk, 60 + (mk == "jitter"), first)
+    f = O.uvw_fields(m, 61)
+    rl = bd = None
+    if geom == "set":
+        rl = rng.uniform(0.1, 2.0, m["nFaces"])
+        bd = rng.uniform(0.01, 0.2, m["nBnd"])
+    R = O.RefKernels(m).uvw_geometry(rl, bd)
+    rc, want, _ = R.uvw_face_loop1(f)
+    assert rc == O.E_SUCCESS
+    got = O.uvw_face_loop1(m, f, rl, bd)
+    assert_same_bits(got, want, O.UVW_INOUT + ("shear",))
+    if geom == "set":
+        for k in ("su", "sv", "sw", "au", "av", "aw", "uB", "shear"):
+            assert np.all(np.isfinite(got[k])), k
+    # the branches all ran: outlets clamped negative fluxes, walls set shear
+    bt = m["regionType"][m["bndRegion"]]
+    bfaces = np.flatnonzero(m["faceBnd"] >= 0)
+    out_f = bfaces[bt[m["faceBnd"][bfaces]] == 2]
+    assert np.all(got["massFlux"][out_f] > 0) and np.any(f["massFlux"][out_f] < 0)
+    if geom == "set":
+        assert np.any(got["shear"][bt == 4] != 0)
+    # region force tangents: zeroed, then the wall shears summed in boundary order
+    R.uvw_state(force_tangent=np.full((m["nRegions"], 3), 7.0))
+    ft0 = R.uvw_region_loop1()
+    assert np.array_equal(ft0, O.uvw_region_loop1(m)) and not ft0.any()
+    ft1 = R.uvw_bnds_loop1()
+    assert_same_bits({"ft": O.uvw_bnds_loop1(m, got["shear"], ft0)}, {"ft": ft1}, ("ft",))
