@@ -103,6 +103,16 @@ SIGNATURES = {
     "cupcfd_gpu_dev_boundary_loop4": ([_VP] * 9, _I),
     "cupcfd_gpu_dev_boundary_loop5": ([_VP] * 6 + [_D, _I, _I, _I, _VP, _VP, _VP], _I),
     "cupcfd_gpu_dev_region_loop": ([_VP] * 5, _I),
+    "cupcfd_gpu_mesh_set_face_rlencos": ([_VP, _VP, _I], _I),
+    "cupcfd_gpu_mesh_set_boundary_distance": ([_VP, _VP, _I], _I),
+    "cupcfd_gpu_mesh_boundary_shear": ([_VP, _VP, _VP, _I], _I),
+    "cupcfd_gpu_mesh_region_force_tangent": ([_VP, _VP, _VP, _I], _I),
+    "cupcfd_gpu_flux_uvw_dolfyn_face_loop1": ([_VP, _D, _D] + [_VP, _I] * 9 + [Vec3View, _I] * 3 + [_VP, _I] * 7, _I),
+    "cupcfd_gpu_flux_uvw_dolfyn_region_loop1": ([_VP], _I),
+    "cupcfd_gpu_flux_uvw_dolfyn_bnds_loop1": ([_VP], _I),
+    "cupcfd_gpu_dev_uvw_face_loop1": ([_VP, _D, _D] + [_VP] * 10 + [_I64] + [_VP] * 8, _I),
+    "cupcfd_gpu_dev_uvw_region_loop1": ([_VP, _VP], _I),
+    "cupcfd_gpu_dev_uvw_bnds_loop1": ([_VP, _VP], _I),
     "cupcfd_gpu_mesh_set_fusion": ([_VP, _I], _I),
     "cupcfd_gpu_mesh_check_status": ([_VP, _VP], _I),
     "cupcfd_gpu_mesh_get_cell_face_csr": ([_VP, _VP, _I, _VP, _I], _I),
@@ -317,6 +327,30 @@ class Mesh:
     def set_region_split(self, splvl):
         sp = np.ascontiguousarray(splvl, np.float64)
         return lib().cupcfd_gpu_mesh_set_region_split(self.h, len(sp), _p(sp))
+
+    def set_face_rlencos(self, rlencos):
+        """getFaceRLencos per face (reference order); None resets to zero."""
+        a = None if rlencos is None else np.ascontiguousarray(rlencos, np.float64)
+        return lib().cupcfd_gpu_mesh_set_face_rlencos(self.h, _p(a), 0 if a is None else len(a))
+
+    def set_boundary_distance(self, distance):
+        """getBoundaryDistance per boundary; None resets to zero."""
+        a = None if distance is None else np.ascontiguousarray(distance, np.float64)
+        return lib().cupcfd_gpu_mesh_set_boundary_distance(self.h, _p(a), 0 if a is None else len(a))
+
+    def boundary_shear(self, value=None):
+        """The boundary shear [nBoundaries, 3] (set first when given)."""
+        out = np.empty((self.nBoundaries, 3))
+        a = None if value is None else np.ascontiguousarray(value, np.float64)
+        check(lib().cupcfd_gpu_mesh_boundary_shear(self.h, _p(a), _p(out), self.nBoundaries))
+        return out
+
+    def region_force_tangent(self, n_regions, value=None):
+        """The region force tangents [nRegions, 3] (set first when given)."""
+        out = np.empty((n_regions, 3))
+        a = None if value is None else np.ascontiguousarray(value, np.float64)
+        check(lib().cupcfd_gpu_mesh_region_force_tangent(self.h, _p(a), _p(out), n_regions))
+        return out
 
     def set_fusion(self, mode):
         """0 auto, 1 always fused, 2 never fused (forward+adjoint)."""
@@ -546,3 +580,51 @@ def dev_boundary_loop5(mesh, massFlux, su, uB, vB, wB, fact, solve, flowFact, fl
 
 def dev_region_loop(mesh, flowFact, flowRegion, flowIn, stream=None):
     check(lib().cupcfd_gpu_dev_region_loop(mesh.h, _p(flowFact), _p(flowRegion), _p(flowIn), _stream(stream)))
+
+
+# ---------------------------------------------------------------------------
+# momentum face loop (UVWKernels.h:45-92)
+# ---------------------------------------------------------------------------
+def FluxUVWDolfynFaceLoop1(mesh, gammaBlend, small, uCell, vCell, wCell, uBoundary, vBoundary, wBoundary, visEffCell,
+                           visEffBoundary, massFlux, dudx, dvdx, dwdx, rFace, su, sv, sw, au, av, aw):
+    """Mirror of cupcfd::fvm::FluxUVWDolfynFaceLoop1 (UVWKernels.h:45-67) on
+    host FP64 arrays in the reference's numbering; in/out arrays (boundary
+    velocities, massFlux, rFace, su..aw) are updated in place; dudx/dvdx/dwdx
+    are (n,3) or (n,4) (leading pad slot). Returns an eCodes value."""
+    def a(x):
+        return [_p(x), 0 if x is None else len(x)]
+    args = [mesh.h, float(gammaBlend), float(small)]
+    for x in (uCell, vCell, wCell, uBoundary, vBoundary, wBoundary, visEffCell, visEffBoundary, massFlux):
+        args += a(x)
+    for vv in (dudx, dvdx, dwdx):
+        args += [_vec(vv), len(vv)]
+    args += a(rFace)
+    for x in (su, sv, sw, au, av, aw):
+        args += a(x)
+    return lib().cupcfd_gpu_flux_uvw_dolfyn_face_loop1(*args)
+
+
+def FluxUVWDolfynRegionLoop1(mesh):
+    return lib().cupcfd_gpu_flux_uvw_dolfyn_region_loop1(mesh.h)
+
+
+def FluxUVWDolfynBndsLoop1(mesh):
+    return lib().cupcfd_gpu_flux_uvw_dolfyn_bnds_loop1(mesh.h)
+
+
+def dev_uvw_face_loop1(mesh, gammaBlend, small, u, v, w, uB, vB, wB, visC, visB, massFlux, grads, rFace, su, sv, sw,
+                       au, av, aw, stream=None):
+    """Device-resident momentum face loop: torch CUDA FP64 tensors in the
+    mesh's internal numbering; grads is (9, ldg) (dudx x,y,z, dvdx, dwdx)."""
+    check(lib().cupcfd_gpu_dev_uvw_face_loop1(
+        mesh.h, float(gammaBlend), float(small), _p(u), _p(v), _p(w), _p(uB), _p(vB), _p(wB), _p(visC), _p(visB),
+        _p(massFlux), _p(grads), int(grads.stride(0)), _p(rFace), _p(su), _p(sv), _p(sw), _p(au), _p(av), _p(aw),
+        _stream(stream)))
+
+
+def dev_uvw_region_loop1(mesh, stream=None):
+    check(lib().cupcfd_gpu_dev_uvw_region_loop1(mesh.h, _stream(stream)))
+
+
+def dev_uvw_bnds_loop1(mesh, stream=None):
+    check(lib().cupcfd_gpu_dev_uvw_bnds_loop1(mesh.h, _stream(stream)))

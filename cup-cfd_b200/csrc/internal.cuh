@@ -122,6 +122,16 @@ struct cupcfd_gpu_mesh {
     int *bndSorted = nullptr, *bndSortedCellInt = nullptr, *bndSortedCellRef = nullptr;
     bool bndMapsOk = false;
     std::vector<int> hRegionType;
+    // momentum loops (FluxUVWDolfyn*): getFaceRLencos per internal face and
+    // getBoundaryDistance per boundary (null = all zero until set), boundary
+    // shear [3 nB] and region force tangents [3 nR] (zero until written), and
+    // per internal face the source of its carried face value (kernels_uvw.cuh),
+    // rebuilt after the regions change
+    double *rlencos = nullptr, *bndDist = nullptr, *bndShear = nullptr, *regionFT = nullptr;
+    double *rlencosBuf = nullptr, *bndDistBuf = nullptr;  // storage behind rlencos / bndDist once set
+    int regionFTcap = 0;
+    int *uvwCarry = nullptr;
+    bool uvwCarryValid = false;
     // wavefront-fused forward+adjoint: numbering bandwidth (largest
     // |c - neighbour|), per-tile publication flags, work counter + error word
     int bandwidth = 0;

@@ -22,6 +22,7 @@
 
 #include "arith.cuh"
 #include "internal.cuh"
+#include "sell.cuh"
 
 namespace cupcfd_gpu {
 
@@ -56,45 +57,6 @@ __device__ __forceinline__ double4 ldg4(const double4 *p) {
 }
 __device__ __forceinline__ float4 ldg4(const float4 *p) { return __ldg(p); }
 
-struct SellView {
-    const int *slicePtr;
-    const int2 *inc;
-    int width;  // common slice width, or 0 when widths vary
-};
-
-// The cell's first incidence entry and its slice width (entries per lane).
-// With a common width (every hexahedral mesh) the position is arithmetic,
-// which takes a dependent load off the head of every cell's load chain.
-__device__ __forceinline__ const int2 *cell_entries(const SellView &sv, int c, int &w) {
-    int s = c >> 5;
-    if (sv.width) {
-        w = sv.width;
-        return sv.inc + (s * 32 * sv.width + (c & 31));  // entries fit in int (slicePtr is int)
-    }
-    int p0 = __ldg(sv.slicePtr + s);
-    w = (__ldg(sv.slicePtr + s + 1) - p0) >> 5;
-    return sv.inc + p0 + (c & 31);
-}
-
-// Read-only 8-byte load of an incidence entry. With CUPCFD_L2_PREFETCH the
-// load asks L2 to fetch 256-byte blocks from DRAM (the incidence stream is
-// read sequentially slice by slice).
-__device__ __forceinline__ int2 ld_entry(const int2 *p) {
-#ifdef CUPCFD_L2_PREFETCH
-    int2 v;
-    asm("ld.global.nc.L2::256B.v2.s32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "l"(p));
-    return v;
-#else
-    return __ldg(p);
-#endif
-}
-
-// Entries k0 .. k0+W-1 of the cell (padding {-1,-1} past its slice width).
-template <int W>
-__device__ __forceinline__ void load_entries(const int2 *e, int k0, int w, int2 (&en)[W]) {
-#pragma unroll
-    for (int j = 0; j < W; j++) en[j] = (k0 + j < w) ? ld_entry(e + 32 * (k0 + j)) : make_int2(-1, -1);
-}
 
 // Entries per chunk in the unrolled kernels (six covers a hex cell in one
 // chunk; wider cells take more chunks) and the minimum resident blocks per

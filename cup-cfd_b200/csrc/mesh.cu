@@ -939,6 +939,13 @@ extern "C" int cupcfd_gpu_mesh_set_regions(cupcfd_gpu_mesh *m, int32_t nR, const
     CG_CHECK_CUDA(cudaStreamSynchronize(st));
     m->nR = nR;
     m->hRegionType.assign(type, type + nR);
+    m->uvwCarryValid = false;  // the carried-value sources depend on the region types
+    if (m->regionFT && nR <= m->regionFTcap) {
+        CG_CHECK_CUDA(cudaMemsetAsync(m->regionFT, 0, sizeof(double) * 3 * nR, st));
+        CG_CHECK_CUDA(cudaStreamSynchronize(st));
+    } else {
+        m->regionFTcap = 0;  // reallocated (zeroed) by the next momentum loop
+    }
     m->allDefaultRegions = true;
     for (int r = 0; r < nR; r++)
         if (type[r] != CUPCFD_RTYPE_DEFAULT) m->allDefaultRegions = false;

@@ -414,6 +414,64 @@ int cupcfd_gpu_dev_boundary_loop5(cupcfd_gpu_mesh *mesh, double *massFlux, doubl
 int cupcfd_gpu_dev_region_loop(cupcfd_gpu_mesh *mesh, double *flowFact, const double *flowRegion,
                                const double *flowIn, void *stream);
 
+/* ------------------------------------------------------------------------ */
+/* momentum face loop (UVWKernels.h:45-92, UVWKernels.ipp:38-544), FP64     */
+/* ------------------------------------------------------------------------ */
+
+/* Mesh state the momentum loops read and write. rlencos[nFaces] (reference
+ * face order; replaces setFaceRLencos/getFaceRLencos,
+ * UnstructuredMeshInterface.h:757-770) and distance[nBoundaries] (replaces
+ * getBoundaryDistance, :1225-1238) are zero until set, as on every mesh a
+ * MeshSource builds (UnstructuredMeshInterface.ipp:1809-1810,
+ * MeshStructGenSource.cpp:1251-1258); NULL resets to zero. The boundary shear
+ * [3*nBoundaries] (get/setBoundaryShear, :1333-1346, :1527) and region force
+ * tangents [3*nRegions] (get/setRegionForceTangent, :1909-1922, :2225) are
+ * xyz-interleaved; `in` (may be NULL) is written first, then `out` (may be
+ * NULL) read. Both start at zero; cupcfd_gpu_mesh_set_regions zeroes the
+ * force tangents. */
+int cupcfd_gpu_mesh_set_face_rlencos(cupcfd_gpu_mesh *mesh, const double *rlencos, int32_t nFaces);
+int cupcfd_gpu_mesh_set_boundary_distance(cupcfd_gpu_mesh *mesh, const double *distance, int32_t nBoundaries);
+int cupcfd_gpu_mesh_boundary_shear(cupcfd_gpu_mesh *mesh, const double *in, double *out, int32_t nBoundaries);
+int cupcfd_gpu_mesh_region_force_tangent(cupcfd_gpu_mesh *mesh, const double *in, double *out, int32_t nRegions);
+
+/* cupcfd::fvm::FluxUVWDolfynFaceLoop1 (UVWKernels.h:45-67): host buffers in
+ * the reference's numbering, same parameters in the same order; dudx/dvdx/
+ * dwdx are vec3 views of the EuclideanVector<double,3> arrays. Updates
+ * massFlux (outlet faces: negative fluxes become `small`), rFace (interior
+ * faces), su/sv/sw, au/av/aw, u/v/wBoundary and the mesh's boundary shear
+ * (wall faces) bit-identically to the reference. The reference carries
+ * uFace/vFace/wFace and visFace from one face to the next in label order
+ * (declared outside its face loop, UVWKernels.ipp:74-75: interior faces read
+ * the values of the last inlet or outlet face before them, symmetry faces the
+ * visFace of the last interior, inlet or outlet face); where the reference
+ * reads them before any face set them (uninitialised there) they are zero
+ * here. Arrays shorter than the mesh return E_INVALID_INDEX. */
+int cupcfd_gpu_flux_uvw_dolfyn_face_loop1(
+    cupcfd_gpu_mesh *mesh, double gammaBlend, double small, const double *uCell, int32_t nUCell,
+    const double *vCell, int32_t nVCell, const double *wCell, int32_t nWCell, double *uBoundary, int32_t nUBoundary,
+    double *vBoundary, int32_t nVBoundary, double *wBoundary, int32_t nWBoundary, const double *visEffCell,
+    int32_t nVisEffCell, const double *visEffBoundary, int32_t nVisEffBoundary, double *massFlux, int32_t nMassFlux,
+    cupcfd_vec3_view dudx, int32_t nDudx, cupcfd_vec3_view dvdx, int32_t nDvdx, cupcfd_vec3_view dwdx, int32_t nDwdx,
+    double *rFace, int32_t nRFace, double *su, int32_t nSu, double *sv, int32_t nSv, double *sw, int32_t nSw,
+    double *au, int32_t nAu, double *av, int32_t nAv, double *aw, int32_t nAw);
+/* FluxUVWDolfynRegionLoop1 (UVWKernels.ipp:517-524): force tangents = 0.
+ * FluxUVWDolfynBndsLoop1 (UVWKernels.ipp:527-544): each wall boundary adds
+ * its shear onto its region's force tangent, in boundary order. */
+int cupcfd_gpu_flux_uvw_dolfyn_region_loop1(cupcfd_gpu_mesh *mesh);
+int cupcfd_gpu_flux_uvw_dolfyn_bnds_loop1(cupcfd_gpu_mesh *mesh);
+
+/* The same on device arrays in the mesh's internal numbering and a caller
+ * stream: cell arrays [nCells], grads = 9 blocks of leading dimension ldg
+ * (dudx x, y, z, dvdx x, y, z, dwdx x, y, z), face arrays [nFaces] and rFace
+ * [2*nFaces] in internal face order, boundary arrays by boundary id. */
+int cupcfd_gpu_dev_uvw_face_loop1(cupcfd_gpu_mesh *mesh, double gammaBlend, double small, const double *uCell,
+                                  const double *vCell, const double *wCell, double *uBoundary, double *vBoundary,
+                                  double *wBoundary, const double *visEffCell, const double *visEffBoundary,
+                                  double *massFlux, const double *grads, int64_t ldg, double *rFace, double *su,
+                                  double *sv, double *sw, double *au, double *av, double *aw, void *stream);
+int cupcfd_gpu_dev_uvw_region_loop1(cupcfd_gpu_mesh *mesh, void *stream);
+int cupcfd_gpu_dev_uvw_bnds_loop1(cupcfd_gpu_mesh *mesh, void *stream);
+
 /* Number of kernels this library launched since load (all threads). */
 int64_t cupcfd_gpu_launch_count(void);
 
