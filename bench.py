@@ -227,6 +227,74 @@ def cpu_baseline(n, procs, reps):
             "ms_per_step": t * 1e3}
 
 
+def cpu_uvw(n, reps):
+    """Gfaces/s of the reference's FluxUVWDolfynFaceLoop1 (FP64, one core) on
+    an n^3 generated mesh with its default region, as the reference's
+    FluxUVWDolfynFaceLoop1Benchmark runs it (BenchmarkKernels.cpp:751-860)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    m = O.structgen(n, n, n)
+    f = O.uvw_fields(m, SEED)
+    if O.load_ref() is not None:
+        kind = "reference"
+        _, _, secs = O.RefKernels(m).uvw_geometry().uvw_face_loop1(f, reps=reps)
+    else:
+        kind = "port"
+        secs = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            O.uvw_face_loop1(m, f)
+            secs.append(time.perf_counter() - t0)
+    t = statistics.median(secs)
+    return {"value": m["nFaces"] / t / 1e9, "unit": "Gfaces/s", "cores": 1, "kind": kind, "ms_per_call": t * 1e3,
+            "sample": f"{n}^3 generated mesh ({m['nFaces']} faces), default region; median of {reps} calls"}
+
+
+def bench_uvw(cg, mesh, dev, st, g, steps, warmup, peak):
+    """The momentum face loop (FluxUVWDolfynFaceLoop1, FP64) through the
+    device-resident call on the bench mesh: the generated mesh with its
+    default region and zero rlencos, the reference benchmark's configuration.
+    Inputs drawn as that benchmark draws them (U[1e-6, 1e-2]), gradients
+    1e-2 N(0,1). Algorithmic bytes per call: per cell u, v, w, visEff, nine
+    gradient components, the cell centre (read) and su..aw (read and written)
+    = 224; per interior face S, lambda, massFlux, two cell ids (read) and
+    rFace (written) = 64; per boundary face its region id = 4."""
+    import torch
+    nC, nF, nFi, nB = mesh.nCells, mesh.nFaces, mesh.nInteriorFaces, mesh.nBoundaries
+    D = dict(dtype=torch.float64, device=dev)
+
+    def U(n):
+        return torch.rand(n, generator=g, **D) * (1e-2 - 1e-6) + 1e-6
+
+    c = {k: U(nC) for k in ("u", "v", "w", "visC", "su", "sv", "sw", "au", "av", "aw")}
+    grads = torch.randn(9, nC, generator=g, **D) * 1e-2
+    b = {k: U(nB) for k in ("uB", "vB", "wB", "visB")}
+    mf = U(nF)
+    rf = torch.zeros(2 * nF, **D)
+
+    def call():
+        cg.dev_uvw_face_loop1(mesh, 0.9, 1e-18, c["u"], c["v"], c["w"], b["uB"], b["vB"], b["wB"], c["visC"], b["visB"],
+                              mf, grads, rf, c["su"], c["sv"], c["sw"], c["au"], c["av"], c["aw"], stream=st)
+
+    for _ in range(warmup):
+        call()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(steps):
+        call()
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    alg = 224 * nC + 64 * nFi + 4 * nB
+    gbs = alg / (ms * 1e-3) / 1e9
+    return {"call": "cupcfd_gpu_dev_uvw_face_loop1 (FP64, bit-identical to the reference)", "kernel": "k_uvw_f64",
+            "ms_per_call": ms, "value": nF / (ms * 1e-3) / 1e9, "unit": "Gfaces/s", "steps": steps,
+            "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+                         "algorithmic_bytes_per_launch": alg},
+            "config": "generated mesh, default region, rlencos 0 (the reference benchmark's case)"}
+
+
 # ---------------------------------------------------------------------------
 # reference arm
 # ---------------------------------------------------------------------------
@@ -451,6 +519,18 @@ def run_gpu(a):
     # ---- roofline of the dominant kernel, from the device timers of the timed region
     bm = bytes_model(nC, nF, nFi, nB)
     peak, peak_src = measured_peaks()
+
+    # ---- the momentum face loop (the next operator after the path), FP64, same mesh
+    uvw = None
+    if not a.no_uvw:
+        uvw = bench_uvw(cg, mesh, dev, st, g, max(3, K // 4), 3, peak)
+        uvw["roofline"]["peak_source"] = peak_src
+        if rank == 0 and world == 1 and not a.no_cpu:
+            try:
+                uvw["cpu_reference"] = cpu_uvw(a.cpu_n, 5)
+            except Exception as ex:
+                uvw["cpu_reference"] = {"value": None, "sample": f"failed: {ex}"}
+        torch.cuda.synchronize()
     kbytes = {"k_fwd_madj_f32_pf": bm["fwd_madj_f32"], "k_gadj_f32_pf": bm["gadj_f32"], "k_fused_f32": bm["pipeline_f32"],
               "k_fwd_f32_pf": bm["fwd_f32"], "k_fwd_f32": bm["fwd_f32"], "k_adj_f32_pf": bm["adj_f32"],
               "k_adj_f32": bm["adj_f32"]}
@@ -501,6 +581,7 @@ def run_gpu(a):
             "error_vs_fp64": errors,
             "e2e": e2e,
             "cpu_baseline": cpu,
+            "uvw_face_loop1": uvw,
             "gpu_launches": launches,
             "clocks": clk,
             "mesh_build_s": t_build,
@@ -525,6 +606,7 @@ def main():
     ap.add_argument("--cpu-n", type=int, default=64, help="CPU baseline sample: cpu_n^3 mesh")
     ap.add_argument("--cpu-reps", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-uvw", action="store_true", help="skip the momentum face loop measurement")
     a = ap.parse_args()
     if a.warmup < 3:
         a.warmup = 3

@@ -92,174 +92,215 @@ __device__ __forceinline__ double vis_face_of(const UvwArgs &a, int g) {
     return dm(visac, rl);
 }
 
-__global__ void __launch_bounds__(256) k_uvw_f64(const __grid_constant__ UvwArgs a) {
+// How an incidence's terms update its cell (t[0..9] from uvw_terms), in the
+// reference's operand order:
+enum UvwKind : int {
+    UVW_NONE = 0,    // padding, default-region boundary
+    UVW_OWNER = 1,   // interior, cell1: s = ((s - blend) + fde) - fdi          (UVWKernels.ipp:216-223)
+    UVW_NEIGH = 2,   // interior, cell2: s = ((s + blend) - fde) + fdi
+    UVW_INOUT = 3,   // inlet / outlet: a = a - f; s = ((s - f*uF) + fde) - fdi (:309-317, :370-378)
+    UVW_WALLSYM = 4  // symmetry / wall: a = a + X; s = (s + X*u) - force       (:424-431, :490-497)
+};
+
+// The terms one incidence (entry en of cell c) contributes to its cell, and
+// the face's own outputs when c owns the face. Returns the UvwKind.
+__device__ __forceinline__ int uvw_terms(const UvwArgs &a, int c, int2 en, double (&t)[10]) {
+    const int64_t L = a.ldg;
+    auto gr = [&](int q, int cell) { return a.grads[q * L + cell]; };
+    const int f = en.x >> 1;
+    const bool owner = (en.x & 1) == 0;
+    const double4 G = a.fg[f];
+    const double rl = a.rlencos ? a.rlencos[f] : 0.0;
+    if (en.y >= 0) {
+        // interior face (UVWKernels.ipp:145-228)
+        const int ip = owner ? c : en.y, in = owner ? en.y : c;
+        const double facn = G.w, facp = ds(1.0, facn);
+        double du[3], dv[3], dw[3];
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            du[d] = da(dm(gr(d, in), facn), dm(gr(d, ip), facp));
+            dv[d] = da(dm(gr(3 + d, in), facn), dm(gr(3 + d, ip), facp));
+            dw[d] = da(dm(gr(6 + d, in), facn), dm(gr(6 + d, ip), facp));
+        }
+        const double visac = da(dm(a.visC[in], facn), dm(a.visC[ip], facp));
+        const double4 Cn = a.cc[in], Cp = a.cc[ip];
+        const double x0 = ds(Cn.x, Cp.x), x1 = ds(Cn.y, Cp.y), x2 = ds(Cn.z, Cp.z);
+        const double visFace = dm(visac, rl);
+        double uF = 0.0, vF = 0.0, wF = 0.0;
+        const int cr = a.carry[f];
+        if (cr >= 0) {
+            uF = a.u[cr]; vF = a.v[cr]; wF = a.w[cr];
+        } else if (cr <= -2) {
+            const double *r = a.regionUVW + 3 * (-2 - cr);
+            uF = r[0]; vF = r[1]; wF = r[2];
+        }
+        const double mf = a.massFlux[f];
+        const double fmin = std_min(mf, 0.0), fmax = std_max(mf, 0.0);
+        const double fuci = da(dm(fmin, a.u[in]), dm(fmax, a.u[ip]));
+        const double fvci = da(dm(fmin, a.v[in]), dm(fmax, a.v[ip]));
+        const double fwci = da(dm(fmin, a.w[in]), dm(fmax, a.w[ip]));
+        t[0] = dm(a.gammaBlend, ds(dm(mf, uF), fuci));
+        t[3] = dm(a.gammaBlend, ds(dm(mf, vF), fvci));
+        t[6] = dm(a.gammaBlend, ds(dm(mf, wF), fwci));
+        t[1] = dm(visac, da(da(dm(da(du[0], du[0]), G.x), dm(da(du[1], dv[0]), G.y)), dm(da(du[2], dw[0]), G.z)));
+        t[4] = dm(visac, da(da(dm(da(du[1], dv[0]), G.x), dm(da(dv[1], dv[1]), G.y)), dm(da(dv[2], dw[1]), G.z)));
+        t[7] = dm(visac, da(da(dm(da(du[2], dw[0]), G.x), dm(da(dw[1], dv[2]), G.y)), dm(da(dw[2], dw[2]), G.z)));
+        t[2] = dm(visFace, dot0(du[0], du[1], du[2], x0, x1, x2));
+        t[5] = dm(visFace, dot0(dv[0], dv[1], dv[2], x0, x1, x2));
+        t[8] = dm(visFace, dot0(dw[0], dw[1], dw[2], x0, x1, x2));
+        if (owner) {
+            a.rFace[2 * (int64_t) f] = ds(-visFace, std_max(mf, 0.0));
+            a.rFace[2 * (int64_t) f + 1] = da(-visFace, std_min(mf, 0.0));
+        }
+        return owner ? UVW_OWNER : UVW_NEIGH;
+    }
+    // boundary face: c is its owner
+    const int ib = -1 - en.y;
+    const int ir = a.bndRegion[ib];
+    const int it = a.regionType[ir];
+    if (it == CUPCFD_RTYPE_DEFAULT) return UVW_NONE;
+    const double4 X = a.fc[f], Cp = a.cc[c];
+    const double x0 = ds(X.x, Cp.x), x1 = ds(X.y, Cp.y), x2 = ds(X.z, Cp.z);
+    const double uc = a.u[c], vc = a.v[c], wc = a.w[c];
+    const double du0 = gr(0, c), du1 = gr(1, c), du2 = gr(2, c);
+    const double dv0 = gr(3, c), dv1 = gr(4, c), dv2 = gr(5, c);
+    const double dw0 = gr(6, c), dw1 = gr(7, c), dw2 = gr(8, c);
+    if (it == CUPCFD_RTYPE_INLET || it == CUPCFD_RTYPE_OUTLET) {
+        // UVWKernels.ipp:259-382 (outlet: operands of two sums swapped,
+        // which IEEE addition does not see)
+        double uF, vF, wF, visac;
+        if (it == CUPCFD_RTYPE_INLET) {
+            const double *r = a.regionUVW + 3 * ir;
+            uF = r[0]; vF = r[1]; wF = r[2];
+            visac = a.visB[ib];
+        } else {
+            uF = uc; vF = vc; wF = wc;
+            visac = a.visC[c];
+        }
+        const double visFace = dm(visac, rl);
+        double mf = a.massFlux[f];
+        if (it == CUPCFD_RTYPE_OUTLET && mf < 0.0) {
+            mf = a.small;
+            a.massFlux[f] = mf;
+        }
+        const double fl = da(-visFace, std_min(mf, 0.0));
+        t[0] = dm(fl, uF); t[3] = dm(fl, vF); t[6] = dm(fl, wF);
+        t[1] = dm(visac, da(da(dm(da(du0, du0), G.x), dm(da(du1, dv0), G.y)), dm(da(du2, dw0), G.z)));
+        t[4] = dm(visac, da(da(dm(da(du1, dv0), G.x), dm(da(dv1, dv1), G.y)), dm(da(dv2, dw1), G.z)));
+        t[7] = dm(visac, da(da(dm(da(du2, dw0), G.x), dm(da(dw1, dv2), G.y)), dm(da(dw2, dw2), G.z)));
+        t[2] = dm(visFace, dot0(du0, du1, du2, x0, x1, x2));
+        t[5] = dm(visFace, dot0(dv0, dv1, dv2, x0, x1, x2));
+        t[8] = dm(visFace, dot0(dw0, dw1, dw2, x0, x1, x2));
+        t[9] = fl;
+        a.uB[ib] = uF; a.vB[ib] = vF; a.wB[ib] = wF;
+        return UVW_INOUT;
+    }
+    const double area = X.w;
+    double Xc, f0 = 0.0, f1 = 0.0, f2 = 0.0;
+    if (it == CUPCFD_RTYPE_SYMP) {
+        // UVWKernels.ipp:383-436; visFace carried from an earlier face
+        const int g = a.carry[f];
+        Xc = g >= 0 ? vis_face_of(a, g) : 0.0;
+        const double visac = a.visC[c];
+        const double us0 = da(uc, dot0(du0, du1, du2, x0, x1, x2));
+        const double us1 = da(vc, dot0(dv0, dv1, dv2, x0, x1, x2));
+        const double us2 = da(wc, dot0(dw0, dw1, dw2, x0, x1, x2));
+        double n0 = ds(0.0, G.x), n1 = ds(0.0, G.y), n2 = ds(0.0, G.z);
+        normalise(n0, n1, n2);
+        const double dp = dot0(us0, us1, us2, n0, n1, n2);
+        const double dn = a.bndDist ? a.bndDist[ib] : 0.0;
+        const double tv = dm(2.0, visac);
+        f0 = dm(dvd(dm(tv, dm(dp, n0)), dn), area);
+        f1 = dm(dvd(dm(tv, dm(dp, n1)), dn), area);
+        f2 = dm(dvd(dm(tv, dm(dp, n2)), dn), area);
+        a.uB[ib] = us0; a.vB[ib] = us1; a.wB[ib] = us2;
+    } else {
+        // wall, UVWKernels.ipp:437-510
+        const double *uw = a.regionUVW + 3 * ir;
+        const double visac = a.visB[ib];
+        Xc = dvd(dm(visac, area), __dsqrt_rn(dot0(x0, x1, x2, x0, x1, x2)));
+        double n0 = G.x, n1 = G.y, n2 = G.z;
+        normalise(n0, n1, n2);
+        const double up0 = ds(uc, uw[0]), up1 = ds(vc, uw[1]), up2 = ds(wc, uw[2]);
+        const double dp = dot0(up0, up1, up2, n0, n1, n2);
+        const double ut0 = ds(up0, dm(dp, n0)), ut1 = ds(up1, dm(dp, n1)), ut2 = ds(up2, dm(dp, n2));
+        const double uvel = da(da(fabs(ut0), fabs(ut1)), fabs(ut2));
+        if (uvel > a.small) {
+            const double dn = a.bndDist ? a.bndDist[ib] : 0.0;
+            f0 = dm(dvd(dm(visac, ut0), dn), area);
+            f1 = dm(dvd(dm(visac, ut1), dn), area);
+            f2 = dm(dvd(dm(visac, ut2), dn), area);
+        }
+        a.shear[3 * (int64_t) ib] = f0;
+        a.shear[3 * (int64_t) ib + 1] = f1;
+        a.shear[3 * (int64_t) ib + 2] = f2;
+        a.uB[ib] = uw[0]; a.vB[ib] = uw[1]; a.wB[ib] = uw[2];
+    }
+    t[0] = dm(Xc, uc); t[3] = dm(Xc, vc); t[6] = dm(Xc, wc);
+    t[1] = f0; t[4] = f1; t[7] = f2;
+    t[9] = Xc;
+    return UVW_WALLSYM;
+}
+
+// Applies one incidence's terms to the cell's running su/sv/sw (s) and
+// au/av/aw (ad).
+__device__ __forceinline__ void uvw_fold(int kind, const double (&t)[10], double (&s)[3], double (&ad)[3]) {
+    switch (kind) {
+    case UVW_OWNER:
+#pragma unroll
+        for (int q = 0; q < 3; q++) s[q] = ds(da(ds(s[q], t[3 * q]), t[3 * q + 1]), t[3 * q + 2]);
+        break;
+    case UVW_NEIGH:
+#pragma unroll
+        for (int q = 0; q < 3; q++) s[q] = da(ds(da(s[q], t[3 * q]), t[3 * q + 1]), t[3 * q + 2]);
+        break;
+    case UVW_INOUT:
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            ad[q] = ds(ad[q], t[9]);
+            s[q] = ds(da(ds(s[q], t[3 * q]), t[3 * q + 1]), t[3 * q + 2]);
+        }
+        break;
+    case UVW_WALLSYM:
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            ad[q] = da(ad[q], t[9]);
+            s[q] = ds(da(s[q], t[3 * q]), t[3 * q + 1]);
+        }
+        break;
+    default:
+        break;
+    }
+}
+
+// One thread per cell, incidences in order. (One thread per incidence with
+// the terms staged in shared memory and one warp folding them measured
+// slower: 4.2-5.0 ms against 2.3 ms at 256^3.)
+#ifndef UVW_CELL_MINB
+#define UVW_CELL_MINB 3  // resident 256-thread blocks per SM asked of the register allocator (80 registers)
+#endif
+#ifndef UVW_CHUNK
+#define UVW_CHUNK 6      // incidence entries loaded ahead (a hexahedral cell in one chunk)
+#endif
+__global__ void __launch_bounds__(256, UVW_CELL_MINB) k_uvw_f64(const __grid_constant__ UvwArgs a) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= a.nC) return;
     int wdt;
     const int2 *e = cell_entries(a.sv, c, wdt);
-    const int64_t L = a.ldg;
-    auto gr = [&](int q, int cell) { return a.grads[q * L + cell]; };
-    double su = a.su[c], sv = a.sv_[c], sw = a.sw[c], au = a.au[c], av = a.av[c], aw = a.aw[c];
-    const double uc = a.u[c], vc = a.v[c], wc = a.w[c];
-    for (int k = 0; k < wdt; k++) {
-        int2 en = ld_entry(e + 32 * k);
-        if (en.x < 0) break;
-        const int f = en.x >> 1;
-        const bool owner = (en.x & 1) == 0;
-        const double4 G = a.fg[f];
-        const double rl = a.rlencos ? a.rlencos[f] : 0.0;
-        if (en.y >= 0) {
-            // interior face (UVWKernels.ipp:145-228)
-            const int ip = owner ? c : en.y, in = owner ? en.y : c;
-            const double facn = G.w, facp = ds(1.0, facn);
-            double du[3], dv[3], dw[3];
-#pragma unroll
-            for (int d = 0; d < 3; d++) {
-                du[d] = da(dm(gr(d, in), facn), dm(gr(d, ip), facp));
-                dv[d] = da(dm(gr(3 + d, in), facn), dm(gr(3 + d, ip), facp));
-                dw[d] = da(dm(gr(6 + d, in), facn), dm(gr(6 + d, ip), facp));
-            }
-            const double visac = da(dm(a.visC[in], facn), dm(a.visC[ip], facp));
-            const double4 Cn = a.cc[in], Cp = a.cc[ip];
-            const double x0 = ds(Cn.x, Cp.x), x1 = ds(Cn.y, Cp.y), x2 = ds(Cn.z, Cp.z);
-            const double visFace = dm(visac, rl);
-            double uF = 0.0, vF = 0.0, wF = 0.0;
-            const int cr = a.carry[f];
-            if (cr >= 0) {
-                uF = a.u[cr]; vF = a.v[cr]; wF = a.w[cr];
-            } else if (cr <= -2) {
-                const double *r = a.regionUVW + 3 * (-2 - cr);
-                uF = r[0]; vF = r[1]; wF = r[2];
-            }
-            const double mf = a.massFlux[f];
-            const double fuce = dm(mf, uF), fvce = dm(mf, vF), fwce = dm(mf, wF);
-            const double fude = dm(visac, da(da(dm(da(du[0], du[0]), G.x), dm(da(du[1], dv[0]), G.y)), dm(da(du[2], dw[0]), G.z)));
-            const double fvde = dm(visac, da(da(dm(da(du[1], dv[0]), G.x), dm(da(dv[1], dv[1]), G.y)), dm(da(dv[2], dw[1]), G.z)));
-            const double fwde = dm(visac, da(da(dm(da(du[2], dw[0]), G.x), dm(da(dw[1], dv[2]), G.y)), dm(da(dw[2], dw[2]), G.z)));
-            const double fmin = std_min(mf, 0.0), fmax = std_max(mf, 0.0);
-            const double uin = owner ? a.u[in] : uc, uip = owner ? uc : a.u[ip];
-            const double vin = owner ? a.v[in] : vc, vip = owner ? vc : a.v[ip];
-            const double win = owner ? a.w[in] : wc, wip = owner ? wc : a.w[ip];
-            const double fuci = da(dm(fmin, uin), dm(fmax, uip));
-            const double fvci = da(dm(fmin, vin), dm(fmax, vip));
-            const double fwci = da(dm(fmin, win), dm(fmax, wip));
-            const double fudi = dm(visFace, dot0(du[0], du[1], du[2], x0, x1, x2));
-            const double fvdi = dm(visFace, dot0(dv[0], dv[1], dv[2], x0, x1, x2));
-            const double fwdi = dm(visFace, dot0(dw[0], dw[1], dw[2], x0, x1, x2));
-            const double bu = dm(a.gammaBlend, ds(fuce, fuci));
-            const double bv = dm(a.gammaBlend, ds(fvce, fvci));
-            const double bw = dm(a.gammaBlend, ds(fwce, fwci));
-            if (owner) {
-                a.rFace[2 * (int64_t) f] = ds(-visFace, std_max(mf, 0.0));
-                a.rFace[2 * (int64_t) f + 1] = da(-visFace, std_min(mf, 0.0));
-                su = ds(da(ds(su, bu), fude), fudi);
-                sv = ds(da(ds(sv, bv), fvde), fvdi);
-                sw = ds(da(ds(sw, bw), fwde), fwdi);
-            } else {
-                su = da(ds(da(su, bu), fude), fudi);
-                sv = da(ds(da(sv, bv), fvde), fvdi);
-                sw = da(ds(da(sw, bw), fwde), fwdi);
-            }
-            continue;
-        }
-        // boundary face: this cell is its owner
-        const int ib = -1 - en.y;
-        const int ir = a.bndRegion[ib];
-        const int it = a.regionType[ir];
-        if (it == CUPCFD_RTYPE_DEFAULT) continue;
-        const double4 X = a.fc[f], Cp = a.cc[c];
-        const double x0 = ds(X.x, Cp.x), x1 = ds(X.y, Cp.y), x2 = ds(X.z, Cp.z);
-        const double du0 = gr(0, c), du1 = gr(1, c), du2 = gr(2, c);
-        const double dv0 = gr(3, c), dv1 = gr(4, c), dv2 = gr(5, c);
-        const double dw0 = gr(6, c), dw1 = gr(7, c), dw2 = gr(8, c);
-        if (it == CUPCFD_RTYPE_INLET || it == CUPCFD_RTYPE_OUTLET) {
-            // UVWKernels.ipp:259-382 (outlet: operands of two sums swapped,
-            // which IEEE addition does not see)
-            double uF, vF, wF, visac;
-            if (it == CUPCFD_RTYPE_INLET) {
-                const double *r = a.regionUVW + 3 * ir;
-                uF = r[0]; vF = r[1]; wF = r[2];
-                visac = a.visB[ib];
-            } else {
-                uF = uc; vF = vc; wF = wc;
-                visac = a.visC[c];
-            }
-            const double visFace = dm(visac, rl);
-            const double fude = dm(visac, da(da(dm(da(du0, du0), G.x), dm(da(du1, dv0), G.y)), dm(da(du2, dw0), G.z)));
-            const double fvde = dm(visac, da(da(dm(da(du1, dv0), G.x), dm(da(dv1, dv1), G.y)), dm(da(dv2, dw1), G.z)));
-            const double fwde = dm(visac, da(da(dm(da(du2, dw0), G.x), dm(da(dw1, dv2), G.y)), dm(da(dw2, dw2), G.z)));
-            const double fudi = dm(visFace, dot0(du0, du1, du2, x0, x1, x2));
-            const double fvdi = dm(visFace, dot0(dv0, dv1, dv2, x0, x1, x2));
-            const double fwdi = dm(visFace, dot0(dw0, dw1, dw2, x0, x1, x2));
-            double mf = a.massFlux[f];
-            if (it == CUPCFD_RTYPE_OUTLET && mf < 0.0) {
-                mf = a.small;
-                a.massFlux[f] = mf;
-            }
-            const double fl = da(-visFace, std_min(mf, 0.0));
-            au = ds(au, fl);
-            su = ds(da(ds(su, dm(fl, uF)), fude), fudi);
-            av = ds(av, fl);
-            sv = ds(da(ds(sv, dm(fl, vF)), fvde), fvdi);
-            aw = ds(aw, fl);
-            sw = ds(da(ds(sw, dm(fl, wF)), fwde), fwdi);
-            a.uB[ib] = uF; a.vB[ib] = vF; a.wB[ib] = wF;
-        } else if (it == CUPCFD_RTYPE_SYMP) {
-            // UVWKernels.ipp:383-436; visFace carried from an earlier face
-            const int g = a.carry[f];
-            const double visFace = g >= 0 ? vis_face_of(a, g) : 0.0;
-            const double visac = a.visC[c];
-            const double us0 = da(uc, dot0(du0, du1, du2, x0, x1, x2));
-            const double us1 = da(vc, dot0(dv0, dv1, dv2, x0, x1, x2));
-            const double us2 = da(wc, dot0(dw0, dw1, dw2, x0, x1, x2));
-            double n0 = ds(0.0, G.x), n1 = ds(0.0, G.y), n2 = ds(0.0, G.z);
-            normalise(n0, n1, n2);
-            const double dp = dot0(us0, us1, us2, n0, n1, n2);
-            const double dn = a.bndDist ? a.bndDist[ib] : 0.0;
-            const double area = X.w, tv = dm(2.0, visac);
-            const double f0 = dm(dvd(dm(tv, dm(dp, n0)), dn), area);
-            const double f1 = dm(dvd(dm(tv, dm(dp, n1)), dn), area);
-            const double f2 = dm(dvd(dm(tv, dm(dp, n2)), dn), area);
-            au = da(au, visFace);
-            av = da(av, visFace);
-            aw = da(aw, visFace);
-            su = ds(da(su, dm(visFace, uc)), f0);
-            sv = ds(da(sv, dm(visFace, vc)), f1);
-            sw = ds(da(sw, dm(visFace, wc)), f2);
-            a.uB[ib] = us0; a.vB[ib] = us1; a.wB[ib] = us2;
-        } else if (it == CUPCFD_RTYPE_WALL) {
-            // UVWKernels.ipp:437-510
-            const double *uw = a.regionUVW + 3 * ir;
-            const double visac = a.visB[ib];
-            const double area = X.w;
-            const double coef = dvd(dm(visac, area), __dsqrt_rn(dot0(x0, x1, x2, x0, x1, x2)));
-            double n0 = G.x, n1 = G.y, n2 = G.z;
-            normalise(n0, n1, n2);
-            const double up0 = ds(uc, uw[0]), up1 = ds(vc, uw[1]), up2 = ds(wc, uw[2]);
-            const double dp = dot0(up0, up1, up2, n0, n1, n2);
-            const double ut0 = ds(up0, dm(dp, n0)), ut1 = ds(up1, dm(dp, n1)), ut2 = ds(up2, dm(dp, n2));
-            const double uvel = da(da(fabs(ut0), fabs(ut1)), fabs(ut2));
-            double f0 = 0.0, f1 = 0.0, f2 = 0.0;
-            if (uvel > a.small) {
-                const double dn = a.bndDist ? a.bndDist[ib] : 0.0;
-                f0 = dm(dvd(dm(visac, ut0), dn), area);
-                f1 = dm(dvd(dm(visac, ut1), dn), area);
-                f2 = dm(dvd(dm(visac, ut2), dn), area);
-            }
-            a.shear[3 * (int64_t) ib] = f0;
-            a.shear[3 * (int64_t) ib + 1] = f1;
-            a.shear[3 * (int64_t) ib + 2] = f2;
-            au = da(au, coef);
-            av = da(av, coef);
-            aw = da(aw, coef);
-            su = ds(da(su, dm(coef, uc)), f0);
-            sv = ds(da(sv, dm(coef, vc)), f1);
-            sw = ds(da(sw, dm(coef, wc)), f2);
-            a.uB[ib] = uw[0]; a.vB[ib] = uw[1]; a.wB[ib] = uw[2];
+    double s[3] = {a.su[c], a.sv_[c], a.sw[c]}, ad[3] = {a.au[c], a.av[c], a.aw[c]};
+    // the chunk's entries first (independent loads), then incidence by incidence
+    for (int k0 = 0; k0 < wdt; k0 += UVW_CHUNK) {
+        int2 en[UVW_CHUNK];
+        load_entries<UVW_CHUNK>(e, k0, wdt, en);
+        for (int j = 0; j < UVW_CHUNK; j++) {
+            if (en[j].x < 0) break;
+            double t[10];
+            int kind = uvw_terms(a, c, en[j], t);
+            uvw_fold(kind, t, s, ad);
         }
     }
-    a.su[c] = su; a.sv_[c] = sv; a.sw[c] = sw;
-    a.au[c] = au; a.av[c] = av; a.aw[c] = aw;
+    a.su[c] = s[0]; a.sv_[c] = s[1]; a.sw[c] = s[2];
+    a.au[c] = ad[0]; a.av[c] = ad[1]; a.aw[c] = ad[2];
 }
 
 // ---------------------------------------------------------------------------

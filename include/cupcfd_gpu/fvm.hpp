@@ -4,6 +4,8 @@
 //   cupcfd::fvm::GradientPhiGaussDolfyn  (include/fvm/implementation/component/GradientKernels.h:48-54)
 //   cupcfd::fvm::FluxMassDolfynFaceLoop  (include/fvm/implementation/component/MassKernels.h:48-81)
 //   cupcfd::fvm::FluxMassDolfynBoundaryLoop1-5, FluxMassDolfynRegionLoop (MassKernels.h:90-171)
+//   cupcfd::fvm::FluxUVWDolfynFaceLoop1, FluxUVWDolfynRegionLoop1, FluxUVWDolfynBndsLoop1
+//                                        (include/fvm/implementation/component/UVWKernels.h:45-92)
 // in namespace cupcfd::fvm::gpu, so a call site switches by namespace only:
 //
 //   status = cupcfd::fvm::gpu::GradientPhiGaussDolfyn(mesh, nGradient, phiCell, nPhiCell,
@@ -152,10 +154,62 @@ int upload(Mesh &mesh, cupcfd_gpu_mesh **out) {
             for (int r = 0; r < nR; r++) sp[r] = (double) mesh.getRegionSplvl(r);
             rc = cupcfd_gpu_mesh_set_region_split(*out, nR, sp.data());
         }
-        if (rc != CUPCFD_E_SUCCESS) {
-            cupcfd_gpu_mesh_destroy(*out);
-            *out = nullptr;
+    }
+    // momentum-loop geometry (getFaceRLencos, getBoundaryDistance); zero on
+    // every MeshSource-built mesh, uploaded only when some entry is not
+    if (rc == CUPCFD_E_SUCCESS) {
+        std::vector<double> rl(nF), bd(nB);
+        bool rlAny = false, bdAny = false;
+        for (int f = 0; f < nF; f++) rlAny |= (rl[f] = (double) mesh.getFaceRLencos(f)) != 0.0;
+        for (int b = 0; b < nB; b++) bdAny |= (bd[b] = (double) mesh.getBoundaryDistance(b)) != 0.0;
+        if (rlAny) rc = cupcfd_gpu_mesh_set_face_rlencos(*out, rl.data(), nF);
+        if (rc == CUPCFD_E_SUCCESS && bdAny) rc = cupcfd_gpu_mesh_set_boundary_distance(*out, bd.data(), nB);
+    }
+    if (rc != CUPCFD_E_SUCCESS && *out) {
+        cupcfd_gpu_mesh_destroy(*out);
+        *out = nullptr;
+    }
+    return rc;
+}
+
+// Boundary shears and region force tangents between the host mesh (the
+// reference's state, get/setBoundaryShear, get/setRegionForceTangent) and the
+// device mesh. toHost: only boundaries of `onlyType` (-1: all) are written.
+template <class Mesh>
+int sync_shear(Mesh &mesh, cupcfd_gpu_mesh *m, bool toHost, int onlyType) {
+    const int nB = (int) mesh.properties.lBoundaries;
+    std::vector<double> sh(3 * (size_t) nB);
+    if (!toHost)
+        for (int b = 0; b < nB; b++) {
+            auto v = mesh.getBoundaryShear(b);
+            for (int d = 0; d < 3; d++) sh[3 * b + d] = (double) v.cmp[d];
         }
+    int rc = cupcfd_gpu_mesh_boundary_shear(m, toHost ? nullptr : sh.data(), toHost ? sh.data() : nullptr, nB);
+    if (rc != CUPCFD_E_SUCCESS || !toHost) return rc;
+    for (int b = 0; b < nB; b++) {
+        if (onlyType >= 0 && (int) mesh.getRegionType(mesh.getBoundaryRegionID(b)) != onlyType) continue;
+        auto v = mesh.getBoundaryShear(b);
+        for (int d = 0; d < 3; d++) v.cmp[d] = sh[3 * b + d];
+        mesh.setBoundaryShear(b, v);
+    }
+    return rc;
+}
+
+template <class Mesh>
+int sync_force_tangent(Mesh &mesh, cupcfd_gpu_mesh *m, bool toHost) {
+    const int nR = (int) mesh.properties.lRegions;
+    std::vector<double> ft(3 * (size_t) nR);
+    if (!toHost)
+        for (int r = 0; r < nR; r++) {
+            auto v = mesh.getRegionForceTangent(r);
+            for (int d = 0; d < 3; d++) ft[3 * r + d] = (double) v.cmp[d];
+        }
+    int rc = cupcfd_gpu_mesh_region_force_tangent(m, toHost ? nullptr : ft.data(), toHost ? ft.data() : nullptr, nR);
+    if (rc != CUPCFD_E_SUCCESS || !toHost) return rc;
+    for (int r = 0; r < nR; r++) {
+        auto v = mesh.getRegionForceTangent(r);
+        for (int d = 0; d < 3; d++) v.cmp[d] = ft[3 * r + d];
+        mesh.setRegionForceTangent(r, v);
     }
     return rc;
 }
@@ -292,6 +346,53 @@ ecode_t FluxMassDolfynRegionLoop(Mesh &mesh, double *flowFact, I nFlowFact, doub
     if (rc != CUPCFD_E_SUCCESS) return (ecode_t) rc;
     return (ecode_t) cupcfd_gpu_flux_mass_dolfyn_region_loop(m, flowFact, (int32_t) nFlowFact, flowRegion,
                                                             (int32_t) nFlowRegion, flowIn);
+}
+
+// FluxUVWDolfynFaceLoop1 (UVWKernels.h:45-67), T = double. rlencos and the
+// boundary distances are those read when the mesh was attached; the wall
+// shears the loop computes are written back through setBoundaryShear.
+template <class Mesh, class I, class Vec>
+ecode_t FluxUVWDolfynFaceLoop1(Mesh &mesh, double gammaBlend, double small, double *uCell, I nUCell, double *vCell,
+                               I nVCell, double *wCell, I nWCell, double *uBoundary, I nUBoundary, double *vBoundary,
+                               I nVBoundary, double *wBoundary, I nWBoundary, double *visEffCell, I nVisEffCell,
+                               double *visEffBoundary, I nVisEffBoundary, double *massFlux, I nMassFlux, Vec *dudx,
+                               I nDudx, Vec *dvdx, I nDvdx, Vec *dwdx, I nDwdx, double *rFace, I nRFace, double *su,
+                               I nSu, double *sv, I nSv, double *sw, I nSw, double *au, I nAu, double *av, I nAv,
+                               double *aw, I nAw) {
+    static_assert(sizeof(I) == 4, "int32 indices");
+    cupcfd_gpu_mesh *m = nullptr;
+    int rc = attach(mesh, &m);
+    if (rc != CUPCFD_E_SUCCESS) return (ecode_t) rc;
+    rc = cupcfd_gpu_flux_uvw_dolfyn_face_loop1(
+        m, gammaBlend, small, uCell, nUCell, vCell, nVCell, wCell, nWCell, uBoundary, nUBoundary, vBoundary,
+        nVBoundary, wBoundary, nWBoundary, visEffCell, nVisEffCell, visEffBoundary, nVisEffBoundary, massFlux,
+        nMassFlux, detail::view_of(dudx), nDudx, detail::view_of(dvdx), nDvdx, detail::view_of(dwdx), nDwdx, rFace,
+        nRFace, su, nSu, sv, nSv, sw, nSw, au, nAu, av, nAv, aw, nAw);
+    if (rc == CUPCFD_E_SUCCESS) rc = detail::sync_shear(mesh, m, true, CUPCFD_RTYPE_WALL);
+    return (ecode_t) rc;
+}
+
+// FluxUVWDolfynRegionLoop1 / FluxUVWDolfynBndsLoop1 (UVWKernels.h:72-92) on
+// the host mesh's force tangents and shears (read, computed on the GPU,
+// written back). The reference's return void; these return the status.
+template <class Mesh>
+ecode_t FluxUVWDolfynRegionLoop1(Mesh &mesh) {
+    cupcfd_gpu_mesh *m = nullptr;
+    int rc = attach(mesh, &m);
+    if (rc == CUPCFD_E_SUCCESS) rc = cupcfd_gpu_flux_uvw_dolfyn_region_loop1(m);
+    if (rc == CUPCFD_E_SUCCESS) rc = detail::sync_force_tangent(mesh, m, true);
+    return (ecode_t) rc;
+}
+
+template <class Mesh>
+ecode_t FluxUVWDolfynBndsLoop1(Mesh &mesh) {
+    cupcfd_gpu_mesh *m = nullptr;
+    int rc = attach(mesh, &m);
+    if (rc == CUPCFD_E_SUCCESS) rc = detail::sync_shear(mesh, m, false, -1);
+    if (rc == CUPCFD_E_SUCCESS) rc = detail::sync_force_tangent(mesh, m, false);
+    if (rc == CUPCFD_E_SUCCESS) rc = cupcfd_gpu_flux_uvw_dolfyn_bnds_loop1(m);
+    if (rc == CUPCFD_E_SUCCESS) rc = detail::sync_force_tangent(mesh, m, true);
+    return (ecode_t) rc;
 }
 
 }  // namespace gpu

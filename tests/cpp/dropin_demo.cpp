@@ -7,7 +7,9 @@
 //   cupcfd::fvm::GradientPhiGaussDolfyn        (reference CPU template)
 //   cupcfd::fvm::gpu::GradientPhiGaussDolfyn   (this library, B200)
 // and likewise FluxMassDolfynFaceLoop with inlet/outlet/symmetry/wall
-// regions, and requires bit-identical results. Exit status 0 on success.
+// regions, the mass boundary / region loops and the momentum loops
+// (FluxUVWDolfynFaceLoop1, RegionLoop1, BndsLoop1), and requires
+// bit-identical results. Exit status 0 on success.
 //
 // Built by `make -C oracle dropin` (needs the reference sources); the binary
 // lands in oracle/_ref/ next to the reference build it links.
@@ -23,6 +25,7 @@
 #include "GradientKernels.h"
 #include "MassKernels.h"
 #include "MeshStructGenSource.h"
+#include "UVWKernels.h"
 #include "cupcfd_gpu/fvm.hpp"
 
 namespace euc = cupcfd::geometry::euclidean;
@@ -93,6 +96,19 @@ int main(int argc, char **argv) {
     std::vector<double> splvl = {0.5, 0.75, 0.25, 1.0};  // getRegionSplvl
     mesh.a.boundaryFace = bface.data();
     mesh.a.regionSplvl = splvl.data();
+    // momentum-loop geometry and state (getFaceRLencos, getBoundaryDistance,
+    // boundary shear, region force tangents), set before the first attach
+    std::vector<double> rlc(nF), bdist(nB), shear(3 * nB, 0.0), ftan(3 * nR, 0.0);
+    {
+        std::mt19937_64 g(7);
+        std::uniform_real_distribution<double> u01(0.0, 1.0);
+        for (auto &x : rlc) x = 0.25 + u01(g);
+        for (auto &x : bdist) x = 0.01 + 0.1 * u01(g);
+    }
+    mesh.a.faceRLencos = rlc.data();
+    mesh.a.boundaryDistance = bdist.data();
+    mesh.a.boundaryShear = shear.data();
+    mesh.a.regionForceTangent = ftan.data();
 
     std::mt19937_64 rng(20261203);
     std::uniform_real_distribution<double> U(-1.0, 1.0);
@@ -186,8 +202,55 @@ int main(int argc, char **argv) {
             s5[0] != s5[1])
             return fail("boundary loop arrays differ from the reference");
     }
+    // ---- FluxUVWDolfynFaceLoop1, RegionLoop1, BndsLoop1 (boundary 0, on face 0, is an inlet)
+    {
+        namespace ref = cupcfd::fvm;
+        namespace g = cupcfd::fvm::gpu;
+        std::uniform_real_distribution<double> Usm(1e-6, 1e-2);
+        auto draw = [&](int n) { std::vector<double> a(n); for (auto &x : a) x = Usm(rng); return a; };
+        std::vector<double> uc = draw(nC), vc = draw(nC), wc = draw(nC), visc = draw(nC), visb = draw(nB);
+        std::vector<double> mf0 = draw(nF);
+        for (int f = 0; f < nF; f += 3) mf0[f] = -mf0[f];
+        std::vector<euc::EuclideanVector<double, 3>> du(nC), dv(nC), dw(nC);
+        for (int c = 0; c < nC; c++)
+            for (int d = 0; d < 3; d++) { du[c].cmp[d] = 1e-2 * N01(rng); dv[c].cmp[d] = 1e-2 * N01(rng); dw[c].cmp[d] = 1e-2 * N01(rng); }
+        std::vector<double> mf[2] = {mf0, mf0}, rf[2], ub[2], vb[2], wb[2], s[2][6];
+        std::vector<double> rf0(2 * nF);
+        for (auto &x : rf0) x = U(rng);
+        std::vector<double> sa0 = draw(nC), ub0 = draw(nB);
+        for (int r = 0; r < 2; r++) {
+            rf[r] = rf0; ub[r] = ub0; vb[r] = ub0; wb[r] = ub0;
+            for (int q = 0; q < 6; q++) s[r][q] = sa0;
+        }
+        cupcfd::error::eCodes st0 = ref::FluxUVWDolfynFaceLoop1(
+            mesh, 0.9, 1e-18, uc.data(), nC, vc.data(), nC, wc.data(), nC, ub[0].data(), nB, vb[0].data(), nB,
+            wb[0].data(), nB, visc.data(), nC, visb.data(), nB, mf[0].data(), nF, du.data(), nC, dv.data(), nC, dw.data(),
+            nC, rf[0].data(), 2 * nF, s[0][0].data(), nC, s[0][1].data(), nC, s[0][2].data(), nC, s[0][3].data(), nC,
+            s[0][4].data(), nC, s[0][5].data(), nC);
+        std::vector<double> shearRef = shear;
+        std::fill(shear.begin(), shear.end(), 0.0);
+        cupcfd::error::eCodes st1 = g::FluxUVWDolfynFaceLoop1(
+            mesh, 0.9, 1e-18, uc.data(), nC, vc.data(), nC, wc.data(), nC, ub[1].data(), nB, vb[1].data(), nB,
+            wb[1].data(), nB, visc.data(), nC, visb.data(), nB, mf[1].data(), nF, du.data(), nC, dv.data(), nC, dw.data(),
+            nC, rf[1].data(), 2 * nF, s[1][0].data(), nC, s[1][1].data(), nC, s[1][2].data(), nC, s[1][3].data(), nC,
+            s[1][4].data(), nC, s[1][5].data(), nC);
+        if (st0 != cupcfd::error::E_SUCCESS || st1 != cupcfd::error::E_SUCCESS) return fail("momentum loop status");
+        if (mf[0] != mf[1] || rf[0] != rf[1] || ub[0] != ub[1] || vb[0] != vb[1] || wb[0] != wb[1] || shear != shearRef)
+            return fail("momentum loop face / boundary arrays differ from the reference");
+        for (int q = 0; q < 6; q++)
+            if (s[0][q] != s[1][q]) return fail("momentum loop su..aw differ from the reference");
+        std::fill(ftan.begin(), ftan.end(), 7.0);
+        ref::FluxUVWDolfynRegionLoop1(mesh);
+        ref::FluxUVWDolfynBndsLoop1(mesh);
+        std::vector<double> ftRef = ftan;
+        std::fill(ftan.begin(), ftan.end(), 7.0);
+        if (g::FluxUVWDolfynRegionLoop1(mesh) != cupcfd::error::E_SUCCESS ||
+            g::FluxUVWDolfynBndsLoop1(mesh) != cupcfd::error::E_SUCCESS)
+            return fail("momentum region / boundary loop status");
+        if (ftan != ftRef) return fail("region force tangents differ from the reference");
+    }
     cupcfd::fvm::gpu::release(mesh);
-    std::printf("OK dropin %dx%dx%d: %d cells, %d faces; gradient (nGradient 1-3), mass flux and the boundary / "
-                "region loops bit-identical\n", nx, ny, nz, nC, nF);
+    std::printf("OK dropin %dx%dx%d: %d cells, %d faces; gradient (nGradient 1-3), mass flux, the boundary / "
+                "region loops and the momentum loops bit-identical\n", nx, ny, nz, nC, nF);
     return 0;
 }
