@@ -525,6 +525,7 @@ def run_gpu(a):
     if not a.no_uvw:
         uvw = bench_uvw(cg, mesh, dev, st, g, max(3, K // 4), 3, peak)
         uvw["roofline"]["peak_source"] = peak_src
+        uvw["roofline"]["traffic"] = profile_traffic().get(f"k_uvw_f64@{n}")
         if rank == 0 and world == 1 and not a.no_cpu:
             try:
                 uvw["cpu_reference"] = cpu_uvw(a.cpu_n, 5)

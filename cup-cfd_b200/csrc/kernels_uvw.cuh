@@ -64,7 +64,7 @@ struct UvwArgs {
     const double *regionUVW;
     const double *rlencos;                 // [nF] internal, null = zero
     const double *bndDist;                 // [nB], null = zero
-    const int *carry;                      // [nF] internal
+    const int *carry;                      // [nF] internal; null when no region is an inlet, outlet or symmetry
     double gammaBlend, small;
     const double *u, *v, *w, *visC;        // [nC] internal
     const double *visB;                    // [nB]
@@ -127,7 +127,7 @@ __device__ __forceinline__ int uvw_terms(const UvwArgs &a, int c, int2 en, doubl
         const double x0 = ds(Cn.x, Cp.x), x1 = ds(Cn.y, Cp.y), x2 = ds(Cn.z, Cp.z);
         const double visFace = dm(visac, rl);
         double uF = 0.0, vF = 0.0, wF = 0.0;
-        const int cr = a.carry[f];
+        const int cr = a.carry ? a.carry[f] : -1;
         if (cr >= 0) {
             uF = a.u[cr]; vF = a.v[cr]; wF = a.w[cr];
         } else if (cr <= -2) {
@@ -199,7 +199,7 @@ __device__ __forceinline__ int uvw_terms(const UvwArgs &a, int c, int2 en, doubl
     double Xc, f0 = 0.0, f1 = 0.0, f2 = 0.0;
     if (it == CUPCFD_RTYPE_SYMP) {
         // UVWKernels.ipp:383-436; visFace carried from an earlier face
-        const int g = a.carry[f];
+        const int g = a.carry ? a.carry[f] : -1;
         Xc = g >= 0 ? vis_face_of(a, g) : 0.0;
         const double visac = a.visC[c];
         const double us0 = da(uc, dot0(du0, du1, du2, x0, x1, x2));

@@ -76,7 +76,11 @@ int run_face_loop(cupcfd_gpu_mesh *m, double gammaBlend, double small, const dou
     a.fcells = m->faceCells;
     a.fg = m->fg64; a.fc = m->fc64; a.cc = m->cc64;
     a.bndRegion = m->bndRegion; a.regionType = m->regionType; a.regionUVW = m->regionUVW;
-    a.rlencos = m->rlencos; a.bndDist = m->bndDist; a.carry = m->uvwCarry;
+    // the carried values matter only with an inlet, outlet or symmetry region
+    bool carried = false;
+    for (int t : m->hRegionType)
+        carried |= t == CUPCFD_RTYPE_INLET || t == CUPCFD_RTYPE_OUTLET || t == CUPCFD_RTYPE_SYMP;
+    a.rlencos = m->rlencos; a.bndDist = m->bndDist; a.carry = carried ? m->uvwCarry : nullptr;
     a.gammaBlend = gammaBlend; a.small = small;
     a.u = u; a.v = v; a.w = w; a.visC = visC; a.visB = visB;
     a.grads = grads; a.ldg = ldg;
