@@ -8,14 +8,17 @@
 //
 // Layout (little-endian): a 64-byte header
 //   char magic[8] = "CUPCFDM1"; int32 version = 1; int32 nCells, nFaces,
-//   nBoundaries, nRegions; int32 flags (bit 0: xpac/xnac present);
+//   nBoundaries, nRegions; int32 flags (bit 0: xpac/xnac present, bit 1:
+//   rlencos present, bit 2: boundary distances present);
 //   int32 reserved[8] = 0
 // then, in this order, faceCell1, faceCell2, faceBnd [nFaces] int32;
 // faceLambda, faceArea [nFaces] and faceNorm, faceCenter [3 nFaces] float64;
 // faceXpac, faceXnac [3 nFaces] float64 when flags bit 0 is set; cellCenter [3 nCells],
 // cellVolume [nCells] float64; regionType [nRegions] int32, regionUVW
 // [3 nRegions], regionDen, regionSplvl [nRegions] float64; bndRegion
-// [nBoundaries] int32; and last the FNV-1a 64-bit hash of everything before it.
+// [nBoundaries] int32; faceRLencos [nFaces] float64 when flags bit 1 is set;
+// boundaryDistance [nBoundaries] float64 when flags bit 2 is set; and last
+// the FNV-1a 64-bit hash of everything before it.
 #include <cstdio>
 #include <cstring>
 #include <exception>
@@ -107,6 +110,21 @@ int mesh_save(const cupcfd_gpu_mesh *m, const char *path) {
             xn[o] = b[f].x; xn[o + 1] = b[f].y; xn[o + 2] = b[f].z;
         }
     }
+    std::vector<double> rl, bd;  // momentum-loop geometry, when set
+    if (m->rlencos) {
+        flags |= 2;
+        std::vector<double> a;
+        std::vector<int> n2o;
+        CG_TRY(download(a, (const double *) m->rlencos, (size_t) nF, st));
+        CG_TRY(download(n2o, (const int *) m->faceN2O, (size_t) nF, st));
+        CG_CHECK_CUDA(cudaStreamSynchronize(st));
+        rl.resize(nF);
+        for (int f = 0; f < nF; f++) rl[n2o[f]] = a[f];
+    }
+    if (m->bndDist) {
+        flags |= 4;
+        CG_TRY(download(bd, (const double *) m->bndDist, (size_t) nB, st));
+    }
     std::vector<int32_t> rtype(m->hRegionType.begin(), m->hRegionType.end()), breg;
     std::vector<double> ruvw, rden, rsp;
     CG_TRY(download(ruvw, (const double *) m->regionUVW, 3 * (size_t) nR, st));
@@ -131,6 +149,8 @@ int mesh_save(const cupcfd_gpu_mesh *m, const char *path) {
     if (flags & 1) ok = ok && put(fl, h, xp) && put(fl, h, xn);
     ok = ok && put(fl, h, cc) && put(fl, h, vol) && put(fl, h, rtype) && put(fl, h, ruvw) && put(fl, h, rden) &&
          put(fl, h, rsp) && put(fl, h, breg);
+    if (flags & 2) ok = ok && put(fl, h, rl);
+    if (flags & 4) ok = ok && put(fl, h, bd);
     ok = ok && fwrite(&h.h, sizeof(h.h), 1, fl.f) == 1;
     CG_RETURN_IF(!ok, CUPCFD_E_ERROR, std::string("mesh_save: write to ") + path + " failed");
     CG_RETURN_IF(fclose(fl.f) != 0, CUPCFD_E_ERROR, std::string("mesh_save: closing ") + path + " failed");
@@ -148,12 +168,13 @@ int mesh_load(const char *path, const cupcfd_mesh_options *opt, cupcfd_gpu_mesh 
     CG_RETURN_IF(fread(&hd, sizeof(hd), 1, fl.f) != 1 || std::memcmp(hd.magic, MAGIC, 8) != 0,
                  CUPCFD_E_INVALID_FILE_FORMAT, std::string("mesh_load: ") + path + " is not a mesh file");
     CG_RETURN_IF(hd.version != VERSION, CUPCFD_E_INVALID_FILE_FORMAT, "mesh_load: unknown format version");
-    CG_RETURN_IF(hd.nCells < 1 || hd.nFaces < 1 || hd.nBnd < 0 || hd.nRegions < 1 || (hd.flags & ~1) != 0,
+    CG_RETURN_IF(hd.nCells < 1 || hd.nFaces < 1 || hd.nBnd < 0 || hd.nRegions < 1 || (hd.flags & ~7) != 0,
                  CUPCFD_E_INVALID_FILE_FORMAT, "mesh_load: header out of range");
     const size_t nC = hd.nCells, nF = hd.nFaces, nB = hd.nBnd, nR = hd.nRegions;
     // the size the header implies, checked before anything is allocated
     size_t want = sizeof(Header) + nF * (3 * 4 + 2 * 8 + 6 * 8) + ((hd.flags & 1) ? nF * 6 * 8 : 0) + nC * 4 * 8 +
-                  nR * (4 + 5 * 8) + nB * 4 + sizeof(uint64_t);
+                  nR * (4 + 5 * 8) + nB * 4 + ((hd.flags & 2) ? nF * 8 : 0) + ((hd.flags & 4) ? nB * 8 : 0) +
+                  sizeof(uint64_t);
     CG_RETURN_IF(fseek(fl.f, 0, SEEK_END) != 0, CUPCFD_E_ERROR, "mesh_load: cannot seek");
     long have = ftell(fl.f);
     CG_RETURN_IF(have < 0 || (size_t) have != want, CUPCFD_E_INVALID_FILE_FORMAT,
@@ -162,12 +183,14 @@ int mesh_load(const char *path, const cupcfd_mesh_options *opt, cupcfd_gpu_mesh 
     Fnv h;
     h.add(&hd, sizeof(hd));
     std::vector<int32_t> c1, c2, bnd, rtype, breg;
-    std::vector<double> lam, area, S, X, xp, xn, cc, vol, ruvw, rden, rsp;
+    std::vector<double> lam, area, S, X, xp, xn, cc, vol, ruvw, rden, rsp, rl, bd;
     bool ok = get(fl, h, c1, nF) && get(fl, h, c2, nF) && get(fl, h, bnd, nF) && get(fl, h, lam, nF) &&
               get(fl, h, area, nF) && get(fl, h, S, 3 * nF) && get(fl, h, X, 3 * nF);
     if (hd.flags & 1) ok = ok && get(fl, h, xp, 3 * nF) && get(fl, h, xn, 3 * nF);
     ok = ok && get(fl, h, cc, 3 * nC) && get(fl, h, vol, nC) && get(fl, h, rtype, nR) && get(fl, h, ruvw, 3 * nR) &&
          get(fl, h, rden, nR) && get(fl, h, rsp, nR) && get(fl, h, breg, nB);
+    if (hd.flags & 2) ok = ok && get(fl, h, rl, nF);
+    if (hd.flags & 4) ok = ok && get(fl, h, bd, nB);
     uint64_t stored = 0;
     ok = ok && fread(&stored, sizeof(stored), 1, fl.f) == 1;
     CG_RETURN_IF(!ok, CUPCFD_E_INVALID_FILE_FORMAT, std::string("mesh_load: ") + path + " is truncated");
@@ -188,6 +211,8 @@ int mesh_load(const char *path, const cupcfd_mesh_options *opt, cupcfd_gpu_mesh 
     int rc = cupcfd_gpu_mesh_set_regions(m, (int32_t) nR, rtype.data(), ruvw.data(), rden.data(), breg.data(),
                                          (int32_t) nB);
     if (rc == CUPCFD_E_SUCCESS) rc = cupcfd_gpu_mesh_set_region_split(m, (int32_t) nR, rsp.data());
+    if (rc == CUPCFD_E_SUCCESS && !rl.empty()) rc = cupcfd_gpu_mesh_set_face_rlencos(m, rl.data(), (int32_t) nF);
+    if (rc == CUPCFD_E_SUCCESS && (hd.flags & 4)) rc = cupcfd_gpu_mesh_set_boundary_distance(m, bd.data(), (int32_t) nB);
     if (rc != CUPCFD_E_SUCCESS) {
         std::string msg = cupcfd_gpu_last_error();
         cupcfd_gpu_mesh_destroy(m);

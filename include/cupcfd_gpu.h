@@ -2,7 +2,11 @@
  * cupcfd_gpu.h - C ABI of the B200 (sm_100a) implementation of CUP-CFD's
  * finite-volume face-loop path: the Gauss-Green cell gradient
  * (GradientPhiGaussDolfyn) and the face mass-flux loop
- * (FluxMassDolfynFaceLoop) over the reference's MiniSoA mesh.
+ * (FluxMassDolfynFaceLoop) over the reference's MiniSoA mesh, with their
+ * adjoints; and the operators either side of it: the mass boundary / region
+ * loops (FluxMassDolfynBoundaryLoop1-5, FluxMassDolfynRegionLoop), the
+ * momentum face loop (FluxUVWDolfynFaceLoop1, RegionLoop1, BndsLoop1) and
+ * mesh files.
  *
  * Plain C: pointers, sizes and int status codes only. Status codes are the
  * reference's eCodes values (include/error/Error.h:32-144): CUPCFD_E_SUCCESS
@@ -11,7 +15,7 @@
  *
  * Two layers:
  *  1. Reference-facing calls (cupcfd_gpu_gradient_phi_gauss_dolfyn,
- *     cupcfd_gpu_flux_mass_dolfyn_face_loop): HOST buffers in the
+ *     cupcfd_gpu_flux_mass_dolfyn_*, cupcfd_gpu_flux_uvw_dolfyn_*): HOST buffers in the
  *     reference's numbering and layout, including the 32-byte (double) /
  *     24-byte (float) stride of the vptr-carrying EuclideanVector<T,3>
  *     arrays. Each call copies inputs to the device, runs, and copies the
@@ -167,14 +171,16 @@ int cupcfd_gpu_mesh_create_jittered(int32_t nx, int32_t ny, int32_t nz, double j
  * part of this build, so a device mesh is saved to, and reloaded from, a
  * raw-binary file holding its source arrays in the reference's numbering:
  * a 64-byte header (magic "CUPCFDM1", version 1, nCells, nFaces,
- * nBoundaries, nRegions, flags bit 0 = xpac/xnac present), then faceCell1,
- * faceCell2, faceBnd (int32), faceLambda, faceArea, faceNorm[3],
- * faceCenter[3], [faceXpac[3], faceXnac[3]], cellCenter[3], cellVolume
- * (float64), regionType (int32), regionUVW[3], regionDen, regionSplvl
- * (float64), bndRegion (int32), and an FNV-1a 64-bit hash of all the bytes
- * before it. Little-endian. Loading rebuilds the device layout exactly as
- * cupcfd_gpu_mesh_create with `opt`, then installs the regions and split
- * levels, so kernels on a loaded mesh give the saved mesh's bits.
+ * nBoundaries, nRegions, flags: bit 0 xpac/xnac present, bit 1 rlencos
+ * present, bit 2 boundary distances present), then faceCell1, faceCell2,
+ * faceBnd (int32), faceLambda, faceArea, faceNorm[3], faceCenter[3],
+ * [faceXpac[3], faceXnac[3]], cellCenter[3], cellVolume (float64),
+ * regionType (int32), regionUVW[3], regionDen, regionSplvl (float64),
+ * bndRegion (int32), [faceRLencos], [boundaryDistance] (float64), and an
+ * FNV-1a 64-bit hash of all the bytes before it. Little-endian. Loading rebuilds the device layout exactly as
+ * cupcfd_gpu_mesh_create with `opt`, then installs the regions, split
+ * levels, rlencos and boundary distances, so kernels on a loaded mesh give
+ * the saved mesh's bits.
  * Errors: CUPCFD_E_FILE_MISSING (cannot open), CUPCFD_E_INVALID_FILE_FORMAT
  * (magic, version, header ranges, size, truncation or hash wrong), as the
  * reference's readers return (Error.h:44, Error.h:139). */

@@ -31,9 +31,10 @@ def _fnv1a64(data: bytes) -> int:
     return h
 
 
-def mesh_file_bytes(m, splvl):
+def mesh_file_bytes(m, splvl, rlencos=None, bnd_dist=None):
     """Bytes of a mesh file for the host mesh ``m`` (oracle dict, regions
-    optional) and split levels ``splvl``."""
+    optional), split levels ``splvl`` and the optional momentum-loop
+    geometry (rlencos per face, distance per boundary)."""
     nC, nF, nB = int(m["nCells"]), int(m["nFaces"]), int(m["nBnd"])
     nR = int(m.get("nRegions", 1))
     rtype = np.asarray(m.get("regionType", np.zeros(1, np.int32)), np.int32)
@@ -42,18 +43,23 @@ def mesh_file_bytes(m, splvl):
     breg = np.asarray(m.get("bndRegion", np.zeros(nB, np.int32)), np.int32)
     xp = np.asarray(m.get("faceXpac", np.zeros((nF, 3))), np.float64)
     xn = np.asarray(m.get("faceXnac", np.zeros((nF, 3))), np.float64)
-    flags = int(bool(np.any(xp != 0) or np.any(xn != 0)))
+    flags = int(bool(np.any(xp != 0) or np.any(xn != 0))) | (2 if rlencos is not None else 0) | \
+        (4 if bnd_dist is not None else 0)
     hdr = b"CUPCFDM1" + struct.pack("<6i", 1, nC, nF, nB, nR, flags) + bytes(32)
     parts = [hdr]
     for k in ("faceCell1", "faceCell2", "faceBnd"):
         parts.append(np.ascontiguousarray(m[k], "<i4").tobytes())
     for k in ("faceLambda", "faceArea", "faceNorm", "faceCenter"):
         parts.append(np.ascontiguousarray(m[k], "<f8").tobytes())
-    if flags:
+    if flags & 1:
         parts += [np.ascontiguousarray(xp, "<f8").tobytes(), np.ascontiguousarray(xn, "<f8").tobytes()]
     parts += [np.ascontiguousarray(m["cellCenter"], "<f8").tobytes(), np.ascontiguousarray(m["cellVolume"], "<f8").tobytes(),
               rtype.astype("<i4").tobytes(), ruvw.astype("<f8").tobytes(), rden.astype("<f8").tobytes(),
               np.asarray(splvl, "<f8").tobytes(), breg.astype("<i4").tobytes()]
+    if rlencos is not None:
+        parts.append(np.ascontiguousarray(rlencos, "<f8").tobytes())
+    if bnd_dist is not None:
+        parts.append(np.ascontiguousarray(bnd_dist, "<f8").tobytes())
     body = b"".join(parts)
     return body + struct.pack("<Q", _fnv1a64(body))
 
@@ -91,10 +97,12 @@ def test_missing_file(cg, tmp_path):
     assert rc == cg.E_FILE_MISSING and "cannot open" in msg
 
 
-@pytest.mark.parametrize("xpac", [False, True])
-def test_damaged_files_rejected(cg, tmp_path, xpac):
+@pytest.mark.parametrize("xpac,geom", [(False, False), (True, False), (False, True)])
+def test_damaged_files_rejected(cg, tmp_path, xpac, geom):
     m, splvl = _case(xpac)
-    good = mesh_file_bytes(m, splvl)
+    rng = np.random.default_rng(5)
+    rl, bd = (rng.uniform(0.1, 1, m["nFaces"]), rng.uniform(0.01, 0.1, m["nBnd"])) if geom else (None, None)
+    good = mesh_file_bytes(m, splvl, rl, bd)
     p = tmp_path / "m.cupcfdm"
 
     def rc_of(data):
@@ -106,7 +114,9 @@ def test_damaged_files_rejected(cg, tmp_path, xpac):
         "version": good[:8] + struct.pack("<i", 2) + good[12:],
         "cells0": good[:12] + struct.pack("<i", 0) + good[16:],
         "faces+1": good[:16] + struct.pack("<i", int(m["nFaces"]) + 1) + good[20:],
-        "flags": good[:28] + struct.pack("<i", 2) + good[32:],
+        "flags": good[:28] + struct.pack("<i", 8) + good[32:],
+        "flags without arrays": good[:28] + struct.pack("<i", 6 | (1 if xpac else 0)) + good[32:] if not geom else
+        good[:28] + struct.pack("<i", 1 if xpac else 0) + good[32:],
         "truncated": good[:-9],
         "extra": good + b"\0",
         "header only": good[:64],
@@ -222,3 +232,22 @@ def test_structgen_mesh_round_trip(cg, gpu, tmp_path):
     assert p.read_bytes() == mesh_file_bytes(O.structgen(9, 8, 7), np.zeros(1))
     with pytest.raises(cg.CupcfdError):
         cg.Mesh.load(tmp_path / "absent.cupcfdm")
+
+
+@pytest.mark.gpu
+def test_round_trip_momentum_geometry(cg, gpu, tmp_path):
+    """rlencos and boundary distances travel with the file, and the momentum
+    loop gives the same bits on the loaded mesh."""
+    from test_gpu_uvw import _host, _check
+    from test_oracle_vs_reference import uvw_case
+    m, rng = uvw_case("jitter", 80, "outlet")
+    rl, bd = rng.uniform(0.1, 2.0, m["nFaces"]), rng.uniform(0.01, 0.2, m["nBnd"])
+    mesh = cg.Mesh.from_arrays(m, order=cg.ORDER_MORTON)
+    assert mesh.set_regions(m["regionType"], m["regionUVW"], m["regionDen"], m["bndRegion"]) == cg.E_SUCCESS
+    assert mesh.set_face_rlencos(rl) == cg.E_SUCCESS and mesh.set_boundary_distance(bd) == cg.E_SUCCESS
+    p = tmp_path / "g.cupcfdm"
+    assert mesh.save(p) == cg.E_SUCCESS
+    assert p.read_bytes() == mesh_file_bytes(m, np.zeros(m["nRegions"]), rl, bd)
+    loaded = cg.Mesh.load(p, order=cg.ORDER_RCM)
+    f = O.uvw_fields(m, 81)
+    _check(_host(cg, loaded, f), O.uvw_face_loop1(m, f, rl, bd))
