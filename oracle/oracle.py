@@ -166,6 +166,69 @@ def jitter(nx, ny, nz, amount=0.25, seed=1, permute=True):
     return _finish_mesh(m)
 
 
+def merge_cells(m, frac=0.3, seed=1, max_cells=3):
+    """A polyhedral mesh from a hex mesh: interior faces removed at random
+    (a fraction ``frac`` of them, in a seeded order) with their two cells
+    merged into one; a merged cell holds at most ``max_cells`` hexahedra
+    (cells of 6 to 14 faces, more with a larger cap), so the cells of a
+    32-cell slice have different face counts. The merged cell keeps its lowest label; cells are relabelled
+    in ascending order, faces keep their relative order, boundaries their
+    ids. Centre = mean of the merged centres, volume = their sum. Geometry is
+    then not that of a real polyhedron, which the face loops do not need:
+    they are checked for bit-identity on whatever arrays the mesh holds."""
+    nc, nf = int(m["nCells"]), int(m["nFaces"])
+    rng = np.random.Generator(np.random.Philox(key=seed))
+    parent = np.arange(nc)
+
+    def find(c):
+        while parent[c] != c:
+            parent[c] = parent[parent[c]]
+            c = parent[c]
+        return c
+
+    c1, c2 = m["faceCell1"].astype(np.int64), m["faceCell2"].astype(np.int64)
+    interior = np.flatnonzero(c2 >= 0)
+    order = rng.permutation(interior)
+    removed = np.zeros(nf, bool)
+    size = np.ones(nc, np.int64)
+    for f in order[: int(frac * len(interior))]:
+        a, b = find(c1[f]), find(c2[f])
+        if a == b or size[a] + size[b] > max_cells:
+            continue
+        lo, hi = min(a, b), max(a, b)
+        parent[hi] = lo
+        size[lo] += size[hi]
+    rep = np.array([find(c) for c in range(nc)])
+    # faces whose two cells now coincide disappear
+    for f in interior:
+        if rep[c1[f]] == rep[c2[f]]:
+            removed[f] = True
+    keep_cells = np.flatnonzero(rep == np.arange(nc))
+    new_id = -np.ones(nc, np.int64)
+    new_id[keep_cells] = np.arange(len(keep_cells))
+    keep_f = np.flatnonzero(~removed)
+    out = dict(m)
+    out["nCells"], out["nFaces"] = int(len(keep_cells)), int(len(keep_f))
+    out["faceCell1"] = new_id[rep[c1[keep_f]]].astype(np.int32)
+    c2k = c2[keep_f]
+    out["faceCell2"] = np.where(c2k >= 0, new_id[rep[np.maximum(c2k, 0)]], -1).astype(np.int32)
+    for k in ("faceBnd", "faceLambda", "faceArea"):
+        out[k] = np.ascontiguousarray(m[k][keep_f])
+    for k in ("faceNorm", "faceCenter", "faceXpac", "faceXnac"):
+        out[k] = np.ascontiguousarray(m[k][keep_f])
+    cc = np.zeros((len(keep_cells), 3))
+    cnt = np.zeros(len(keep_cells))
+    vol = np.zeros(len(keep_cells))
+    np.add.at(cc, new_id[rep], m["cellCenter"])
+    np.add.at(cnt, new_id[rep], 1.0)
+    np.add.at(vol, new_id[rep], m["cellVolume"])
+    out["cellCenter"] = cc / cnt[:, None]
+    out["cellVolume"] = vol
+    for k in ("cellPerm", "facePerm"):
+        out.pop(k, None)
+    return out
+
+
 def cell_face_csr(m):
     nc, nf = m["nCells"], m["nFaces"]
     nnz = int(nf + np.count_nonzero(m["faceCell2"] >= 0))

@@ -209,3 +209,35 @@ def test_uvw_face_loop1_bit_exact(mk, first, geom):
     assert np.array_equal(ft0, O.uvw_region_loop1(m)) and not ft0.any()
     ft1 = R.uvw_bnds_loop1()
     assert_same_bits({"ft": O.uvw_bnds_loop1(m, got["shear"], ft0)}, {"ft": ft1}, ("ft",))
+
+
+@pytest.mark.parametrize("max_cells", [3, 6])
+def test_polyhedral_mesh_bit_exact(max_cells):
+    """Cells of 6 to 26 faces (hexahedra merged across removed faces): the
+    gradient, the full mass-flux loop with regions, the boundary loops and
+    the momentum loop agree with the reference templates bit for bit."""
+    m = O.merge_cells(O.jitter(9, 8, 7, 0.25, seed=5, permute=True), 0.4, 11, max_cells=max_cells)
+    m, splvl, rng = _with_regions(m, 90 + max_cells)
+    assert m["faceBnd"][0] >= 0
+    m["bndRegion"][m["faceBnd"][0]] = 2
+    deg = np.diff(O.cell_face_csr(m)[0])
+    assert deg.min() == 6 and deg.max() >= 14
+    f = O.fields(m, 91, full=True)
+    f["massFlux"] = rng.standard_normal(m["nFaces"])
+    R = O.RefKernels(m)
+    for ng in (1, 2):
+        rc, g, go, _ = R.gradient(f["phi"], f["phiB"], ng)
+        rc2, g2, go2 = O.gradient(m, f["phi"], f["phiB"], ng)
+        assert rc == rc2 == O.E_SUCCESS and np.array_equal(g, g2) and np.array_equal(go, go2)
+    rc, want, _ = R.flux_mass(f)
+    rc2, got = O.flux_mass_face_loop(m, f)
+    assert rc == rc2 == O.E_SUCCESS
+    for k in ("massFlux", "su", "rface", "denB"):
+        assert np.array_equal(got[k], want[k]), k
+    R.boundary_loops(splvl)
+    mf = rng.uniform(1e-6, 1e-2, m["nFaces"])
+    assert O.boundary_loop1(m, mf) == R.boundary_loop1(mf)
+    fu = O.uvw_fields(m, 92)
+    rl, bd = rng.uniform(0.1, 2.0, m["nFaces"]), rng.uniform(0.01, 0.2, m["nBnd"])
+    rc, want, _ = R.uvw_geometry(rl, bd).uvw_face_loop1(fu)
+    assert_same_bits(O.uvw_face_loop1(m, fu, rl, bd), want, O.UVW_INOUT + ("shear",))
