@@ -112,6 +112,8 @@ SIGNATURES = {
     "cupcfd_gpu_flux_uvw_dolfyn_bnds_loop1": ([_VP], _I),
     "cupcfd_gpu_dev_uvw_face_loop1": ([_VP, _D, _D] + [_VP] * 10 + [_I64] + [_VP] * 8, _I),
     "cupcfd_gpu_dev_uvw_region_loop1": ([_VP, _VP], _I),
+    "cupcfd_gpu_dev_halo_pack": ([_VP, _I, _I, _I64, _VP, _I, _VP, _VP], _I),
+    "cupcfd_gpu_dev_halo_unpack": ([_VP, _I, _I, _I, _VP, _VP, _I64, _VP], _I),
     "cupcfd_gpu_dev_uvw_bnds_loop1": ([_VP, _VP], _I),
     "cupcfd_gpu_mesh_set_fusion": ([_VP, _I], _I),
     "cupcfd_gpu_mesh_check_status": ([_VP, _VP], _I),

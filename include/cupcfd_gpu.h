@@ -478,6 +478,24 @@ int cupcfd_gpu_dev_uvw_face_loop1(cupcfd_gpu_mesh *mesh, double gammaBlend, doub
 int cupcfd_gpu_dev_uvw_region_loop1(cupcfd_gpu_mesh *mesh, void *stream);
 int cupcfd_gpu_dev_uvw_bnds_loop1(cupcfd_gpu_mesh *mesh, void *stream);
 
+/* ------------------------------------------------------------------------ */
+/* halo exchange of a mesh split across ranks                               */
+/* ------------------------------------------------------------------------ */
+
+/* Pack / unpack halves of a two-sided halo exchange (replace
+ * ExchangePatternTwoSidedNonBlocking::packSendBuffer / unpackRecvBuffer,
+ * src/comm/implementation/component/ExchangePatternTwoSidedNonBlocking.cpp:129-170),
+ * on device arrays and a caller stream; the transfer between them is the
+ * caller's (NCCL send / recv). Element-major buffers:
+ *   pack:   dst[i*ncomp + c]  = src[c*ld + idx[i]]   (i < n, c < ncomp)
+ *   unpack: dst[c*ld + idx[i]] = src[i*ncomp + c]
+ * elemSize 4, 8 or 16 (a float4 state record as one element); idx[n] are
+ * cells in the mesh's internal numbering (device int32). */
+int cupcfd_gpu_dev_halo_pack(const void *src, int32_t elemSize, int32_t ncomp, int64_t ld, const int32_t *idx,
+                             int32_t n, void *dst, void *stream);
+int cupcfd_gpu_dev_halo_unpack(const void *src, int32_t elemSize, int32_t ncomp, int32_t n, const int32_t *idx,
+                               void *dst, int64_t ld, void *stream);
+
 /* Number of kernels this library launched since load (all threads). */
 int64_t cupcfd_gpu_launch_count(void);
 
