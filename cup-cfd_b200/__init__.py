@@ -87,6 +87,9 @@ SIGNATURES = {
     "cupcfd_gpu_mesh_destroy": ([_VP], _I),
     "cupcfd_gpu_mesh_save": ([_VP, C.c_char_p], _I),
     "cupcfd_gpu_mesh_load": ([C.c_char_p, _VP, _VP], _I),
+    "cupcfd_gpu_hdf5_mesh_counts": ([C.c_char_p, _VP, _VP, _VP, _VP], _I),
+    "cupcfd_gpu_hdf5_mesh_read": ([C.c_char_p, _I, _I, _I] + [_VP] * 11, _I),
+    "cupcfd_gpu_mesh_load_hdf5": ([C.c_char_p, _VP, _VP], _I),
     "cupcfd_gpu_mesh_get_info": ([_VP, _VP], _I),
     "cupcfd_gpu_mesh_set_regions": ([_VP, _I, _VP, _VP, _VP, _VP, _I], _I),
     "cupcfd_gpu_mesh_set_region_split": ([_VP, _I, _VP], _I),
@@ -295,6 +298,14 @@ class Mesh:
         if return_code:
             return rc, (cls(h) if rc == E_SUCCESS else None)
         check(rc)
+        return cls(h)
+
+    @classmethod
+    def load_hdf5(cls, path, order=ORDER_MORTON, precisions=(1 << PREC_F64) | (1 << PREC_F32C), device=-1):
+        """A mesh from one of the reference's HDF5 mesh files (MeshHDF5Source)."""
+        h = C.c_void_p()
+        o = cls._opts(order, precisions, device)
+        check(lib().cupcfd_gpu_mesh_load_hdf5(os.fsencode(path), C.byref(o), C.byref(h)))
         return cls(h)
 
     def save(self, path):
@@ -630,3 +641,24 @@ def dev_uvw_region_loop1(mesh, stream=None):
 
 def dev_uvw_bnds_loop1(mesh, stream=None):
     check(lib().cupcfd_gpu_dev_uvw_bnds_loop1(mesh.h, _stream(stream)))
+
+
+# ---------------------------------------------------------------------------
+# the reference's HDF5 mesh files (MeshHDF5Source)
+# ---------------------------------------------------------------------------
+def hdf5_mesh_read(path):
+    """Host arrays of an HDF5 mesh file in the reference's numbering, as a
+    dict in the oracle's mesh format (plus bndDistance), or raises
+    CupcfdError with the library's code."""
+    n = [C.c_int32() for _ in range(4)]
+    check(lib().cupcfd_gpu_hdf5_mesh_counts(os.fsencode(path), *[C.byref(x) for x in n]))
+    nC, nF, nB, nR = (x.value for x in n)
+    m = dict(nCells=nC, nFaces=nF, nBnd=nB, nRegions=max(nR, 1),
+             faceCell1=np.empty(nF, np.int32), faceCell2=np.empty(nF, np.int32), faceBnd=np.empty(nF, np.int32),
+             faceLambda=np.empty(nF), faceArea=np.empty(nF), faceNorm=np.empty((nF, 3)), faceCenter=np.empty((nF, 3)),
+             cellCenter=np.empty((nC, 3)), cellVolume=np.empty(nC), bndRegion=np.empty(nB, np.int32),
+             bndDistance=np.empty(nB))
+    check(lib().cupcfd_gpu_hdf5_mesh_read(os.fsencode(path), nC, nF, nB, *[_p(m[k]) for k in (
+        "faceCell1", "faceCell2", "faceBnd", "faceLambda", "faceArea", "faceNorm", "faceCenter", "cellCenter",
+        "cellVolume", "bndRegion", "bndDistance")]))
+    return m

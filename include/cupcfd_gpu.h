@@ -187,6 +187,32 @@ int cupcfd_gpu_mesh_create_jittered(int32_t nx, int32_t ny, int32_t nz, double j
 int cupcfd_gpu_mesh_save(const cupcfd_gpu_mesh *mesh, const char *path);
 int cupcfd_gpu_mesh_load(const char *path, const cupcfd_mesh_options *opt, cupcfd_gpu_mesh **out);
 
+/* Mesh ingest from the reference's HDF5 mesh files, as MeshHDF5Source reads
+ * them (src/geometry/mesh/implementation/source/MeshHDF5Source.cpp:42-1130)
+ * and addData lays them out on one rank (UnstructuredMeshInterface.ipp:
+ * 1464-1862): root attributes ncel, nfac, nbnd, nreg; /face/{cell1, cell2,
+ * bnd, lambda, area, n, x}, /cell/{x, vol}, /bnd/{rid, distance}; 1-based
+ * labels; cell2 = 0 marks a boundary face. The library reads the HDF5 format
+ * itself (superblock 0/1, symbol-table groups, version-1 object headers,
+ * compact or contiguous little-endian datasets; an unallocated dataset reads
+ * as its fill value); other files return CUPCFD_E_INVALID_FILE_FORMAT, a
+ * missing one CUPCFD_E_FILE_MISSING, labels out of range CUPCFD_E_INVALID_INDEX.
+ *   counts: the four root attributes;
+ *   read:   the arrays in the reference's (0-based) numbering into host
+ *           buffers (any may be NULL): faceCell1/2, faceBnd [nFaces] (-1 on
+ *           interior faces / cell2 of boundary faces), faceLambda, faceArea
+ *           [nFaces], faceNorm, faceCenter [3*nFaces], cellCenter [3*nCells],
+ *           cellVolume [nCells], bndRegion, bndDistance [nBoundaries];
+ *   load:   the device mesh, with default regions, the boundaries' regions
+ *           and distances. */
+int cupcfd_gpu_hdf5_mesh_counts(const char *path, int32_t *nCells, int32_t *nFaces, int32_t *nBoundaries,
+                                int32_t *nRegions);
+int cupcfd_gpu_hdf5_mesh_read(const char *path, int32_t nCells, int32_t nFaces, int32_t nBoundaries, int32_t *faceCell1,
+                              int32_t *faceCell2, int32_t *faceBnd, double *faceLambda, double *faceArea,
+                              double *faceNorm, double *faceCenter, double *cellCenter, double *cellVolume,
+                              int32_t *bndRegion, double *bndDistance);
+int cupcfd_gpu_mesh_load_hdf5(const char *path, const cupcfd_mesh_options *opt, cupcfd_gpu_mesh **out);
+
 int cupcfd_gpu_mesh_destroy(cupcfd_gpu_mesh *mesh);
 int cupcfd_gpu_mesh_get_info(const cupcfd_gpu_mesh *mesh, cupcfd_mesh_info *info);
 
