@@ -288,7 +288,7 @@ def bench_uvw(cg, mesh, dev, st, g, steps, warmup, peak):
     ms = e0.elapsed_time(e1) / steps
     alg = 224 * nC + 64 * nFi + 4 * nB
     gbs = alg / (ms * 1e-3) / 1e9
-    return {"call": "cupcfd_gpu_dev_uvw_face_loop1 (FP64, bit-identical to the reference)", "kernel": "k_uvw_f64",
+    return {"call": "cupcfd_gpu_dev_uvw_face_loop1 (FP64, bit-identical to the reference)", "kernel": "k_uvw_f64_pf",
             "ms_per_call": ms, "value": nF / (ms * 1e-3) / 1e9, "unit": "Gfaces/s", "steps": steps,
             "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
                          "algorithmic_bytes_per_launch": alg},
@@ -525,7 +525,7 @@ def run_gpu(a):
     if not a.no_uvw:
         uvw = bench_uvw(cg, mesh, dev, st, g, max(3, K // 4), 3, peak)
         uvw["roofline"]["peak_source"] = peak_src
-        uvw["roofline"]["traffic"] = profile_traffic().get(f"k_uvw_f64@{n}")
+        uvw["roofline"]["traffic"] = profile_traffic().get(f"k_uvw_f64_pf@{n}")
         if rank == 0 and world == 1 and not a.no_cpu:
             try:
                 uvw["cpu_reference"] = cpu_uvw(a.cpu_n, 5)

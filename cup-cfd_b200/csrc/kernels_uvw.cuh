@@ -28,6 +28,7 @@
 
 #include "arith.cuh"
 #include "internal.cuh"
+#include "prefetch.cuh"
 #include "sell.cuh"
 
 namespace cupcfd_gpu {
@@ -282,9 +283,7 @@ __device__ __forceinline__ void uvw_fold(int kind, const double (&t)[10], double
 #ifndef UVW_CHUNK
 #define UVW_CHUNK 6      // incidence entries loaded ahead (a hexahedral cell in one chunk)
 #endif
-__global__ void __launch_bounds__(256, UVW_CELL_MINB) k_uvw_f64(const __grid_constant__ UvwArgs a) {
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= a.nC) return;
+__device__ __forceinline__ void uvw_cell(const UvwArgs &a, int c) {
     int wdt;
     const int2 *e = cell_entries(a.sv, c, wdt);
     double s[3] = {a.su[c], a.sv_[c], a.sw[c]}, ad[3] = {a.au[c], a.av[c], a.aw[c]};
@@ -301,6 +300,38 @@ __global__ void __launch_bounds__(256, UVW_CELL_MINB) k_uvw_f64(const __grid_con
     }
     a.su[c] = s[0]; a.sv_[c] = s[1]; a.sw[c] = s[2];
     a.au[c] = ad[0]; a.av[c] = ad[1]; a.aw[c] = ad[2];
+}
+
+__global__ void __launch_bounds__(256, UVW_CELL_MINB) k_uvw_f64(const __grid_constant__ UvwArgs a) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < a.nC) uvw_cell(a, c);
+}
+
+// The same with the L2 prefetch of the tile one wave of this kernel's
+// resident blocks ahead (prefetch.cuh): its entries, face records and mass
+// fluxes, and its cells' entries in the twenty cell arrays the loop reads.
+// Needs the owner-sorted face order, 256-thread blocks and 16-byte aligned
+// arrays. 2.13 ms at 256^3 against 2.21 ms without the prefetch.
+__global__ void __launch_bounds__(STAGED_TILE, UVW_CELL_MINB) k_uvw_f64_pf(const __grid_constant__ UvwArgs a,
+                                                                          PrefetchArgs pf) {
+    constexpr int T = STAGED_TILE;
+    const int c = blockIdx.x * T + threadIdx.x;
+    const int tp = blockIdx.x + pf.dist;
+    const bool lead = threadIdx.x == T - 32 && tp < pf.nTiles;
+    __shared__ int4 s_rng;
+    if (lead) fetch_ranges_async(&s_rng, pf.desc + tp);
+    if (c < a.nC) uvw_cell(a, c);
+    if (lead) {
+        const int64_t L = a.ldg;
+        const void *const cellSrc[20] = {a.u, a.v, a.w, a.visC, a.su, a.sv_, a.sw, a.au, a.av, a.aw,
+                                         a.grads, a.grads + L, a.grads + 2 * L, a.grads + 3 * L, a.grads + 4 * L,
+                                         a.grads + 5 * L, a.grads + 6 * L, a.grads + 7 * L, a.grads + 8 * L, a.cc};
+        int cellBytes[20];
+#pragma unroll
+        for (int i = 0; i < 19; i++) cellBytes[i] = T * 8;
+        cellBytes[19] = T * 32;
+        prefetch_tile<20>(pf, tp, ranges_ready(&s_rng), a.fg, 32, (const double *) a.massFlux, cellSrc, cellBytes);
+    }
 }
 
 // ---------------------------------------------------------------------------

@@ -1,0 +1,78 @@
+// Tiles of 256 consecutive internal cells and the L2 prefetch of a tile's
+// contiguous ranges (inline device code and plain structs only, so several
+// translation units can include it).
+//
+// Because faces are numbered by owner slice, everything a tile reads in
+// order is one contiguous range of device memory: its incidence entries,
+// the records of the faces its cells own, and its cells' entries in every
+// cell array. TileDesc holds those ranges, built once per mesh. In the
+// prefetch kernels one lane per 256-cell block asks L2 to fetch the ranges
+// of the tile `dist` blocks ahead (cp.async.bulk.prefetch.L2), so the
+// streamed loads of later blocks become L2 hits; shared memory and L1 are
+// untouched and the per-cell arithmetic is that of the plain kernels.
+#pragma once
+
+#include "internal.cuh"
+
+namespace cupcfd_gpu {
+
+constexpr int STAGED_TILE = 256;
+
+// Per-tile ranges, built once per mesh.
+struct TileDesc {
+    int entStart, entEnd;  // incidence entries of the tile's eight slices
+    int fs, fe;            // faces owned by the tile's cells
+    unsigned w03, w47;     // slice widths (entries per lane), one byte per slice
+    int pad0, pad1;
+};
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned) __cvta_generic_to_shared(p); }
+
+struct PrefetchArgs {
+    const TileDesc *desc;
+    const int2 *inc;
+    int nC, nF, nTiles, dist;
+};
+
+__device__ __forceinline__ void bulk_prefetch_l2(const void *p, unsigned bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// The first half of a tile descriptor: {entStart, entEnd, fs, fe}.
+__device__ __forceinline__ int4 load_ranges(const TileDesc *d) { return __ldg(reinterpret_cast<const int4 *>(d)); }
+
+// The same 16 bytes fetched asynchronously into shared memory (cp.async),
+// so no register is held while the thread works; ranges_ready() waits for it.
+__device__ __forceinline__ void fetch_ranges_async(int4 *dst, const TileDesc *d) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n\tcp.async.commit_group;" ::"r"(smem_u32(dst)), "l"(d)
+                 : "memory");
+}
+__device__ __forceinline__ int4 ranges_ready(const int4 *src) {
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    return *src;
+}
+
+// Prefetches a tile's ranges: its entries, its owned faces' records (fgSize
+// bytes each) and gface values (widened to whole 16-byte units inside the
+// array), and, when the tile is whole, the cell arrays (cellBytes per tile).
+template <int NCELL, class TG>
+__device__ __forceinline__ void prefetch_tile(const PrefetchArgs &p, int t, const int4 &d, const void *fg,
+                                              int fgSize, const TG *gface, const void *const (&cellSrc)[NCELL],
+                                              const int (&cellBytes)[NCELL]) {
+    constexpr int PER16 = 16 / (int) sizeof(TG);
+    const int entStart = d.x, entEnd = d.y, fs = d.z, fe = d.w;
+    if (entEnd > entStart) bulk_prefetch_l2(p.inc + entStart, (unsigned) (entEnd - entStart) * 8u);
+    if (fe > fs)
+        bulk_prefetch_l2(static_cast<const unsigned char *>(fg) + (size_t) fs * fgSize, (unsigned) (fe - fs) * (unsigned) fgSize);
+    if (gface) {
+        int gfA = fs & ~(PER16 - 1), gfB = (fe + PER16 - 1) & ~(PER16 - 1);
+        if (gfB > p.nF) gfB = fe & ~(PER16 - 1);
+        if (gfB > gfA) bulk_prefetch_l2(gface + gfA, (unsigned) (gfB - gfA) * (unsigned) sizeof(TG));
+    }
+    if ((long long) (t + 1) * STAGED_TILE <= (long long) p.nC)
+        for (int i = 0; i < NCELL; i++)
+            bulk_prefetch_l2(static_cast<const unsigned char *>(cellSrc[i]) + (size_t) t * cellBytes[i],
+                             (unsigned) cellBytes[i]);
+}
+
+}  // namespace cupcfd_gpu
