@@ -16,6 +16,9 @@ namespace {
 
 constexpr int BLK = 256;
 
+// the L2-prefetch kernels, indexing cupcfd_gpu_mesh::prefetchWave
+enum PfKernel { PF_FWD_F32 = 0, PF_ADJ_F32, PF_FWD_F64, PF_ADJ_F64, PF_FWD_MADJ, PF_GADJ };
+
 // scratch slots of a mesh (each grows on demand and is reused across calls)
 enum Slot {
     S_ERR = 0, S_GEOM = 1, S_IN0, S_IN1, S_IN2, S_IN3, S_IN4, S_IN5, S_IN6, S_IN7,
@@ -189,11 +192,23 @@ int staged_setup(cupcfd_gpu_mesh *m, cudaStream_t st) {
     }
     if (!smemOk) m->stagedGrid[0] = m->stagedGrid[1] = m->stagedSmem[0] = m->stagedSmem[1] = 0;
     // L2-prefetch variant: prefetch one wave of resident blocks ahead (the
-    // block that will take this block's place), the best distance measured
-    int nbPf = 0;
-    CG_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nbPf, k_fwd_f32_pf, STAGED_TILE, 0));
-    m->prefetchDist = sms * std::max(1, nbPf);
-    if (const char *e = std::getenv("CUPCFD_PREFETCH_DIST")) if (*e) m->prefetchDist = std::max(1, std::atoi(e));
+    // block that will take this block's place), the best distance measured;
+    // each kernel's own wave (the gradient adjoint holds more blocks per SM
+    // than the forward: 0.345 ms at its 740-tile wave against 0.359 ms at
+    // the forward's 592 at 256^3)
+    const void *pfKern[6] = {(const void *) k_fwd_f32_pf, (const void *) k_adj_f32_pf, (const void *) k_fwd_f64_pf,
+                             (const void *) k_adj_f64_pf, (const void *) k_fwd_madj_f32_pf, (const void *) k_gadj_f32_pf};
+    for (int i = 0; i < 6; i++) {
+        int nb = 0;
+        CG_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pfKern[i], STAGED_TILE, 0));
+        m->prefetchWave[i] = sms * std::max(1, nb);
+    }
+    m->prefetchDist = m->prefetchWave[PF_FWD_F32];
+    if (const char *e = std::getenv("CUPCFD_PREFETCH_DIST"))
+        if (*e) {
+            m->prefetchDist = std::max(1, std::atoi(e));
+            for (int &w : m->prefetchWave) w = m->prefetchDist;
+        }
     // 1: L2 prefetch (the default, fastest measured); 2: shared-memory stages
     // (FP32 forward/adjoint, when they fit); CUPCFD_TILE_MODE overrides
     m->tileMode = 1;
@@ -203,14 +218,14 @@ int staged_setup(cupcfd_gpu_mesh *m, cudaStream_t st) {
     return CUPCFD_E_SUCCESS;
 }
 
-PrefetchArgs prefetch_args(const cupcfd_gpu_mesh *m) {
+PrefetchArgs prefetch_args(const cupcfd_gpu_mesh *m, int kernel = -1) {
     PrefetchArgs p;
     p.desc = (const TileDesc *) m->tileDesc;
     p.inc = m->sell.inc;
     p.nC = m->nC;
     p.nF = m->nF;
     p.nTiles = m->nTiles;
-    p.dist = m->prefetchDist;
+    p.dist = kernel >= 0 && m->prefetchWave[kernel] > 0 ? m->prefetchWave[kernel] : m->prefetchDist;
     return p;
 }
 
@@ -528,7 +543,7 @@ const char *launch_fwd_f32(const cupcfd_gpu_mesh *m, const void *phi, const void
         k_fwd_f32_pf<<<grid_for(m->nC, BLK), BLK, 0, st>>>(m->nC, sell(m), m->fg32, (const float *) phi,
                                                           (const float *) phiB, m->vol, (const float4 *) state,
                                                           (const float *) gface, (float *) grad, (float *) massFlux,
-                                                          part, m->nC, prefetch_args(m));
+                                                          part, m->nC, prefetch_args(m, PF_FWD_F32));
         return "k_fwd_f32_pf";
     }
     if (tiles && m->stagedGrid[0] > 0) {
@@ -554,7 +569,7 @@ const char *launch_fwd_f64(const cupcfd_gpu_mesh *m, const void *phi, const void
         k_fwd_f64_pf<<<grid_for(m->nC, BLK), BLK, 0, st>>>(m->nC, sell(m), m->fg64, (const double *) phi,
                                                           (const double *) phiB, m->vol, (const double *) state,
                                                           (const double *) gface, (double *) grad, (double *) massFlux,
-                                                          part, m->nC, prefetch_args(m));
+                                                          part, m->nC, prefetch_args(m, PF_FWD_F64));
         return "k_fwd_f64_pf";
     }
     k_fwd_f64<BLK><<<grid_for(m->nC, BLK), BLK, 0, st>>>(m->nC, sell(m), m->fg64, (const double *) phi,
@@ -608,7 +623,7 @@ extern "C" int cupcfd_gpu_dev_adjoint(cupcfd_gpu_mesh *m, int32_t precision, con
         kt.set_name("k_adj_f64_pf");
         k_adj_f64_pf<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg64, (const double *) grad, 2.0, (const double *) state,
                                            (const double *) gface, (double *) phiBar, (double *) phiBBar,
-                                           (double *) stateBar, m->nC, prefetch_args(m));
+                                           (double *) stateBar, m->nC, prefetch_args(m, PF_ADJ_F64));
     } else if (precision == CUPCFD_PREC_F64) {
         kt.set_name("k_adj_f64");
         k_adj_f64<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg64, (const double *) grad, 2.0, (const double *) state,
@@ -617,7 +632,7 @@ extern "C" int cupcfd_gpu_dev_adjoint(cupcfd_gpu_mesh *m, int32_t precision, con
         kt.set_name("k_adj_f32_pf");
         k_adj_f32_pf<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg32, (const float *) grad, 2.f, (const float4 *) state,
                                            (const float *) gface, (float *) phiBar, (float *) phiBBar,
-                                           (float4 *) stateBar, m->nC, prefetch_args(m));
+                                           (float4 *) stateBar, m->nC, prefetch_args(m, PF_ADJ_F32));
     } else if (m->staged && m->stagedGrid[1] > 0 && aligned16(grad) && aligned16(state) && aligned16(gface) &&
                m->nC % 4 == 0) {
         kt.set_name("k_adj_f32_staged");
@@ -661,7 +676,7 @@ extern "C" int cupcfd_gpu_dev_forward_adjoint(cupcfd_gpu_mesh *m, int32_t precis
         unsigned grid = grid_for(m->nC, BLK);
         double *part;
         CG_TRY(scratch(m, S_LOSS, grid, &part));
-        PrefetchArgs pf = prefetch_args(m);
+        PrefetchArgs pf = prefetch_args(m, PF_FWD_MADJ), pfg = prefetch_args(m, PF_GADJ);
         {
             KTIMER("k_fwd_madj_f32_pf", st);
             k_fwd_madj_f32_pf<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg32, (const float *) phi, (const float *) phiB,
@@ -677,7 +692,7 @@ extern "C" int cupcfd_gpu_dev_forward_adjoint(cupcfd_gpu_mesh *m, int32_t precis
         {
             KTIMER("k_gadj_f32_pf", st);
             k_gadj_f32_pf<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg32, (const float *) grad, 2.f, (float *) phiBar,
-                                                (float *) phiBBar, m->nC, pf);
+                                                (float *) phiBBar, m->nC, pfg);
             CG_LAUNCHED();
         }
         return CUPCFD_E_SUCCESS;

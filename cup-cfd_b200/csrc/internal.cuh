@@ -150,6 +150,7 @@ struct cupcfd_gpu_mesh {
     int stagedSmem[2] = {0, 0};
     int tileMode = 0;             // 0 unstaged, 1 L2 prefetch, 2 shared-memory stages
     int prefetchDist = 0;         // tiles ahead for the L2 prefetch variant
+    int prefetchWave[6] = {0, 0, 0, 0, 0, 0};  // per prefetch kernel (PfKernel in api.cu): one wave of its blocks
 
     std::vector<cupcfd_gpu::DevBuf> owned;  // everything above, freed by destroy
     std::vector<cupcfd_gpu::DevBuf> scratch; // reusable buffers for host-buffer calls
