@@ -49,6 +49,33 @@ struct Acc2 {
     __device__ __forceinline__ double value() const { return (double) s + (double) e; }
 };
 
+// Two Acc2 sums advanced together by the sm_100 packed FP32x2 operations
+// (__fmul2_rn, __ffma2_rn, __fadd2_rn): half the issued instructions. Each
+// lane performs exactly Acc2::add_prod's IEEE operations, x - y being
+// written fma(y, -1, x), which rounds the same exact value x + (-y), so the
+// lanes are bit-identical to two Acc2. add_x advances lane x alone.
+struct Acc2x2 {
+    float2 s = {0.f, 0.f}, e = {0.f, 0.f};
+    __device__ __forceinline__ void add_prod(float2 a, float2 b) {
+        const float2 m1 = make_float2(-1.f, -1.f);
+        float2 p = __fmul2_rn(a, b);
+        float2 ep = __ffma2_rn(a, b, __fmul2_rn(p, m1));
+        float2 t = __fadd2_rn(s, p);
+        float2 bp = __ffma2_rn(s, m1, t);
+        float2 es = __fadd2_rn(__ffma2_rn(__ffma2_rn(bp, m1, t), m1, s), __ffma2_rn(bp, m1, p));
+        s = t;
+        e = __fadd2_rn(e, __fadd2_rn(ep, es));
+    }
+    __device__ __forceinline__ void add_x(float a, float b) {
+        Acc2 h;
+        h.s = s.x; h.e = e.x;
+        h.add_prod(a, b);
+        s.x = h.s; e.x = h.e;
+    }
+    __device__ __forceinline__ double x() const { return (double) s.x + (double) e.x; }
+    __device__ __forceinline__ double y() const { return (double) s.y + (double) e.y; }
+};
+
 // 32-byte read-only load as two 128-bit loads (no __ldg overload for double4)
 __device__ __forceinline__ double4 ldg4(const double4 *p) {
     double2 a = __ldg(reinterpret_cast<const double2 *>(p));

@@ -171,7 +171,9 @@ __device__ __forceinline__ double fwd_madj_cell_f32(int c, const SellView &sv, c
     const int2 *e = cell_entries(sv, c, w);
     float phic = phi[c];
     float4 sc = st[c];
-    Acc2 ax, ay, az, rb, ub, vb, wb;
+    // seven Dot2 sums in packed pairs: (gx, gy), (gz, rhobar), (ubar, vbar), wbar
+    Acc2x2 axy, azr, uvb;
+    Acc2 wb;
     double lsum = 0.0;
     for (int k0 = 0; k0 < w; k0 += CH) {
         int2 en[CH];
@@ -199,6 +201,8 @@ __device__ __forceinline__ double fwd_madj_cell_f32(int c, const SellView &sv, c
             float phif;
             if (o < 0) {
                 phif = pv[j];
+                axy.add_prod(make_float2(phif, phif), make_float2(G[j].x, G[j].y));
+                azr.add_x(phif, G[j].z);
             } else {
                 float facn = G[j].w, facp = 1.f - facn;
                 phif = isN ? fmaf(facn, phic, facp * pv[j]) : fmaf(facn, pv[j], facp * phic);
@@ -216,18 +220,20 @@ __device__ __forceinline__ double fwd_madj_cell_f32(int c, const SellView &sv, c
                 float denA = fmaf(wc, sc.x, wo * so[j].x);
                 float uA = fmaf(wc, sc.y, wo * so[j].y), vA = fmaf(wc, sc.z, wo * so[j].z), wA = fmaf(wc, sc.w, wo * so[j].w);
                 float a = wc * gf[j];
-                rb.add_prod(a, fmaf(uA, G[j].x, fmaf(vA, G[j].y, wA * G[j].z)));
+                float q = fmaf(uA, G[j].x, fmaf(vA, G[j].y, wA * G[j].z));
                 float b = a * denA;
-                ub.add_prod(b, G[j].x); vb.add_prod(b, G[j].y); wb.add_prod(b, G[j].z);
+                axy.add_prod(make_float2(phif, phif), make_float2(G[j].x, G[j].y));
+                azr.add_prod(make_float2(phif, a), make_float2(G[j].z, q));
+                uvb.add_prod(make_float2(b, b), make_float2(G[j].x, G[j].y));
+                wb.add_prod(b, G[j].z);
             }
-            ax.add_prod(phif, G[j].x); ay.add_prod(phif, G[j].y); az.add_prod(phif, G[j].z);
         }
     }
     double V = vol[c];
     double fact = 1.0 / V;
-    float rx = (float) (ax.value() * fact), ry = (float) (ay.value() * fact), rz = (float) (az.value() * fact);
+    float rx = (float) (axy.x() * fact), ry = (float) (axy.y() * fact), rz = (float) (azr.x() * fact);
     g[c] = rx; g[ldc + c] = ry; g[2 * ldc + c] = rz;
-    stbar[c] = make_float4((float) rb.value(), (float) ub.value(), (float) vb.value(), (float) wb.value());
+    stbar[c] = make_float4((float) azr.y(), (float) uvb.x(), (float) uvb.y(), (float) wb.value());
     return __fma_rn(V, __fma_rn((double) rx, (double) rx, __fma_rn((double) ry, (double) ry, __dmul_rn((double) rz, (double) rz))),
                     lsum);
 }
