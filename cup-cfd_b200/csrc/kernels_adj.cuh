@@ -267,11 +267,24 @@ __global__ void __launch_bounds__(BLOCK, CUPCFD_MINB_F32) k_fwd_f32(int nC, Sell
     if (lossPart) block_sum_store<BLOCK>(l, lossPart);
 }
 
-// Deterministic final reduction of per-block partials (fixed order).
+// Deterministic final reduction of per-block partials (fixed order): thread
+// t adds part[t], part[t + blockDim], ... in that order, then a tree over
+// the block. The loads of each group of 16 are issued before its adds, so
+// they overlap instead of each add waiting on its own load.
 __global__ void k_reduce_partials(int n, const double *__restrict__ part, double *__restrict__ out) {
     __shared__ double red[1024];
+    constexpr int U = 16;
+    const int bd = blockDim.x;
     double t = 0.0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) t += part[i];
+    int i = threadIdx.x;
+    for (; i + (U - 1) * bd < n; i += U * bd) {
+        double v[U];
+#pragma unroll
+        for (int j = 0; j < U; j++) v[j] = __ldg(part + i + j * bd);
+#pragma unroll
+        for (int j = 0; j < U; j++) t += v[j];
+    }
+    for (; i < n; i += bd) t += part[i];
     red[threadIdx.x] = t;
     __syncthreads();
     for (int k = blockDim.x / 2; k > 0; k >>= 1) {
