@@ -9,7 +9,8 @@ chain in the mesh's internal numbering, with every scalar left on the
 device, and must give the same bits. Meshes: structured and jittered with
 permuted numbering, six boundary regions (inlet, two outlets, symmetry,
 wall, default) assigned at random, so that cells with several outlet faces
-exercise the ordered su update.
+exercise the ordered su update; the large jittered mesh (112 x 104 x 96,
+64,768 boundaries) takes the id-ordered sums through many staged passes.
 """
 import numpy as np
 import pytest
@@ -21,7 +22,9 @@ pytestmark = pytest.mark.gpu
 
 
 def _setup(cg, kind, order):
-    base = O.structgen(20, 18, 16) if kind == "struct" else O.jitter(17, 15, 13, 0.25, seed=8, permute=True)
+    base = {"struct": lambda: O.structgen(20, 18, 16),
+            "jitter": lambda: O.jitter(17, 15, 13, 0.25, seed=8, permute=True),
+            "large": lambda: O.jitter(112, 104, 96, 0.25, seed=8, permute=True)}[kind]()
     m, splvl, rng = _with_regions(base, 41 if kind == "struct" else 42)
     mesh = cg.Mesh.from_arrays(m, order=order)
     assert mesh.set_regions(m["regionType"], m["regionUVW"], m["regionDen"], m["bndRegion"]) == cg.E_SUCCESS
@@ -69,7 +72,7 @@ def _host_chain(cg, mesh, d, solve):
     return r
 
 
-@pytest.mark.parametrize("kind,order", [("struct", 2), ("jitter", 3), ("jitter", 0)])
+@pytest.mark.parametrize("kind,order", [("struct", 2), ("jitter", 3), ("jitter", 0), ("large", 3)])
 @pytest.mark.parametrize("solve", [(1, 1, 1), (0, 1, 0)])
 def test_boundary_loops_bit_exact(cg, gpu, kind, order, solve):
     m, splvl, mesh, d = _setup(cg, kind, order)

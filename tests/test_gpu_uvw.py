@@ -174,3 +174,23 @@ def test_uvw_errors(cg, gpu):
     assert mesh.set_boundary_distance(np.zeros(m["nBnd"] + 1)) == cg.E_ARRAY_SIZE_MISMATCH
     with pytest.raises(cg.CupcfdError):
         mesh.region_force_tangent(m["nRegions"] + 1)
+
+
+def test_uvw_large_jittered_permuted(cg, gpu):
+    """A 128^3 jittered mesh with permuted numbering (2,097,152 cells,
+    6,340,608 faces), six random regions, set rlencos and boundary distances,
+    in reverse Cuthill-McKee order: every output bit for bit against the
+    oracle, and the region / boundary loops after it."""
+    from test_oracle_vs_reference import _with_regions
+    base = O.jitter(128, 128, 128, 0.25, seed=9, permute=True)
+    m, _, rng = _with_regions(base, 90)
+    f = O.uvw_fields(m, 91)
+    rl, bd = rng.uniform(0.1, 2.0, m["nFaces"]), rng.uniform(0.01, 0.2, m["nBnd"])
+    want = O.uvw_face_loop1(m, f, rl, bd)
+    mesh = _mesh(cg, m, cg.ORDER_RCM, rl, bd)
+    _check(_host(cg, mesh, f), want)
+    assert cg.FluxUVWDolfynRegionLoop1(mesh) == cg.E_SUCCESS
+    ft0 = mesh.region_force_tangent(m["nRegions"])
+    assert same(ft0, O.uvw_region_loop1(m))
+    assert cg.FluxUVWDolfynBndsLoop1(mesh) == cg.E_SUCCESS
+    assert same(mesh.region_force_tangent(m["nRegions"]), O.uvw_bnds_loop1(m, want["shear"], ft0))
