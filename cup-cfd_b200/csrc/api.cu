@@ -983,6 +983,51 @@ extern "C" int cupcfd_gpu_flux_mass_dolfyn_face_loop(
     return CUPCFD_E_SUCCESS;
 }
 
+namespace {
+// The copy-back stream and events of a mesh's host forward+adjoint.
+int pipe_init(cupcfd_gpu_mesh *m) {
+    if (m->outStream) return CUPCFD_E_SUCCESS;
+    for (cudaEvent_t &e : m->pipeEv)
+        if (!e) CG_CHECK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    CG_CHECK_CUDA(cudaStreamCreateWithFlags(&m->outStream, cudaStreamNonBlocking));
+    return CUPCFD_E_SUCCESS;
+}
+
+// One part of the benchmark adjoint with the plain adjoint kernels: the
+// gradient part (phibar, phibBar from g, hscale 2) when state and gface are
+// null, the mass part (stateBar) when g is null and hscale 0. Each output's
+// sum is the one the combined kernels form, so the results are theirs.
+int launch_adj_part(const cupcfd_gpu_mesh *m, bool f64, const void *g, double hscale, const void *state,
+                    const void *gface, void *phiBar, void *phiBBar, void *stateBar, cudaStream_t st) {
+    unsigned grid = grid_for(m->nC, BLK);
+    if (f64)
+        k_adj_f64<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg64, (const double *) g, hscale, (const double *) state,
+                                        (const double *) gface, (double *) phiBar, (double *) phiBBar,
+                                        (double *) stateBar, m->nC);
+    else
+        k_adj_f32<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg32, (const float *) g, (float) hscale,
+                                        (const float4 *) state, (const float *) gface, (float *) phiBar,
+                                        (float *) phiBBar, (float4 *) stateBar, m->nC);
+    CG_LAUNCHED();
+    return CUPCFD_E_SUCCESS;
+}
+}  // namespace
+
+// Host-buffer forward+adjoint. The host link carries about 1.1 GB in and
+// 1.5 GB out per call at 256^3, against about 1 ms of kernels, so the call is
+// ordered for the link rather than the kernels: each result goes back as soon
+// as it exists, while the next inputs still come in (the link carries both
+// directions at once).
+//   mesh stream:  phi in -> gradient -> gradient adjoint -> [e0] -> state in
+//                 -> mass flux -> [e1] -> gface in -> loss -> mass adjoint -> [e2]
+//   copy stream:  after e0 the gradient and phiBar out (while the state comes
+//                 in), after e1 the mass fluxes (while gface comes in), after
+//                 e2 the state adjoint and the loss
+// The kernels are the device calls' (gradient, mass flux, the two parts of
+// the adjoint, and the loss from the stored gradient and mass fluxes), whose
+// results equal cupcfd_gpu_dev_forward_adjoint's bit for bit. With the fused forward+adjoint
+// selected (cupcfd_gpu_mesh_set_fusion 1) the call runs that launch after all
+// inputs are in and copies everything back after it.
 extern "C" int cupcfd_gpu_forward_adjoint(cupcfd_gpu_mesh *m, int32_t precision, const double *phi, const double *phiB,
                                           const double *den, const double *u, const double *v, const double *w,
                                           const double *gface, double *grad, double *massFlux, double *phiBar,
@@ -999,19 +1044,15 @@ extern "C" int cupcfd_gpu_forward_adjoint(cupcfd_gpu_mesh *m, int32_t precision,
     unsigned gC = grid_for(nC, BLK), gF = grid_for(nF, BLK);
     bool f64 = precision == CUPCFD_PREC_F64;
     size_t es = f64 ? 8 : 4;
-    // host -> device (reference numbering, FP64)
+    bool pipe = !use_fused(m, precision);
+    if (pipe) CG_TRY(pipe_init(m));
+    cudaStream_t so = pipe ? m->outStream : st;
+    // host -> device staging (reference numbering, FP64)
     double *in;
     void *phiI, *phibI, *stI, *gI, *gradI, *mfI, *pbI, *pbbI, *sbI;
     CG_TRY(scratch(m, S_IN0, 5 * (size_t) nC + nB + nF, &in));
     double *hPhi = in, *hR = in + nC, *hU = in + 2 * (size_t) nC, *hV = in + 3 * (size_t) nC, *hW = in + 4 * (size_t) nC;
     double *hPb = in + 5 * (size_t) nC, *hG = hPb + nB;
-    CG_CHECK_CUDA(cudaMemcpyAsync(hPhi, phi, 8 * (size_t) nC, cudaMemcpyHostToDevice, st));
-    CG_CHECK_CUDA(cudaMemcpyAsync(hR, den, 8 * (size_t) nC, cudaMemcpyHostToDevice, st));
-    CG_CHECK_CUDA(cudaMemcpyAsync(hU, u, 8 * (size_t) nC, cudaMemcpyHostToDevice, st));
-    CG_CHECK_CUDA(cudaMemcpyAsync(hV, v, 8 * (size_t) nC, cudaMemcpyHostToDevice, st));
-    CG_CHECK_CUDA(cudaMemcpyAsync(hW, w, 8 * (size_t) nC, cudaMemcpyHostToDevice, st));
-    if (nB > 0) CG_CHECK_CUDA(cudaMemcpyAsync(hPb, phiB, 8 * (size_t) nB, cudaMemcpyHostToDevice, st));
-    CG_CHECK_CUDA(cudaMemcpyAsync(hG, gface, 8 * (size_t) nF, cudaMemcpyHostToDevice, st));
     // internal numbering, compute precision
     CG_TRY(m->scratchBuf(S_IN1, (size_t) nC * es, &phiI));
     CG_TRY(m->scratchBuf(S_IN2, (size_t) std::max(nB, 1) * es, &phibI));
@@ -1022,52 +1063,100 @@ extern "C" int cupcfd_gpu_forward_adjoint(cupcfd_gpu_mesh *m, int32_t precision,
     CG_TRY(m->scratchBuf(S_OUT2, (size_t) nC * es, &pbI));
     CG_TRY(m->scratchBuf(S_OUT3, (size_t) std::max(nB, 1) * es, &pbbI));
     CG_TRY(m->scratchBuf(S_OUT4, 4 * (size_t) nC * es, &sbI));
-    double *dloss;
+    double *dloss, *part, *out;
     CG_TRY(scratch(m, S_NORM, 1, &dloss));
-    if (f64) {
-        k_gather<double, double><<<gC, BLK, 0, st>>>(nC, 1, m->cellN2O, hPhi, 0, (double *) phiI, 0);
-        k_gather<double, double><<<gC, BLK, 0, st>>>(nC, 4, m->cellN2O, hR, nC, (double *) stI, ldc);
-        if (nB > 0) CG_CHECK_CUDA(cudaMemcpyAsync(phibI, hPb, 8 * (size_t) nB, cudaMemcpyDeviceToDevice, st));
-        k_gather<double, double><<<gF, BLK, 0, st>>>(nF, 1, m->faceN2O, hG, 0, (double *) gI, 0);
-    } else {
-        k_gather<double, float><<<gC, BLK, 0, st>>>(nC, 1, m->cellN2O, hPhi, 0, (float *) phiI, 0);
-        k_state_to_f4<<<gC, BLK, 0, st>>>(nC, m->cellN2O, hR, hU, hV, hW, (float4 *) stI);
-        if (nB > 0) k_convert<double, float><<<grid_for(nB, BLK), BLK, 0, st>>>(nB, hPb, (float *) phibI);
-        k_gather<double, float><<<gF, BLK, 0, st>>>(nF, 1, m->faceN2O, hG, 0, (float *) gI, 0);
-    }
-    g_launches.fetch_add(4);
-    CG_CHECK_CUDA(cudaGetLastError());
-    CG_TRY(cupcfd_gpu_dev_forward_adjoint(m, precision, phiI, phibI, stI, gI, gradI, mfI, pbI, pbbI, sbI, dloss, st));
-    // back to reference numbering (FP64) and to the host
-    double *out;
+    CG_TRY(scratch(m, S_LOSS, gC, &part));
     CG_TRY(scratch(m, S_IN5, 8 * (size_t) nC + nF + nB, &out));
     double *oG = out, *oMf = out + 3 * (size_t) nC, *oPb = oMf + nF, *oR = oPb + nC, *oU = oR + nC, *oV = oU + nC,
            *oW = oV + nC, *oPbb = oW + nC;
+
+    // phi in, gradient
+    CG_CHECK_CUDA(cudaMemcpyAsync(hPhi, phi, 8 * (size_t) nC, cudaMemcpyHostToDevice, st));
+    if (nB > 0) CG_CHECK_CUDA(cudaMemcpyAsync(hPb, phiB, 8 * (size_t) nB, cudaMemcpyHostToDevice, st));
     if (f64) {
-        k_blocks_to_aos<double, double><<<gC, BLK, 0, st>>>(nC, 3, m->cellO2N, (const double *) gradI, ldc, oG);
-        k_faces_to_ref<double><<<gF, BLK, 0, st>>>(nF, m->faceO2N, m->faceCells, (const double *) mfI, oMf, 1);
-        k_gather<double, double><<<gC, BLK, 0, st>>>(nC, 1, m->cellO2N, (const double *) pbI, 0, oPb, 0);
-        k_gather<double, double><<<gC, BLK, 0, st>>>(nC, 4, m->cellO2N, (const double *) sbI, ldc, oR, nC);
-        if (nB > 0) CG_CHECK_CUDA(cudaMemcpyAsync(oPbb, pbbI, 8 * (size_t) nB, cudaMemcpyDeviceToDevice, st));
+        k_gather<double, double><<<gC, BLK, 0, st>>>(nC, 1, m->cellN2O, hPhi, 0, (double *) phiI, 0);
+        if (nB > 0) CG_CHECK_CUDA(cudaMemcpyAsync(phibI, hPb, 8 * (size_t) nB, cudaMemcpyDeviceToDevice, st));
     } else {
-        k_blocks_to_aos<float, double><<<gC, BLK, 0, st>>>(nC, 3, m->cellO2N, (const float *) gradI, ldc, oG);
-        k_faces_to_ref<float><<<gF, BLK, 0, st>>>(nF, m->faceO2N, m->faceCells, (const float *) mfI, oMf, 1);
-        k_gather<float, double><<<gC, BLK, 0, st>>>(nC, 1, m->cellO2N, (const float *) pbI, 0, oPb, 0);
-        k_f4_to_ref<<<gC, BLK, 0, st>>>(nC, m->cellO2N, (const float4 *) sbI, oR, oU, oV, oW);
-        if (nB > 0) k_convert<float, double><<<grid_for(nB, BLK), BLK, 0, st>>>(nB, (const float *) pbbI, oPbb);
+        k_gather<double, float><<<gC, BLK, 0, st>>>(nC, 1, m->cellN2O, hPhi, 0, (float *) phiI, 0);
+        if (nB > 0) {
+            k_convert<double, float><<<grid_for(nB, BLK), BLK, 0, st>>>(nB, hPb, (float *) phibI);
+            g_launches.fetch_add(1, std::memory_order_relaxed);
+        }
     }
-    g_launches.fetch_add(5);
-    CG_CHECK_CUDA(cudaGetLastError());
-    if (grad) CG_CHECK_CUDA(cudaMemcpyAsync(grad, oG, 24 * (size_t) nC, cudaMemcpyDeviceToHost, st));
-    if (massFlux) CG_CHECK_CUDA(cudaMemcpyAsync(massFlux, oMf, 8 * (size_t) nF, cudaMemcpyDeviceToHost, st));
-    if (phiBar) CG_CHECK_CUDA(cudaMemcpyAsync(phiBar, oPb, 8 * (size_t) nC, cudaMemcpyDeviceToHost, st));
-    if (denBar) CG_CHECK_CUDA(cudaMemcpyAsync(denBar, oR, 8 * (size_t) nC, cudaMemcpyDeviceToHost, st));
-    if (uBar) CG_CHECK_CUDA(cudaMemcpyAsync(uBar, oU, 8 * (size_t) nC, cudaMemcpyDeviceToHost, st));
-    if (vBar) CG_CHECK_CUDA(cudaMemcpyAsync(vBar, oV, 8 * (size_t) nC, cudaMemcpyDeviceToHost, st));
-    if (wBar) CG_CHECK_CUDA(cudaMemcpyAsync(wBar, oW, 8 * (size_t) nC, cudaMemcpyDeviceToHost, st));
-    if (phiBBar && nB > 0) CG_CHECK_CUDA(cudaMemcpyAsync(phiBBar, oPbb, 8 * (size_t) nB, cudaMemcpyDeviceToHost, st));
-    if (loss) CG_CHECK_CUDA(cudaMemcpyAsync(loss, dloss, 8, cudaMemcpyDeviceToHost, st));
-    CG_CHECK_CUDA(cudaStreamSynchronize(st));
+    CG_LAUNCHED();
+    if (pipe) {
+        CG_TRY(launch_grad_once(m, precision, false, false, phiI, phibI, nullptr, gradI, nullptr, st));
+        CG_TRY(launch_adj_part(m, f64, gradI, 2.0, nullptr, nullptr, pbI, pbbI, nullptr, st));
+        CG_CHECK_CUDA(cudaEventRecord(m->pipeEv[0], st));
+    }
+    // state in, mass flux
+    CG_CHECK_CUDA(cudaMemcpyAsync(hR, den, 8 * (size_t) nC, cudaMemcpyHostToDevice, st));
+    CG_CHECK_CUDA(cudaMemcpyAsync(hU, u, 8 * (size_t) nC, cudaMemcpyHostToDevice, st));
+    CG_CHECK_CUDA(cudaMemcpyAsync(hV, v, 8 * (size_t) nC, cudaMemcpyHostToDevice, st));
+    CG_CHECK_CUDA(cudaMemcpyAsync(hW, w, 8 * (size_t) nC, cudaMemcpyHostToDevice, st));
+    if (f64) k_gather<double, double><<<gC, BLK, 0, st>>>(nC, 4, m->cellN2O, hR, nC, (double *) stI, ldc);
+    else k_state_to_f4<<<gC, BLK, 0, st>>>(nC, m->cellN2O, hR, hU, hV, hW, (float4 *) stI);
+    CG_LAUNCHED();
+    if (pipe) {
+        CG_TRY(cupcfd_gpu_dev_mass_plain(m, precision, stI, mfI, st));
+        CG_CHECK_CUDA(cudaEventRecord(m->pipeEv[1], st));
+    }
+    // gface in, loss and adjoint
+    CG_CHECK_CUDA(cudaMemcpyAsync(hG, gface, 8 * (size_t) nF, cudaMemcpyHostToDevice, st));
+    if (f64) k_gather<double, double><<<gF, BLK, 0, st>>>(nF, 1, m->faceN2O, hG, 0, (double *) gI, 0);
+    else k_gather<double, float><<<gF, BLK, 0, st>>>(nF, 1, m->faceN2O, hG, 0, (float *) gI, 0);
+    CG_LAUNCHED();
+    if (pipe) {
+        if (f64)
+            k_loss<double><<<gC, 256, 0, st>>>(nC, sell(m), (const double *) gI, (const double *) mfI,
+                                               (const double *) gradI, m->vol, part, ldc);
+        else
+            k_loss<float><<<gC, 256, 0, st>>>(nC, sell(m), (const float *) gI, (const float *) mfI,
+                                              (const float *) gradI, m->vol, part, ldc);
+        CG_LAUNCHED();
+        k_reduce_partials<<<1, 1024, 0, st>>>((int) gC, part, dloss);
+        CG_LAUNCHED();
+        CG_TRY(launch_adj_part(m, f64, nullptr, 0.0, stI, gI, nullptr, nullptr, sbI, st));
+        CG_CHECK_CUDA(cudaEventRecord(m->pipeEv[2], st));
+    } else {
+        CG_TRY(cupcfd_gpu_dev_forward_adjoint(m, precision, phiI, phibI, stI, gI, gradI, mfI, pbI, pbbI, sbI, dloss, st));
+    }
+
+    // back to reference numbering (FP64) and to the host, on the copy stream
+    if (pipe) CG_CHECK_CUDA(cudaStreamWaitEvent(so, m->pipeEv[0], 0));
+    if (f64) {
+        k_blocks_to_aos<double, double><<<gC, BLK, 0, so>>>(nC, 3, m->cellO2N, (const double *) gradI, ldc, oG);
+        k_gather<double, double><<<gC, BLK, 0, so>>>(nC, 1, m->cellO2N, (const double *) pbI, 0, oPb, 0);
+        if (nB > 0) CG_CHECK_CUDA(cudaMemcpyAsync(oPbb, pbbI, 8 * (size_t) nB, cudaMemcpyDeviceToDevice, so));
+    } else {
+        k_blocks_to_aos<float, double><<<gC, BLK, 0, so>>>(nC, 3, m->cellO2N, (const float *) gradI, ldc, oG);
+        k_gather<float, double><<<gC, BLK, 0, so>>>(nC, 1, m->cellO2N, (const float *) pbI, 0, oPb, 0);
+        if (nB > 0) {
+            k_convert<float, double><<<grid_for(nB, BLK), BLK, 0, so>>>(nB, (const float *) pbbI, oPbb);
+            g_launches.fetch_add(1, std::memory_order_relaxed);
+        }
+    }
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    CG_LAUNCHED();
+    if (grad) CG_CHECK_CUDA(cudaMemcpyAsync(grad, oG, 24 * (size_t) nC, cudaMemcpyDeviceToHost, so));
+    if (phiBar) CG_CHECK_CUDA(cudaMemcpyAsync(phiBar, oPb, 8 * (size_t) nC, cudaMemcpyDeviceToHost, so));
+    if (phiBBar && nB > 0) CG_CHECK_CUDA(cudaMemcpyAsync(phiBBar, oPbb, 8 * (size_t) nB, cudaMemcpyDeviceToHost, so));
+    if (pipe) CG_CHECK_CUDA(cudaStreamWaitEvent(so, m->pipeEv[1], 0));
+    if (f64) k_faces_to_ref<double><<<gF, BLK, 0, so>>>(nF, m->faceO2N, m->faceCells, (const double *) mfI, oMf, 1);
+    else k_faces_to_ref<float><<<gF, BLK, 0, so>>>(nF, m->faceO2N, m->faceCells, (const float *) mfI, oMf, 1);
+    CG_LAUNCHED();
+    if (massFlux) CG_CHECK_CUDA(cudaMemcpyAsync(massFlux, oMf, 8 * (size_t) nF, cudaMemcpyDeviceToHost, so));
+    if (pipe) CG_CHECK_CUDA(cudaStreamWaitEvent(so, m->pipeEv[2], 0));
+    if (f64) k_gather<double, double><<<gC, BLK, 0, so>>>(nC, 4, m->cellO2N, (const double *) sbI, ldc, oR, nC);
+    else k_f4_to_ref<<<gC, BLK, 0, so>>>(nC, m->cellO2N, (const float4 *) sbI, oR, oU, oV, oW);
+    CG_LAUNCHED();
+    if (denBar) CG_CHECK_CUDA(cudaMemcpyAsync(denBar, oR, 8 * (size_t) nC, cudaMemcpyDeviceToHost, so));
+    if (uBar) CG_CHECK_CUDA(cudaMemcpyAsync(uBar, oU, 8 * (size_t) nC, cudaMemcpyDeviceToHost, so));
+    if (vBar) CG_CHECK_CUDA(cudaMemcpyAsync(vBar, oV, 8 * (size_t) nC, cudaMemcpyDeviceToHost, so));
+    if (wBar) CG_CHECK_CUDA(cudaMemcpyAsync(wBar, oW, 8 * (size_t) nC, cudaMemcpyDeviceToHost, so));
+    if (loss) CG_CHECK_CUDA(cudaMemcpyAsync(loss, dloss, 8, cudaMemcpyDeviceToHost, so));
+    CG_CHECK_CUDA(cudaStreamSynchronize(so));
+    if (pipe) CG_CHECK_CUDA(cudaStreamSynchronize(st));
     return cupcfd_gpu_mesh_check_status(m, st);
 }
 

@@ -267,6 +267,35 @@ __global__ void __launch_bounds__(BLOCK, CUPCFD_MINB_F32) k_fwd_f32(int nC, Sell
     if (lossPart) block_sum_store<BLOCK>(l, lossPart);
 }
 
+// The benchmark loss from a forward already in memory (gradient g, mass
+// fluxes m): per cell, gface_f m_f summed over the interior faces it owns in
+// entry order, then V_c |g_c|^2 added, and the per-block partials of
+// block_sum_store. The arithmetic and order are those of fwd_cell_f64 /
+// fwd_cell_f32 / fwd_madj_cell_f32 (T = float: the FP32 values widened), so
+// the partials, and the reduced loss, equal theirs bit for bit.
+template <class T>
+__global__ void __launch_bounds__(256) k_loss(int nC, SellView sv, const T *__restrict__ gface,
+                                              const T *__restrict__ mflux, const T *__restrict__ g,
+                                              const double *__restrict__ vol, double *__restrict__ lossPart,
+                                              int64_t ldc) {
+    int c = blockIdx.x * 256 + threadIdx.x;
+    double l = 0.0;
+    if (c < nC) {
+        int w;
+        const int2 *e = cell_entries(sv, c, w);
+        double lsum = 0.0;
+        for (int k = 0; k < w; k++) {
+            int2 en = ld_entry(e + 32 * k);
+            if (en.x < 0 || en.y < 0 || (en.x & 1)) continue;  // padding, boundary, or not the owner
+            int f = en.x >> 1;
+            lsum = __fma_rn((double) __ldg(gface + f), (double) __ldg(mflux + f), lsum);
+        }
+        double rx = g[c], ry = g[ldc + c], rz = g[2 * ldc + c];
+        l = __fma_rn(vol[c], __fma_rn(rx, rx, __fma_rn(ry, ry, __dmul_rn(rz, rz))), lsum);
+    }
+    block_sum_store<256>(l, lossPart);
+}
+
 // Deterministic final reduction of per-block partials (fixed order): thread
 // t adds part[t], part[t + blockDim], ... in that order, then a tree over
 // the block. The loads of each group of 16 are issued before its adds, so

@@ -426,3 +426,64 @@ def test_fused_host_call_matches_oracle(cg, gpu, order, fusion):
     for k, v in A.items():
         e = errs(out[k], v)
         assert e["norm"] <= 1e-13 and e["rms"] <= 1e-13, (k, e)
+
+
+@pytest.mark.parametrize("order", [1, 3])
+@pytest.mark.parametrize("prec", [0, 1])
+@pytest.mark.parametrize("mk", ["jitter", "poly"])
+def test_host_call_equals_device_call(cg, gpu, order, prec, mk):
+    """The host-buffer forward+adjoint (gradient, mass flux, loss and adjoint
+    as separate launches, results copied back on a second stream while later
+    inputs come in) returns what cupcfd_gpu_dev_forward_adjoint computes from
+    the same values, bit for bit, the loss included; boundary faces' mass
+    fluxes come back as zero."""
+    import torch
+    dev = torch.device("cuda:0")
+    if mk == "jitter":
+        ref = O.jitter(22, 20, 18, 0.25, seed=21, permute=True)
+    else:
+        ref = O.merge_cells(O.jitter(16, 15, 14, 0.25, seed=23, permute=True), 0.3, 24, max_cells=4)
+    mesh = cg.Mesh.from_arrays(ref, order=order)
+    f = O.fields(ref, 25)
+    gface = np.random.Generator(np.random.Philox(key=26)).standard_normal(ref["nFaces"])
+    host = cg.forward_adjoint(mesh, prec, f["phi"], f["phiB"], f["den"], f["u"], f["v"], f["w"], gface)
+    c2o, f2o = mesh.numbering()
+    nC, nF, nB = mesh.nCells, mesh.nFaces, mesh.nBoundaries
+    dt = torch.float64 if prec == cg.PREC_F64 else torch.float32
+
+    def T(a):
+        return torch.from_numpy(np.ascontiguousarray(a)).to(device=dev, dtype=dt)
+
+    st4 = np.stack([f[k][c2o] for k in ("den", "u", "v", "w")])
+    state = T(st4) if prec == cg.PREC_F64 else T(st4.T)
+    out = dict(grad=torch.full((3, nC), float("nan"), dtype=dt, device=dev),
+               mf=torch.zeros(nF, dtype=dt, device=dev), pb=torch.full((nC,), float("nan"), dtype=dt, device=dev),
+               pbb=torch.full((nB,), float("nan"), dtype=dt, device=dev), sb=torch.full_like(state, float("nan")),
+               loss=torch.zeros(1, dtype=torch.float64, device=dev))
+    s = torch.cuda.current_stream()
+    cg.dev_forward_adjoint(mesh, prec, T(f["phi"][c2o]), T(f["phiB"]), state, T(gface[f2o]), out["grad"], out["mf"],
+                           out["pb"], out["pbb"], out["sb"], out["loss"], stream=s)
+    assert mesh.check_status(s) == cg.E_SUCCESS
+    torch.cuda.synchronize()
+
+    def to_ref(t, n2o):
+        a = t.cpu().double().numpy()
+        r = np.empty_like(a)
+        r[..., n2o] = a
+        return r
+
+    def bits(a, b, what):
+        a, b = np.ascontiguousarray(a, np.float64), np.ascontiguousarray(b, np.float64)
+        assert a.shape == b.shape and np.array_equal(a.view(np.int64), b.view(np.int64)), what
+
+    bits(host["grad"], to_ref(out["grad"], c2o).T, "grad")
+    inner = ref["faceCell2"] >= 0
+    mf = to_ref(out["mf"], f2o)
+    bits(host["massFlux"][inner], mf[inner], "massFlux")
+    assert np.all(host["massFlux"][~inner] == 0.0)
+    bits(host["phiBar"], to_ref(out["pb"], c2o), "phiBar")
+    bits(host["phiBBar"], out["pbb"].cpu().double().numpy(), "phiBBar")
+    sb = to_ref(out["sb"] if prec == cg.PREC_F64 else out["sb"].t(), c2o)
+    for i, k in enumerate(("denBar", "uBar", "vBar", "wBar")):
+        bits(host[k], sb[i], k)
+    bits(host["loss"], out["loss"].cpu().numpy(), "loss")
