@@ -90,6 +90,10 @@ SIGNATURES = {
     "cupcfd_gpu_hdf5_mesh_counts": ([C.c_char_p, _VP, _VP, _VP, _VP], _I),
     "cupcfd_gpu_hdf5_mesh_read": ([C.c_char_p, _I, _I, _I] + [_VP] * 11, _I),
     "cupcfd_gpu_mesh_load_hdf5": ([C.c_char_p, _VP, _VP], _I),
+    "cupcfd_gpu_hdf5_mesh_write": ([C.c_char_p, _I, _I, _I, _I] + [_VP] * 11, _I),
+    "cupcfd_gpu_mesh_save_hdf5": ([_VP, C.c_char_p], _I),
+    "cupcfd_gpu_hdf5_dataset_shape": ([C.c_char_p, C.c_char_p, _VP, _VP, _VP], _I),
+    "cupcfd_gpu_hdf5_dataset_read": ([C.c_char_p, C.c_char_p, _VP, C.c_int64], _I),
     "cupcfd_gpu_mesh_get_info": ([_VP, _VP], _I),
     "cupcfd_gpu_mesh_set_regions": ([_VP, _I, _VP, _VP, _VP, _VP, _I], _I),
     "cupcfd_gpu_mesh_set_region_split": ([_VP, _I, _VP], _I),
@@ -312,6 +316,11 @@ class Mesh:
         """Write the mesh's source arrays, regions and split levels to a
         raw-binary mesh file (format in include/cupcfd_gpu.h)."""
         return lib().cupcfd_gpu_mesh_save(self.h, os.fsencode(path))
+
+    def save_hdf5(self, path):
+        """Write the mesh in the reference's HDF5 mesh layout (regions as
+        boundary region ids; their types are not part of that format)."""
+        check(lib().cupcfd_gpu_mesh_save_hdf5(self.h, os.fsencode(path)))
 
     def close(self):
         if getattr(self, "h", None):
@@ -662,3 +671,34 @@ def hdf5_mesh_read(path):
         "faceCell1", "faceCell2", "faceBnd", "faceLambda", "faceArea", "faceNorm", "faceCenter", "cellCenter",
         "cellVolume", "bndRegion", "bndDistance")]))
     return m
+
+
+def hdf5_mesh_write(path, m, bnd_distance=None):
+    """Write mesh dict ``m`` (the oracle's format: 0-based ids, faceCell2 -1
+    and faceBnd the boundary id on boundary faces; bndRegion optional) as an
+    HDF5 mesh file in the reference's layout."""
+    nC, nF, nB = int(m["nCells"]), int(m["nFaces"]), int(m["nBnd"])
+    a = dict(c1=np.ascontiguousarray(m["faceCell1"], np.int32), c2=np.ascontiguousarray(m["faceCell2"], np.int32),
+             fb=np.ascontiguousarray(m["faceBnd"], np.int32), lam=np.ascontiguousarray(m["faceLambda"], np.float64),
+             area=np.ascontiguousarray(m["faceArea"], np.float64),
+             S=np.ascontiguousarray(m["faceNorm"], np.float64).reshape(-1),
+             X=np.ascontiguousarray(m["faceCenter"], np.float64).reshape(-1),
+             cc=np.ascontiguousarray(m["cellCenter"], np.float64).reshape(-1),
+             vol=np.ascontiguousarray(m["cellVolume"], np.float64))
+    breg = None if m.get("bndRegion") is None else np.ascontiguousarray(m["bndRegion"], np.int32)
+    dist = None if bnd_distance is None else np.ascontiguousarray(bnd_distance, np.float64)
+    check(lib().cupcfd_gpu_hdf5_mesh_write(os.fsencode(path), nC, nF, nB, int(m.get("nRegions", 1)),
+                                           *[_p(a[k]) for k in ("c1", "c2", "fb", "lam", "area", "S", "X", "cc", "vol")],
+                                           _p(breg), _p(dist)))
+
+
+def hdf5_dataset(path, name):
+    """Any numeric dataset of an HDF5 mesh file, as float64 with its shape
+    (integers exact)."""
+    nd, isr = C.c_int32(), C.c_int32()
+    dims = (C.c_int64 * 4)()
+    check(lib().cupcfd_gpu_hdf5_dataset_shape(os.fsencode(path), name.encode(), C.byref(nd), dims, C.byref(isr)))
+    shape = tuple(int(dims[i]) for i in range(nd.value))
+    out = np.empty(shape, np.float64)
+    check(lib().cupcfd_gpu_hdf5_dataset_read(os.fsencode(path), name.encode(), _p(out), out.size))
+    return out

@@ -20,6 +20,16 @@
 // with boundary label /face/bnd; geometry is read as stored (/face/lambda,
 // area, n, x; /cell/x, vol); boundaries take region /bnd/rid and distance
 // /bnd/distance; regions are default regions (CupCfdSoAMesh.cpp:211-221).
+//
+// The writer produces the same layout in the same oldest structures (superblock
+// version 0, one symbol-table node per group, version 1 object headers,
+// contiguous little-endian int32 / float64 datasets, int32 root attributes),
+// with every dataset MeshHDF5Source reads for the mesh's connectivity and
+// geometry: /cell/{nfaces, cface, x, vol}, /face/{cell1, cell2, bnd, lambda,
+// area, n, x}, /bnd/{face, rid, distance} and root attributes ncel, nfac,
+// nbnd, nreg, nvrt. Vertices are not part of this library's meshes: nvrt is 0
+// and the vertex datasets (/vert, /face/vertices, /bnd/vertices) are absent.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <exception>
@@ -414,6 +424,214 @@ HostMesh read_mesh(const std::string &path) {
     return m;
 }
 
+// ---------------------------------------------------------------------------
+// Writer (the structures of the file comment; field layouts as the HDF
+// Group's File Format Specification gives them for these versions)
+// ---------------------------------------------------------------------------
+class H5Writer {
+public:
+    H5Writer() : b_(96, 0) {}  // superblock + root symbol-table entry, filled in by finish()
+
+    uint64_t dataset_i32(const int32_t *v, std::initializer_list<uint64_t> dims) {
+        return dataset(v, dims, 4, type_i32());
+    }
+    uint64_t dataset_f64(const double *v, std::initializer_list<uint64_t> dims) {
+        return dataset(v, dims, 8, type_f64());
+    }
+
+    // A group of named objects (at most 2K = 8, one symbol-table node) with
+    // optional scalar int32 attributes; returns its object header address.
+    uint64_t group(std::vector<std::pair<std::string, uint64_t>> ents,
+                   const std::vector<std::pair<std::string, int32_t>> &attrs = {}) {
+        std::sort(ents.begin(), ents.end());
+        if (ents.size() > 2 * LEAF_K) throw H5Error{CUPCFD_E_ERROR, "group too large for one symbol-table node"};
+        std::vector<uint8_t> heap(8, 0);  // offset 0: the empty name
+        std::vector<uint64_t> off;
+        for (auto &e : ents) {
+            off.push_back(heap.size());
+            heap.insert(heap.end(), e.first.begin(), e.first.end());
+            heap.push_back(0);
+            heap.resize(pad8(heap.size()), 0);
+        }
+        uint64_t heapData = alloc(heap);
+        std::vector<uint8_t> hp;
+        put_bytes(hp, "HEAP", 4); put_n(hp, 0, 4);
+        put_n(hp, heap.size(), 8); put_n(hp, UNDEF, 8); put_n(hp, heapData, 8);
+        uint64_t heapAddr = alloc(hp);
+        std::vector<uint8_t> sn;
+        put_bytes(sn, "SNOD", 4); put_n(sn, 1, 1); put_n(sn, 0, 1); put_n(sn, ents.size(), 2);
+        for (size_t i = 0; i < ents.size(); i++) {
+            put_n(sn, off[i], 8); put_n(sn, ents[i].second, 8); put_n(sn, 0, 4); put_n(sn, 0, 4);
+            sn.resize(sn.size() + 16, 0);
+        }
+        sn.resize(8 + 40 * 2 * LEAF_K, 0);
+        uint64_t snod = alloc(sn);
+        std::vector<uint8_t> tr;
+        put_bytes(tr, "TREE", 4); put_n(tr, 0, 1); put_n(tr, 0, 1); put_n(tr, 1, 2);
+        put_n(tr, UNDEF, 8); put_n(tr, UNDEF, 8);
+        put_n(tr, 0, 8); put_n(tr, snod, 8); put_n(tr, ents.empty() ? 0 : off.back(), 8);
+        tr.resize(24 + 8 * (2 * NODE_K + 1) + 8 * 2 * NODE_K, 0);
+        uint64_t tree = alloc(tr);
+        std::vector<std::vector<uint8_t>> msgs;
+        std::vector<uint8_t> stab;
+        put_n(stab, tree, 8); put_n(stab, heapAddr, 8);
+        msgs.push_back(message(0x11, stab));
+        for (auto &a : attrs) {
+            std::vector<uint8_t> nm(a.first.begin(), a.first.end());
+            nm.push_back(0);
+            std::vector<uint8_t> dt = type_i32(), sp = space({1}), body;
+            put_n(body, 1, 1); put_n(body, 0, 1); put_n(body, nm.size(), 2); put_n(body, dt.size(), 2);
+            put_n(body, sp.size(), 2);
+            append_padded(body, nm); append_padded(body, dt); append_padded(body, sp);
+            put_n(body, (uint32_t) a.second, 4);
+            msgs.push_back(message(0x0C, body));
+        }
+        rootTree_ = tree;
+        rootHeap_ = heapAddr;
+        return object_header(msgs);
+    }
+
+    // Fills in the superblock with `root` (the last group() call's header)
+    // as the root group and writes the file.
+    void write(uint64_t root, const std::string &path) {
+        std::vector<uint8_t> sb;
+        static const uint8_t sig[8] = {0x89, 'H', 'D', 'F', '\r', '\n', 0x1a, '\n'};
+        sb.insert(sb.end(), sig, sig + 8);
+        const uint8_t vers[8] = {0, 0, 0, 0, 0, 8, 8, 0};  // superblock, free space, root table, -, shared header, offsets, lengths, -
+        sb.insert(sb.end(), vers, vers + 8);
+        put_n(sb, LEAF_K, 2); put_n(sb, NODE_K, 2); put_n(sb, 0, 4);
+        put_n(sb, 0, 8); put_n(sb, UNDEF, 8); put_n(sb, b_.size(), 8); put_n(sb, UNDEF, 8);
+        put_n(sb, 0, 8); put_n(sb, root, 8); put_n(sb, 1, 4); put_n(sb, 0, 4);  // root entry: cache type 1
+        put_n(sb, rootTree_, 8); put_n(sb, rootHeap_, 8);
+        std::memcpy(b_.data(), sb.data(), 96);
+        FILE *f = std::fopen(path.c_str(), "wb");
+        if (!f) throw H5Error{CUPCFD_E_FILE_MISSING, "cannot open " + path + " for writing"};
+        bool ok = std::fwrite(b_.data(), 1, b_.size(), f) == b_.size();
+        ok = (std::fclose(f) == 0) && ok;
+        if (!ok) throw H5Error{CUPCFD_E_ERROR, "writing " + path + " failed"};
+    }
+
+private:
+    static constexpr int LEAF_K = 4, NODE_K = 16;
+    std::vector<uint8_t> b_;
+    uint64_t rootTree_ = UNDEF, rootHeap_ = UNDEF;
+
+    static size_t pad8(size_t n) { return (n + 7) & ~size_t(7); }
+    static void put_n(std::vector<uint8_t> &v, uint64_t x, int n) {
+        for (int i = 0; i < n; i++) v.push_back((uint8_t) (x >> (8 * i)));
+    }
+    static void put_bytes(std::vector<uint8_t> &v, const char *p, int n) { v.insert(v.end(), p, p + n); }
+    static void append_padded(std::vector<uint8_t> &v, const std::vector<uint8_t> &a) {
+        v.insert(v.end(), a.begin(), a.end());
+        v.resize(v.size() + (pad8(a.size()) - a.size()), 0);
+    }
+    uint64_t alloc(const void *p, size_t n) {
+        uint64_t a = b_.size();
+        const uint8_t *q = static_cast<const uint8_t *>(p);
+        b_.insert(b_.end(), q, q + n);
+        b_.resize(pad8(b_.size()), 0);
+        return a;
+    }
+    uint64_t alloc(const std::vector<uint8_t> &v) { return alloc(v.data(), v.size()); }
+    static std::vector<uint8_t> message(int type, std::vector<uint8_t> body) {
+        body.resize(pad8(body.size()), 0);
+        std::vector<uint8_t> m;
+        put_n(m, type, 2); put_n(m, body.size(), 2); put_n(m, 0, 4);  // type, size, flags, reserved
+        m.insert(m.end(), body.begin(), body.end());
+        return m;
+    }
+    uint64_t object_header(const std::vector<std::vector<uint8_t>> &msgs) {
+        std::vector<uint8_t> h;
+        size_t body = 0;
+        for (auto &m : msgs) body += m.size();
+        put_n(h, 1, 1); put_n(h, 0, 1); put_n(h, msgs.size(), 2); put_n(h, 1, 4); put_n(h, body, 4); put_n(h, 0, 4);
+        for (auto &m : msgs) h.insert(h.end(), m.begin(), m.end());
+        return alloc(h);
+    }
+    static std::vector<uint8_t> space(std::initializer_list<uint64_t> dims) {
+        std::vector<uint8_t> v;
+        put_n(v, 1, 1); put_n(v, dims.size(), 1); put_n(v, 0, 2); put_n(v, 0, 4);
+        for (uint64_t d : dims) put_n(v, d, 8);
+        return v;
+    }
+    static std::vector<uint8_t> type_i32() {  // class 0 (fixed point), version 1, signed, little-endian
+        std::vector<uint8_t> v = {0x10, 0x08, 0, 0};
+        put_n(v, 4, 4); put_n(v, 0, 2); put_n(v, 32, 2);
+        return v;
+    }
+    static std::vector<uint8_t> type_f64() {  // class 1 (IEEE), version 1, little-endian, sign at bit 63
+        std::vector<uint8_t> v = {0x11, 0x20, 63, 0};
+        put_n(v, 8, 4);
+        put_n(v, 0, 2); put_n(v, 64, 2); put_n(v, 52, 1); put_n(v, 11, 1); put_n(v, 0, 1); put_n(v, 52, 1);
+        put_n(v, 1023, 4);
+        return v;
+    }
+    uint64_t dataset(const void *v, std::initializer_list<uint64_t> dims, int es, const std::vector<uint8_t> &dt) {
+        uint64_t n = 1;
+        for (uint64_t d : dims) n *= d;
+        uint64_t data = alloc(v, (size_t) (n * es));  // the host is little-endian, as the datatypes state
+        std::vector<uint8_t> layout = {3, 1};          // version 3, contiguous
+        put_n(layout, data, 8); put_n(layout, n * es, 8);
+        return object_header({message(0x01, space(dims)), message(0x03, dt), message(0x08, layout)});
+    }
+};
+
+// The datasets of a mesh in MeshHDF5Source's layout (0-based arrays in;
+// labels written 1-based), checked for consistency first.
+void write_mesh(const std::string &path, int nC, int nF, int nB, int nR, const int32_t *c1, const int32_t *c2,
+                const int32_t *fb, const double *lam, const double *area, const double *S, const double *X,
+                const double *cc, const double *vol, const int32_t *breg, const double *bdist) {
+    if (nC < 1 || nF < 1 || nB < 0 || nR < 1) throw H5Error{CUPCFD_E_ARRAY_SIZE_MISMATCH, "counts out of range"};
+    std::vector<int32_t> l1(nF), l2(nF), lb(nF), nfaces(nC, 0), bface(nB, 0), rid(nB, 1);
+    for (int f = 0; f < nF; f++) {
+        if (c1[f] < 0 || c1[f] >= nC || c2[f] < -1 || c2[f] >= nC)
+            throw H5Error{CUPCFD_E_INVALID_INDEX, "a face's cell id is out of range"};
+        l1[f] = c1[f] + 1;
+        l2[f] = c2[f] + 1;  // 0 on a boundary face
+        nfaces[c1[f]]++;
+        if (c2[f] >= 0) {
+            nfaces[c2[f]]++;
+            lb[f] = 0;
+        } else {
+            if (fb[f] < 0 || fb[f] >= nB || bface[fb[f]] != 0)
+                throw H5Error{CUPCFD_E_INVALID_INDEX, "boundary ids are not one per boundary face"};
+            bface[fb[f]] = f + 1;
+            lb[f] = fb[f] + 1;
+        }
+    }
+    for (int b = 0; b < nB; b++) {
+        if (bface[b] == 0) throw H5Error{CUPCFD_E_INVALID_INDEX, "a boundary id has no face"};
+        if (breg) {
+            if (breg[b] < 0 || breg[b] >= nR) throw H5Error{CUPCFD_E_INVALID_INDEX, "a boundary's region is out of range"};
+            rid[b] = breg[b] + 1;
+        }
+    }
+    // /cell/cface: each cell's faces, ascending face label, padded with 0
+    const int maxF = *std::max_element(nfaces.begin(), nfaces.end());
+    std::vector<int32_t> cface((size_t) nC * maxF, 0), fill(nC, 0);
+    for (int f = 0; f < nF; f++) {
+        cface[(size_t) c1[f] * maxF + fill[c1[f]]++] = f + 1;
+        if (c2[f] >= 0) cface[(size_t) c2[f] * maxF + fill[c2[f]]++] = f + 1;
+    }
+    std::vector<double> dist(nB, 0.0);
+    if (bdist) std::copy(bdist, bdist + nB, dist.begin());
+    H5Writer w;
+    const uint64_t C = (uint64_t) nC, F = (uint64_t) nF, B = (uint64_t) nB;
+    uint64_t cell = w.group({{"nfaces", w.dataset_i32(nfaces.data(), {C})},
+                             {"cface", w.dataset_i32(cface.data(), {C, (uint64_t) maxF})},
+                             {"x", w.dataset_f64(cc, {C, 3})},
+                             {"vol", w.dataset_f64(vol, {C})}});
+    uint64_t face = w.group({{"cell1", w.dataset_i32(l1.data(), {F})}, {"cell2", w.dataset_i32(l2.data(), {F})},
+                             {"bnd", w.dataset_i32(lb.data(), {F})}, {"lambda", w.dataset_f64(lam, {F})},
+                             {"area", w.dataset_f64(area, {F})}, {"n", w.dataset_f64(S, {F, 3})},
+                             {"x", w.dataset_f64(X, {F, 3})}});
+    uint64_t bnd = w.group({{"face", w.dataset_i32(bface.data(), {B})}, {"rid", w.dataset_i32(rid.data(), {B})},
+                            {"distance", w.dataset_f64(dist.data(), {B})}});
+    uint64_t root = w.group({{"cell", cell}, {"face", face}, {"bnd", bnd}},
+                            {{"ncel", nC}, {"nfac", nF}, {"nbnd", nB}, {"nreg", nR}, {"nvrt", 0}});
+    w.write(root, path);
+}
+
 template <class F>
 int guarded(const char *what, F &&f) {
     try {
@@ -497,4 +715,71 @@ extern "C" int cupcfd_gpu_mesh_load_hdf5(const char *path, const cupcfd_mesh_opt
     }
     *out = g;
     return CUPCFD_E_SUCCESS;
+}
+
+extern "C" int cupcfd_gpu_hdf5_mesh_write(const char *path, int32_t nCells, int32_t nFaces, int32_t nBoundaries,
+                                          int32_t nRegions, const int32_t *faceCell1, const int32_t *faceCell2,
+                                          const int32_t *faceBnd, const double *faceLambda, const double *faceArea,
+                                          const double *faceNorm, const double *faceCenter, const double *cellCenter,
+                                          const double *cellVolume, const int32_t *bndRegion,
+                                          const double *bndDistance) {
+    clear_error();
+    CG_RETURN_IF(!path || !faceCell1 || !faceCell2 || !faceBnd || !faceLambda || !faceArea || !faceNorm ||
+                     !faceCenter || !cellCenter || !cellVolume,
+                 CUPCFD_E_NULL_PTR, "hdf5_mesh_write: null argument");
+    return guarded("hdf5_mesh_write", [&] {
+        write_mesh(path, nCells, nFaces, nBoundaries, nRegions, faceCell1, faceCell2, faceBnd, faceLambda, faceArea,
+                   faceNorm, faceCenter, cellCenter, cellVolume, bndRegion, bndDistance);
+        return CUPCFD_E_SUCCESS;
+    });
+}
+
+extern "C" int cupcfd_gpu_mesh_save_hdf5(const cupcfd_gpu_mesh *m, const char *path) {
+    clear_error();
+    CG_RETURN_IF(!m || !path, CUPCFD_E_NULL_PTR, "mesh_save_hdf5: null argument");
+    CG_TRY(make_device_current(m->device));
+    const int nC = m->nC, nF = m->nF, nB = m->nB;
+    std::vector<int32_t> c1(nF), c2(nF), bnd(nF), breg(nB, 0);
+    std::vector<double> lam(nF), area(nF), S(3 * (size_t) nF), X(3 * (size_t) nF), cc(3 * (size_t) nC), vol(nC),
+        dist(nB, 0.0);
+    CG_TRY(cupcfd_gpu_mesh_get_geometry(m, c1.data(), c2.data(), bnd.data(), lam.data(), area.data(), S.data(),
+                                        X.data(), cc.data(), vol.data()));
+    CG_CHECK_CUDA(cudaStreamSynchronize(m->stream));
+    if (nB > 0 && m->bndRegion)
+        CG_CHECK_CUDA(cudaMemcpy(breg.data(), m->bndRegion, sizeof(int32_t) * nB, cudaMemcpyDeviceToHost));
+    if (nB > 0 && m->bndDist)
+        CG_CHECK_CUDA(cudaMemcpy(dist.data(), m->bndDist, sizeof(double) * nB, cudaMemcpyDeviceToHost));
+    return guarded("mesh_save_hdf5", [&] {
+        write_mesh(path, nC, nF, nB, std::max(m->nR, 1), c1.data(), c2.data(), bnd.data(), lam.data(), area.data(),
+                   S.data(), X.data(), cc.data(), vol.data(), breg.data(), dist.data());
+        return CUPCFD_E_SUCCESS;
+    });
+}
+
+extern "C" int cupcfd_gpu_hdf5_dataset_shape(const char *path, const char *name, int32_t *ndims, int64_t *dims,
+                                             int32_t *isReal) {
+    clear_error();
+    CG_RETURN_IF(!path || !name || !ndims || !dims || !isReal, CUPCFD_E_NULL_PTR, "hdf5_dataset_shape: null argument");
+    return guarded("hdf5_dataset_shape", [&] {
+        H5File h(path);
+        Dataset ds = h.dataset(name);
+        if (ds.dims.size() > 4) fail(std::string(name) + " has more than 4 dimensions");
+        *ndims = (int32_t) ds.dims.size();
+        for (size_t i = 0; i < ds.dims.size(); i++) dims[i] = (int64_t) ds.dims[i];
+        *isReal = ds.cls == 1;
+        return CUPCFD_E_SUCCESS;
+    });
+}
+
+extern "C" int cupcfd_gpu_hdf5_dataset_read(const char *path, const char *name, double *out, int64_t n) {
+    clear_error();
+    CG_RETURN_IF(!path || !name || !out, CUPCFD_E_NULL_PTR, "hdf5_dataset_read: null argument");
+    return guarded("hdf5_dataset_read", [&] {
+        H5File h(path);
+        Dataset ds = h.dataset(name);
+        if ((int64_t) ds.count() != n) throw H5Error{CUPCFD_E_ARRAY_SIZE_MISMATCH, std::string(name) + " has another size"};
+        std::vector<double> v = h.real(ds);
+        std::copy(v.begin(), v.end(), out);
+        return CUPCFD_E_SUCCESS;
+    });
 }

@@ -213,6 +213,34 @@ int cupcfd_gpu_hdf5_mesh_read(const char *path, int32_t nCells, int32_t nFaces, 
                               int32_t *bndRegion, double *bndDistance);
 int cupcfd_gpu_mesh_load_hdf5(const char *path, const cupcfd_mesh_options *opt, cupcfd_gpu_mesh **out);
 
+/* Mesh files in the same HDF5 layout, written by the library (the datasets
+ * MeshHDF5Source.cpp:215-1130 reads for connectivity and geometry): root
+ * attributes ncel, nfac, nbnd, nreg and nvrt (0: no vertices are stored, so
+ * /vert, /face/vertices and /bnd/vertices are absent); /cell/{nfaces, cface
+ * ([nCells][max faces], each cell's face labels ascending, 0-padded), x, vol};
+ * /face/{cell1, cell2 (0 on boundary faces), bnd (0 on interior faces),
+ * lambda, area, n, x}; /bnd/{face, rid, distance}; labels 1-based.
+ *   write:      host arrays as cupcfd_gpu_hdf5_mesh_read returns them
+ *               (0-based; bndRegion and bndDistance may be NULL: region 0,
+ *               distance 0). Face cells out of range, or boundary ids that
+ *               are not one per boundary face, return CUPCFD_E_INVALID_INDEX;
+ *               a file that cannot be created CUPCFD_E_FILE_MISSING;
+ *   save:       a device mesh, its boundaries' regions and distances (region
+ *               types are not part of the format: loading gives default
+ *               regions, as for the reference's files);
+ *   dataset:    any numeric dataset of such a file by path ("/cell/cface"):
+ *               its shape (up to 4 dimensions, isReal 0 for integers), and
+ *               its values as doubles (row-major, n = the element count). */
+int cupcfd_gpu_hdf5_mesh_write(const char *path, int32_t nCells, int32_t nFaces, int32_t nBoundaries,
+                               int32_t nRegions, const int32_t *faceCell1, const int32_t *faceCell2,
+                               const int32_t *faceBnd, const double *faceLambda, const double *faceArea,
+                               const double *faceNorm, const double *faceCenter, const double *cellCenter,
+                               const double *cellVolume, const int32_t *bndRegion, const double *bndDistance);
+int cupcfd_gpu_mesh_save_hdf5(const cupcfd_gpu_mesh *mesh, const char *path);
+int cupcfd_gpu_hdf5_dataset_shape(const char *path, const char *name, int32_t *ndims, int64_t *dims,
+                                  int32_t *isReal);
+int cupcfd_gpu_hdf5_dataset_read(const char *path, const char *name, double *out, int64_t n);
+
 int cupcfd_gpu_mesh_destroy(cupcfd_gpu_mesh *mesh);
 int cupcfd_gpu_mesh_get_info(const cupcfd_gpu_mesh *mesh, cupcfd_mesh_info *info);
 
