@@ -103,7 +103,8 @@ __device__ __forceinline__ double fwd_cell_f32(int c, const SellView &sv, const 
     const int2 *e = cell_entries(sv, c, w);
     float phic = phi[c];
     float4 sc = st[c];
-    Acc2 ax, ay, az;
+    Acc2x2 axy;  // (gx, gy) packed, gz alone
+    Acc2 az;
     double lsum = 0.0;
     for (int k0 = 0; k0 < w; k0 += CH) {
         int2 en[CH];
@@ -144,12 +145,13 @@ __device__ __forceinline__ double fwd_cell_f32(int c, const SellView &sv, const 
                     lsum = __fma_rn((double) gf[j], (double) m, lsum);
                 }
             }
-            ax.add_prod(phif, G[j].x); ay.add_prod(phif, G[j].y); az.add_prod(phif, G[j].z);
+            axy.add_prod(make_float2(phif, phif), make_float2(G[j].x, G[j].y));
+            az.add_prod(phif, G[j].z);
         }
     }
     double V = vol[c];
     double fact = 1.0 / V;
-    float rx = (float) (ax.value() * fact), ry = (float) (ay.value() * fact), rz = (float) (az.value() * fact);
+    float rx = (float) (axy.x() * fact), ry = (float) (axy.y() * fact), rz = (float) (az.value() * fact);
     g[c] = rx; g[ldc + c] = ry; g[2 * ldc + c] = rz;
     return __fma_rn(V, __fma_rn((double) rx, (double) rx, __fma_rn((double) ry, (double) ry, __dmul_rn((double) rz, (double) rz))),
                     lsum);
@@ -417,7 +419,8 @@ __device__ __forceinline__ void adj_cell_f32(int c, const SellView &sv, const fl
     if (doG) { hx = hscale * ldg_g<LDCG>(g + c); hy = hscale * ldg_g<LDCG>(g + ldc + c); hz = hscale * ldg_g<LDCG>(g + 2 * ldc + c); }
     float4 sc = make_float4(0, 0, 0, 0);
     if (doM) sc = st[c];
-    Acc2 pb, rb, ub, vb, wb;
+    Acc2 pb, rb, wb;
+    Acc2x2 uvb;  // (ubar, vbar) packed
     for (int k0 = 0; k0 < w; k0 += CH) {
         int2 en[CH];
         load_entries(e, k0, w, en);
@@ -455,12 +458,13 @@ __device__ __forceinline__ void adj_cell_f32(int c, const SellView &sv, const fl
                 float a = wc * gf[j];
                 rb.add_prod(a, fmaf(uF, G[j].x, fmaf(vF, G[j].y, wF * G[j].z)));
                 float b = a * denf;
-                ub.add_prod(b, G[j].x); vb.add_prod(b, G[j].y); wb.add_prod(b, G[j].z);
+                uvb.add_prod(make_float2(b, b), make_float2(G[j].x, G[j].y));
+                wb.add_prod(b, G[j].z);
             }
         }
     }
     if (doG) phibar[c] = (float) pb.value();
-    if (doM) stbar[c] = make_float4((float) rb.value(), (float) ub.value(), (float) vb.value(), (float) wb.value());
+    if (doM) stbar[c] = make_float4((float) rb.value(), (float) uvb.x(), (float) uvb.y(), (float) wb.value());
 }
 
 __global__ void __launch_bounds__(256, CUPCFD_MINB_ADJ_F64) k_adj_f64(int nC, SellView sv, const double4 *__restrict__ fg,
