@@ -295,6 +295,127 @@ def bench_uvw(cg, mesh, dev, st, g, steps, warmup, peak):
             "config": "generated mesh, default region, rlencos 0 (the reference benchmark's case)"}
 
 
+def _time_calls(st, fn, steps, warmup):
+    """Mean device time (ms) of fn() over `steps` calls on stream st, CUDA events."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(steps):
+        fn()
+    e1.record(st)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def bench_boundary_loops(cg, mesh, dev, st, steps):
+    """The mass-flux boundary / region loops (FluxMassDolfynBoundaryLoop1-5,
+    FluxMassDolfynRegionLoop; FP64, bit-identical to the reference) as a
+    solver step chains them, device-resident, on the bench mesh with six
+    regions (default, inlet, two outlets, symmetry, wall) assigned to its
+    boundaries at random. Sums run in boundary order, so the chain is bound
+    by its ordered reductions, not by bytes."""
+    import numpy as np
+    import torch
+    nB, nC, nF = mesh.nBoundaries, mesh.nCells, mesh.nFaces
+    rng = np.random.Generator(np.random.Philox(key=SEED + 7))
+    rtype = np.array([0, 1, 2, 3, 4, 2], np.int32)
+    check = mesh.set_regions(rtype, rng.standard_normal(18), rng.uniform(0.9, 1.1, 6), rng.integers(0, 6, nB))
+    if check != cg.E_SUCCESS or mesh.set_region_split(rng.uniform(0.2, 0.8, 6)) != cg.E_SUCCESS:
+        raise RuntimeError(cg.last_error())
+    D = dict(dtype=torch.float64, device=dev)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(**D)
+    mf = T(rng.uniform(1e-6, 1e-2, nF) * rng.choice([-1.0, 1.0], nF))
+    su = T(rng.standard_normal(nC))
+    u, v, w, den = (T(rng.uniform(1e-6, 1e-2, nB)) for _ in range(4))
+    fr = T(rng.uniform(1e-6, 1e-2, 6))
+    sc = torch.zeros(5, **D)
+    ff = torch.zeros(6, **D)
+
+    def chain():
+        cg.dev_boundary_loop1(mesh, mf, sc[0:1], stream=st)
+        cg.dev_boundary_loop3(mesh, sc[0:1], sc[1:2], stream=st)
+        cg.dev_boundary_loop4(mesh, mf, u, v, w, den, sc[1:2], sc[2:3], stream=st)
+        cg.dev_boundary_loop2(mesh, mf, fr, sc[3:4], stream=st)
+        cg.dev_region_loop(mesh, ff, fr, sc[0:1], stream=st)
+        cg.dev_boundary_loop5(mesh, mf, su, u, v, w, 1.3, (1, 1, 1), ff, sc[4:5], stream=st)
+
+    ms = _time_calls(st, chain, steps, 3)
+    return {"call": "cupcfd_gpu_dev_boundary_loop1..5 + cupcfd_gpu_dev_region_loop (FP64, bit-identical)",
+            "us_per_chain": ms * 1e3, "boundaries": nB, "value": nB / (ms * 1e-3) / 1e9, "unit": "Gboundaries/s",
+            "steps": steps, "config": "bench mesh, six regions assigned to the boundaries at random"}
+
+
+def bench_halo(cg, mesh, dev, st, steps, parts=8):
+    """Halo pack / unpack (cupcfd_gpu_dev_halo_pack / _unpack) for one rank of
+    the bench mesh cut into `parts` z-slabs (the reference's naive
+    partition): the two cell planes its neighbours need, packed from phi,
+    the float4 state and the three gradient components (32 bytes a cell),
+    and as many ghost cells unpacked. The transfer between GPUs is NCCL's and
+    needs more than one GPU; this times the two kernels around it."""
+    import numpy as np
+    import torch
+    n = round(mesh.nCells ** (1 / 3))
+    plane = n * n
+    c2o, _ = mesh.numbering()
+    o2c = np.empty_like(c2o)
+    o2c[c2o] = np.arange(len(c2o), dtype=np.int32)
+    z0 = n // parts * (parts // 2)                      # an interior slab [z0, z0 + n / parts)
+    z1 = z0 + n // parts
+    ref = lambda z: np.arange(z * plane, (z + 1) * plane, dtype=np.int64)
+    send = torch.from_numpy(o2c[np.concatenate([ref(z0), ref(z1 - 1)])].astype(np.int32)).to(dev)
+    ghost = torch.from_numpy(o2c[np.concatenate([ref(z0 - 1), ref(z1)])].astype(np.int32)).to(dev)
+    nC, k = mesh.nCells, send.numel()
+    phi = torch.rand(nC, device=dev)
+    state = torch.rand(nC, 4, device=dev)
+    grad = torch.rand(3, nC, device=dev)
+    bp, bs, bg = torch.empty(k, device=dev), torch.empty(k, 4, device=dev), torch.empty(k, 3, device=dev)
+
+    L, S = cg.lib(), cg._stream(st)
+
+    def exchange():   # (field, element bytes, components, component stride, buffer)
+        for f, es, nc, ld, b in ((phi, 4, 1, 0, bp), (state, 16, 1, 0, bs), (grad, 4, 3, nC, bg)):
+            cg.check(L.cupcfd_gpu_dev_halo_pack(cg._p(f), es, nc, ld, cg._p(send), k, cg._p(b), S))
+        for f, es, nc, ld, b in ((phi, 4, 1, 0, bp), (state, 16, 1, 0, bs), (grad, 4, 3, nC, bg)):
+            cg.check(L.cupcfd_gpu_dev_halo_unpack(cg._p(b), es, nc, k, cg._p(ghost), cg._p(f), ld, S))
+
+    ms = _time_calls(st, exchange, steps, 3)
+    return {"call": "cupcfd_gpu_dev_halo_pack / _unpack (phi, float4 state, 3 gradient components)",
+            "us_per_exchange": ms * 1e3, "cells_packed": k, "cells_unpacked": k,
+            "bytes_per_exchange": 2 * k * (32 + 4), "gbs": 2 * k * (32 + 4) / (ms * 1e-3) / 1e9, "steps": steps,
+            "config": f"one rank of {parts} z-slabs of the bench mesh: 2 planes sent, 2 planes of ghosts"}
+
+
+def bench_mesh_files(cg, n=128):
+    """Mesh files: a generated n^3 mesh written and read back in the
+    reference's HDF5 layout (cupcfd_gpu_mesh_save_hdf5 / _load_hdf5) and in
+    the library's raw-binary format (cupcfd_gpu_mesh_save / _load), host
+    clock, page cache warm."""
+    import tempfile
+    import torch
+    mesh = cg.Mesh.structgen(n, n, n)
+    out = {"mesh": f"{n}^3", "cells": mesh.nCells, "faces": mesh.nFaces}
+    with tempfile.TemporaryDirectory() as d:
+        for kind, save, load in (("hdf5", mesh.save_hdf5, cg.Mesh.load_hdf5),
+                                 ("raw", mesh.save, cg.Mesh.load)):
+            p = os.path.join(d, "m." + kind)
+            t0 = time.perf_counter()
+            save(p)
+            t1 = time.perf_counter()
+            m2 = load(p)
+            torch.cuda.synchronize()
+            t2 = time.perf_counter()
+            size = os.path.getsize(p)
+            m2.close()
+            os.remove(p)
+            out[kind] = {"bytes": size, "save_s": t1 - t0, "load_s": t2 - t1,
+                         "load_gbs": size / (t2 - t1) / 1e9}
+    mesh.close()
+    return out
+
+
 # ---------------------------------------------------------------------------
 # reference arm
 # ---------------------------------------------------------------------------
@@ -532,6 +653,16 @@ def run_gpu(a):
             except Exception as ex:
                 uvw["cpu_reference"] = {"value": None, "sample": f"failed: {ex}"}
         torch.cuda.synchronize()
+    # ---- the other rows either side of the path: boundary / region loops,
+    # halo pack / unpack, mesh files (after the momentum loop, which wants
+    # the mesh's default region)
+    rows = None
+    if not a.no_rows:
+        rows = {"boundary_loops": bench_boundary_loops(cg, mesh, dev, st, max(3, K // 10)),
+                "halo": bench_halo(cg, mesh, dev, st, max(3, K // 10))}
+        if rank == 0 and world == 1:
+            rows["mesh_files"] = bench_mesh_files(cg)
+        torch.cuda.synchronize()
     kbytes = {"k_fwd_madj_f32_pf": bm["fwd_madj_f32"], "k_gadj_f32_pf": bm["gadj_f32"], "k_fused_f32": bm["pipeline_f32"],
               "k_fwd_f32_pf": bm["fwd_f32"], "k_fwd_f32": bm["fwd_f32"], "k_adj_f32_pf": bm["adj_f32"],
               "k_adj_f32": bm["adj_f32"]}
@@ -583,6 +714,7 @@ def run_gpu(a):
             "e2e": e2e,
             "cpu_baseline": cpu,
             "uvw_face_loop1": uvw,
+            "next_rows": rows,
             "gpu_launches": launches,
             "clocks": clk,
             "mesh_build_s": t_build,
@@ -608,6 +740,8 @@ def main():
     ap.add_argument("--cpu-reps", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-uvw", action="store_true", help="skip the momentum face loop measurement")
+    ap.add_argument("--no-rows", action="store_true",
+                    help="skip the boundary-loop, halo and mesh-file measurements")
     a = ap.parse_args()
     if a.warmup < 3:
         a.warmup = 3

@@ -8,6 +8,7 @@
 #include <mutex>
 
 #include "kernels_fused.cuh"
+#include "strided.cuh"
 #include "perm.cuh"
 
 using namespace cupcfd_gpu;
@@ -22,7 +23,7 @@ enum PfKernel { PF_FWD_F32 = 0, PF_ADJ_F32, PF_FWD_F64, PF_ADJ_F64, PF_FWD_MADJ,
 // scratch slots of a mesh (each grows on demand and is reused across calls)
 enum Slot {
     S_ERR = 0, S_GEOM = 1, S_IN0, S_IN1, S_IN2, S_IN3, S_IN4, S_IN5, S_IN6, S_IN7,
-    S_OUT0, S_OUT1, S_OUT2, S_OUT3, S_OUT4, S_GO, S_LOSS, S_CNT, S_NORM
+    S_OUT0, S_OUT1, S_OUT2, S_OUT3, S_OUT4, S_GO, S_LOSS, S_CNT, S_NORM, S_SPAN
 };
 
 template <class T>
@@ -778,25 +779,23 @@ int h2d_real(cupcfd_gpu_mesh *m, int slot, const void *h, int64_t n, int rs, voi
     return CUPCFD_E_SUCCESS;
 }
 
-// strided host vec3 view -> packed device [3n] of rs bytes
+// strided host vec3 view -> packed device [3n] of rs bytes (strided.cuh)
 int h2d_vec3(cupcfd_gpu_mesh *m, int slot, const cupcfd_vec3_view &v, int64_t n, int rs, void **dptr) {
     CG_RETURN_IF(!v.base, CUPCFD_E_NULL_PTR, "null vector array");
-    CG_RETURN_IF(v.stride < 3 * rs || v.offset < 0, CUPCFD_E_CONFIG_INVALID_VALUE, "vector view: bad stride/offset");
-    void *d;
+    CG_RETURN_IF(v.stride < 3 * rs || v.offset < 0 || v.offset + 3 * rs > v.stride, CUPCFD_E_CONFIG_INVALID_VALUE,
+                 "vector view: bad stride/offset");
+    void *d, *span = nullptr;
     CG_TRY(m->scratchBuf(slot, (size_t) std::max<int64_t>(n, 1) * 3 * rs, &d));
-    if (n > 0)
-        CG_CHECK_CUDA(cudaMemcpy2DAsync(d, 3 * rs, (const char *) v.base + v.offset, (size_t) v.stride, 3 * rs, (size_t) n,
-                                        cudaMemcpyHostToDevice, m->stream));
+    if (v.stride != 3 * rs) CG_TRY(m->scratchBuf(S_SPAN, std::max<size_t>(vec3_span_bytes(n, v.stride, v.offset, rs), 1), &span));
+    CG_TRY(upload_vec3_span(v.base, v.stride, v.offset, n, rs, span, d, m->stream));
     *dptr = d;
     return CUPCFD_E_SUCCESS;
 }
 
-// packed device [3n] of rs bytes -> strided host vec3 view
+// packed device [3n] of rs bytes -> strided host vec3 view (strided.cuh;
+// returns once the host records are written unless they are packed)
 int d2h_vec3(cupcfd_gpu_mesh *m, const void *d, void *base, int stride, int offset, int64_t n, int rs) {
-    if (n <= 0) return CUPCFD_E_SUCCESS;
-    CG_CHECK_CUDA(cudaMemcpy2DAsync((char *) base + offset, (size_t) stride, d, 3 * rs, 3 * rs, (size_t) n,
-                                    cudaMemcpyDeviceToHost, m->stream));
-    return CUPCFD_E_SUCCESS;
+    return download_vec3_span(d, base, stride, offset, n, rs, m->hostStage, m->stream);
 }
 
 void zero_vec3_tail(void *base, int stride, int offset, int from, int to, int rs) {

@@ -13,7 +13,7 @@ namespace {
 
 constexpr int BT = 256;
 // scratch slots of the host-buffer calls (kept across calls)
-enum BndSlot { B_MF = 40, B_SU, B_U, B_V, B_W, B_DEN, B_REG, B_REG2, B_SCAL };
+enum BndSlot { B_MF = 40, B_SU, B_U, B_V, B_W, B_DEN, B_REG, B_REG2, B_SCAL, B_SELC, B_SELV, B_SELR };
 
 // Boundary -> face and sorted-boundary -> cell maps for the caller's numbering.
 struct Maps {
@@ -49,27 +49,34 @@ int down(void *h, const void *d, size_t bytes, cudaStream_t st) {
     return CUPCFD_E_SUCCESS;
 }
 
+// The sum over the boundaries of region type `type`, in boundary order, of
+// base[map[ib] * stride + offset], from *init (or initValue) into *out, and
+// into regionAcc[region] (may be null) in the same order.
+int ordered_sum(cupcfd_gpu_mesh *m, int type, const double *base, int stride, int offset, const int *map,
+                const double *init, double initValue, double *out, double *regionAcc, cudaStream_t st) {
+    int *cnt, *regs;
+    double *vals;
+    CG_TRY(slot(m, B_SELC, (size_t) m->nB / SEL_T + 2, &cnt));
+    CG_TRY(slot(m, B_SELV, (size_t) m->nB, &vals));
+    CG_TRY(slot(m, B_SELR, (size_t) m->nB, &regs));
+    return launch_ordered_sum<1>(SelArgs{m->nB, m->bndRegion, m->regionType, type}, base, stride, offset, map, init,
+                                 initValue, out, regionAcc, m->nR, cnt, vals, regs, st);
+}
+
 // ---- the loops on device arrays (face arrays indexed through mp.face, cell
 // arrays through mp.cell); every scalar in device memory ----
 int run_loop1(cupcfd_gpu_mesh *m, Maps mp, const double *mf, double *flowin, cudaStream_t st) {
-    k_bl_sum<<<1, 1024, 0, st>>>(m->nB, m->bndRegion, m->regionType, CUPCFD_RTYPE_INLET, mf, 1, 0, mp.face, nullptr,
-                                 0.0, flowin, nullptr, 0);
-    CG_LAUNCHED();
-    return CUPCFD_E_SUCCESS;
+    return ordered_sum(m, CUPCFD_RTYPE_INLET, mf, 1, 0, mp.face, nullptr, 0.0, flowin, nullptr, st);
 }
 
 int run_loop2(cupcfd_gpu_mesh *m, Maps mp, const double *mf, double *flowRegion, double *flowout, cudaStream_t st) {
-    k_bl_sum<<<1, 1024, 0, st>>>(m->nB, m->bndRegion, m->regionType, CUPCFD_RTYPE_OUTLET, mf, 1, 0, mp.face, nullptr,
-                                 0.0, flowout, flowRegion, m->nR);
-    CG_LAUNCHED();
-    return CUPCFD_E_SUCCESS;
+    return ordered_sum(m, CUPCFD_RTYPE_OUTLET, mf, 1, 0, mp.face, nullptr, 0.0, flowout, flowRegion, st);
 }
 
 int run_loop3(cupcfd_gpu_mesh *m, const double *flowin, double *ratearea, double *areaout, cudaStream_t st) {
     // face areas from the internal {xf, yf, zf, area} records
-    k_bl_sum<<<1, 1024, 0, st>>>(m->nB, m->bndRegion, m->regionType, CUPCFD_RTYPE_OUTLET, (const double *) m->fc64, 4,
-                                 3, m->bndFaceInt, nullptr, 0.0, areaout, nullptr, 0);
-    CG_LAUNCHED();
+    CG_TRY(ordered_sum(m, CUPCFD_RTYPE_OUTLET, (const double *) m->fc64, 4, 3, m->bndFaceInt, nullptr, 0.0, areaout,
+                       nullptr, st));
     k_bl_ratearea<<<1, 1, 0, st>>>(flowin, areaout, ratearea);
     CG_LAUNCHED();
     return CUPCFD_E_SUCCESS;
@@ -82,10 +89,7 @@ int run_loop4(cupcfd_gpu_mesh *m, Maps mp, double *mf, double *uB, double *vB, d
                                                          m->bndFaceInt, m->fg64, m->fc64, mf, uB, vB, wB, denB, ratearea);
         CG_LAUNCHED();
     }
-    k_bl_sum<<<1, 1024, 0, st>>>(m->nB, m->bndRegion, m->regionType, CUPCFD_RTYPE_OUTLET, mf, 1, 0, mp.face, nullptr,
-                                 0.0, flowout, nullptr, 0);
-    CG_LAUNCHED();
-    return CUPCFD_E_SUCCESS;
+    return ordered_sum(m, CUPCFD_RTYPE_OUTLET, mf, 1, 0, mp.face, nullptr, 0.0, flowout, nullptr, st);
 }
 
 int run_loop5(cupcfd_gpu_mesh *m, Maps mp, double *mf, double *su, double *uB, double *vB, double *wB, double fact,
@@ -99,10 +103,7 @@ int run_loop5(cupcfd_gpu_mesh *m, Maps mp, double *mf, double *su, double *uB, d
         CG_LAUNCHED();
     }
     // *flowout2 is not reset (MassKernels.ipp:457-521): the sum starts from its value
-    k_bl_sum<<<1, 1024, 0, st>>>(m->nB, m->bndRegion, m->regionType, CUPCFD_RTYPE_OUTLET, mf, 1, 0, mp.face, flowout2,
-                                 0.0, flowout2, nullptr, 0);
-    CG_LAUNCHED();
-    return CUPCFD_E_SUCCESS;
+    return ordered_sum(m, CUPCFD_RTYPE_OUTLET, mf, 1, 0, mp.face, flowout2, 0.0, flowout2, nullptr, st);
 }
 
 int run_region_loop(cupcfd_gpu_mesh *m, double *flowFact, const double *flowRegion, const double *flowIn,

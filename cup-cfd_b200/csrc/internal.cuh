@@ -158,6 +158,7 @@ struct cupcfd_gpu_mesh {
 
     std::vector<cupcfd_gpu::DevBuf> owned;  // everything above, freed by destroy
     std::vector<cupcfd_gpu::DevBuf> scratch; // reusable buffers for host-buffer calls
+    std::vector<char> hostStage;             // host staging of strided copies back (strided.cuh)
     int64_t bytes = 0;
 
     template <class T>

@@ -3,9 +3,8 @@
 //
 // The reference walks boundaries ib = 0 .. nB-1 and adds into scalars (and,
 // in loop 2, per-region sums) one boundary at a time; reproducing its
-// rounding means adding in that order. k_bl_sum does it with one block: the
-// block stages 1024 boundaries' values in shared memory, one thread adds the
-// selected ones in order, the block moves on. The per-boundary updates
+// rounding means adding in that order (ordered_sum.cuh: the selected
+// boundaries gathered in parallel, then one chain of additions per sum). The per-boundary updates
 // (loops 4 and 5) are independent and run one thread per boundary. Loop 5's
 // su[cell1] -= massFlux applies, per cell, its outlet boundaries in
 // ascending boundary id: one thread per cell over the boundaries sorted by
@@ -18,54 +17,9 @@
 
 #include "arith.cuh"
 #include "internal.cuh"
+#include "ordered_sum.cuh"
 
 namespace cupcfd_gpu {
-
-// Sum, in boundary order, of base[map[ib] * stride + offset] over the
-// boundaries of region type `type`, starting from init; also adds each
-// value into regionAcc[region] (in/out, may be null) in the same order.
-// One block of 1024 threads.
-__global__ void __launch_bounds__(1024) k_bl_sum(int nB, const int *__restrict__ bndRegion,
-                                                 const int *__restrict__ regionType, int type,
-                                                 const double *__restrict__ base, int stride, int offset,
-                                                 const int *__restrict__ map, const double *init, double initValue,
-                                                 double *__restrict__ out, double *__restrict__ regionAcc, int nR) {
-    constexpr int T = 1024;
-    __shared__ double sv[T];
-    __shared__ int sr[T];
-    __shared__ double racc[T];
-    const int tid = threadIdx.x;
-    const bool regionsInSmem = regionAcc && nR <= T;
-    if (regionsInSmem)
-        for (int r = tid; r < nR; r += T) racc[r] = regionAcc[r];
-    double acc = init ? *init : initValue;  // thread 0's running sum
-    for (int b0 = 0; b0 < nB; b0 += T) {
-        int ib = b0 + tid, ir = -1;
-        double v = 0.0;
-        if (ib < nB) {
-            ir = bndRegion[ib];
-            if (regionType[ir] == type) v = base[(size_t) map[ib] * stride + offset];
-            else ir = -1;
-        }
-        sv[tid] = v;
-        sr[tid] = ir;
-        __syncthreads();
-        if (tid == 0) {
-            int n = min(T, nB - b0);
-            for (int k = 0; k < n; k++) {
-                int r = sr[k];
-                if (r < 0) continue;
-                acc = __dadd_rn(acc, sv[k]);
-                if (regionsInSmem) racc[r] = __dadd_rn(racc[r], sv[k]);
-                else if (regionAcc) regionAcc[r] = __dadd_rn(regionAcc[r], sv[k]);
-            }
-        }
-        __syncthreads();
-    }
-    if (tid == 0) *out = acc;
-    if (regionsInSmem)
-        for (int r = tid; r < nR; r += T) regionAcc[r] = racc[r];
-}
 
 // Loop 3's last line: *ratearea = -flowin / areaout (MassKernels.ipp:390).
 __global__ void k_bl_ratearea(const double *__restrict__ flowin, const double *__restrict__ areaout,

@@ -446,49 +446,4 @@ __global__ void __launch_bounds__(CARRY_T) k_carry_apply(CarryIn a, const int2 *
     carry[fi] = code;
 }
 
-// FluxUVWDolfynBndsLoop1 (UVWKernels.ipp:527-544): wall boundaries add their
-// shear onto their region's force tangent in boundary order. One block: the
-// block stages BT boundaries, one thread adds in order.
-__global__ void __launch_bounds__(512) k_uvw_bnds(int nB, int nR, const int *__restrict__ bndRegion,
-                                                  const int *__restrict__ regionType, const double *__restrict__ shear,
-                                                  double *__restrict__ ft) {
-    constexpr int T = 512, RMAX = 1024;
-    __shared__ double sv[3 * T];
-    __shared__ int sr[T];
-    __shared__ double racc[3 * RMAX];
-    const int tid = threadIdx.x;
-    const bool inSmem = nR <= RMAX;
-    if (inSmem)
-        for (int r = tid; r < 3 * nR; r += T) racc[r] = ft[r];
-    double *acc = inSmem ? racc : ft;
-    for (int b0 = 0; b0 < nB; b0 += T) {
-        int ib = b0 + tid, ir = -1;
-        if (ib < nB) {
-            ir = bndRegion[ib];
-            if (regionType[ir] == CUPCFD_RTYPE_WALL) {
-                sv[3 * tid] = shear[3 * (int64_t) ib];
-                sv[3 * tid + 1] = shear[3 * (int64_t) ib + 1];
-                sv[3 * tid + 2] = shear[3 * (int64_t) ib + 2];
-            } else {
-                ir = -1;
-            }
-        }
-        sr[tid] = ir;
-        __syncthreads();
-        if (tid == 0) {
-            int n = min(T, nB - b0);
-            for (int k = 0; k < n; k++) {
-                int r = sr[k];
-                if (r < 0) continue;
-                acc[3 * r] = da(acc[3 * r], sv[3 * k]);
-                acc[3 * r + 1] = da(acc[3 * r + 1], sv[3 * k + 1]);
-                acc[3 * r + 2] = da(acc[3 * r + 2], sv[3 * k + 2]);
-            }
-        }
-        __syncthreads();
-    }
-    if (inSmem)
-        for (int r = tid; r < 3 * nR; r += T) ft[r] = racc[r];
-}
-
 }  // namespace cupcfd_gpu

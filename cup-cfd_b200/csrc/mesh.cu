@@ -10,6 +10,7 @@
 #include <cstring>
 #include <mutex>
 
+#include "strided.cuh"
 #include "internal.cuh"
 
 namespace cupcfd_gpu {
@@ -759,14 +760,14 @@ int upload_real(const void *h, int64_t n, int rs, double *dst, float *stage, cud
     return CUPCFD_E_SUCCESS;
 }
 
-int upload_vec3(const cupcfd_vec3_view &v, int64_t n, int rs, double *dst, float *stage, cudaStream_t st) {
-    CG_RETURN_IF(v.stride < 3 * rs || v.offset < 0, CUPCFD_E_CONFIG_INVALID_VALUE, "vec3 view: bad stride/offset");
+// span: device staging of the view's span (strided.cuh)
+int upload_vec3(const cupcfd_vec3_view &v, int64_t n, int rs, double *dst, float *stage, void *span, cudaStream_t st) {
+    CG_RETURN_IF(v.stride < 3 * rs || v.offset < 0 || v.offset + 3 * rs > v.stride, CUPCFD_E_CONFIG_INVALID_VALUE,
+                 "vec3 view: bad stride/offset");
     if (rs == 8) {
-        CG_CHECK_CUDA(cudaMemcpy2DAsync(dst, 24, (const char *) v.base + v.offset, (size_t) v.stride, 24, (size_t) n,
-                                        cudaMemcpyHostToDevice, st));
+        CG_TRY(upload_vec3_span(v.base, v.stride, v.offset, n, 8, span, dst, st));
     } else {
-        CG_CHECK_CUDA(cudaMemcpy2DAsync(stage, 12, (const char *) v.base + v.offset, (size_t) v.stride, 12, (size_t) n,
-                                        cudaMemcpyHostToDevice, st));
+        CG_TRY(upload_vec3_span(v.base, v.stride, v.offset, n, 4, span, stage, st));
         k_f32_to_f64<<<grid_for(3 * n, 256), 256, 0, st>>>(3 * n, stage, dst);
         CG_LAUNCHED();
     }
@@ -844,9 +845,14 @@ extern "C" int cupcfd_gpu_mesh_create(const cupcfd_mesh_view *v, const cupcfd_me
     bool hasX = v->faceXpac.base && v->faceXnac.base;
     if (hasX) { s.xpac = b.get<double>(3 * (size_t) nF); s.xnac = b.get<double>(3 * (size_t) nF); }
     float *stage = rs == 4 ? b.get<float>(3 * (size_t) std::max(nF, nC)) : nullptr;
+    size_t spanBytes = 1;
+    for (const cupcfd_vec3_view *w : {&v->faceNorm, &v->faceCenter, &v->cellCenter, &v->faceXpac, &v->faceXnac})
+        if (w->base && w->stride != 3 * rs)
+            spanBytes = std::max(spanBytes, vec3_span_bytes(w == &v->cellCenter ? nC : nF, w->stride, w->offset, rs));
+    void *span = b.get<char>(spanBytes);
     int rc = CUPCFD_E_SUCCESS;
     if (!s.c1 || !s.c2 || !s.bnd || !s.lam || !s.area || !s.S || !s.xf || !s.cc || !s.vol || (hasX && (!s.xpac || !s.xnac)) ||
-        (rs == 4 && !stage)) {
+        (rs == 4 && !stage) || !span) {
         set_error("mesh_create: out of device memory for the source arrays");
         rc = CUPCFD_E_ERROR;
     }
@@ -857,12 +863,12 @@ extern "C" int cupcfd_gpu_mesh_create(const cupcfd_mesh_view *v, const cupcfd_me
     TRYRC(upload_real(v->faceLambda, nF, rs, s.lam, stage, st));
     TRYRC(upload_real(v->faceArea, nF, rs, s.area, stage, st));
     TRYRC(upload_real(v->cellVolume, nC, rs, s.vol, stage, st));
-    TRYRC(upload_vec3(v->faceNorm, nF, rs, s.S, stage, st));
-    TRYRC(upload_vec3(v->faceCenter, nF, rs, s.xf, stage, st));
-    TRYRC(upload_vec3(v->cellCenter, nC, rs, s.cc, stage, st));
+    TRYRC(upload_vec3(v->faceNorm, nF, rs, s.S, stage, span, st));
+    TRYRC(upload_vec3(v->faceCenter, nF, rs, s.xf, stage, span, st));
+    TRYRC(upload_vec3(v->cellCenter, nC, rs, s.cc, stage, span, st));
     if (hasX) {
-        TRYRC(upload_vec3(v->faceXpac, nF, rs, s.xpac, stage, st));
-        TRYRC(upload_vec3(v->faceXnac, nF, rs, s.xnac, stage, st));
+        TRYRC(upload_vec3(v->faceXpac, nF, rs, s.xpac, stage, span, st));
+        TRYRC(upload_vec3(v->faceXnac, nF, rs, s.xnac, stage, span, st));
     }
     if (rc == CUPCFD_E_SUCCESS && cudaStreamSynchronize(st) != cudaSuccess) {
         set_error("mesh_create: upload failed");

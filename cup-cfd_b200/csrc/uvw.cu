@@ -10,6 +10,8 @@
 #include <mutex>
 
 #include "kernels_uvw.cuh"
+#include "ordered_sum.cuh"
+#include "strided.cuh"
 #include "perm.cuh"
 
 using namespace cupcfd_gpu;
@@ -18,7 +20,7 @@ namespace {
 
 constexpr int BT = 256;
 // scratch slots of the host-buffer call (kept across calls)
-enum UvwSlot { U_CELLS = 60, U_GRADS, U_VEC, U_TMP, U_MF, U_RF, U_BND, U_BLK };
+enum UvwSlot { U_CELLS = 60, U_GRADS, U_VEC, U_TMP, U_MF, U_RF, U_BND, U_BLK, U_SELC, U_SELV, U_SELR, U_SPAN };
 
 template <class T>
 int slot(cupcfd_gpu_mesh *m, int s, size_t n, T **p) {
@@ -165,10 +167,11 @@ int cells_out(cupcfd_gpu_mesh *m, const double *src, double *h, double *tmp, cud
 
 int vec3_in(cupcfd_gpu_mesh *m, const cupcfd_vec3_view &v, double *dst, int64_t ld, double *tmp, cudaStream_t st) {
     CG_RETURN_IF(!v.base, CUPCFD_E_NULL_PTR, "momentum loop: null vector array");
-    CG_RETURN_IF(v.stride < 24 || v.offset < 0, CUPCFD_E_CONFIG_INVALID_VALUE, "momentum loop: bad vector stride/offset");
-    if (m->nC > 0)
-        CG_CHECK_CUDA(cudaMemcpy2DAsync(tmp, 24, (const char *) v.base + v.offset, (size_t) v.stride, 24, (size_t) m->nC,
-                                        cudaMemcpyHostToDevice, st));
+    CG_RETURN_IF(v.stride < 24 || v.offset < 0 || v.offset + 24 > v.stride, CUPCFD_E_CONFIG_INVALID_VALUE,
+                 "momentum loop: bad vector stride/offset");
+    char *span = nullptr;
+    if (v.stride != 24) CG_TRY(slot(m, U_SPAN, vec3_span_bytes(m->nC, v.stride, v.offset, 8), &span));
+    CG_TRY(upload_vec3_span(v.base, v.stride, v.offset, m->nC, 8, span, tmp, st));
     k_aos_to_blocks<double, double><<<grid_for(m->nC, BT), BT, 0, st>>>(m->nC, 3, m->cellN2O, tmp, dst, ld);
     CG_LAUNCHED();
     return CUPCFD_E_SUCCESS;
@@ -337,8 +340,15 @@ extern "C" int cupcfd_gpu_dev_uvw_bnds_loop1(cupcfd_gpu_mesh *m, void *stream) {
     cudaStream_t st = (cudaStream_t) stream;
     CG_TRY(ensure_state(m, st));
     if (m->nB > 0) {
-        k_uvw_bnds<<<1, 512, 0, st>>>(m->nB, m->nR, m->bndRegion, m->regionType, m->bndShear, m->regionFT);
-        CG_LAUNCHED();
+        // wall boundaries add their shear onto their region's force tangent
+        // in boundary order (UVWKernels.ipp:527-544)
+        int *cnt, *regs;
+        double *vals;
+        CG_TRY(slot(m, U_SELC, (size_t) m->nB / SEL_T + 2, &cnt));
+        CG_TRY(slot(m, U_SELV, 3 * (size_t) m->nB, &vals));
+        CG_TRY(slot(m, U_SELR, (size_t) m->nB, &regs));
+        CG_TRY(launch_ordered_sum<3>(SelArgs{m->nB, m->bndRegion, m->regionType, CUPCFD_RTYPE_WALL}, m->bndShear, 3, 0,
+                                     nullptr, nullptr, 0.0, nullptr, m->regionFT, m->nR, cnt, vals, regs, st));
     }
     return CUPCFD_E_SUCCESS;
 }
