@@ -348,6 +348,29 @@ def bench_boundary_loops(cg, mesh, dev, st, steps):
             "steps": steps, "config": "bench mesh, six regions assigned to the boundaries at random"}
 
 
+def cpu_boundary_loops(n, reps):
+    """Gboundaries/s of the reference's boundary-loop chain (its
+    FluxMassDolfynBoundaryLoop1-5 and FluxMassDolfynRegionLoop templates,
+    compiled unchanged, one core) on an n^3 generated mesh with the same six
+    regions assigned at random."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import oracle as O
+    if O.load_ref() is None:
+        return {"value": None, "sample": "reference build absent"}
+    m = O.structgen(n, n, n)
+    rng = np.random.Generator(np.random.Philox(key=SEED + 7))
+    m.update(nRegions=6, regionType=np.array([0, 1, 2, 3, 4, 2], np.int32), regionUVW=rng.standard_normal(18),
+             regionDen=rng.uniform(0.9, 1.1, 6), bndRegion=rng.integers(0, 6, m["nBnd"]).astype(np.int32))
+    R = O.RefKernels(m).boundary_loops(rng.uniform(0.2, 0.8, 6))
+    nF, nB, nC = m["nFaces"], m["nBnd"], m["nCells"]
+    secs = R.boundary_chain(rng.uniform(1e-6, 1e-2, nF) * rng.choice([-1.0, 1.0], nF), rng.standard_normal(nC),
+                            *[rng.uniform(1e-6, 1e-2, nB) for _ in range(4)], rng.uniform(1e-6, 1e-2, 6), reps)
+    t = statistics.median(secs)
+    return {"value": nB / t / 1e9, "unit": "Gboundaries/s", "cores": 1, "kind": "reference", "ms_per_chain": t * 1e3,
+            "sample": f"{n}^3 generated mesh ({nB} boundaries), six random regions; median of {reps} chains"}
+
+
 def bench_halo(cg, mesh, dev, st, steps, parts=8):
     """Halo pack / unpack (cupcfd_gpu_dev_halo_pack / _unpack) for one rank of
     the bench mesh cut into `parts` z-slabs (the reference's naive
@@ -662,6 +685,11 @@ def run_gpu(a):
                 "halo": bench_halo(cg, mesh, dev, st, max(3, K // 10))}
         if rank == 0 and world == 1:
             rows["mesh_files"] = bench_mesh_files(cg)
+            if not a.no_cpu:
+                try:
+                    rows["boundary_loops"]["cpu_reference"] = cpu_boundary_loops(96, 20)
+                except Exception as ex:
+                    rows["boundary_loops"]["cpu_reference"] = {"value": None, "sample": f"failed: {ex}"}
         torch.cuda.synchronize()
     kbytes = {"k_fwd_madj_f32_pf": bm["fwd_madj_f32"], "k_gadj_f32_pf": bm["gadj_f32"], "k_fused_f32": bm["pipeline_f32"],
               "k_fwd_f32_pf": bm["fwd_f32"], "k_fwd_f32": bm["fwd_f32"], "k_adj_f32_pf": bm["adj_f32"],

@@ -86,6 +86,7 @@ def load_ref():
                 _ref.ref_boundary_loop4.argtypes = [C.c_void_p] * 6 + [C.c_double, C.c_void_p]
                 _ref.ref_boundary_loop5.argtypes = [C.c_void_p] * 6 + [C.c_double] + [C.c_int] * 3 + [C.c_void_p] * 2
                 _ref.ref_region_loop.argtypes = [C.c_void_p] * 3 + [C.c_double]
+                _ref.ref_boundary_chain.argtypes = [C.c_void_p] * 9 + [C.c_int, C.c_void_p]
                 _ref.ref_ctx_set_uvw_geometry.argtypes = [C.c_void_p] * 3
                 _ref.ref_uvw_state.argtypes = [C.c_void_p] * 5
                 _ref.ref_uvw_face_loop1.argtypes = [C.c_void_p, C.c_double, C.c_double] + [C.c_void_p] * 19 + [C.c_int, C.c_void_p]
@@ -517,6 +518,15 @@ class RefKernels:
         assert self.ref.ref_boundary_loop5(self.h, _p(mf), _p(s_), _p(u), _p(v), _p(w), float(fact),
                                            *[int(bool(x)) for x in solve], _p(ff), C.byref(out)) == E_SUCCESS
         return mf, s_, u, v, w, out.value
+
+    def boundary_chain(self, massflux, su, ub, vb, wb, denb, flow_region, reps):
+        """Per-call seconds of the reference's boundary-loop chain (loops 1, 3,
+        4, 2, the region loop, 5) run `reps` times in place (timing only)."""
+        a = [_f64(x) for x in (massflux, su, ub, vb, wb, denb, flow_region)]
+        ff = np.zeros(self.m["nRegions"])
+        secs = np.empty(reps)
+        assert self.ref.ref_boundary_chain(self.h, *[_p(x) for x in a], _p(ff), reps, _p(secs)) == E_SUCCESS
+        return secs
 
     def region_loop(self, flow_region, flow_in):
         ff = np.full(self.m["nRegions"], np.nan)

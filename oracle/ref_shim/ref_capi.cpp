@@ -323,6 +323,29 @@ extern "C" int ref_region_loop(void * p, double * flowFact, double * flowRegion,
 	return (int) cupcfd::fvm::FluxMassDolfynRegionLoop(c->mesh, flowFact, c->nR, flowRegion, c->nR, flowIn);
 }
 
+/* The boundary-loop chain of a solver step (loops 1, 3, 4, 2, the region
+ * loop, 5), `reps` times on the same arrays (updated in place, as the GPU
+ * chain does); per-chain seconds go to secs[reps]. Timing only. */
+extern "C" int ref_boundary_chain(void * p, double * massFlux, double * su, double * uB, double * vB, double * wB,
+                                  double * denB, double * flowRegion, double * flowFact, int reps, double * secs) {
+	RefCtx * c = (RefCtx *) p;
+	int st = 0;
+	for (int r = 0; r < reps; r++) {
+		double flowin = 0.0, ratearea = 0.0, flowout = 0.0, flowout2 = 0.25, flowout4 = 0.0;
+		auto t0 = std::chrono::steady_clock::now();
+		st |= ref_boundary_loop1(p, massFlux, &flowin) - (int) cupcfd::error::E_SUCCESS;
+		st |= ref_boundary_loop3(p, flowin, &ratearea) - (int) cupcfd::error::E_SUCCESS;
+		st |= ref_boundary_loop4(p, massFlux, uB, vB, wB, denB, ratearea, &flowout4) - (int) cupcfd::error::E_SUCCESS;
+		st |= ref_boundary_loop2(p, massFlux, flowRegion, &flowout) - (int) cupcfd::error::E_SUCCESS;
+		st |= ref_region_loop(p, flowFact, flowRegion, flowin) - (int) cupcfd::error::E_SUCCESS;
+		st |= ref_boundary_loop5(p, massFlux, su, uB, vB, wB, 1.3, 1, 1, 1, flowFact, &flowout2) -
+		      (int) cupcfd::error::E_SUCCESS;
+		auto t1 = std::chrono::steady_clock::now();
+		if (secs) secs[r] = std::chrono::duration<double>(t1 - t0).count();
+	}
+	return st == 0 ? (int) cupcfd::error::E_SUCCESS : (int) cupcfd::error::E_ERROR;
+}
+
 /* ---- momentum loops (UVWKernels.ipp:38-544), called unchanged ---- */
 extern "C" void ref_ctx_set_uvw_geometry(void * p, const double * rlencos, const double * bdist) {
 	RefCtx * c = (RefCtx *) p;
