@@ -813,8 +813,9 @@ extern "C" int cupcfd_gpu_gradient_phi_gauss_dolfyn(cupcfd_gpu_mesh *m, int32_t 
     CG_RETURN_IF(!m || !phiCell || !dPhidxCell || !dPhidxoCell || (m->nB > 0 && !phiBoundary), CUPCFD_E_NULL_PTR,
                  "GradientPhiGaussDolfyn: null argument");
     CG_RETURN_IF(rs != 4 && rs != 8, CUPCFD_E_CONFIG_INVALID_VALUE, "GradientPhiGaussDolfyn: real_size must be 4 or 8");
-    CG_RETURN_IF(stride < 3 * rs || strideo < 3 * rs || offset < 0 || offseto < 0, CUPCFD_E_CONFIG_INVALID_VALUE,
-                 "GradientPhiGaussDolfyn: bad vector stride/offset");
+    CG_RETURN_IF(stride < 3 * rs || strideo < 3 * rs || offset < 0 || offseto < 0 || offset + 3 * rs > stride ||
+                     offseto + 3 * rs > strideo,
+                 CUPCFD_E_CONFIG_INVALID_VALUE, "GradientPhiGaussDolfyn: bad vector stride/offset");
     CG_TRY(check_prec(m, precision));
     // the reference reads phiCell[ip/in], phiBoundary[ib] and updates dPhidxCell[0..lTCells)
     // (GradientKernels.ipp:90-95,107-111,122-126); short arrays are index errors
@@ -852,7 +853,10 @@ extern "C" int cupcfd_gpu_gradient_phi_gauss_dolfyn(cupcfd_gpu_mesh *m, int32_t 
     else k_blocks_to_aos<float, float><<<grid, BLK, 0, st>>>(nC, 3, m->cellO2N, (const float *) grad, nC, (float *) out);
     CG_LAUNCHED();
     CG_TRY(d2h_vec3(m, out, dPhidxCell, stride, offset, nC, rs));
-    CG_TRY(d2h_vec3(m, out, dPhidxoCell, strideo, offseto, std::min(nC, nDPhidxoCell), rs));
+    if (stride != 3 * rs)  // the packed values are in host staging already: one copy back serves both arrays
+        scatter_vec3_host(m->hostStage.data(), dPhidxoCell, strideo, offseto, std::min(nC, nDPhidxoCell), rs);
+    else
+        CG_TRY(d2h_vec3(m, out, dPhidxoCell, strideo, offseto, std::min(nC, nDPhidxoCell), rs));
     CG_CHECK_CUDA(cudaStreamSynchronize(st));
     // entries past lTCells: zeroed by the reset loop, copied into dPhidxoCell (:66-70, :129-131)
     zero_vec3_tail(dPhidxCell, stride, offset, nC, nDPhidxCell, rs);

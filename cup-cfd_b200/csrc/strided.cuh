@@ -70,6 +70,14 @@ inline int upload_vec3_span(const void *base, int stride, int offset, int64_t n,
     return CUPCFD_E_SUCCESS;
 }
 
+// packed components [3n] in host memory -> the component bytes of n host
+// records (stride, offset)
+inline void scatter_vec3_host(const char *packed, void *base, int stride, int offset, int64_t n, int rs) {
+    char *b = static_cast<char *>(base) + offset;
+    const size_t rec = 3 * (size_t) rs;
+    for (int64_t i = 0; i < n; i++) std::memcpy(b + (size_t) i * stride, packed + (size_t) i * rec, rec);
+}
+
 // packed device [3n] -> the component bytes of n host records (stride,
 // offset). A packed destination is copied into directly (stream-ordered);
 // otherwise the copy goes through host staging and the call returns once the
@@ -86,7 +94,7 @@ inline int download_vec3_span(const void *src, void *base, int stride, int offse
     if (hstage.size() < (size_t) n * rec) hstage.resize((size_t) n * rec);
     CG_CHECK_CUDA(cudaMemcpyAsync(hstage.data(), src, (size_t) n * rec, cudaMemcpyDeviceToHost, st));
     CG_CHECK_CUDA(cudaStreamSynchronize(st));
-    for (int64_t i = 0; i < n; i++) std::memcpy(b + (size_t) i * stride, hstage.data() + (size_t) i * rec, rec);
+    scatter_vec3_host(hstage.data(), base, stride, offset, n, rs);
     return CUPCFD_E_SUCCESS;
 }
 
