@@ -487,3 +487,49 @@ def test_host_call_equals_device_call(cg, gpu, order, prec, mk):
     for i, k in enumerate(("denBar", "uBar", "vBar", "wBar")):
         bits(host[k], sb[i], k)
     bits(host["loss"], out["loss"].cpu().numpy(), "loss")
+
+
+def test_strided_vector_views_upload(cg, gpu):
+    """Mesh creation from the vector arrays in every layout a caller can
+    hand over (packed (n,3); the EuclideanVector layout (n,4) with the
+    components after a pad slot; records whose components are not aligned
+    to 8 bytes, 28-byte records with the components at byte 4): the same
+    device geometry bit for bit."""
+    import ctypes as C
+    ref = O.jitter(9, 8, 7, 0.25, seed=31, permute=True)
+    base = cg.Mesh.from_arrays(ref).geometry()
+    padded = dict(ref)
+    for k in ("faceNorm", "faceCenter", "cellCenter"):
+        a = np.asarray(ref[k], np.float64).reshape(-1, 3)
+        padded[k] = np.concatenate([np.full((len(a), 1), 7.5), a], 1)
+    g4 = cg.Mesh.from_arrays(padded).geometry()
+    for k in base:
+        assert np.array_equal(base[k], g4[k]), k
+    # 28-byte records, components at byte offset 4 (not 8-byte aligned)
+    keep = {}
+
+    def odd(a):
+        a = np.ascontiguousarray(np.asarray(a, np.float64).reshape(-1, 3))
+        buf = np.zeros((len(a), 28), np.uint8)
+        buf[:, 4:] = a.view(np.uint8).reshape(len(a), 24)
+        keep[id(buf)] = buf
+        return cg.Vec3View(buf.ctypes.data, 28, 4)
+
+    v = cg.MeshView()
+    v.nCells, v.nFaces, v.nBoundaries, v.real_size = ref["nCells"], ref["nFaces"], ref["nBnd"], 8
+    arr = {k: np.ascontiguousarray(ref[k]) for k in ("faceCell1", "faceCell2", "faceBnd", "faceLambda", "faceArea",
+                                                     "cellVolume")}
+    v.faceCell1, v.faceCell2, v.faceBnd = (cg._p(arr[k]) for k in ("faceCell1", "faceCell2", "faceBnd"))
+    v.faceLambda, v.faceArea, v.cellVolume = (cg._p(arr[k]) for k in ("faceLambda", "faceArea", "cellVolume"))
+    v.faceNorm, v.faceCenter, v.cellCenter = odd(ref["faceNorm"]), odd(ref["faceCenter"]), odd(ref["cellCenter"])
+    v.faceXpac = v.faceXnac = cg.Vec3View(None, 24, 0)
+    h = C.c_void_p()
+    o = cg.Mesh._opts(cg.ORDER_MORTON, (1 << cg.PREC_F64) | (1 << cg.PREC_F32C), -1)
+    assert cg.lib().cupcfd_gpu_mesh_create(C.byref(v), C.byref(o), C.byref(h)) == cg.E_SUCCESS, cg.last_error()
+    godd = cg.Mesh(h).geometry()
+    for k in base:
+        assert np.array_equal(base[k], godd[k]), k
+    # overlapping records are refused
+    v.faceNorm = cg.Vec3View(v.faceNorm.base, 28, 8)
+    h2 = C.c_void_p()
+    assert cg.lib().cupcfd_gpu_mesh_create(C.byref(v), C.byref(o), C.byref(h2)) == cg.E_CONFIG_INVALID_VALUE
