@@ -72,6 +72,41 @@ def _host_chain(cg, mesh, d, solve):
     return r
 
 
+def test_many_regions_bit_exact(cg, gpu):
+    """2,500 regions (more than one block of region sums: the region sums
+    run in groups of 992): loops 1-5 and the region loop, and the momentum
+    loop's boundary loop (wall shear onto each region's force tangent), bit
+    for bit against the oracle."""
+    base = O.jitter(30, 28, 26, 0.25, seed=12, permute=True)
+    rng = np.random.Generator(np.random.Philox(key=43))
+    nR = 2500
+    m = dict(base)
+    m["nRegions"] = nR
+    m["regionType"] = rng.integers(0, 5, nR).astype(np.int32)
+    m["regionUVW"] = rng.standard_normal(3 * nR)
+    m["regionDen"] = rng.uniform(0.9, 1.1, nR)
+    m["bndRegion"] = rng.integers(0, nR, m["nBnd"]).astype(np.int32)
+    splvl = rng.uniform(0.2, 0.8, nR)
+    mesh = cg.Mesh.from_arrays(m, order=3)
+    assert mesh.set_regions(m["regionType"], m["regionUVW"], m["regionDen"], m["bndRegion"]) == cg.E_SUCCESS
+    assert mesh.set_region_split(splvl) == cg.E_SUCCESS
+    nF, nB, nC = m["nFaces"], m["nBnd"], m["nCells"]
+    d = dict(mf=rng.uniform(1e-6, 1e-2, nF) * rng.choice([-1.0, 1.0], nF),
+             u=rng.uniform(1e-6, 1e-2, nB), v=rng.uniform(1e-6, 1e-2, nB), w=rng.uniform(1e-6, 1e-2, nB),
+             den=rng.uniform(0.9, 1.1, nB), fr=rng.uniform(1e-6, 1e-2, nR), su=rng.standard_normal(nC))
+    want = _oracle_chain(m, splvl, d, (1, 1, 1))
+    got = _host_chain(cg, mesh, d, (1, 1, 1))
+    for k, v in want.items():
+        assert np.array_equal(np.asarray(got[k]), np.asarray(v)), k
+    # momentum loop's boundary loop on a shear the test sets
+    shear = rng.standard_normal((nB, 3))
+    ft0 = rng.standard_normal((nR, 3))
+    mesh.boundary_shear(shear)
+    mesh.region_force_tangent(nR, ft0)
+    assert cg.FluxUVWDolfynBndsLoop1(mesh) == cg.E_SUCCESS
+    assert np.array_equal(mesh.region_force_tangent(nR), O.uvw_bnds_loop1(m, shear, ft0))
+
+
 @pytest.mark.parametrize("kind,order", [("struct", 2), ("jitter", 3), ("jitter", 0), ("large", 3)])
 @pytest.mark.parametrize("solve", [(1, 1, 1), (0, 1, 0)])
 def test_boundary_loops_bit_exact(cg, gpu, kind, order, solve):
