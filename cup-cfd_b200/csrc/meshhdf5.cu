@@ -29,6 +29,11 @@
 // area, n, x}, /bnd/{face, rid, distance} and root attributes ncel, nfac,
 // nbnd, nreg, nvrt. Vertices are not part of this library's meshes: nvrt is 0
 // and the vertex datasets (/vert, /face/vertices, /bnd/vertices) are absent.
+#include <fcntl.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
@@ -68,18 +73,48 @@ struct Dataset {
     }
 };
 
+// The file's bytes, mapped read-only (the reader touches only the
+// structures and datasets it needs; nothing is copied up front).
+class FileBytes {
+public:
+    explicit FileBytes(const std::string &path) {
+        int fd = ::open(path.c_str(), O_RDONLY);
+        if (fd < 0) throw H5Error{CUPCFD_E_FILE_MISSING, "cannot open " + path};
+        struct stat sb;
+        if (::fstat(fd, &sb) != 0) {
+            ::close(fd);
+            throw H5Error{CUPCFD_E_FILE_MISSING, "cannot read " + path};
+        }
+        n_ = (size_t) std::max<off_t>(sb.st_size, 0);
+        if (n_ > 0) {
+            void *m = ::mmap(nullptr, n_, PROT_READ, MAP_PRIVATE, fd, 0);
+            if (m == MAP_FAILED) {
+                ::close(fd);
+                throw H5Error{CUPCFD_E_FILE_MISSING, "cannot map " + path};
+            }
+            p_ = static_cast<const uint8_t *>(m);
+        }
+        ::close(fd);
+    }
+    ~FileBytes() {
+        if (p_) ::munmap(const_cast<uint8_t *>(p_), n_);
+    }
+    FileBytes(const FileBytes &) = delete;
+    FileBytes &operator=(const FileBytes &) = delete;
+    size_t size() const { return n_; }
+    bool empty() const { return n_ == 0; }
+    const uint8_t *data() const { return p_; }
+    const uint8_t *begin() const { return p_; }
+    const uint8_t &operator[](size_t i) const { return p_[i]; }
+
+private:
+    const uint8_t *p_ = nullptr;
+    size_t n_ = 0;
+};
+
 class H5File {
 public:
-    explicit H5File(const std::string &path) {
-        FILE *f = std::fopen(path.c_str(), "rb");
-        if (!f) throw H5Error{CUPCFD_E_FILE_MISSING, "cannot open " + path};
-        std::fseek(f, 0, SEEK_END);
-        long n = std::ftell(f);
-        std::fseek(f, 0, SEEK_SET);
-        d_.resize(n > 0 ? (size_t) n : 0);
-        size_t got = d_.empty() ? 0 : std::fread(d_.data(), 1, d_.size(), f);
-        std::fclose(f);
-        if (got != d_.size()) throw H5Error{CUPCFD_E_FILE_MISSING, "cannot read " + path};
+    explicit H5File(const std::string &path) : d_(path) {
         static const uint8_t sig[8] = {0x89, 'H', 'D', 'F', '\r', '\n', 0x1a, '\n'};
         if (d_.size() < 96 || std::memcmp(d_.data(), sig, 8) != 0) fail("not an HDF5 file");
         int ver = u8(8);
@@ -150,6 +185,10 @@ public:
     std::vector<double> real(const Dataset &ds) const {
         std::vector<double> out(ds.count());
         const uint8_t *p = raw(ds);
+        if (p && ds.cls == 1 && ds.size == 8) {  // little-endian float64, as stored: one copy
+            if (!out.empty()) std::memcpy(out.data(), p, out.size() * 8);
+            return out;
+        }
         for (size_t i = 0; i < out.size(); i++) out[i] = value_real(ds, p ? p + i * ds.size : nullptr);
         return out;
     }
@@ -157,6 +196,14 @@ public:
         if (ds.cls != 0) fail("integer dataset expected");
         std::vector<int64_t> out(ds.count());
         const uint8_t *p = raw(ds);
+        if (p && ds.size == 4 && ds.isSigned) {  // little-endian int32
+            for (size_t i = 0; i < out.size(); i++) {
+                int32_t v;
+                std::memcpy(&v, p + 4 * i, 4);
+                out[i] = v;
+            }
+            return out;
+        }
         for (size_t i = 0; i < out.size(); i++) out[i] = value_int(ds, p ? p + i * ds.size : nullptr);
         return out;
     }
@@ -166,7 +213,7 @@ private:
         int type;
         size_t off, size;
     };
-    std::vector<uint8_t> d_;
+    FileBytes d_;
     uint64_t base_ = 0, root_ = 0;
     size_t rootEntry_ = 0;
 
@@ -431,6 +478,7 @@ HostMesh read_mesh(const std::string &path) {
 class H5Writer {
 public:
     H5Writer() : b_(96, 0) {}  // superblock + root symbol-table entry, filled in by finish()
+    void reserve(size_t bytes) { b_.reserve(bytes); }
 
     uint64_t dataset_i32(const int32_t *v, std::initializer_list<uint64_t> dims) {
         return dataset(v, dims, 4, type_i32());
@@ -616,6 +664,8 @@ void write_mesh(const std::string &path, int nC, int nF, int nB, int nR, const i
     std::vector<double> dist(nB, 0.0);
     if (bdist) std::copy(bdist, bdist + nB, dist.begin());
     H5Writer w;
+    w.reserve((size_t) nF * (3 * 4 + 8 * 8) + (size_t) nC * (4 + 4 * (size_t) maxF + 4 * 8) + (size_t) nB * 16 +
+              (1u << 20));
     const uint64_t C = (uint64_t) nC, F = (uint64_t) nF, B = (uint64_t) nB;
     uint64_t cell = w.group({{"nfaces", w.dataset_i32(nfaces.data(), {C})},
                              {"cface", w.dataset_i32(cface.data(), {C, (uint64_t) maxF})},
