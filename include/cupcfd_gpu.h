@@ -295,7 +295,10 @@ int cupcfd_gpu_mesh_get_numbering(const cupcfd_gpu_mesh *mesh, int32_t *cellNew2
  * components are written; the vptr slot is never touched). nGradient
  * iterations with the non-orthogonal correction of the previous iterate.
  * precision: CUPCFD_PREC_F64 (bit-identical to the reference for T=double)
- * or CUPCFD_PREC_F32C. sign_mode: CUPCFD_SIGN_*. */
+ * or CUPCFD_PREC_F32C. With T=float arrays (real_size 4) neither reproduces
+ * the reference's float instantiation bit for bit (that one rounds every sum
+ * in float): PREC_F64 computes in FP64 and rounds each result to float once.
+ * sign_mode: CUPCFD_SIGN_*. */
 int cupcfd_gpu_gradient_phi_gauss_dolfyn(cupcfd_gpu_mesh *mesh, int32_t nGradient,
                                          const void *phiCell, int32_t nPhiCell,
                                          const void *phiBoundary, int32_t nPhiBoundary,
