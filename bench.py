@@ -397,15 +397,16 @@ def bench_halo(cg, mesh, dev, st, steps, parts=8):
     bp, bs, bg = torch.empty(k, device=dev), torch.empty(k, 4, device=dev), torch.empty(k, 3, device=dev)
 
     L, S = cg.lib(), cg._stream(st)
+    fields = (cg.HaloField * 3)(cg.HaloField(phi.data_ptr(), 4, 1, 0, bp.data_ptr()),
+                                cg.HaloField(state.data_ptr(), 16, 1, 0, bs.data_ptr()),
+                                cg.HaloField(grad.data_ptr(), 4, 3, nC, bg.data_ptr()))
 
-    def exchange():   # (field, element bytes, components, component stride, buffer)
-        for f, es, nc, ld, b in ((phi, 4, 1, 0, bp), (state, 16, 1, 0, bs), (grad, 4, 3, nC, bg)):
-            cg.check(L.cupcfd_gpu_dev_halo_pack(cg._p(f), es, nc, ld, cg._p(send), k, cg._p(b), S))
-        for f, es, nc, ld, b in ((phi, 4, 1, 0, bp), (state, 16, 1, 0, bs), (grad, 4, 3, nC, bg)):
-            cg.check(L.cupcfd_gpu_dev_halo_unpack(cg._p(b), es, nc, k, cg._p(ghost), cg._p(f), ld, S))
+    def exchange():   # the three fields in one pack and one unpack launch
+        cg.check(L.cupcfd_gpu_dev_halo_pack_fields(fields, 3, cg._p(send), k, S))
+        cg.check(L.cupcfd_gpu_dev_halo_unpack_fields(fields, 3, cg._p(ghost), k, S))
 
     ms = _time_calls(st, exchange, steps, 3)
-    return {"call": "cupcfd_gpu_dev_halo_pack / _unpack (phi, float4 state, 3 gradient components)",
+    return {"call": "cupcfd_gpu_dev_halo_pack_fields / _unpack_fields (phi, float4 state, 3 gradient components)",
             "us_per_exchange": ms * 1e3, "cells_packed": k, "cells_unpacked": k,
             "bytes_per_exchange": 2 * k * (32 + 4), "gbs": 2 * k * (32 + 4) / (ms * 1e-3) / 1e9, "steps": steps,
             "config": f"one rank of {parts} z-slabs of the bench mesh: 2 planes sent, 2 planes of ghosts"}

@@ -63,6 +63,11 @@ class MeshView(C.Structure):
                 ("cellCenter", Vec3View), ("cellVolume", C.c_void_p)]
 
 
+class HaloField(C.Structure):
+    _fields_ = [("field", C.c_void_p), ("elemSize", C.c_int32), ("ncomp", C.c_int32), ("ld", C.c_int64),
+                ("buffer", C.c_void_p)]
+
+
 class MeshOptions(C.Structure):
     _fields_ = [("order", C.c_int32), ("precisions", C.c_int32), ("device", C.c_int32)]
 
@@ -121,6 +126,8 @@ SIGNATURES = {
     "cupcfd_gpu_dev_uvw_region_loop1": ([_VP, _VP], _I),
     "cupcfd_gpu_dev_halo_pack": ([_VP, _I, _I, _I64, _VP, _I, _VP, _VP], _I),
     "cupcfd_gpu_dev_halo_unpack": ([_VP, _I, _I, _I, _VP, _VP, _I64, _VP], _I),
+    "cupcfd_gpu_dev_halo_pack_fields": ([_VP, _I, _VP, _I, _VP], _I),
+    "cupcfd_gpu_dev_halo_unpack_fields": ([_VP, _I, _VP, _I, _VP], _I),
     "cupcfd_gpu_dev_uvw_bnds_loop1": ([_VP, _VP], _I),
     "cupcfd_gpu_mesh_set_fusion": ([_VP, _I], _I),
     "cupcfd_gpu_mesh_check_status": ([_VP, _VP], _I),

@@ -72,7 +72,62 @@ int check(int elemSize, int n, int ncomp, int64_t ld, const void *idx, const voi
     return CUPCFD_E_SUCCESS;
 }
 
+// Several fields in one launch: blockIdx.y is the field.
+constexpr int HALO_MAX_FIELDS = 8;
+struct FieldSet {
+    cupcfd_halo_field f[HALO_MAX_FIELDS];
+};
+
+template <class T>
+__device__ __forceinline__ void move(bool pack, int i, int ncomp, int64_t ld, int64_t j, const cupcfd_halo_field &f) {
+    T *field = static_cast<T *>(f.field), *buf = static_cast<T *>(f.buffer);
+    for (int c = 0; c < ncomp; c++) {
+        if (pack) buf[(int64_t) i * ncomp + c] = field[c * ld + j];
+        else field[c * ld + j] = buf[(int64_t) i * ncomp + c];
+    }
+}
+
+__global__ void k_halo_fields(bool pack, int n, const int *__restrict__ idx, const __grid_constant__ FieldSet fs) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const cupcfd_halo_field &f = fs.f[blockIdx.y];
+    const int64_t j = idx[i];
+    switch (f.elemSize) {
+    case 4: move<float>(pack, i, f.ncomp, f.ld, j, f); break;
+    case 8: move<double>(pack, i, f.ncomp, f.ld, j, f); break;
+    default: move<float4>(pack, i, f.ncomp, f.ld, j, f); break;
+    }
+}
+
+int launch_fields(bool pack, const cupcfd_halo_field *fields, int nFields, const int32_t *idx, int32_t n,
+                  cudaStream_t st) {
+    CG_RETURN_IF(!fields || nFields < 0 || nFields > HALO_MAX_FIELDS, CUPCFD_E_CONFIG_INVALID_VALUE,
+                 "halo: 0 to 8 fields per call");
+    FieldSet fs{};
+    for (int k = 0; k < nFields; k++) {
+        const cupcfd_halo_field &f = fields[k];
+        CG_TRY(check(f.elemSize, n, f.ncomp, f.ld, idx, f.field, f.buffer));
+        fs.f[k] = f;
+    }
+    if (n == 0 || nFields == 0) return CUPCFD_E_SUCCESS;
+    k_halo_fields<<<dim3(grid_for(n, HB), nFields), HB, 0, st>>>(pack, n, idx, fs);
+    CG_LAUNCHED();
+    return CUPCFD_E_SUCCESS;
+}
+
 }  // namespace
+
+extern "C" int cupcfd_gpu_dev_halo_pack_fields(const cupcfd_halo_field *fields, int32_t nFields, const int32_t *idx,
+                                               int32_t n, void *stream) {
+    clear_error();
+    return launch_fields(true, fields, nFields, idx, n, (cudaStream_t) stream);
+}
+
+extern "C" int cupcfd_gpu_dev_halo_unpack_fields(const cupcfd_halo_field *fields, int32_t nFields, const int32_t *idx,
+                                                 int32_t n, void *stream) {
+    clear_error();
+    return launch_fields(false, fields, nFields, idx, n, (cudaStream_t) stream);
+}
 
 extern "C" int cupcfd_gpu_dev_halo_pack(const void *src, int32_t elemSize, int32_t ncomp, int64_t ld, const int32_t *idx,
                                         int32_t n, void *dst, void *stream) {

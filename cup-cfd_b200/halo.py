@@ -199,6 +199,26 @@ class Halo:
         cg.check(cg.lib().cupcfd_gpu_dev_halo_unpack(cg._p(recvbuf), es, ncomp, int(self.r_off[-1]),
                                                      cg._p(self.recv_idx), cg._p(field), int(ld), cg._stream(stream)))
 
+    def _fields(self, fields, bufs):
+        """HaloField records of [(field, ncomp, ld)] with their buffers."""
+        arr = (cg.HaloField * len(fields))()
+        for k, ((field, ncomp, ld), buf) in enumerate(zip(fields, bufs)):
+            ld = ld or (field.shape[-1] if ncomp > 1 else 0)
+            arr[k] = cg.HaloField(field.data_ptr(), self._elem(field, ncomp), ncomp, int(ld), buf.data_ptr())
+        return arr
+
+    def pack_fields(self, fields, sendbufs, stream=None):
+        """pack() of several fields [(field, ncomp, ld)] in one launch."""
+        arr = self._fields(fields, sendbufs)
+        cg.check(cg.lib().cupcfd_gpu_dev_halo_pack_fields(arr, len(fields), cg._p(self.send_idx), int(self.s_off[-1]),
+                                                          cg._stream(stream)))
+
+    def unpack_fields(self, recvbufs, fields, stream=None):
+        """unpack() of several fields [(field, ncomp, ld)] in one launch."""
+        arr = self._fields(fields, recvbufs)
+        cg.check(cg.lib().cupcfd_gpu_dev_halo_unpack_fields(arr, len(fields), cg._p(self.recv_idx),
+                                                            int(self.r_off[-1]), cg._stream(stream)))
+
     def transfer(self, sendbuf, recvbuf, ncomp=1, words=1, group=None):
         """Each peer's part of sendbuf to that peer, each peer's part of
         recvbuf from it (NCCL for CUDA tensors, gloo for CPU ones). ``words``

@@ -558,6 +558,21 @@ int cupcfd_gpu_dev_halo_pack(const void *src, int32_t elemSize, int32_t ncomp, i
 int cupcfd_gpu_dev_halo_unpack(const void *src, int32_t elemSize, int32_t ncomp, int32_t n, const int32_t *idx,
                                void *dst, int64_t ld, void *stream);
 
+/* The same for up to 8 fields at once, one launch per call (the fields of
+ * one exchange share the index list): field k moves between fields[k].field
+ * (ncomp components ld apart, elemSize 4, 8 or 16 bytes) and its own
+ * element-major buffer fields[k].buffer, as the single-field calls do. */
+typedef struct cupcfd_halo_field {
+    void *field;
+    int32_t elemSize, ncomp;
+    int64_t ld;
+    void *buffer;
+} cupcfd_halo_field;
+int cupcfd_gpu_dev_halo_pack_fields(const cupcfd_halo_field *fields, int32_t nFields, const int32_t *idx, int32_t n,
+                                    void *stream);
+int cupcfd_gpu_dev_halo_unpack_fields(const cupcfd_halo_field *fields, int32_t nFields, const int32_t *idx, int32_t n,
+                                      void *stream);
+
 /* Number of kernels this library launched since load (all threads). */
 int64_t cupcfd_gpu_launch_count(void);
 

@@ -185,3 +185,44 @@ def test_pack_unpack_layouts(cg, gpu):
         else:
             fn2.reshape(ncomp, -1)[:, ri] = s.reshape(-1, ncomp).T
         assert np.array_equal(field.cpu().numpy(), fn2)
+
+
+def test_pack_fields_equals_single_field_calls(cg, gpu):
+    """The multi-field pack / unpack (one launch per direction) moves the
+    same bits as one single-field call per field: scalar, float4 record and
+    three-component fields, FP32 and FP64."""
+    import torch
+    H, m, part = _setup("jitter")
+    dev = torch.device("cuda:0")
+    loc = H.local_mesh(m, part, 1)
+    mesh = cg.Mesh.from_arrays(loc)
+    h = H.Halo(loc, mesh, dev)
+    nC = mesh.nCells
+    g = torch.Generator(device=dev)
+    g.manual_seed(5)
+    fields = [(torch.rand(nC, generator=g, device=dev), 1, 0),
+              (torch.rand(nC, 4, generator=g, device=dev), 1, 0),
+              (torch.rand(3, nC, generator=g, device=dev, dtype=torch.float64), 3, nC)]
+    words = [1, 4, 1]
+    single = [h.buffers(nc * w, f.dtype)[0] for (f, nc, _), w in zip(fields, words)]
+    for (f, nc, ld), b in zip(fields, single):
+        h.pack(f, b, nc, ld)
+    multi = [torch.full_like(b, float("nan")) for b in single]
+    h.pack_fields(fields, multi)
+    torch.cuda.synchronize()
+    for a, b in zip(single, multi):
+        assert torch.equal(a, b)
+    # unpack random buffers into copies of the fields both ways
+    recv = [torch.rand(max(h.r_off[-1], 1) * nc * w, generator=g, device=dev, dtype=f.dtype)
+            for (f, nc, _), w in zip(fields, words)]
+    one = [f.clone() for f, _, _ in fields]
+    for (f, nc, ld), r, o in zip(fields, recv, one):
+        h.unpack(r, o, nc, ld)
+    both = [f.clone() for f, _, _ in fields]
+    h.unpack_fields(recv, [(o, nc, ld) for o, (_, nc, ld) in zip(both, fields)])
+    torch.cuda.synchronize()
+    for a, b in zip(one, both):
+        assert torch.equal(a, b)
+    # more than 8 fields is refused
+    arr = (cg.HaloField * 9)()
+    assert cg.lib().cupcfd_gpu_dev_halo_pack_fields(arr, 9, cg._p(h.send_idx), 1, None) == cg.E_CONFIG_INVALID_VALUE
