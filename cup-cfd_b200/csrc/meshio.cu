@@ -32,7 +32,7 @@ using namespace cupcfd_gpu;
 namespace {
 
 constexpr char MAGIC[8] = {'C', 'U', 'P', 'C', 'F', 'D', 'M', '1'};
-constexpr int VERSION = 1;
+constexpr int VERSION = 2;  // 2: word-wise checksum
 
 struct Header {
     char magic[8];
@@ -41,14 +41,44 @@ struct Header {
 };
 static_assert(sizeof(Header) == 64, "64-byte header");
 
+// FNV-1a over the little-endian 64-bit words of the byte stream (the stream
+// is every byte added, in order; a last partial word is padded with zero
+// bytes): h = (h ^ word) * prime. A step per eight bytes instead of one per
+// byte; value() is the hash of everything added.
 struct Fnv {
     uint64_t h = 1469598103934665603ULL;
+    unsigned char pend[8] = {0};
+    size_t npend = 0;
+    void word(uint64_t w) {
+        h ^= w;
+        h *= 1099511628211ULL;
+    }
     void add(const void *p, size_t n) {
         const unsigned char *b = (const unsigned char *) p;
-        for (size_t i = 0; i < n; i++) {
-            h ^= b[i];
-            h *= 1099511628211ULL;
+        while (n > 0 && npend > 0) {  // complete a pending word
+            pend[npend++] = *b++;
+            n--;
+            if (npend == 8) {
+                uint64_t w;
+                std::memcpy(&w, pend, 8);
+                word(w);
+                npend = 0;
+            }
         }
+        for (; n >= 8; n -= 8, b += 8) {
+            uint64_t w;
+            std::memcpy(&w, b, 8);
+            word(w);
+        }
+        for (; n > 0; n--) pend[npend++] = *b++;
+    }
+    uint64_t value() const {
+        if (npend == 0) return h;
+        unsigned char last[8] = {0};
+        std::memcpy(last, pend, npend);
+        uint64_t w;
+        std::memcpy(&w, last, 8);
+        return (h ^ w) * 1099511628211ULL;
     }
 };
 
@@ -151,7 +181,8 @@ int mesh_save(const cupcfd_gpu_mesh *m, const char *path) {
          put(fl, h, rsp) && put(fl, h, breg);
     if (flags & 2) ok = ok && put(fl, h, rl);
     if (flags & 4) ok = ok && put(fl, h, bd);
-    ok = ok && fwrite(&h.h, sizeof(h.h), 1, fl.f) == 1;
+    const uint64_t sum = h.value();
+    ok = ok && fwrite(&sum, sizeof(sum), 1, fl.f) == 1;
     CG_RETURN_IF(!ok, CUPCFD_E_ERROR, std::string("mesh_save: write to ") + path + " failed");
     CG_RETURN_IF(fclose(fl.f) != 0, CUPCFD_E_ERROR, std::string("mesh_save: closing ") + path + " failed");
     fl.f = nullptr;
@@ -194,7 +225,7 @@ int mesh_load(const char *path, const cupcfd_mesh_options *opt, cupcfd_gpu_mesh 
     uint64_t stored = 0;
     ok = ok && fread(&stored, sizeof(stored), 1, fl.f) == 1;
     CG_RETURN_IF(!ok, CUPCFD_E_INVALID_FILE_FORMAT, std::string("mesh_load: ") + path + " is truncated");
-    CG_RETURN_IF(stored != h.h, CUPCFD_E_INVALID_FILE_FORMAT, std::string("mesh_load: checksum mismatch in ") + path);
+    CG_RETURN_IF(stored != h.value(), CUPCFD_E_INVALID_FILE_FORMAT, std::string("mesh_load: checksum mismatch in ") + path);
 
     cupcfd_mesh_view v;
     std::memset(&v, 0, sizeof(v));

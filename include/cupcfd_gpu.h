@@ -166,18 +166,21 @@ int cupcfd_gpu_mesh_create_structgen(int32_t nx, int32_t ny, int32_t nz, const d
 int cupcfd_gpu_mesh_create_jittered(int32_t nx, int32_t ny, int32_t nz, double jitter, uint64_t seed, int32_t permute,
                                     const cupcfd_mesh_options *opt, cupcfd_gpu_mesh **out);
 
-/* Mesh files. The reference ingests meshes through MeshHDF5Source
- * (src/geometry/mesh/implementation/source/MeshHDF5Source.cpp); HDF5 is not
- * part of this build, so a device mesh is saved to, and reloaded from, a
- * raw-binary file holding its source arrays in the reference's numbering:
- * a 64-byte header (magic "CUPCFDM1", version 1, nCells, nFaces,
+/* Mesh files of this library (the reference's own HDF5 mesh files are read
+ * and written by the cupcfd_gpu_hdf5_* calls below). A device mesh is saved
+ * to, and reloaded from, a raw-binary file holding everything the device
+ * mesh holds, its source arrays in the reference's numbering:
+ * a 64-byte header (magic "CUPCFDM1", version 2, nCells, nFaces,
  * nBoundaries, nRegions, flags: bit 0 xpac/xnac present, bit 1 rlencos
  * present, bit 2 boundary distances present), then faceCell1, faceCell2,
  * faceBnd (int32), faceLambda, faceArea, faceNorm[3], faceCenter[3],
  * [faceXpac[3], faceXnac[3]], cellCenter[3], cellVolume (float64),
  * regionType (int32), regionUVW[3], regionDen, regionSplvl (float64),
  * bndRegion (int32), [faceRLencos], [boundaryDistance] (float64), and an
- * FNV-1a 64-bit hash of all the bytes before it. Little-endian. Loading rebuilds the device layout exactly as
+ * FNV-1a 64-bit checksum of all the bytes before it, taken over 64-bit
+ * little-endian words (h = (h ^ word) * 1099511628211 from
+ * 14695981039346656037; a last partial word padded with zero bytes).
+ * Little-endian. Loading rebuilds the device layout exactly as
  * cupcfd_gpu_mesh_create with `opt`, then installs the regions, split
  * levels, rlencos and boundary distances, so kernels on a loaded mesh give
  * the saved mesh's bits.

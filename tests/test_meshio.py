@@ -23,11 +23,12 @@ from test_oracle_vs_reference import _with_regions
 
 
 def _fnv1a64(data: bytes) -> int:
-    a = np.frombuffer(data, np.uint8)
+    """FNV-1a over little-endian 64-bit words, a last partial word padded
+    with zero bytes."""
+    a = np.frombuffer(data + bytes(-len(data) % 8), "<u8")
     h = 1469598103934665603
-    for chunk in np.array_split(a, max(1, len(a) // 65536)):
-        for b in chunk.tolist():
-            h = ((h ^ b) * 1099511628211) & 0xFFFFFFFFFFFFFFFF
+    for w in a.tolist():
+        h = ((h ^ w) * 1099511628211) & 0xFFFFFFFFFFFFFFFF
     return h
 
 
@@ -45,7 +46,7 @@ def mesh_file_bytes(m, splvl, rlencos=None, bnd_dist=None):
     xn = np.asarray(m.get("faceXnac", np.zeros((nF, 3))), np.float64)
     flags = int(bool(np.any(xp != 0) or np.any(xn != 0))) | (2 if rlencos is not None else 0) | \
         (4 if bnd_dist is not None else 0)
-    hdr = b"CUPCFDM1" + struct.pack("<6i", 1, nC, nF, nB, nR, flags) + bytes(32)
+    hdr = b"CUPCFDM1" + struct.pack("<6i", 2, nC, nF, nB, nR, flags) + bytes(32)
     parts = [hdr]
     for k in ("faceCell1", "faceCell2", "faceBnd"):
         parts.append(np.ascontiguousarray(m[k], "<i4").tobytes())
@@ -111,7 +112,7 @@ def test_damaged_files_rejected(cg, tmp_path, xpac, geom):
 
     bad = {
         "magic": b"CUPCFDM2" + good[8:],
-        "version": good[:8] + struct.pack("<i", 2) + good[12:],
+        "version": good[:8] + struct.pack("<i", 3) + good[12:],
         "cells0": good[:12] + struct.pack("<i", 0) + good[16:],
         "faces+1": good[:16] + struct.pack("<i", int(m["nFaces"]) + 1) + good[20:],
         "flags": good[:28] + struct.pack("<i", 8) + good[32:],
