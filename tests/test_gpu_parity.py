@@ -533,3 +533,25 @@ def test_strided_vector_views_upload(cg, gpu):
     v.faceNorm = cg.Vec3View(v.faceNorm.base, 28, 8)
     h2 = C.c_void_p()
     assert cg.lib().cupcfd_gpu_mesh_create(C.byref(v), C.byref(o), C.byref(h2)) == cg.E_CONFIG_INVALID_VALUE
+
+
+def test_host_call_null_outputs(cg, gpu):
+    """Outputs of the host forward+adjoint may be NULL: the others come back
+    unchanged."""
+    ref = O.jitter(12, 11, 10, 0.25, seed=41, permute=True)
+    mesh = cg.Mesh.from_arrays(ref, order=cg.ORDER_OWNER)
+    f = O.fields(ref, 42)
+    gface = np.random.Generator(np.random.Philox(key=43)).standard_normal(ref["nFaces"])
+    full = cg.forward_adjoint(mesh, cg.PREC_F32C, f["phi"], f["phiB"], f["den"], f["u"], f["v"], f["w"], gface)
+    out = {k: np.full_like(v, np.nan) for k, v in full.items()}
+    keep = ("phiBar", "uBar", "loss")
+    rc = cg.lib().cupcfd_gpu_forward_adjoint(
+        mesh.h, cg.PREC_F32C, *[cg._p(np.ascontiguousarray(f[k])) for k in ("phi", "phiB", "den", "u", "v", "w")],
+        cg._p(gface), *[cg._p(out[k]) if k in keep else None for k in ("grad", "massFlux", "phiBar", "phiBBar", "denBar",
+                                                                      "uBar", "vBar", "wBar", "loss")])
+    assert rc == cg.E_SUCCESS, cg.last_error()
+    for k in out:
+        if k in keep:
+            assert np.array_equal(out[k], full[k]), k
+        else:
+            assert np.all(np.isnan(out[k])), k
