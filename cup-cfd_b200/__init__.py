@@ -37,7 +37,7 @@ E_FILE_MISSING = 10
 E_INVALID_FILE_FORMAT = 105
 
 RTYPE_DEFAULT, RTYPE_INLET, RTYPE_OUTLET, RTYPE_SYMP, RTYPE_WALL = range(5)
-PREC_F64, PREC_F32C = 0, 1
+PREC_F64, PREC_F32C, PREC_F32REF = 0, 1, 2
 ORDER_NATIVE, ORDER_MORTON, ORDER_OWNER, ORDER_RCM = 0, 1, 2, 3
 SIGN_REFERENCE, SIGN_SIGNED = 0, 1
 

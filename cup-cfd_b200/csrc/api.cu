@@ -231,10 +231,13 @@ PrefetchArgs prefetch_args(const cupcfd_gpu_mesh *m, int kernel = -1) {
 }
 
 
-int check_prec(const cupcfd_gpu_mesh *m, int precision) {
-    CG_RETURN_IF(precision != CUPCFD_PREC_F64 && precision != CUPCFD_PREC_F32C, CUPCFD_E_CONFIG_INVALID_VALUE,
-                 "unknown precision");
-    CG_RETURN_IF(!(m->precisions & (1 << precision)), CUPCFD_E_CONFIG_INVALID_VALUE,
+// allowRef: the gradient calls also take CUPCFD_PREC_F32REF (FP32 geometry)
+int check_prec(const cupcfd_gpu_mesh *m, int precision, bool allowRef = false) {
+    CG_RETURN_IF(precision != CUPCFD_PREC_F64 && precision != CUPCFD_PREC_F32C &&
+                     !(allowRef && precision == CUPCFD_PREC_F32REF),
+                 CUPCFD_E_CONFIG_INVALID_VALUE, "unknown precision");
+    const int geom = precision == CUPCFD_PREC_F32REF ? CUPCFD_PREC_F32C : precision;
+    CG_RETURN_IF(!(m->precisions & (1 << geom)), CUPCFD_E_CONFIG_INVALID_VALUE,
                  "the mesh was created without this precision's geometry");
     return CUPCFD_E_SUCCESS;
 }
@@ -269,6 +272,13 @@ int launch_grad_once(cupcfd_gpu_mesh *m, int precision, bool corr, bool sgn, con
         else if (!corr && sgn) k_grad_f64<false, true><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg64, m->fc64, m->cc64, pp, pb, m->vol, go, g, gc, ldc);
         else if (corr && !sgn) k_grad_f64<true, false><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg64, m->fc64, m->cc64, pp, pb, m->vol, go, g, gc, ldc);
         else k_grad_f64<true, true><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg64, m->fc64, m->cc64, pp, pb, m->vol, go, g, gc, ldc);
+    } else if (precision == CUPCFD_PREC_F32REF) {
+        const float *pp = (const float *) phi, *pb = (const float *) phiB, *go = (const float *) prev;
+        float *g = (float *) grad, *gc = (float *) gcopy;
+        if (!corr && !sgn) k_grad_f32ref<false, false><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg32, m->fc32, m->cc32, pp, pb, m->vol, go, g, gc, ldc);
+        else if (!corr && sgn) k_grad_f32ref<false, true><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg32, m->fc32, m->cc32, pp, pb, m->vol, go, g, gc, ldc);
+        else if (corr && !sgn) k_grad_f32ref<true, false><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg32, m->fc32, m->cc32, pp, pb, m->vol, go, g, gc, ldc);
+        else k_grad_f32ref<true, true><<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg32, m->fc32, m->cc32, pp, pb, m->vol, go, g, gc, ldc);
     } else {
         const float *pp = (const float *) phi, *pb = (const float *) phiB, *go = (const float *) prev;
         float *g = (float *) grad, *gc = (float *) gcopy;
@@ -449,7 +459,7 @@ extern "C" int cupcfd_gpu_dev_gradient(cupcfd_gpu_mesh *m, int32_t precision, in
                                        const void *phi, const void *phiB, void *grad, void *grad_o, void *stream) {
     clear_error();
     CG_RETURN_IF(!m, CUPCFD_E_NULL_PTR, "dev_gradient: null mesh");
-    CG_TRY(check_prec(m, precision));
+    CG_TRY(check_prec(m, precision, true));
     CG_RETURN_IF(sign_mode != CUPCFD_SIGN_REFERENCE && sign_mode != CUPCFD_SIGN_SIGNED, CUPCFD_E_CONFIG_INVALID_VALUE,
                  "unknown sign_mode");
     CG_RETURN_IF(!phi || !grad || (m->nB > 0 && !phiB), CUPCFD_E_NULL_PTR, "dev_gradient: null device pointer");
@@ -816,7 +826,7 @@ extern "C" int cupcfd_gpu_gradient_phi_gauss_dolfyn(cupcfd_gpu_mesh *m, int32_t 
     CG_RETURN_IF(stride < 3 * rs || strideo < 3 * rs || offset < 0 || offseto < 0 || offset + 3 * rs > stride ||
                      offseto + 3 * rs > strideo,
                  CUPCFD_E_CONFIG_INVALID_VALUE, "GradientPhiGaussDolfyn: bad vector stride/offset");
-    CG_TRY(check_prec(m, precision));
+    CG_TRY(check_prec(m, precision, true));
     // the reference reads phiCell[ip/in], phiBoundary[ib] and updates dPhidxCell[0..lTCells)
     // (GradientKernels.ipp:90-95,107-111,122-126); short arrays are index errors
     CG_RETURN_IF(nPhiCell < m->nC || nPhiBoundary < m->nB || nDPhidxCell < m->nC || nDPhidxoCell < 0 ||

@@ -279,6 +279,81 @@ __global__ void __launch_bounds__(256, CUPCFD_MINB_F32) k_grad_f32(int nC, SellV
 }
 
 // ---------------------------------------------------------------------------
+// Gradient with the arithmetic of the reference's T=float instantiation
+// (GradientKernels.ipp:38-136 with T = float): every product and sum rounds
+// in float, facp = 1.0 - facn and fact = 1.0 / vol are evaluated in double
+// and rounded to float (the literals are double), the correction's dot
+// product accumulates from 0 in float (EuclideanVector.ipp dotProduct).
+// vol holds the float volumes exactly (a mesh uploaded from float arrays).
+// ---------------------------------------------------------------------------
+template <bool CORR, bool SIGNED>
+__global__ void __launch_bounds__(256, CUPCFD_MINB_F32) k_grad_f32ref(int nC, SellView sv, const float4 *__restrict__ fg,
+                                                     const float4 *__restrict__ fc, const float4 *__restrict__ cc,
+                                                     const float *__restrict__ phi, const float *__restrict__ phiB,
+                                                     const double *__restrict__ vol, const float *__restrict__ go,
+                                                     float *__restrict__ g, float *__restrict__ gcopy, int64_t ldc) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nC) return;
+    int w;
+    const int2 *e = cell_entries(sv, c, w);
+    const float phic = phi[c];
+    float4 xc = make_float4(0, 0, 0, 0);
+    float gc0 = 0, gc1 = 0, gc2 = 0;
+    if (CORR) {
+        xc = cc[c];
+        gc0 = go[c]; gc1 = go[ldc + c]; gc2 = go[2 * ldc + c];
+    }
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    for (int k = 0; k < w; k++) {
+        const int2 en = ld_entry(e + 32 * k);
+        const int code = en.x;
+        if (code < 0) break;
+        const bool isN = code & 1;
+        const int o = en.y;
+        const float4 G = __ldg(fg + (code >> 1));
+        float phif;
+        if (o < 0) {
+            phif = __ldg(phiB + (-1 - o));
+        } else {
+            const float facn = G.w, facp = (float) (1.0 - (double) facn);
+            const float pv = __ldg(phi + o);
+            const float phN = isN ? phic : pv, phP = isN ? pv : phic;
+            phif = __fadd_rn(__fmul_rn(phN, facn), __fmul_rn(phP, facp));
+            if (CORR) {
+                const float4 xo = __ldg(cc + o), xf = __ldg(fc + (code >> 1));
+                const float go0 = __ldg(go + o), go1 = __ldg(go + ldc + o), go2 = __ldg(go + 2 * ldc + o);
+                const float4 xN = isN ? xc : xo, xP = isN ? xo : xc;
+                const float gN0 = isN ? gc0 : go0, gN1 = isN ? gc1 : go1, gN2 = isN ? gc2 : go2;
+                const float gP0 = isN ? go0 : gc0, gP1 = isN ? go1 : gc1, gP2 = isN ? go2 : gc2;
+                // xac = xN facn + xP facp; dPhidxac likewise; corr = xf - xac
+                const float d0 = __fsub_rn(xf.x, __fadd_rn(__fmul_rn(xN.x, facn), __fmul_rn(xP.x, facp)));
+                const float d1 = __fsub_rn(xf.y, __fadd_rn(__fmul_rn(xN.y, facn), __fmul_rn(xP.y, facp)));
+                const float d2 = __fsub_rn(xf.z, __fadd_rn(__fmul_rn(xN.z, facn), __fmul_rn(xP.z, facp)));
+                const float a0 = __fadd_rn(__fmul_rn(gN0, facn), __fmul_rn(gP0, facp));
+                const float a1 = __fadd_rn(__fmul_rn(gN1, facn), __fmul_rn(gP1, facp));
+                const float a2 = __fadd_rn(__fmul_rn(gN2, facn), __fmul_rn(gP2, facp));
+                float dot = 0.f;
+                dot = __fadd_rn(dot, __fmul_rn(a0, d0));
+                dot = __fadd_rn(dot, __fmul_rn(a1, d1));
+                dot = __fadd_rn(dot, __fmul_rn(a2, d2));
+                phif = __fadd_rn(phif, dot);
+            }
+        }
+        if (SIGNED && isN) {
+            ax = __fsub_rn(ax, __fmul_rn(phif, G.x)); ay = __fsub_rn(ay, __fmul_rn(phif, G.y));
+            az = __fsub_rn(az, __fmul_rn(phif, G.z));
+        } else {
+            ax = __fadd_rn(ax, __fmul_rn(phif, G.x)); ay = __fadd_rn(ay, __fmul_rn(phif, G.y));
+            az = __fadd_rn(az, __fmul_rn(phif, G.z));
+        }
+    }
+    const float fact = (float) (1.0 / vol[c]);
+    const float rx = __fmul_rn(ax, fact), ry = __fmul_rn(ay, fact), rz = __fmul_rn(az, fact);
+    g[c] = rx; g[ldc + c] = ry; g[2 * ldc + c] = rz;
+    if (gcopy) { gcopy[c] = rx; gcopy[ldc + c] = ry; gcopy[2 * ldc + c] = rz; }
+}
+
+// ---------------------------------------------------------------------------
 // Plain mass flux m_f = rho_f (u_f . S_f), one thread per face.
 // F64: state as four component blocks [4][ldc] (rho, u, v, w).
 // ---------------------------------------------------------------------------

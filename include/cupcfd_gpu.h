@@ -61,6 +61,9 @@ extern "C" {
 #define CUPCFD_PREC_F64 0  /* plain FP64; same operand order as the reference, bit-identical results */
 #define CUPCFD_PREC_F32C 1 /* FP32 storage and arithmetic, compensated (Dot2) cell accumulation,
                               FP64 volumes and final scaling */
+#define CUPCFD_PREC_F32REF 2 /* gradient calls only: the arithmetic of the reference's T=float
+                                instantiation (float sums in its order), bit-identical to it on a
+                                mesh uploaded from the same float arrays; uses the FP32 geometry */
 
 /* ---- internal numbering of a device mesh ---- */
 #define CUPCFD_ORDER_NATIVE 0 /* cells and faces in the reference's local order */
@@ -298,9 +301,10 @@ int cupcfd_gpu_mesh_get_numbering(const cupcfd_gpu_mesh *mesh, int32_t *cellNew2
  * components are written; the vptr slot is never touched). nGradient
  * iterations with the non-orthogonal correction of the previous iterate.
  * precision: CUPCFD_PREC_F64 (bit-identical to the reference for T=double)
- * or CUPCFD_PREC_F32C. With T=float arrays (real_size 4) neither reproduces
- * the reference's float instantiation bit for bit (that one rounds every sum
- * in float): PREC_F64 computes in FP64 and rounds each result to float once.
+ * or CUPCFD_PREC_F32C; for T=float arrays (real_size 4) CUPCFD_PREC_F32REF
+ * reproduces the reference's float instantiation bit for bit on a mesh
+ * created from the same float arrays (PREC_F64 computes in FP64 and rounds
+ * each result to float once; PREC_F32C is the compensated FP32 path).
  * sign_mode: CUPCFD_SIGN_*. */
 int cupcfd_gpu_gradient_phi_gauss_dolfyn(cupcfd_gpu_mesh *mesh, int32_t nGradient,
                                          const void *phiCell, int32_t nPhiCell,

@@ -87,12 +87,31 @@ def load_ref():
                 _ref.ref_boundary_loop5.argtypes = [C.c_void_p] * 6 + [C.c_double] + [C.c_int] * 3 + [C.c_void_p] * 2
                 _ref.ref_region_loop.argtypes = [C.c_void_p] * 3 + [C.c_double]
                 _ref.ref_boundary_chain.argtypes = [C.c_void_p] * 9 + [C.c_int, C.c_void_p]
+                _ref.ref_gradient_phi_gauss_f32.argtypes = [C.c_int] * 3 + [C.c_void_p] * 8 + [C.c_int] + [C.c_void_p] * 4
                 _ref.ref_ctx_set_uvw_geometry.argtypes = [C.c_void_p] * 3
                 _ref.ref_uvw_state.argtypes = [C.c_void_p] * 5
                 _ref.ref_uvw_face_loop1.argtypes = [C.c_void_p, C.c_double, C.c_double] + [C.c_void_p] * 19 + [C.c_int, C.c_void_p]
                 _ref.ref_uvw_region_loop1.argtypes = [C.c_void_p]
                 _ref.ref_uvw_bnds_loop1.argtypes = [C.c_void_p]
         return _ref
+
+
+def ref_gradient_f32(m, phi, phiB, nGradient):
+    """GradientPhiGaussDolfyn of the reference's T=float instantiation
+    (compiled unchanged) on mesh ``m`` with its geometry rounded to float:
+    (dPhidx, dPhidxo) as float32 [nCells, 3]."""
+    ref = load_ref()
+    assert ref is not None, "reference build absent"
+    f32 = lambda k: np.ascontiguousarray(np.asarray(m[k]).reshape(-1), np.float32)
+    i32 = lambda k: np.ascontiguousarray(m[k], np.int32)
+    nC, nF, nB = int(m["nCells"]), int(m["nFaces"]), int(m["nBnd"])
+    g, go = np.zeros((nC, 3), np.float32), np.zeros((nC, 3), np.float32)
+    a = [i32("faceCell1"), i32("faceCell2"), i32("faceBnd"), f32("faceLambda"), f32("faceNorm"), f32("faceCenter"),
+         f32("cellCenter"), f32("cellVolume")]
+    ph, pb = np.ascontiguousarray(phi, np.float32), np.ascontiguousarray(phiB, np.float32)
+    rc = ref.ref_gradient_phi_gauss_f32(nC, nF, nB, *[_p(x) for x in a], int(nGradient), _p(ph), _p(pb), _p(g), _p(go))
+    assert rc == E_SUCCESS, rc
+    return g, go
 
 
 # ---------------------------------------------------------------------------

@@ -247,6 +247,43 @@ extern "C" int ref_gradient_phi_gauss(void * p, int nGradient, double * phi, int
 	return (int) st;
 }
 
+/* GradientPhiGaussDolfyn of the reference's T=float instantiation
+ * (BenchmarkKernels.cpp:1134-1138 instantiates the kernels for float and
+ * double meshes) on a float mesh given by its arrays; dPhidx / dPhidxo get
+ * the components [3*nCells]. Only the getters the gradient calls are set. */
+typedef msh::UnstructuredMeshInterface<int, int, float, int> RefMeshF;
+extern "C" int ref_gradient_phi_gauss_f32(int nCells, int nFaces, int nBnd, const int * faceCell1,
+                                          const int * faceCell2, const int * faceBnd, const float * faceLambda,
+                                          const float * faceNorm, const float * faceCenter,
+                                          const float * cellCenter, const float * cellVolume, int nGradient,
+                                          float * phi, float * phiB, float * dPhidx, float * dPhidxo) {
+	RefMeshF mesh;
+	mesh.properties.lOCells = nCells;
+	mesh.properties.lGhCells = 0;
+	mesh.properties.lTCells = nCells;
+	mesh.properties.lFaces = nFaces;
+	mesh.properties.lBoundaries = nBnd;
+	mesh.properties.lRegions = 1;
+	mesh.a = {};
+	mesh.a.faceCell1 = faceCell1;
+	mesh.a.faceCell2 = faceCell2;
+	mesh.a.faceBoundary = faceBnd;
+	mesh.a.faceLambda = faceLambda;
+	mesh.a.faceNorm = faceNorm;
+	mesh.a.faceCenter = faceCenter;
+	mesh.a.cellCenter = cellCenter;
+	mesh.a.cellVolume = cellVolume;
+	std::vector<euc::EuclideanVector<float,3>> g(nCells), go(nCells);
+	cupcfd::error::eCodes st = cupcfd::fvm::GradientPhiGaussDolfyn(mesh, nGradient, phi, nCells, phiB, nBnd,
+	                                                               g.data(), nCells, go.data(), nCells);
+	for (int i = 0; i < nCells; i++)
+		for (int d = 0; d < 3; d++) {
+			dPhidx[3*i+d] = g[i].cmp[d];
+			dPhidxo[3*i+d] = go[i].cmp[d];
+		}
+	return (int) st;
+}
+
 /* Runs FluxMassDolfynFaceLoop `reps` times with the reference's full
  * argument list. Vector fields are xyz-interleaved [3*nCells]. The arrays
  * massFlux, su, rface, denB and the te/ed/viseff/t boundary arrays are

@@ -555,3 +555,32 @@ def test_host_call_null_outputs(cg, gpu):
             assert np.array_equal(out[k], full[k]), k
         else:
             assert np.all(np.isnan(out[k])), k
+
+
+@pytest.mark.parametrize("mk", ["struct", "jitter"])
+@pytest.mark.parametrize("ngrad", [1, 2, 3])
+def test_gradient_float_instantiation_bit_exact(cg, gpu, mk, ngrad):
+    """GradientPhiGaussDolfyn with T=float arrays and CUPCFD_PREC_F32REF
+    against the reference's own T=float instantiation (compiled unchanged),
+    on a mesh uploaded from the same float arrays: bit for bit, the
+    non-orthogonal correction of later iterations included."""
+    if O.load_ref() is None:
+        pytest.skip("reference build absent")
+    ref = O.structgen(11, 9, 8) if mk == "struct" else O.jitter(11, 9, 8, 0.25, seed=52, permute=True)
+    m32 = dict(ref)
+    for k in ("faceLambda", "faceArea", "faceNorm", "faceCenter", "cellCenter", "cellVolume"):
+        m32[k] = np.ascontiguousarray(np.asarray(ref[k]), np.float32)
+    f = O.fields(ref, 53)
+    phi, phiB = f["phi"].astype(np.float32), f["phiB"].astype(np.float32)
+    want, want_o = O.ref_gradient_f32(m32, phi, phiB, ngrad)
+    mesh = cg.Mesh.from_arrays(m32, order=cg.ORDER_OWNER)
+    n = ref["nCells"]
+    g = np.full((n, 4), np.nan, np.float32)
+    go = np.full((n, 4), np.nan, np.float32)
+    rc = cg.GradientPhiGaussDolfyn(mesh, ngrad, phi, phiB, g, go, precision=cg.PREC_F32REF)
+    assert rc == cg.E_SUCCESS, cg.last_error()
+    assert np.array_equal(g[:, 1:].view(np.int32), want.view(np.int32))
+    assert np.array_equal(go[:, 1:].view(np.int32), want_o.view(np.int32))
+    # the precision exists for the gradient calls only
+    out = cg.lib().cupcfd_gpu_forward_adjoint(mesh.h, cg.PREC_F32REF, *[None] * 16)
+    assert out in (cg.E_NULL_PTR, cg.E_CONFIG_INVALID_VALUE)
