@@ -46,7 +46,9 @@ using ecode_t = int;
 // Precision and numbering used for meshes attached implicitly. Change before
 // the first call on a mesh (or release it and attach again).
 struct Settings {
-    int precision = CUPCFD_PREC_F64;  // bit-identical to the reference for T = double
+    int precision = CUPCFD_PREC_F64;  // bit-identical to the reference for T = double (and, for the
+                                      // gradient with T = float, taken as CUPCFD_PREC_F32REF: the
+                                      // float instantiation's own arithmetic)
     int sign_mode = CUPCFD_SIGN_REFERENCE;
     int order = CUPCFD_ORDER_MORTON;
     int device = -1;
@@ -254,7 +256,11 @@ ecode_t GradientPhiGaussDolfyn(Mesh &mesh, I nGradient, T *phiCell, I nPhiCell, 
     rc = cupcfd_gpu_gradient_phi_gauss_dolfyn(m, (int32_t) nGradient, phiCell, (int32_t) nPhiCell, phiBoundary,
                                               (int32_t) nPhiBoundary, dPhidxCell, (int32_t) nDPhidxCell, v.stride,
                                               v.offset, dPhidxoCell, (int32_t) nDPhidxoCell, vo.stride, vo.offset,
-                                              (int32_t) sizeof(T), settings().precision, settings().sign_mode);
+                                              (int32_t) sizeof(T),
+                                              sizeof(T) == 4 && settings().precision == CUPCFD_PREC_F64
+                                                  ? CUPCFD_PREC_F32REF
+                                                  : settings().precision,
+                                              settings().sign_mode);
     return (ecode_t) rc;
 }
 
