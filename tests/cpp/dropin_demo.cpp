@@ -250,7 +250,38 @@ int main(int argc, char **argv) {
         if (ftan != ftRef) return fail("region force tangents differ from the reference");
     }
     cupcfd::fvm::gpu::release(mesh);
-    std::printf("OK dropin %dx%dx%d: %d cells, %d faces; gradient (nGradient 1-3), mass flux, the boundary / "
-                "region loops and the momentum loops bit-identical\n", nx, ny, nz, nC, nF);
+
+    // ---- GradientPhiGaussDolfyn on a T = float mesh (the same geometry
+    // rounded to float): the reference's float instantiation and the drop-in
+    typedef msh::UnstructuredMeshInterface<int, int, float, int> MeshF;
+    auto tof = [](const std::vector<double> &v) { return std::vector<float>(v.begin(), v.end()); };
+    std::vector<float> lamF = tof(lam), SF = tof(S), XF = tof(X), areaF = tof(area), ZF = tof(Z), CF = tof(C),
+                       volF = tof(vol), ruvwF = tof(ruvw), rdenF = tof(rden), phiF = tof(phi), phiBF = tof(phiB);
+    MeshF meshF;
+    meshF.properties = {nC, 0, nC, nF, nB, nR};
+    meshF.a = {c1.data(), c2.data(), bnd.data(), lamF.data(), SF.data(), XF.data(), areaF.data(), ZF.data(), ZF.data(),
+               CF.data(), volF.data(), breg.data(), rtype.data(), ruvwF.data(), rdenF.data()};
+    meshF.a.boundaryFace = bface.data();
+    std::vector<float> splvlF = tof(splvl), rlcF = tof(rlc), bdistF = tof(bdist), shearF(3 * nB, 0.f), ftanF(3 * nR, 0.f);
+    meshF.a.regionSplvl = splvlF.data();
+    meshF.a.faceRLencos = rlcF.data();
+    meshF.a.boundaryDistance = bdistF.data();
+    meshF.a.boundaryShear = shearF.data();
+    meshF.a.regionForceTangent = ftanF.data();
+    for (int nGrad = 1; nGrad <= 3; nGrad++) {
+        std::vector<euc::EuclideanVector<float, 3>> g1(nC), go1(nC), g2(nC), go2(nC);
+        cupcfd::error::eCodes s1 = cupcfd::fvm::GradientPhiGaussDolfyn(meshF, nGrad, phiF.data(), nC, phiBF.data(), nB,
+                                                                        g1.data(), nC, go1.data(), nC);
+        cupcfd::error::eCodes s2 = cupcfd::fvm::gpu::GradientPhiGaussDolfyn(meshF, nGrad, phiF.data(), nC, phiBF.data(),
+                                                                             nB, g2.data(), nC, go2.data(), nC);
+        if (s1 != cupcfd::error::E_SUCCESS || s2 != cupcfd::error::E_SUCCESS) return fail("float gradient status");
+        for (int i = 0; i < nC; i++)
+            for (int d = 0; d < 3; d++)
+                if (std::memcmp(&g1[i].cmp[d], &g2[i].cmp[d], 4) != 0 || std::memcmp(&go1[i].cmp[d], &go2[i].cmp[d], 4) != 0)
+                    return fail("float gradient differs from the reference's float instantiation");
+    }
+    cupcfd::fvm::gpu::release(meshF);
+    std::printf("OK dropin %dx%dx%d: %d cells, %d faces; gradient (nGradient 1-3, double and float meshes), mass "
+                "flux, the boundary / region loops and the momentum loops bit-identical\n", nx, ny, nz, nC, nF);
     return 0;
 }
