@@ -111,13 +111,18 @@ __global__ void __launch_bounds__(SEL_T) k_sel_write(SelArgs a, const double *__
 // pass 4 (one block): over the K = *total selected entries in order,
 // *out = init + v_0 + v_1 + ... (NV = 1, when out is not null) and, for the
 // regions r0 .. r0 + SEL_REGIONS - 1 below nR, regionAcc[NV r + q] +=
-// v_k[q] over region r's entries (regionAcc in/out, may be null).
+// v_k[q] over region r's entries (regionAcc in/out, may be null). Entries
+// move through shared memory in batches of SB, double-buffered: each thread
+// loads its entry of the next batch into registers before the chains of the
+// current batch run, and stores it after them, so the loads' latency hides
+// behind the chains and a batch costs one barrier.
 template <int NV>
 __global__ void __launch_bounds__(SEL_T) k_sel_sum(const int *__restrict__ total, const double *__restrict__ vals,
                                                    const int *__restrict__ regs, const double *init, double initValue,
                                                    double *out, double *regionAcc, int nR, int r0) {
-    __shared__ double sv[SEL_T * NV];
-    __shared__ int sr[SEL_T];
+    constexpr int SB = NV == 1 ? SEL_T : SEL_T / 2;  // 2 x (SB entries) fit the static shared memory
+    __shared__ double sv[2][SB * NV];
+    __shared__ int sr[2][SB];
     const int K = *total;
     const int tid = threadIdx.x;
     const bool doTotal = out != nullptr && tid == 0;
@@ -126,27 +131,44 @@ __global__ void __launch_bounds__(SEL_T) k_sel_sum(const int *__restrict__ total
     double racc[NV];
 #pragma unroll
     for (int q = 0; q < NV; q++) racc[q] = myR >= 0 ? regionAcc[NV * (size_t) myR + q] : 0.0;
-    for (int b0 = 0; b0 < K; b0 += SEL_T) {
-        const int k = b0 + tid;
-        if (k < K) {
+    if (tid < SB && tid < K) {
 #pragma unroll
-            for (int q = 0; q < NV; q++) sv[NV * tid + q] = vals[(size_t) NV * k + q];
-            sr[tid] = regs[k];
+        for (int q = 0; q < NV; q++) sv[0][NV * tid + q] = vals[(size_t) NV * tid + q];
+        sr[0][tid] = regs[tid];
+    }
+    __syncthreads();
+    int buf = 0;
+    for (int b0 = 0; b0 < K; b0 += SB) {
+        const int kn = b0 + SB + tid;
+        const bool hasNext = tid < SB && kn < K;
+        double vn[NV];
+        int rn = -1;
+        if (hasNext) {
+#pragma unroll
+            for (int q = 0; q < NV; q++) vn[q] = vals[(size_t) NV * kn + q];
+            rn = regs[kn];
         }
-        __syncthreads();
-        const int n = min(SEL_T, K - b0);
+        const int n = min(SB, K - b0);
+        const double *cv = sv[buf];
+        const int *cr = sr[buf];
         if (doTotal) {
 #pragma unroll 16
-            for (int j = 0; j < n; j++) acc = __dadd_rn(acc, sv[NV * j]);
+            for (int j = 0; j < n; j++) acc = __dadd_rn(acc, cv[NV * j]);
         } else if (myR >= 0) {
 #pragma unroll 8
             for (int j = 0; j < n; j++)
-                if (sr[j] == myR) {
+                if (cr[j] == myR) {
 #pragma unroll
-                    for (int q = 0; q < NV; q++) racc[q] = __dadd_rn(racc[q], sv[NV * j + q]);
+                    for (int q = 0; q < NV; q++) racc[q] = __dadd_rn(racc[q], cv[NV * j + q]);
                 }
         }
+        if (hasNext) {
+#pragma unroll
+            for (int q = 0; q < NV; q++) sv[buf ^ 1][NV * tid + q] = vn[q];
+            sr[buf ^ 1][tid] = rn;
+        }
         __syncthreads();
+        buf ^= 1;
     }
     if (doTotal) *out = acc;
     if (myR >= 0) {
