@@ -173,7 +173,7 @@ class Clocks:
 # CPU baseline: the reference's own kernels on a bounded sample
 # ---------------------------------------------------------------------------
 def _cpu_worker(args):
-    n, nz_local, z0, reps = args
+    n, nz_local, z0, reps, warmup = args
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import numpy as np
     import oracle as O
@@ -186,45 +186,73 @@ def _cpu_worker(args):
     kind = "reference"
     if O.load_ref() is not None:
         R = O.RefKernels(m)
+        if warmup:
+            R.gradient(f["phi"], f["phiB"], 1, reps=warmup)
+            R.flux_mass(f, reps=warmup)
         _, _, _, sg = R.gradient(f["phi"], f["phiB"], 1, reps=reps)
         _, _, sm = R.flux_mass(f, reps=reps)
         t = [a + b for a, b in zip(sg, sm)]
     else:
         kind = "port"
         t = []
-        for _ in range(reps):
+        for i in range(warmup + reps):
             t0 = time.perf_counter()
             O.gradient(m, f["phi"], f["phiB"], 1)
             O.flux_mass_face_loop(m, f)
-            t.append(time.perf_counter() - t0)
+            if i >= warmup:
+                t.append(time.perf_counter() - t0)
     return kind, m["nFaces"], t
 
 
-def cpu_baseline(n, procs, reps):
+def slab_faces(n, nz_local, top):
+    """Faces a z-slab of nz_local planes of the n^3 mesh owns: its x- and
+    y-faces and the z-faces below each of its planes (and above the top plane
+    for the topmost slab), so that the slabs' counts add up to the mesh's."""
+    return 2 * (n + 1) * n * nz_local + n * n * (nz_local + (1 if top else 0))
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_baseline(n, procs, reps, warmup=0, slabs=None):
     """Gfaces/s of the reference's forward face loops (GradientPhiGaussDolfyn +
-    FluxMassDolfynFaceLoop, FP64; the reference has no adjoint) on `procs`
-    independent processes over z-slabs of an n^3 mesh."""
+    FluxMassDolfynFaceLoop, FP64; the reference has no adjoint) on an n^3 mesh
+    cut into `slabs` z-slabs (default: one per process), each slab with one
+    ghost layer, as mpirun with NaivePartitioner cuts it. `procs` independent
+    processes run the first `procs` slabs; with procs = slabs that is the
+    whole mesh, and per repetition the slowest slab bounds the step."""
     import multiprocessing as mp
-    nC, nF, nFi, nB = face_counts(n)
-    slabs = [(n, n // procs + (1 if r < n % procs else 0)) for r in range(procs)]
-    z, jobs = 0, []
-    for _, nzl in slabs:
-        jobs.append((n, nzl, z, reps))
-        z += nzl
+    slabs = slabs or procs
+    assert 1 <= procs <= slabs <= n
+    nz = [n // slabs + (1 if r < n % slabs else 0) for r in range(slabs)]
+    z, jobs, faces = 0, [], 0
+    for r in range(procs):
+        jobs.append((n, nz[r], z, reps, warmup))
+        faces += slab_faces(n, nz[r], r == slabs - 1)
+        z += nz[r]
     if procs == 1:
         res = [_cpu_worker(jobs[0])]
     else:
         with mp.get_context("spawn").Pool(procs) as pool:
             res = pool.map(_cpu_worker, jobs)
     kind = res[0][0]
-    # per repetition, the slowest process bounds the step (all ranks run in lock step)
     per_rep = [max(r[2][i] for r in res) for i in range(reps)]
     t = statistics.median(per_rep)
-    return {"value": nF / t / 1e9, "unit": "Gfaces/s", "cores": procs, "kind": kind,
-            "sample": f"{n}^3 structured mesh ({nF} faces) in {procs} z-slab(s) with one ghost layer; "
-                      f"reference GradientPhiGaussDolfyn + FluxMassDolfynFaceLoop (FP64 forward; the "
-                      f"reference has no adjoint); median of {reps} repetitions; unique faces / slowest slab",
-            "ms_per_step": t * 1e3}
+    part = "the whole mesh" if procs == slabs else f"{procs} of the {slabs} slabs ({faces} of its faces)"
+    return {"value": faces / t / 1e9, "unit": "Gfaces/s", "cores": procs, "kind": kind, "cpu_model": cpu_model(),
+            "sample": f"{n}^3 structured mesh cut into {slabs} z-slab(s) with one ghost layer, {part}; reference "
+                      f"GradientPhiGaussDolfyn + FluxMassDolfynFaceLoop compiled unchanged (FP64 forward; the "
+                      f"reference has no adjoint); {warmup} warm-up and {reps} timed repetitions, median, "
+                      f"faces owned / slowest slab",
+            "ms_per_step": t * 1e3, "warmup": warmup, "reps": reps}
 
 
 def cpu_uvw(n, reps):
@@ -443,21 +471,38 @@ def bench_mesh_files(cg, n=128):
 # ---------------------------------------------------------------------------
 # reference arm
 # ---------------------------------------------------------------------------
+def workload_config(n, order, world):
+    """The `config` of a bench line for the n^3 workload (both arms print it)."""
+    nC, nF, nFi, nB = face_counts(n)
+    bm = bytes_model(nC, nF, nFi, nB)
+    return {"workload": f"structgen {n}^3 unit cube, FP32-compensated forward+adjoint of "
+                        f"GradientPhiGaussDolfyn + FluxMassDolfynFaceLoop",
+            "mesh": f"{n}^3", "cells": nC, "faces": nF, "interior_faces": nFi, "boundary_faces": nB,
+            "order": ["native", "morton", "owner", "rcm"][order], "parallelism": f"replicas x{world}",
+            "l2": f"inputs larger than L2 ({bm['pipeline_f32'] / 1e9:.2f} GB compulsory traffic per step)"}
+
+
 def run_reference(a):
+    """The reference's own CPU kernels (oracle/_ref: GradientKernels.ipp and
+    MassKernels.ipp compiled unchanged) on every host core, on the GPU arm's
+    mesh: the n^3 mesh in one z-slab per core, as mpirun -n P with
+    NaivePartitioner runs it (the kernels exchange nothing). The reference has
+    no adjoint, so each step is its forward face loops."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    procs = os.cpu_count() or 1
+    procs = min(os.cpu_count() or 1, a.cpu_n)
     n = a.cpu_n
-    reps = max(3, min(a.steps, 20))
+    reps = max(3, min(a.steps, 30))
+    warmup = min(a.warmup, 10)
     t0 = time.time()
-    cb = cpu_baseline(n, procs, reps)
-    nC, nF, nFi, nB = face_counts(a.n)
+    cb = cpu_baseline(n, procs, reps, warmup)
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "Gfaces/s", "n_gpus": a.gpus,
-            "steps": reps, "warmup": 0, "ms_per_step": cb["ms_per_step"], "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-            "config": {"workload": f"reference CPU face loops, bounded sample of the {a.n}^3 workload", "mesh": f"{n}^3",
-                       "cells": n ** 3},
+            "steps": reps, "warmup": warmup, "ms_per_step": cb["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": workload_config(n, a.order, a.gpus),
+            "reference_step": "GradientPhiGaussDolfyn + FluxMassDolfynFaceLoop forward, FP64 (the reference has no "
+                              "adjoint)",
             "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "Gfaces/s", "h2d_bytes_per_step": 0,
                                         "d2h_bytes_per_step": 0},
             "wall_s": round(time.time() - t0, 1)}
@@ -622,6 +667,9 @@ def run_gpu(a):
         "grad": err(grad.contiguous(), grad64),
         "massFlux": err(mflux.contiguous(), mf64),
         "phiBar": err(pbar, pbar64),
+        "phiBBar": err(pbbar, pbbar64),
+        "denBar": err(sbar[:, 0].contiguous(), sbar64[0].contiguous()),
+        "uvwBar": err(sbar[:, 1:].t().contiguous(), sbar64[1:].contiguous()),
         "stateBar": err(sbar.t().contiguous(), sbar64),
         "loss_rel": abs(float(loss.item()) - float(loss64.item())) / abs(float(loss64.item())),
     }
@@ -673,7 +721,7 @@ def run_gpu(a):
         uvw["roofline"]["traffic"] = profile_traffic().get(f"k_uvw_f64_pf@{n}")
         if rank == 0 and world == 1 and not a.no_cpu:
             try:
-                uvw["cpu_reference"] = cpu_uvw(a.cpu_n, 5)
+                uvw["cpu_reference"] = cpu_uvw(min(a.cpu_n, 64), 5)
             except Exception as ex:
                 uvw["cpu_reference"] = {"value": None, "sample": f"failed: {ex}"}
         torch.cuda.synchronize()
@@ -715,7 +763,7 @@ def run_gpu(a):
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
         try:
-            cpu = cpu_baseline(a.cpu_n, 1, a.cpu_reps)
+            cpu = cpu_baseline(a.cpu_n, 1, a.cpu_reps, 2, slabs=16)
         except Exception as ex:  # the baseline never blocks the GPU line
             cpu = {"value": None, "unit": "Gfaces/s", "cores": 1, "kind": "reference", "sample": f"failed: {ex}"}
 
@@ -724,11 +772,7 @@ def run_gpu(a):
             "metric": METRIC, "value": value, "unit": "Gfaces/s", "n_gpus": world, "steps": K, "warmup": a.warmup,
             "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic, seeded: phi~U[-1,1], u,v,w~N(0,1), rho~U[0.9,1.1], phiB~U[-1,1], g_f~N(0,1)",
-            "config": {"workload": f"structgen {n}^3 unit cube, FP32-compensated forward+adjoint of "
-                                   f"GradientPhiGaussDolfyn + FluxMassDolfynFaceLoop",
-                       "mesh": f"{n}^3", "cells": nC, "faces": nF, "interior_faces": nFi, "boundary_faces": nB,
-                       "order": ["native", "morton", "owner", "rcm"][a.order], "parallelism": f"replicas x{world}",
-                       "l2": f"inputs larger than L2 ({bm['pipeline_f32'] / 1e9:.2f} GB compulsory traffic per step)"},
+            "config": workload_config(n, a.order, world),
             "roofline": roof,
             "kernels": kernels,
             "separate_calls": separate,
@@ -765,13 +809,17 @@ def main():
     ap.add_argument("--order", type=int, default=2, help="0 native, 1 morton, 2 owner, 3 rcm")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=5)
-    ap.add_argument("--cpu-n", type=int, default=64, help="CPU baseline sample: cpu_n^3 mesh")
-    ap.add_argument("--cpu-reps", type=int, default=20)
+    ap.add_argument("--cpu-n", type=int, default=None,
+                    help="mesh of the CPU reference (default: the GPU arm's n); the reference arm cuts it into one "
+                         "z-slab per host core, the 1-core baseline times one slab of 16")
+    ap.add_argument("--cpu-reps", type=int, default=10)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-uvw", action="store_true", help="skip the momentum face loop measurement")
     ap.add_argument("--no-rows", action="store_true",
                     help="skip the boundary-loop, halo and mesh-file measurements")
     a = ap.parse_args()
+    if a.cpu_n is None:
+        a.cpu_n = a.n
     if a.warmup < 3:
         a.warmup = 3
     if a.impl == "reference":

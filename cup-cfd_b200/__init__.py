@@ -75,7 +75,7 @@ class MeshOptions(C.Structure):
 class MeshInfo(C.Structure):
     _fields_ = [(n, C.c_int32) for n in ("nCells", "nFaces", "nInteriorFaces", "nBoundaries", "nRegions",
                                          "nIncidences", "maxCellFaces", "order", "precisions", "bandwidth")] + [
-        ("deviceBytes", C.c_int64), ("stagedCtas", C.c_int32), ("stagedSmem", C.c_int32)]
+        ("deviceBytes", C.c_int64), ("tiles", C.c_int32), ("reserved", C.c_int32)]
 
 
 # exported symbols of include/cupcfd_gpu.h with their ctypes signatures
@@ -129,9 +129,9 @@ SIGNATURES = {
     "cupcfd_gpu_dev_halo_pack_fields": ([_VP, _I, _VP, _I, _VP], _I),
     "cupcfd_gpu_dev_halo_unpack_fields": ([_VP, _I, _VP, _I, _VP], _I),
     "cupcfd_gpu_dev_uvw_bnds_loop1": ([_VP, _VP], _I),
-    "cupcfd_gpu_mesh_set_fusion": ([_VP, _I], _I),
     "cupcfd_gpu_mesh_check_status": ([_VP, _VP], _I),
     "cupcfd_gpu_mesh_get_cell_face_csr": ([_VP, _VP, _I, _VP, _I], _I),
+    "cupcfd_gpu_mesh_get_incidences": ([_VP, _VP, _I, _VP, _VP, _I], _I),
     "cupcfd_gpu_mesh_get_geometry": ([_VP] * 10, _I),
     "cupcfd_gpu_mesh_get_numbering": ([_VP, _VP, _VP], _I),
     "cupcfd_gpu_gradient_phi_gauss_dolfyn": ([_VP, _I, _VP, _I, _VP, _I, _VP, _I, _I, _I, _VP, _I, _I, _I, _I, _I, _I], _I),
@@ -251,7 +251,7 @@ class Mesh:
         self.nBoundaries, self.nIncidences, self.maxCellFaces = info.nBoundaries, info.nIncidences, info.maxCellFaces
         self.order, self.precisions, self.deviceBytes = info.order, info.precisions, info.deviceBytes
         self.bandwidth = info.bandwidth
-        self.stagedCtas, self.stagedSmem = info.stagedCtas, info.stagedSmem
+        self.tiles = bool(info.tiles)
 
     @staticmethod
     def _opts(order, precisions, device):
@@ -381,10 +381,6 @@ class Mesh:
         check(lib().cupcfd_gpu_mesh_region_force_tangent(self.h, _p(a), _p(out), n_regions))
         return out
 
-    def set_fusion(self, mode):
-        """0 auto, 1 always fused, 2 never fused (forward+adjoint)."""
-        check(lib().cupcfd_gpu_mesh_set_fusion(self.h, int(mode)))
-
     def check_status(self, stream=None):
         return lib().cupcfd_gpu_mesh_check_status(self.h, _stream(stream))
 
@@ -393,6 +389,14 @@ class Mesh:
         adj = np.empty(self.nIncidences, np.int32)
         check(lib().cupcfd_gpu_mesh_get_cell_face_csr(self.h, _p(xadj), len(xadj), _p(adj), len(adj)))
         return xadj, adj
+
+    def incidences(self):
+        """The kernels' incidence lists per internal cell: (xadj, face << 1 | role, other)."""
+        xadj = np.empty(self.nCells + 1, np.int32)
+        face = np.empty(self.nIncidences, np.int32)
+        other = np.empty(self.nIncidences, np.int32)
+        check(lib().cupcfd_gpu_mesh_get_incidences(self.h, _p(xadj), len(xadj), _p(face), _p(other), len(face)))
+        return xadj, face, other
 
     def geometry(self):
         nF, nC = self.nFaces, self.nCells

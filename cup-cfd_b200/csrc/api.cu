@@ -7,7 +7,7 @@
 #include <map>
 #include <mutex>
 
-#include "kernels_fused.cuh"
+#include "kernels_pf.cuh"
 #include "strided.cuh"
 #include "perm.cuh"
 
@@ -77,77 +77,16 @@ class KernelTimer {
 };
 #define KTIMER(name, stream) KernelTimer ktimer_(name, stream)
 
-// ---------------------------------------------------------------------------
-// staged face loops (kernels_staged.cuh): stage-ring depth, stage
-// capacities, shared-memory layout and the launch conditions
-// ---------------------------------------------------------------------------
-#ifndef CUPCFD_STAGES
-#define CUPCFD_STAGES 3
-#endif
-// stage capacities per cell of a tile: incidence entries, and owned faces
-// in halves (7 -> 3.5 faces per cell; a hexahedral cell owns about 3)
-#ifndef CUPCFD_STAGED_ENT_PER_CELL
-#define CUPCFD_STAGED_ENT_PER_CELL 6
-#endif
-#ifndef CUPCFD_STAGED_FACE_HALVES
-#define CUPCFD_STAGED_FACE_HALVES 7
-#endif
-constexpr int STAGES = CUPCFD_STAGES;
-static_assert(STAGES >= 2 && STAGES <= 8, "stage ring of 2 to 8 stages");
-
-inline int round_up(int x, int k) { return (x + k - 1) / k * k; }
-
-StageLayout staged_layout(const cupcfd_gpu_mesh *m, bool forward) {
-    constexpr int T = STAGED_TILE;
-    StageLayout L{};
-    L.entCap = m->stagedEntCap;
-    L.faceCap = m->stagedFaceCap;
-    L.gfCap = L.faceCap + 8;
-    int o = 0;
-    L.ent = o; o += L.entCap * 8;
-    L.fg = o; o += L.faceCap * 16;
-    L.gf = o; o += L.gfCap * 4;
-    if (forward) {  // phi, state, vol
-        L.c0 = o; o += T * 4;
-        L.c1 = o; o += T * 16;
-        L.c2 = o; o += T * 8;
-        L.c3 = o;
-    } else {        // g (three component blocks), state
-        L.c0 = o; o += T * 4;
-        L.c1 = o; o += T * 4;
-        L.c2 = o; o += T * 4;
-        L.c3 = o; o += T * 16;
-    }
-    L.bytes = round_up(o, 128);
-    L.base = round_up(64 + 64 * STAGES, 128);
-    return L;
-}
-inline int staged_smem(const StageLayout &L) { return L.base + STAGES * L.bytes; }
-
 inline bool aligned16(const void *p) { return ((uintptr_t) p & 15u) == 0; }
 
-StagedArgs staged_args(const cupcfd_gpu_mesh *m, bool forward) {
-    StagedArgs a;
-    a.nC = m->nC;
-    a.nF = m->nF;
-    a.nTiles = m->nTiles;
-    a.desc = (const TileDesc *) m->tileDesc;
-    a.inc = m->sell.inc;
-    a.L = staged_layout(m, forward);
-    a.spinLimit = 1 << 20;
-    a.err = m->fusedCtl + 1;
-    return a;
-}
-
-// Builds the per-tile ranges (used by the L2-prefetch kernels of both
-// precisions) and sizes the FP32 shared-memory staged launches; leaves
-// m->staged false (plain kernels only) when the mesh does not allow it.
-int staged_setup(cupcfd_gpu_mesh *m, cudaStream_t st) {
-    m->staged = false;
+// Builds the per-tile ranges the L2-prefetch kernels of both precisions read
+// and the prefetch distance of each kernel; leaves m->tiles false (plain
+// kernels only) when the faces are not numbered by owner tile (the native
+// numbering keeps the reference's face order) or a slice is too wide.
+int tiles_setup(cupcfd_gpu_mesh *m, cudaStream_t st) {
+    m->tiles = false;
     if (m->nF < 1 || m->nC < 1) return CUPCFD_E_SUCCESS;
-    const char *env = std::getenv("CUPCFD_STAGED");
-    if (env && std::strcmp(env, "0") == 0) return CUPCFD_E_SUCCESS;
-    m->nTiles = (int) grid_for(m->nC, STAGED_TILE);
+    m->nTiles = (int) grid_for(m->nC, TILE_CELLS);
     TileDesc *desc;
     CG_TRY(m->alloc(&desc, (size_t) m->nTiles));
     m->tileDesc = desc;
@@ -163,45 +102,19 @@ int staged_setup(cupcfd_gpu_mesh *m, cudaStream_t st) {
     CG_CHECK_CUDA(cudaMemcpyAsync(h, aux, sizeof(h), cudaMemcpyDeviceToHost, st));
     CG_CHECK_CUDA(cudaStreamSynchronize(st));
     if (h[3] != 0 || h[2] > 255) return CUPCFD_E_SUCCESS;  // faces not by owner tile, or too wide a slice
-    // capacities: the largest tile's counts, at most the compile-time limits;
-    // CUPCFD_STAGED_ENT_CAP / CUPCFD_STAGED_FACE_CAP (per tile) lower them,
-    // which sends the overflow through the global-memory path
-    int entLim = STAGED_TILE * CUPCFD_STAGED_ENT_PER_CELL, faceLim = STAGED_TILE * CUPCFD_STAGED_FACE_HALVES / 2;
-    if (const char *e = std::getenv("CUPCFD_STAGED_ENT_CAP")) if (*e) entLim = std::min(entLim, std::atoi(e));
-    if (const char *e = std::getenv("CUPCFD_STAGED_FACE_CAP")) if (*e) faceLim = std::min(faceLim, std::atoi(e));
-    m->stagedEntCap = std::max(32, round_up(std::min(h[0], entLim), 32));
-    m->stagedFaceCap = std::max(4, round_up(std::min(h[1], faceLim), 4));
-    int dev = 0, sms = 0, optin = 0;
+    int dev = 0, sms = 0;
     CG_CHECK_CUDA(cudaGetDevice(&dev));
     CG_CHECK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    CG_CHECK_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    const void *kern[2] = {(const void *) k_fwd_f32_staged<STAGES>, (const void *) k_adj_f32_staged<STAGES>};
-    bool smemOk = (m->precisions & (1 << CUPCFD_PREC_F32C)) != 0;
-    for (int i = 0; i < 2 && smemOk; i++) {
-        int smem = staged_smem(staged_layout(m, i == 0));
-        cudaFuncAttributes fa;
-        CG_CHECK_CUDA(cudaFuncGetAttributes(&fa, kern[i]));
-        int nb = 0;
-        if (smem + (int) fa.sharedSizeBytes <= optin) {
-            CG_CHECK_CUDA(cudaFuncSetAttribute(kern[i], cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               optin - (int) fa.sharedSizeBytes));
-            CG_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern[i], STAGED_TILE, smem));
-        }
-        smemOk = nb >= 1;
-        m->stagedGrid[i] = smemOk ? std::min(m->nTiles, sms * nb) : 0;
-        m->stagedSmem[i] = smemOk ? smem : 0;
-    }
-    if (!smemOk) m->stagedGrid[0] = m->stagedGrid[1] = m->stagedSmem[0] = m->stagedSmem[1] = 0;
-    // L2-prefetch variant: prefetch one wave of resident blocks ahead (the
-    // block that will take this block's place), the best distance measured;
-    // each kernel's own wave (the gradient adjoint holds more blocks per SM
-    // than the forward: 0.345 ms at its 740-tile wave against 0.359 ms at
-    // the forward's 592 at 256^3)
+    // prefetch one wave of resident blocks ahead (the block that will take
+    // this block's place), the best distance measured; each kernel's own
+    // wave (the gradient adjoint holds more blocks per SM than the forward:
+    // 0.345 ms at its 740-tile wave against 0.359 ms at the forward's 592 at
+    // 256^3)
     const void *pfKern[6] = {(const void *) k_fwd_f32_pf, (const void *) k_adj_f32_pf, (const void *) k_fwd_f64_pf,
                              (const void *) k_adj_f64_pf, (const void *) k_fwd_madj_f32_pf, (const void *) k_gadj_f32_pf};
     for (int i = 0; i < 6; i++) {
         int nb = 0;
-        CG_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pfKern[i], STAGED_TILE, 0));
+        CG_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pfKern[i], TILE_CELLS, 0));
         m->prefetchWave[i] = sms * std::max(1, nb);
     }
     m->prefetchDist = m->prefetchWave[PF_FWD_F32];
@@ -210,12 +123,9 @@ int staged_setup(cupcfd_gpu_mesh *m, cudaStream_t st) {
             m->prefetchDist = std::max(1, std::atoi(e));
             for (int &w : m->prefetchWave) w = m->prefetchDist;
         }
-    // 1: L2 prefetch (the default, fastest measured); 2: shared-memory stages
-    // (FP32 forward/adjoint, when they fit); CUPCFD_TILE_MODE overrides
-    m->tileMode = 1;
-    if (const char *e = std::getenv("CUPCFD_TILE_MODE")) if (*e) m->tileMode = std::atoi(e);
-    if (m->tileMode == 2 && m->stagedGrid[0] == 0) m->tileMode = 1;
-    m->staged = m->tileMode != 0;
+    // CUPCFD_TILE_MODE=0 keeps the plain kernels (identical results), for comparisons
+    const char *e = std::getenv("CUPCFD_TILE_MODE");
+    m->tiles = !(e && std::strcmp(e, "0") == 0);
     return CUPCFD_E_SUCCESS;
 }
 
@@ -302,115 +212,18 @@ int mesh_post_build(cupcfd_gpu_mesh *m, cudaStream_t st) {
     k_bandwidth<<<grid_for(nC, BLK), BLK, 0, st>>>(nC, sell(m), bw);
     CG_LAUNCHED();
     CG_CHECK_CUDA(cudaMemcpyAsync(&m->bandwidth, bw, sizeof(int), cudaMemcpyDeviceToHost, st));
-    int dev = 0, sms = 0, b32 = 0, b64 = 0;
-    CG_CHECK_CUDA(cudaGetDevice(&dev));
-    CG_CHECK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    CG_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b32, k_fused_f32, FUSED_TILE, 0));
-    CG_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b64, k_fused_f64, FUSED_TILE, 0));
-    m->fusedGrid[0] = sms * b32;
-    m->fusedGrid[1] = sms * b64;
-    // per-round completion counters of the fused launch (zeroed before each
-    // launch; at most one round per tile) and the error word
-    CG_TRY(m->alloc(&m->tileFlags, (size_t) grid_for(nC, FUSED_TILE) + 1));
-    CG_TRY(m->alloc(&m->fusedCtl, 2));
-    CG_CHECK_CUDA(cudaMemsetAsync(m->fusedCtl, 0, 2 * sizeof(int), st));
-    CG_TRY(staged_setup(m, st));
+    CG_TRY(tiles_setup(m, st));
     CG_CHECK_CUDA(cudaStreamSynchronize(st));
     return CUPCFD_E_SUCCESS;
 }
 }  // namespace cupcfd_gpu
 
-namespace {
-// Tiles beyond j whose gradients the adjoint of tile j reads.
-int fused_ahead_tiles(const cupcfd_gpu_mesh *m) { return (m->bandwidth + FUSED_TILE - 1) / FUSED_TILE + 1; }
-
-// Rounds between a tile's forward and its adjoint: the adjoint of round r
-// then needs forward rounds < r only.
-int fused_lag_rounds(const cupcfd_gpu_mesh *m, int grid) {
-    return 1 + (fused_ahead_tiles(m) + grid - 1) / grid;
-}
-
-// The fused launch runs only on request (mode 1): measured on B200 at 256^3
-// it is slower than the two launches (its tile body runs about 40% slower
-// even with every wait removed, and the L2 hits it is built for did not
-// materialise), so the auto mode takes the two launches.
-bool use_fused(const cupcfd_gpu_mesh *m, int precision) {
-    return m->fusion == 1 && m->fusedGrid[precision == CUPCFD_PREC_F64] > 0;
-}
-
-int launch_fused(cupcfd_gpu_mesh *m, int precision, const void *phi, const void *phiB, const void *state,
-                 const void *gface, void *grad, void *massFlux, void *phiBar, void *phiBBar, void *stateBar,
-                 double *loss, cudaStream_t st) {
-    int nTiles = (int) grid_for(m->nC, FUSED_TILE);
-    double *part;
-    CG_TRY(scratch(m, S_LOSS, (size_t) nTiles, &part));
-    int grid = std::min(nTiles, m->fusedGrid[precision == CUPCFD_PREC_F64]);
-    FusedCtl k;
-    k.done = m->tileFlags;
-    k.err = m->fusedCtl + 1;
-    k.nTiles = nTiles;
-    k.nRounds = (nTiles + grid - 1) / grid;
-    k.aheadTiles = fused_ahead_tiles(m);
-    k.lagRounds = fused_lag_rounds(m, grid);
-    k.spinLimit = 1 << 22;
-    k.pf = prefetch_args(m);
-    k.pf.dist = grid;
-    // the prefetch reads whole 16-byte-aligned ranges of the user arrays
-    // (the gradient's component blocks too)
-    if (precision != CUPCFD_PREC_F32C || !m->staged || !aligned16(phi) || !aligned16(state) || !aligned16(gface) ||
-        !aligned16(grad) || m->nC % 4 != 0)
-        k.pf.desc = nullptr;
-    CG_CHECK_CUDA(cudaMemsetAsync(m->tileFlags, 0, sizeof(unsigned) * (size_t) k.nRounds, st));
-    int nC = m->nC;
-    SellView sv = sell(m);
-    int64_t ldc = m->nC;
-    // cooperative launch: every CTA co-resident, which the waits need
-    if (precision == CUPCFD_PREC_F64) {
-        const double4 *fg = m->fg64;
-        const double *vol = m->vol;
-        void *args[] = {&nC, &k, &sv, (void *) &fg, (void *) &phi, (void *) &phiB, (void *) &vol, (void *) &state,
-                        (void *) &gface, &grad, &massFlux, &phiBar, &phiBBar, &stateBar, &part, &ldc};
-        KTIMER("k_fused_f64", st);
-        CG_CHECK_CUDA(cudaLaunchCooperativeKernel((const void *) k_fused_f64, grid, FUSED_TILE, args, 0, st));
-    } else {
-        const float4 *fg = m->fg32;
-        const double *vol = m->vol;
-        void *args[] = {&nC, &k, &sv, (void *) &fg, (void *) &phi, (void *) &phiB, (void *) &vol, (void *) &state,
-                        (void *) &gface, &grad, &massFlux, &phiBar, &phiBBar, &stateBar, &part, &ldc};
-        KTIMER("k_fused_f32", st);
-        CG_CHECK_CUDA(cudaLaunchCooperativeKernel((const void *) k_fused_f32, grid, FUSED_TILE, args, 0, st));
-    }
-    CG_LAUNCHED();
-    if (loss) {
-        k_reduce_partials<<<1, 1024, 0, st>>>(nTiles, part, loss);
-        CG_LAUNCHED();
-    }
-    return CUPCFD_E_SUCCESS;
-}
-}  // namespace
-
-extern "C" int cupcfd_gpu_mesh_set_fusion(cupcfd_gpu_mesh *m, int32_t mode) {
-    clear_error();
-    CG_RETURN_IF(!m, CUPCFD_E_NULL_PTR, "set_fusion: null mesh");
-    CG_RETURN_IF(mode < 0 || mode > 2, CUPCFD_E_CONFIG_INVALID_VALUE, "set_fusion: mode must be 0, 1 or 2");
-    m->fusion = mode;
-    return CUPCFD_E_SUCCESS;
-}
-
 extern "C" int cupcfd_gpu_mesh_check_status(cupcfd_gpu_mesh *m, void *stream) {
     clear_error();
     CG_RETURN_IF(!m, CUPCFD_E_NULL_PTR, "check_status: null mesh");
     CG_TRY(make_device_current(m->device));
-    cudaStream_t st = as_stream(stream);
-    int h = 0;
-    CG_CHECK_CUDA(cudaMemcpyAsync(&h, m->fusedCtl + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
-    CG_CHECK_CUDA(cudaStreamSynchronize(st));
-    if (h) {
-        CG_CHECK_CUDA(cudaMemsetAsync(m->fusedCtl + 1, 0, sizeof(int), st));
-        CG_CHECK_CUDA(cudaStreamSynchronize(st));
-        set_error("a device-side wait (fused forward+adjoint or staged face loop) expired; its outputs are invalid");
-        return CUPCFD_E_ERROR;
-    }
+    CG_CHECK_CUDA(cudaStreamSynchronize(as_stream(stream)));
+    CG_CHECK_CUDA(cudaGetLastError());
     return CUPCFD_E_SUCCESS;
 }
 
@@ -544,24 +357,18 @@ extern "C" int cupcfd_gpu_dev_mass_plain_adjoint(cupcfd_gpu_mesh *m, int32_t pre
 }
 
 namespace {
-// FP32 forward: the staged kernel when the mesh and the pointers allow it
-// (identical results), else the unstaged one. One launch either way; the
-// caller checks it. part: per-256-cell loss partials, or null.
+// FP32 forward: the L2-prefetch kernel when the mesh has tile ranges and the
+// arrays start on 16-byte boundaries, else the plain one (identical results).
+// One launch either way; the caller checks it. part: per-256-cell loss
+// partials, or null.
 const char *launch_fwd_f32(const cupcfd_gpu_mesh *m, const void *phi, const void *phiB, const void *state,
                            const void *gface, void *grad, void *massFlux, double *part, cudaStream_t st) {
-    bool tiles = m->staged && aligned16(phi) && aligned16(state) && (!gface || aligned16(gface));
-    if (tiles && m->tileMode == 1) {
+    if (m->tiles && aligned16(phi) && aligned16(state) && (!gface || aligned16(gface))) {
         k_fwd_f32_pf<<<grid_for(m->nC, BLK), BLK, 0, st>>>(m->nC, sell(m), m->fg32, (const float *) phi,
                                                           (const float *) phiB, m->vol, (const float4 *) state,
                                                           (const float *) gface, (float *) grad, (float *) massFlux,
                                                           part, m->nC, prefetch_args(m, PF_FWD_F32));
         return "k_fwd_f32_pf";
-    }
-    if (tiles && m->stagedGrid[0] > 0) {
-        k_fwd_f32_staged<STAGES><<<m->stagedGrid[0], STAGED_TILE, m->stagedSmem[0], st>>>(
-            staged_args(m, true), m->fg32, (const float *) phi, (const float *) phiB, m->vol, (const float4 *) state,
-            (const float *) gface, (float *) grad, (float *) massFlux, part, m->nC);
-        return "k_fwd_f32_staged";
     }
     k_fwd_f32<BLK><<<grid_for(m->nC, BLK), BLK, 0, st>>>(m->nC, sell(m), m->fg32, (const float *) phi,
                                                          (const float *) phiB, m->vol, (const float4 *) state,
@@ -575,7 +382,7 @@ const char *launch_fwd_f32(const cupcfd_gpu_mesh *m, const void *phi, const void
 // else the plain one. Identical results.
 const char *launch_fwd_f64(const cupcfd_gpu_mesh *m, const void *phi, const void *phiB, const void *state,
                            const void *gface, void *grad, void *massFlux, double *part, cudaStream_t st) {
-    if (m->staged && m->tileMode == 1 && aligned16(phi) && aligned16(state) && (!gface || aligned16(gface)) &&
+    if (m->tiles && aligned16(phi) && aligned16(state) && (!gface || aligned16(gface)) &&
         m->nC % 2 == 0) {
         k_fwd_f64_pf<<<grid_for(m->nC, BLK), BLK, 0, st>>>(m->nC, sell(m), m->fg64, (const double *) phi,
                                                           (const double *) phiB, m->vol, (const double *) state,
@@ -629,7 +436,7 @@ extern "C" int cupcfd_gpu_dev_adjoint(cupcfd_gpu_mesh *m, int32_t precision, con
     cudaStream_t st = as_stream(stream);
     unsigned grid = grid_for(m->nC, BLK);
     KernelTimer kt(nullptr, st);
-    if (precision == CUPCFD_PREC_F64 && m->staged && m->tileMode == 1 && aligned16(grad) && aligned16(state) &&
+    if (precision == CUPCFD_PREC_F64 && m->tiles && aligned16(grad) && aligned16(state) &&
         aligned16(gface) && m->nC % 2 == 0) {
         kt.set_name("k_adj_f64_pf");
         k_adj_f64_pf<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg64, (const double *) grad, 2.0, (const double *) state,
@@ -639,17 +446,11 @@ extern "C" int cupcfd_gpu_dev_adjoint(cupcfd_gpu_mesh *m, int32_t precision, con
         kt.set_name("k_adj_f64");
         k_adj_f64<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg64, (const double *) grad, 2.0, (const double *) state,
                                         (const double *) gface, (double *) phiBar, (double *) phiBBar, (double *) stateBar, m->nC);
-    } else if (m->staged && m->tileMode == 1 && aligned16(grad) && aligned16(state) && aligned16(gface) && m->nC % 4 == 0) {
+    } else if (m->tiles && aligned16(grad) && aligned16(state) && aligned16(gface) && m->nC % 4 == 0) {
         kt.set_name("k_adj_f32_pf");
         k_adj_f32_pf<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg32, (const float *) grad, 2.f, (const float4 *) state,
                                            (const float *) gface, (float *) phiBar, (float *) phiBBar,
                                            (float4 *) stateBar, m->nC, prefetch_args(m, PF_ADJ_F32));
-    } else if (m->staged && m->stagedGrid[1] > 0 && aligned16(grad) && aligned16(state) && aligned16(gface) &&
-               m->nC % 4 == 0) {
-        kt.set_name("k_adj_f32_staged");
-        k_adj_f32_staged<STAGES><<<m->stagedGrid[1], STAGED_TILE, m->stagedSmem[1], st>>>(
-            staged_args(m, false), m->fg32, (const float *) grad, 2.f, (const float4 *) state, (const float *) gface,
-            (float *) phiBar, (float *) phiBBar, (float4 *) stateBar, m->nC);
     } else {
         kt.set_name("k_adj_f32");
         k_adj_f32<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg32, (const float *) grad, 2.f, (const float4 *) state,
@@ -667,15 +468,7 @@ extern "C" int cupcfd_gpu_dev_forward_adjoint(cupcfd_gpu_mesh *m, int32_t precis
     double *lp = loss;
     if (!lp) CG_TRY(scratch(m, S_NORM, 1, &lp));
     CG_TRY(check_prec(m, precision));
-    if (use_fused(m, precision)) {
-        CG_RETURN_IF(!phi || !state || !grad || !massFlux || !phiBar || !stateBar || (m->nB > 0 && (!phiB || !phiBBar)),
-                     CUPCFD_E_NULL_PTR, "dev_forward_adjoint: null argument");
-        CG_TRY(check_align(precision, {phi, phiB, gface, grad, massFlux, phiBar, phiBBar}, {state, stateBar}));
-        CG_RETURN_IF(((uintptr_t) lp) % 8 != 0, CUPCFD_E_CONFIG_INVALID_VALUE, "dev_forward_adjoint: loss not 8-byte aligned");
-        return launch_fused(m, precision, phi, phiB, state, gface, grad, massFlux, phiBar, phiBBar, stateBar, lp,
-                            as_stream(stream));
-    }
-    if (precision == CUPCFD_PREC_F32C && m->staged && m->tileMode == 1 && aligned16(phi) && aligned16(state) &&
+    if (precision == CUPCFD_PREC_F32C && m->tiles && aligned16(phi) && aligned16(state) &&
         aligned16(gface) && aligned16(grad) && aligned16(stateBar) && m->nC % 4 == 0) {
         // forward with the mass-flux adjoint, then the gradient adjoint: the
         // state and gface stream through one pass only
@@ -1038,9 +831,7 @@ int launch_adj_part(const cupcfd_gpu_mesh *m, bool f64, const void *g, double hs
 //                 e2 the state adjoint and the loss
 // The kernels are the device calls' (gradient, mass flux, the two parts of
 // the adjoint, and the loss from the stored gradient and mass fluxes), whose
-// results equal cupcfd_gpu_dev_forward_adjoint's bit for bit. With the fused forward+adjoint
-// selected (cupcfd_gpu_mesh_set_fusion 1) the call runs that launch after all
-// inputs are in and copies everything back after it.
+// results equal cupcfd_gpu_dev_forward_adjoint's bit for bit.
 extern "C" int cupcfd_gpu_forward_adjoint(cupcfd_gpu_mesh *m, int32_t precision, const double *phi, const double *phiB,
                                           const double *den, const double *u, const double *v, const double *w,
                                           const double *gface, double *grad, double *massFlux, double *phiBar,
@@ -1057,9 +848,8 @@ extern "C" int cupcfd_gpu_forward_adjoint(cupcfd_gpu_mesh *m, int32_t precision,
     unsigned gC = grid_for(nC, BLK), gF = grid_for(nF, BLK);
     bool f64 = precision == CUPCFD_PREC_F64;
     size_t es = f64 ? 8 : 4;
-    bool pipe = !use_fused(m, precision);
-    if (pipe) CG_TRY(pipe_init(m));
-    cudaStream_t so = pipe ? m->outStream : st;
+    CG_TRY(pipe_init(m));
+    cudaStream_t so = m->outStream;
     // host -> device staging (reference numbering, FP64)
     double *in;
     void *phiI, *phibI, *stI, *gI, *gradI, *mfI, *pbI, *pbbI, *sbI;
@@ -1097,11 +887,9 @@ extern "C" int cupcfd_gpu_forward_adjoint(cupcfd_gpu_mesh *m, int32_t precision,
         }
     }
     CG_LAUNCHED();
-    if (pipe) {
-        CG_TRY(launch_grad_once(m, precision, false, false, phiI, phibI, nullptr, gradI, nullptr, st));
-        CG_TRY(launch_adj_part(m, f64, gradI, 2.0, nullptr, nullptr, pbI, pbbI, nullptr, st));
-        CG_CHECK_CUDA(cudaEventRecord(m->pipeEv[0], st));
-    }
+    CG_TRY(launch_grad_once(m, precision, false, false, phiI, phibI, nullptr, gradI, nullptr, st));
+    CG_TRY(launch_adj_part(m, f64, gradI, 2.0, nullptr, nullptr, pbI, pbbI, nullptr, st));
+    CG_CHECK_CUDA(cudaEventRecord(m->pipeEv[0], st));
     // state in, mass flux
     CG_CHECK_CUDA(cudaMemcpyAsync(hR, den, 8 * (size_t) nC, cudaMemcpyHostToDevice, st));
     CG_CHECK_CUDA(cudaMemcpyAsync(hU, u, 8 * (size_t) nC, cudaMemcpyHostToDevice, st));
@@ -1110,33 +898,27 @@ extern "C" int cupcfd_gpu_forward_adjoint(cupcfd_gpu_mesh *m, int32_t precision,
     if (f64) k_gather<double, double><<<gC, BLK, 0, st>>>(nC, 4, m->cellN2O, hR, nC, (double *) stI, ldc);
     else k_state_to_f4<<<gC, BLK, 0, st>>>(nC, m->cellN2O, hR, hU, hV, hW, (float4 *) stI);
     CG_LAUNCHED();
-    if (pipe) {
-        CG_TRY(cupcfd_gpu_dev_mass_plain(m, precision, stI, mfI, st));
-        CG_CHECK_CUDA(cudaEventRecord(m->pipeEv[1], st));
-    }
+    CG_TRY(cupcfd_gpu_dev_mass_plain(m, precision, stI, mfI, st));
+    CG_CHECK_CUDA(cudaEventRecord(m->pipeEv[1], st));
     // gface in, loss and adjoint
     CG_CHECK_CUDA(cudaMemcpyAsync(hG, gface, 8 * (size_t) nF, cudaMemcpyHostToDevice, st));
     if (f64) k_gather<double, double><<<gF, BLK, 0, st>>>(nF, 1, m->faceN2O, hG, 0, (double *) gI, 0);
     else k_gather<double, float><<<gF, BLK, 0, st>>>(nF, 1, m->faceN2O, hG, 0, (float *) gI, 0);
     CG_LAUNCHED();
-    if (pipe) {
-        if (f64)
-            k_loss<double><<<gC, 256, 0, st>>>(nC, sell(m), (const double *) gI, (const double *) mfI,
-                                               (const double *) gradI, m->vol, part, ldc);
-        else
-            k_loss<float><<<gC, 256, 0, st>>>(nC, sell(m), (const float *) gI, (const float *) mfI,
-                                              (const float *) gradI, m->vol, part, ldc);
-        CG_LAUNCHED();
-        k_reduce_partials<<<1, 1024, 0, st>>>((int) gC, part, dloss);
-        CG_LAUNCHED();
-        CG_TRY(launch_adj_part(m, f64, nullptr, 0.0, stI, gI, nullptr, nullptr, sbI, st));
-        CG_CHECK_CUDA(cudaEventRecord(m->pipeEv[2], st));
-    } else {
-        CG_TRY(cupcfd_gpu_dev_forward_adjoint(m, precision, phiI, phibI, stI, gI, gradI, mfI, pbI, pbbI, sbI, dloss, st));
-    }
+    if (f64)
+        k_loss<double><<<gC, 256, 0, st>>>(nC, sell(m), (const double *) gI, (const double *) mfI,
+                                           (const double *) gradI, m->vol, part, ldc);
+    else
+        k_loss<float><<<gC, 256, 0, st>>>(nC, sell(m), (const float *) gI, (const float *) mfI,
+                                          (const float *) gradI, m->vol, part, ldc);
+    CG_LAUNCHED();
+    k_reduce_partials<<<1, 1024, 0, st>>>((int) gC, part, dloss);
+    CG_LAUNCHED();
+    CG_TRY(launch_adj_part(m, f64, nullptr, 0.0, stI, gI, nullptr, nullptr, sbI, st));
+    CG_CHECK_CUDA(cudaEventRecord(m->pipeEv[2], st));
 
     // back to reference numbering (FP64) and to the host, on the copy stream
-    if (pipe) CG_CHECK_CUDA(cudaStreamWaitEvent(so, m->pipeEv[0], 0));
+    CG_CHECK_CUDA(cudaStreamWaitEvent(so, m->pipeEv[0], 0));
     if (f64) {
         k_blocks_to_aos<double, double><<<gC, BLK, 0, so>>>(nC, 3, m->cellO2N, (const double *) gradI, ldc, oG);
         k_gather<double, double><<<gC, BLK, 0, so>>>(nC, 1, m->cellO2N, (const double *) pbI, 0, oPb, 0);
@@ -1154,12 +936,12 @@ extern "C" int cupcfd_gpu_forward_adjoint(cupcfd_gpu_mesh *m, int32_t precision,
     if (grad) CG_CHECK_CUDA(cudaMemcpyAsync(grad, oG, 24 * (size_t) nC, cudaMemcpyDeviceToHost, so));
     if (phiBar) CG_CHECK_CUDA(cudaMemcpyAsync(phiBar, oPb, 8 * (size_t) nC, cudaMemcpyDeviceToHost, so));
     if (phiBBar && nB > 0) CG_CHECK_CUDA(cudaMemcpyAsync(phiBBar, oPbb, 8 * (size_t) nB, cudaMemcpyDeviceToHost, so));
-    if (pipe) CG_CHECK_CUDA(cudaStreamWaitEvent(so, m->pipeEv[1], 0));
+    CG_CHECK_CUDA(cudaStreamWaitEvent(so, m->pipeEv[1], 0));
     if (f64) k_faces_to_ref<double><<<gF, BLK, 0, so>>>(nF, m->faceO2N, m->faceCells, (const double *) mfI, oMf, 1);
     else k_faces_to_ref<float><<<gF, BLK, 0, so>>>(nF, m->faceO2N, m->faceCells, (const float *) mfI, oMf, 1);
     CG_LAUNCHED();
     if (massFlux) CG_CHECK_CUDA(cudaMemcpyAsync(massFlux, oMf, 8 * (size_t) nF, cudaMemcpyDeviceToHost, so));
-    if (pipe) CG_CHECK_CUDA(cudaStreamWaitEvent(so, m->pipeEv[2], 0));
+    CG_CHECK_CUDA(cudaStreamWaitEvent(so, m->pipeEv[2], 0));
     if (f64) k_gather<double, double><<<gC, BLK, 0, so>>>(nC, 4, m->cellO2N, (const double *) sbI, ldc, oR, nC);
     else k_f4_to_ref<<<gC, BLK, 0, so>>>(nC, m->cellO2N, (const float4 *) sbI, oR, oU, oV, oW);
     CG_LAUNCHED();
@@ -1169,8 +951,8 @@ extern "C" int cupcfd_gpu_forward_adjoint(cupcfd_gpu_mesh *m, int32_t precision,
     if (wBar) CG_CHECK_CUDA(cudaMemcpyAsync(wBar, oW, 8 * (size_t) nC, cudaMemcpyDeviceToHost, so));
     if (loss) CG_CHECK_CUDA(cudaMemcpyAsync(loss, dloss, 8, cudaMemcpyDeviceToHost, so));
     CG_CHECK_CUDA(cudaStreamSynchronize(so));
-    if (pipe) CG_CHECK_CUDA(cudaStreamSynchronize(st));
-    return cupcfd_gpu_mesh_check_status(m, st);
+    CG_CHECK_CUDA(cudaStreamSynchronize(st));
+    return CUPCFD_E_SUCCESS;
 }
 
 // ===========================================================================
@@ -1200,8 +982,24 @@ namespace {
 constexpr int NOALLOC_MAX_PARTIALS = 65536;
 constexpr int NOALLOC_MAX_DEVICES = 64;
 static __device__ __align__(256) double g_noalloc_partials[NOALLOC_MAX_PARTIALS];
-static double *g_noalloc_ptr[NOALLOC_MAX_DEVICES];
-static std::atomic<int> g_noalloc_ready[NOALLOC_MAX_DEVICES];
+// Per device, the array's device address once looked up (null until then).
+// The pointer is its own ready flag: threads that race on a device's first
+// call may each look the address up, and they store the same value.
+static std::atomic<double *> g_noalloc_ptr[NOALLOC_MAX_DEVICES];
+
+// Makes `dev` current for the lifetime of the guard and gives the caller's
+// device back afterwards (cudaGetDevice / cudaSetDevice allocate nothing).
+struct DeviceGuard {
+    int prev = -1;
+    bool ok = false;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) return;
+        ok = prev == dev || cudaSetDevice(dev) == cudaSuccess;
+    }
+    ~DeviceGuard() {
+        if (ok && prev >= 0) cudaSetDevice(prev);
+    }
+};
 }  // namespace
 
 extern "C" int cupcfd_gpu_dev_forward_noalloc(cupcfd_gpu_mesh *m, int32_t precision, const void *phi,
@@ -1221,17 +1019,18 @@ extern "C" int cupcfd_gpu_dev_forward_noalloc(cupcfd_gpu_mesh *m, int32_t precis
     if (loss && grid > (unsigned) NOALLOC_MAX_PARTIALS) return CUPCFD_E_ARRAY_SIZE_MISMATCH;
     int dev = m->device;
     if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return CUPCFD_E_NOT_IMPLEMENTED;
-    if (cudaSetDevice(dev) != cudaSuccess) return CUPCFD_E_ERROR;
+    DeviceGuard guard(dev);
+    if (!guard.ok) return CUPCFD_E_ERROR;
     double *part = nullptr;
     if (loss) {
         // one-time set-up per device, with that device current
-        if (g_noalloc_ready[dev].load(std::memory_order_acquire) == 0) {
+        part = g_noalloc_ptr[dev].load(std::memory_order_acquire);
+        if (!part) {
             void *p = nullptr;
             if (cudaGetSymbolAddress(&p, g_noalloc_partials) != cudaSuccess) return CUPCFD_E_ERROR;
-            g_noalloc_ptr[dev] = (double *) p;
-            g_noalloc_ready[dev].store(1, std::memory_order_release);
+            part = (double *) p;
+            g_noalloc_ptr[dev].store(part, std::memory_order_release);
         }
-        part = g_noalloc_ptr[dev];
     }
     cudaStream_t st = as_stream(stream);
     if (precision == CUPCFD_PREC_F64)

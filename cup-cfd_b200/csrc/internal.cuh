@@ -136,24 +136,13 @@ struct cupcfd_gpu_mesh {
     int regionFTcap = 0;
     int *uvwCarry = nullptr;
     bool uvwCarryValid = false;
-    // wavefront-fused forward+adjoint: numbering bandwidth (largest
-    // |c - neighbour|), per-tile publication flags, work counter + error word
-    int bandwidth = 0;
-    int fusion = 0;               // 0 auto, 1 always, 2 never
-    unsigned *tileFlags = nullptr; // per-CTA progress counters of the fused launch
-    int *fusedCtl = nullptr;      // [1] error bits ([0] unused)
-    int fusedGrid[2] = {0, 0};    // resident CTAs of the FP32 / FP64 fused kernels
-    // staged face loops: per-tile ranges (TileDesc[nTiles], 256-cell tiles),
-    // the largest tile's entry and owned-face counts, resident CTAs of the
-    // FP32 staged forward / adjoint and their dynamic shared memory
+    int bandwidth = 0;            // numbering bandwidth: largest |c - neighbour|
+    // L2-prefetch face loops: per-tile ranges (TileDesc[nTiles], 256-cell
+    // tiles); tiles false when the faces are not numbered by owner tile
     void *tileDesc = nullptr;
     int nTiles = 0;
-    bool staged = false;
-    int stagedEntCap = 0, stagedFaceCap = 0;  // stage capacities (entries, faces per tile)
-    int stagedGrid[2] = {0, 0};
-    int stagedSmem[2] = {0, 0};
-    int tileMode = 0;             // 0 unstaged, 1 L2 prefetch, 2 shared-memory stages
-    int prefetchDist = 0;         // tiles ahead for the L2 prefetch variant
+    bool tiles = false;
+    int prefetchDist = 0;         // tiles ahead for the L2 prefetch
     int prefetchWave[6] = {0, 0, 0, 0, 0, 0};  // per prefetch kernel (PfKernel in api.cu): one wave of its blocks
 
     std::vector<cupcfd_gpu::DevBuf> owned;  // everything above, freed by destroy

@@ -34,16 +34,32 @@ namespace cupcfd_gpu {
 // with Knuth's TwoSum error term, and the errors are accumulated separately.
 // The result is as accurate as if computed in twice the working precision.
 // ---------------------------------------------------------------------------
+#ifndef CUPCFD_COMP
+#define CUPCFD_COMP 2
+#endif
 struct Acc2 {
     float s = 0.f, e = 0.f;
     __device__ __forceinline__ void add_prod(float a, float b) {
         float p = __fmul_rn(a, b);
+#if CUPCFD_COMP == 2
         float ep = __fmaf_rn(a, b, -p);
         float t = __fadd_rn(s, p);
         float bp = __fsub_rn(t, s);
         float es = __fadd_rn(__fsub_rn(s, __fsub_rn(t, bp)), __fsub_rn(p, bp));
         s = t;
         e = __fadd_rn(e, __fadd_rn(ep, es));
+#elif CUPCFD_COMP == 1
+        float t = __fadd_rn(s, p);
+        float bp = __fsub_rn(t, s);
+        float es = __fadd_rn(__fsub_rn(s, __fsub_rn(t, bp)), __fsub_rn(p, bp));
+        s = t;
+        e = __fadd_rn(e, es);
+#else
+        float y = __fadd_rn(p, e);
+        float t = __fadd_rn(s, y);
+        e = __fadd_rn(__fsub_rn(s, t), y);
+        s = t;
+#endif
     }
     __device__ __forceinline__ void sub_prod(float a, float b) { add_prod(-a, b); }
     __device__ __forceinline__ double value() const { return (double) s + (double) e; }
@@ -59,12 +75,25 @@ struct Acc2x2 {
     __device__ __forceinline__ void add_prod(float2 a, float2 b) {
         const float2 m1 = make_float2(-1.f, -1.f);
         float2 p = __fmul2_rn(a, b);
+#if CUPCFD_COMP == 2
         float2 ep = __ffma2_rn(a, b, __fmul2_rn(p, m1));
         float2 t = __fadd2_rn(s, p);
         float2 bp = __ffma2_rn(s, m1, t);
         float2 es = __fadd2_rn(__ffma2_rn(__ffma2_rn(bp, m1, t), m1, s), __ffma2_rn(bp, m1, p));
         s = t;
         e = __fadd2_rn(e, __fadd2_rn(ep, es));
+#elif CUPCFD_COMP == 1
+        float2 t = __fadd2_rn(s, p);
+        float2 bp = __ffma2_rn(s, m1, t);
+        float2 es = __fadd2_rn(__ffma2_rn(__ffma2_rn(bp, m1, t), m1, s), __ffma2_rn(bp, m1, p));
+        s = t;
+        e = __fadd2_rn(e, es);
+#else
+        float2 y = __fadd2_rn(p, e);
+        float2 t = __fadd2_rn(s, y);
+        e = __fadd2_rn(__ffma2_rn(t, m1, s), y);
+        s = t;
+#endif
     }
     __device__ __forceinline__ void add_x(float a, float b) {
         Acc2 h;

@@ -312,9 +312,9 @@ __global__ void __launch_bounds__(256, UVW_CELL_MINB) k_uvw_f64(const __grid_con
 // fluxes, and its cells' entries in the twenty cell arrays the loop reads.
 // Needs the owner-sorted face order, 256-thread blocks and 16-byte aligned
 // arrays. 2.13 ms at 256^3 against 2.21 ms without the prefetch.
-__global__ void __launch_bounds__(STAGED_TILE, UVW_CELL_MINB) k_uvw_f64_pf(const __grid_constant__ UvwArgs a,
+__global__ void __launch_bounds__(TILE_CELLS, UVW_CELL_MINB) k_uvw_f64_pf(const __grid_constant__ UvwArgs a,
                                                                           PrefetchArgs pf) {
-    constexpr int T = STAGED_TILE;
+    constexpr int T = TILE_CELLS;
     const int c = blockIdx.x * T + threadIdx.x;
     const int tp = blockIdx.x + pf.dist;
     const bool lead = threadIdx.x == T - 32 && tp < pf.nTiles;

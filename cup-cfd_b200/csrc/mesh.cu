@@ -6,6 +6,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <climits>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
@@ -226,7 +227,7 @@ __global__ void k_slice_width(int nC, int nSlices, const int *__restrict__ cellN
         d = xadj[o + 1] - xadj[o];
     }
     for (int k = 16; k > 0; k >>= 1) d = max(d, __shfl_xor_sync(0xffffffffu, d, k));
-    if (lane == 0) words[s] = 32 * d;
+    if (lane == 0) words[s] = d > INT_MAX / 32 ? INT_MAX : 32 * d;  // an overfull slice is refused by the host
 }
 
 __global__ void k_fill_sell(int nC, const int *__restrict__ cellN2O, const int *__restrict__ cellO2N,
@@ -643,6 +644,18 @@ int build_mesh_from_source(cupcfd_gpu_mesh *m, const Source &s, const cupcfd_mes
         CG_CHECK_CUDA(cudaMemsetAsync(words + nSlices, 0, sizeof(int), st));
         k_slice_width<<<grid_for((int64_t) nSlices * 32, B), B, 0, st>>>(nC, nSlices, m->cellN2O, m->refXadj, words);
         CG_LAUNCHED();
+        {
+            // The slice pointers are int: padded slices of wide cells can hold
+            // more entries in all than an int counts even below 2^30 faces, so
+            // the total is summed in 64 bits first and such meshes are refused.
+            std::vector<int> hw((size_t) nSlices);
+            CG_CHECK_CUDA(cudaMemcpyAsync(hw.data(), words, sizeof(int) * (size_t) nSlices, cudaMemcpyDeviceToHost, st));
+            CG_CHECK_CUDA(cudaStreamSynchronize(st));
+            int64_t total64 = 0;
+            for (int w : hw) total64 += w;
+            CG_RETURN_IF(total64 > (int64_t) INT_MAX, CUPCFD_E_NOT_IMPLEMENTED,
+                         "mesh: padded incidence lists exceed 2^31 - 1 entries");
+        }
         CG_TRY(m->alloc(&m->sell.slicePtr, (size_t) nSlices + 1));
         CG_TRY(exclusive_scan(words, m->sell.slicePtr, nSlices + 1, st));
         int total = 0;
@@ -899,8 +912,8 @@ extern "C" int cupcfd_gpu_mesh_get_info(const cupcfd_gpu_mesh *m, cupcfd_mesh_in
     info->precisions = m->precisions;
     info->bandwidth = m->bandwidth;
     info->deviceBytes = m->bytes;
-    info->stagedCtas = m->staged ? m->stagedGrid[0] : 0;
-    info->stagedSmem = m->staged ? m->stagedSmem[0] : 0;
+    info->tiles = m->tiles ? 1 : 0;
+    info->reserved = 0;
     return CUPCFD_E_SUCCESS;
 }
 
@@ -971,6 +984,36 @@ extern "C" int cupcfd_gpu_mesh_get_cell_face_csr(const cupcfd_gpu_mesh *m, int32
     CG_CHECK_CUDA(cudaMemcpyAsync(xadj, m->refXadj, sizeof(int) * nXAdj, cudaMemcpyDeviceToHost, m->stream));
     CG_CHECK_CUDA(cudaMemcpyAsync(adj, m->refAdj, sizeof(int) * (size_t) nAdj, cudaMemcpyDeviceToHost, m->stream));
     CG_CHECK_CUDA(cudaStreamSynchronize(m->stream));
+    return CUPCFD_E_SUCCESS;
+}
+
+extern "C" int cupcfd_gpu_mesh_get_incidences(const cupcfd_gpu_mesh *m, int32_t *xadj, int32_t nXAdj, int32_t *face,
+                                              int32_t *other, int32_t nInc) {
+    clear_error();
+    CG_RETURN_IF(!m || !xadj || !face || !other, CUPCFD_E_NULL_PTR, "get_incidences: null argument");
+    CG_RETURN_IF(nXAdj != m->nC + 1 || nInc != m->nInc, CUPCFD_E_ARRAY_SIZE_MISMATCH, "get_incidences: size mismatch");
+    CG_TRY(make_device_current(m->device));
+    const int nS = m->sell.nSlices;
+    std::vector<int> sp((size_t) nS + 1);
+    std::vector<int2> inc((size_t) m->sell.nEntries);
+    CG_CHECK_CUDA(cudaMemcpyAsync(sp.data(), m->sell.slicePtr, sizeof(int) * sp.size(), cudaMemcpyDeviceToHost, m->stream));
+    CG_CHECK_CUDA(cudaMemcpyAsync(inc.data(), m->sell.inc, sizeof(int2) * inc.size(), cudaMemcpyDeviceToHost, m->stream));
+    CG_CHECK_CUDA(cudaStreamSynchronize(m->stream));
+    int64_t k = 0;
+    xadj[0] = 0;
+    for (int c = 0; c < m->nC; c++) {
+        const int s = c >> 5, lane = c & 31, w = (sp[s + 1] - sp[s]) >> 5;
+        for (int j = 0; j < w; j++) {
+            const int2 e = inc[(size_t) sp[s] + 32 * (size_t) j + lane];
+            if (e.x < 0) break;  // padding follows a cell's real entries
+            CG_RETURN_IF(k >= nInc, CUPCFD_E_ERROR, "get_incidences: more entries than incidences");
+            face[k] = e.x;
+            other[k] = e.y;
+            k++;
+        }
+        xadj[c + 1] = (int32_t) k;
+    }
+    CG_RETURN_IF(k != nInc, CUPCFD_E_ERROR, "get_incidences: fewer entries than incidences");
     return CUPCFD_E_SUCCESS;
 }
 

@@ -16,7 +16,7 @@
 
 namespace cupcfd_gpu {
 
-constexpr int STAGED_TILE = 256;
+constexpr int TILE_CELLS = 256;
 
 // Per-tile ranges, built once per mesh.
 struct TileDesc {
@@ -69,7 +69,7 @@ __device__ __forceinline__ void prefetch_tile(const PrefetchArgs &p, int t, cons
         if (gfB > p.nF) gfB = fe & ~(PER16 - 1);
         if (gfB > gfA) bulk_prefetch_l2(gface + gfA, (unsigned) (gfB - gfA) * (unsigned) sizeof(TG));
     }
-    if ((long long) (t + 1) * STAGED_TILE <= (long long) p.nC)
+    if ((long long) (t + 1) * TILE_CELLS <= (long long) p.nC)
         for (int i = 0; i < NCELL; i++)
             bulk_prefetch_l2(static_cast<const unsigned char *>(cellSrc[i]) + (size_t) t * cellBytes[i],
                              (unsigned) cellBytes[i]);

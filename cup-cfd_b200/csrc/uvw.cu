@@ -90,7 +90,7 @@ int prefetch_wave(int device) {
     if (it != wave.end()) return it->second;
     int sms = 148, blocks = UVW_CELL_MINB;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_uvw_f64_pf, STAGED_TILE, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_uvw_f64_pf, TILE_CELLS, 0);
     int d = std::max(1, sms * std::max(1, blocks));
     if (const char *e = std::getenv("CUPCFD_PREFETCH_DIST")) if (*e) d = std::max(1, std::atoi(e));
     wave[device] = d;
@@ -123,7 +123,7 @@ int run_face_loop(cupcfd_gpu_mesh *m, double gammaBlend, double small, const dou
     // the L2-prefetch form when the mesh has tile ranges and every streamed
     // array starts on a 16-byte boundary (same arithmetic, same bits)
     auto a16 = [](const void *p) { return ((uintptr_t) p & 15u) == 0; };
-    const bool pfOk = m->staged && m->tileMode == 1 && m->tileDesc && a16(u) && a16(v) && a16(w) && a16(visC) &&
+    const bool pfOk = m->tiles && m->tileDesc && a16(u) && a16(v) && a16(w) && a16(visC) &&
                       a16(su) && a16(sv) && a16(sw) && a16(au) && a16(av) && a16(aw) && a16(grads) &&
                       (ldg % 2) == 0 && a16(massFlux) && !prefetch_disabled();
     if (pfOk) {
@@ -134,7 +134,7 @@ int run_face_loop(cupcfd_gpu_mesh *m, double gammaBlend, double small, const dou
         pf.nF = m->nF;
         pf.nTiles = m->nTiles;
         pf.dist = prefetch_wave(m->device);
-        k_uvw_f64_pf<<<grid_for(m->nC, STAGED_TILE), STAGED_TILE, 0, st>>>(a, pf);
+        k_uvw_f64_pf<<<grid_for(m->nC, TILE_CELLS), TILE_CELLS, 0, st>>>(a, pf);
     } else {
         k_uvw_f64<<<grid_for(m->nC, BT), BT, 0, st>>>(a);
     }

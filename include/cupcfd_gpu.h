@@ -126,8 +126,8 @@ typedef struct {
     int32_t order, precisions;
     int32_t bandwidth;   /* largest |c - neighbour| of the internal numbering */
     int64_t deviceBytes; /* device memory held by the mesh */
-    int32_t stagedCtas;  /* CTAs of a staged FP32 forward launch; 0 when this mesh runs the unstaged kernels only */
-    int32_t stagedSmem;  /* its dynamic shared memory per CTA, bytes */
+    int32_t tiles;       /* 1 when the face loops take the L2-prefetch kernels (faces numbered by owner tile) */
+    int32_t reserved;
 } cupcfd_mesh_info;
 
 typedef struct cupcfd_gpu_mesh cupcfd_gpu_mesh;
@@ -250,16 +250,11 @@ int cupcfd_gpu_hdf5_dataset_read(const char *path, const char *name, double *out
 int cupcfd_gpu_mesh_destroy(cupcfd_gpu_mesh *mesh);
 int cupcfd_gpu_mesh_get_info(const cupcfd_gpu_mesh *mesh, cupcfd_mesh_info *info);
 
-/* Forward+adjoint execution: 1 = one wavefront-fused cooperative launch
- * (forward and adjoint tiles interleaved, the adjoint of a tile a few rounds
- * behind its forward); 0 (auto) and 2 = two launches, the faster on B200 at
- * every size measured: a forward that also runs the mass-flux adjoint, then
- * the gradient adjoint. All modes give bit-identical results. */
-int cupcfd_gpu_mesh_set_fusion(cupcfd_gpu_mesh *mesh, int32_t mode);
-
-/* Synchronises the mesh's work and returns CUPCFD_E_ERROR (message in
- * cupcfd_gpu_last_error) if a device-side wait of an earlier asynchronous
- * call expired; clears the condition. CUPCFD_E_SUCCESS otherwise. */
+/* Synchronises `stream` (the asynchronous device calls' stream) and returns
+ * CUPCFD_E_ERROR (message in cupcfd_gpu_last_error) if the work on it
+ * failed, CUPCFD_E_SUCCESS otherwise. No kernel of this library waits on
+ * another block, a peer or a flag, so a failed launch is the only
+ * asynchronous error there is. */
 int cupcfd_gpu_mesh_check_status(cupcfd_gpu_mesh *mesh, void *stream);
 
 /* Boundary regions (CupCfdSoAMesh region/boundary arrays): regionType[nRegions]
@@ -279,6 +274,17 @@ int cupcfd_gpu_mesh_set_region_split(cupcfd_gpu_mesh *mesh, int32_t nRegions, co
  * xadj[nCells+1], adj[nIncidences]) for bit-exact comparison with
  * CupCfdSoAMesh::cellFaceMapCSRXAdj / cellFaceMapCSRAdj. */
 int cupcfd_gpu_mesh_get_cell_face_csr(const cupcfd_gpu_mesh *mesh, int32_t *xadj, int32_t nXAdj, int32_t *adj, int32_t nAdj);
+
+/* Downloads the incidence lists the face-loop kernels read, in the mesh's
+ * internal numbering, as a CSR over internal cells (host arrays xadj[nCells+1],
+ * face[nIncidences], other[nIncidences]): face = internal face id << 1 | role
+ * (0 when the cell is the face's cell1, 1 when it is its cell2), other = the
+ * face's other internal cell or -1 - boundaryId. Mapped back through
+ * cupcfd_gpu_mesh_get_numbering, cell c's list equals row cellN2O[c] of
+ * CupCfdSoAMesh::cellFaceMapCSRAdj, in order. No counterpart in the reference
+ * (it checks a renumbering). */
+int cupcfd_gpu_mesh_get_incidences(const cupcfd_gpu_mesh *mesh, int32_t *xadj, int32_t nXAdj, int32_t *face,
+                                   int32_t *other, int32_t nInc);
 
 /* Downloads the FP64 source arrays in the reference's numbering (any pointer
  * may be NULL): faceCell1/2, faceBnd [nFaces], faceLambda, faceArea [nFaces],
@@ -452,8 +458,10 @@ int cupcfd_gpu_dev_adjoint(cupcfd_gpu_mesh *mesh, int32_t precision, const void 
  * 16,777,216 cells; larger meshes return CUPCFD_E_ARRAY_SIZE_MISMATCH. All
  * calls share the array: calls whose kernels overlap on the GPU race. The
  * first call on a device sets up the array's address with that device
- * current; make it before any stream capture. Errors are reported by status
- * code only (cupcfd_gpu_last_error is not updated). */
+ * current; make it before any stream capture. The call runs on the mesh's
+ * device and gives the caller's current device back before it returns.
+ * Errors are reported by status code only (cupcfd_gpu_last_error is not
+ * updated). */
 int cupcfd_gpu_dev_forward_noalloc(cupcfd_gpu_mesh *mesh, int32_t precision, const void *phi, const void *phiB,
                                    const void *state, const void *gface, void *grad, void *massFlux, double *loss,
                                    void *stream);

@@ -50,7 +50,9 @@ def parse(text):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("CUPCFD_REFERENCE")
+    if not ref:
+        sys.exit("usage: %s REFERENCE_CHECKOUT (or set CUPCFD_REFERENCE)" % sys.argv[0])
     src = os.path.join(ref, REL)
     with open(src) as fh:
         cases = parse(fh.read())

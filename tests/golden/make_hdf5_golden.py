@@ -49,7 +49,9 @@ def parse(text):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("CUPCFD_REFERENCE")
+    if not ref:
+        sys.exit("usage: %s REFERENCE_CHECKOUT (or set CUPCFD_REFERENCE)" % sys.argv[0])
     with open(os.path.join(ref, REL)) as fh:
         cases = parse(fh.read())
     out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "meshhdf5source_golden.json")

@@ -35,7 +35,7 @@ def _rank(rank, world, port, q):
     try:
         t = bench.max_over_ranks(1.0 + rank, dist, "cpu")      # rank r took 1 + r seconds
         v = bench.job_gfaces(world, 2_000_000_000, t)
-        args = bench.argparse.Namespace(gpus=world, steps=3, warmup=3, n=8, cpu_n=6, cpu_reps=3)
+        args = bench.argparse.Namespace(gpus=world, steps=3, warmup=3, n=6, cpu_n=6, cpu_reps=3, order=2)
         out = io.StringIO()
         with redirect_stdout(out):
             rc = bench.run_reference(args)
@@ -65,3 +65,8 @@ def test_two_gloo_ranks_time_max_and_reference_arm_on_rank0():
     assert line["impl"] == "reference" and line["n_gpus"] == 2
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
     assert line["cpu_baseline"]["value"] == line["value"] > 0
+    # the reference arm runs the GPU arm's workload, with its steps and warm-up
+    sys.path.insert(0, ROOT)
+    import bench
+    assert line["config"] == bench.workload_config(6, 2, 2)
+    assert line["steps"] == 3 and line["warmup"] == 3

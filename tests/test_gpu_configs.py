@@ -1,10 +1,10 @@
 """Parity at the benchmark configurations' own sizes.
 
-  config 2: 256^3 structured, FP32-compensated forward + adjoint against the
-            FP64 path on the same mesh and fields (the FP64 path is
-            bit-identical to the oracle, pinned at smaller sizes); the
-            bounds of tests/test_gpu_parity.py, normwise / RMS / floored
-            elementwise.
+  config 2: 256^3 structured, against the oracle itself: the FP64 forward
+            bit for bit and its adjoint within 1e-13; the FP32-compensated
+            forward + adjoint against the oracle fed the same FP32-rounded
+            inputs, every output within 1e-6 normwise and RMS, elementwise
+            within 16 u sum|term| (forward) or the floored 5e-5 (adjoint).
   config 3: 192^3 jittered, cell and face numbering permuted: the FP64
             gradient and mass flux bit-identical to the oracle, the FP32
             path within the same normwise / RMS bounds and, element by
@@ -24,7 +24,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from test_gpu_parity import as_f32, assert_f32c, errs, _adjoint_oracle
+from test_gpu_parity import as_f32, assert_f32c, assert_incidences_match, errs, _adjoint_oracle, _loss_oracle
 
 pytestmark = pytest.mark.gpu
 
@@ -45,50 +45,78 @@ def _cell2_volume(cg, mesh):
     return c2[f2o], vol[c2o]
 
 
-def test_config2_f32c_vs_fp64_256(cg, gpu):
-    torch = _torch()
-    dev = torch.device("cuda:0")
+@pytest.fixture(scope="module")
+def config2():
+    """The 256^3 unit-cube mesh of the oracle with seeded fields and face
+    weights in the reference's numbering (about 9 GB of host memory, 16 s)."""
+    ref = O.structgen(256, 256, 256)
+    f = O.fields(ref, 20261205)
+    gface = np.random.Generator(np.random.Philox(key=20261211)).standard_normal(ref["nFaces"])
+    return ref, f, gface
+
+
+def test_config2_fp64_256_equals_oracle(cg, gpu, config2):
+    """FP64 forward bit for bit, FP64 adjoint within 1e-13, against the
+    oracle itself on the 256^3 benchmark mesh (host-buffer call)."""
+    ref, f, gface = config2
     mesh = cg.Mesh.structgen(256, 256, 256, order=cg.ORDER_OWNER)
-    nC, nF, nB = mesh.nCells, mesh.nFaces, mesh.nBoundaries
-    g = torch.Generator(device=dev)
-    g.manual_seed(20261205)
-    phi = (torch.rand(nC, generator=g, device=dev) * 2 - 1)
-    phiB = (torch.rand(nB, generator=g, device=dev) * 2 - 1)
-    st = torch.randn(nC, 4, generator=g, device=dev)
-    st[:, 0] = 0.9 + 0.2 * torch.rand(nC, generator=g, device=dev)
-    gface = torch.randn(nF, generator=g, device=dev)
-    s = torch.cuda.current_stream()
-    out32 = dict(grad=torch.empty(3, nC, device=dev), mf=torch.zeros(nF, device=dev), pb=torch.empty(nC, device=dev),
-                 pbb=torch.empty(nB, device=dev), sb=torch.empty(nC, 4, device=dev),
-                 loss=torch.zeros(1, dtype=torch.float64, device=dev))
-    cg.dev_forward_adjoint(mesh, cg.PREC_F32C, phi, phiB, st, gface, out32["grad"], out32["mf"], out32["pb"],
-                           out32["pbb"], out32["sb"], out32["loss"], stream=s)
-    st64 = st.double().t().contiguous()
-    out64 = dict(grad=torch.empty(3, nC, dtype=torch.float64, device=dev),
-                 mf=torch.zeros(nF, dtype=torch.float64, device=dev),
-                 pb=torch.empty(nC, dtype=torch.float64, device=dev),
-                 pbb=torch.empty(nB, dtype=torch.float64, device=dev),
-                 sb=torch.empty(4, nC, dtype=torch.float64, device=dev),
-                 loss=torch.zeros(1, dtype=torch.float64, device=dev))
-    cg.dev_forward_adjoint(mesh, cg.PREC_F64, phi.double(), phiB.double(), st64, gface.double(), out64["grad"],
-                           out64["mf"], out64["pb"], out64["pbb"], out64["sb"], out64["loss"], stream=s)
-    assert mesh.check_status(s) == cg.E_SUCCESS
-    torch.cuda.synchronize()
-    c2, _ = _cell2_volume(cg, mesh)
-    inner = torch.from_numpy(c2 >= 0).to(dev)
-    pairs = [("grad", out32["grad"], out64["grad"], 1e-5), ("massFlux", out32["mf"][inner], out64["mf"][inner], 1e-5),
-             ("phiBar", out32["pb"], out64["pb"], 5e-5), ("phiBBar", out32["pbb"], out64["pbb"], 5e-5),
-             ("stateBar", out32["sb"].t().contiguous(), out64["sb"], 5e-5)]
-    for name, a, b, elem in pairs:
-        rms = float(torch.sqrt(torch.mean(b * b)))
-        e = cg.error_norms(a.contiguous(), b.contiguous(), 1e-2 * rms)
-        assert e["max_rel_norm"] <= 1e-6 and e["rms_rel"] <= 1e-6 and e["max_rel_floor"] <= elem, (name, e)
-    assert abs(float(out32["loss"]) - float(out64["loss"])) <= 1e-6 * abs(float(out64["loss"]))
+    out = cg.forward_adjoint(mesh, cg.PREC_F64, f["phi"], f["phiB"], f["den"], f["u"], f["v"], f["w"], gface)
+    rc, g_ref, _ = O.gradient(ref, f["phi"], f["phiB"], 1)
+    mf_ref = O.mass_plain(ref, f["den"], f["u"], f["v"], f["w"])
+    inner = ref["faceCell2"] >= 0
+    assert np.array_equal(out["grad"], g_ref)
+    assert np.array_equal(out["massFlux"][inner], mf_ref[inner])
+    for k, v in _adjoint_oracle(ref, f, gface).items():
+        e = errs(out[k], v)
+        assert e["norm"] <= 1e-13 and e["rms"] <= 1e-13, (k, e)
+    mesh.close()
+
+
+def test_config2_f32c_256_vs_oracle(cg, gpu, config2):
+    """FP32-compensated forward + adjoint on the 256^3 benchmark mesh against
+    the FP64 oracle fed the same FP32-rounded fields: every output (gradient,
+    mass flux, dL/dphi, dL/dphi_b, dL/d(rho, u, v, w)) within 1e-6 normwise
+    and RMS; gradient and mass flux element by element within
+    16 u sum|term| (u = 2^-24, sum|term| from the oracle on absolute values),
+    the adjoints within 5e-5 floored at 1e-2 rms; the loss within 1e-6."""
+    ref, f, gface = config2
+    mesh = cg.Mesh.structgen(256, 256, 256, order=cg.ORDER_OWNER)
+    f32 = {k: as_f32(v) if isinstance(v, np.ndarray) and v.dtype == np.float64 else v for k, v in f.items()}
+    g32 = as_f32(gface)
+    out = cg.forward_adjoint(mesh, cg.PREC_F32C, f32["phi"], f32["phiB"], f32["den"], f32["u"], f32["v"], f32["w"],
+                             g32)
+    mesh.close()
+    r32 = dict(ref)
+    for k in ("faceNorm", "faceLambda"):
+        r32[k] = as_f32(ref[k])
+    rc, g_ref, _ = O.gradient(r32, f32["phi"], f32["phiB"], 1)
+    mf_ref = O.mass_plain(r32, f32["den"], f32["u"], f32["v"], f32["w"])
+    inner = ref["faceCell2"] >= 0
+    for got, want, what in ((out["grad"], g_ref, "grad"), (out["massFlux"][inner], mf_ref[inner], "massFlux")):
+        e = errs(got, want)
+        assert e["norm"] <= 1e-6 and e["rms"] <= 1e-6, (what, e)
+    ra = dict(r32)
+    ra["faceNorm"] = np.abs(r32["faceNorm"])
+    rc, g_abs, _ = O.gradient(ra, np.abs(f32["phi"]), np.abs(f32["phiB"]), 1)
+    mf_abs = O.mass_plain(ra, np.abs(f32["den"]), np.abs(f32["u"]), np.abs(f32["v"]), np.abs(f32["w"]))
+    u = 2.0 ** -24
+    assert np.all(np.abs(out["grad"] - g_ref) <= 16 * u * g_abs), "gradient above 16 u sum|term|"
+    assert np.all(np.abs(out["massFlux"][inner] - mf_ref[inner]) <= 16 * u * mf_abs[inner]), "mass flux above 16 u sum|term|"
+    for k, v in _adjoint_oracle(r32, f32, g32).items():
+        assert_f32c(out[k], v, k, elem=5e-5)
+    L, _, _ = _loss_oracle(r32, f32, g32)
+    assert abs(out["loss"][0] - L) <= 1e-6 * abs(L)
 
 
 def test_config3_jittered_permuted_192(cg, gpu):
     ref = O.jitter(192, 192, 192, 0.25, seed=3, permute=True)
     mesh = cg.Mesh.jittered(192, 192, 192, 0.25, seed=3, permute=True, order=cg.ORDER_RCM)
+    # connectivity: the reference-numbered CSR, and the RCM-renumbered lists
+    # the kernels read, both bit for bit against the oracle's
+    xadj, adj = mesh.cell_face_csr()
+    rx, ra = O.cell_face_csr(ref)
+    assert np.array_equal(xadj, rx) and np.array_equal(adj, ra)
+    assert_incidences_match(mesh, ref)
     f = O.fields(ref, 20261206)
     rc, g_ref, _ = O.gradient(ref, f["phi"], f["phiB"], 1)
     mf_ref = O.mass_plain(ref, f["den"], f["u"], f["v"], f["w"])

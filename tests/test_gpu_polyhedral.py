@@ -6,8 +6,8 @@ different numbers of entries and faces. Every path is checked against the
 oracle (itself bit-identical to the reference on these meshes,
 tests/test_oracle_vs_reference.py): FP64 bit for bit, FP32-compensated
 within the error bounds of the hexahedral tests, and the forward+adjoint
-variants (L2-prefetch tiles, plain kernels, wavefront-fused launch, host
-call) against each other bit for bit.
+variants (the one forward+adjoint call, the separate forward and adjoint
+calls, the host call) against each other bit for bit.
 """
 import numpy as np
 import pytest
@@ -91,15 +91,15 @@ def test_forward_adjoint_host_call(cg, gpu, order):
 
 @pytest.mark.parametrize("order", ORDERS)
 @pytest.mark.parametrize("prec", [0, 1])
-def test_fused_equals_two_pass(cg, gpu, order, prec):
-    """Wavefront-fused launch, L2-prefetch tiles (aligned arrays) and the
-    plain kernels give the same bits on ragged slices and tiles."""
+def test_forward_adjoint_equals_separate_calls(cg, gpu, order, prec):
+    """The forward+adjoint call and the separate forward and adjoint calls
+    give the same bits on ragged slices and tiles."""
     import torch
     m = _poly(6, dims=(24, 22, 20), frac=0.3)
     mesh = cg.Mesh.from_arrays(m, order=order)
     fields = _dev_fields(mesh, prec, 5)
-    a = _run_fa(cg, mesh, prec, fields, 1)
-    b = _run_fa(cg, mesh, prec, fields, 2)
+    a = _run_fa(cg, mesh, prec, fields, False)
+    b = _run_fa(cg, mesh, prec, fields, True)
     for k in ("grad", "mflux", "pb", "pbb", "sb"):
         assert torch.equal(a[k], b[k]), k
 

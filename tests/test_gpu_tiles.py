@@ -1,13 +1,10 @@
-"""The tile-path kernels against the plain ones, and the two incidence layouts.
+"""The L2-prefetch tile kernels against the plain ones.
 
 Every variant runs the same per-cell arithmetic in the same face order, so
 results must be bit-identical:
   - the L2-prefetch kernels (the default when the user arrays start on
     16-byte boundaries) against the plain kernels, which the same call runs
     when phi, gface and the gradient are passed as views offset by one float;
-  - the shared-memory staged kernels (CUPCFD_TILE_MODE=2 at mesh creation),
-    including stage capacities lowered far below the tiles' needs so entries
-    and faces overflow to the global-memory path;
   - the two-launch forward+adjoint (forward with the mass-flux adjoint, then
     the gradient adjoint) against dev_forward + dev_adjoint.
 The device timers name the kernels each call ran, so every test checks that
@@ -112,59 +109,24 @@ def test_prefetch_equals_plain(cg, gpu, kind, dims, order):
     _assert_same(a, b)
 
 
-@pytest.mark.parametrize("kind,dims,order", CASES)
-def test_staged_smem_equals_plain(cg, gpu, kind, dims, order, monkeypatch):
-    import torch
-    monkeypatch.setenv("CUPCFD_TILE_MODE", "2")
-    mesh = _mesh(cg, kind, dims, order)
-    assert mesh.stagedCtas > 0 and mesh.stagedSmem > 0
-    fields = _fields(torch, mesh, 5)
-    a = _run(cg, torch, mesh, *fields, offset=False)
-    ka = _run.kernels
-    b = _run(cg, torch, mesh, *fields, offset=True)
-    assert "k_fwd_f32_staged" in ka and "k_fwd_f32" in _run.kernels
-    if mesh.nCells % 4 == 0:
-        assert "k_adj_f32_staged" in ka
-    _assert_same(a, b)
-
-
-def test_native_numbering_is_unstaged(cg, gpu):
+def test_native_numbering_runs_plain_kernels(cg, gpu):
     """ORDER_NATIVE keeps the reference's face numbering, which is not sorted
     by owner, so there are no tile ranges and the mesh runs the plain
     kernels."""
     import torch
     mesh = cg.Mesh.structgen(16, 12, 8, order=cg.ORDER_NATIVE)
-    assert mesh.stagedCtas == 0
+    assert not mesh.tiles
     _run(cg, torch, mesh, *_fields(torch, mesh, 1), offset=False)
     assert _run.kernels == {"k_fwd_f32", "k_reduce_partials", "k_adj_f32"}
 
 
-def test_staged_overflow_to_global(cg, gpu, monkeypatch):
-    """Stage buffers far smaller than a tile's ranges: the entries and faces
-    beyond them are read from global memory, results unchanged."""
-    import torch
-    monkeypatch.setenv("CUPCFD_TILE_MODE", "2")
-    monkeypatch.setenv("CUPCFD_STAGED_ENT_CAP", "64")
-    monkeypatch.setenv("CUPCFD_STAGED_FACE_CAP", "8")
-    small = cg.Mesh.structgen(30, 20, 10, order=cg.ORDER_MORTON)
-    monkeypatch.delenv("CUPCFD_STAGED_ENT_CAP")
-    monkeypatch.delenv("CUPCFD_STAGED_FACE_CAP")
-    full = cg.Mesh.structgen(30, 20, 10, order=cg.ORDER_MORTON)
-    assert 0 < small.stagedSmem < full.stagedSmem
-    fields = _fields(torch, small, 9)
-    ref = _run(cg, torch, full, *fields, offset=True)
-    _assert_same(_run(cg, torch, small, *fields, offset=False), ref)
-    assert "k_fwd_f32_staged" in _run.kernels
-    _assert_same(_run(cg, torch, full, *fields, offset=False), ref)
-
-
 def test_tile_path_can_be_disabled(cg, gpu, monkeypatch):
     import torch
-    monkeypatch.setenv("CUPCFD_STAGED", "0")
+    monkeypatch.setenv("CUPCFD_TILE_MODE", "0")
     off = cg.Mesh.structgen(16, 16, 16, order=cg.ORDER_OWNER)
-    monkeypatch.delenv("CUPCFD_STAGED")
+    monkeypatch.delenv("CUPCFD_TILE_MODE")
     on = cg.Mesh.structgen(16, 16, 16, order=cg.ORDER_OWNER)
-    assert off.stagedCtas == 0 and on.stagedCtas > 0
+    assert not off.tiles and on.tiles
     fields = _fields(torch, on, 3)
     a = _run(cg, torch, off, *fields, offset=False)
     assert _run.kernels == {"k_fwd_f32", "k_reduce_partials", "k_adj_f32"}

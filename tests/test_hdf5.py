@@ -32,8 +32,20 @@ from h5write import mesh_hdf5_bytes
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLD = json.load(open(os.path.join(HERE, "golden", "meshhdf5source_golden.json")))
-FIXTURE = os.path.join("/root/reference", GOLD["fixture"])
-need_fixture = pytest.mark.skipif(not os.path.exists(FIXTURE), reason="reference fixture absent")
+
+
+def _reference_root():
+    """The reference checkout: CUPCFD_REFERENCE, else the one oracle/Makefile
+    compiled oracle/_ref from (empty when neither exists)."""
+    env = os.environ.get("CUPCFD_REFERENCE")
+    if env:
+        return env
+    rec = os.path.join(os.path.dirname(HERE), "oracle", "_ref", "reference_root.txt")
+    return open(rec).read().strip() if os.path.exists(rec) else ""
+
+
+FIXTURE = os.path.join(_reference_root(), GOLD["fixture"]) if _reference_root() else ""
+need_fixture = pytest.mark.skipif(not (FIXTURE and os.path.exists(FIXTURE)), reason="reference fixture absent")
 
 
 def _case(name):

@@ -53,6 +53,7 @@ def test_noalloc_forward_equals_forward_twice(cg, gpu, prec):
         g1, m1, l1 = _outputs(torch, mesh, phi.dtype)
         rc = cg.dev_forward_noalloc(mesh, prec, phi, phiB, st, g1, m1, gface=gface, loss=l1, stream=s)
         assert rc == cg.E_SUCCESS
+        assert torch.cuda.current_device() == 0              # the caller's device is given back
         torch.cuda.synchronize()
         assert torch.equal(g0, g1)
         assert torch.equal(m0, m1)
