@@ -105,6 +105,32 @@ struct Acc2x2 {
     __device__ __forceinline__ double y() const { return (double) s.y + (double) e.y; }
 };
 
+// ---------------------------------------------------------------------------
+// FP32 face interpolation seen from one of the face's two cells: x_f =
+// wc x_c + wo x_o (wc the weight of this cell's value, wo of the other's),
+// rounded as fmaf(wc, x_c, wo * x_o). For the face's owner (cell1, P)
+// wc = 1 - lambda and wo = lambda (MassKernels.ipp:140-153: lambda weights
+// the neighbour). The owner's mass flux and both cells' adjoint terms use
+// these same values, so the owner computes rho_f and u_f . S_f once for both.
+// ---------------------------------------------------------------------------
+struct FaceW {
+    float wc, wo;
+};
+__device__ __forceinline__ FaceW face_weights(float lam, bool isN) {
+    const float facp = 1.f - lam;
+    return FaceW{isN ? lam : facp, isN ? facp : lam};
+}
+__device__ __forceinline__ float interp(const FaceW &w, float xc, float xo) { return fmaf(w.wc, xc, w.wo * xo); }
+// {rho, u, v, w} in two packed FP32x2 operations; every lane rounds as interp()
+__device__ __forceinline__ float4 interp4(const FaceW &w, float4 sc, float4 so) {
+    const float2 wc2 = make_float2(w.wc, w.wc), wo2 = make_float2(w.wo, w.wo);
+    const float2 a = __ffma2_rn(wc2, make_float2(sc.x, sc.y), __fmul2_rn(wo2, make_float2(so.x, so.y)));
+    const float2 b = __ffma2_rn(wc2, make_float2(sc.z, sc.w), __fmul2_rn(wo2, make_float2(so.z, so.w)));
+    return make_float4(a.x, a.y, b.x, b.y);
+}
+// u_f . S_f of an interpolated state {rho, u, v, w} and a face record {S, lambda}
+__device__ __forceinline__ float udots(float4 s, float4 G) { return fmaf(s.y, G.x, fmaf(s.z, G.y, s.w * G.z)); }
+
 // 32-byte read-only load as two 128-bit loads (no __ldg overload for double4)
 __device__ __forceinline__ double4 ldg4(const double4 *p) {
     double2 a = __ldg(reinterpret_cast<const double2 *>(p));
@@ -279,8 +305,7 @@ __global__ void __launch_bounds__(256, CUPCFD_MINB_F32) k_grad_f32(int nC, SellV
                 phif = pv[j];
             } else {
                 float facn = G[j].w, facp = 1.f - facn;
-                float phN = isN ? phic : pv[j], phP = isN ? pv[j] : phic;
-                phif = fmaf(facn, phN, facp * phP);
+                phif = interp(face_weights(facn, isN), phic, pv[j]);
                 if (CORR) {
                     float4 xo = __ldg(cc + o), xf = __ldg(fc + (code >> 1));
                     float go0 = __ldg(go + o), go1 = __ldg(go + ldc + o), go2 = __ldg(go + 2 * ldc + o);
@@ -412,13 +437,9 @@ __global__ void __launch_bounds__(256) k_mass_plain_f32(int nF, const int2 *__re
     int2 pn = fcells[f];
     if (pn.y < 0) return;
     float4 G = fg[f];
-    float facn = G.w, facp = 1.f - facn;
     float4 sP = __ldg(st + pn.x), sN = __ldg(st + pn.y);
-    float denf = fmaf(facn, sN.x, facp * sP.x);
-    float uF = fmaf(facn, sN.y, facp * sP.y);
-    float vF = fmaf(facn, sN.z, facp * sP.z);
-    float wF = fmaf(facn, sN.w, facp * sP.w);
-    mflux[f] = denf * fmaf(uF, G.x, fmaf(vF, G.y, wF * G.z));
+    float4 sf = interp4(face_weights(G.w, false), sP, sN);  // seen from the owner
+    mflux[f] = sf.x * udots(sf, G);
 }
 
 }  // namespace cupcfd_gpu

@@ -133,14 +133,11 @@ __device__ __forceinline__ double fwd_cell_f32(int c, const SellView &sv, const 
             if (o < 0) {
                 phif = pv[j];
             } else {
-                float facn = G[j].w, facp = 1.f - facn;
-                phif = isN ? fmaf(facn, phic, facp * pv[j]) : fmaf(facn, pv[j], facp * phic);
-                if (!isN) {
-                    float denf = fmaf(facn, so[j].x, facp * sc.x);
-                    float uF = fmaf(facn, so[j].y, facp * sc.y);
-                    float vF = fmaf(facn, so[j].z, facp * sc.z);
-                    float wF = fmaf(facn, so[j].w, facp * sc.w);
-                    float m = denf * fmaf(uF, G[j].x, fmaf(vF, G[j].y, wF * G[j].z));
+                const FaceW fw = face_weights(G[j].w, isN);
+                phif = interp(fw, phic, pv[j]);
+                if (!isN) {  // the owner computes m_f
+                    const float4 sf = interp4(fw, sc, so[j]);
+                    const float m = sf.x * udots(sf, G[j]);
                     mflux[code >> 1] = m;
                     lsum = __fma_rn((double) gf[j], (double) m, lsum);
                 }
@@ -206,24 +203,19 @@ __device__ __forceinline__ double fwd_madj_cell_f32(int c, const SellView &sv, c
                 axy.add_prod(make_float2(phif, phif), make_float2(G[j].x, G[j].y));
                 azr.add_x(phif, G[j].z);
             } else {
-                float facn = G[j].w, facp = 1.f - facn;
-                phif = isN ? fmaf(facn, phic, facp * pv[j]) : fmaf(facn, pv[j], facp * phic);
+                const FaceW fw = face_weights(G[j].w, isN);
+                phif = interp(fw, phic, pv[j]);
+                // rho_f and u_f . S_f from this cell's side: the owner's mass
+                // flux and this cell's mass-adjoint terms (adj_cell_f32)
+                const float4 sf = interp4(fw, sc, so[j]);
+                const float q = udots(sf, G[j]);
                 if (!isN) {
-                    float denf = fmaf(facn, so[j].x, facp * sc.x);
-                    float uF = fmaf(facn, so[j].y, facp * sc.y);
-                    float vF = fmaf(facn, so[j].z, facp * sc.z);
-                    float wF = fmaf(facn, so[j].w, facp * sc.w);
-                    float m = denf * fmaf(uF, G[j].x, fmaf(vF, G[j].y, wF * G[j].z));
+                    const float m = sf.x * q;
                     mflux[code >> 1] = m;
                     lsum = __fma_rn((double) gf[j], (double) m, lsum);
                 }
-                // mass part of the adjoint (adj_cell_f32)
-                float wc = isN ? facn : facp, wo = isN ? facp : facn;
-                float denA = fmaf(wc, sc.x, wo * so[j].x);
-                float uA = fmaf(wc, sc.y, wo * so[j].y), vA = fmaf(wc, sc.z, wo * so[j].z), wA = fmaf(wc, sc.w, wo * so[j].w);
-                float a = wc * gf[j];
-                float q = fmaf(uA, G[j].x, fmaf(vA, G[j].y, wA * G[j].z));
-                float b = a * denA;
+                const float a = fw.wc * gf[j];
+                const float b = a * sf.x;
                 axy.add_prod(make_float2(phif, phif), make_float2(G[j].x, G[j].y));
                 azr.add_prod(make_float2(phif, a), make_float2(G[j].z, q));
                 uvb.add_prod(make_float2(b, b), make_float2(G[j].x, G[j].y));
@@ -445,19 +437,16 @@ __device__ __forceinline__ void adj_cell_f32(int c, const SellView &sv, const fl
                 if (doG) phibBar[-1 - o] = fmaf(hx, G[j].x, fmaf(hy, G[j].y, hz * G[j].z));
                 continue;
             }
-            bool isN = code & 1;
-            float facn = G[j].w, facp = 1.f - facn;
-            float wc = isN ? facn : facp, wo = isN ? facp : facn;
+            const FaceW fw = face_weights(G[j].w, code & 1);
             if (doG) {
                 float sx = fmaf(hscale, go[j][0], hx), sy = fmaf(hscale, go[j][1], hy), sz = fmaf(hscale, go[j][2], hz);
-                pb.add_prod(wc, fmaf(sx, G[j].x, fmaf(sy, G[j].y, sz * G[j].z)));
+                pb.add_prod(fw.wc, fmaf(sx, G[j].x, fmaf(sy, G[j].y, sz * G[j].z)));
             }
             if (doM) {
-                float denf = fmaf(wc, sc.x, wo * so[j].x);
-                float uF = fmaf(wc, sc.y, wo * so[j].y), vF = fmaf(wc, sc.z, wo * so[j].z), wF = fmaf(wc, sc.w, wo * so[j].w);
-                float a = wc * gf[j];
-                rb.add_prod(a, fmaf(uF, G[j].x, fmaf(vF, G[j].y, wF * G[j].z)));
-                float b = a * denf;
+                const float4 sf = interp4(fw, sc, so[j]);
+                const float a = fw.wc * gf[j];
+                rb.add_prod(a, udots(sf, G[j]));
+                const float b = a * sf.x;
                 uvb.add_prod(make_float2(b, b), make_float2(G[j].x, G[j].y));
                 wb.add_prod(b, G[j].z);
             }

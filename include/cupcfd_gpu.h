@@ -49,6 +49,7 @@ extern "C" {
 #define CUPCFD_E_NOT_IMPLEMENTED 109    /* E_NOT_IMPLEMENTED, Error.h:143 */
 #define CUPCFD_E_FILE_MISSING 10        /* E_FILE_MISSING, Error.h:44 */
 #define CUPCFD_E_INVALID_FILE_FORMAT 105 /* E_INVALID_FILE_FORMAT, Error.h:139 */
+#define CUPCFD_E_CONFIG_OPT_NOT_FOUND 92 /* E_CONFIG_OPT_NOT_FOUND, Error.h:126 */
 
 /* ---- region types: cupcfd::geometry::mesh::RType (UnstructuredMeshInterface.h:58-65) ---- */
 #define CUPCFD_RTYPE_DEFAULT 0

@@ -47,6 +47,7 @@ extern "C" int ref_ecode_null_ptr() { return (int) cupcfd::error::E_NULL_PTR; }
 extern "C" int ref_ecode_not_implemented() { return (int) cupcfd::error::E_NOT_IMPLEMENTED; }
 extern "C" int ref_ecode_file_missing() { return (int) cupcfd::error::E_FILE_MISSING; }
 extern "C" int ref_ecode_invalid_file_format() { return (int) cupcfd::error::E_INVALID_FILE_FORMAT; }
+extern "C" int ref_ecode_config_opt_not_found() { return (int) cupcfd::error::E_CONFIG_OPT_NOT_FOUND; }
 extern "C" int ref_sizeof_euclidean_vector_f64() { return (int) sizeof(euc::EuclideanVector<double,3>); }
 extern "C" int ref_sizeof_euclidean_vector_f32() { return (int) sizeof(euc::EuclideanVector<float,3>); }
 extern "C" int ref_offsetof_cmp_f64() {

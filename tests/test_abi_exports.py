@@ -49,7 +49,7 @@ def test_status_constants_match_reference_enum(cg):
     # values of cupcfd::error::eCodes (include/error/Error.h:32-144, enum from 0)
     assert consts == {"E_ARRAY_SIZE_MISMATCH": 25, "E_INVALID_INDEX": 68, "E_CONFIG_INVALID_VALUE": 90,
                       "E_SUCCESS": 95, "E_ERROR": 98, "E_NULL_PTR": 99, "E_NOT_IMPLEMENTED": 109,
-                      "E_FILE_MISSING": 10, "E_INVALID_FILE_FORMAT": 105}
+                      "E_FILE_MISSING": 10, "E_INVALID_FILE_FORMAT": 105, "E_CONFIG_OPT_NOT_FOUND": 92}
     assert (cg.E_SUCCESS, cg.E_INVALID_INDEX, cg.E_ERROR) == (95, 68, 98)
 
 

@@ -98,6 +98,7 @@ def test_error_codes_match_reference_enum():
     assert ref.ref_ecode_not_implemented() == 109
     assert ref.ref_ecode_file_missing() == 10
     assert ref.ref_ecode_invalid_file_format() == 105
+    assert ref.ref_ecode_config_opt_not_found() == 92
     # EuclideanVector<T,3> carries a vptr: 32-byte (double) / 24-byte (float) stride, components at +8
     assert ref.ref_sizeof_euclidean_vector_f64() == 32
     assert ref.ref_sizeof_euclidean_vector_f32() == 24
