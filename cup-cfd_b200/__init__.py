@@ -137,6 +137,9 @@ SIGNATURES = {
     "cupcfd_gpu_gradient_phi_gauss_dolfyn": ([_VP, _I, _VP, _I, _VP, _I, _VP, _I, _I, _I, _VP, _I, _I, _I, _I, _I, _I], _I),
     "cupcfd_gpu_flux_mass_dolfyn_face_loop": ([_VP, Vec3View, _I, Vec3View, _I, Vec3View, _I, Vec3View, _I]
                                               + [_VP, _I] * 10 + [_D] + [_VP] * 4 + [_I] * 4 + [_VP, _I] * 8, _I),
+    "cupcfd_gpu_flux_mass_dolfyn_face_loop_f32": ([_VP, Vec3View, _I, Vec3View, _I, Vec3View, _I, Vec3View, _I]
+                                                  + [_VP, _I] * 10 + [C.c_float] + [_VP] * 4 + [_I] * 4
+                                                  + [_VP, _I] * 8, _I),
     "cupcfd_gpu_forward_adjoint": ([_VP, _I] + [_VP] * 16, _I),
     "cupcfd_gpu_dev_permute_cells": ([_VP, _I, _I, _VP, _I, _I64, _VP, _I, _I64, _VP], _I),
     "cupcfd_gpu_dev_permute_faces": ([_VP, _I, _VP, _I, _VP, _I, _VP], _I),
@@ -436,22 +439,27 @@ def FluxMassDolfynFaceLoop(mesh, dudx, dvdx, dwdx, dpdx, denCell, denBoundary, u
                            teCell, teBoundary, edCell, edBoundary, viseffCell, viseffBoundary, tCell, tBoundary):
     """Mirror of cupcfd::fvm::FluxMassDolfynFaceLoop (MassKernels.h:48-81).
     ``counters`` is an int32 array [icinl, icout, icsym, icwal] updated in
-    place; in/out arrays are updated in place. Returns an eCodes value."""
+    place; in/out arrays are updated in place. Returns an eCodes value.
+    float32 arrays run the reference's T = float instantiation
+    (cupcfd_gpu_flux_mass_dolfyn_face_loop_f32), float64 arrays T = double."""
     cnt = counters
     ptrs = [C.c_void_p(cnt.ctypes.data + 4 * k) for k in range(4)]
+    f32 = np.asarray(denCell).dtype == np.float32
 
     def a(x):
         return (_p(x), 0 if x is None else len(x))
 
     args = [mesh.h]
     for vv in (dudx, dvdx, dwdx, dpdx):
-        args += [_vec(vv), len(vv)]
+        args += [_vec(vv, 4 if f32 else 8), len(vv)]
     for x in (denCell, denBoundary, uCell, vCell, wCell, massFlux, p, ar, su):
         args += list(a(x))
     args += [_p(rface), len(rface), float(small)] + ptrs
     args += [int(bool(solveTurbEnergy)), int(bool(solveTurbDiss)), int(bool(solveVisc)), int(bool(solveEnthalpy))]
     for x in (teCell, teBoundary, edCell, edBoundary, viseffCell, viseffBoundary, tCell, tBoundary):
         args += list(a(x))
+    if f32:
+        return lib().cupcfd_gpu_flux_mass_dolfyn_face_loop_f32(*args)
     return lib().cupcfd_gpu_flux_mass_dolfyn_face_loop(*args)
 
 

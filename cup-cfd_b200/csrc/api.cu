@@ -667,20 +667,25 @@ extern "C" int cupcfd_gpu_gradient_phi_gauss_dolfyn(cupcfd_gpu_mesh *m, int32_t 
     return CUPCFD_E_SUCCESS;
 }
 
-extern "C" int cupcfd_gpu_flux_mass_dolfyn_face_loop(
+namespace {
+// FluxMassDolfynFaceLoop over host arrays of the reference's real type T
+// (double: FP64 geometry, bit-identical to T = double; float: the mesh's FP32
+// geometry and the float instantiation's arithmetic, k_mass_full_f32ref).
+template <class T>
+int flux_mass_face_loop_t(
     cupcfd_gpu_mesh *m, cupcfd_vec3_view dudx, int32_t nDudx, cupcfd_vec3_view dvdx, int32_t nDvdx, cupcfd_vec3_view dwdx,
-    int32_t nDwdx, cupcfd_vec3_view dpdx, int32_t nDpdx, const double *den, int32_t nDen, double *denB, int32_t nDenB,
-    const double *u, int32_t nU, const double *v, int32_t nV, const double *w, int32_t nW, double *massFlux,
-    int32_t nMassFlux, const double *p, int32_t nP, const double *ar, int32_t nAr, double *su, int32_t nSu, double *rface,
-    int32_t nRFace, double small, int32_t *icinl, int32_t *icout, int32_t *icsym, int32_t *icwal, int32_t solveTurbEnergy,
-    int32_t solveTurbDiss, int32_t solveVisc, int32_t solveEnthalpy, const double *teC, int32_t nTeC, double *teB,
-    int32_t nTeB, const double *edC, int32_t nEdC, double *edB, int32_t nEdB, const double *visC, int32_t nVisC,
-    double *visB, int32_t nVisB, const double *tC, int32_t nTC, double *tB, int32_t nTB) {
-    clear_error();
+    int32_t nDwdx, cupcfd_vec3_view dpdx, int32_t nDpdx, const T *den, int32_t nDen, T *denB, int32_t nDenB,
+    const T *u, int32_t nU, const T *v, int32_t nV, const T *w, int32_t nW, T *massFlux,
+    int32_t nMassFlux, const T *p, int32_t nP, const T *ar, int32_t nAr, T *su, int32_t nSu, T *rface,
+    int32_t nRFace, T small, int32_t *icinl, int32_t *icout, int32_t *icsym, int32_t *icwal, int32_t solveTurbEnergy,
+    int32_t solveTurbDiss, int32_t solveVisc, int32_t solveEnthalpy, const T *teC, int32_t nTeC, T *teB,
+    int32_t nTeB, const T *edC, int32_t nEdC, T *edB, int32_t nEdB, const T *visC, int32_t nVisC,
+    T *visB, int32_t nVisB, const T *tC, int32_t nTC, T *tB, int32_t nTB) {
+    constexpr bool F64 = sizeof(T) == 8;
     CG_RETURN_IF(!m || !den || !u || !v || !w || !massFlux || !p || !ar || !su || !rface || !icinl || !icout || !icsym ||
                      !icwal,
                  CUPCFD_E_NULL_PTR, "FluxMassDolfynFaceLoop: null argument");
-    CG_TRY(check_prec(m, CUPCFD_PREC_F64));
+    CG_TRY(check_prec(m, F64 ? CUPCFD_PREC_F64 : CUPCFD_PREC_F32C));
     int nC = m->nC, nF = m->nF, nB = m->nB;
     // index checks of the reference's DEBUG build (MassKernels.ipp:101-138, 203-245)
     CG_RETURN_IF(nDudx < nC || nDvdx < nC || nDwdx < nC || nDpdx < nC || nDen < nC || nU < nC || nV < nC || nW < nC ||
@@ -688,8 +693,8 @@ extern "C" int cupcfd_gpu_flux_mass_dolfyn_face_loop(
                  CUPCFD_E_INVALID_INDEX, "FluxMassDolfynFaceLoop: array shorter than the mesh needs");
     bool anyOutlet = false, anyInlet = false;
     for (int t : m->hRegionType) { anyOutlet |= t == CUPCFD_RTYPE_OUTLET; anyInlet |= t == CUPCFD_RTYPE_INLET; }
-    const double *bcI[4] = {teC, edC, visC, tC};
-    double *bcO[4] = {teB, edB, visB, tB};
+    const T *bcI[4] = {teC, edC, visC, tC};
+    T *bcO[4] = {teB, edB, visB, tB};
     int nbcI[4] = {nTeC, nEdC, nVisC, nTC}, nbcO[4] = {nTeB, nEdB, nVisB, nTB};
     int flags = (solveTurbEnergy ? 1 : 0) | (solveTurbDiss ? 2 : 0) | (solveVisc ? 4 : 0) | (solveEnthalpy ? 8 : 0);
     if (anyOutlet)
@@ -703,7 +708,7 @@ extern "C" int cupcfd_gpu_flux_mass_dolfyn_face_loop(
     int64_t ldc = nC;
     unsigned gC = grid_for(nC, BLK), gF = grid_for(nF, BLK);
     // gradients: four packed [3nC] reference arrays -> 12 internal blocks
-    double *grads, *cs, *mf, *rf, *suD, *tmp, *bcIn = nullptr, *bcOut = nullptr, *denBD;
+    T *grads, *cs, *mf, *rf, *suD, *tmp, *bcIn = nullptr, *bcOut = nullptr, *denBD;
     int *cnt;
     CG_TRY(scratch(m, S_IN0, 12 * (size_t) nC, &grads));
     CG_TRY(scratch(m, S_IN1, 6 * (size_t) nC, &cs));
@@ -716,77 +721,116 @@ extern "C" int cupcfd_gpu_flux_mass_dolfyn_face_loop(
     cupcfd_vec3_view vv[4] = {dudx, dvdx, dwdx, dpdx};
     for (int q = 0; q < 4; q++) {
         void *d;
-        CG_TRY(h2d_vec3(m, S_IN3, vv[q], nC, 8, &d));
-        k_aos_to_blocks<double, double><<<gC, BLK, 0, st>>>(nC, 3, m->cellN2O, (const double *) d, grads + 3 * q * ldc, ldc);
+        CG_TRY(h2d_vec3(m, S_IN3, vv[q], nC, (int) sizeof(T), &d));
+        k_aos_to_blocks<T, T><<<gC, BLK, 0, st>>>(nC, 3, m->cellN2O, (const T *) d, grads + 3 * q * ldc, ldc);
         CG_LAUNCHED();
     }
-    const double *cin[6] = {den, u, v, w, p, ar};
+    const T *cin[6] = {den, u, v, w, p, ar};
     for (int q = 0; q < 6; q++) {
-        CG_CHECK_CUDA(cudaMemcpyAsync(tmp, cin[q], sizeof(double) * nC, cudaMemcpyHostToDevice, st));
-        k_gather<double, double><<<gC, BLK, 0, st>>>(nC, 1, m->cellN2O, tmp, 0, cs + q * ldc, 0);
+        CG_CHECK_CUDA(cudaMemcpyAsync(tmp, cin[q], sizeof(T) * nC, cudaMemcpyHostToDevice, st));
+        k_gather<T, T><<<gC, BLK, 0, st>>>(nC, 1, m->cellN2O, tmp, 0, cs + q * ldc, 0);
         CG_LAUNCHED();
     }
     // in/out arrays: massFlux, rface (faces), su (cells), denB (boundaries)
-    CG_CHECK_CUDA(cudaMemcpyAsync(tmp, massFlux, sizeof(double) * nF, cudaMemcpyHostToDevice, st));
-    k_gather<double, double><<<gF, BLK, 0, st>>>(nF, 1, m->faceN2O, tmp, 0, mf, 0);
+    CG_CHECK_CUDA(cudaMemcpyAsync(tmp, massFlux, sizeof(T) * nF, cudaMemcpyHostToDevice, st));
+    k_gather<T, T><<<gF, BLK, 0, st>>>(nF, 1, m->faceN2O, tmp, 0, mf, 0);
     CG_LAUNCHED();
-    CG_CHECK_CUDA(cudaMemcpyAsync(tmp, rface, sizeof(double) * 2 * nF, cudaMemcpyHostToDevice, st));
-    k_gather_pairs<<<gF, BLK, 0, st>>>(nF, m->faceN2O, tmp, rf);
+    CG_CHECK_CUDA(cudaMemcpyAsync(tmp, rface, sizeof(T) * 2 * nF, cudaMemcpyHostToDevice, st));
+    k_gather_pairs<T><<<gF, BLK, 0, st>>>(nF, m->faceN2O, tmp, rf);
     CG_LAUNCHED();
     if (anyInlet) {
-        CG_CHECK_CUDA(cudaMemcpyAsync(tmp, su, sizeof(double) * nC, cudaMemcpyHostToDevice, st));
-        k_gather<double, double><<<gC, BLK, 0, st>>>(nC, 1, m->cellN2O, tmp, 0, suD, 0);
+        CG_CHECK_CUDA(cudaMemcpyAsync(tmp, su, sizeof(T) * nC, cudaMemcpyHostToDevice, st));
+        k_gather<T, T><<<gC, BLK, 0, st>>>(nC, 1, m->cellN2O, tmp, 0, suD, 0);
         CG_LAUNCHED();
     }
     if (anyOutlet && nB > 0) {
-        CG_CHECK_CUDA(cudaMemcpyAsync(denBD, denB, sizeof(double) * nB, cudaMemcpyHostToDevice, st));
+        CG_CHECK_CUDA(cudaMemcpyAsync(denBD, denB, sizeof(T) * nB, cudaMemcpyHostToDevice, st));
         if (flags) {
             CG_TRY(scratch(m, S_IN4, 4 * (size_t) nC, &bcIn));
             CG_TRY(scratch(m, S_OUT4, 4 * (size_t) nB, &bcOut));
             for (int q = 0; q < 4; q++) {
                 if (!(flags & (1 << q))) continue;
-                CG_CHECK_CUDA(cudaMemcpyAsync(tmp, bcI[q], sizeof(double) * nC, cudaMemcpyHostToDevice, st));
-                k_gather<double, double><<<gC, BLK, 0, st>>>(nC, 1, m->cellN2O, tmp, 0, bcIn + q * ldc, 0);
+                CG_CHECK_CUDA(cudaMemcpyAsync(tmp, bcI[q], sizeof(T) * nC, cudaMemcpyHostToDevice, st));
+                k_gather<T, T><<<gC, BLK, 0, st>>>(nC, 1, m->cellN2O, tmp, 0, bcIn + q * ldc, 0);
                 CG_LAUNCHED();
-                CG_CHECK_CUDA(cudaMemcpyAsync(bcOut + (size_t) q * nB, bcO[q], sizeof(double) * nB, cudaMemcpyHostToDevice, st));
+                CG_CHECK_CUDA(cudaMemcpyAsync(bcOut + (size_t) q * nB, bcO[q], sizeof(T) * nB, cudaMemcpyHostToDevice, st));
             }
         }
     }
     CG_CHECK_CUDA(cudaMemsetAsync(cnt, 0, 4 * sizeof(int), st));
-    k_mass_full_f64<<<gF, BLK, 0, st>>>(nF, m->faceCells, m->fg64, m->fc64, m->fxp64, m->fxn64, m->cc64, m->vol, grads, cs, ldc,
-                                        m->bndRegion, m->regionType, m->regionUVW, m->regionDen, small, flags, mf, rf, denBD,
-                                        bcIn, bcOut, nB, cnt);
+    if constexpr (F64)
+        k_mass_full_f64<<<gF, BLK, 0, st>>>(nF, m->faceCells, m->fg64, m->fc64, m->fxp64, m->fxn64, m->cc64, m->vol, grads, cs,
+                                            ldc, m->bndRegion, m->regionType, m->regionUVW, m->regionDen, small, flags, mf, rf,
+                                            denBD, bcIn, bcOut, nB, cnt);
+    else
+        k_mass_full_f32ref<<<gF, BLK, 0, st>>>(nF, m->faceCells, m->fg32, m->fc32, m->fxp64, m->fxn64, m->cc32, m->vol, grads,
+                                               cs, ldc, m->bndRegion, m->regionType, m->regionUVW, m->regionDen, small, flags,
+                                               mf, rf, denBD, bcIn, bcOut, nB, cnt);
     CG_LAUNCHED();
     if (anyInlet) {
-        k_inlet_su<<<gC, BLK, 0, st>>>(nC, sell(m), m->bndRegion, m->regionType, mf, suD);
+        k_inlet_su<T><<<gC, BLK, 0, st>>>(nC, sell(m), m->bndRegion, m->regionType, mf, suD);
         CG_LAUNCHED();
     }
     // back to reference numbering and to the host
-    double *hmf, *hrf;
+    T *hmf, *hrf;
     CG_TRY(scratch(m, S_IN5, (size_t) nF, &hmf));
     CG_TRY(scratch(m, S_IN6, 2 * (size_t) nF, &hrf));
-    k_gather<double, double><<<gF, BLK, 0, st>>>(nF, 1, m->faceO2N, mf, 0, hmf, 0);
+    k_gather<T, T><<<gF, BLK, 0, st>>>(nF, 1, m->faceO2N, mf, 0, hmf, 0);
     CG_LAUNCHED();
-    k_gather_pairs<<<gF, BLK, 0, st>>>(nF, m->faceO2N, rf, hrf);
+    k_gather_pairs<T><<<gF, BLK, 0, st>>>(nF, m->faceO2N, rf, hrf);
     CG_LAUNCHED();
-    CG_CHECK_CUDA(cudaMemcpyAsync(massFlux, hmf, sizeof(double) * nF, cudaMemcpyDeviceToHost, st));
-    CG_CHECK_CUDA(cudaMemcpyAsync(rface, hrf, sizeof(double) * 2 * nF, cudaMemcpyDeviceToHost, st));
+    CG_CHECK_CUDA(cudaMemcpyAsync(massFlux, hmf, sizeof(T) * nF, cudaMemcpyDeviceToHost, st));
+    CG_CHECK_CUDA(cudaMemcpyAsync(rface, hrf, sizeof(T) * 2 * nF, cudaMemcpyDeviceToHost, st));
     if (anyInlet) {
-        k_gather<double, double><<<gC, BLK, 0, st>>>(nC, 1, m->cellO2N, suD, 0, tmp, 0);
+        k_gather<T, T><<<gC, BLK, 0, st>>>(nC, 1, m->cellO2N, suD, 0, tmp, 0);
         CG_LAUNCHED();
-        CG_CHECK_CUDA(cudaMemcpyAsync(su, tmp, sizeof(double) * nC, cudaMemcpyDeviceToHost, st));
+        CG_CHECK_CUDA(cudaMemcpyAsync(su, tmp, sizeof(T) * nC, cudaMemcpyDeviceToHost, st));
     }
     if (anyOutlet && nB > 0) {
-        CG_CHECK_CUDA(cudaMemcpyAsync(denB, denBD, sizeof(double) * nB, cudaMemcpyDeviceToHost, st));
+        CG_CHECK_CUDA(cudaMemcpyAsync(denB, denBD, sizeof(T) * nB, cudaMemcpyDeviceToHost, st));
         for (int q = 0; q < 4; q++)
             if (flags & (1 << q))
-                CG_CHECK_CUDA(cudaMemcpyAsync(bcO[q], bcOut + (size_t) q * nB, sizeof(double) * nB, cudaMemcpyDeviceToHost, st));
+                CG_CHECK_CUDA(cudaMemcpyAsync(bcO[q], bcOut + (size_t) q * nB, sizeof(T) * nB, cudaMemcpyDeviceToHost, st));
     }
     int hc[4];
     CG_CHECK_CUDA(cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, st));
     CG_CHECK_CUDA(cudaStreamSynchronize(st));
     *icinl += hc[0]; *icout += hc[1]; *icsym += hc[2]; *icwal += hc[3];
     return CUPCFD_E_SUCCESS;
+}
+
+}  // namespace
+
+extern "C" int cupcfd_gpu_flux_mass_dolfyn_face_loop(
+    cupcfd_gpu_mesh *m, cupcfd_vec3_view dudx, int32_t nDudx, cupcfd_vec3_view dvdx, int32_t nDvdx, cupcfd_vec3_view dwdx,
+    int32_t nDwdx, cupcfd_vec3_view dpdx, int32_t nDpdx, const double *den, int32_t nDen, double *denB, int32_t nDenB,
+    const double *u, int32_t nU, const double *v, int32_t nV, const double *w, int32_t nW, double *massFlux,
+    int32_t nMassFlux, const double *p, int32_t nP, const double *ar, int32_t nAr, double *su, int32_t nSu, double *rface,
+    int32_t nRFace, double small, int32_t *icinl, int32_t *icout, int32_t *icsym, int32_t *icwal, int32_t solveTurbEnergy,
+    int32_t solveTurbDiss, int32_t solveVisc, int32_t solveEnthalpy, const double *teC, int32_t nTeC, double *teB,
+    int32_t nTeB, const double *edC, int32_t nEdC, double *edB, int32_t nEdB, const double *visC, int32_t nVisC,
+    double *visB, int32_t nVisB, const double *tC, int32_t nTC, double *tB, int32_t nTB) {
+    clear_error();
+    return flux_mass_face_loop_t<double>(m, dudx, nDudx, dvdx, nDvdx, dwdx, nDwdx, dpdx, nDpdx, den, nDen, denB, nDenB, u,
+                                         nU, v, nV, w, nW, massFlux, nMassFlux, p, nP, ar, nAr, su, nSu, rface, nRFace, small,
+                                         icinl, icout, icsym, icwal, solveTurbEnergy, solveTurbDiss, solveVisc, solveEnthalpy,
+                                         teC, nTeC, teB, nTeB, edC, nEdC, edB, nEdB, visC, nVisC, visB, nVisB, tC, nTC, tB, nTB);
+}
+
+extern "C" int cupcfd_gpu_flux_mass_dolfyn_face_loop_f32(
+    cupcfd_gpu_mesh *m, cupcfd_vec3_view dudx, int32_t nDudx, cupcfd_vec3_view dvdx, int32_t nDvdx, cupcfd_vec3_view dwdx,
+    int32_t nDwdx, cupcfd_vec3_view dpdx, int32_t nDpdx, const float *den, int32_t nDen, float *denB, int32_t nDenB,
+    const float *u, int32_t nU, const float *v, int32_t nV, const float *w, int32_t nW, float *massFlux,
+    int32_t nMassFlux, const float *p, int32_t nP, const float *ar, int32_t nAr, float *su, int32_t nSu, float *rface,
+    int32_t nRFace, float small, int32_t *icinl, int32_t *icout, int32_t *icsym, int32_t *icwal, int32_t solveTurbEnergy,
+    int32_t solveTurbDiss, int32_t solveVisc, int32_t solveEnthalpy, const float *teC, int32_t nTeC, float *teB,
+    int32_t nTeB, const float *edC, int32_t nEdC, float *edB, int32_t nEdB, const float *visC, int32_t nVisC,
+    float *visB, int32_t nVisB, const float *tC, int32_t nTC, float *tB, int32_t nTB) {
+    clear_error();
+    return flux_mass_face_loop_t<float>(m, dudx, nDudx, dvdx, nDvdx, dwdx, nDwdx, dpdx, nDpdx, den, nDen, denB, nDenB, u,
+                                        nU, v, nV, w, nW, massFlux, nMassFlux, p, nP, ar, nAr, su, nSu, rface, nRFace, small,
+                                        icinl, icout, icsym, icwal, solveTurbEnergy, solveTurbDiss, solveVisc, solveEnthalpy,
+                                        teC, nTeC, teB, nTeB, edC, nEdC, edB, nEdB, visC, nVisC, visB, nVisB, tC, nTC, tB, nTB);
 }
 
 namespace {

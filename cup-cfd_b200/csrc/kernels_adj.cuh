@@ -618,23 +618,144 @@ __global__ void __launch_bounds__(256) k_mass_full_f64(
     }
 }
 
+// ---------------------------------------------------------------------------
+// FluxMassDolfynFaceLoop of the reference's T = float instantiation
+// (MassKernels.ipp:95-306 with T = float; BenchmarkKernels.cpp:1134-1138
+// instantiates it for CupCfdSoAMesh<int,float,int>), one thread per face:
+// every product, sum and quotient rounds in float in the reference's operand
+// order; facp = 1.0 - facn is evaluated in double and rounded to float (the
+// literal is double); EuclideanVector::dotProduct accumulates from 0 in
+// float; normalise takes the float square root of the float dot product
+// (length() widens sqrtf's result to double, which the float scalar takes
+// back exactly) and multiplies by 1.0f / length (EuclideanVector.cpp:83-109).
+// The comparison massFlux < 0.0 widens to double, which changes nothing.
+// Geometry is the mesh's FP32 copy (exact for a mesh uploaded from float
+// arrays); volumes, xpac / xnac and region values are held in double and
+// hold the float values exactly. Layouts as k_mass_full_f64.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fa(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fs(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float fdot0(float a0, float a1, float a2, float b0, float b1, float b2) {
+    float d = 0.f;
+    d = fa(d, fm(a0, b0));
+    d = fa(d, fm(a1, b1));
+    d = fa(d, fm(a2, b2));
+    return d;
+}
+
+__global__ void __launch_bounds__(256) k_mass_full_f32ref(
+    int nF, const int2 *__restrict__ fcells, const float4 *__restrict__ fg, const float4 *__restrict__ fc,
+    const double4 *__restrict__ fxp, const double4 *__restrict__ fxn, const float4 *__restrict__ cc,
+    const double *__restrict__ vol, const float *__restrict__ grads, const float *__restrict__ cs, int64_t ldc,
+    const int *__restrict__ bndRegion, const int *__restrict__ regionType, const double *__restrict__ regionUVW,
+    const double *__restrict__ regionDen, float small, int flags, float *__restrict__ mflux,
+    float *__restrict__ rface, float *__restrict__ denB, const float *__restrict__ bcIn, float *__restrict__ bcOut,
+    int nB, int *__restrict__ cnt) {
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nF) return;
+    int2 pn = fcells[f];
+    float4 G = fg[f];
+    int ip = pn.x;
+    if (pn.y >= 0) {
+        int in = pn.y;
+        float4 xP = cc[ip], xN = cc[in];
+        float4 X = fc[f];
+        float facn = G.w, facp = (float) (1.0 - (double) facn);
+        const float *du = grads, *dvv = grads + 3 * ldc, *dw = grads + 6 * ldc, *dp = grads + 9 * ldc;
+        float duac[3], dvac[3], dwac[3];
+        for (int d = 0; d < 3; d++) {
+            duac[d] = fa(fm(du[d * ldc + in], facn), fm(du[d * ldc + ip], facp));
+            dvac[d] = fa(fm(dvv[d * ldc + in], facn), fm(dvv[d * ldc + ip], facp));
+            dwac[d] = fa(fm(dw[d * ldc + in], facn), fm(dw[d * ldc + ip], facp));
+        }
+        const float *den = cs, *u = cs + ldc, *v = cs + 2 * ldc, *w = cs + 3 * ldc, *p = cs + 4 * ldc, *ar = cs + 5 * ldc;
+        float denf = fa(fm(den[in], facn), fm(den[ip], facp));
+        float xac0 = fa(fm(xN.x, facn), fm(xP.x, facp));
+        float xac1 = fa(fm(xN.y, facn), fm(xP.y, facp));
+        float xac2 = fa(fm(xN.z, facn), fm(xP.z, facp));
+        float de0 = fs(X.x, xac0), de1 = fs(X.y, xac1), de2 = fs(X.z, xac2);
+        float uF = fa(fa(fm(u[in], facn), fm(u[ip], facp)), fdot0(duac[0], duac[1], duac[2], de0, de1, de2));
+        float vF = fa(fa(fm(v[in], facn), fm(v[ip], facp)), fdot0(dvac[0], dvac[1], dvac[2], de0, de1, de2));
+        float wF = fa(fa(fm(w[in], facn), fm(w[ip], facp)), fdot0(dwac[0], dwac[1], dwac[2], de0, de1, de2));
+        float m = fm(denf, fa(fa(fm(uF, G.x), fm(vF, G.y)), fm(wF, G.z)));
+        float n0 = G.x, n1 = G.y, n2 = G.z;
+        float L = __fsqrt_rn(fdot0(n0, n1, n2, n0, n1, n2));
+        if (L != 0.f) {
+            float sc = __fdiv_rn(1.f, L);
+            n0 = fm(n0, sc); n1 = fm(n1, sc); n2 = fm(n2, sc);
+        }
+        float xa0 = 0, xa1 = 0, xa2 = 0, xb0 = 0, xb1 = 0, xb2 = 0;
+        if (fxp) {
+            double4 a = fxp[f], b = fxn[f];
+            xa0 = (float) a.x; xa1 = (float) a.y; xa2 = (float) a.z;
+            xb0 = (float) b.x; xb1 = (float) b.y; xb2 = (float) b.z;
+        }
+        float dpP0 = dp[ip], dpP1 = dp[ldc + ip], dpP2 = dp[2 * ldc + ip];
+        float pip = fa(p[ip], fdot0(dpP0, dpP1, dpP2, fs(xa0, xP.x), fs(xa1, xP.y), fs(xa2, xP.z)));
+        float pin = fa(p[in], fdot0(dpP0, dpP1, dpP2, fs(xa0, xN.x), fs(xa1, xN.y), fs(xa2, xN.z)));  // dpdx[ip] (MassKernels.ipp:169)
+        float xpn0 = fs(xb0, xa0), xpn1 = fs(xb1, xa1), xpn2 = fs(xb2, xa2);
+        float apv1 = fm(den[ip], ar[ip]);
+        float apv2 = fm(den[in], ar[in]);
+        float apv = fa(fm(apv2, facn), fm(apv1, facp));
+        float factv = fa(fm((float) vol[in], facn), fm((float) vol[ip], facp));
+        apv = fm(apv, __fdiv_rn(fm(X.w, factv), fdot0(fs(xN.x, xP.x), fs(xN.y, xP.y), fs(xN.z, xP.z), n0, n1, n2)));
+        float dpx = fm(fa(fm(dp[in], facn), fm(dpP0, facp)), xpn0);
+        float dpy = fm(fa(fm(dp[ldc + in], facn), fm(dpP1, facp)), xpn1);
+        float dpz = fm(fa(fm(dp[2 * ldc + in], facn), fm(dpP2, facp)), xpn2);
+        rface[2 * (int64_t) f] = -apv;
+        rface[2 * (int64_t) f + 1] = -apv;
+        mflux[f] = fs(m, fm(apv, fs(fs(fs(fs(pin, pip), dpx), dpy), dpz)));
+        return;
+    }
+    int ib = -1 - pn.y;
+    int ir = bndRegion[ib];
+    int it = regionType[ir];
+    if (it == CUPCFD_RTYPE_INLET) {
+        atomicAdd(&cnt[0], 1);
+        float d = fdot0((float) regionUVW[3 * ir], (float) regionUVW[3 * ir + 1], (float) regionUVW[3 * ir + 2], G.x, G.y,
+                        G.z);
+        mflux[f] = fm((float) regionDen[ir], d);
+    } else if (it == CUPCFD_RTYPE_OUTLET) {
+        atomicAdd(&cnt[1], 1);
+        const float *den = cs, *u = cs + ldc, *v = cs + 2 * ldc, *w = cs + 3 * ldc;
+        float denf = den[ip];
+        denB[ib] = denf;
+        float m = fm(denf, fa(fa(fm(u[ip], G.x), fm(v[ip], G.y)), fm(w[ip], G.z)));
+        if (m < 0.f) {
+            m = small;
+            for (int q = 0; q < 4; q++)
+                if (flags & (1 << q)) bcOut[(int64_t) q * nB + ib] = bcIn[q * ldc + ip];
+        }
+        mflux[f] = m;
+    } else if (it == CUPCFD_RTYPE_SYMP) {
+        atomicAdd(&cnt[2], 1);
+        mflux[f] = 0.f;
+    } else if (it == CUPCFD_RTYPE_WALL) {
+        atomicAdd(&cnt[3], 1);
+        mflux[f] = 0.f;
+    }
+}
+
 // su[ip] -= massFlux over the cell's inlet faces in ascending reference face
-// id (MassKernels.ipp:258), one thread per cell.
+// id (MassKernels.ipp:258), one thread per cell; T double or float (each
+// subtraction rounds in T).
+template <class T>
 __global__ void __launch_bounds__(256) k_inlet_su(int nC, SellView sv, const int *__restrict__ bndRegion,
-                                                  const int *__restrict__ regionType, const double *__restrict__ mflux,
-                                                  double *__restrict__ su) {
+                                                  const int *__restrict__ regionType, const T *__restrict__ mflux,
+                                                  T *__restrict__ su) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nC) return;
     int w;
     const int2 *e = cell_entries(sv, c, w);
-    double v = su[c];
+    T v = su[c];
     bool touched = false;
     for (int k = 0; k < w; k++) {
         int2 en = e[32 * k];
         if (en.x < 0) break;
         if (en.y >= 0) continue;
         if (regionType[bndRegion[-1 - en.y]] != CUPCFD_RTYPE_INLET) continue;
-        v = ds(v, mflux[en.x >> 1]);
+        v = v - mflux[en.x >> 1];
         touched = true;
     }
     if (touched) su[c] = v;

@@ -75,7 +75,8 @@ __global__ void k_convert(int64_t n, const TS *__restrict__ a, TD *__restrict__ 
 }
 
 // rface pairs: dst[2i], dst[2i+1] = src[2 map[i]], src[2 map[i]+1]
-__global__ void k_gather_pairs(int n, const int *__restrict__ map, const double *__restrict__ src, double *__restrict__ dst) {
+template <class T>
+__global__ void k_gather_pairs(int n, const int *__restrict__ map, const T *__restrict__ src, T *__restrict__ dst) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int j = map[i];

@@ -283,7 +283,7 @@ extern "C" int cupcfd_gpu_flux_uvw_dolfyn_face_loop1(
     k_gather<double, double><<<grid_for(nF, BT), BT, 0, st>>>(nF, 1, m->faceN2O, tmp, 0, mf, 0);
     CG_LAUNCHED();
     CG_TRY(up(tmp, rFace, sizeof(double) * 2 * nF, st));
-    k_gather_pairs<<<grid_for(nF, BT), BT, 0, st>>>(nF, m->faceN2O, tmp, rf);
+    k_gather_pairs<double><<<grid_for(nF, BT), BT, 0, st>>>(nF, m->faceN2O, tmp, rf);
     CG_LAUNCHED();
     // boundaries (same ids on both sides): uB vB wB visB
     double *hb[4] = {uB, vB, wB, const_cast<double *>(visB)};
@@ -297,7 +297,7 @@ extern "C" int cupcfd_gpu_flux_uvw_dolfyn_face_loop1(
     k_gather<double, double><<<grid_for(nF, BT), BT, 0, st>>>(nF, 1, m->faceO2N, mf, 0, tmp, 0);
     CG_LAUNCHED();
     CG_TRY(down(massFlux, tmp, sizeof(double) * nF, st));
-    k_gather_pairs<<<grid_for(nF, BT), BT, 0, st>>>(nF, m->faceO2N, rf, tmp);
+    k_gather_pairs<double><<<grid_for(nF, BT), BT, 0, st>>>(nF, m->faceO2N, rf, tmp);
     CG_LAUNCHED();
     CG_TRY(down(rFace, tmp, sizeof(double) * 2 * nF, st));
     double *cout_[6] = {su, sv, sw, au, av, aw};

@@ -343,6 +343,30 @@ int cupcfd_gpu_flux_mass_dolfyn_face_loop(cupcfd_gpu_mesh *mesh,
                                           const double *viseffCell, int32_t nViseffCell, double *viseffBoundary, int32_t nViseffBoundary,
                                           const double *tCell, int32_t nTCell, double *tBoundary, int32_t nTBoundary);
 
+/* FluxMassDolfynFaceLoop of the reference's T = float instantiation
+ * (BenchmarkKernels.cpp:1134-1138 instantiates the kernels for
+ * CupCfdSoAMesh<int,float,int>): the same parameters with float arrays and
+ * EuclideanVector<float,3> views (24-byte stride, components at +8), and the
+ * float instantiation's own arithmetic (float products and sums in the
+ * reference's order; 1.0 - lambda in double, rounded to float), on the
+ * mesh's FP32 geometry, which a mesh uploaded from float arrays holds
+ * exactly. Results are those of the reference's float build bit for bit.
+ * The mesh must have CUPCFD_PREC_F32C geometry. */
+int cupcfd_gpu_flux_mass_dolfyn_face_loop_f32(cupcfd_gpu_mesh *mesh,
+                                              cupcfd_vec3_view dudx, int32_t nDudx, cupcfd_vec3_view dvdx, int32_t nDvdx,
+                                              cupcfd_vec3_view dwdx, int32_t nDwdx, cupcfd_vec3_view dpdx, int32_t nDpdx,
+                                              const float *denCell, int32_t nDenCell, float *denBoundary, int32_t nDenBoundary,
+                                              const float *uCell, int32_t nUCell, const float *vCell, int32_t nVCell,
+                                              const float *wCell, int32_t nWCell, float *massFlux, int32_t nMassFlux,
+                                              const float *p, int32_t nP, const float *ar, int32_t nAr,
+                                              float *su, int32_t nSu, float *rface, int32_t nRFace, float small,
+                                              int32_t *icinl, int32_t *icout, int32_t *icsym, int32_t *icwal,
+                                              int32_t solveTurbEnergy, int32_t solveTurbDiss, int32_t solveVisc, int32_t solveEnthalpy,
+                                              const float *teCell, int32_t nTeCell, float *teBoundary, int32_t nTeBoundary,
+                                              const float *edCell, int32_t nEdCell, float *edBoundary, int32_t nEdBoundary,
+                                              const float *viseffCell, int32_t nViseffCell, float *viseffBoundary, int32_t nViseffBoundary,
+                                              const float *tCell, int32_t nTCell, float *tBoundary, int32_t nTBoundary);
+
 /* Forward + adjoint of the plain face loops through host buffers (the
  * benchmark's end-to-end call). Inputs (host, reference numbering, FP64):
  * phi[nCells], phiB[nBoundaries], den/u/v/w[nCells], gface[nFaces] (loss

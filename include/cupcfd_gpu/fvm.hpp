@@ -2,7 +2,8 @@
 //
 // Same names and parameter lists as the reference's templates
 //   cupcfd::fvm::GradientPhiGaussDolfyn  (include/fvm/implementation/component/GradientKernels.h:48-54)
-//   cupcfd::fvm::FluxMassDolfynFaceLoop  (include/fvm/implementation/component/MassKernels.h:48-81)
+//   cupcfd::fvm::FluxMassDolfynFaceLoop  (include/fvm/implementation/component/MassKernels.h:48-81),
+//                                        for T = double and T = float meshes
 //   cupcfd::fvm::FluxMassDolfynBoundaryLoop1-5, FluxMassDolfynRegionLoop (MassKernels.h:90-171)
 //   cupcfd::fvm::FluxUVWDolfynFaceLoop1, FluxUVWDolfynRegionLoop1, FluxUVWDolfynBndsLoop1
 //                                        (include/fvm/implementation/component/UVWKernels.h:45-92)
@@ -281,6 +282,34 @@ ecode_t FluxMassDolfynFaceLoop(Mesh &mesh, Vec *dudx, I nDudx, Vec *dvdx, I nDvd
     int rc = attach(mesh, &m);
     if (rc != CUPCFD_E_SUCCESS) return (ecode_t) rc;
     rc = cupcfd_gpu_flux_mass_dolfyn_face_loop(
+        m, detail::view_of(dudx), nDudx, detail::view_of(dvdx), nDvdx, detail::view_of(dwdx), nDwdx,
+        detail::view_of(dpdx), nDpdx, denCell, nDenCell, denBoundary, nDenBoundary, uCell, nUCell, vCell, nVCell,
+        wCell, nWCell, massFlux, nMassFlux, p, nP, ar, nAr, su, nSu, rface, nRFace, small, (int32_t *) icinl,
+        (int32_t *) icout, (int32_t *) icsym, (int32_t *) icwal, solveTurbEnergy, solveTurbDiss, solveVisc,
+        solveEnthalpy, teCell, nTeCell, teBoundary, nTeBoundary, edCell, nEdCell, edBoundary, nEdBoundary,
+        viseffCell, nViseffCell, viseffBoundary, nViseffBoundary, tCell, nTCell, tBoundary, nTBoundary);
+    return (ecode_t) rc;
+}
+
+// FluxMassDolfynFaceLoop, T = float: the reference's float instantiation
+// (BenchmarkKernels.cpp:1134-1138) on a CupCfdSoAMesh<int,float,int>, with
+// its arithmetic (cupcfd_gpu_flux_mass_dolfyn_face_loop_f32)
+template <class Mesh, class I, class Vec>
+ecode_t FluxMassDolfynFaceLoop(Mesh &mesh, Vec *dudx, I nDudx, Vec *dvdx, I nDvdx, Vec *dwdx, I nDwdx, Vec *dpdx,
+                               I nDpdx, float *denCell, I nDenCell, float *denBoundary, I nDenBoundary,
+                               float *uCell, I nUCell, float *vCell, I nVCell, float *wCell, I nWCell,
+                               float *massFlux, I nMassFlux, float *p, I nP, float *ar, I nAr, float *su, I nSu,
+                               float *rface, I nRFace, float small, I *icinl, I *icout, I *icsym, I *icwal,
+                               bool solveTurbEnergy, bool solveTurbDiss, bool solveVisc, bool solveEnthalpy,
+                               float *teCell, I nTeCell, float *teBoundary, I nTeBoundary, float *edCell,
+                               I nEdCell, float *edBoundary, I nEdBoundary, float *viseffCell, I nViseffCell,
+                               float *viseffBoundary, I nViseffBoundary, float *tCell, I nTCell, float *tBoundary,
+                               I nTBoundary) {
+    static_assert(sizeof(I) == 4, "int32 indices");
+    cupcfd_gpu_mesh *m = nullptr;
+    int rc = attach(mesh, &m);
+    if (rc != CUPCFD_E_SUCCESS) return (ecode_t) rc;
+    rc = cupcfd_gpu_flux_mass_dolfyn_face_loop_f32(
         m, detail::view_of(dudx), nDudx, detail::view_of(dvdx), nDvdx, detail::view_of(dwdx), nDwdx,
         detail::view_of(dpdx), nDpdx, denCell, nDenCell, denBoundary, nDenBoundary, uCell, nUCell, vCell, nVCell,
         wCell, nWCell, massFlux, nMassFlux, p, nP, ar, nAr, su, nSu, rface, nRFace, small, (int32_t *) icinl,

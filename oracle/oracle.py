@@ -114,6 +114,34 @@ def ref_gradient_f32(m, phi, phiB, nGradient):
     return g, go
 
 
+def ref_flux_mass_f32(m, f):
+    """FluxMassDolfynFaceLoop of the reference's T=float instantiation
+    (compiled unchanged) on mesh ``m`` with its geometry and regions rounded
+    to float, fields ``f`` (as fields(full=True)) rounded to float. Returns
+    (rc, out) like flux_mass_face_loop, out arrays float32."""
+    ref = load_ref()
+    assert ref is not None, "reference build absent"
+    f32 = lambda x: np.ascontiguousarray(np.asarray(x).reshape(-1), np.float32)
+    i32 = lambda x: np.ascontiguousarray(x, np.int32)
+    nC, nF, nB, nR = int(m["nCells"]), int(m["nFaces"]), int(m["nBnd"]), int(m["nRegions"])
+    geo = [i32(m["faceCell1"]), i32(m["faceCell2"]), i32(m["faceBnd"])] + [
+        f32(m[k]) for k in ("faceLambda", "faceNorm", "faceCenter", "faceArea", "faceXpac", "faceXnac", "cellCenter",
+                            "cellVolume")] + [i32(m["bndRegion"]), i32(m["regionType"]), f32(m["regionUVW"]), f32(m["regionDen"])]
+    a = {k: f32(f[k]) for k in ("dudx", "dvdx", "dwdx", "dpdx", "den", "u", "v", "w", "p", "ar", "teC", "edC", "visC", "tC")}
+    out = {k: f32(f[k]).copy() for k in ("massFlux", "su", "rface", "denB", "teB", "edB", "visB", "tB")}
+    cnt = [C.c_int(int(f.get(k, 0))) for k in ("icinl", "icout", "icsym", "icwal")]
+    fn = ref.ref_flux_mass_face_loop_f32
+    fn.argtypes = [C.c_int] * 4 + [C.c_void_p] * 29 + [C.c_float] + [C.c_void_p] * 4 + [C.c_int] * 4 + [C.c_void_p] * 8
+    rc = fn(nC, nF, nB, nR, *[_p(x) for x in geo], _p(a["dudx"]), _p(a["dvdx"]), _p(a["dwdx"]), _p(a["dpdx"]),
+            _p(a["den"]), _p(out["denB"]), _p(a["u"]), _p(a["v"]), _p(a["w"]), _p(out["massFlux"]), _p(a["p"]),
+            _p(a["ar"]), _p(out["su"]), _p(out["rface"]), float(np.float32(f["small"])), *[C.byref(c) for c in cnt],
+            *[int(bool(f.get(k, False))) for k in ("solveTurbEnergy", "solveTurbDiss", "solveVisc", "solveEnthalpy")],
+            _p(a["teC"]), _p(out["teB"]), _p(a["edC"]), _p(out["edB"]), _p(a["visC"]), _p(out["visB"]), _p(a["tC"]),
+            _p(out["tB"]))
+    out.update(icinl=cnt[0].value, icout=cnt[1].value, icsym=cnt[2].value, icwal=cnt[3].value)
+    return rc, out
+
+
 # ---------------------------------------------------------------------------
 # meshes
 # ---------------------------------------------------------------------------

@@ -285,6 +285,60 @@ extern "C" int ref_gradient_phi_gauss_f32(int nCells, int nFaces, int nBnd, cons
 	return (int) st;
 }
 
+/* FluxMassDolfynFaceLoop of the reference's T=float instantiation on a float
+ * mesh given by its arrays (xyz-interleaved vectors), regions included;
+ * vector fields [3*nCells]; in/out arrays updated in place as the reference
+ * does. */
+extern "C" int ref_flux_mass_face_loop_f32(int nCells, int nFaces, int nBnd, int nRegions, const int * faceCell1,
+                                           const int * faceCell2, const int * faceBnd, const float * faceLambda,
+                                           const float * faceNorm, const float * faceCenter, const float * faceArea,
+                                           const float * faceXpac, const float * faceXnac, const float * cellCenter,
+                                           const float * cellVolume, const int * bndRegion, const int * regionType,
+                                           const float * regionUVW, const float * regionDen,
+                                           const float * dudx, const float * dvdx, const float * dwdx, const float * dpdx,
+                                           float * den, float * denB, float * u, float * v, float * w,
+                                           float * massFlux, float * pr, float * ar, float * su, float * rface,
+                                           float small, int * icinl, int * icout, int * icsym, int * icwal,
+                                           int solveTurbEnergy, int solveTurbDiss, int solveVisc, int solveEnthalpy,
+                                           float * teC, float * teB, float * edC, float * edB,
+                                           float * visC, float * visB, float * tC, float * tB) {
+	RefMeshF mesh;
+	mesh.properties.lOCells = nCells;
+	mesh.properties.lGhCells = 0;
+	mesh.properties.lTCells = nCells;
+	mesh.properties.lFaces = nFaces;
+	mesh.properties.lBoundaries = nBnd;
+	mesh.properties.lRegions = nRegions;
+	mesh.a = {};
+	mesh.a.faceCell1 = faceCell1;
+	mesh.a.faceCell2 = faceCell2;
+	mesh.a.faceBoundary = faceBnd;
+	mesh.a.faceLambda = faceLambda;
+	mesh.a.faceNorm = faceNorm;
+	mesh.a.faceCenter = faceCenter;
+	mesh.a.faceArea = faceArea;
+	mesh.a.faceXpac = faceXpac;
+	mesh.a.faceXnac = faceXnac;
+	mesh.a.cellCenter = cellCenter;
+	mesh.a.cellVolume = cellVolume;
+	mesh.a.boundaryRegion = bndRegion;
+	mesh.a.regionType = regionType;
+	mesh.a.regionUVW = regionUVW;
+	mesh.a.regionDen = regionDen;
+	std::vector<euc::EuclideanVector<float,3>> gu(nCells), gv(nCells), gw(nCells), gp(nCells);
+	for (int i = 0; i < nCells; i++)
+		for (int d = 0; d < 3; d++) {
+			gu[i].cmp[d] = dudx[3*i+d]; gv[i].cmp[d] = dvdx[3*i+d];
+			gw[i].cmp[d] = dwdx[3*i+d]; gp[i].cmp[d] = dpdx[3*i+d];
+		}
+	return (int) cupcfd::fvm::FluxMassDolfynFaceLoop(mesh,
+		gu.data(), nCells, gv.data(), nCells, gw.data(), nCells, gp.data(), nCells,
+		den, nCells, denB, nBnd, u, nCells, v, nCells, w, nCells, massFlux, nFaces, pr, nCells, ar, nCells, su, nCells,
+		rface, 2 * nFaces, small, icinl, icout, icsym, icwal,
+		solveTurbEnergy != 0, solveTurbDiss != 0, solveVisc != 0, solveEnthalpy != 0,
+		teC, nCells, teB, nBnd, edC, nCells, edB, nBnd, visC, nCells, visB, nBnd, tC, nCells, tB, nBnd);
+}
+
 /* Runs FluxMassDolfynFaceLoop `reps` times with the reference's full
  * argument list. Vector fields are xyz-interleaved [3*nCells]. The arrays
  * massFlux, su, rface, denB and the te/ed/viseff/t boundary arrays are

@@ -243,6 +243,51 @@ def test_mass_full_f64_bit_exact(cg, gpu, order, regions, jit):
         assert o[k] == o_ref[k], k
 
 
+@pytest.mark.parametrize("order", [1, 3])
+@pytest.mark.parametrize("jit", [False, True])
+@pytest.mark.parametrize("xpac", [False, True])
+def test_mass_float_instantiation_bit_exact(cg, gpu, order, jit, xpac):
+    """FluxMassDolfynFaceLoop with T=float arrays on a mesh uploaded from float
+    arrays against the reference's own T=float instantiation (compiled
+    unchanged): every output bit for bit, with all four region types, the
+    outlet backflow copies and (xpac) nonzero xpac / xnac."""
+    if O.load_ref() is None:
+        pytest.skip("reference build absent")
+    ref = O.jitter(9, 7, 8, 0.25, seed=2, permute=True) if jit else O.structgen(9, 7, 8)
+    ref = dict(ref)
+    rng = np.random.default_rng(81)
+    ref["nRegions"] = 5
+    ref["regionType"] = np.array([0, 1, 2, 3, 4], np.int32)
+    ref["regionUVW"] = rng.standard_normal((5, 3))
+    ref["regionDen"] = rng.uniform(0.5, 1.5, 5)
+    ref["bndRegion"] = rng.integers(0, 5, ref["nBnd"]).astype(np.int32)
+    if xpac:
+        ref["faceXpac"] = np.asarray(ref["faceCenter"]) + 0.01 * rng.standard_normal((ref["nFaces"], 3))
+        ref["faceXnac"] = np.asarray(ref["faceCenter"]) + 0.01 * rng.standard_normal((ref["nFaces"], 3))
+    m32 = dict(ref)
+    for k in ("faceLambda", "faceArea", "faceNorm", "faceCenter", "faceXpac", "faceXnac", "cellCenter", "cellVolume",
+              "regionUVW", "regionDen"):
+        m32[k] = np.ascontiguousarray(np.asarray(ref[k]), np.float32)
+    mesh = cg.Mesh.from_arrays(m32, order=order)
+    assert mesh.set_regions(ref["regionType"], m32["regionUVW"].astype(np.float64), m32["regionDen"].astype(np.float64),
+                            ref["bndRegion"]) == cg.E_SUCCESS
+    f = O.fields(ref, 82, full=True)
+    f["massFlux"] = rng.standard_normal(ref["nFaces"])   # boundary entries must survive
+    f["solveTurbEnergy"] = f["solveTurbDiss"] = f["solveEnthalpy"] = True
+    f32 = {k: (np.ascontiguousarray(v, np.float32) if isinstance(v, np.ndarray) else v) for k, v in f.items()}
+    rc, want = O.ref_flux_mass_f32(m32, f32)
+    out = {k: np.array(f32[k], np.float32, copy=True) for k in ("massFlux", "su", "rface", "denB", "teB", "edB", "visB", "tB")}
+    cnt = np.zeros(4, np.int32)
+    rc2 = cg.FluxMassDolfynFaceLoop(mesh, f32["dudx"], f32["dvdx"], f32["dwdx"], f32["dpdx"], f32["den"], out["denB"],
+                                    f32["u"], f32["v"], f32["w"], out["massFlux"], f32["p"], f32["ar"], out["su"],
+                                    out["rface"], np.float32(f["small"]), cnt, True, True, True, True, f32["teC"],
+                                    out["teB"], f32["edC"], out["edB"], f32["visC"], out["visB"], f32["tC"], out["tB"])
+    assert rc == rc2 == cg.E_SUCCESS, cg.last_error()
+    for k in ("massFlux", "su", "rface", "denB", "teB", "edB", "visB", "tB"):
+        assert np.array_equal(out[k].view(np.int32), want[k].view(np.int32)), k
+    assert list(cnt) == [want["icinl"], want["icout"], want["icsym"], want["icwal"]]
+    assert want["icinl"] > 0 and want["icout"] > 0 and want["icsym"] > 0 and want["icwal"] > 0
+
 # ---------------------------------------------------------------------------
 # FP32-compensated path: error bounds against the FP64 oracle
 # ---------------------------------------------------------------------------
