@@ -120,6 +120,7 @@ SIGNATURES = {
     "cupcfd_gpu_mesh_boundary_shear": ([_VP, _VP, _VP, _I], _I),
     "cupcfd_gpu_mesh_region_force_tangent": ([_VP, _VP, _VP, _I], _I),
     "cupcfd_gpu_flux_uvw_dolfyn_face_loop1": ([_VP, _D, _D] + [_VP, _I] * 9 + [Vec3View, _I] * 3 + [_VP, _I] * 7, _I),
+    "cupcfd_gpu_flux_uvw_dolfyn_face_loop1_f32": ([_VP, C.c_float, C.c_float] + [_VP, _I] * 9 + [Vec3View, _I] * 3 + [_VP, _I] * 7, _I),
     "cupcfd_gpu_flux_uvw_dolfyn_region_loop1": ([_VP], _I),
     "cupcfd_gpu_flux_uvw_dolfyn_bnds_loop1": ([_VP], _I),
     "cupcfd_gpu_dev_uvw_face_loop1": ([_VP, _D, _D] + [_VP] * 10 + [_I64] + [_VP] * 8, _I),
@@ -629,19 +630,25 @@ def dev_region_loop(mesh, flowFact, flowRegion, flowIn, stream=None):
 def FluxUVWDolfynFaceLoop1(mesh, gammaBlend, small, uCell, vCell, wCell, uBoundary, vBoundary, wBoundary, visEffCell,
                            visEffBoundary, massFlux, dudx, dvdx, dwdx, rFace, su, sv, sw, au, av, aw):
     """Mirror of cupcfd::fvm::FluxUVWDolfynFaceLoop1 (UVWKernels.h:45-67) on
-    host FP64 arrays in the reference's numbering; in/out arrays (boundary
+    host arrays in the reference's numbering; in/out arrays (boundary
     velocities, massFlux, rFace, su..aw) are updated in place; dudx/dvdx/dwdx
-    are (n,3) or (n,4) (leading pad slot). Returns an eCodes value."""
+    are (n,3) or (n,4) (leading pad slot). float32 arrays run the reference's
+    T = float instantiation, float64 arrays T = double. Returns an eCodes
+    value."""
+    f32 = np.asarray(uCell).dtype == np.float32
+
     def a(x):
         return [_p(x), 0 if x is None else len(x)]
     args = [mesh.h, float(gammaBlend), float(small)]
     for x in (uCell, vCell, wCell, uBoundary, vBoundary, wBoundary, visEffCell, visEffBoundary, massFlux):
         args += a(x)
     for vv in (dudx, dvdx, dwdx):
-        args += [_vec(vv), len(vv)]
+        args += [_vec(vv, 4 if f32 else 8), len(vv)]
     args += a(rFace)
     for x in (su, sv, sw, au, av, aw):
         args += a(x)
+    if f32:
+        return lib().cupcfd_gpu_flux_uvw_dolfyn_face_loop1_f32(*args)
     return lib().cupcfd_gpu_flux_uvw_dolfyn_face_loop1(*args)
 
 

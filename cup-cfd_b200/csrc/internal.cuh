@@ -91,6 +91,7 @@ struct cupcfd_gpu_mesh {
     int nC = 0, nF = 0, nB = 0, nFi = 0, nR = 0;
     int nInc = 0, maxDeg = 0;
     int order = 0, precisions = 0;
+    int realSize = 8;           // bytes of the real type the source arrays held (4: a T = float mesh)
     bool xpacZero = true;       // all xpac = xnac = 0 (meshes built through a MeshSource)
     bool allDefaultRegions = true;
 

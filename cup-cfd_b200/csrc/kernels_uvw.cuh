@@ -33,64 +33,120 @@
 
 namespace cupcfd_gpu {
 
+// Arithmetic of the two instantiations the reference compiles
+// (BenchmarkKernels.cpp:1134-1138), one IEEE rounding per operator:
+//   T = double: FP64 throughout.
+//   T = float:  float throughout, except where the float build widens:
+//     facp = 1.0 - facn (double literal, then rounded to float), 2.0 * visac
+//     (double, exact, then float), and the wall's fabs(ut0) + fabs(ut1) +
+//     fabs(ut2) (the C library's double fabs in the reference's scope, a
+//     double sum rounded once to float). normalise() and the wall's
+//     xpn.length() take the float square root of the float dot product
+//     (length() widens sqrtf's result to double and the float scalar takes it
+//     back exactly; EuclideanVector.cpp:93-109).
+template <class T>
+struct UvwReal;
+template <>
+struct UvwReal<double> {
+    using V4 = double4;
+    static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+    static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+    static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+    static __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
+    static __device__ __forceinline__ double sqrt_(double a) { return __dsqrt_rn(a); }
+    static __device__ __forceinline__ double one_minus(double x) { return __dsub_rn(1.0, x); }
+    static __device__ __forceinline__ double twice(double x) { return __dmul_rn(2.0, x); }
+    static __device__ __forceinline__ double abs_sum3(double a, double b, double c) {
+        return __dadd_rn(__dadd_rn(fabs(a), fabs(b)), fabs(c));
+    }
+};
+template <>
+struct UvwReal<float> {
+    using V4 = float4;
+    static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+    static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+    static __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+    static __device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
+    static __device__ __forceinline__ float sqrt_(float a) { return __fsqrt_rn(a); }
+    static __device__ __forceinline__ float one_minus(float x) { return (float) __dsub_rn(1.0, (double) x); }
+    static __device__ __forceinline__ float twice(float x) { return (float) __dmul_rn(2.0, (double) x); }
+    static __device__ __forceinline__ float abs_sum3(float a, float b, float c) {
+        return (float) __dadd_rn(__dadd_rn(fabs((double) a), fabs((double) b)), fabs((double) c));
+    }
+};
+
 // std::min / std::max of <algorithm>: min(a,b) = b < a ? b : a,
 // max(a,b) = a < b ? b : a (the first argument wins ties and NaN compares).
-__device__ __forceinline__ double std_min(double a, double b) { return (b < a) ? b : a; }
-__device__ __forceinline__ double std_max(double a, double b) { return (a < b) ? b : a; }
+template <class T>
+__device__ __forceinline__ T std_min(T a, T b) { return (b < a) ? b : a; }
+template <class T>
+__device__ __forceinline__ T std_max(T a, T b) { return (a < b) ? b : a; }
 
 // EuclideanVector::dotProduct (EuclideanVector.cpp:83-90): accumulated from 0.
-__device__ __forceinline__ double dot0(double a0, double a1, double a2, double b0, double b1, double b2) {
-    double d = 0.0;
-    d = da(d, dm(a0, b0));
-    d = da(d, dm(a1, b1));
-    d = da(d, dm(a2, b2));
+template <class T>
+__device__ __forceinline__ T dot0(T a0, T a1, T a2, T b0, T b1, T b2) {
+    using R = UvwReal<T>;
+    T d = T(0);
+    d = R::add(d, R::mul(a0, b0));
+    d = R::add(d, R::mul(a1, b1));
+    d = R::add(d, R::mul(a2, b2));
     return d;
 }
 
 // EuclideanVector::normalise (EuclideanVector.cpp:100-109)
-__device__ __forceinline__ void normalise(double &x, double &y, double &z) {
-    double L = __dsqrt_rn(dot0(x, y, z, x, y, z));
-    if (L != 0.0) {
-        double sc = dvd(1.0, L);
-        x = dm(x, sc); y = dm(y, sc); z = dm(z, sc);
+template <class T>
+__device__ __forceinline__ void normalise(T &x, T &y, T &z) {
+    using R = UvwReal<T>;
+    T L = R::sqrt_(dot0(x, y, z, x, y, z));
+    if (L != T(0)) {
+        T sc = R::div(T(1), L);
+        x = R::mul(x, sc); y = R::mul(y, sc); z = R::mul(z, sc);
     }
 }
 
+// Face geometry is the mesh's FP64 copy for T = double and its FP32 copy for
+// T = float (exact for a mesh uploaded from float arrays); rlencos, boundary
+// distances and region values are held in double (the float values exactly)
+// and the boundary shears are written to the mesh's double array.
+template <class T>
 struct UvwArgs {
+    using V4 = typename UvwReal<T>::V4;
     int nC;
     SellView sv;
     const int2 *fcells;
-    const double4 *fg, *fc, *cc;           // {S, lambda}, {x_f, area}, {x_c, 0}
+    const V4 *fg, *fc, *cc;                // {S, lambda}, {x_f, area}, {x_c, 0}
     const int *bndRegion, *regionType;
     const double *regionUVW;
     const double *rlencos;                 // [nF] internal, null = zero
     const double *bndDist;                 // [nB], null = zero
     const int *carry;                      // [nF] internal; null when no region is an inlet, outlet or symmetry
-    double gammaBlend, small;
-    const double *u, *v, *w, *visC;        // [nC] internal
-    const double *visB;                    // [nB]
-    const double *grads;                   // 9 blocks [ldg]: dudx xyz, dvdx xyz, dwdx xyz
+    T gammaBlend, small;
+    const T *u, *v, *w, *visC;             // [nC] internal
+    const T *visB;                         // [nB]
+    const T *grads;                        // 9 blocks [ldg]: dudx xyz, dvdx xyz, dwdx xyz
     int64_t ldg;
-    double *uB, *vB, *wB;                  // [nB]
-    double *massFlux, *rFace;              // [nF], [2 nF] internal
+    T *uB, *vB, *wB;                       // [nB]
+    T *massFlux, *rFace;                   // [nF], [2 nF] internal
     double *shear;                         // [3 nB]
-    double *su, *sv_, *sw, *au, *av, *aw;  // [nC] internal
+    T *su, *sv_, *sw, *au, *av, *aw;       // [nC] internal
 };
 
 // visFace that face g leaves behind (interior, inlet and outlet faces set it,
 // UVWKernels.ipp:160, 274, 335).
-__device__ __forceinline__ double vis_face_of(const UvwArgs &a, int g) {
+template <class T>
+__device__ __forceinline__ T vis_face_of(const UvwArgs<T> &a, int g) {
+    using R = UvwReal<T>;
     int2 pn = a.fcells[g];
-    double rl = a.rlencos ? a.rlencos[g] : 0.0;
-    double visac;
+    T rl = a.rlencos ? (T) a.rlencos[g] : T(0);
+    T visac;
     if (pn.y >= 0) {
-        double facn = a.fg[g].w, facp = ds(1.0, facn);
-        visac = da(dm(a.visC[pn.y], facn), dm(a.visC[pn.x], facp));
+        T facn = a.fg[g].w, facp = R::one_minus(facn);
+        visac = R::add(R::mul(a.visC[pn.y], facn), R::mul(a.visC[pn.x], facp));
     } else {
         int ib = -1 - pn.y;
         visac = a.regionType[a.bndRegion[ib]] == CUPCFD_RTYPE_INLET ? a.visB[ib] : a.visC[pn.x];
     }
-    return dm(visac, rl);
+    return R::mul(visac, rl);
 }
 
 // How an incidence's terms update its cell (t[0..9] from uvw_terms), in the
@@ -105,53 +161,59 @@ enum UvwKind : int {
 
 // The terms one incidence (entry en of cell c) contributes to its cell, and
 // the face's own outputs when c owns the face. Returns the UvwKind.
-__device__ __forceinline__ int uvw_terms(const UvwArgs &a, int c, int2 en, double (&t)[10]) {
+template <class T>
+__device__ __forceinline__ int uvw_terms(const UvwArgs<T> &a, int c, int2 en, T (&t)[10]) {
+    using R = UvwReal<T>;
+    using V4 = typename UvwReal<T>::V4;
     const int64_t L = a.ldg;
     auto gr = [&](int q, int cell) { return a.grads[q * L + cell]; };
     const int f = en.x >> 1;
     const bool owner = (en.x & 1) == 0;
-    const double4 G = a.fg[f];
-    const double rl = a.rlencos ? a.rlencos[f] : 0.0;
+    const V4 G = a.fg[f];
+    const T rl = a.rlencos ? (T) a.rlencos[f] : T(0);
     if (en.y >= 0) {
         // interior face (UVWKernels.ipp:145-228)
         const int ip = owner ? c : en.y, in = owner ? en.y : c;
-        const double facn = G.w, facp = ds(1.0, facn);
-        double du[3], dv[3], dw[3];
+        const T facn = G.w, facp = R::one_minus(facn);
+        T du[3], dv[3], dw[3];
 #pragma unroll
         for (int d = 0; d < 3; d++) {
-            du[d] = da(dm(gr(d, in), facn), dm(gr(d, ip), facp));
-            dv[d] = da(dm(gr(3 + d, in), facn), dm(gr(3 + d, ip), facp));
-            dw[d] = da(dm(gr(6 + d, in), facn), dm(gr(6 + d, ip), facp));
+            du[d] = R::add(R::mul(gr(d, in), facn), R::mul(gr(d, ip), facp));
+            dv[d] = R::add(R::mul(gr(3 + d, in), facn), R::mul(gr(3 + d, ip), facp));
+            dw[d] = R::add(R::mul(gr(6 + d, in), facn), R::mul(gr(6 + d, ip), facp));
         }
-        const double visac = da(dm(a.visC[in], facn), dm(a.visC[ip], facp));
-        const double4 Cn = a.cc[in], Cp = a.cc[ip];
-        const double x0 = ds(Cn.x, Cp.x), x1 = ds(Cn.y, Cp.y), x2 = ds(Cn.z, Cp.z);
-        const double visFace = dm(visac, rl);
-        double uF = 0.0, vF = 0.0, wF = 0.0;
+        const T visac = R::add(R::mul(a.visC[in], facn), R::mul(a.visC[ip], facp));
+        const V4 Cn = a.cc[in], Cp = a.cc[ip];
+        const T x0 = R::sub(Cn.x, Cp.x), x1 = R::sub(Cn.y, Cp.y), x2 = R::sub(Cn.z, Cp.z);
+        const T visFace = R::mul(visac, rl);
+        T uF = T(0), vF = T(0), wF = T(0);
         const int cr = a.carry ? a.carry[f] : -1;
         if (cr >= 0) {
             uF = a.u[cr]; vF = a.v[cr]; wF = a.w[cr];
         } else if (cr <= -2) {
             const double *r = a.regionUVW + 3 * (-2 - cr);
-            uF = r[0]; vF = r[1]; wF = r[2];
+            uF = (T) r[0]; vF = (T) r[1]; wF = (T) r[2];
         }
-        const double mf = a.massFlux[f];
-        const double fmin = std_min(mf, 0.0), fmax = std_max(mf, 0.0);
-        const double fuci = da(dm(fmin, a.u[in]), dm(fmax, a.u[ip]));
-        const double fvci = da(dm(fmin, a.v[in]), dm(fmax, a.v[ip]));
-        const double fwci = da(dm(fmin, a.w[in]), dm(fmax, a.w[ip]));
-        t[0] = dm(a.gammaBlend, ds(dm(mf, uF), fuci));
-        t[3] = dm(a.gammaBlend, ds(dm(mf, vF), fvci));
-        t[6] = dm(a.gammaBlend, ds(dm(mf, wF), fwci));
-        t[1] = dm(visac, da(da(dm(da(du[0], du[0]), G.x), dm(da(du[1], dv[0]), G.y)), dm(da(du[2], dw[0]), G.z)));
-        t[4] = dm(visac, da(da(dm(da(du[1], dv[0]), G.x), dm(da(dv[1], dv[1]), G.y)), dm(da(dv[2], dw[1]), G.z)));
-        t[7] = dm(visac, da(da(dm(da(du[2], dw[0]), G.x), dm(da(dw[1], dv[2]), G.y)), dm(da(dw[2], dw[2]), G.z)));
-        t[2] = dm(visFace, dot0(du[0], du[1], du[2], x0, x1, x2));
-        t[5] = dm(visFace, dot0(dv[0], dv[1], dv[2], x0, x1, x2));
-        t[8] = dm(visFace, dot0(dw[0], dw[1], dw[2], x0, x1, x2));
+        const T mf = a.massFlux[f];
+        const T fmin = std_min(mf, T(0)), fmax = std_max(mf, T(0));
+        const T fuci = R::add(R::mul(fmin, a.u[in]), R::mul(fmax, a.u[ip]));
+        const T fvci = R::add(R::mul(fmin, a.v[in]), R::mul(fmax, a.v[ip]));
+        const T fwci = R::add(R::mul(fmin, a.w[in]), R::mul(fmax, a.w[ip]));
+        t[0] = R::mul(a.gammaBlend, R::sub(R::mul(mf, uF), fuci));
+        t[3] = R::mul(a.gammaBlend, R::sub(R::mul(mf, vF), fvci));
+        t[6] = R::mul(a.gammaBlend, R::sub(R::mul(mf, wF), fwci));
+        t[1] = R::mul(visac, R::add(R::add(R::mul(R::add(du[0], du[0]), G.x), R::mul(R::add(du[1], dv[0]), G.y)),
+                                    R::mul(R::add(du[2], dw[0]), G.z)));
+        t[4] = R::mul(visac, R::add(R::add(R::mul(R::add(du[1], dv[0]), G.x), R::mul(R::add(dv[1], dv[1]), G.y)),
+                                    R::mul(R::add(dv[2], dw[1]), G.z)));
+        t[7] = R::mul(visac, R::add(R::add(R::mul(R::add(du[2], dw[0]), G.x), R::mul(R::add(dw[1], dv[2]), G.y)),
+                                    R::mul(R::add(dw[2], dw[2]), G.z)));
+        t[2] = R::mul(visFace, dot0(du[0], du[1], du[2], x0, x1, x2));
+        t[5] = R::mul(visFace, dot0(dv[0], dv[1], dv[2], x0, x1, x2));
+        t[8] = R::mul(visFace, dot0(dw[0], dw[1], dw[2], x0, x1, x2));
         if (owner) {
-            a.rFace[2 * (int64_t) f] = ds(-visFace, std_max(mf, 0.0));
-            a.rFace[2 * (int64_t) f + 1] = da(-visFace, std_min(mf, 0.0));
+            a.rFace[2 * (int64_t) f] = R::sub(-visFace, std_max(mf, T(0)));
+            a.rFace[2 * (int64_t) f + 1] = R::add(-visFace, std_min(mf, T(0)));
         }
         return owner ? UVW_OWNER : UVW_NEIGH;
     }
@@ -160,84 +222,88 @@ __device__ __forceinline__ int uvw_terms(const UvwArgs &a, int c, int2 en, doubl
     const int ir = a.bndRegion[ib];
     const int it = a.regionType[ir];
     if (it == CUPCFD_RTYPE_DEFAULT) return UVW_NONE;
-    const double4 X = a.fc[f], Cp = a.cc[c];
-    const double x0 = ds(X.x, Cp.x), x1 = ds(X.y, Cp.y), x2 = ds(X.z, Cp.z);
-    const double uc = a.u[c], vc = a.v[c], wc = a.w[c];
-    const double du0 = gr(0, c), du1 = gr(1, c), du2 = gr(2, c);
-    const double dv0 = gr(3, c), dv1 = gr(4, c), dv2 = gr(5, c);
-    const double dw0 = gr(6, c), dw1 = gr(7, c), dw2 = gr(8, c);
+    const V4 X = a.fc[f], Cp = a.cc[c];
+    const T x0 = R::sub(X.x, Cp.x), x1 = R::sub(X.y, Cp.y), x2 = R::sub(X.z, Cp.z);
+    const T uc = a.u[c], vc = a.v[c], wc = a.w[c];
+    const T du0 = gr(0, c), du1 = gr(1, c), du2 = gr(2, c);
+    const T dv0 = gr(3, c), dv1 = gr(4, c), dv2 = gr(5, c);
+    const T dw0 = gr(6, c), dw1 = gr(7, c), dw2 = gr(8, c);
     if (it == CUPCFD_RTYPE_INLET || it == CUPCFD_RTYPE_OUTLET) {
         // UVWKernels.ipp:259-382 (outlet: operands of two sums swapped,
         // which IEEE addition does not see)
-        double uF, vF, wF, visac;
+        T uF, vF, wF, visac;
         if (it == CUPCFD_RTYPE_INLET) {
             const double *r = a.regionUVW + 3 * ir;
-            uF = r[0]; vF = r[1]; wF = r[2];
+            uF = (T) r[0]; vF = (T) r[1]; wF = (T) r[2];
             visac = a.visB[ib];
         } else {
             uF = uc; vF = vc; wF = wc;
             visac = a.visC[c];
         }
-        const double visFace = dm(visac, rl);
-        double mf = a.massFlux[f];
-        if (it == CUPCFD_RTYPE_OUTLET && mf < 0.0) {
+        const T visFace = R::mul(visac, rl);
+        T mf = a.massFlux[f];
+        if (it == CUPCFD_RTYPE_OUTLET && mf < T(0)) {
             mf = a.small;
             a.massFlux[f] = mf;
         }
-        const double fl = da(-visFace, std_min(mf, 0.0));
-        t[0] = dm(fl, uF); t[3] = dm(fl, vF); t[6] = dm(fl, wF);
-        t[1] = dm(visac, da(da(dm(da(du0, du0), G.x), dm(da(du1, dv0), G.y)), dm(da(du2, dw0), G.z)));
-        t[4] = dm(visac, da(da(dm(da(du1, dv0), G.x), dm(da(dv1, dv1), G.y)), dm(da(dv2, dw1), G.z)));
-        t[7] = dm(visac, da(da(dm(da(du2, dw0), G.x), dm(da(dw1, dv2), G.y)), dm(da(dw2, dw2), G.z)));
-        t[2] = dm(visFace, dot0(du0, du1, du2, x0, x1, x2));
-        t[5] = dm(visFace, dot0(dv0, dv1, dv2, x0, x1, x2));
-        t[8] = dm(visFace, dot0(dw0, dw1, dw2, x0, x1, x2));
+        const T fl = R::add(-visFace, std_min(mf, T(0)));
+        t[0] = R::mul(fl, uF); t[3] = R::mul(fl, vF); t[6] = R::mul(fl, wF);
+        t[1] = R::mul(visac, R::add(R::add(R::mul(R::add(du0, du0), G.x), R::mul(R::add(du1, dv0), G.y)),
+                                    R::mul(R::add(du2, dw0), G.z)));
+        t[4] = R::mul(visac, R::add(R::add(R::mul(R::add(du1, dv0), G.x), R::mul(R::add(dv1, dv1), G.y)),
+                                    R::mul(R::add(dv2, dw1), G.z)));
+        t[7] = R::mul(visac, R::add(R::add(R::mul(R::add(du2, dw0), G.x), R::mul(R::add(dw1, dv2), G.y)),
+                                    R::mul(R::add(dw2, dw2), G.z)));
+        t[2] = R::mul(visFace, dot0(du0, du1, du2, x0, x1, x2));
+        t[5] = R::mul(visFace, dot0(dv0, dv1, dv2, x0, x1, x2));
+        t[8] = R::mul(visFace, dot0(dw0, dw1, dw2, x0, x1, x2));
         t[9] = fl;
         a.uB[ib] = uF; a.vB[ib] = vF; a.wB[ib] = wF;
         return UVW_INOUT;
     }
-    const double area = X.w;
-    double Xc, f0 = 0.0, f1 = 0.0, f2 = 0.0;
+    const T area = X.w;
+    T Xc, f0 = T(0), f1 = T(0), f2 = T(0);
     if (it == CUPCFD_RTYPE_SYMP) {
         // UVWKernels.ipp:383-436; visFace carried from an earlier face
         const int g = a.carry ? a.carry[f] : -1;
-        Xc = g >= 0 ? vis_face_of(a, g) : 0.0;
-        const double visac = a.visC[c];
-        const double us0 = da(uc, dot0(du0, du1, du2, x0, x1, x2));
-        const double us1 = da(vc, dot0(dv0, dv1, dv2, x0, x1, x2));
-        const double us2 = da(wc, dot0(dw0, dw1, dw2, x0, x1, x2));
-        double n0 = ds(0.0, G.x), n1 = ds(0.0, G.y), n2 = ds(0.0, G.z);
+        Xc = g >= 0 ? vis_face_of(a, g) : T(0);
+        const T visac = a.visC[c];
+        const T us0 = R::add(uc, dot0(du0, du1, du2, x0, x1, x2));
+        const T us1 = R::add(vc, dot0(dv0, dv1, dv2, x0, x1, x2));
+        const T us2 = R::add(wc, dot0(dw0, dw1, dw2, x0, x1, x2));
+        T n0 = R::sub(T(0), G.x), n1 = R::sub(T(0), G.y), n2 = R::sub(T(0), G.z);
         normalise(n0, n1, n2);
-        const double dp = dot0(us0, us1, us2, n0, n1, n2);
-        const double dn = a.bndDist ? a.bndDist[ib] : 0.0;
-        const double tv = dm(2.0, visac);
-        f0 = dm(dvd(dm(tv, dm(dp, n0)), dn), area);
-        f1 = dm(dvd(dm(tv, dm(dp, n1)), dn), area);
-        f2 = dm(dvd(dm(tv, dm(dp, n2)), dn), area);
+        const T dp = dot0(us0, us1, us2, n0, n1, n2);
+        const T dn = a.bndDist ? (T) a.bndDist[ib] : T(0);
+        const T tv = R::twice(visac);
+        f0 = R::mul(R::div(R::mul(tv, R::mul(dp, n0)), dn), area);
+        f1 = R::mul(R::div(R::mul(tv, R::mul(dp, n1)), dn), area);
+        f2 = R::mul(R::div(R::mul(tv, R::mul(dp, n2)), dn), area);
         a.uB[ib] = us0; a.vB[ib] = us1; a.wB[ib] = us2;
     } else {
         // wall, UVWKernels.ipp:437-510
         const double *uw = a.regionUVW + 3 * ir;
-        const double visac = a.visB[ib];
-        Xc = dvd(dm(visac, area), __dsqrt_rn(dot0(x0, x1, x2, x0, x1, x2)));
-        double n0 = G.x, n1 = G.y, n2 = G.z;
+        const T uw0 = (T) uw[0], uw1 = (T) uw[1], uw2 = (T) uw[2];
+        const T visac = a.visB[ib];
+        Xc = R::div(R::mul(visac, area), R::sqrt_(dot0(x0, x1, x2, x0, x1, x2)));
+        T n0 = G.x, n1 = G.y, n2 = G.z;
         normalise(n0, n1, n2);
-        const double up0 = ds(uc, uw[0]), up1 = ds(vc, uw[1]), up2 = ds(wc, uw[2]);
-        const double dp = dot0(up0, up1, up2, n0, n1, n2);
-        const double ut0 = ds(up0, dm(dp, n0)), ut1 = ds(up1, dm(dp, n1)), ut2 = ds(up2, dm(dp, n2));
-        const double uvel = da(da(fabs(ut0), fabs(ut1)), fabs(ut2));
+        const T up0 = R::sub(uc, uw0), up1 = R::sub(vc, uw1), up2 = R::sub(wc, uw2);
+        const T dp = dot0(up0, up1, up2, n0, n1, n2);
+        const T ut0 = R::sub(up0, R::mul(dp, n0)), ut1 = R::sub(up1, R::mul(dp, n1)), ut2 = R::sub(up2, R::mul(dp, n2));
+        const T uvel = R::abs_sum3(ut0, ut1, ut2);
         if (uvel > a.small) {
-            const double dn = a.bndDist ? a.bndDist[ib] : 0.0;
-            f0 = dm(dvd(dm(visac, ut0), dn), area);
-            f1 = dm(dvd(dm(visac, ut1), dn), area);
-            f2 = dm(dvd(dm(visac, ut2), dn), area);
+            const T dn = a.bndDist ? (T) a.bndDist[ib] : T(0);
+            f0 = R::mul(R::div(R::mul(visac, ut0), dn), area);
+            f1 = R::mul(R::div(R::mul(visac, ut1), dn), area);
+            f2 = R::mul(R::div(R::mul(visac, ut2), dn), area);
         }
-        a.shear[3 * (int64_t) ib] = f0;
-        a.shear[3 * (int64_t) ib + 1] = f1;
-        a.shear[3 * (int64_t) ib + 2] = f2;
-        a.uB[ib] = uw[0]; a.vB[ib] = uw[1]; a.wB[ib] = uw[2];
+        a.shear[3 * (int64_t) ib] = (double) f0;
+        a.shear[3 * (int64_t) ib + 1] = (double) f1;
+        a.shear[3 * (int64_t) ib + 2] = (double) f2;
+        a.uB[ib] = uw0; a.vB[ib] = uw1; a.wB[ib] = uw2;
     }
-    t[0] = dm(Xc, uc); t[3] = dm(Xc, vc); t[6] = dm(Xc, wc);
+    t[0] = R::mul(Xc, uc); t[3] = R::mul(Xc, vc); t[6] = R::mul(Xc, wc);
     t[1] = f0; t[4] = f1; t[7] = f2;
     t[9] = Xc;
     return UVW_WALLSYM;
@@ -245,28 +311,30 @@ __device__ __forceinline__ int uvw_terms(const UvwArgs &a, int c, int2 en, doubl
 
 // Applies one incidence's terms to the cell's running su/sv/sw (s) and
 // au/av/aw (ad).
-__device__ __forceinline__ void uvw_fold(int kind, const double (&t)[10], double (&s)[3], double (&ad)[3]) {
+template <class T>
+__device__ __forceinline__ void uvw_fold(int kind, const T (&t)[10], T (&s)[3], T (&ad)[3]) {
+    using R = UvwReal<T>;
     switch (kind) {
     case UVW_OWNER:
 #pragma unroll
-        for (int q = 0; q < 3; q++) s[q] = ds(da(ds(s[q], t[3 * q]), t[3 * q + 1]), t[3 * q + 2]);
+        for (int q = 0; q < 3; q++) s[q] = R::sub(R::add(R::sub(s[q], t[3 * q]), t[3 * q + 1]), t[3 * q + 2]);
         break;
     case UVW_NEIGH:
 #pragma unroll
-        for (int q = 0; q < 3; q++) s[q] = da(ds(da(s[q], t[3 * q]), t[3 * q + 1]), t[3 * q + 2]);
+        for (int q = 0; q < 3; q++) s[q] = R::add(R::sub(R::add(s[q], t[3 * q]), t[3 * q + 1]), t[3 * q + 2]);
         break;
     case UVW_INOUT:
 #pragma unroll
         for (int q = 0; q < 3; q++) {
-            ad[q] = ds(ad[q], t[9]);
-            s[q] = ds(da(ds(s[q], t[3 * q]), t[3 * q + 1]), t[3 * q + 2]);
+            ad[q] = R::sub(ad[q], t[9]);
+            s[q] = R::sub(R::add(R::sub(s[q], t[3 * q]), t[3 * q + 1]), t[3 * q + 2]);
         }
         break;
     case UVW_WALLSYM:
 #pragma unroll
         for (int q = 0; q < 3; q++) {
-            ad[q] = da(ad[q], t[9]);
-            s[q] = ds(da(s[q], t[3 * q]), t[3 * q + 1]);
+            ad[q] = R::add(ad[q], t[9]);
+            s[q] = R::sub(R::add(s[q], t[3 * q]), t[3 * q + 1]);
         }
         break;
     default:
@@ -283,17 +351,18 @@ __device__ __forceinline__ void uvw_fold(int kind, const double (&t)[10], double
 #ifndef UVW_CHUNK
 #define UVW_CHUNK 6      // incidence entries loaded ahead (a hexahedral cell in one chunk)
 #endif
-__device__ __forceinline__ void uvw_cell(const UvwArgs &a, int c) {
+template <class T>
+__device__ __forceinline__ void uvw_cell(const UvwArgs<T> &a, int c) {
     int wdt;
     const int2 *e = cell_entries(a.sv, c, wdt);
-    double s[3] = {a.su[c], a.sv_[c], a.sw[c]}, ad[3] = {a.au[c], a.av[c], a.aw[c]};
+    T s[3] = {a.su[c], a.sv_[c], a.sw[c]}, ad[3] = {a.au[c], a.av[c], a.aw[c]};
     // the chunk's entries first (independent loads), then incidence by incidence
     for (int k0 = 0; k0 < wdt; k0 += UVW_CHUNK) {
         int2 en[UVW_CHUNK];
         load_entries<UVW_CHUNK>(e, k0, wdt, en);
         for (int j = 0; j < UVW_CHUNK; j++) {
             if (en[j].x < 0) break;
-            double t[10];
+            T t[10];
             int kind = uvw_terms(a, c, en[j], t);
             uvw_fold(kind, t, s, ad);
         }
@@ -302,22 +371,17 @@ __device__ __forceinline__ void uvw_cell(const UvwArgs &a, int c) {
     a.au[c] = ad[0]; a.av[c] = ad[1]; a.aw[c] = ad[2];
 }
 
-__global__ void __launch_bounds__(256, UVW_CELL_MINB) k_uvw_f64(const __grid_constant__ UvwArgs a) {
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c < a.nC) uvw_cell(a, c);
-}
-
 // The same with the L2 prefetch of the tile one wave of this kernel's
 // resident blocks ahead (prefetch.cuh): its entries, face records and mass
 // fluxes, and its cells' entries in the twenty cell arrays the loop reads.
 // Needs the owner-sorted face order, 256-thread blocks and 16-byte aligned
-// arrays. 2.13 ms at 256^3 against 2.21 ms without the prefetch.
-__global__ void __launch_bounds__(TILE_CELLS, UVW_CELL_MINB) k_uvw_f64_pf(const __grid_constant__ UvwArgs a,
-                                                                          PrefetchArgs pf) {
-    constexpr int T = TILE_CELLS;
-    const int c = blockIdx.x * T + threadIdx.x;
+// arrays.
+template <class T>
+__device__ __forceinline__ void uvw_cell_pf(const UvwArgs<T> &a, const PrefetchArgs &pf) {
+    constexpr int TC = TILE_CELLS;
+    const int c = blockIdx.x * TC + threadIdx.x;
     const int tp = blockIdx.x + pf.dist;
-    const bool lead = threadIdx.x == T - 32 && tp < pf.nTiles;
+    const bool lead = threadIdx.x == TC - 32 && tp < pf.nTiles;
     __shared__ int4 s_rng;
     if (lead) fetch_ranges_async(&s_rng, pf.desc + tp);
     if (c < a.nC) uvw_cell(a, c);
@@ -328,10 +392,31 @@ __global__ void __launch_bounds__(TILE_CELLS, UVW_CELL_MINB) k_uvw_f64_pf(const 
                                          a.grads + 5 * L, a.grads + 6 * L, a.grads + 7 * L, a.grads + 8 * L, a.cc};
         int cellBytes[20];
 #pragma unroll
-        for (int i = 0; i < 19; i++) cellBytes[i] = T * 8;
-        cellBytes[19] = T * 32;
-        prefetch_tile<20>(pf, tp, ranges_ready(&s_rng), a.fg, 32, (const double *) a.massFlux, cellSrc, cellBytes);
+        for (int i = 0; i < 19; i++) cellBytes[i] = TC * (int) sizeof(T);
+        cellBytes[19] = TC * (int) sizeof(typename UvwReal<T>::V4);
+        prefetch_tile<20>(pf, tp, ranges_ready(&s_rng), a.fg, (int) sizeof(typename UvwReal<T>::V4),
+                          (const T *) a.massFlux, cellSrc, cellBytes);
     }
+}
+
+// FP64 (the reference's T = double): plain and L2-prefetch launches.
+// 2.13 ms at 256^3 with the prefetch against 2.21 ms without.
+__global__ void __launch_bounds__(256, UVW_CELL_MINB) k_uvw_f64(const __grid_constant__ UvwArgs<double> a) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < a.nC) uvw_cell(a, c);
+}
+__global__ void __launch_bounds__(TILE_CELLS, UVW_CELL_MINB) k_uvw_f64_pf(const __grid_constant__ UvwArgs<double> a,
+                                                                          PrefetchArgs pf) {
+    uvw_cell_pf(a, pf);
+}
+// The reference's T = float instantiation.
+__global__ void __launch_bounds__(256, UVW_CELL_MINB) k_uvw_f32ref(const __grid_constant__ UvwArgs<float> a) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < a.nC) uvw_cell(a, c);
+}
+__global__ void __launch_bounds__(TILE_CELLS, UVW_CELL_MINB) k_uvw_f32ref_pf(const __grid_constant__ UvwArgs<float> a,
+                                                                             PrefetchArgs pf) {
+    uvw_cell_pf(a, pf);
 }
 
 // ---------------------------------------------------------------------------

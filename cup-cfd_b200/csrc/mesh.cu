@@ -895,6 +895,7 @@ extern "C" int cupcfd_gpu_mesh_create(const cupcfd_mesh_view *v, const cupcfd_me
         set_error(e);
         return rc;
     }
+    m->realSize = rs;
     *out = m;
     return CUPCFD_E_SUCCESS;
 }

@@ -12,7 +12,9 @@
 // 32 + j region j's accumulators, each reading the dense values a block-sized
 // batch at a time from shared memory. A chain costs one dependent add per
 // selected boundary, against a shared-memory round trip and a branch per
-// boundary when one thread walked all of them.
+// boundary when one thread walked all of them. F32: the chains add in float
+// (the reference's T = float instantiation); values and accumulators stay in
+// double arrays, which hold the float values exactly.
 //
 // Kernels and helpers sit in an unnamed namespace (at file scope, as in
 // perm.cuh): each translation unit that includes this header gets its own
@@ -116,7 +118,7 @@ __global__ void __launch_bounds__(SEL_T) k_sel_write(SelArgs a, const double *__
 // loads its entry of the next batch into registers before the chains of the
 // current batch run, and stores it after them, so the loads' latency hides
 // behind the chains and a batch costs one barrier.
-template <int NV>
+template <int NV, bool F32 = false>
 __global__ void __launch_bounds__(SEL_T) k_sel_sum(const int *__restrict__ total, const double *__restrict__ vals,
                                                    const int *__restrict__ regs, const double *init, double initValue,
                                                    double *out, double *regionAcc, int nR, int r0) {
@@ -153,13 +155,15 @@ __global__ void __launch_bounds__(SEL_T) k_sel_sum(const int *__restrict__ total
         const int *cr = sr[buf];
         if (doTotal) {
 #pragma unroll 16
-            for (int j = 0; j < n; j++) acc = __dadd_rn(acc, cv[NV * j]);
+            for (int j = 0; j < n; j++) acc = F32 ? (double) __fadd_rn((float) acc, (float) cv[NV * j]) : __dadd_rn(acc, cv[NV * j]);
         } else if (myR >= 0) {
 #pragma unroll 8
             for (int j = 0; j < n; j++)
                 if (cr[j] == myR) {
 #pragma unroll
-                    for (int q = 0; q < NV; q++) racc[q] = __dadd_rn(racc[q], cv[NV * j + q]);
+                    for (int q = 0; q < NV; q++)
+                        racc[q] = F32 ? (double) __fadd_rn((float) racc[q], (float) cv[NV * j + q])
+                                      : __dadd_rn(racc[q], cv[NV * j + q]);
                 }
         }
         if (hasNext) {
@@ -179,7 +183,7 @@ __global__ void __launch_bounds__(SEL_T) k_sel_sum(const int *__restrict__ total
 
 // The four passes. Scratch: cnt [nB / SEL_T + 2] ints, vals [NV nB]
 // doubles, regs [nB] ints. out may be init (the sum continues from it).
-template <int NV>
+template <int NV, bool F32 = false>
 int launch_ordered_sum(const SelArgs &a, const double *base, int stride, int offset, const int *map,
                        const double *init, double initValue, double *out, double *regionAcc, int nR, int *cnt,
                        double *vals, int *regs, cudaStream_t st) {
@@ -196,7 +200,7 @@ int launch_ordered_sum(const SelArgs &a, const double *base, int stride, int off
     }
     const int groups = regionAcc ? std::max(1, (nR + SEL_REGIONS - 1) / SEL_REGIONS) : 1;
     for (int g = 0; g < groups; g++) {
-        k_sel_sum<NV><<<1, SEL_T, 0, st>>>(cnt + nBlk, vals, regs, g == 0 ? init : nullptr, initValue,
+        k_sel_sum<NV, F32><<<1, SEL_T, 0, st>>>(cnt + nBlk, vals, regs, g == 0 ? init : nullptr, initValue,
                                            g == 0 ? out : nullptr, regionAcc, nR, g * SEL_REGIONS);
         CG_LAUNCHED();
     }

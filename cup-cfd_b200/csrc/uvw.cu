@@ -30,10 +30,13 @@ int slot(cupcfd_gpu_mesh *m, int s, size_t n, T **p) {
     return CUPCFD_E_SUCCESS;
 }
 
-int check_mesh(const cupcfd_gpu_mesh *m) {
+// geomPrec: the geometry the call reads (FP64 for T = double, FP32 for the
+// float instantiation)
+int check_mesh(const cupcfd_gpu_mesh *m, int geomPrec = CUPCFD_PREC_F64) {
     CG_RETURN_IF(!m, CUPCFD_E_NULL_PTR, "momentum loop: null mesh");
-    CG_RETURN_IF(!(m->precisions & (1 << CUPCFD_PREC_F64)), CUPCFD_E_CONFIG_INVALID_VALUE,
-                 "momentum loop: the mesh was created without FP64 geometry");
+    CG_RETURN_IF(!(m->precisions & (1 << geomPrec)), CUPCFD_E_CONFIG_INVALID_VALUE,
+                 geomPrec == CUPCFD_PREC_F64 ? "momentum loop: the mesh was created without FP64 geometry"
+                                             : "momentum loop: the mesh was created without FP32 geometry");
     CG_RETURN_IF(!m->bndMapsOk, CUPCFD_E_INVALID_INDEX,
                  "momentum loop: the mesh's boundary ids are not a permutation of 0 .. nBoundaries-1");
     return make_device_current(m->device);
@@ -79,34 +82,40 @@ bool prefetch_disabled() {
     return off;
 }
 
-// Prefetch distance of k_uvw_f64_pf: one wave of its resident blocks
-// (SMs x blocks per SM), the measured optimum (2.13 ms at 256^3 against
-// 2.35-2.39 ms for 1/3 to 4/3 of a wave; CUPCFD_PREFETCH_DIST overrides).
-int prefetch_wave(int device) {
+// Prefetch distance of the L2-prefetch kernel `kern`: one wave of its
+// resident blocks (SMs x blocks per SM), the measured optimum for
+// k_uvw_f64_pf (2.13 ms at 256^3 against 2.35-2.39 ms for 1/3 to 4/3 of a
+// wave; CUPCFD_PREFETCH_DIST overrides).
+int prefetch_wave(int device, const void *kern) {
     static std::mutex mu;
-    static std::map<int, int> wave;
+    static std::map<std::pair<int, const void *>, int> wave;
     std::lock_guard<std::mutex> g(mu);
-    auto it = wave.find(device);
+    auto it = wave.find({device, kern});
     if (it != wave.end()) return it->second;
     int sms = 148, blocks = UVW_CELL_MINB;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_uvw_f64_pf, TILE_CELLS, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kern, TILE_CELLS, 0);
     int d = std::max(1, sms * std::max(1, blocks));
     if (const char *e = std::getenv("CUPCFD_PREFETCH_DIST")) if (*e) d = std::max(1, std::atoi(e));
-    wave[device] = d;
+    wave[{device, kern}] = d;
     return d;
 }
 
-int run_face_loop(cupcfd_gpu_mesh *m, double gammaBlend, double small, const double *u, const double *v,
-                  const double *w, double *uB, double *vB, double *wB, const double *visC, const double *visB,
-                  double *massFlux, const double *grads, int64_t ldg, double *rFace, double *su, double *sv, double *sw,
-                  double *au, double *av, double *aw, cudaStream_t st) {
+template <class T>
+int run_face_loop(cupcfd_gpu_mesh *m, T gammaBlend, T small, const T *u, const T *v, const T *w, T *uB, T *vB, T *wB,
+                  const T *visC, const T *visB, T *massFlux, const T *grads, int64_t ldg, T *rFace, T *su, T *sv,
+                  T *sw, T *au, T *av, T *aw, cudaStream_t st) {
+    constexpr bool F64 = sizeof(T) == 8;
     CG_TRY(ensure_state(m, st));
-    UvwArgs a;
+    UvwArgs<T> a;
     a.nC = m->nC;
     a.sv = SellView{m->sell.slicePtr, m->sell.inc, m->sell.width};
     a.fcells = m->faceCells;
-    a.fg = m->fg64; a.fc = m->fc64; a.cc = m->cc64;
+    if constexpr (F64) {
+        a.fg = m->fg64; a.fc = m->fc64; a.cc = m->cc64;
+    } else {
+        a.fg = m->fg32; a.fc = m->fc32; a.cc = m->cc32;
+    }
     a.bndRegion = m->bndRegion; a.regionType = m->regionType; a.regionUVW = m->regionUVW;
     // the carried values matter only with an inlet, outlet or symmetry region
     bool carried = false;
@@ -125,7 +134,7 @@ int run_face_loop(cupcfd_gpu_mesh *m, double gammaBlend, double small, const dou
     auto a16 = [](const void *p) { return ((uintptr_t) p & 15u) == 0; };
     const bool pfOk = m->tiles && m->tileDesc && a16(u) && a16(v) && a16(w) && a16(visC) &&
                       a16(su) && a16(sv) && a16(sw) && a16(au) && a16(av) && a16(aw) && a16(grads) &&
-                      (ldg % 2) == 0 && a16(massFlux) && !prefetch_disabled();
+                      (ldg * (int64_t) sizeof(T)) % 16 == 0 && a16(massFlux) && !prefetch_disabled();
     if (pfOk) {
         PrefetchArgs pf;
         pf.desc = (const TileDesc *) m->tileDesc;
@@ -133,10 +142,18 @@ int run_face_loop(cupcfd_gpu_mesh *m, double gammaBlend, double small, const dou
         pf.nC = m->nC;
         pf.nF = m->nF;
         pf.nTiles = m->nTiles;
-        pf.dist = prefetch_wave(m->device);
-        k_uvw_f64_pf<<<grid_for(m->nC, TILE_CELLS), TILE_CELLS, 0, st>>>(a, pf);
+        if constexpr (F64) {
+            pf.dist = prefetch_wave(m->device, (const void *) k_uvw_f64_pf);
+            k_uvw_f64_pf<<<grid_for(m->nC, TILE_CELLS), TILE_CELLS, 0, st>>>(a, pf);
+        } else {
+            pf.dist = prefetch_wave(m->device, (const void *) k_uvw_f32ref_pf);
+            k_uvw_f32ref_pf<<<grid_for(m->nC, TILE_CELLS), TILE_CELLS, 0, st>>>(a, pf);
+        }
     } else {
-        k_uvw_f64<<<grid_for(m->nC, BT), BT, 0, st>>>(a);
+        if constexpr (F64)
+            k_uvw_f64<<<grid_for(m->nC, BT), BT, 0, st>>>(a);
+        else
+            k_uvw_f32ref<<<grid_for(m->nC, BT), BT, 0, st>>>(a);
     }
     CG_LAUNCHED();
     return CUPCFD_E_SUCCESS;
@@ -151,28 +168,32 @@ int down(void *h, const void *d, size_t bytes, cudaStream_t st) {
     return CUPCFD_E_SUCCESS;
 }
 
-// reference-numbered [n] double array (3 per element when vec) on the host
+// reference-numbered [n] array of T (3 per element when vec) on the host
 // -> device, then to internal order
-int cells_in(cupcfd_gpu_mesh *m, const double *h, double *dst, double *tmp, cudaStream_t st) {
-    CG_TRY(up(tmp, h, sizeof(double) * m->nC, st));
-    k_gather<double, double><<<grid_for(m->nC, BT), BT, 0, st>>>(m->nC, 1, m->cellN2O, tmp, 0, dst, 0);
+template <class T>
+int cells_in(cupcfd_gpu_mesh *m, const T *h, T *dst, T *tmp, cudaStream_t st) {
+    CG_TRY(up(tmp, h, sizeof(T) * m->nC, st));
+    k_gather<T, T><<<grid_for(m->nC, BT), BT, 0, st>>>(m->nC, 1, m->cellN2O, tmp, 0, dst, 0);
     CG_LAUNCHED();
     return CUPCFD_E_SUCCESS;
 }
-int cells_out(cupcfd_gpu_mesh *m, const double *src, double *h, double *tmp, cudaStream_t st) {
-    k_gather<double, double><<<grid_for(m->nC, BT), BT, 0, st>>>(m->nC, 1, m->cellO2N, src, 0, tmp, 0);
+template <class T>
+int cells_out(cupcfd_gpu_mesh *m, const T *src, T *h, T *tmp, cudaStream_t st) {
+    k_gather<T, T><<<grid_for(m->nC, BT), BT, 0, st>>>(m->nC, 1, m->cellO2N, src, 0, tmp, 0);
     CG_LAUNCHED();
-    return down(h, tmp, sizeof(double) * m->nC, st);
+    return down(h, tmp, sizeof(T) * m->nC, st);
 }
 
-int vec3_in(cupcfd_gpu_mesh *m, const cupcfd_vec3_view &v, double *dst, int64_t ld, double *tmp, cudaStream_t st) {
+template <class T>
+int vec3_in(cupcfd_gpu_mesh *m, const cupcfd_vec3_view &v, T *dst, int64_t ld, T *tmp, cudaStream_t st) {
+    constexpr int RS = (int) sizeof(T);
     CG_RETURN_IF(!v.base, CUPCFD_E_NULL_PTR, "momentum loop: null vector array");
-    CG_RETURN_IF(v.stride < 24 || v.offset < 0 || v.offset + 24 > v.stride, CUPCFD_E_CONFIG_INVALID_VALUE,
+    CG_RETURN_IF(v.stride < 3 * RS || v.offset < 0 || v.offset + 3 * RS > v.stride, CUPCFD_E_CONFIG_INVALID_VALUE,
                  "momentum loop: bad vector stride/offset");
     char *span = nullptr;
-    if (v.stride != 24) CG_TRY(slot(m, U_SPAN, vec3_span_bytes(m->nC, v.stride, v.offset, 8), &span));
-    CG_TRY(upload_vec3_span(v.base, v.stride, v.offset, m->nC, 8, span, tmp, st));
-    k_aos_to_blocks<double, double><<<grid_for(m->nC, BT), BT, 0, st>>>(m->nC, 3, m->cellN2O, tmp, dst, ld);
+    if (v.stride != 3 * RS) CG_TRY(slot(m, U_SPAN, vec3_span_bytes(m->nC, v.stride, v.offset, RS), &span));
+    CG_TRY(upload_vec3_span(v.base, v.stride, v.offset, m->nC, RS, span, tmp, st));
+    k_aos_to_blocks<T, T><<<grid_for(m->nC, BT), BT, 0, st>>>(m->nC, 3, m->cellN2O, tmp, dst, ld);
     CG_LAUNCHED();
     return CUPCFD_E_SUCCESS;
 }
@@ -245,14 +266,14 @@ extern "C" int cupcfd_gpu_mesh_region_force_tangent(cupcfd_gpu_mesh *m, const do
 // ===========================================================================
 // FluxUVWDolfynFaceLoop1 on host buffers
 // ===========================================================================
-extern "C" int cupcfd_gpu_flux_uvw_dolfyn_face_loop1(
-    cupcfd_gpu_mesh *m, double gammaBlend, double small, const double *u, int32_t nU, const double *v, int32_t nV,
-    const double *w, int32_t nW, double *uB, int32_t nUB, double *vB, int32_t nVB, double *wB, int32_t nWB,
-    const double *visC, int32_t nVisC, const double *visB, int32_t nVisB, double *massFlux, int32_t nMassFlux,
-    cupcfd_vec3_view dudx, int32_t nDudx, cupcfd_vec3_view dvdx, int32_t nDvdx, cupcfd_vec3_view dwdx, int32_t nDwdx,
-    double *rFace, int32_t nRFace, double *su, int32_t nSu, double *sv, int32_t nSv, double *sw, int32_t nSw,
-    double *au, int32_t nAu, double *av, int32_t nAv, double *aw, int32_t nAw) {
-    clear_error();
+namespace {
+template <class T>
+int uvw_face_loop1_t(cupcfd_gpu_mesh *m, T gammaBlend, T small, const T *u, int32_t nU, const T *v, int32_t nV,
+                     const T *w, int32_t nW, T *uB, int32_t nUB, T *vB, int32_t nVB, T *wB, int32_t nWB,
+                     const T *visC, int32_t nVisC, const T *visB, int32_t nVisB, T *massFlux, int32_t nMassFlux,
+                     cupcfd_vec3_view dudx, int32_t nDudx, cupcfd_vec3_view dvdx, int32_t nDvdx, cupcfd_vec3_view dwdx,
+                     int32_t nDwdx, T *rFace, int32_t nRFace, T *su, int32_t nSu, T *sv, int32_t nSv, T *sw,
+                     int32_t nSw, T *au, int32_t nAu, T *av, int32_t nAv, T *aw, int32_t nAw) {
     CG_RETURN_IF(!m || !u || !v || !w || !visC || !massFlux || !rFace || !su || !sv || !sw || !au || !av || !aw ||
                      (m->nB > 0 && (!uB || !vB || !wB || !visB)),
                  CUPCFD_E_NULL_PTR, "FluxUVWDolfynFaceLoop1: null argument");
@@ -262,10 +283,10 @@ extern "C" int cupcfd_gpu_flux_uvw_dolfyn_face_loop1(
                      nSv < nC || nSw < nC || nAu < nC || nAv < nC || nAw < nC || nMassFlux < nF || nRFace < 2 * nF ||
                      nUB < nB || nVB < nB || nWB < nB || nVisB < nB,
                  CUPCFD_E_INVALID_INDEX, "FluxUVWDolfynFaceLoop1: array shorter than the mesh needs");
-    CG_TRY(check_mesh(m));
+    CG_TRY(check_mesh(m, sizeof(T) == 8 ? CUPCFD_PREC_F64 : CUPCFD_PREC_F32C));
     cudaStream_t st = m->stream;
     const int64_t ld = nC;
-    double *cells, *grads, *vec, *tmp, *mf, *rf, *bnd;
+    T *cells, *grads, *vec, *tmp, *mf, *rf, *bnd;
     CG_TRY(slot(m, U_CELLS, 10 * (size_t) nC, &cells));
     CG_TRY(slot(m, U_GRADS, 9 * (size_t) nC, &grads));
     CG_TRY(slot(m, U_VEC, 3 * (size_t) nC, &vec));
@@ -274,37 +295,65 @@ extern "C" int cupcfd_gpu_flux_uvw_dolfyn_face_loop1(
     CG_TRY(slot(m, U_RF, 2 * (size_t) nF, &rf));
     CG_TRY(slot(m, U_BND, 4 * (size_t) nB, &bnd));
     // cells: u v w visC su sv sw au av aw
-    const double *cin[10] = {u, v, w, visC, su, sv, sw, au, av, aw};
+    const T *cin[10] = {u, v, w, visC, su, sv, sw, au, av, aw};
     for (int q = 0; q < 10; q++) CG_TRY(cells_in(m, cin[q], cells + q * ld, tmp, st));
     const cupcfd_vec3_view vv[3] = {dudx, dvdx, dwdx};
     for (int q = 0; q < 3; q++) CG_TRY(vec3_in(m, vv[q], grads + 3 * q * ld, ld, vec, st));
     // faces: massFlux, rFace pairs
-    CG_TRY(up(tmp, massFlux, sizeof(double) * nF, st));
-    k_gather<double, double><<<grid_for(nF, BT), BT, 0, st>>>(nF, 1, m->faceN2O, tmp, 0, mf, 0);
+    CG_TRY(up(tmp, massFlux, sizeof(T) * nF, st));
+    k_gather<T, T><<<grid_for(nF, BT), BT, 0, st>>>(nF, 1, m->faceN2O, tmp, 0, mf, 0);
     CG_LAUNCHED();
-    CG_TRY(up(tmp, rFace, sizeof(double) * 2 * nF, st));
-    k_gather_pairs<double><<<grid_for(nF, BT), BT, 0, st>>>(nF, m->faceN2O, tmp, rf);
+    CG_TRY(up(tmp, rFace, sizeof(T) * 2 * nF, st));
+    k_gather_pairs<T><<<grid_for(nF, BT), BT, 0, st>>>(nF, m->faceN2O, tmp, rf);
     CG_LAUNCHED();
     // boundaries (same ids on both sides): uB vB wB visB
-    double *hb[4] = {uB, vB, wB, const_cast<double *>(visB)};
-    for (int q = 0; q < 4; q++) CG_TRY(up(bnd + (size_t) q * nB, hb[q], sizeof(double) * nB, st));
-    double *c = cells;
+    T *hb[4] = {uB, vB, wB, const_cast<T *>(visB)};
+    for (int q = 0; q < 4; q++) CG_TRY(up(bnd + (size_t) q * nB, hb[q], sizeof(T) * nB, st));
+    T *c = cells;
     CG_TRY(run_face_loop(m, gammaBlend, small, c, c + ld, c + 2 * ld, bnd, bnd + nB, bnd + 2 * (size_t) nB, c + 3 * ld,
                          bnd + 3 * (size_t) nB, mf, grads, ld, rf, c + 4 * ld, c + 5 * ld, c + 6 * ld, c + 7 * ld,
                          c + 8 * ld, c + 9 * ld, st));
     // back to the reference's numbering; one staging buffer, reused in
     // stream order (each copy out finishes before the next gather runs)
-    k_gather<double, double><<<grid_for(nF, BT), BT, 0, st>>>(nF, 1, m->faceO2N, mf, 0, tmp, 0);
+    k_gather<T, T><<<grid_for(nF, BT), BT, 0, st>>>(nF, 1, m->faceO2N, mf, 0, tmp, 0);
     CG_LAUNCHED();
-    CG_TRY(down(massFlux, tmp, sizeof(double) * nF, st));
-    k_gather_pairs<double><<<grid_for(nF, BT), BT, 0, st>>>(nF, m->faceO2N, rf, tmp);
+    CG_TRY(down(massFlux, tmp, sizeof(T) * nF, st));
+    k_gather_pairs<T><<<grid_for(nF, BT), BT, 0, st>>>(nF, m->faceO2N, rf, tmp);
     CG_LAUNCHED();
-    CG_TRY(down(rFace, tmp, sizeof(double) * 2 * nF, st));
-    double *cout_[6] = {su, sv, sw, au, av, aw};
+    CG_TRY(down(rFace, tmp, sizeof(T) * 2 * nF, st));
+    T *cout_[6] = {su, sv, sw, au, av, aw};
     for (int q = 0; q < 6; q++) CG_TRY(cells_out(m, c + (4 + q) * ld, cout_[q], tmp, st));
-    for (int q = 0; q < 3; q++) CG_TRY(down(hb[q], bnd + (size_t) q * nB, sizeof(double) * nB, st));
+    for (int q = 0; q < 3; q++) CG_TRY(down(hb[q], bnd + (size_t) q * nB, sizeof(T) * nB, st));
     CG_CHECK_CUDA(cudaStreamSynchronize(st));
     return CUPCFD_E_SUCCESS;
+}
+
+}  // namespace
+
+extern "C" int cupcfd_gpu_flux_uvw_dolfyn_face_loop1(
+    cupcfd_gpu_mesh *m, double gammaBlend, double small, const double *u, int32_t nU, const double *v, int32_t nV,
+    const double *w, int32_t nW, double *uB, int32_t nUB, double *vB, int32_t nVB, double *wB, int32_t nWB,
+    const double *visC, int32_t nVisC, const double *visB, int32_t nVisB, double *massFlux, int32_t nMassFlux,
+    cupcfd_vec3_view dudx, int32_t nDudx, cupcfd_vec3_view dvdx, int32_t nDvdx, cupcfd_vec3_view dwdx, int32_t nDwdx,
+    double *rFace, int32_t nRFace, double *su, int32_t nSu, double *sv, int32_t nSv, double *sw, int32_t nSw,
+    double *au, int32_t nAu, double *av, int32_t nAv, double *aw, int32_t nAw) {
+    clear_error();
+    return uvw_face_loop1_t<double>(m, gammaBlend, small, u, nU, v, nV, w, nW, uB, nUB, vB, nVB, wB, nWB, visC, nVisC,
+                                    visB, nVisB, massFlux, nMassFlux, dudx, nDudx, dvdx, nDvdx, dwdx, nDwdx, rFace,
+                                    nRFace, su, nSu, sv, nSv, sw, nSw, au, nAu, av, nAv, aw, nAw);
+}
+
+extern "C" int cupcfd_gpu_flux_uvw_dolfyn_face_loop1_f32(
+    cupcfd_gpu_mesh *m, float gammaBlend, float small, const float *u, int32_t nU, const float *v, int32_t nV,
+    const float *w, int32_t nW, float *uB, int32_t nUB, float *vB, int32_t nVB, float *wB, int32_t nWB,
+    const float *visC, int32_t nVisC, const float *visB, int32_t nVisB, float *massFlux, int32_t nMassFlux,
+    cupcfd_vec3_view dudx, int32_t nDudx, cupcfd_vec3_view dvdx, int32_t nDvdx, cupcfd_vec3_view dwdx, int32_t nDwdx,
+    float *rFace, int32_t nRFace, float *su, int32_t nSu, float *sv, int32_t nSv, float *sw, int32_t nSw,
+    float *au, int32_t nAu, float *av, int32_t nAv, float *aw, int32_t nAw) {
+    clear_error();
+    return uvw_face_loop1_t<float>(m, gammaBlend, small, u, nU, v, nV, w, nW, uB, nUB, vB, nVB, wB, nWB, visC, nVisC,
+                                   visB, nVisB, massFlux, nMassFlux, dudx, nDudx, dvdx, nDvdx, dwdx, nDwdx, rFace,
+                                   nRFace, su, nSu, sv, nSv, sw, nSw, au, nAu, av, nAv, aw, nAw);
 }
 
 // ===========================================================================
@@ -321,8 +370,8 @@ extern "C" int cupcfd_gpu_dev_uvw_face_loop1(cupcfd_gpu_mesh *m, double gammaBle
                  CUPCFD_E_NULL_PTR, "dev_uvw_face_loop1: null argument");
     CG_RETURN_IF(ldg < m->nC, CUPCFD_E_INVALID_INDEX, "dev_uvw_face_loop1: gradient leading dimension below nCells");
     CG_TRY(check_mesh(m));
-    return run_face_loop(m, gammaBlend, small, u, v, w, uB, vB, wB, visC, visB, massFlux, grads, ldg, rFace, su, sv, sw,
-                         au, av, aw, (cudaStream_t) stream);
+    return run_face_loop<double>(m, gammaBlend, small, u, v, w, uB, vB, wB, visC, visB, massFlux, grads, ldg, rFace, su,
+                                 sv, sw, au, av, aw, (cudaStream_t) stream);
 }
 
 extern "C" int cupcfd_gpu_dev_uvw_region_loop1(cupcfd_gpu_mesh *m, void *stream) {
@@ -347,8 +396,14 @@ extern "C" int cupcfd_gpu_dev_uvw_bnds_loop1(cupcfd_gpu_mesh *m, void *stream) {
         CG_TRY(slot(m, U_SELC, (size_t) m->nB / SEL_T + 2, &cnt));
         CG_TRY(slot(m, U_SELV, 3 * (size_t) m->nB, &vals));
         CG_TRY(slot(m, U_SELR, (size_t) m->nB, &regs));
-        CG_TRY(launch_ordered_sum<3>(SelArgs{m->nB, m->bndRegion, m->regionType, CUPCFD_RTYPE_WALL}, m->bndShear, 3, 0,
-                                     nullptr, nullptr, 0.0, nullptr, m->regionFT, m->nR, cnt, vals, regs, st));
+        // (in float on a mesh of the reference's T = float instantiation)
+        const SelArgs sa{m->nB, m->bndRegion, m->regionType, CUPCFD_RTYPE_WALL};
+        const int rc = m->realSize == 4
+                           ? launch_ordered_sum<3, true>(sa, m->bndShear, 3, 0, nullptr, nullptr, 0.0, nullptr,
+                                                         m->regionFT, m->nR, cnt, vals, regs, st)
+                           : launch_ordered_sum<3>(sa, m->bndShear, 3, 0, nullptr, nullptr, 0.0, nullptr, m->regionFT,
+                                                   m->nR, cnt, vals, regs, st);
+        CG_TRY(rc);
     }
     return CUPCFD_E_SUCCESS;
 }

@@ -562,9 +562,25 @@ int cupcfd_gpu_flux_uvw_dolfyn_face_loop1(
     cupcfd_vec3_view dudx, int32_t nDudx, cupcfd_vec3_view dvdx, int32_t nDvdx, cupcfd_vec3_view dwdx, int32_t nDwdx,
     double *rFace, int32_t nRFace, double *su, int32_t nSu, double *sv, int32_t nSv, double *sw, int32_t nSw,
     double *au, int32_t nAu, double *av, int32_t nAv, double *aw, int32_t nAw);
+/* The same loop of the reference's T = float instantiation: float arrays,
+ * EuclideanVector<float,3> views, the float build's arithmetic on the mesh's
+ * FP32 geometry (exact for a mesh uploaded from float arrays), results bit
+ * for bit those of the reference's float build. The mesh must have
+ * CUPCFD_PREC_F32C geometry. */
+int cupcfd_gpu_flux_uvw_dolfyn_face_loop1_f32(
+    cupcfd_gpu_mesh *mesh, float gammaBlend, float small, const float *uCell, int32_t nUCell,
+    const float *vCell, int32_t nVCell, const float *wCell, int32_t nWCell, float *uBoundary, int32_t nUBoundary,
+    float *vBoundary, int32_t nVBoundary, float *wBoundary, int32_t nWBoundary, const float *visEffCell,
+    int32_t nVisEffCell, const float *visEffBoundary, int32_t nVisEffBoundary, float *massFlux, int32_t nMassFlux,
+    cupcfd_vec3_view dudx, int32_t nDudx, cupcfd_vec3_view dvdx, int32_t nDvdx, cupcfd_vec3_view dwdx, int32_t nDwdx,
+    float *rFace, int32_t nRFace, float *su, int32_t nSu, float *sv, int32_t nSv, float *sw, int32_t nSw,
+    float *au, int32_t nAu, float *av, int32_t nAv, float *aw, int32_t nAw);
 /* FluxUVWDolfynRegionLoop1 (UVWKernels.ipp:517-524): force tangents = 0.
  * FluxUVWDolfynBndsLoop1 (UVWKernels.ipp:527-544): each wall boundary adds
- * its shear onto its region's force tangent, in boundary order. */
+ * its shear onto its region's force tangent, in boundary order; in float on
+ * a mesh created from float arrays (real_size 4, the reference's T = float
+ * instantiation), in double otherwise. The shears and tangents are kept in
+ * double either way (a float mesh's values exactly). */
 int cupcfd_gpu_flux_uvw_dolfyn_region_loop1(cupcfd_gpu_mesh *mesh);
 int cupcfd_gpu_flux_uvw_dolfyn_bnds_loop1(cupcfd_gpu_mesh *mesh);
 

@@ -407,6 +407,31 @@ ecode_t FluxUVWDolfynFaceLoop1(Mesh &mesh, double gammaBlend, double small, doub
     return (ecode_t) rc;
 }
 
+// FluxUVWDolfynFaceLoop1, T = float: the reference's float instantiation
+// (cupcfd_gpu_flux_uvw_dolfyn_face_loop1_f32). rlencos and the
+// boundary distances are those read when the mesh was attached; the wall
+// shears the loop computes are written back through setBoundaryShear.
+template <class Mesh, class I, class Vec>
+ecode_t FluxUVWDolfynFaceLoop1(Mesh &mesh, float gammaBlend, float small, float *uCell, I nUCell, float *vCell,
+                               I nVCell, float *wCell, I nWCell, float *uBoundary, I nUBoundary, float *vBoundary,
+                               I nVBoundary, float *wBoundary, I nWBoundary, float *visEffCell, I nVisEffCell,
+                               float *visEffBoundary, I nVisEffBoundary, float *massFlux, I nMassFlux, Vec *dudx,
+                               I nDudx, Vec *dvdx, I nDvdx, Vec *dwdx, I nDwdx, float *rFace, I nRFace, float *su,
+                               I nSu, float *sv, I nSv, float *sw, I nSw, float *au, I nAu, float *av, I nAv,
+                               float *aw, I nAw) {
+    static_assert(sizeof(I) == 4, "int32 indices");
+    cupcfd_gpu_mesh *m = nullptr;
+    int rc = attach(mesh, &m);
+    if (rc != CUPCFD_E_SUCCESS) return (ecode_t) rc;
+    rc = cupcfd_gpu_flux_uvw_dolfyn_face_loop1_f32(
+        m, gammaBlend, small, uCell, nUCell, vCell, nVCell, wCell, nWCell, uBoundary, nUBoundary, vBoundary,
+        nVBoundary, wBoundary, nWBoundary, visEffCell, nVisEffCell, visEffBoundary, nVisEffBoundary, massFlux,
+        nMassFlux, detail::view_of(dudx), nDudx, detail::view_of(dvdx), nDvdx, detail::view_of(dwdx), nDwdx, rFace,
+        nRFace, su, nSu, sv, nSv, sw, nSw, au, nAu, av, nAv, aw, nAw);
+    if (rc == CUPCFD_E_SUCCESS) rc = detail::sync_shear(mesh, m, true, CUPCFD_RTYPE_WALL);
+    return (ecode_t) rc;
+}
+
 // FluxUVWDolfynRegionLoop1 / FluxUVWDolfynBndsLoop1 (UVWKernels.h:72-92) on
 // the host mesh's force tangents and shears (read, computed on the GPU,
 // written back). The reference's return void; these return the status.

@@ -952,3 +952,165 @@ int orc_uvw_bnds_loop1(const orc_mesh *m, const double *shear, double *forceTang
     }
     return ORC_E_SUCCESS;
 }
+
+/* ------------------------------------------------------------------------
+ * The momentum loops of the reference's T = float instantiation
+ * (UVWKernels.ipp:38-544 with T = float). Every product, sum and quotient
+ * rounds in float in the reference's operand order, with three exceptions
+ * the float build has:
+ *   - facp = 1.0 - facn: the literal is double, the result rounded to float;
+ *   - the wall branch's uvel = fabs(ut0) + fabs(ut1) + fabs(ut2): fabs is
+ *     the C library's double function in the reference's scope, so the sum
+ *     is double and rounds to float once on assignment (checked against the
+ *     compiled float build in tests/test_oracle_vs_reference.py);
+ *   - EuclideanVector::length() widens sqrtf's result to double, which the
+ *     float scalars of normalise() and of the wall's xpn_length take back
+ *     exactly (EuclideanVector.cpp:93-109), so both are the float sqrt.
+ * 2.0 * visac (symmetry) is exact in double and exact again as float.
+ * ------------------------------------------------------------------------ */
+static float dot3f(const float *a, const float *b) {
+    float d = 0.0f;
+    for (int k = 0; k < 3; k++) d += a[k] * b[k];
+    return d;
+}
+static void normalise3f(float *x) {
+    float len = sqrtf(dot3f(x, x));
+    if (len != 0.0f) {
+        float sc = 1.0f / len;
+        x[0] *= sc; x[1] *= sc; x[2] *= sc;
+    }
+}
+static float std_minf(float a, float b) { return (b < a) ? b : a; }
+static float std_maxf(float a, float b) { return (a < b) ? b : a; }
+
+int orc_uvw_face_loop1_f32(const orc_mesh_f *m, const float *rlencos, const float *bndDist, float gammaBlend, float small,
+                           const float *u, const float *v, const float *w, float *uB, float *vB, float *wB,
+                           const float *visC, const float *visB, float *massFlux,
+                           const float *dudx, const float *dvdx, const float *dwdx, float *rFace,
+                           float *su, float *sv, float *sw, float *au, float *av, float *aw, float *shear) {
+    float uFace = 0.0f, vFace = 0.0f, wFace = 0.0f, visFace = 0.0f;
+    for (int i = 0; i < m->nFaces; i++) {
+        int ip = m->faceCell1[i];
+        const float *S = m->faceNorm + 3 * i;
+        float rl = rlencos ? rlencos[i] : 0.0f;
+        if (m->faceBnd[i] < 0) {
+            int in = m->faceCell2[i];
+            float facn = m->faceLambda[i];
+            float facp = (float) (1.0 - (double) facn);
+            float du[3], dv[3], dw[3], xpn[3];
+            for (int d = 0; d < 3; d++) {
+                du[d] = dudx[3 * in + d] * facn + dudx[3 * ip + d] * facp;
+                dv[d] = dvdx[3 * in + d] * facn + dvdx[3 * ip + d] * facp;
+                dw[d] = dwdx[3 * in + d] * facn + dwdx[3 * ip + d] * facp;
+                xpn[d] = m->cellCenter[3 * in + d] - m->cellCenter[3 * ip + d];
+            }
+            float visac = visC[in] * facn + visC[ip] * facp;
+            visFace = visac * rl;
+            float mf = massFlux[i];
+            float fuce = mf * uFace, fvce = mf * vFace, fwce = mf * wFace;
+            float fude1 = (du[0] + du[0]) * S[0] + (du[1] + dv[0]) * S[1] + (du[2] + dw[0]) * S[2];
+            float fvde1 = (du[1] + dv[0]) * S[0] + (dv[1] + dv[1]) * S[1] + (dv[2] + dw[1]) * S[2];
+            float fwde1 = (du[2] + dw[0]) * S[0] + (dw[1] + dv[2]) * S[1] + (dw[2] + dw[2]) * S[2];
+            float fude = visac * fude1, fvde = visac * fvde1, fwde = visac * fwde1;
+            float fmin = std_minf(mf, 0.0f), fmax = std_maxf(mf, 0.0f);
+            float fuci = fmin * u[in] + fmax * u[ip];
+            float fvci = fmin * v[in] + fmax * v[ip];
+            float fwci = fmin * w[in] + fmax * w[ip];
+            float fudi = visFace * dot3f(du, xpn), fvdi = visFace * dot3f(dv, xpn), fwdi = visFace * dot3f(dw, xpn);
+            rFace[2 * i] = -visFace - std_maxf(mf, 0.0f);
+            rFace[2 * i + 1] = -visFace + std_minf(mf, 0.0f);
+            float bu = gammaBlend * (fuce - fuci), bv = gammaBlend * (fvce - fvci), bw = gammaBlend * (fwce - fwci);
+            su[ip] = su[ip] - bu + fude - fudi;
+            su[in] = su[in] + bu - fude + fudi;
+            sv[ip] = sv[ip] - bv + fvde - fvdi;
+            sv[in] = sv[in] + bv - fvde + fvdi;
+            sw[ip] = sw[ip] - bw + fwde - fwdi;
+            sw[in] = sw[in] + bw - fwde + fwdi;
+            continue;
+        }
+        int ib = m->faceBnd[i], ir = m->bndRegion[ib], it = m->regionType[ir];
+        const float *X = m->faceCenter + 3 * i;
+        const float *du = dudx + 3 * ip, *dv = dvdx + 3 * ip, *dw = dwdx + 3 * ip;
+        float xpn[3];
+        for (int d = 0; d < 3; d++) xpn[d] = X[d] - m->cellCenter[3 * ip + d];
+        if (it == ORC_RTYPE_INLET || it == ORC_RTYPE_OUTLET) {
+            float visac, fvde, fwde;
+            float fude = (du[0] + du[0]) * S[0] + (du[1] + dv[0]) * S[1] + (du[2] + dw[0]) * S[2];
+            if (it == ORC_RTYPE_INLET) {
+                uFace = m->regionUVW[3 * ir]; vFace = m->regionUVW[3 * ir + 1]; wFace = m->regionUVW[3 * ir + 2];
+                visac = visB[ib];
+                fvde = (du[1] + dv[0]) * S[0] + (dv[1] + dv[1]) * S[1] + (dv[2] + dw[1]) * S[2];
+                fwde = (du[2] + dw[0]) * S[0] + (dw[1] + dv[2]) * S[1] + (dw[2] + dw[2]) * S[2];
+            } else {
+                visac = visC[ip];
+                uFace = u[ip]; vFace = v[ip]; wFace = w[ip];
+                fvde = (dv[0] + du[1]) * S[0] + (dv[1] + dv[1]) * S[1] + (dv[2] + dw[1]) * S[2];
+                fwde = (dw[0] + du[2]) * S[0] + (dw[1] + dv[2]) * S[1] + (dw[2] + dw[2]) * S[2];
+            }
+            visFace = visac * rl;
+            fude = visac * fude; fvde = visac * fvde; fwde = visac * fwde;
+            float fudi = visFace * dot3f(du, xpn), fvdi = visFace * dot3f(dv, xpn), fwdi = visFace * dot3f(dw, xpn);
+            if (it == ORC_RTYPE_OUTLET && massFlux[i] < 0.0) massFlux[i] = small;
+            float f = -visFace + std_minf(massFlux[i], 0.0f);
+            au[ip] = au[ip] - f;
+            su[ip] = su[ip] - f * uFace + fude - fudi;
+            uB[ib] = uFace;
+            av[ip] = av[ip] - f;
+            sv[ip] = sv[ip] - f * vFace + fvde - fvdi;
+            vB[ib] = vFace;
+            aw[ip] = aw[ip] - f;
+            sw[ip] = sw[ip] - f * wFace + fwde - fwdi;
+            wB[ib] = wFace;
+        } else if (it == ORC_RTYPE_SYMP) {
+            float visac = visC[ip];
+            float us[3] = {u[ip] + dot3f(du, xpn), v[ip] + dot3f(dv, xpn), w[ip] + dot3f(dw, xpn)};
+            float xn[3] = {0.0f - S[0], 0.0f - S[1], 0.0f - S[2]};
+            normalise3f(xn);
+            float dp = dot3f(us, xn);
+            float dn = bndDist ? bndDist[ib] : 0.0f;
+            float tv = (float) (2.0 * (double) visac);
+            float force[3];
+            for (int d = 0; d < 3; d++) force[d] = ((tv * (dp * xn[d])) / dn) * m->faceArea[i];
+            au[ip] = au[ip] + visFace;
+            av[ip] = av[ip] + visFace;
+            aw[ip] = aw[ip] + visFace;
+            su[ip] = su[ip] + visFace * u[ip] - force[0];
+            sv[ip] = sv[ip] + visFace * v[ip] - force[1];
+            sw[ip] = sw[ip] + visFace * w[ip] - force[2];
+            uB[ib] = us[0]; vB[ib] = us[1]; wB[ib] = us[2];
+        } else if (it == ORC_RTYPE_WALL) {
+            const float *uw = m->regionUVW + 3 * ir;
+            float visac = visB[ib];
+            float coef = visac * m->faceArea[i] / sqrtf(dot3f(xpn, xpn));
+            float xn[3] = {S[0], S[1], S[2]};
+            normalise3f(xn);
+            float up[3] = {u[ip] - uw[0], v[ip] - uw[1], w[ip] - uw[2]};
+            float dp = dot3f(up, xn);
+            float ut[3] = {up[0] - dp * xn[0], up[1] - dp * xn[1], up[2] - dp * xn[2]};
+            float uvel = (float) (fabs((double) ut[0]) + fabs((double) ut[1]) + fabs((double) ut[2]));
+            float force[3] = {0.0f, 0.0f, 0.0f};
+            if (uvel > small) {
+                float dn = bndDist ? bndDist[ib] : 0.0f;
+                for (int d = 0; d < 3; d++) force[d] = ((visac * ut[d]) / dn) * m->faceArea[i];
+            }
+            for (int d = 0; d < 3; d++) shear[3 * ib + d] = force[d];
+            au[ip] = au[ip] + coef;
+            av[ip] = av[ip] + coef;
+            aw[ip] = aw[ip] + coef;
+            su[ip] = su[ip] + coef * u[ip] - force[0];
+            sv[ip] = sv[ip] + coef * v[ip] - force[1];
+            sw[ip] = sw[ip] + coef * w[ip] - force[2];
+            uB[ib] = uw[0]; vB[ib] = uw[1]; wB[ib] = uw[2];
+        }
+    }
+    return ORC_E_SUCCESS;
+}
+
+int orc_uvw_bnds_loop1_f32(const orc_mesh_f *m, const float *shear, float *forceTangent) {
+    for (int ib = 0; ib < m->nBnd; ib++) {
+        int ir = m->bndRegion[ib];
+        if (m->regionType[ir] != ORC_RTYPE_WALL) continue;
+        for (int d = 0; d < 3; d++) forceTangent[3 * ir + d] = forceTangent[3 * ir + d] + shear[3 * ib + d];
+    }
+    return ORC_E_SUCCESS;
+}

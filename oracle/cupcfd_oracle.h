@@ -66,6 +66,18 @@ int orc_jitter_build(int nx, int ny, int nz, double jitter, unsigned long long s
 int orc_cell_face_csr(int nCells, int nFaces, const int *faceCell1, const int *faceCell2, int *xadj, int *adj);
 
 /* ---- kernels ---- */
+/* The same mesh with float geometry and region values: the arrays a
+ * CupCfdSoAMesh<int,float,int> holds (the reference's T = float
+ * instantiation, BenchmarkKernels.cpp:1134-1138). */
+typedef struct {
+    int nCells, nFaces, nBnd, nRegions;
+    const int *faceCell1, *faceCell2, *faceBnd;
+    const float *faceLambda, *faceNorm, *faceCenter, *faceArea, *faceXpac, *faceXnac;
+    const float *cellCenter, *cellVolume;
+    const int *bndRegion, *regionType;
+    const float *regionUVW, *regionDen;
+} orc_mesh_f;
+
 int orc_gradient_phi_gauss(const orc_mesh *m, int nGradient,
                            const double *phi, int nPhi, const double *phiB, int nPhiB,
                            double *dPhidx, int nDPhidx, double *dPhidxo, int nDPhidxo);
@@ -110,6 +122,14 @@ int orc_uvw_face_loop1(const orc_mesh *m, const double *rlencos, const double *b
                        double *su, double *sv, double *sw, double *au, double *av, double *aw, double *shear);
 int orc_uvw_region_loop1(const orc_mesh *m, double *forceTangent);
 int orc_uvw_bnds_loop1(const orc_mesh *m, const double *shear, double *forceTangent);
+/* The momentum loops of the reference's T = float instantiation: the same
+ * loops with float arrays and the float build's arithmetic (see .c). */
+int orc_uvw_face_loop1_f32(const orc_mesh_f *m, const float *rlencos, const float *bndDist, float gammaBlend, float small,
+                           const float *u, const float *v, const float *w, float *uB, float *vB, float *wB,
+                           const float *visC, const float *visB, float *massFlux,
+                           const float *dudx, const float *dvdx, const float *dwdx, float *rFace,
+                           float *su, float *sv, float *sw, float *au, float *av, float *aw, float *shear);
+int orc_uvw_bnds_loop1_f32(const orc_mesh_f *m, const float *shear, float *forceTangent);
 int orc_mass_plain_forward(const orc_mesh *m, const double *den, const double *u, const double *v, const double *w,
                            double *massFlux);
 int orc_mass_plain_adjoint(const orc_mesh *m, const double *den, const double *u, const double *v, const double *w,

@@ -623,6 +623,85 @@ def uvw_face_loop1(m, f, rlencos=None, bnd_dist=None):
     return out
 
 
+class _OrcMeshF(C.Structure):
+    _fields_ = [("nCells", C.c_int), ("nFaces", C.c_int), ("nBnd", C.c_int), ("nRegions", C.c_int)] + [
+        (n, C.c_void_p) for n in ("faceCell1", "faceCell2", "faceBnd", "faceLambda", "faceNorm", "faceCenter",
+                                  "faceArea", "faceXpac", "faceXnac", "cellCenter", "cellVolume", "bndRegion",
+                                  "regionType", "regionUVW", "regionDen")]
+
+
+def _f32(a):
+    return None if a is None else np.ascontiguousarray(np.asarray(a).reshape(-1), np.float32)
+
+
+def _float_mesh(m):
+    """Arrays of mesh ``m`` as a CupCfdSoAMesh<int,float,int> holds them
+    (float geometry and region values) and an orc_mesh_f over them."""
+    keep = {k: np.ascontiguousarray(m[k], np.int32) for k in ("faceCell1", "faceCell2", "faceBnd", "bndRegion",
+                                                              "regionType")}
+    for k in ("faceLambda", "faceNorm", "faceCenter", "faceArea", "faceXpac", "faceXnac", "cellCenter", "cellVolume",
+              "regionUVW", "regionDen"):
+        keep[k] = _f32(m[k])
+    s = _OrcMeshF(int(m["nCells"]), int(m["nFaces"]), int(m["nBnd"]), int(m["nRegions"]),
+                  *[_p(keep[n]) for n, _ in _OrcMeshF._fields_[4:]])
+    return s, keep
+
+
+def _uvw_f32_inputs(f):
+    a = {k: _f32(f[k]) for k in ("u", "v", "w", "visC", "visB", "dudx", "dvdx", "dwdx")}
+    out = {k: _f32(f[k]).copy() for k in UVW_INOUT}
+    return a, out
+
+
+def uvw_loops_f32(m, f, rlencos=None, bnd_dist=None):
+    """The momentum loops of the reference's T = float instantiation (C
+    restatement): FluxUVWDolfynFaceLoop1 on float inputs, then the region
+    force tangents (zeroed by FluxUVWDolfynRegionLoop1, the wall shears added
+    by FluxUVWDolfynBndsLoop1). Returns the in/out arrays (float32), shear
+    [nBnd, 3] and the force tangents [nRegions, 3]."""
+    s, keep = _float_mesh(m)
+    a, out = _uvw_f32_inputs(f)
+    out["shear"] = np.zeros((m["nBnd"], 3), np.float32)
+    rl, bd = _f32(rlencos), _f32(bnd_dist)
+    lib = load()
+    lib.orc_uvw_face_loop1_f32.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_float] + [C.c_void_p] * 20
+    rc = lib.orc_uvw_face_loop1_f32(C.byref(s), _p(rl), _p(bd), float(np.float32(f["gammaBlend"])),
+                                    float(np.float32(f["small"])), _p(a["u"]), _p(a["v"]), _p(a["w"]), _p(out["uB"]),
+                                    _p(out["vB"]), _p(out["wB"]), _p(a["visC"]), _p(a["visB"]), _p(out["massFlux"]),
+                                    _p(a["dudx"]), _p(a["dvdx"]), _p(a["dwdx"]), _p(out["rFace"]),
+                                    *[_p(out[k]) for k in ("su", "sv", "sw", "au", "av", "aw")], _p(out["shear"]))
+    assert rc == E_SUCCESS
+    ft = np.zeros((m["nRegions"], 3), np.float32)
+    assert lib.orc_uvw_bnds_loop1_f32(C.byref(s), _p(out["shear"]), _p(ft)) == E_SUCCESS
+    out["forceTangent"] = ft
+    return out
+
+
+def ref_uvw_loops_f32(m, f, rlencos=None, bnd_dist=None):
+    """The same loops of the reference's own T = float instantiation
+    (compiled unchanged), on the same float arrays."""
+    ref = load_ref()
+    assert ref is not None, "reference build absent"
+    _, keep = _float_mesh(m)
+    a, out = _uvw_f32_inputs(f)
+    nF, nB, nR = int(m["nFaces"]), int(m["nBnd"]), int(m["nRegions"])
+    rl = _f32(rlencos) if rlencos is not None else np.zeros(nF, np.float32)
+    bd = _f32(bnd_dist) if bnd_dist is not None else np.zeros(nB, np.float32)
+    out["shear"] = np.zeros((nB, 3), np.float32)
+    out["forceTangent"] = np.full((nR, 3), 7.0, np.float32)
+    fn = ref.ref_uvw_loops_f32
+    fn.argtypes = [C.c_int] * 4 + [C.c_void_p] * 15 + [C.c_float, C.c_float] + [C.c_void_p] * 21
+    geo = [keep[k] for k in ("faceCell1", "faceCell2", "faceBnd", "faceLambda", "faceNorm", "faceCenter", "faceArea",
+                             "cellCenter", "cellVolume", "bndRegion", "regionType", "regionUVW", "regionDen")]
+    rc = fn(int(m["nCells"]), nF, nB, nR, *[_p(x) for x in geo], _p(rl), _p(bd), float(np.float32(f["gammaBlend"])),
+            float(np.float32(f["small"])), _p(a["u"]), _p(a["v"]), _p(a["w"]), _p(out["uB"]), _p(out["vB"]),
+            _p(out["wB"]), _p(a["visC"]), _p(a["visB"]), _p(out["massFlux"]), _p(a["dudx"]), _p(a["dvdx"]),
+            _p(a["dwdx"]), _p(out["rFace"]), *[_p(out[k]) for k in ("su", "sv", "sw", "au", "av", "aw")],
+            _p(out["shear"]), _p(out["forceTangent"]))
+    assert rc == E_SUCCESS, rc
+    return out
+
+
 def uvw_region_loop1(m):
     ft = np.full((m["nRegions"], 3), np.nan)
     assert load().orc_uvw_region_loop1(C.byref(_cmesh(m)), _p(ft)) == E_SUCCESS

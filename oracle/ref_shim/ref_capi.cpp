@@ -482,3 +482,59 @@ extern "C" int ref_uvw_face_loop1(void * p, double gammaBlend, double small, dou
 
 extern "C" void ref_uvw_region_loop1(void * p) { cupcfd::fvm::FluxUVWDolfynRegionLoop1(((RefCtx *) p)->mesh); }
 extern "C" void ref_uvw_bnds_loop1(void * p) { cupcfd::fvm::FluxUVWDolfynBndsLoop1(((RefCtx *) p)->mesh); }
+
+/* The momentum loops of the reference's T=float instantiation on a float
+ * mesh given by its arrays (xyz-interleaved vectors): FluxUVWDolfynFaceLoop1,
+ * then FluxUVWDolfynRegionLoop1 and FluxUVWDolfynBndsLoop1 on the mesh's
+ * shears and force tangents, which come back in shear[3*nBnd] and
+ * ftan[3*nRegions] (ftan in: the tangents before the region loop zeroes
+ * them, unused). In/out arrays updated in place as the reference does. */
+extern "C" int ref_uvw_loops_f32(int nCells, int nFaces, int nBnd, int nRegions, const int * faceCell1,
+                                 const int * faceCell2, const int * faceBnd, const float * faceLambda,
+                                 const float * faceNorm, const float * faceCenter, const float * faceArea,
+                                 const float * cellCenter, const float * cellVolume, const int * bndRegion,
+                                 const int * regionType, const float * regionUVW, const float * regionDen,
+                                 const float * rlencos, const float * bdist, float gammaBlend, float small,
+                                 float * u, float * v, float * w, float * uB, float * vB, float * wB, float * visC,
+                                 float * visB, float * massFlux, const float * dudx, const float * dvdx,
+                                 const float * dwdx, float * rFace, float * su, float * sv, float * sw, float * au,
+                                 float * av, float * aw, float * shear, float * ftan) {
+	RefMeshF mesh;
+	mesh.properties.lOCells = nCells;
+	mesh.properties.lGhCells = 0;
+	mesh.properties.lTCells = nCells;
+	mesh.properties.lFaces = nFaces;
+	mesh.properties.lBoundaries = nBnd;
+	mesh.properties.lRegions = nRegions;
+	mesh.a = {};
+	mesh.a.faceCell1 = faceCell1;
+	mesh.a.faceCell2 = faceCell2;
+	mesh.a.faceBoundary = faceBnd;
+	mesh.a.faceLambda = faceLambda;
+	mesh.a.faceNorm = faceNorm;
+	mesh.a.faceCenter = faceCenter;
+	mesh.a.faceArea = faceArea;
+	mesh.a.cellCenter = cellCenter;
+	mesh.a.cellVolume = cellVolume;
+	mesh.a.boundaryRegion = bndRegion;
+	mesh.a.regionType = regionType;
+	mesh.a.regionUVW = regionUVW;
+	mesh.a.regionDen = regionDen;
+	mesh.a.faceRLencos = rlencos;
+	mesh.a.boundaryDistance = bdist;
+	mesh.a.boundaryShear = shear;
+	mesh.a.regionForceTangent = ftan;
+	std::vector<euc::EuclideanVector<float,3>> gu(nCells), gv(nCells), gw(nCells);
+	for (int i = 0; i < nCells; i++)
+		for (int d = 0; d < 3; d++) {
+			gu[i].cmp[d] = dudx[3*i+d]; gv[i].cmp[d] = dvdx[3*i+d]; gw[i].cmp[d] = dwdx[3*i+d];
+		}
+	cupcfd::error::eCodes st = cupcfd::fvm::FluxUVWDolfynFaceLoop1(mesh, gammaBlend, small, u, nCells, v, nCells,
+		w, nCells, uB, nBnd, vB, nBnd, wB, nBnd, visC, nCells, visB, nBnd, massFlux, nFaces, gu.data(), nCells,
+		gv.data(), nCells, gw.data(), nCells, rFace, 2 * nFaces, su, nCells, sv, nCells, sw, nCells, au, nCells,
+		av, nCells, aw, nCells);
+	if (st != cupcfd::error::E_SUCCESS) return (int) st;
+	cupcfd::fvm::FluxUVWDolfynRegionLoop1(mesh);
+	cupcfd::fvm::FluxUVWDolfynBndsLoop1(mesh);
+	return (int) st;
+}

@@ -80,6 +80,56 @@ def test_uvw_face_loop1_bit_exact(cg, gpu, mk, order, first, geom):
     assert same(mesh.region_force_tangent(m["nRegions"]), O.uvw_bnds_loop1(m, want["shear"], ft0))
 
 
+def same32(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    if a.shape != b.shape or a.dtype != np.float32 or b.dtype != np.float32:
+        return False
+    na, nb = np.isnan(a), np.isnan(b)
+    return np.array_equal(na, nb) and np.array_equal(a[~na].view(np.int32), b[~nb].view(np.int32))
+
+
+@pytest.mark.parametrize("mk,order", [("struct", 1), ("jitter", 3)])
+@pytest.mark.parametrize("first", ["outlet", "inlet"])
+@pytest.mark.parametrize("geom", ["zero", "set"])
+def test_uvw_loops_float_instantiation_bit_exact(cg, gpu, mk, order, first, geom):
+    """The momentum loops with T=float arrays on a mesh uploaded from float
+    arrays (face loop, region loop, boundary loop in float) against the
+    reference's own float build, every output bit for bit."""
+    if O.load_ref() is None:
+        pytest.skip("reference build absent")
+    m, rng = uvw_case(mk, 80 + (mk == "jitter"), first)
+    f = O.uvw_fields(m, 83)
+    rl = bd = None
+    if geom == "set":
+        rl = rng.uniform(0.1, 2.0, m["nFaces"]).astype(np.float32)
+        bd = rng.uniform(0.01, 0.2, m["nBnd"]).astype(np.float32)
+    want = O.ref_uvw_loops_f32(m, f, rl, bd)
+    m32 = dict(m)
+    for k in ("faceLambda", "faceArea", "faceNorm", "faceCenter", "cellCenter", "cellVolume"):
+        m32[k] = np.ascontiguousarray(np.asarray(m[k]), np.float32)
+    r32 = dict(m, regionUVW=np.asarray(m["regionUVW"], np.float32).astype(np.float64),
+               regionDen=np.asarray(m["regionDen"], np.float32).astype(np.float64))
+    mesh = cg.Mesh.from_arrays(m32, order=order)
+    assert mesh.set_regions(r32["regionType"], r32["regionUVW"], r32["regionDen"], r32["bndRegion"]) == cg.E_SUCCESS
+    if rl is not None:
+        assert mesh.set_face_rlencos(rl.astype(np.float64)) == cg.E_SUCCESS
+        assert mesh.set_boundary_distance(bd.astype(np.float64)) == cg.E_SUCCESS
+    g = {k: np.ascontiguousarray(f[k], np.float32) for k in ("u", "v", "w", "visC", "visB", "dudx", "dvdx", "dwdx")}
+    out = {k: np.array(f[k], np.float32, copy=True) for k in O.UVW_INOUT}
+    rc = cg.FluxUVWDolfynFaceLoop1(mesh, np.float32(f["gammaBlend"]), np.float32(f["small"]), g["u"], g["v"], g["w"],
+                                   out["uB"], out["vB"], out["wB"], g["visC"], g["visB"], out["massFlux"], g["dudx"],
+                                   g["dvdx"], g["dwdx"], out["rFace"], out["su"], out["sv"], out["sw"], out["au"],
+                                   out["av"], out["aw"])
+    assert rc == cg.E_SUCCESS, cg.last_error()
+    for k in O.UVW_INOUT:
+        assert same32(out[k], want[k]), k
+    assert same32(mesh.boundary_shear().astype(np.float32), want["shear"])
+    mesh.region_force_tangent(m["nRegions"], np.full((m["nRegions"], 3), 7.0))
+    assert cg.FluxUVWDolfynRegionLoop1(mesh) == cg.E_SUCCESS
+    assert cg.FluxUVWDolfynBndsLoop1(mesh) == cg.E_SUCCESS
+    assert same32(mesh.region_force_tangent(m["nRegions"]).astype(np.float32), want["forceTangent"])
+
+
 @pytest.mark.parametrize("order", [0, 1, 3])
 def test_uvw_default_regions(cg, gpu, order):
     """The generated mesh with its single default region (what the

@@ -212,6 +212,31 @@ def test_uvw_face_loop1_bit_exact(mk, first, geom):
     assert_same_bits({"ft": O.uvw_bnds_loop1(m, got["shear"], ft0)}, {"ft": ft1}, ("ft",))
 
 
+@pytest.mark.parametrize("mk", ["struct", "jitter"])
+@pytest.mark.parametrize("first", ["outlet", "inlet"])
+@pytest.mark.parametrize("geom", ["zero", "set"])
+def test_uvw_loops_float_instantiation_bit_exact(mk, first, geom):
+    """The momentum loops of the reference's T=float instantiation (face
+    loop, region loop, boundary loop): the C float restatement against the
+    reference's own float build, every output bit for bit, infinities and
+    NaNs of the zero-distance case included."""
+    m, rng = uvw_case(mk, 70 + (mk == "jitter"), first)
+    f = O.uvw_fields(m, 71)
+    rl = bd = None
+    if geom == "set":
+        rl = rng.uniform(0.1, 2.0, m["nFaces"])
+        bd = rng.uniform(0.01, 0.2, m["nBnd"])
+    want = O.ref_uvw_loops_f32(m, f, rl, bd)
+    got = O.uvw_loops_f32(m, f, rl, bd)
+    for k in O.UVW_INOUT + ("shear", "forceTangent"):
+        a, b = np.asarray(got[k]), np.asarray(want[k])
+        assert a.dtype == b.dtype == np.float32 and a.shape == b.shape, k
+        assert np.array_equal(a.view(np.int32), b.view(np.int32)), k
+    if geom == "set":
+        bt = m["regionType"][m["bndRegion"]]
+        assert np.any(got["shear"][bt == 4] != 0) and np.all(np.isfinite(got["su"]))
+
+
 @pytest.mark.parametrize("max_cells", [3, 6])
 def test_polyhedral_mesh_bit_exact(max_cells):
     """Cells of 6 to 26 faces (hexahedra merged across removed faces): the
