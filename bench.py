@@ -674,40 +674,49 @@ def run_gpu(a):
         "loss_rel": abs(float(loss.item()) - float(loss64.item())) / abs(float(loss64.item())),
     }
 
-    # ---- end to end through the reference-facing host-buffer call
-    e2e = None
+    # ---- end to end through the reference-facing host-buffer call: float
+    # host arrays (the FP32 path's own storage type, the reference's T = float
+    # arrays), and for comparison the FP64 arrays of the T = double call
     K2 = max(1, min(K, a.e2e_steps))
-    hb = {}
-    for nm, cnt in (("phi", nC), ("phiB", nB), ("den", nC), ("u", nC), ("v", nC), ("w", nC), ("gface", nF)):
-        hb[nm] = torch.empty(cnt, dtype=torch.float64, pin_memory=True)
-    hb["phi"].copy_(phi64.cpu()); hb["phiB"].copy_(phiB64.cpu())
-    hb["den"].copy_(rho.double().cpu()); hb["u"].copy_(uvw[0].double().cpu())
-    hb["v"].copy_(uvw[1].double().cpu()); hb["w"].copy_(uvw[2].double().cpu()); hb["gface"].copy_(gf64.cpu())
-    out = {"grad": torch.empty(nC, 3, dtype=torch.float64, pin_memory=True),
-           "massFlux": torch.empty(nF, dtype=torch.float64, pin_memory=True),
-           "phiBar": torch.empty(nC, dtype=torch.float64, pin_memory=True),
-           "phiBBar": torch.empty(nB, dtype=torch.float64, pin_memory=True),
-           "denBar": torch.empty(nC, dtype=torch.float64, pin_memory=True),
-           "uBar": torch.empty(nC, dtype=torch.float64, pin_memory=True),
-           "vBar": torch.empty(nC, dtype=torch.float64, pin_memory=True),
-           "wBar": torch.empty(nC, dtype=torch.float64, pin_memory=True),
-           "loss": torch.empty(1, dtype=torch.float64, pin_memory=True)}
-    hn = {k: v.numpy() for k, v in hb.items()}
-    on = {k: v.numpy() for k, v in out.items()}
-    args_e2e = (mesh, F32, hn["phi"], hn["phiB"], hn["den"], hn["u"], hn["v"], hn["w"], hn["gface"])
-    cg.forward_adjoint(*args_e2e, out=on)   # warm (allocates the mesh's scratch buffers)
-    if dist:
-        dist.barrier()
-    t0 = time.perf_counter()
-    for _ in range(K2):
-        cg.forward_adjoint(*args_e2e, out=on)
-    te = (time.perf_counter() - t0) / K2
-    te = max_over_ranks(te, dist, dev)
-    h2d = 8 * (5 * nC + nB + nF)
-    d2h = 8 * (3 * nC + nF + 5 * nC + nB + 1)
-    e2e = {"value": job_gfaces(world, nF, te), "unit": "Gfaces/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-           "ms_per_step": te * 1e3, "steps": K2,
-           "call": "cupcfd_gpu_forward_adjoint (host FP64 buffers in reference numbering, pinned)"}
+
+    def host_call(dt, steps):
+        hb = {}
+        for nm, cnt in (("phi", nC), ("phiB", nB), ("den", nC), ("u", nC), ("v", nC), ("w", nC), ("gface", nF)):
+            hb[nm] = torch.empty(cnt, dtype=dt, pin_memory=True)
+        hb["phi"].copy_(phi.cpu()); hb["phiB"].copy_(phiB.cpu())
+        hb["den"].copy_(rho.cpu()); hb["u"].copy_(uvw[0].cpu())
+        hb["v"].copy_(uvw[1].cpu()); hb["w"].copy_(uvw[2].cpu()); hb["gface"].copy_(gface.cpu())
+        out = {"grad": torch.empty(nC, 3, dtype=dt, pin_memory=True),
+               "massFlux": torch.empty(nF, dtype=dt, pin_memory=True),
+               "phiBar": torch.empty(nC, dtype=dt, pin_memory=True),
+               "phiBBar": torch.empty(nB, dtype=dt, pin_memory=True),
+               "denBar": torch.empty(nC, dtype=dt, pin_memory=True),
+               "uBar": torch.empty(nC, dtype=dt, pin_memory=True),
+               "vBar": torch.empty(nC, dtype=dt, pin_memory=True),
+               "wBar": torch.empty(nC, dtype=dt, pin_memory=True),
+               "loss": torch.empty(1, dtype=torch.float64, pin_memory=True)}
+        hn = {k: v.numpy() for k, v in hb.items()}
+        on = {k: v.numpy() for k, v in out.items()}
+        args = (mesh, F32, hn["phi"], hn["phiB"], hn["den"], hn["u"], hn["v"], hn["w"], hn["gface"])
+        cg.forward_adjoint(*args, out=on)   # warm (allocates the mesh's scratch buffers)
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            cg.forward_adjoint(*args, out=on)
+        te = (time.perf_counter() - t0) / steps
+        te = max_over_ranks(te, dist, dev)
+        es = torch.tensor([], dtype=dt).element_size()
+        h2d = es * (5 * nC + nB + nF)
+        d2h = es * (3 * nC + nF + 5 * nC + nB) + 8
+        return {"value": job_gfaces(world, nF, te), "unit": "Gfaces/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "ms_per_step": te * 1e3, "steps": steps}
+
+    e2e = host_call(torch.float32, K2)
+    e2e["call"] = ("cupcfd_gpu_forward_adjoint_f32 (pinned host float arrays in the reference's numbering: the "
+                   "FP32 path's storage type, the reference's T = float arrays)")
+    e2e_f64 = host_call(torch.float64, max(1, K2 // 2))
+    e2e_f64["call"] = "cupcfd_gpu_forward_adjoint (pinned host FP64 arrays in the reference's numbering)"
 
     # ---- roofline of the dominant kernel, from the device timers of the timed region
     bm = bytes_model(nC, nF, nFi, nB)
@@ -785,6 +794,7 @@ def run_gpu(a):
                                      "ms_per_step": ms64fa},
             "error_vs_fp64": errors,
             "e2e": e2e,
+            "e2e_fp64_host_arrays": e2e_f64,
             "cpu_baseline": cpu,
             "uvw_face_loop1": uvw,
             "next_rows": rows,

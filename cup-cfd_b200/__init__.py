@@ -142,6 +142,7 @@ SIGNATURES = {
                                                   + [_VP, _I] * 10 + [C.c_float] + [_VP] * 4 + [_I] * 4
                                                   + [_VP, _I] * 8, _I),
     "cupcfd_gpu_forward_adjoint": ([_VP, _I] + [_VP] * 16, _I),
+    "cupcfd_gpu_forward_adjoint_f32": ([_VP, _I] + [_VP] * 16, _I),
     "cupcfd_gpu_dev_permute_cells": ([_VP, _I, _I, _VP, _I, _I64, _VP, _I, _I64, _VP], _I),
     "cupcfd_gpu_dev_permute_faces": ([_VP, _I, _VP, _I, _VP, _I, _VP], _I),
     "cupcfd_gpu_dev_gradient": ([_VP, _I, _I, _I, _VP, _VP, _VP, _VP, _VP], _I),
@@ -466,15 +467,19 @@ def FluxMassDolfynFaceLoop(mesh, dudx, dvdx, dwdx, dpdx, denCell, denBoundary, u
 
 def forward_adjoint(mesh, precision, phi, phiB, den, u, v, w, gface, out=None):
     """Forward + adjoint of the benchmark loss through host buffers.
-    Returns a dict of host FP64 arrays (grad (n,3), massFlux, phiBar,
-    phiBBar, denBar, uBar, vBar, wBar, loss)."""
+    Returns a dict of host arrays (grad (n,3), massFlux, phiBar, phiBBar,
+    denBar, uBar, vBar, wBar; FP64, or float32 when phi is float32 -- the
+    float-array call, cupcfd_gpu_forward_adjoint_f32) and loss (FP64)."""
     nC, nF, nB = mesh.nCells, mesh.nFaces, mesh.nBoundaries
+    f32 = np.asarray(phi).dtype == np.float32
+    dt = np.float32 if f32 else np.float64
     if out is None:
-        out = dict(grad=np.empty((nC, 3)), massFlux=np.empty(nF), phiBar=np.empty(nC), phiBBar=np.empty(nB),
-                   denBar=np.empty(nC), uBar=np.empty(nC), vBar=np.empty(nC), wBar=np.empty(nC), loss=np.empty(1))
-    check(lib().cupcfd_gpu_forward_adjoint(mesh.h, precision, _p(phi), _p(phiB), _p(den), _p(u), _p(v), _p(w), _p(gface),
-                                           *[_p(out[k]) for k in ("grad", "massFlux", "phiBar", "phiBBar", "denBar",
-                                                                  "uBar", "vBar", "wBar", "loss")]))
+        out = dict(grad=np.empty((nC, 3), dt), massFlux=np.empty(nF, dt), phiBar=np.empty(nC, dt),
+                   phiBBar=np.empty(nB, dt), denBar=np.empty(nC, dt), uBar=np.empty(nC, dt), vBar=np.empty(nC, dt),
+                   wBar=np.empty(nC, dt), loss=np.empty(1))
+    fn = lib().cupcfd_gpu_forward_adjoint_f32 if f32 else lib().cupcfd_gpu_forward_adjoint
+    check(fn(mesh.h, precision, _p(phi), _p(phiB), _p(den), _p(u), _p(v), _p(w), _p(gface),
+             *[_p(out[k]) for k in ("grad", "massFlux", "phiBar", "phiBBar", "denBar", "uBar", "vBar", "wBar", "loss")]))
     return out
 
 

@@ -876,12 +876,15 @@ int launch_adj_part(const cupcfd_gpu_mesh *m, bool f64, const void *g, double hs
 // The kernels are the device calls' (gradient, mass flux, the two parts of
 // the adjoint, and the loss from the stored gradient and mass fluxes), whose
 // results equal cupcfd_gpu_dev_forward_adjoint's bit for bit.
-extern "C" int cupcfd_gpu_forward_adjoint(cupcfd_gpu_mesh *m, int32_t precision, const double *phi, const double *phiB,
-                                          const double *den, const double *u, const double *v, const double *w,
-                                          const double *gface, double *grad, double *massFlux, double *phiBar,
-                                          double *phiBBar, double *denBar, double *uBar, double *vBar, double *wBar,
-                                          double *loss) {
-    clear_error();
+namespace {
+// The host-buffer forward+adjoint over host arrays of type H (double: the
+// reference's T = double arrays; float: T = float arrays, half the bytes on
+// the host link). The compute precision is `precision` either way.
+template <class H>
+int forward_adjoint_t(cupcfd_gpu_mesh *m, int32_t precision, const H *phi, const H *phiB, const H *den, const H *u,
+                      const H *v, const H *w, const H *gface, H *grad, H *massFlux, H *phiBar, H *phiBBar, H *denBar,
+                      H *uBar, H *vBar, H *wBar, double *loss) {
+    constexpr size_t HS = sizeof(H);
     CG_RETURN_IF(!m || !phi || !den || !u || !v || !w || !gface || (m->nB > 0 && !phiB), CUPCFD_E_NULL_PTR,
                  "forward_adjoint: null input");
     CG_TRY(check_prec(m, precision));
@@ -894,12 +897,12 @@ extern "C" int cupcfd_gpu_forward_adjoint(cupcfd_gpu_mesh *m, int32_t precision,
     size_t es = f64 ? 8 : 4;
     CG_TRY(pipe_init(m));
     cudaStream_t so = m->outStream;
-    // host -> device staging (reference numbering, FP64)
-    double *in;
+    // host -> device staging (reference numbering, host type)
+    H *in;
     void *phiI, *phibI, *stI, *gI, *gradI, *mfI, *pbI, *pbbI, *sbI;
     CG_TRY(scratch(m, S_IN0, 5 * (size_t) nC + nB + nF, &in));
-    double *hPhi = in, *hR = in + nC, *hU = in + 2 * (size_t) nC, *hV = in + 3 * (size_t) nC, *hW = in + 4 * (size_t) nC;
-    double *hPb = in + 5 * (size_t) nC, *hG = hPb + nB;
+    H *hPhi = in, *hR = in + nC, *hU = in + 2 * (size_t) nC, *hV = in + 3 * (size_t) nC, *hW = in + 4 * (size_t) nC;
+    H *hPb = in + 5 * (size_t) nC, *hG = hPb + nB;
     // internal numbering, compute precision
     CG_TRY(m->scratchBuf(S_IN1, (size_t) nC * es, &phiI));
     CG_TRY(m->scratchBuf(S_IN2, (size_t) std::max(nB, 1) * es, &phibI));
@@ -910,23 +913,27 @@ extern "C" int cupcfd_gpu_forward_adjoint(cupcfd_gpu_mesh *m, int32_t precision,
     CG_TRY(m->scratchBuf(S_OUT2, (size_t) nC * es, &pbI));
     CG_TRY(m->scratchBuf(S_OUT3, (size_t) std::max(nB, 1) * es, &pbbI));
     CG_TRY(m->scratchBuf(S_OUT4, 4 * (size_t) nC * es, &sbI));
-    double *dloss, *part, *out;
+    double *dloss, *part;
+    H *out;
     CG_TRY(scratch(m, S_NORM, 1, &dloss));
     CG_TRY(scratch(m, S_LOSS, gC, &part));
     CG_TRY(scratch(m, S_IN5, 8 * (size_t) nC + nF + nB, &out));
-    double *oG = out, *oMf = out + 3 * (size_t) nC, *oPb = oMf + nF, *oR = oPb + nC, *oU = oR + nC, *oV = oU + nC,
+    H *oG = out, *oMf = out + 3 * (size_t) nC, *oPb = oMf + nF, *oR = oPb + nC, *oU = oR + nC, *oV = oU + nC,
            *oW = oV + nC, *oPbb = oW + nC;
 
     // phi in, gradient
-    CG_CHECK_CUDA(cudaMemcpyAsync(hPhi, phi, 8 * (size_t) nC, cudaMemcpyHostToDevice, st));
-    if (nB > 0) CG_CHECK_CUDA(cudaMemcpyAsync(hPb, phiB, 8 * (size_t) nB, cudaMemcpyHostToDevice, st));
+    CG_CHECK_CUDA(cudaMemcpyAsync(hPhi, phi, HS * (size_t) nC, cudaMemcpyHostToDevice, st));
+    if (nB > 0) CG_CHECK_CUDA(cudaMemcpyAsync(hPb, phiB, HS * (size_t) nB, cudaMemcpyHostToDevice, st));
     if (f64) {
-        k_gather<double, double><<<gC, BLK, 0, st>>>(nC, 1, m->cellN2O, hPhi, 0, (double *) phiI, 0);
-        if (nB > 0) CG_CHECK_CUDA(cudaMemcpyAsync(phibI, hPb, 8 * (size_t) nB, cudaMemcpyDeviceToDevice, st));
-    } else {
-        k_gather<double, float><<<gC, BLK, 0, st>>>(nC, 1, m->cellN2O, hPhi, 0, (float *) phiI, 0);
+        k_gather<H, double><<<gC, BLK, 0, st>>>(nC, 1, m->cellN2O, hPhi, 0, (double *) phiI, 0);
         if (nB > 0) {
-            k_convert<double, float><<<grid_for(nB, BLK), BLK, 0, st>>>(nB, hPb, (float *) phibI);
+            k_convert<H, double><<<grid_for(nB, BLK), BLK, 0, st>>>(nB, hPb, (double *) phibI);
+            g_launches.fetch_add(1, std::memory_order_relaxed);
+        }
+    } else {
+        k_gather<H, float><<<gC, BLK, 0, st>>>(nC, 1, m->cellN2O, hPhi, 0, (float *) phiI, 0);
+        if (nB > 0) {
+            k_convert<H, float><<<grid_for(nB, BLK), BLK, 0, st>>>(nB, hPb, (float *) phibI);
             g_launches.fetch_add(1, std::memory_order_relaxed);
         }
     }
@@ -935,19 +942,19 @@ extern "C" int cupcfd_gpu_forward_adjoint(cupcfd_gpu_mesh *m, int32_t precision,
     CG_TRY(launch_adj_part(m, f64, gradI, 2.0, nullptr, nullptr, pbI, pbbI, nullptr, st));
     CG_CHECK_CUDA(cudaEventRecord(m->pipeEv[0], st));
     // state in, mass flux
-    CG_CHECK_CUDA(cudaMemcpyAsync(hR, den, 8 * (size_t) nC, cudaMemcpyHostToDevice, st));
-    CG_CHECK_CUDA(cudaMemcpyAsync(hU, u, 8 * (size_t) nC, cudaMemcpyHostToDevice, st));
-    CG_CHECK_CUDA(cudaMemcpyAsync(hV, v, 8 * (size_t) nC, cudaMemcpyHostToDevice, st));
-    CG_CHECK_CUDA(cudaMemcpyAsync(hW, w, 8 * (size_t) nC, cudaMemcpyHostToDevice, st));
-    if (f64) k_gather<double, double><<<gC, BLK, 0, st>>>(nC, 4, m->cellN2O, hR, nC, (double *) stI, ldc);
-    else k_state_to_f4<<<gC, BLK, 0, st>>>(nC, m->cellN2O, hR, hU, hV, hW, (float4 *) stI);
+    CG_CHECK_CUDA(cudaMemcpyAsync(hR, den, HS * (size_t) nC, cudaMemcpyHostToDevice, st));
+    CG_CHECK_CUDA(cudaMemcpyAsync(hU, u, HS * (size_t) nC, cudaMemcpyHostToDevice, st));
+    CG_CHECK_CUDA(cudaMemcpyAsync(hV, v, HS * (size_t) nC, cudaMemcpyHostToDevice, st));
+    CG_CHECK_CUDA(cudaMemcpyAsync(hW, w, HS * (size_t) nC, cudaMemcpyHostToDevice, st));
+    if (f64) k_gather<H, double><<<gC, BLK, 0, st>>>(nC, 4, m->cellN2O, hR, nC, (double *) stI, ldc);
+    else k_state_to_f4<H><<<gC, BLK, 0, st>>>(nC, m->cellN2O, hR, hU, hV, hW, (float4 *) stI);
     CG_LAUNCHED();
     CG_TRY(cupcfd_gpu_dev_mass_plain(m, precision, stI, mfI, st));
     CG_CHECK_CUDA(cudaEventRecord(m->pipeEv[1], st));
     // gface in, loss and adjoint
-    CG_CHECK_CUDA(cudaMemcpyAsync(hG, gface, 8 * (size_t) nF, cudaMemcpyHostToDevice, st));
-    if (f64) k_gather<double, double><<<gF, BLK, 0, st>>>(nF, 1, m->faceN2O, hG, 0, (double *) gI, 0);
-    else k_gather<double, float><<<gF, BLK, 0, st>>>(nF, 1, m->faceN2O, hG, 0, (float *) gI, 0);
+    CG_CHECK_CUDA(cudaMemcpyAsync(hG, gface, HS * (size_t) nF, cudaMemcpyHostToDevice, st));
+    if (f64) k_gather<H, double><<<gF, BLK, 0, st>>>(nF, 1, m->faceN2O, hG, 0, (double *) gI, 0);
+    else k_gather<H, float><<<gF, BLK, 0, st>>>(nF, 1, m->faceN2O, hG, 0, (float *) gI, 0);
     CG_LAUNCHED();
     if (f64)
         k_loss<double><<<gC, 256, 0, st>>>(nC, sell(m), (const double *) gI, (const double *) mfI,
@@ -961,42 +968,67 @@ extern "C" int cupcfd_gpu_forward_adjoint(cupcfd_gpu_mesh *m, int32_t precision,
     CG_TRY(launch_adj_part(m, f64, nullptr, 0.0, stI, gI, nullptr, nullptr, sbI, st));
     CG_CHECK_CUDA(cudaEventRecord(m->pipeEv[2], st));
 
-    // back to reference numbering (FP64) and to the host, on the copy stream
+    // back to reference numbering (host type) and to the host, on the copy stream
     CG_CHECK_CUDA(cudaStreamWaitEvent(so, m->pipeEv[0], 0));
     if (f64) {
-        k_blocks_to_aos<double, double><<<gC, BLK, 0, so>>>(nC, 3, m->cellO2N, (const double *) gradI, ldc, oG);
-        k_gather<double, double><<<gC, BLK, 0, so>>>(nC, 1, m->cellO2N, (const double *) pbI, 0, oPb, 0);
-        if (nB > 0) CG_CHECK_CUDA(cudaMemcpyAsync(oPbb, pbbI, 8 * (size_t) nB, cudaMemcpyDeviceToDevice, so));
-    } else {
-        k_blocks_to_aos<float, double><<<gC, BLK, 0, so>>>(nC, 3, m->cellO2N, (const float *) gradI, ldc, oG);
-        k_gather<float, double><<<gC, BLK, 0, so>>>(nC, 1, m->cellO2N, (const float *) pbI, 0, oPb, 0);
+        k_blocks_to_aos<double, H><<<gC, BLK, 0, so>>>(nC, 3, m->cellO2N, (const double *) gradI, ldc, oG);
+        k_gather<double, H><<<gC, BLK, 0, so>>>(nC, 1, m->cellO2N, (const double *) pbI, 0, oPb, 0);
         if (nB > 0) {
-            k_convert<float, double><<<grid_for(nB, BLK), BLK, 0, so>>>(nB, (const float *) pbbI, oPbb);
+            k_convert<double, H><<<grid_for(nB, BLK), BLK, 0, so>>>(nB, (const double *) pbbI, oPbb);
+            g_launches.fetch_add(1, std::memory_order_relaxed);
+        }
+    } else {
+        k_blocks_to_aos<float, H><<<gC, BLK, 0, so>>>(nC, 3, m->cellO2N, (const float *) gradI, ldc, oG);
+        k_gather<float, H><<<gC, BLK, 0, so>>>(nC, 1, m->cellO2N, (const float *) pbI, 0, oPb, 0);
+        if (nB > 0) {
+            k_convert<float, H><<<grid_for(nB, BLK), BLK, 0, so>>>(nB, (const float *) pbbI, oPbb);
             g_launches.fetch_add(1, std::memory_order_relaxed);
         }
     }
     g_launches.fetch_add(1, std::memory_order_relaxed);
     CG_LAUNCHED();
-    if (grad) CG_CHECK_CUDA(cudaMemcpyAsync(grad, oG, 24 * (size_t) nC, cudaMemcpyDeviceToHost, so));
-    if (phiBar) CG_CHECK_CUDA(cudaMemcpyAsync(phiBar, oPb, 8 * (size_t) nC, cudaMemcpyDeviceToHost, so));
-    if (phiBBar && nB > 0) CG_CHECK_CUDA(cudaMemcpyAsync(phiBBar, oPbb, 8 * (size_t) nB, cudaMemcpyDeviceToHost, so));
+    if (grad) CG_CHECK_CUDA(cudaMemcpyAsync(grad, oG, 3 * HS * (size_t) nC, cudaMemcpyDeviceToHost, so));
+    if (phiBar) CG_CHECK_CUDA(cudaMemcpyAsync(phiBar, oPb, HS * (size_t) nC, cudaMemcpyDeviceToHost, so));
+    if (phiBBar && nB > 0) CG_CHECK_CUDA(cudaMemcpyAsync(phiBBar, oPbb, HS * (size_t) nB, cudaMemcpyDeviceToHost, so));
     CG_CHECK_CUDA(cudaStreamWaitEvent(so, m->pipeEv[1], 0));
-    if (f64) k_faces_to_ref<double><<<gF, BLK, 0, so>>>(nF, m->faceO2N, m->faceCells, (const double *) mfI, oMf, 1);
-    else k_faces_to_ref<float><<<gF, BLK, 0, so>>>(nF, m->faceO2N, m->faceCells, (const float *) mfI, oMf, 1);
+    if (f64) k_faces_to_ref<double, H><<<gF, BLK, 0, so>>>(nF, m->faceO2N, m->faceCells, (const double *) mfI, oMf, 1);
+    else k_faces_to_ref<float, H><<<gF, BLK, 0, so>>>(nF, m->faceO2N, m->faceCells, (const float *) mfI, oMf, 1);
     CG_LAUNCHED();
-    if (massFlux) CG_CHECK_CUDA(cudaMemcpyAsync(massFlux, oMf, 8 * (size_t) nF, cudaMemcpyDeviceToHost, so));
+    if (massFlux) CG_CHECK_CUDA(cudaMemcpyAsync(massFlux, oMf, HS * (size_t) nF, cudaMemcpyDeviceToHost, so));
     CG_CHECK_CUDA(cudaStreamWaitEvent(so, m->pipeEv[2], 0));
-    if (f64) k_gather<double, double><<<gC, BLK, 0, so>>>(nC, 4, m->cellO2N, (const double *) sbI, ldc, oR, nC);
-    else k_f4_to_ref<<<gC, BLK, 0, so>>>(nC, m->cellO2N, (const float4 *) sbI, oR, oU, oV, oW);
+    if (f64) k_gather<double, H><<<gC, BLK, 0, so>>>(nC, 4, m->cellO2N, (const double *) sbI, ldc, oR, nC);
+    else k_f4_to_ref<H><<<gC, BLK, 0, so>>>(nC, m->cellO2N, (const float4 *) sbI, oR, oU, oV, oW);
     CG_LAUNCHED();
-    if (denBar) CG_CHECK_CUDA(cudaMemcpyAsync(denBar, oR, 8 * (size_t) nC, cudaMemcpyDeviceToHost, so));
-    if (uBar) CG_CHECK_CUDA(cudaMemcpyAsync(uBar, oU, 8 * (size_t) nC, cudaMemcpyDeviceToHost, so));
-    if (vBar) CG_CHECK_CUDA(cudaMemcpyAsync(vBar, oV, 8 * (size_t) nC, cudaMemcpyDeviceToHost, so));
-    if (wBar) CG_CHECK_CUDA(cudaMemcpyAsync(wBar, oW, 8 * (size_t) nC, cudaMemcpyDeviceToHost, so));
+    if (denBar) CG_CHECK_CUDA(cudaMemcpyAsync(denBar, oR, HS * (size_t) nC, cudaMemcpyDeviceToHost, so));
+    if (uBar) CG_CHECK_CUDA(cudaMemcpyAsync(uBar, oU, HS * (size_t) nC, cudaMemcpyDeviceToHost, so));
+    if (vBar) CG_CHECK_CUDA(cudaMemcpyAsync(vBar, oV, HS * (size_t) nC, cudaMemcpyDeviceToHost, so));
+    if (wBar) CG_CHECK_CUDA(cudaMemcpyAsync(wBar, oW, HS * (size_t) nC, cudaMemcpyDeviceToHost, so));
     if (loss) CG_CHECK_CUDA(cudaMemcpyAsync(loss, dloss, 8, cudaMemcpyDeviceToHost, so));
     CG_CHECK_CUDA(cudaStreamSynchronize(so));
     CG_CHECK_CUDA(cudaStreamSynchronize(st));
     return CUPCFD_E_SUCCESS;
+}
+
+}  // namespace
+
+extern "C" int cupcfd_gpu_forward_adjoint(cupcfd_gpu_mesh *m, int32_t precision, const double *phi, const double *phiB,
+                                          const double *den, const double *u, const double *v, const double *w,
+                                          const double *gface, double *grad, double *massFlux, double *phiBar,
+                                          double *phiBBar, double *denBar, double *uBar, double *vBar, double *wBar,
+                                          double *loss) {
+    clear_error();
+    return forward_adjoint_t<double>(m, precision, phi, phiB, den, u, v, w, gface, grad, massFlux, phiBar, phiBBar,
+                                     denBar, uBar, vBar, wBar, loss);
+}
+
+extern "C" int cupcfd_gpu_forward_adjoint_f32(cupcfd_gpu_mesh *m, int32_t precision, const float *phi, const float *phiB,
+                                              const float *den, const float *u, const float *v, const float *w,
+                                              const float *gface, float *grad, float *massFlux, float *phiBar,
+                                              float *phiBBar, float *denBar, float *uBar, float *vBar, float *wBar,
+                                              double *loss) {
+    clear_error();
+    return forward_adjoint_t<float>(m, precision, phi, phiB, den, u, v, w, gface, grad, massFlux, phiBar, phiBBar,
+                                    denBar, uBar, vBar, wBar, loss);
 }
 
 // ===========================================================================

@@ -42,16 +42,18 @@ __global__ void k_blocks_to_aos(int n, int ncomp, const int *__restrict__ o2n, c
 }
 
 // float4 state <-> blocks
-__global__ void k_state_to_f4(int n, const int *__restrict__ n2o, const double *__restrict__ r, const double *__restrict__ u,
-                              const double *__restrict__ v, const double *__restrict__ w, float4 *__restrict__ out) {
+template <class TS>
+__global__ void k_state_to_f4(int n, const int *__restrict__ n2o, const TS *__restrict__ r, const TS *__restrict__ u,
+                              const TS *__restrict__ v, const TS *__restrict__ w, float4 *__restrict__ out) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int o = n2o[i];
     out[i] = make_float4((float) r[o], (float) u[o], (float) v[o], (float) w[o]);
 }
 
-__global__ void k_f4_to_ref(int n, const int *__restrict__ o2n, const float4 *__restrict__ in, double *__restrict__ r,
-                            double *__restrict__ u, double *__restrict__ v, double *__restrict__ w) {
+template <class TD>
+__global__ void k_f4_to_ref(int n, const int *__restrict__ o2n, const float4 *__restrict__ in, TD *__restrict__ r,
+                            TD *__restrict__ u, TD *__restrict__ v, TD *__restrict__ w) {
     int o = blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= n) return;
     float4 s = in[o2n[o]];
@@ -59,13 +61,13 @@ __global__ void k_f4_to_ref(int n, const int *__restrict__ o2n, const float4 *__
 }
 
 // face data internal -> reference (boundary entries zero when zeroBnd)
-template <class TS>
+template <class TS, class TD = double>
 __global__ void k_faces_to_ref(int nF, const int *__restrict__ o2n, const int2 *__restrict__ fcells, const TS *__restrict__ src,
-                               double *__restrict__ dst, int zeroBnd) {
+                               TD *__restrict__ dst, int zeroBnd) {
     int o = blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= nF) return;
     int i = o2n[o];
-    dst[o] = (zeroBnd && fcells[i].y < 0) ? 0.0 : (double) src[i];
+    dst[o] = (zeroBnd && fcells[i].y < 0) ? TD(0) : (TD) src[i];
 }
 
 template <class TS, class TD>

@@ -385,6 +385,16 @@ int cupcfd_gpu_forward_adjoint(cupcfd_gpu_mesh *mesh, int32_t precision,
                                const double *v, const double *w, const double *gface,
                                double *grad, double *massFlux, double *phiBar, double *phiBBar,
                                double *denBar, double *uBar, double *vBar, double *wBar, double *loss);
+/* The same call on float host arrays (the reference's T = float arrays):
+ * half the bytes cross the host link. With CUPCFD_PREC_F32C the kernels see
+ * exactly the values the FP64-array call gives them after its conversion,
+ * so every output is that call's, rounded to float (exactly: the FP32 path's
+ * outputs are float values). The loss stays double. */
+int cupcfd_gpu_forward_adjoint_f32(cupcfd_gpu_mesh *mesh, int32_t precision,
+                                   const float *phi, const float *phiB, const float *den, const float *u,
+                                   const float *v, const float *w, const float *gface,
+                                   float *grad, float *massFlux, float *phiBar, float *phiBBar,
+                                   float *denBar, float *uBar, float *vBar, float *wBar, double *loss);
 
 /* The boundary / region loops of the mass-flux step, FP64, bit-identical to
  * the reference (MassKernels.h:90-171, MassKernels.ipp:311-554): host

@@ -501,6 +501,25 @@ def test_host_call_matches_oracle(cg, gpu, order):
 
 
 @pytest.mark.parametrize("order", [1, 3])
+def test_host_call_float_arrays_equal_double_arrays(cg, gpu, order):
+    """The FP32 forward+adjoint through float host arrays
+    (cupcfd_gpu_forward_adjoint_f32) returns the FP64-array call's results
+    rounded to float, which are exact (the FP32 path's outputs are floats),
+    and the same loss."""
+    ref = O.jitter(14, 12, 11, 0.25, seed=18, permute=True)
+    mesh = cg.Mesh.from_arrays(ref, order=order)
+    f = O.fields(ref, 19)
+    gface = np.random.Generator(np.random.Philox(key=20)).standard_normal(ref["nFaces"])
+    ins = [as_f32(f[k]) for k in ("phi", "phiB", "den", "u", "v", "w")] + [as_f32(gface)]
+    o64 = cg.forward_adjoint(mesh, cg.PREC_F32C, *ins)
+    o32 = cg.forward_adjoint(mesh, cg.PREC_F32C, *[x.astype(np.float32) for x in ins])
+    for k in ("grad", "massFlux", "phiBar", "phiBBar", "denBar", "uBar", "vBar", "wBar"):
+        assert o32[k].dtype == np.float32, k
+        assert np.array_equal(o32[k].astype(np.float64), o64[k]), k
+    assert o32["loss"][0] == o64["loss"][0]
+
+
+@pytest.mark.parametrize("order", [1, 3])
 @pytest.mark.parametrize("prec", [0, 1])
 @pytest.mark.parametrize("mk", ["jitter", "poly"])
 def test_host_call_equals_device_call(cg, gpu, order, prec, mk):
