@@ -109,6 +109,14 @@ SIGNATURES = {
     "cupcfd_gpu_flux_mass_dolfyn_boundary_loop5": ([_VP, _VP, _I, _VP, _I, _VP, _I, _VP, _I, _VP, _I, _D, _I, _I, _I,
                                                     _VP, _I, _VP], _I),
     "cupcfd_gpu_flux_mass_dolfyn_region_loop": ([_VP, _VP, _I, _VP, _I, _D], _I),
+    "cupcfd_gpu_flux_mass_dolfyn_boundary_loop1_f32": ([_VP, _VP, _I, _VP], _I),
+    "cupcfd_gpu_flux_mass_dolfyn_boundary_loop2_f32": ([_VP, _VP, _I, _VP, _I, _VP], _I),
+    "cupcfd_gpu_flux_mass_dolfyn_boundary_loop3_f32": ([_VP, C.c_float, _VP], _I),
+    "cupcfd_gpu_flux_mass_dolfyn_boundary_loop4_f32": ([_VP, _VP, _I, _VP, _I, _VP, _I, _VP, _I, _VP, _I, C.c_float,
+                                                        _VP], _I),
+    "cupcfd_gpu_flux_mass_dolfyn_boundary_loop5_f32": ([_VP, _VP, _I, _VP, _I, _VP, _I, _VP, _I, _VP, _I, C.c_float,
+                                                        _I, _I, _I, _VP, _I, _VP], _I),
+    "cupcfd_gpu_flux_mass_dolfyn_region_loop_f32": ([_VP, _VP, _I, _VP, _I, C.c_float], _I),
     "cupcfd_gpu_dev_boundary_loop1": ([_VP, _VP, _VP, _VP], _I),
     "cupcfd_gpu_dev_boundary_loop2": ([_VP, _VP, _VP, _VP, _VP], _I),
     "cupcfd_gpu_dev_boundary_loop3": ([_VP, _VP, _VP, _VP], _I),
@@ -554,52 +562,69 @@ def error_norms(a, b, floor=0.0, stream=None):
 # ---------------------------------------------------------------------------
 # boundary / region loops of the mass-flux step (MassKernels.ipp:311-554).
 # Host arrays in the reference's numbering; in/out arrays are updated in
-# place, scalar outputs returned. Each returns (status, outputs...).
+# place, scalar outputs returned. Each returns (status, outputs...). float64
+# arrays run the reference's T = double instantiation, float32 arrays its
+# T = float one (the _f32 calls); all arrays of a call share one type.
 # ---------------------------------------------------------------------------
-def _h(a):
-    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
-    return a
+def _bnd_kind(first, *rest):
+    dt = np.asarray(first).dtype
+    assert dt in (np.float64, np.float32), dt
+    for a in (first,) + rest:
+        assert a.dtype == dt and a.flags["C_CONTIGUOUS"], "arrays must share one real type and be contiguous"
+    f32 = dt == np.float32
+    return f32, (C.c_float if f32 else C.c_double), ("_f32" if f32 else "")
+
+
+def _bnd_fn(name, suffix):
+    return getattr(lib(), "cupcfd_gpu_flux_mass_dolfyn_" + name + suffix)
 
 
 def FluxMassDolfynBoundaryLoop1(mesh, massFlux):
-    out = C.c_double(np.nan)
-    rc = lib().cupcfd_gpu_flux_mass_dolfyn_boundary_loop1(mesh.h, _p(_h(massFlux)), len(massFlux), C.byref(out))
+    f32, S, sfx = _bnd_kind(massFlux)
+    out = S(np.nan)
+    rc = _bnd_fn("boundary_loop1", sfx)(mesh.h, _p(massFlux), len(massFlux), C.byref(out))
     return rc, out.value
 
 
 def FluxMassDolfynBoundaryLoop2(mesh, massFlux, flowRegion):
-    out = C.c_double(np.nan)
-    rc = lib().cupcfd_gpu_flux_mass_dolfyn_boundary_loop2(mesh.h, _p(_h(massFlux)), len(massFlux), _p(_h(flowRegion)),
-                                                          len(flowRegion), C.byref(out))
+    f32, S, sfx = _bnd_kind(massFlux, flowRegion)
+    out = S(np.nan)
+    rc = _bnd_fn("boundary_loop2", sfx)(mesh.h, _p(massFlux), len(massFlux), _p(flowRegion), len(flowRegion),
+                                        C.byref(out))
     return rc, out.value
 
 
-def FluxMassDolfynBoundaryLoop3(mesh, flowin):
-    out = C.c_double(np.nan)
-    rc = lib().cupcfd_gpu_flux_mass_dolfyn_boundary_loop3(mesh.h, float(flowin), C.byref(out))
+def FluxMassDolfynBoundaryLoop3(mesh, flowin, f32=False):
+    """f32: the T = float instantiation (flowin rounded to float)."""
+    S, sfx = (C.c_float, "_f32") if f32 else (C.c_double, "")
+    out = S(np.nan)
+    rc = _bnd_fn("boundary_loop3", sfx)(mesh.h, float(flowin), C.byref(out))
     return rc, out.value
 
 
 def FluxMassDolfynBoundaryLoop4(mesh, massFlux, uB, vB, wB, denB, ratearea):
-    out = C.c_double(np.nan)
-    rc = lib().cupcfd_gpu_flux_mass_dolfyn_boundary_loop4(
-        mesh.h, _p(_h(massFlux)), len(massFlux), _p(_h(uB)), len(uB), _p(_h(vB)), len(vB), _p(_h(wB)), len(wB),
-        _p(_h(denB)), len(denB), float(ratearea), C.byref(out))
+    f32, S, sfx = _bnd_kind(massFlux, uB, vB, wB, denB)
+    out = S(np.nan)
+    rc = _bnd_fn("boundary_loop4", sfx)(
+        mesh.h, _p(massFlux), len(massFlux), _p(uB), len(uB), _p(vB), len(vB), _p(wB), len(wB),
+        _p(denB), len(denB), float(ratearea), C.byref(out))
     return rc, out.value
 
 
 def FluxMassDolfynBoundaryLoop5(mesh, massFlux, su, uB, vB, wB, fact, solve, flowFact, flowout2):
-    out = C.c_double(flowout2)
-    rc = lib().cupcfd_gpu_flux_mass_dolfyn_boundary_loop5(
-        mesh.h, _p(_h(massFlux)), len(massFlux), _p(_h(su)), len(su), _p(_h(uB)), len(uB), _p(_h(vB)), len(vB),
-        _p(_h(wB)), len(wB), float(fact), *[int(bool(x)) for x in solve], _p(_h(flowFact)), len(flowFact),
+    f32, S, sfx = _bnd_kind(massFlux, su, uB, vB, wB, flowFact)
+    out = S(flowout2)
+    rc = _bnd_fn("boundary_loop5", sfx)(
+        mesh.h, _p(massFlux), len(massFlux), _p(su), len(su), _p(uB), len(uB), _p(vB), len(vB),
+        _p(wB), len(wB), float(fact), *[int(bool(x)) for x in solve], _p(flowFact), len(flowFact),
         C.byref(out))
     return rc, out.value
 
 
 def FluxMassDolfynRegionLoop(mesh, flowFact, flowRegion, flowIn):
-    return lib().cupcfd_gpu_flux_mass_dolfyn_region_loop(mesh.h, _p(_h(flowFact)), len(flowFact), _p(_h(flowRegion)),
-                                                        len(flowRegion), float(flowIn))
+    f32, S, sfx = _bnd_kind(flowFact, flowRegion)
+    return _bnd_fn("region_loop", sfx)(mesh.h, _p(flowFact), len(flowFact), _p(flowRegion), len(flowRegion),
+                                       float(flowIn))
 
 
 def dev_boundary_loop1(mesh, massFlux, flowin, stream=None):

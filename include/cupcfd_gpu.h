@@ -428,6 +428,30 @@ int cupcfd_gpu_flux_mass_dolfyn_boundary_loop5(cupcfd_gpu_mesh *mesh, double *ma
 int cupcfd_gpu_flux_mass_dolfyn_region_loop(cupcfd_gpu_mesh *mesh, double *flowFact, int32_t nFlowFact,
                                            const double *flowRegion, int32_t nFlowRegion, double flowIn);
 
+/* The same loops, the reference's T = float instantiation
+ * (MassKernels.ipp:311-554 with T = float): float host arrays, float
+ * arithmetic in the reference's order, bit-identical to it. The mesh's
+ * geometry and split levels enter rounded to float (exact for a mesh made
+ * from float arrays, as the reference's float mesh is). */
+int cupcfd_gpu_flux_mass_dolfyn_boundary_loop1_f32(cupcfd_gpu_mesh *mesh, const float *massFlux, int32_t nMassFlux,
+                                                   float *flowin);
+int cupcfd_gpu_flux_mass_dolfyn_boundary_loop2_f32(cupcfd_gpu_mesh *mesh, const float *massFlux, int32_t nMassFlux,
+                                                   float *flowRegion, int32_t nFlowRegion, float *flowout);
+int cupcfd_gpu_flux_mass_dolfyn_boundary_loop3_f32(cupcfd_gpu_mesh *mesh, float flowin, float *ratearea);
+int cupcfd_gpu_flux_mass_dolfyn_boundary_loop4_f32(cupcfd_gpu_mesh *mesh, float *massFlux, int32_t nMassFlux,
+                                                   float *uBoundary, int32_t nUBoundary, float *vBoundary,
+                                                   int32_t nVBoundary, float *wBoundary, int32_t nWBoundary,
+                                                   const float *denBoundary, int32_t nDenBoundary, float ratearea,
+                                                   float *flowout);
+int cupcfd_gpu_flux_mass_dolfyn_boundary_loop5_f32(cupcfd_gpu_mesh *mesh, float *massFlux, int32_t nMassFlux,
+                                                   float *su, int32_t nSu, float *uBoundary, int32_t nUBoundary,
+                                                   float *vBoundary, int32_t nVBoundary, float *wBoundary,
+                                                   int32_t nWBoundary, float fact, int32_t solveU, int32_t solveV,
+                                                   int32_t solveW, const float *flowFact, int32_t nFlowFact,
+                                                   float *flowout2);
+int cupcfd_gpu_flux_mass_dolfyn_region_loop_f32(cupcfd_gpu_mesh *mesh, float *flowFact, int32_t nFlowFact,
+                                               const float *flowRegion, int32_t nFlowRegion, float flowIn);
+
 /* ------------------------------------------------------------------------ */
 /* device-resident calls (device pointers, internal numbering, async)        */
 /* ------------------------------------------------------------------------ */

@@ -4,9 +4,11 @@
 //   cupcfd::fvm::GradientPhiGaussDolfyn  (include/fvm/implementation/component/GradientKernels.h:48-54)
 //   cupcfd::fvm::FluxMassDolfynFaceLoop  (include/fvm/implementation/component/MassKernels.h:48-81),
 //                                        for T = double and T = float meshes
-//   cupcfd::fvm::FluxMassDolfynBoundaryLoop1-5, FluxMassDolfynRegionLoop (MassKernels.h:90-171)
+//   cupcfd::fvm::FluxMassDolfynBoundaryLoop1-5, FluxMassDolfynRegionLoop (MassKernels.h:90-171),
+//                                        for T = double and T = float
 //   cupcfd::fvm::FluxUVWDolfynFaceLoop1, FluxUVWDolfynRegionLoop1, FluxUVWDolfynBndsLoop1
-//                                        (include/fvm/implementation/component/UVWKernels.h:45-92)
+//                                        (include/fvm/implementation/component/UVWKernels.h:45-92),
+//                                        face loop for T = double and T = float
 // in namespace cupcfd::fvm::gpu, so a call site switches by namespace only:
 //
 //   status = cupcfd::fvm::gpu::GradientPhiGaussDolfyn(mesh, nGradient, phiCell, nPhiCell,
@@ -381,6 +383,70 @@ ecode_t FluxMassDolfynRegionLoop(Mesh &mesh, double *flowFact, I nFlowFact, doub
     if (rc != CUPCFD_E_SUCCESS) return (ecode_t) rc;
     return (ecode_t) cupcfd_gpu_flux_mass_dolfyn_region_loop(m, flowFact, (int32_t) nFlowFact, flowRegion,
                                                             (int32_t) nFlowRegion, flowIn);
+}
+
+// The same loops, T = float: the reference's float instantiation on a
+// CupCfdSoAMesh<int,float,int> (float arithmetic in the reference's order).
+template <class Mesh, class I>
+ecode_t FluxMassDolfynBoundaryLoop1(Mesh &mesh, float *massFlux, I nMassFlux, float *flowin) {
+    cupcfd_gpu_mesh *m = nullptr;
+    int rc = attach(mesh, &m);
+    if (rc != CUPCFD_E_SUCCESS) return (ecode_t) rc;
+    return (ecode_t) cupcfd_gpu_flux_mass_dolfyn_boundary_loop1_f32(m, massFlux, (int32_t) nMassFlux, flowin);
+}
+
+template <class Mesh, class I>
+ecode_t FluxMassDolfynBoundaryLoop2(Mesh &mesh, float *massFlux, I nMassFlux, float *flowRegion, I nFlowRegion,
+                                    float *flowout) {
+    cupcfd_gpu_mesh *m = nullptr;
+    int rc = attach(mesh, &m);
+    if (rc != CUPCFD_E_SUCCESS) return (ecode_t) rc;
+    return (ecode_t) cupcfd_gpu_flux_mass_dolfyn_boundary_loop2_f32(m, massFlux, (int32_t) nMassFlux, flowRegion,
+                                                                    (int32_t) nFlowRegion, flowout);
+}
+
+template <class Mesh>
+ecode_t FluxMassDolfynBoundaryLoop3(Mesh &mesh, float flowin, float *ratearea) {
+    cupcfd_gpu_mesh *m = nullptr;
+    int rc = attach(mesh, &m);
+    if (rc != CUPCFD_E_SUCCESS) return (ecode_t) rc;
+    return (ecode_t) cupcfd_gpu_flux_mass_dolfyn_boundary_loop3_f32(m, flowin, ratearea);
+}
+
+template <class Mesh, class I>
+ecode_t FluxMassDolfynBoundaryLoop4(Mesh &mesh, float *massFlux, I nMassFlux, float *uBoundary, I nUBoundary,
+                                    float *vBoundary, I nVboundary, float *wBoundary, I nWBoundary,
+                                    float *denBoundary, I nDenBoundary, float ratearea, float *flowout) {
+    cupcfd_gpu_mesh *m = nullptr;
+    int rc = attach(mesh, &m);
+    if (rc != CUPCFD_E_SUCCESS) return (ecode_t) rc;
+    return (ecode_t) cupcfd_gpu_flux_mass_dolfyn_boundary_loop4_f32(
+        m, massFlux, (int32_t) nMassFlux, uBoundary, (int32_t) nUBoundary, vBoundary, (int32_t) nVboundary, wBoundary,
+        (int32_t) nWBoundary, denBoundary, (int32_t) nDenBoundary, ratearea, flowout);
+}
+
+template <class Mesh, class I>
+ecode_t FluxMassDolfynBoundaryLoop5(Mesh &mesh, float *massFlux, I nMassFlux, float *su, I nSu, float *uBoundary,
+                                    I nUBoundary, float *vBoundary, I nVBoundary, float *wBoundary, I nWBoundary,
+                                    float fact, bool solveU, bool solveV, bool solveW, float *flowFact,
+                                    I nFlowFact, float *flowout2) {
+    cupcfd_gpu_mesh *m = nullptr;
+    int rc = attach(mesh, &m);
+    if (rc != CUPCFD_E_SUCCESS) return (ecode_t) rc;
+    return (ecode_t) cupcfd_gpu_flux_mass_dolfyn_boundary_loop5_f32(
+        m, massFlux, (int32_t) nMassFlux, su, (int32_t) nSu, uBoundary, (int32_t) nUBoundary, vBoundary,
+        (int32_t) nVBoundary, wBoundary, (int32_t) nWBoundary, fact, solveU, solveV, solveW, flowFact,
+        (int32_t) nFlowFact, flowout2);
+}
+
+template <class Mesh, class I>
+ecode_t FluxMassDolfynRegionLoop(Mesh &mesh, float *flowFact, I nFlowFact, float *flowRegion, I nFlowRegion,
+                                 float flowIn) {
+    cupcfd_gpu_mesh *m = nullptr;
+    int rc = attach(mesh, &m);
+    if (rc != CUPCFD_E_SUCCESS) return (ecode_t) rc;
+    return (ecode_t) cupcfd_gpu_flux_mass_dolfyn_region_loop_f32(m, flowFact, (int32_t) nFlowFact, flowRegion,
+                                                                (int32_t) nFlowRegion, flowIn);
 }
 
 // FluxUVWDolfynFaceLoop1 (UVWKernels.h:45-67), T = double. rlencos and the

@@ -702,6 +702,33 @@ def ref_uvw_loops_f32(m, f, rlencos=None, bnd_dist=None):
     return out
 
 
+def ref_boundary_chain_f32(m, splvl, d, fact, solve, flowout2):
+    """The boundary-loop chain (loops 1, 3, 4, 2, the region loop, 5) of the
+    reference's own T = float instantiation (compiled unchanged) on mesh
+    ``m``'s float arrays: d holds mf [nFaces], su [nCells], u, v, w, den
+    [nBnd], fr [nRegions] (rounded to float). Returns the arrays after
+    loop 4 (mf4, u4, v4, w4), loop 2 (fr2), the region loop (ff) and loop 5
+    (mf5, su5, u5, v5, w5), and the scalars flowin, ratearea, flowout4,
+    flowout2 (loop 2's) and fo2 (loop 5's, continued from ``flowout2``)."""
+    ref = load_ref()
+    assert ref is not None, "reference build absent"
+    _, keep = _float_mesh(m)
+    a = {k: _f32(d[k]).copy() for k in ("mf", "su", "u", "v", "w", "den", "fr")}
+    nR = int(m["nRegions"])
+    ff = np.full(nR, np.nan, np.float32)
+    out = np.zeros(5, np.float32)
+    sp = _f32(splvl)
+    fn = ref.ref_boundary_chain_f32
+    fn.argtypes = [C.c_int] * 4 + [C.c_void_p] * 15 + [C.c_float] + [C.c_int] * 3 + [C.c_float, C.c_void_p]
+    rc = fn(int(m["nCells"]), int(m["nFaces"]), int(m["nBnd"]), nR, _p(keep["faceCell1"]), _p(keep["faceBnd"]),
+            _p(keep["faceNorm"]), _p(keep["faceArea"]), _p(keep["bndRegion"]), _p(keep["regionType"]), _p(sp),
+            _p(a["mf"]), _p(a["su"]), _p(a["u"]), _p(a["v"]), _p(a["w"]), _p(a["den"]), _p(a["fr"]), _p(ff),
+            float(np.float32(fact)), *[int(bool(x)) for x in solve], float(np.float32(flowout2)), _p(out))
+    assert rc == E_SUCCESS, rc
+    return dict(mf5=a["mf"], su5=a["su"], u5=a["u"], v5=a["v"], w5=a["w"], fr2=a["fr"], ff=ff,
+                flowin=out[0], ratearea=out[1], flowout4=out[2], flowout2=out[3], fo2=out[4])
+
+
 def uvw_region_loop1(m):
     ft = np.full((m["nRegions"], 3), np.nan)
     assert load().orc_uvw_region_loop1(C.byref(_cmesh(m)), _p(ft)) == E_SUCCESS

@@ -438,6 +438,52 @@ extern "C" int ref_boundary_chain(void * p, double * massFlux, double * su, doub
 	return st == 0 ? (int) cupcfd::error::E_SUCCESS : (int) cupcfd::error::E_ERROR;
 }
 
+/* The boundary-loop chain (loops 1, 3, 4, 2, the region loop, 5) of the
+ * reference's T=float instantiation on a float mesh given by its arrays,
+ * once, arrays updated in place; out[5] = flowin, ratearea, flowout (loop 4),
+ * flowout (loop 2), flowout2 (from flowout2In). */
+extern "C" int ref_boundary_chain_f32(int nCells, int nFaces, int nBnd, int nRegions, const int * faceCell1,
+                                      const int * faceBnd, const float * faceNorm, const float * faceArea,
+                                      const int * bndRegion, const int * regionType, const float * splvl,
+                                      float * massFlux, float * su, float * uB, float * vB, float * wB,
+                                      const float * denB, float * flowRegion, float * flowFact, float fact,
+                                      int solveU, int solveV, int solveW, float flowout2In, float * out) {
+	RefMeshF mesh;
+	mesh.properties.lOCells = nCells;
+	mesh.properties.lGhCells = 0;
+	mesh.properties.lTCells = nCells;
+	mesh.properties.lFaces = nFaces;
+	mesh.properties.lBoundaries = nBnd;
+	mesh.properties.lRegions = nRegions;
+	mesh.a = {};
+	mesh.a.faceCell1 = faceCell1;
+	mesh.a.faceBoundary = faceBnd;
+	mesh.a.faceNorm = faceNorm;
+	mesh.a.faceArea = faceArea;
+	mesh.a.boundaryRegion = bndRegion;
+	mesh.a.regionType = regionType;
+	mesh.a.regionSplvl = splvl;
+	std::vector<int> bface(nBnd > 0 ? nBnd : 1, -1);
+	for (int f = 0; f < nFaces; f++)
+		if (faceBnd[f] > -1) bface[faceBnd[f]] = f;
+	mesh.a.boundaryFace = bface.data();
+	float flowin = 0.0f, ratearea = 0.0f, flowout4 = 0.0f, flowout = 0.0f, flowout2 = flowout2In;
+	std::vector<float> den(denB, denB + nBnd);
+	int st = 0;
+	const int ok = (int) cupcfd::error::E_SUCCESS;
+	st |= (int) cupcfd::fvm::FluxMassDolfynBoundaryLoop1(mesh, massFlux, nFaces, &flowin) - ok;
+	st |= (int) cupcfd::fvm::FluxMassDolfynBoundaryLoop3(mesh, flowin, &ratearea) - ok;
+	st |= (int) cupcfd::fvm::FluxMassDolfynBoundaryLoop4(mesh, massFlux, nFaces, uB, nBnd, vB, nBnd, wB, nBnd,
+	                                                       den.data(), nBnd, ratearea, &flowout4) - ok;
+	st |= (int) cupcfd::fvm::FluxMassDolfynBoundaryLoop2(mesh, massFlux, nFaces, flowRegion, nRegions, &flowout) - ok;
+	st |= (int) cupcfd::fvm::FluxMassDolfynRegionLoop(mesh, flowFact, nRegions, flowRegion, nRegions, flowin) - ok;
+	st |= (int) cupcfd::fvm::FluxMassDolfynBoundaryLoop5(mesh, massFlux, nFaces, su, nCells, uB, nBnd, vB, nBnd, wB,
+	                                                       nBnd, fact, solveU != 0, solveV != 0, solveW != 0,
+	                                                       flowFact, nRegions, &flowout2) - ok;
+	out[0] = flowin; out[1] = ratearea; out[2] = flowout4; out[3] = flowout; out[4] = flowout2;
+	return st == 0 ? ok : (int) cupcfd::error::E_ERROR;
+}
+
 /* ---- momentum loops (UVWKernels.ipp:38-544), called unchanged ---- */
 extern "C" void ref_ctx_set_uvw_geometry(void * p, const double * rlencos, const double * bdist) {
 	RefCtx * c = (RefCtx *) p;

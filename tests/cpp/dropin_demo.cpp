@@ -44,6 +44,63 @@ static bool same(const std::vector<euc::EuclideanVector<double, 3>> &a, const st
     return true;
 }
 
+// FluxMassDolfynBoundaryLoop1, 3, 4, 2, RegionLoop, 5 in a solver step's
+// order through the reference's templates and through the drop-in, on the
+// same mesh (real type T) and inputs: nullptr when every scalar and array is
+// bit-identical, else what differs.
+template <class T>
+static bool same_bits(const std::vector<T> &a, const std::vector<T> &b) {
+    return a.size() == b.size() && std::memcmp(a.data(), b.data(), sizeof(T) * a.size()) == 0;
+}
+template <class T>
+static bool same_bits(T a, T b) { return std::memcmp(&a, &b, sizeof(T)) == 0; }
+
+template <class T, class M, class R>
+static const char *boundary_chain(M &mesh, int nC, int nF, int nB, int nR, R &rng) {
+    namespace ref = cupcfd::fvm;
+    namespace g = cupcfd::fvm::gpu;
+    std::uniform_real_distribution<double> U(-1.0, 1.0);
+    std::vector<T> mf0(nF);
+    for (auto &x : mf0) x = (T) (U(rng) * 1e-2);
+    T fin[2], rate[2], fo4[2], fo2[2], fo5[2] = {(T) 0.125, (T) 0.125};
+    std::vector<T> mf[2] = {mf0, mf0}, ub[2], vb[2], wb[2], fr[2], ff[2], s5[2];
+    std::vector<T> denb(nB);
+    for (auto &x : denb) x = (T) (1.0 + 0.1 * U(rng));
+    for (int r = 0; r < 2; r++) {
+        ub[r].assign(nB, (T) 0.01); vb[r].assign(nB, (T) 0.02); wb[r].assign(nB, (T) 0.03);
+        fr[r].assign(nR, (T) 0.001); ff[r].assign(nR, (T) -1.0); s5[r].assign(nC, (T) 0.5);
+    }
+    cupcfd::error::eCodes st[2][6];
+    st[0][0] = ref::FluxMassDolfynBoundaryLoop1(mesh, mf[0].data(), nF, &fin[0]);
+    st[1][0] = g::FluxMassDolfynBoundaryLoop1(mesh, mf[1].data(), nF, &fin[1]);
+    st[0][1] = ref::FluxMassDolfynBoundaryLoop3(mesh, fin[0], &rate[0]);
+    st[1][1] = g::FluxMassDolfynBoundaryLoop3(mesh, fin[1], &rate[1]);
+    st[0][2] = ref::FluxMassDolfynBoundaryLoop4(mesh, mf[0].data(), nF, ub[0].data(), nB, vb[0].data(), nB,
+                                                wb[0].data(), nB, denb.data(), nB, rate[0], &fo4[0]);
+    st[1][2] = g::FluxMassDolfynBoundaryLoop4(mesh, mf[1].data(), nF, ub[1].data(), nB, vb[1].data(), nB,
+                                              wb[1].data(), nB, denb.data(), nB, rate[1], &fo4[1]);
+    st[0][3] = ref::FluxMassDolfynBoundaryLoop2(mesh, mf[0].data(), nF, fr[0].data(), nR, &fo2[0]);
+    st[1][3] = g::FluxMassDolfynBoundaryLoop2(mesh, mf[1].data(), nF, fr[1].data(), nR, &fo2[1]);
+    st[0][4] = ref::FluxMassDolfynRegionLoop(mesh, ff[0].data(), nR, fr[0].data(), nR, fin[0]);
+    st[1][4] = g::FluxMassDolfynRegionLoop(mesh, ff[1].data(), nR, fr[1].data(), nR, fin[1]);
+    st[0][5] = ref::FluxMassDolfynBoundaryLoop5(mesh, mf[0].data(), nF, s5[0].data(), nC, ub[0].data(), nB,
+                                                vb[0].data(), nB, wb[0].data(), nB, (T) 1.25, true, false, true,
+                                                ff[0].data(), nR, &fo5[0]);
+    st[1][5] = g::FluxMassDolfynBoundaryLoop5(mesh, mf[1].data(), nF, s5[1].data(), nC, ub[1].data(), nB,
+                                              vb[1].data(), nB, wb[1].data(), nB, (T) 1.25, true, false, true,
+                                              ff[1].data(), nR, &fo5[1]);
+    for (int k = 0; k < 6; k++)
+        if (st[0][k] != cupcfd::error::E_SUCCESS || st[1][k] != cupcfd::error::E_SUCCESS)
+            return "boundary loop status";
+    if (!(same_bits(fin[0], fin[1]) && same_bits(rate[0], rate[1]) && same_bits(fo4[0], fo4[1]) &&
+          same_bits(fo2[0], fo2[1]) && same_bits(fo5[0], fo5[1])))
+        return "boundary loop scalars differ from the reference";
+    if (!(same_bits(mf[0], mf[1]) && same_bits(ub[0], ub[1]) && same_bits(vb[0], vb[1]) && same_bits(wb[0], wb[1]) &&
+          same_bits(fr[0], fr[1]) && same_bits(ff[0], ff[1]) && same_bits(s5[0], s5[1])))
+        return "boundary loop arrays differ from the reference";
+    return nullptr;
+}
+
 int main(int argc, char **argv) {
     int n = argc > 1 ? std::atoi(argv[1]) : 12;
     int nx = n, ny = n - 1, nz = n + 2;
@@ -161,47 +218,7 @@ int main(int argc, char **argv) {
         if (o[0].c[k] != o[1].c[k]) return fail("region counters differ");
 
     // ---- FluxMassDolfynBoundaryLoop1-5 and FluxMassDolfynRegionLoop (outlet region 1, inlet region 0)
-    {
-        namespace ref = cupcfd::fvm;
-        namespace g = cupcfd::fvm::gpu;
-        std::vector<double> mf0(nF);
-        for (auto &x : mf0) x = U(rng) * 1e-2;
-        double fin[2], rate[2], fo4[2], fo2[2], fo5[2] = {0.125, 0.125};
-        std::vector<double> mf[2] = {mf0, mf0}, ub[2], vb[2], wb[2], fr[2], ff[2], s5[2];
-        std::vector<double> denb(nB);
-        for (auto &x : denb) x = 1.0 + 0.1 * U(rng);
-        for (int r = 0; r < 2; r++) {
-            ub[r].assign(nB, 0.01); vb[r].assign(nB, 0.02); wb[r].assign(nB, 0.03);
-            fr[r].assign(nR, 0.001); ff[r].assign(nR, -1.0); s5[r].assign(nC, 0.5);
-        }
-        cupcfd::error::eCodes st[2][6];
-        st[0][0] = ref::FluxMassDolfynBoundaryLoop1(mesh, mf[0].data(), nF, &fin[0]);
-        st[1][0] = g::FluxMassDolfynBoundaryLoop1(mesh, mf[1].data(), nF, &fin[1]);
-        st[0][1] = ref::FluxMassDolfynBoundaryLoop3(mesh, fin[0], &rate[0]);
-        st[1][1] = g::FluxMassDolfynBoundaryLoop3(mesh, fin[1], &rate[1]);
-        st[0][2] = ref::FluxMassDolfynBoundaryLoop4(mesh, mf[0].data(), nF, ub[0].data(), nB, vb[0].data(), nB,
-                                                    wb[0].data(), nB, denb.data(), nB, rate[0], &fo4[0]);
-        st[1][2] = g::FluxMassDolfynBoundaryLoop4(mesh, mf[1].data(), nF, ub[1].data(), nB, vb[1].data(), nB,
-                                                  wb[1].data(), nB, denb.data(), nB, rate[1], &fo4[1]);
-        st[0][3] = ref::FluxMassDolfynBoundaryLoop2(mesh, mf[0].data(), nF, fr[0].data(), nR, &fo2[0]);
-        st[1][3] = g::FluxMassDolfynBoundaryLoop2(mesh, mf[1].data(), nF, fr[1].data(), nR, &fo2[1]);
-        st[0][4] = ref::FluxMassDolfynRegionLoop(mesh, ff[0].data(), nR, fr[0].data(), nR, fin[0]);
-        st[1][4] = g::FluxMassDolfynRegionLoop(mesh, ff[1].data(), nR, fr[1].data(), nR, fin[1]);
-        st[0][5] = ref::FluxMassDolfynBoundaryLoop5(mesh, mf[0].data(), nF, s5[0].data(), nC, ub[0].data(), nB,
-                                                    vb[0].data(), nB, wb[0].data(), nB, 1.25, true, false, true,
-                                                    ff[0].data(), nR, &fo5[0]);
-        st[1][5] = g::FluxMassDolfynBoundaryLoop5(mesh, mf[1].data(), nF, s5[1].data(), nC, ub[1].data(), nB,
-                                                  vb[1].data(), nB, wb[1].data(), nB, 1.25, true, false, true,
-                                                  ff[1].data(), nR, &fo5[1]);
-        for (int k = 0; k < 6; k++)
-            if (st[0][k] != cupcfd::error::E_SUCCESS || st[1][k] != cupcfd::error::E_SUCCESS)
-                return fail("boundary loop status");
-        if (!(fin[0] == fin[1] && rate[0] == rate[1] && fo4[0] == fo4[1] && fo2[0] == fo2[1] && fo5[0] == fo5[1]))
-            return fail("boundary loop scalars differ from the reference");
-        if (mf[0] != mf[1] || ub[0] != ub[1] || vb[0] != vb[1] || wb[0] != wb[1] || fr[0] != fr[1] || ff[0] != ff[1] ||
-            s5[0] != s5[1])
-            return fail("boundary loop arrays differ from the reference");
-    }
+    if (const char *e = boundary_chain<double>(mesh, nC, nF, nB, nR, rng)) return fail(e);
     // ---- FluxUVWDolfynFaceLoop1, RegionLoop1, BndsLoop1 (boundary 0, on face 0, is an inlet)
     {
         namespace ref = cupcfd::fvm;
@@ -280,8 +297,11 @@ int main(int argc, char **argv) {
                 if (std::memcmp(&g1[i].cmp[d], &g2[i].cmp[d], 4) != 0 || std::memcmp(&go1[i].cmp[d], &go2[i].cmp[d], 4) != 0)
                     return fail("float gradient differs from the reference's float instantiation");
     }
+    // ---- the boundary / region loops on the float mesh
+    if (const char *e = boundary_chain<float>(meshF, nC, nF, nB, nR, rng)) return fail(e);
     cupcfd::fvm::gpu::release(meshF);
     std::printf("OK dropin %dx%dx%d: %d cells, %d faces; gradient (nGradient 1-3, double and float meshes), mass "
-                "flux, the boundary / region loops and the momentum loops bit-identical\n", nx, ny, nz, nC, nF);
+                "flux, the boundary / region loops (double and float meshes) and the momentum loops "
+                "bit-identical\n", nx, ny, nz, nC, nF);
     return 0;
 }

@@ -47,12 +47,14 @@ def _oracle_chain(m, splvl, d, solve):
                 flowout2=flowout2, ff=ff, mf5=mf5, su5=su5, u5=u5, v5=v5, w5=w5, fo2=fo2)
 
 
-def _host_chain(cg, mesh, d, solve):
+def _host_chain(cg, mesh, d, solve, f32=False):
+    """The chain through the host-buffer calls; f32: float32 arrays (the
+    reference's T = float instantiation)."""
     r = {}
     E = cg.E_SUCCESS
     rc, r["flowin"] = cg.FluxMassDolfynBoundaryLoop1(mesh, d["mf"].copy())
     assert rc == E
-    rc, r["ratearea"] = cg.FluxMassDolfynBoundaryLoop3(mesh, r["flowin"])
+    rc, r["ratearea"] = cg.FluxMassDolfynBoundaryLoop3(mesh, r["flowin"], f32=f32)
     assert rc == E
     mf, u, v, w = d["mf"].copy(), d["u"].copy(), d["v"].copy(), d["w"].copy()
     rc, r["flowout4"] = cg.FluxMassDolfynBoundaryLoop4(mesh, mf, u, v, w, d["den"].copy(), r["ratearea"])
@@ -62,7 +64,7 @@ def _host_chain(cg, mesh, d, solve):
     rc, r["flowout2"] = cg.FluxMassDolfynBoundaryLoop2(mesh, mf, fr)
     assert rc == E
     r["fr2"] = fr
-    ff = np.full(len(fr), np.nan)
+    ff = np.full(len(fr), np.nan, fr.dtype)
     assert cg.FluxMassDolfynRegionLoop(mesh, ff, fr, r["flowin"]) == E
     r["ff"] = ff
     su = d["su"].copy()
@@ -163,6 +165,37 @@ def test_device_loops_equal_host_loops(cg, gpu, kind, order):
     assert np.array_equal(to_ref(mf, f2o), host["mf5"]) and np.array_equal(to_ref(su, c2o), host["su5"])
     for k, t in (("u5", u), ("v5", v), ("w5", w)):
         assert np.array_equal(H(t), host[k]), k
+
+
+@pytest.mark.parametrize("kind,order", [("struct", 2), ("jitter", 3), ("large", 0)])
+def test_float_instantiation_bit_exact(cg, gpu, kind, order):
+    """The _f32 calls (float32 host arrays) on a mesh made from float arrays
+    against the reference's own T = float instantiation (compiled
+    unchanged) on the same float arrays: the whole chain, every array and
+    scalar bit for bit."""
+    if O.load_ref() is None:
+        pytest.skip("reference build absent")
+    m, splvl, _, d = _setup(cg, kind, order)
+    m32 = dict(m)
+    for k in ("faceLambda", "faceArea", "faceNorm", "faceCenter", "faceXpac", "faceXnac", "cellCenter", "cellVolume",
+              "regionUVW", "regionDen"):
+        if m.get(k) is not None:
+            m32[k] = np.ascontiguousarray(np.asarray(m[k]), np.float32)
+    sp32 = splvl.astype(np.float32)
+    mesh = cg.Mesh.from_arrays(m32, order=order)
+    assert mesh.set_regions(m["regionType"], m32["regionUVW"].astype(np.float64),
+                            m32["regionDen"].astype(np.float64), m["bndRegion"]) == cg.E_SUCCESS
+    assert mesh.set_region_split(sp32.astype(np.float64)) == cg.E_SUCCESS
+    d32 = {k: np.ascontiguousarray(v, np.float32) for k, v in d.items()}
+    solve = (1, 0, 1)
+    want = O.ref_boundary_chain_f32(m32, sp32, d32, 1.3, solve, 0.25)
+    got = _host_chain(cg, mesh, d32, solve, f32=True)
+    for k in ("flowin", "ratearea", "flowout4", "flowout2", "fo2"):
+        assert np.float32(got[k]).view(np.int32) == np.float32(want[k]).view(np.int32), (k, got[k], want[k])
+    for k in ("mf5", "su5", "u5", "v5", "w5", "fr2", "ff"):
+        assert got[k].dtype == np.float32
+        assert np.array_equal(got[k].view(np.int32), want[k].view(np.int32)), k
+    assert want["flowin"] != 0 and want["fo2"] != 0.25
 
 
 def test_boundary_loop_errors(cg, gpu):
