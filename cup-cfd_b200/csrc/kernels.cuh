@@ -28,20 +28,49 @@ namespace cupcfd_gpu {
 
 
 // ---------------------------------------------------------------------------
-// Dot2 compensated accumulation (Ogita, Rump & Oishi, "Accurate sum and dot
-// product", SIAM J. Sci. Comput. 26(6), 2005): each product is split into
-// its rounded value and exact error (TwoProduct via FMA), the sum is kept
-// with Knuth's TwoSum error term, and the errors are accumulated separately.
-// The result is as accurate as if computed in twice the working precision.
+// Compensated accumulation of products, after Dot2 (Ogita, Rump & Oishi,
+// "Accurate sum and dot product", SIAM J. Sci. Comput. 26(6), 2005): the sum
+// s is advanced by p = fl(a b) with Knuth's TwoSum, and the error of the
+// product and of the addition are accumulated separately in e. CUPCFD_COMP:
+//   3 (default): TwoSum computes nbp = s - t (t = s + p), av = t + nbp and
+//     the exact ar = s - av; the product's error a b - p and TwoSum's exact
+//     low part p - (t - s) are taken together as one FMA, fma(a, b, nbp)
+//     = a b - (t - s), rounded once. That rounding is of the order u^2 |t|,
+//     the order of Dot2's own error accumulation, so the result keeps
+//     Dot2's bound (as if computed in twice the working precision) in 8
+//     operations instead of Dot2's 10 (packed: 8 instead of 11).
+//   2: Dot2 as published (TwoProduct by FMA, TwoSum, errors summed).
+//   1: TwoSum without the product's error.
+//   0: Kahan's compensated sum (Fast2Sum on p + e).
 // ---------------------------------------------------------------------------
 #ifndef CUPCFD_COMP
-#define CUPCFD_COMP 2
+#define CUPCFD_COMP 3
 #endif
+//
+// Every form starts from the rounded product p = fl(a b), written as
+// fma(a, b, +0): the same value (a b + 0 rounds once; a zero product comes
+// out +0, which no sum below tells apart from -0). The packed form needs it:
+// with a plain packed multiply feeding a packed add, the add came out as one
+// fused fma(a, b, s) on B200 with CUDA 12.9 (measured: the packed lanes then
+// equal, bit for bit, an emulation of that fusion, and differ from the scalar
+// form on 62% of random six-term sums), even when both were written as
+// mul.rn.f32x2 / add.rn.f32x2 in inline PTX. That takes the product's
+// rounding out of TwoSum's input and loses the error term where the sum
+// cancels (checked in exact arithmetic: up to one ulp of the terms). The
+// result of an FMA is not contracted again, and the scalar form uses the
+// same expression so that a packed lane and Acc2 give the same bits.
 struct Acc2 {
     float s = 0.f, e = 0.f;
     __device__ __forceinline__ void add_prod(float a, float b) {
-        float p = __fmul_rn(a, b);
-#if CUPCFD_COMP == 2
+        float p = __fmaf_rn(a, b, 0.f);
+#if CUPCFD_COMP == 3
+        float t = __fadd_rn(s, p);
+        float nbp = __fsub_rn(s, t);
+        float ar = __fsub_rn(s, __fadd_rn(t, nbp));
+        float brp = __fmaf_rn(a, b, nbp);
+        s = t;
+        e = __fadd_rn(e, __fadd_rn(ar, brp));
+#elif CUPCFD_COMP == 2
         float ep = __fmaf_rn(a, b, -p);
         float t = __fadd_rn(s, p);
         float bp = __fsub_rn(t, s);
@@ -74,8 +103,15 @@ struct Acc2x2 {
     float2 s = {0.f, 0.f}, e = {0.f, 0.f};
     __device__ __forceinline__ void add_prod(float2 a, float2 b) {
         const float2 m1 = make_float2(-1.f, -1.f);
-        float2 p = __fmul2_rn(a, b);
-#if CUPCFD_COMP == 2
+        float2 p = __ffma2_rn(a, b, make_float2(0.f, 0.f));
+#if CUPCFD_COMP == 3
+        float2 t = __fadd2_rn(s, p);
+        float2 nbp = __ffma2_rn(t, m1, s);
+        float2 ar = __ffma2_rn(__fadd2_rn(t, nbp), m1, s);
+        float2 brp = __ffma2_rn(a, b, nbp);
+        s = t;
+        e = __fadd2_rn(e, __fadd2_rn(ar, brp));
+#elif CUPCFD_COMP == 2
         float2 ep = __ffma2_rn(a, b, __fmul2_rn(p, m1));
         float2 t = __fadd2_rn(s, p);
         float2 bp = __ffma2_rn(s, m1, t);
@@ -262,7 +298,7 @@ __global__ void __launch_bounds__(256, CUPCFD_MINB_F64) k_grad_f64(int nC, SellV
 }
 
 // ---------------------------------------------------------------------------
-// Gradient, FP32 storage and arithmetic, Dot2 accumulation, FP64 1/V.
+// Gradient, FP32 storage and arithmetic, compensated accumulation (Acc2), FP64 1/V.
 // ---------------------------------------------------------------------------
 template <bool CORR, bool SIGNED>
 __global__ void __launch_bounds__(256, CUPCFD_MINB_F32) k_grad_f32(int nC, SellView sv, const float4 *__restrict__ fg,

@@ -159,7 +159,7 @@ __device__ __forceinline__ double fwd_cell_f32(int c, const SellView &sv, const 
 // forward of fwd_cell_f32 plus, over every interior face, the rhobar / ubar
 // accumulation of adj_cell_f32, with the same arithmetic in the same face
 // order, so stbar equals the one the full adjoint writes bit for bit.
-template <int CH>
+template <int CH, int PIPE = 0>
 __device__ __forceinline__ double fwd_madj_cell_f32(int c, const SellView &sv, const float4 *__restrict__ fg,
                                                     const float *__restrict__ phi, const float *__restrict__ phiB,
                                                     const double *__restrict__ vol, const float4 *__restrict__ st,
@@ -170,13 +170,13 @@ __device__ __forceinline__ double fwd_madj_cell_f32(int c, const SellView &sv, c
     const int2 *e = cell_entries(sv, c, w);
     float phic = phi[c];
     float4 sc = st[c];
-    // seven Dot2 sums in packed pairs: (gx, gy), (gz, rhobar), (ubar, vbar), wbar
+    // seven compensated sums in packed pairs: (gx, gy), (gz, rhobar), (ubar, vbar), wbar
     Acc2x2 axy, azr, uvb;
     Acc2 wb;
     double lsum = 0.0;
+    int2 en[CH];
+    load_entries(e, 0, w, en);
     for (int k0 = 0; k0 < w; k0 += CH) {
-        int2 en[CH];
-        load_entries(e, k0, w, en);
         float4 G[CH], so[CH];
         float pv[CH], gf[CH];
 #pragma unroll
@@ -191,6 +191,8 @@ __device__ __forceinline__ double fwd_madj_cell_f32(int c, const SellView &sv, c
                 gf[j] = __ldg(gface + f);
             }
         }
+        int2 nx[CH];
+        if (PIPE) load_entries(e, k0 + CH, w, nx);
 #pragma unroll
         for (int j = 0; j < CH; j++) {
             int code = en[j].x;
@@ -222,6 +224,7 @@ __device__ __forceinline__ double fwd_madj_cell_f32(int c, const SellView &sv, c
                 wb.add_prod(b, G[j].z);
             }
         }
+        next_entries<PIPE>(e, k0 + CH, w, en, nx);
     }
     double V = vol[c];
     double fact = 1.0 / V;
@@ -399,7 +402,7 @@ __device__ __forceinline__ void adj_cell_f64(int c, const SellView &sv, const do
     if (doM) { stbar[c] = rb; stbar[ldc + c] = ub; stbar[2 * ldc + c] = vb; stbar[3 * ldc + c] = wb; }
 }
 
-template <bool LDCG, int CH = CUPCFD_ADJ_CHUNK>
+template <bool LDCG, int CH = CUPCFD_ADJ_CHUNK, int PIPE = 0>
 __device__ __forceinline__ void adj_cell_f32(int c, const SellView &sv, const float4 *__restrict__ fg, const float *g,
                                              float hscale, const float4 *__restrict__ st,
                                              const float *__restrict__ gface, float *__restrict__ phibar,
@@ -413,9 +416,9 @@ __device__ __forceinline__ void adj_cell_f32(int c, const SellView &sv, const fl
     if (doM) sc = st[c];
     Acc2 pb, rb, wb;
     Acc2x2 uvb;  // (ubar, vbar) packed
+    int2 en[CH];
+    load_entries(e, 0, w, en);
     for (int k0 = 0; k0 < w; k0 += CH) {
-        int2 en[CH];
-        load_entries(e, k0, w, en);
         float4 G[CH], so[CH];
         float go[CH][3], gf[CH];
 #pragma unroll
@@ -428,6 +431,8 @@ __device__ __forceinline__ void adj_cell_f32(int c, const SellView &sv, const fl
             if (doG) { go[j][0] = ldg_g<LDCG>(g + o); go[j][1] = ldg_g<LDCG>(g + ldc + o); go[j][2] = ldg_g<LDCG>(g + 2 * ldc + o); }
             if (doM) { so[j] = __ldg(st + o); gf[j] = __ldg(gface + f); }
         }
+        int2 nx[CH];
+        if (PIPE) load_entries(e, k0 + CH, w, nx);
 #pragma unroll
         for (int j = 0; j < CH; j++) {
             int code = en[j].x;
@@ -451,6 +456,7 @@ __device__ __forceinline__ void adj_cell_f32(int c, const SellView &sv, const fl
                 wb.add_prod(b, G[j].z);
             }
         }
+        next_entries<PIPE>(e, k0 + CH, w, en, nx);
     }
     if (doG) phibar[c] = (float) pb.value();
     if (doM) stbar[c] = make_float4((float) rb.value(), (float) uvb.x(), (float) uvb.y(), (float) wb.value());

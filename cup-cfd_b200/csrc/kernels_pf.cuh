@@ -123,8 +123,16 @@ __global__ void __launch_bounds__(TILE_CELLS, CUPCFD_MINB_FWD_MADJ)
 }
 
 // Gradient part of the adjoint only (adj_cell_f32 without the mass part):
-// phibar and phibBar.
-__global__ void __launch_bounds__(TILE_CELLS, CUPCFD_MINB_F32)
+// phibar and phibBar. The next chunk's entries load during the current
+// chunk's arithmetic (CUPCFD_GADJ_PIPE) within the 40 registers that six
+// resident blocks per SM leave (CUPCFD_MINB_GADJ): chosen by measurement.
+#ifndef CUPCFD_GADJ_PIPE
+#define CUPCFD_GADJ_PIPE 1
+#endif
+#ifndef CUPCFD_MINB_GADJ
+#define CUPCFD_MINB_GADJ 6
+#endif
+__global__ void __launch_bounds__(TILE_CELLS, CUPCFD_MINB_GADJ)
     k_gadj_f32_pf(int nC, SellView sv, const float4 *__restrict__ fg, const float *__restrict__ g, float hscale,
                   float *__restrict__ phibar, float *__restrict__ phibBar, int64_t ldc, PrefetchArgs pf) {
     constexpr int T = TILE_CELLS;
@@ -135,7 +143,9 @@ __global__ void __launch_bounds__(TILE_CELLS, CUPCFD_MINB_F32)
     const void *const cellSrc[3] = {g, g + ldc, g + 2 * ldc};
     const int cellBytes[3] = {T * 4, T * 4, T * 4};
     if (lead) fetch_ranges_async(&s_rng, pf.desc + tp);
-    if (c < nC) adj_cell_f32<false>(c, sv, fg, g, hscale, nullptr, nullptr, phibar, phibBar, nullptr, ldc);
+    if (c < nC)
+        adj_cell_f32<false, CUPCFD_ADJ_CHUNK, CUPCFD_GADJ_PIPE>(c, sv, fg, g, hscale, nullptr, nullptr, phibar,
+                                                                phibBar, nullptr, ldc);
     if (lead) prefetch_tile<3>(pf, tp, ranges_ready(&s_rng), fg, 16, (const float *) nullptr, cellSrc, cellBytes);
 }
 

@@ -47,4 +47,17 @@ __device__ __forceinline__ void load_entries(const int2 *e, int k0, int w, int2 
     for (int j = 0; j < W; j++) en[j] = (k0 + j < w) ? ld_entry(e + 32 * (k0 + j)) : make_int2(-1, -1);
 }
 
+// The entries of the cell's next chunk into en: with PIPE they were loaded
+// into nx before the current chunk's arithmetic (so their latency overlaps
+// it; two more registers per entry), else they are loaded now.
+template <int PIPE, int W>
+__device__ __forceinline__ void next_entries(const int2 *e, int k0, int w, int2 (&en)[W], const int2 (&nx)[W]) {
+    if (PIPE) {
+#pragma unroll
+        for (int j = 0; j < W; j++) en[j] = nx[j];
+    } else {
+        load_entries(e, k0, w, en);
+    }
+}
+
 }  // namespace cupcfd_gpu

@@ -60,7 +60,7 @@ extern "C" {
 
 /* ---- arithmetic of a call ---- */
 #define CUPCFD_PREC_F64 0  /* plain FP64; same operand order as the reference, bit-identical results */
-#define CUPCFD_PREC_F32C 1 /* FP32 storage and arithmetic, compensated (Dot2) cell accumulation,
+#define CUPCFD_PREC_F32C 1 /* FP32 storage and arithmetic, compensated (TwoSum) cell accumulation,
                               FP64 volumes and final scaling */
 #define CUPCFD_PREC_F32REF 2 /* gradient calls only: the arithmetic of the reference's T=float
                                 instantiation (float sums in its order), bit-identical to it on a

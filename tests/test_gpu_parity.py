@@ -4,8 +4,9 @@ FP64 path: bit-identical to the oracle, which is itself bit-identical to the
 reference's own CPU kernels (tests/test_oracle_vs_reference.py). The stated
 contract is <= 1e-12 relative; the tests assert equality of every element.
 
-FP32-compensated path: FP32 fields and geometry, Dot2 accumulation, FP64
-volumes. Measured against the FP64 oracle fed the same FP32-rounded inputs.
+FP32-compensated path: FP32 fields and geometry, compensated (TwoSum, after
+Dot2) accumulation, FP64 volumes. Measured against the FP64 oracle fed the
+same FP32-rounded inputs.
 Tolerances:
   normwise   max|d| / max|ref|                      <= 1e-6
   rms        ||d||_2 / ||ref||_2                    <= 1e-6
@@ -13,7 +14,7 @@ Tolerances:
 Each face term carries one FP32 rounding (about 6e-8 of the term); a cell
 sum of six terms that cancels down to 1e-2 of the typical magnitude turns
 that into ~1e-5 relative, and the adjoint sums (two interpolations per term)
-reach a few 1e-5. The sums themselves are compensated (Dot2) and add nothing.
+reach a few 1e-5. The sums themselves are compensated and add nothing.
 """
 import numpy as np
 import pytest
