@@ -323,6 +323,45 @@ def bench_uvw(cg, mesh, dev, st, g, steps, warmup, peak):
             "config": "generated mesh, default region, rlencos 0 (the reference benchmark's case)"}
 
 
+def host_link(dev, mb=256, reps=5):
+    """Pinned host <-> device copy bandwidth of this box (GB/s): each
+    direction alone, and each direction while the other runs on a second
+    stream (the host call overlaps them). Bounds the e2e figure."""
+    import torch
+    n = mb * 2 ** 20 // 4
+    h_in = torch.ones(n, dtype=torch.float32, pin_memory=True)
+    h_out = torch.empty(n, dtype=torch.float32, pin_memory=True)
+    d_a = torch.empty(n, dtype=torch.float32, device=dev)
+    d_b = torch.ones(n, dtype=torch.float32, device=dev)
+    s1, s2 = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+
+    def run(h2d, d2h):
+        if h2d:
+            with torch.cuda.stream(s1):
+                d_a.copy_(h_in, non_blocking=True)
+        if d2h:
+            with torch.cuda.stream(s2):
+                h_out.copy_(d_b, non_blocking=True)
+        torch.cuda.current_stream().wait_stream(s1)
+        torch.cuda.current_stream().wait_stream(s2)
+
+    def ms(h2d, d2h):
+        run(h2d, d2h)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            run(h2d, d2h)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    gb = n * 4 / 1e9
+    both = ms(True, True)
+    return {"h2d_gbs": gb / ms(True, False) * 1e3, "d2h_gbs": gb / ms(False, True) * 1e3,
+            "each_way_concurrent_gbs": gb / both * 1e3, "bytes": n * 4, "unit": "GB/s"}
+
+
 def _time_calls(st, fn, steps, warmup):
     """Mean device time (ms) of fn() over `steps` calls on stream st, CUDA events."""
     import torch
@@ -717,6 +756,7 @@ def run_gpu(a):
                    "FP32 path's storage type, the reference's T = float arrays)")
     e2e_f64 = host_call(torch.float64, max(1, K2 // 2))
     e2e_f64["call"] = "cupcfd_gpu_forward_adjoint (pinned host FP64 arrays in the reference's numbering)"
+    link = host_link(dev)
 
     # ---- roofline of the dominant kernel, from the device timers of the timed region
     bm = bytes_model(nC, nF, nFi, nB)
@@ -795,6 +835,7 @@ def run_gpu(a):
             "error_vs_fp64": errors,
             "e2e": e2e,
             "e2e_fp64_host_arrays": e2e_f64,
+            "host_link": link,
             "cpu_baseline": cpu,
             "uvw_face_loop1": uvw,
             "next_rows": rows,
