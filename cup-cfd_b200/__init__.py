@@ -75,7 +75,7 @@ class MeshOptions(C.Structure):
 class MeshInfo(C.Structure):
     _fields_ = [(n, C.c_int32) for n in ("nCells", "nFaces", "nInteriorFaces", "nBoundaries", "nRegions",
                                          "nIncidences", "maxCellFaces", "order", "precisions", "bandwidth")] + [
-        ("deviceBytes", C.c_int64), ("tiles", C.c_int32), ("reserved", C.c_int32)]
+        ("deviceBytes", C.c_int64), ("tiles", C.c_int32), ("fullWidth", C.c_int32)]
 
 
 # exported symbols of include/cupcfd_gpu.h with their ctypes signatures
@@ -265,6 +265,7 @@ class Mesh:
         self.order, self.precisions, self.deviceBytes = info.order, info.precisions, info.deviceBytes
         self.bandwidth = info.bandwidth
         self.tiles = bool(info.tiles)
+        self.full_width = info.fullWidth
 
     @staticmethod
     def _opts(order, precisions, device):

@@ -37,6 +37,17 @@ int scratch(cupcfd_gpu_mesh *m, int slot, size_t n, T **p) {
 inline cudaStream_t as_stream(void *s) { return (cudaStream_t) s; }
 inline SellView sell(const cupcfd_gpu_mesh *m) { return SellView{m->sell.slicePtr, m->sell.inc, m->sell.width}; }
 
+// The width the L2-prefetch kernels are specialised for (kernels_pf.cuh:
+// WF), set by tiles_setup: 6 when every cell has exactly six incidences
+// (all hexahedral meshes), else 0 (the general kernels).
+inline int full_width(const cupcfd_gpu_mesh *m) { return m->fullWidth; }
+// launches the L2-prefetch kernel template K at the mesh's full width
+#define CG_LAUNCH_PF(m, K, grid, st, ...)                                      \
+    do {                                                                       \
+        if (full_width(m) == 6) K<6><<<(grid), BLK, 0, (st)>>>(__VA_ARGS__);   \
+        else K<0><<<(grid), BLK, 0, (st)>>>(__VA_ARGS__);                      \
+    } while (0)
+
 // ---------------------------------------------------------------------------
 // device timers (cupcfd_gpu_timing_*): a KTIMER scope records one event
 // before and one after the launch it encloses, on the launch's stream
@@ -110,8 +121,19 @@ int tiles_setup(cupcfd_gpu_mesh *m, cudaStream_t st) {
     // wave (the gradient adjoint holds more blocks per SM than the forward:
     // 0.345 ms at its 740-tile wave against 0.359 ms at the forward's 592 at
     // 256^3)
-    const void *pfKern[6] = {(const void *) k_fwd_f32_pf, (const void *) k_adj_f32_pf, (const void *) k_fwd_f64_pf,
-                             (const void *) k_adj_f64_pf, (const void *) k_fwd_madj_f32_pf, (const void *) k_gadj_f32_pf};
+    // CUPCFD_FULL_WIDTH=0 keeps the general kernels on hexahedral meshes
+    // (identical results), for comparisons
+    const char *fw = std::getenv("CUPCFD_FULL_WIDTH");
+    m->fullWidth = m->sell.width == 6 && (int64_t) m->nInc == 6 * (int64_t) m->nC &&
+                   !(fw && std::strcmp(fw, "0") == 0) ? 6 : 0;
+    const bool w6 = full_width(m) == 6;
+    const void *pfKern[6] = {
+        w6 ? (const void *) k_fwd_f32_pf<6> : (const void *) k_fwd_f32_pf<0>,
+        w6 ? (const void *) k_adj_f32_pf<6> : (const void *) k_adj_f32_pf<0>,
+        w6 ? (const void *) k_fwd_f64_pf<6> : (const void *) k_fwd_f64_pf<0>,
+        w6 ? (const void *) k_adj_f64_pf<6> : (const void *) k_adj_f64_pf<0>,
+        w6 ? (const void *) k_fwd_madj_f32_pf<6> : (const void *) k_fwd_madj_f32_pf<0>,
+        w6 ? (const void *) k_gadj_f32_pf<6> : (const void *) k_gadj_f32_pf<0>};
     for (int i = 0; i < 6; i++) {
         int nb = 0;
         CG_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pfKern[i], TILE_CELLS, 0));
@@ -364,10 +386,9 @@ namespace {
 const char *launch_fwd_f32(const cupcfd_gpu_mesh *m, const void *phi, const void *phiB, const void *state,
                            const void *gface, void *grad, void *massFlux, double *part, cudaStream_t st) {
     if (m->tiles && aligned16(phi) && aligned16(state) && (!gface || aligned16(gface))) {
-        k_fwd_f32_pf<<<grid_for(m->nC, BLK), BLK, 0, st>>>(m->nC, sell(m), m->fg32, (const float *) phi,
-                                                          (const float *) phiB, m->vol, (const float4 *) state,
-                                                          (const float *) gface, (float *) grad, (float *) massFlux,
-                                                          part, m->nC, prefetch_args(m, PF_FWD_F32));
+        CG_LAUNCH_PF(m, k_fwd_f32_pf, grid_for(m->nC, BLK), st, m->nC, sell(m), m->fg32, (const float *) phi,
+                     (const float *) phiB, m->vol, (const float4 *) state, (const float *) gface, (float *) grad,
+                     (float *) massFlux, part, m->nC, prefetch_args(m, PF_FWD_F32));
         return "k_fwd_f32_pf";
     }
     k_fwd_f32<BLK><<<grid_for(m->nC, BLK), BLK, 0, st>>>(m->nC, sell(m), m->fg32, (const float *) phi,
@@ -384,10 +405,9 @@ const char *launch_fwd_f64(const cupcfd_gpu_mesh *m, const void *phi, const void
                            const void *gface, void *grad, void *massFlux, double *part, cudaStream_t st) {
     if (m->tiles && aligned16(phi) && aligned16(state) && (!gface || aligned16(gface)) &&
         m->nC % 2 == 0) {
-        k_fwd_f64_pf<<<grid_for(m->nC, BLK), BLK, 0, st>>>(m->nC, sell(m), m->fg64, (const double *) phi,
-                                                          (const double *) phiB, m->vol, (const double *) state,
-                                                          (const double *) gface, (double *) grad, (double *) massFlux,
-                                                          part, m->nC, prefetch_args(m, PF_FWD_F64));
+        CG_LAUNCH_PF(m, k_fwd_f64_pf, grid_for(m->nC, BLK), st, m->nC, sell(m), m->fg64, (const double *) phi,
+                     (const double *) phiB, m->vol, (const double *) state, (const double *) gface, (double *) grad,
+                     (double *) massFlux, part, m->nC, prefetch_args(m, PF_FWD_F64));
         return "k_fwd_f64_pf";
     }
     k_fwd_f64<BLK><<<grid_for(m->nC, BLK), BLK, 0, st>>>(m->nC, sell(m), m->fg64, (const double *) phi,
@@ -439,18 +459,18 @@ extern "C" int cupcfd_gpu_dev_adjoint(cupcfd_gpu_mesh *m, int32_t precision, con
     if (precision == CUPCFD_PREC_F64 && m->tiles && aligned16(grad) && aligned16(state) &&
         aligned16(gface) && m->nC % 2 == 0) {
         kt.set_name("k_adj_f64_pf");
-        k_adj_f64_pf<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg64, (const double *) grad, 2.0, (const double *) state,
-                                           (const double *) gface, (double *) phiBar, (double *) phiBBar,
-                                           (double *) stateBar, m->nC, prefetch_args(m, PF_ADJ_F64));
+        CG_LAUNCH_PF(m, k_adj_f64_pf, grid, st, m->nC, sell(m), m->fg64, (const double *) grad, 2.0,
+                     (const double *) state, (const double *) gface, (double *) phiBar, (double *) phiBBar,
+                     (double *) stateBar, m->nC, prefetch_args(m, PF_ADJ_F64));
     } else if (precision == CUPCFD_PREC_F64) {
         kt.set_name("k_adj_f64");
         k_adj_f64<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg64, (const double *) grad, 2.0, (const double *) state,
                                         (const double *) gface, (double *) phiBar, (double *) phiBBar, (double *) stateBar, m->nC);
     } else if (m->tiles && aligned16(grad) && aligned16(state) && aligned16(gface) && m->nC % 4 == 0) {
         kt.set_name("k_adj_f32_pf");
-        k_adj_f32_pf<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg32, (const float *) grad, 2.f, (const float4 *) state,
-                                           (const float *) gface, (float *) phiBar, (float *) phiBBar,
-                                           (float4 *) stateBar, m->nC, prefetch_args(m, PF_ADJ_F32));
+        CG_LAUNCH_PF(m, k_adj_f32_pf, grid, st, m->nC, sell(m), m->fg32, (const float *) grad, 2.f,
+                     (const float4 *) state, (const float *) gface, (float *) phiBar, (float *) phiBBar,
+                     (float4 *) stateBar, m->nC, prefetch_args(m, PF_ADJ_F32));
     } else {
         kt.set_name("k_adj_f32");
         k_adj_f32<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg32, (const float *) grad, 2.f, (const float4 *) state,
@@ -483,9 +503,9 @@ extern "C" int cupcfd_gpu_dev_forward_adjoint(cupcfd_gpu_mesh *m, int32_t precis
         PrefetchArgs pf = prefetch_args(m, PF_FWD_MADJ), pfg = prefetch_args(m, PF_GADJ);
         {
             KTIMER("k_fwd_madj_f32_pf", st);
-            k_fwd_madj_f32_pf<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg32, (const float *) phi, (const float *) phiB,
-                                                m->vol, (const float4 *) state, (const float *) gface, (float *) grad,
-                                                (float *) massFlux, (float4 *) stateBar, part, m->nC, pf);
+            CG_LAUNCH_PF(m, k_fwd_madj_f32_pf, grid, st, m->nC, sell(m), m->fg32, (const float *) phi,
+                         (const float *) phiB, m->vol, (const float4 *) state, (const float *) gface, (float *) grad,
+                         (float *) massFlux, (float4 *) stateBar, part, m->nC, pf);
             CG_LAUNCHED();
         }
         {
@@ -495,8 +515,8 @@ extern "C" int cupcfd_gpu_dev_forward_adjoint(cupcfd_gpu_mesh *m, int32_t precis
         }
         {
             KTIMER("k_gadj_f32_pf", st);
-            k_gadj_f32_pf<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg32, (const float *) grad, 2.f, (float *) phiBar,
-                                                (float *) phiBBar, m->nC, pfg);
+            CG_LAUNCH_PF(m, k_gadj_f32_pf, grid, st, m->nC, sell(m), m->fg32, (const float *) grad, 2.f,
+                         (float *) phiBar, (float *) phiBBar, m->nC, pfg);
             CG_LAUNCHED();
         }
         return CUPCFD_E_SUCCESS;

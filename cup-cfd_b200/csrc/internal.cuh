@@ -92,6 +92,7 @@ struct cupcfd_gpu_mesh {
     int nInc = 0, maxDeg = 0;
     int order = 0, precisions = 0;
     int realSize = 8;           // bytes of the real type the source arrays held (4: a T = float mesh)
+    int fullWidth = 0;          // 6: every cell has six incidences, the prefetch kernels' specialisation
     bool xpacZero = true;       // all xpac = xnac = 0 (meshes built through a MeshSource)
     bool allDefaultRegions = true;
 

@@ -31,7 +31,7 @@ __device__ __forceinline__ void block_sum_store(double v, double *out) {
 
 // Per-cell body of the FP64 fused forward (exact reference arithmetic).
 // Returns this cell's loss contribution (0 when gface is null).
-template <int CH>
+template <int CH, int WF = 0>
 __device__ __forceinline__ double fwd_cell_f64(int c, const SellView &sv, const double4 *__restrict__ fg,
                                                const double *__restrict__ phi, const double *__restrict__ phiB,
                                                const double *__restrict__ vol, const double *__restrict__ st,
@@ -39,6 +39,7 @@ __device__ __forceinline__ double fwd_cell_f64(int c, const SellView &sv, const 
                                                double *__restrict__ mflux, int64_t ldc) {
     int w;
     const int2 *e = cell_entries(sv, c, w);
+    if (WF) w = WF;  // every cell has exactly WF entries (a full, uniform slice width)
     double phic = phi[c];
     double r0 = st[c], u0 = st[ldc + c], v0 = st[2 * ldc + c], w0 = st[3 * ldc + c];
     double ax = 0.0, ay = 0.0, az = 0.0, lsum = 0.0;
@@ -50,7 +51,7 @@ __device__ __forceinline__ double fwd_cell_f64(int c, const SellView &sv, const 
 #pragma unroll
         for (int j = 0; j < CH; j++) {
             int code = en[j].x;
-            if (code < 0) continue;
+            if (!WF && code < 0) continue;
             int f = code >> 1, o = en[j].y;
             G[j] = ldg4(fg + f);
             pv[j] = o >= 0 ? __ldg(phi + o) : __ldg(phiB + (-1 - o));
@@ -63,7 +64,7 @@ __device__ __forceinline__ double fwd_cell_f64(int c, const SellView &sv, const 
 #pragma unroll
         for (int j = 0; j < CH; j++) {
             int code = en[j].x;
-            if (code < 0) continue;
+            if (!WF && code < 0) continue;
             bool isN = code & 1;
             int o = en[j].y;
             double phif;
@@ -93,7 +94,7 @@ __device__ __forceinline__ double fwd_cell_f64(int c, const SellView &sv, const 
 }
 
 // Per-cell body of the FP32 fused forward; state as float4 {rho, u, v, w}.
-template <int CH>
+template <int CH, int WF = 0>
 __device__ __forceinline__ double fwd_cell_f32(int c, const SellView &sv, const float4 *__restrict__ fg,
                                                const float *__restrict__ phi, const float *__restrict__ phiB,
                                                const double *__restrict__ vol, const float4 *__restrict__ st,
@@ -101,6 +102,7 @@ __device__ __forceinline__ double fwd_cell_f32(int c, const SellView &sv, const 
                                                float *__restrict__ mflux, int64_t ldc) {
     int w;
     const int2 *e = cell_entries(sv, c, w);
+    if (WF) w = WF;  // every cell has exactly WF entries (a full, uniform slice width)
     float phic = phi[c];
     float4 sc = st[c];
     Acc2x2 axy;  // (gx, gy) packed, gz alone
@@ -114,7 +116,7 @@ __device__ __forceinline__ double fwd_cell_f32(int c, const SellView &sv, const 
 #pragma unroll
         for (int j = 0; j < CH; j++) {
             int code = en[j].x;
-            if (code < 0) continue;
+            if (!WF && code < 0) continue;
             int f = code >> 1, o = en[j].y;
             G[j] = __ldg(fg + f);
             pv[j] = o >= 0 ? __ldg(phi + o) : __ldg(phiB + (-1 - o));
@@ -126,7 +128,7 @@ __device__ __forceinline__ double fwd_cell_f32(int c, const SellView &sv, const 
 #pragma unroll
         for (int j = 0; j < CH; j++) {
             int code = en[j].x;
-            if (code < 0) continue;
+            if (!WF && code < 0) continue;
             bool isN = code & 1;
             int o = en[j].y;
             float phif;
@@ -159,7 +161,7 @@ __device__ __forceinline__ double fwd_cell_f32(int c, const SellView &sv, const 
 // forward of fwd_cell_f32 plus, over every interior face, the rhobar / ubar
 // accumulation of adj_cell_f32, with the same arithmetic in the same face
 // order, so stbar equals the one the full adjoint writes bit for bit.
-template <int CH, int PIPE = 0>
+template <int CH, int PIPE = 0, int WF = 0>
 __device__ __forceinline__ double fwd_madj_cell_f32(int c, const SellView &sv, const float4 *__restrict__ fg,
                                                     const float *__restrict__ phi, const float *__restrict__ phiB,
                                                     const double *__restrict__ vol, const float4 *__restrict__ st,
@@ -168,6 +170,7 @@ __device__ __forceinline__ double fwd_madj_cell_f32(int c, const SellView &sv, c
                                                     int64_t ldc) {
     int w;
     const int2 *e = cell_entries(sv, c, w);
+    if (WF) w = WF;  // every cell has exactly WF entries (a full, uniform slice width)
     float phic = phi[c];
     float4 sc = st[c];
     // seven compensated sums in packed pairs: (gx, gy), (gz, rhobar), (ubar, vbar), wbar
@@ -182,7 +185,7 @@ __device__ __forceinline__ double fwd_madj_cell_f32(int c, const SellView &sv, c
 #pragma unroll
         for (int j = 0; j < CH; j++) {
             int code = en[j].x;
-            if (code < 0) continue;
+            if (!WF && code < 0) continue;
             int f = code >> 1, o = en[j].y;
             G[j] = __ldg(fg + f);
             pv[j] = o >= 0 ? __ldg(phi + o) : __ldg(phiB + (-1 - o));
@@ -196,7 +199,7 @@ __device__ __forceinline__ double fwd_madj_cell_f32(int c, const SellView &sv, c
 #pragma unroll
         for (int j = 0; j < CH; j++) {
             int code = en[j].x;
-            if (code < 0) continue;
+            if (!WF && code < 0) continue;
             bool isN = code & 1;
             int o = en[j].y;
             float phif;
@@ -337,13 +340,14 @@ __device__ __forceinline__ float ldg_g(const float *p) { return LDCG ? __ldcg(p)
 template <bool LDCG>
 __device__ __forceinline__ double ldg_g(const double *p) { return LDCG ? __ldcg(p) : __ldg(p); }
 
-template <bool LDCG, int CH = CUPCFD_ADJ_CHUNK_F64>
+template <bool LDCG, int CH = CUPCFD_ADJ_CHUNK_F64, int WF = 0>
 __device__ __forceinline__ void adj_cell_f64(int c, const SellView &sv, const double4 *__restrict__ fg,
                                              const double *g, double hscale, const double *__restrict__ st,
                                              const double *__restrict__ gface, double *__restrict__ phibar,
                                              double *__restrict__ phibBar, double *__restrict__ stbar, int64_t ldc) {
     int w;
     const int2 *e = cell_entries(sv, c, w);
+    if (WF) w = WF;  // every cell has exactly WF entries (a full, uniform slice width)
     bool doG = hscale != 0.0, doM = gface != nullptr;
     double hx = 0, hy = 0, hz = 0;
     if (doG) { hx = hscale * ldg_g<LDCG>(g + c); hy = hscale * ldg_g<LDCG>(g + ldc + c); hz = hscale * ldg_g<LDCG>(g + 2 * ldc + c); }
@@ -358,7 +362,7 @@ __device__ __forceinline__ void adj_cell_f64(int c, const SellView &sv, const do
 #pragma unroll
         for (int j = 0; j < CH; j++) {
             int code = en[j].x;
-            if (code < 0) continue;
+            if (!WF && code < 0) continue;
             int f = code >> 1, o = en[j].y;
             G[j] = ldg4(fg + f);
             if (o < 0) continue;
@@ -372,7 +376,7 @@ __device__ __forceinline__ void adj_cell_f64(int c, const SellView &sv, const do
 #pragma unroll
         for (int j = 0; j < CH; j++) {
             int code = en[j].x;
-            if (code < 0) continue;
+            if (!WF && code < 0) continue;
             int o = en[j].y;
             if (o < 0) {
                 if (doG) phibBar[-1 - o] = __fma_rn(hx, G[j].x, __fma_rn(hy, G[j].y, __dmul_rn(hz, G[j].z)));
@@ -402,13 +406,14 @@ __device__ __forceinline__ void adj_cell_f64(int c, const SellView &sv, const do
     if (doM) { stbar[c] = rb; stbar[ldc + c] = ub; stbar[2 * ldc + c] = vb; stbar[3 * ldc + c] = wb; }
 }
 
-template <bool LDCG, int CH = CUPCFD_ADJ_CHUNK, int PIPE = 0>
+template <bool LDCG, int CH = CUPCFD_ADJ_CHUNK, int PIPE = 0, int WF = 0>
 __device__ __forceinline__ void adj_cell_f32(int c, const SellView &sv, const float4 *__restrict__ fg, const float *g,
                                              float hscale, const float4 *__restrict__ st,
                                              const float *__restrict__ gface, float *__restrict__ phibar,
                                              float *__restrict__ phibBar, float4 *__restrict__ stbar, int64_t ldc) {
     int w;
     const int2 *e = cell_entries(sv, c, w);
+    if (WF) w = WF;  // every cell has exactly WF entries (a full, uniform slice width)
     bool doG = hscale != 0.f, doM = gface != nullptr;
     float hx = 0, hy = 0, hz = 0;
     if (doG) { hx = hscale * ldg_g<LDCG>(g + c); hy = hscale * ldg_g<LDCG>(g + ldc + c); hz = hscale * ldg_g<LDCG>(g + 2 * ldc + c); }
@@ -424,7 +429,7 @@ __device__ __forceinline__ void adj_cell_f32(int c, const SellView &sv, const fl
 #pragma unroll
         for (int j = 0; j < CH; j++) {
             int code = en[j].x;
-            if (code < 0) continue;
+            if (!WF && code < 0) continue;
             int f = code >> 1, o = en[j].y;
             G[j] = __ldg(fg + f);
             if (o < 0) continue;
@@ -436,7 +441,7 @@ __device__ __forceinline__ void adj_cell_f32(int c, const SellView &sv, const fl
 #pragma unroll
         for (int j = 0; j < CH; j++) {
             int code = en[j].x;
-            if (code < 0) continue;
+            if (!WF && code < 0) continue;
             int o = en[j].y;
             if (o < 0) {
                 if (doG) phibBar[-1 - o] = fmaf(hx, G[j].x, fmaf(hy, G[j].y, hz * G[j].z));

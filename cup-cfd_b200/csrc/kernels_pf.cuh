@@ -19,8 +19,15 @@ namespace cupcfd_gpu {
 // block asks L2 to fetch the contiguous ranges of the tile `dist` blocks
 // ahead (cp.async.bulk.prefetch.L2). Shared memory and L1 are untouched;
 // the streamed loads of later blocks become L2 hits.
+//
+// WF: 0 for any mesh; 6 when every cell has exactly six incidences (all
+// hexahedral meshes: every slice six entries wide, no padding). The cell
+// loop then has a compile-time trip count: no padding checks, the chunks
+// unrolled and their loads scheduled across chunks (same arithmetic in the
+// same order, so the same bits).
 // ---------------------------------------------------------------------------
 
+template <int WF>
 __global__ void __launch_bounds__(TILE_CELLS, CUPCFD_MINB_F32)
     k_fwd_f32_pf(int nC, SellView sv, const float4 *__restrict__ fg, const float *__restrict__ phi,
                  const float *__restrict__ phiB, const double *__restrict__ vol, const float4 *__restrict__ st,
@@ -35,11 +42,12 @@ __global__ void __launch_bounds__(TILE_CELLS, CUPCFD_MINB_F32)
     const int cellBytes[3] = {T * 4, T * 16, T * 8};
     if (lead) fetch_ranges_async(&s_rng, pf.desc + tp);
     double l = 0.0;
-    if (c < nC) l = fwd_cell_f32<CUPCFD_FWD_CHUNK>(c, sv, fg, phi, phiB, vol, st, gface, g, mflux, ldc);
+    if (c < nC) l = fwd_cell_f32<CUPCFD_FWD_CHUNK, WF>(c, sv, fg, phi, phiB, vol, st, gface, g, mflux, ldc);
     if (lead) prefetch_tile<3>(pf, tp, ranges_ready(&s_rng), fg, 16, gface, cellSrc, cellBytes);
     if (lossPart) block_sum_store<T>(l, lossPart);
 }
 
+template <int WF>
 __global__ void __launch_bounds__(TILE_CELLS, CUPCFD_MINB_F32)
     k_adj_f32_pf(int nC, SellView sv, const float4 *__restrict__ fg, const float *__restrict__ g, float hscale,
                  const float4 *__restrict__ st, const float *__restrict__ gface, float *__restrict__ phibar,
@@ -52,12 +60,13 @@ __global__ void __launch_bounds__(TILE_CELLS, CUPCFD_MINB_F32)
     const void *const cellSrc[4] = {g, g + ldc, g + 2 * ldc, st};
     const int cellBytes[4] = {T * 4, T * 4, T * 4, T * 16};
     if (lead) fetch_ranges_async(&s_rng, pf.desc + tp);
-    if (c < nC) adj_cell_f32<false>(c, sv, fg, g, hscale, st, gface, phibar, phibBar, stbar, ldc);
+    if (c < nC) adj_cell_f32<false, CUPCFD_ADJ_CHUNK, 0, WF>(c, sv, fg, g, hscale, st, gface, phibar, phibBar, stbar, ldc);
     if (lead) prefetch_tile<4>(pf, tp, ranges_ready(&s_rng), fg, 16, gface, cellSrc, cellBytes);
 }
 
 // FP64 forward (fwd_cell_f64, exact reference arithmetic) with the same L2
 // prefetch; the state's four component blocks are prefetched one by one.
+template <int WF>
 __global__ void __launch_bounds__(TILE_CELLS, CUPCFD_MINB_FWD_F64)
     k_fwd_f64_pf(int nC, SellView sv, const double4 *__restrict__ fg, const double *__restrict__ phi,
                  const double *__restrict__ phiB, const double *__restrict__ vol, const double *__restrict__ st,
@@ -72,12 +81,13 @@ __global__ void __launch_bounds__(TILE_CELLS, CUPCFD_MINB_FWD_F64)
     const int cellBytes[6] = {T * 8, T * 8, T * 8, T * 8, T * 8, T * 8};
     if (lead) fetch_ranges_async(&s_rng, pf.desc + tp);
     double l = 0.0;
-    if (c < nC) l = fwd_cell_f64<CUPCFD_FWD_CHUNK_F64>(c, sv, fg, phi, phiB, vol, st, gface, g, mflux, ldc);
+    if (c < nC) l = fwd_cell_f64<CUPCFD_FWD_CHUNK_F64, WF>(c, sv, fg, phi, phiB, vol, st, gface, g, mflux, ldc);
     if (lead) prefetch_tile<6>(pf, tp, ranges_ready(&s_rng), fg, 32, gface, cellSrc, cellBytes);
     if (lossPart) block_sum_store<T>(l, lossPart);
 }
 
 // FP64 adjoint (adj_cell_f64) with the same L2 prefetch.
+template <int WF>
 __global__ void __launch_bounds__(TILE_CELLS, CUPCFD_MINB_ADJ_F64)
     k_adj_f64_pf(int nC, SellView sv, const double4 *__restrict__ fg, const double *__restrict__ g, double hscale,
                  const double *__restrict__ st, const double *__restrict__ gface, double *__restrict__ phibar,
@@ -90,7 +100,7 @@ __global__ void __launch_bounds__(TILE_CELLS, CUPCFD_MINB_ADJ_F64)
     const void *const cellSrc[7] = {g, g + ldc, g + 2 * ldc, st, st + ldc, st + 2 * ldc, st + 3 * ldc};
     const int cellBytes[7] = {T * 8, T * 8, T * 8, T * 8, T * 8, T * 8, T * 8};
     if (lead) fetch_ranges_async(&s_rng, pf.desc + tp);
-    if (c < nC) adj_cell_f64<false>(c, sv, fg, g, hscale, st, gface, phibar, phibBar, stbar, ldc);
+    if (c < nC) adj_cell_f64<false, CUPCFD_ADJ_CHUNK_F64, WF>(c, sv, fg, g, hscale, st, gface, phibar, phibBar, stbar, ldc);
     if (lead) prefetch_tile<7>(pf, tp, ranges_ready(&s_rng), fg, 32, gface, cellSrc, cellBytes);
 }
 
@@ -103,6 +113,7 @@ __global__ void __launch_bounds__(TILE_CELLS, CUPCFD_MINB_ADJ_F64)
 #ifndef CUPCFD_MINB_FWD_MADJ
 #define CUPCFD_MINB_FWD_MADJ 4
 #endif
+template <int WF>
 __global__ void __launch_bounds__(TILE_CELLS, CUPCFD_MINB_FWD_MADJ)
     k_fwd_madj_f32_pf(int nC, SellView sv, const float4 *__restrict__ fg, const float *__restrict__ phi,
                       const float *__restrict__ phiB, const double *__restrict__ vol, const float4 *__restrict__ st,
@@ -117,7 +128,7 @@ __global__ void __launch_bounds__(TILE_CELLS, CUPCFD_MINB_FWD_MADJ)
     const int cellBytes[3] = {T * 4, T * 16, T * 8};
     if (lead) fetch_ranges_async(&s_rng, pf.desc + tp);
     double l = 0.0;
-    if (c < nC) l = fwd_madj_cell_f32<CUPCFD_FWD_MADJ_CHUNK>(c, sv, fg, phi, phiB, vol, st, gface, g, mflux, stbar, ldc);
+    if (c < nC) l = fwd_madj_cell_f32<CUPCFD_FWD_MADJ_CHUNK, 0, WF>(c, sv, fg, phi, phiB, vol, st, gface, g, mflux, stbar, ldc);
     if (lead) prefetch_tile<3>(pf, tp, ranges_ready(&s_rng), fg, 16, gface, cellSrc, cellBytes);
     if (lossPart) block_sum_store<T>(l, lossPart);
 }
@@ -132,6 +143,7 @@ __global__ void __launch_bounds__(TILE_CELLS, CUPCFD_MINB_FWD_MADJ)
 #ifndef CUPCFD_MINB_GADJ
 #define CUPCFD_MINB_GADJ 6
 #endif
+template <int WF>
 __global__ void __launch_bounds__(TILE_CELLS, CUPCFD_MINB_GADJ)
     k_gadj_f32_pf(int nC, SellView sv, const float4 *__restrict__ fg, const float *__restrict__ g, float hscale,
                   float *__restrict__ phibar, float *__restrict__ phibBar, int64_t ldc, PrefetchArgs pf) {
@@ -144,7 +156,7 @@ __global__ void __launch_bounds__(TILE_CELLS, CUPCFD_MINB_GADJ)
     const int cellBytes[3] = {T * 4, T * 4, T * 4};
     if (lead) fetch_ranges_async(&s_rng, pf.desc + tp);
     if (c < nC)
-        adj_cell_f32<false, CUPCFD_ADJ_CHUNK, CUPCFD_GADJ_PIPE>(c, sv, fg, g, hscale, nullptr, nullptr, phibar,
+        adj_cell_f32<false, CUPCFD_ADJ_CHUNK, CUPCFD_GADJ_PIPE, WF>(c, sv, fg, g, hscale, nullptr, nullptr, phibar,
                                                                 phibBar, nullptr, ldc);
     if (lead) prefetch_tile<3>(pf, tp, ranges_ready(&s_rng), fg, 16, (const float *) nullptr, cellSrc, cellBytes);
 }

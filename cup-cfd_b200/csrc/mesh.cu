@@ -914,7 +914,7 @@ extern "C" int cupcfd_gpu_mesh_get_info(const cupcfd_gpu_mesh *m, cupcfd_mesh_in
     info->bandwidth = m->bandwidth;
     info->deviceBytes = m->bytes;
     info->tiles = m->tiles ? 1 : 0;
-    info->reserved = 0;
+    info->fullWidth = m->tiles ? m->fullWidth : 0;
     return CUPCFD_E_SUCCESS;
 }
 

@@ -128,7 +128,8 @@ typedef struct {
     int32_t bandwidth;   /* largest |c - neighbour| of the internal numbering */
     int64_t deviceBytes; /* device memory held by the mesh */
     int32_t tiles;       /* 1 when the face loops take the L2-prefetch kernels (faces numbered by owner tile) */
-    int32_t reserved;
+    int32_t fullWidth;   /* 6 when those kernels run their six-incidence specialisation (every cell has six
+                            faces: hexahedral meshes), else 0 */
 } cupcfd_mesh_info;
 
 typedef struct cupcfd_gpu_mesh cupcfd_gpu_mesh;

@@ -186,6 +186,51 @@ def test_forward_adjoint_pipeline_equals_separate_calls(cg, gpu, kind, dims, ord
     _assert_same(_run_pipeline(cg, torch, mesh, *fields, offset=True), ref)
 
 
+@pytest.mark.parametrize("kind,dims,order", [("structgen", (40, 32, 24), "ORDER_RCM"),
+                                             ("structgen", (33, 17, 9), "ORDER_MORTON"),
+                                             ("jittered", (20, 18, 16), "ORDER_OWNER")])
+def test_six_incidence_kernels_equal_general_kernels(cg, gpu, kind, dims, order, monkeypatch):
+    """On hexahedral meshes the L2-prefetch kernels run a specialisation for
+    cells of exactly six incidences (compile-time trip count, no padding
+    checks): the same arithmetic in the same order, so the forward+adjoint
+    pipeline, the separate FP32 calls and the FP64 forward give the same bits
+    as the general kernels (CUPCFD_FULL_WIDTH=0 at mesh creation)."""
+    import torch
+    monkeypatch.setenv("CUPCFD_FULL_WIDTH", "0")
+    general = _mesh(cg, kind, dims, order)
+    monkeypatch.delenv("CUPCFD_FULL_WIDTH")
+    six = _mesh(cg, kind, dims, order)
+    assert six.tiles and general.tiles and six.full_width == 6 and general.full_width == 0
+    fields = _fields(torch, six, 13)
+    _assert_same(_run_pipeline(cg, torch, six, *fields, offset=False),
+                 _run_pipeline(cg, torch, general, *fields, offset=False))
+    _assert_same(_run(cg, torch, six, *fields, offset=False), _run(cg, torch, general, *fields, offset=False))
+    phi = fields[0].double()
+    phiB = fields[1].double()
+    st = fields[2].double().t().contiguous()
+    gface = fields[3].double()
+    outs = []
+    for mesh in (six, general):
+        grad = torch.full((3, mesh.nCells), float("nan"), dtype=torch.float64, device="cuda:0")
+        mf = torch.zeros(mesh.nFaces, dtype=torch.float64, device="cuda:0")
+        loss = torch.zeros(1, dtype=torch.float64, device="cuda:0")
+        cg.dev_forward(mesh, cg.PREC_F64, phi, phiB, st, grad, mf, gface=gface, loss=loss,
+                       stream=torch.cuda.current_stream())
+        mesh.check_status()
+        torch.cuda.synchronize()
+        outs.append((grad, mf, loss))
+    for x, y in zip(*outs):
+        assert torch.equal(x, y)
+
+
+def test_polyhedral_mesh_runs_general_kernels(cg, gpu):
+    """Cells of other face counts keep the general kernels."""
+    import oracle as O
+    m = O.merge_cells(O.jitter(9, 8, 7, 0.25, seed=5, permute=True), 0.4, 11, max_cells=6)
+    mesh = cg.Mesh.from_arrays(m, order=cg.ORDER_OWNER)
+    assert mesh.tiles and mesh.full_width == 0
+
+
 def test_device_timers_name_the_pipeline_kernels(cg, gpu):
     """cupcfd_gpu_timing_*: the forward+adjoint call's three launches, each
     timed on its stream, counted per kernel, and cleared by the read."""
