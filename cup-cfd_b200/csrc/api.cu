@@ -35,6 +35,26 @@ int scratch(cupcfd_gpu_mesh *m, int slot, size_t n, T **p) {
 }
 
 inline cudaStream_t as_stream(void *s) { return (cudaStream_t) s; }
+
+// The mesh's second stream and its events (created on first use): the host
+// forward+adjoint's copy-back stream, and the loss reduction beside the
+// gradient adjoint in the device forward+adjoint.
+// The stream has the device's highest priority, so that the loss
+// reduction's one block is placed as soon as an SM has room for it, not
+// after the gradient adjoint's blocks.
+#ifndef CUPCFD_AUX_PRIORITY
+#define CUPCFD_AUX_PRIORITY 1
+#endif
+int pipe_init(cupcfd_gpu_mesh *m) {
+    if (m->outStream) return CUPCFD_E_SUCCESS;
+    for (cudaEvent_t &e : m->pipeEv)
+        if (!e) CG_CHECK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    int lo = 0, hi = 0;
+    CG_CHECK_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    CG_CHECK_CUDA(cudaStreamCreateWithPriority(&m->outStream, cudaStreamNonBlocking, CUPCFD_AUX_PRIORITY ? hi : lo));
+    return CUPCFD_E_SUCCESS;
+}
+
 inline SellView sell(const cupcfd_gpu_mesh *m) { return SellView{m->sell.slicePtr, m->sell.inc, m->sell.width}; }
 
 // The width the L2-prefetch kernels are specialised for (kernels_pf.cuh:
@@ -500,6 +520,7 @@ extern "C" int cupcfd_gpu_dev_forward_adjoint(cupcfd_gpu_mesh *m, int32_t precis
         unsigned grid = grid_for(m->nC, BLK);
         double *part;
         CG_TRY(scratch(m, S_LOSS, grid, &part));
+        CG_TRY(pipe_init(m));
         PrefetchArgs pf = prefetch_args(m, PF_FWD_MADJ), pfg = prefetch_args(m, PF_GADJ);
         {
             KTIMER("k_fwd_madj_f32_pf", st);
@@ -509,16 +530,24 @@ extern "C" int cupcfd_gpu_dev_forward_adjoint(cupcfd_gpu_mesh *m, int32_t precis
             CG_LAUNCHED();
         }
         {
-            KTIMER("k_reduce_partials", st);
-            k_reduce_partials<<<1, 1024, 0, st>>>((int) grid, part, lp);
+            // the FP64 loss reduction (one block) runs on the mesh's second
+            // stream beside the gradient adjoint, which does not need it;
+            // the caller's stream waits for both
+            cudaStream_t so = m->outStream;
+            CG_CHECK_CUDA(cudaEventRecord(m->pipeEv[0], st));
+            CG_CHECK_CUDA(cudaStreamWaitEvent(so, m->pipeEv[0], 0));
+            KTIMER("k_reduce_partials", so);
+            k_reduce_partials<<<1, 1024, 0, so>>>((int) grid, part, lp);
             CG_LAUNCHED();
         }
+        CG_CHECK_CUDA(cudaEventRecord(m->pipeEv[1], m->outStream));
         {
             KTIMER("k_gadj_f32_pf", st);
             CG_LAUNCH_PF(m, k_gadj_f32_pf, grid, st, m->nC, sell(m), m->fg32, (const float *) grad, 2.f,
                          (float *) phiBar, (float *) phiBBar, m->nC, pfg);
             CG_LAUNCHED();
         }
+        CG_CHECK_CUDA(cudaStreamWaitEvent(st, m->pipeEv[1], 0));
         return CUPCFD_E_SUCCESS;
     }
     CG_TRY(cupcfd_gpu_dev_forward(m, precision, phi, phiB, state, gface, grad, massFlux, lp, stream));
@@ -853,16 +882,8 @@ extern "C" int cupcfd_gpu_flux_mass_dolfyn_face_loop_f32(
                                         teC, nTeC, teB, nTeB, edC, nEdC, edB, nEdB, visC, nVisC, visB, nVisB, tC, nTC, tB, nTB);
 }
 
-namespace {
-// The copy-back stream and events of a mesh's host forward+adjoint.
-int pipe_init(cupcfd_gpu_mesh *m) {
-    if (m->outStream) return CUPCFD_E_SUCCESS;
-    for (cudaEvent_t &e : m->pipeEv)
-        if (!e) CG_CHECK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    CG_CHECK_CUDA(cudaStreamCreateWithFlags(&m->outStream, cudaStreamNonBlocking));
-    return CUPCFD_E_SUCCESS;
-}
 
+namespace {
 // One part of the benchmark adjoint with the plain adjoint kernels: the
 // gradient part (phibar, phibBar from g, hscale 2) when state and gface are
 // null, the mass part (stateBar) when g is null and hscale 0. Each output's

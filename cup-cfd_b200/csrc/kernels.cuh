@@ -179,7 +179,11 @@ __device__ __forceinline__ float4 ldg4(const float4 *p) { return __ldg(p); }
 // Entries per chunk in the unrolled kernels (six covers a hex cell in one
 // chunk; wider cells take more chunks) and the minimum resident blocks per
 // SM the register allocation must allow, per kernel family. Chosen by
-// measurement on B200; overridable at build time.
+// measurement on B200; overridable at build time. The per-cell routines of
+// the forward and adjoint also take WF: 0 for any mesh, or the number of
+// incidences every cell has (6 for hexahedral meshes), which fixes the
+// chunk loop's trip count at compile time and drops the padding tests
+// (kernels_pf.cuh).
 #ifndef CUPCFD_GRAD_CHUNK
 #define CUPCFD_GRAD_CHUNK 6
 #endif
