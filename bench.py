@@ -826,7 +826,9 @@ def run_gpu(a):
             "kernels": kernels,
             "separate_calls": separate,
             "mesh": {"order": ["native", "morton", "owner", "rcm"][a.order], "bandwidth": mesh.bandwidth,
-                     "forward_adjoint": "two launches: forward with the mass-flux adjoint, then the gradient adjoint"},
+                     "incidence_width": mesh.full_width or "general",
+                     "forward_adjoint": ("two launches: forward with the mass-flux adjoint, then the gradient "
+                                         "adjoint; the FP64 loss reduction on a second stream beside the second")},
             "fp64_plain_forward": {"value": world * nF / (ms64 * 1e-3) / 1e9, "unit": "Gfaces/s", "ms_per_step": ms64,
                                    "gbs": bm["fwd_f64"] / (ms64 * 1e-3) / 1e9,
                                    "frac": bm["fwd_f64"] / (ms64 * 1e-3) / 1e9 / peak},
