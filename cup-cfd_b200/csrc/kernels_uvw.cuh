@@ -131,6 +131,24 @@ struct UvwArgs {
     T *su, *sv_, *sw, *au, *av, *aw;       // [nC] internal
 };
 
+// The values of the thread's own cell that every incidence reads (centre,
+// velocity, viscosity, the nine gradient components): loaded once per cell
+// instead of once per incidence. The terms use them exactly where the
+// reference uses cell1's or cell2's values, so the arithmetic is unchanged.
+template <class T>
+struct UvwOwn {
+    typename UvwReal<T>::V4 cc;
+    T u, v, w, vis, g[9];
+};
+template <class T>
+__device__ __forceinline__ UvwOwn<T> uvw_own(const UvwArgs<T> &a, int c) {
+    UvwOwn<T> o;
+    o.cc = a.cc[c]; o.u = a.u[c]; o.v = a.v[c]; o.w = a.w[c]; o.vis = a.visC[c];
+#pragma unroll
+    for (int q = 0; q < 9; q++) o.g[q] = a.grads[q * a.ldg + c];
+    return o;
+}
+
 // visFace that face g leaves behind (interior, inlet and outlet faces set it,
 // UVWKernels.ipp:160, 274, 335).
 template <class T>
@@ -162,7 +180,7 @@ enum UvwKind : int {
 // The terms one incidence (entry en of cell c) contributes to its cell, and
 // the face's own outputs when c owns the face. Returns the UvwKind.
 template <class T>
-__device__ __forceinline__ int uvw_terms(const UvwArgs<T> &a, int c, int2 en, T (&t)[10]) {
+__device__ __forceinline__ int uvw_terms(const UvwArgs<T> &a, int c, const UvwOwn<T> &own, int2 en, T (&t)[10]) {
     using R = UvwReal<T>;
     using V4 = typename UvwReal<T>::V4;
     const int64_t L = a.ldg;
@@ -173,17 +191,22 @@ __device__ __forceinline__ int uvw_terms(const UvwArgs<T> &a, int c, int2 en, T 
     const T rl = a.rlencos ? (T) a.rlencos[f] : T(0);
     if (en.y >= 0) {
         // interior face (UVWKernels.ipp:145-228)
-        const int ip = owner ? c : en.y, in = owner ? en.y : c;
+        const int o = en.y;  // the other cell: cell2 (in) for the owner, cell1 (ip) for the neighbour
         const T facn = G.w, facp = R::one_minus(facn);
+        // the other cell's and this cell's weights: facn weights cell2 (in),
+        // facp cell1 (ip); x_in*facn + x_ip*facp is then x_o*wO + x_c*wC for
+        // either role (IEEE addition commutes exactly)
+        const T wO = owner ? facn : facp, wC = owner ? facp : facn;
         T du[3], dv[3], dw[3];
 #pragma unroll
         for (int d = 0; d < 3; d++) {
-            du[d] = R::add(R::mul(gr(d, in), facn), R::mul(gr(d, ip), facp));
-            dv[d] = R::add(R::mul(gr(3 + d, in), facn), R::mul(gr(3 + d, ip), facp));
-            dw[d] = R::add(R::mul(gr(6 + d, in), facn), R::mul(gr(6 + d, ip), facp));
+            du[d] = R::add(R::mul(gr(d, o), wO), R::mul(own.g[d], wC));
+            dv[d] = R::add(R::mul(gr(3 + d, o), wO), R::mul(own.g[3 + d], wC));
+            dw[d] = R::add(R::mul(gr(6 + d, o), wO), R::mul(own.g[6 + d], wC));
         }
-        const T visac = R::add(R::mul(a.visC[in], facn), R::mul(a.visC[ip], facp));
-        const V4 Cn = a.cc[in], Cp = a.cc[ip];
+        const T visac = R::add(R::mul(a.visC[o], wO), R::mul(own.vis, wC));
+        const V4 Co = a.cc[o];
+        const V4 Cn = owner ? Co : own.cc, Cp = owner ? own.cc : Co;
         const T x0 = R::sub(Cn.x, Cp.x), x1 = R::sub(Cn.y, Cp.y), x2 = R::sub(Cn.z, Cp.z);
         const T visFace = R::mul(visac, rl);
         T uF = T(0), vF = T(0), wF = T(0);
@@ -196,9 +219,10 @@ __device__ __forceinline__ int uvw_terms(const UvwArgs<T> &a, int c, int2 en, T 
         }
         const T mf = a.massFlux[f];
         const T fmin = std_min(mf, T(0)), fmax = std_max(mf, T(0));
-        const T fuci = R::add(R::mul(fmin, a.u[in]), R::mul(fmax, a.u[ip]));
-        const T fvci = R::add(R::mul(fmin, a.v[in]), R::mul(fmax, a.v[ip]));
-        const T fwci = R::add(R::mul(fmin, a.w[in]), R::mul(fmax, a.w[ip]));
+        const T mO = owner ? fmin : fmax, mC = owner ? fmax : fmin;  // fmin weights cell2, fmax cell1
+        const T fuci = R::add(R::mul(mO, a.u[o]), R::mul(mC, own.u));
+        const T fvci = R::add(R::mul(mO, a.v[o]), R::mul(mC, own.v));
+        const T fwci = R::add(R::mul(mO, a.w[o]), R::mul(mC, own.w));
         t[0] = R::mul(a.gammaBlend, R::sub(R::mul(mf, uF), fuci));
         t[3] = R::mul(a.gammaBlend, R::sub(R::mul(mf, vF), fvci));
         t[6] = R::mul(a.gammaBlend, R::sub(R::mul(mf, wF), fwci));
@@ -222,12 +246,12 @@ __device__ __forceinline__ int uvw_terms(const UvwArgs<T> &a, int c, int2 en, T 
     const int ir = a.bndRegion[ib];
     const int it = a.regionType[ir];
     if (it == CUPCFD_RTYPE_DEFAULT) return UVW_NONE;
-    const V4 X = a.fc[f], Cp = a.cc[c];
+    const V4 X = a.fc[f], Cp = own.cc;
     const T x0 = R::sub(X.x, Cp.x), x1 = R::sub(X.y, Cp.y), x2 = R::sub(X.z, Cp.z);
-    const T uc = a.u[c], vc = a.v[c], wc = a.w[c];
-    const T du0 = gr(0, c), du1 = gr(1, c), du2 = gr(2, c);
-    const T dv0 = gr(3, c), dv1 = gr(4, c), dv2 = gr(5, c);
-    const T dw0 = gr(6, c), dw1 = gr(7, c), dw2 = gr(8, c);
+    const T uc = own.u, vc = own.v, wc = own.w;
+    const T du0 = own.g[0], du1 = own.g[1], du2 = own.g[2];
+    const T dv0 = own.g[3], dv1 = own.g[4], dv2 = own.g[5];
+    const T dw0 = own.g[6], dw1 = own.g[7], dw2 = own.g[8];
     if (it == CUPCFD_RTYPE_INLET || it == CUPCFD_RTYPE_OUTLET) {
         // UVWKernels.ipp:259-382 (outlet: operands of two sums swapped,
         // which IEEE addition does not see)
@@ -238,7 +262,7 @@ __device__ __forceinline__ int uvw_terms(const UvwArgs<T> &a, int c, int2 en, T 
             visac = a.visB[ib];
         } else {
             uF = uc; vF = vc; wF = wc;
-            visac = a.visC[c];
+            visac = own.vis;
         }
         const T visFace = R::mul(visac, rl);
         T mf = a.massFlux[f];
@@ -267,7 +291,7 @@ __device__ __forceinline__ int uvw_terms(const UvwArgs<T> &a, int c, int2 en, T 
         // UVWKernels.ipp:383-436; visFace carried from an earlier face
         const int g = a.carry ? a.carry[f] : -1;
         Xc = g >= 0 ? vis_face_of(a, g) : T(0);
-        const T visac = a.visC[c];
+        const T visac = own.vis;
         const T us0 = R::add(uc, dot0(du0, du1, du2, x0, x1, x2));
         const T us1 = R::add(vc, dot0(dv0, dv1, dv2, x0, x1, x2));
         const T us2 = R::add(wc, dot0(dw0, dw1, dw2, x0, x1, x2));
@@ -346,7 +370,8 @@ __device__ __forceinline__ void uvw_fold(int kind, const T (&t)[10], T (&s)[3], 
 // the terms staged in shared memory and one warp folding them measured
 // slower: 4.2-5.0 ms against 2.3 ms at 256^3.)
 #ifndef UVW_CELL_MINB
-#define UVW_CELL_MINB 3  // resident 256-thread blocks per SM asked of the register allocator (80 registers)
+#define UVW_CELL_MINB 2  // resident 256-thread blocks per SM asked of the register allocator (118 registers:
+                         // the own-cell values held for the whole cell; 3 blocks at 80 spill them)
 #endif
 #ifndef UVW_CHUNK
 #define UVW_CHUNK 6      // incidence entries loaded ahead (a hexahedral cell in one chunk)
@@ -356,6 +381,7 @@ __device__ __forceinline__ void uvw_cell(const UvwArgs<T> &a, int c) {
     int wdt;
     const int2 *e = cell_entries(a.sv, c, wdt);
     T s[3] = {a.su[c], a.sv_[c], a.sw[c]}, ad[3] = {a.au[c], a.av[c], a.aw[c]};
+    const UvwOwn<T> own = uvw_own(a, c);
     // the chunk's entries first (independent loads), then incidence by incidence
     for (int k0 = 0; k0 < wdt; k0 += UVW_CHUNK) {
         int2 en[UVW_CHUNK];
@@ -363,7 +389,7 @@ __device__ __forceinline__ void uvw_cell(const UvwArgs<T> &a, int c) {
         for (int j = 0; j < UVW_CHUNK; j++) {
             if (en[j].x < 0) break;
             T t[10];
-            int kind = uvw_terms(a, c, en[j], t);
+            int kind = uvw_terms(a, c, own, en[j], t);
             uvw_fold(kind, t, s, ad);
         }
     }
@@ -400,7 +426,9 @@ __device__ __forceinline__ void uvw_cell_pf(const UvwArgs<T> &a, const PrefetchA
 }
 
 // FP64 (the reference's T = double): plain and L2-prefetch launches.
-// 2.13 ms at 256^3 with the prefetch against 2.21 ms without.
+// At 256^3 on one box: 2.15 ms with the own-cell values held at two blocks
+// per SM, against 2.22 ms reloading them at three; 2.01 ms with the weights
+// selected once per incidence instead of each value.
 __global__ void __launch_bounds__(256, UVW_CELL_MINB) k_uvw_f64(const __grid_constant__ UvwArgs<double> a) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c < a.nC) uvw_cell(a, c);
