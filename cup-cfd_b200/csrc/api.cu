@@ -36,9 +36,9 @@ int scratch(cupcfd_gpu_mesh *m, int slot, size_t n, T **p) {
 
 inline cudaStream_t as_stream(void *s) { return (cudaStream_t) s; }
 
-// The mesh's second stream and its events (created on first use): the host
-// forward+adjoint's copy-back stream, and the loss reduction beside the
-// gradient adjoint in the device forward+adjoint.
+// The mesh's second and third streams and their events (created on first
+// use): the host forward+adjoint's copy-back and copy-in streams, and the
+// loss reduction beside the gradient adjoint in the device forward+adjoint.
 // The stream has the device's highest priority, so that the loss
 // reduction's one block is placed as soon as an SM has room for it, not
 // after the gradient adjoint's blocks.
@@ -49,6 +49,9 @@ int pipe_init(cupcfd_gpu_mesh *m) {
     if (m->outStream) return CUPCFD_E_SUCCESS;
     for (cudaEvent_t &e : m->pipeEv)
         if (!e) CG_CHECK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    for (cudaEvent_t &e : m->inEv)
+        if (!e) CG_CHECK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    if (!m->inStream) CG_CHECK_CUDA(cudaStreamCreateWithFlags(&m->inStream, cudaStreamNonBlocking));
     int lo = 0, hi = 0;
     CG_CHECK_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
     CG_CHECK_CUDA(cudaStreamCreateWithPriority(&m->outStream, cudaStreamNonBlocking, CUPCFD_AUX_PRIORITY ? hi : lo));
@@ -962,9 +965,16 @@ int forward_adjoint_t(cupcfd_gpu_mesh *m, int32_t precision, const H *phi, const
     H *oG = out, *oMf = out + 3 * (size_t) nC, *oPb = oMf + nF, *oR = oPb + nC, *oU = oR + nC, *oV = oU + nC,
            *oW = oV + nC, *oPbb = oW + nC;
 
+    // The inputs go in on the copy-in stream, each set's arrival an event the
+    // computation waits for, so the copy engine carries the next set while the
+    // GPU computes on the last (issued in this order, so that host staging of
+    // pageable arrays still overlaps the computation).
+    cudaStream_t si = m->inStream;
     // phi in, gradient
-    CG_CHECK_CUDA(cudaMemcpyAsync(hPhi, phi, HS * (size_t) nC, cudaMemcpyHostToDevice, st));
-    if (nB > 0) CG_CHECK_CUDA(cudaMemcpyAsync(hPb, phiB, HS * (size_t) nB, cudaMemcpyHostToDevice, st));
+    CG_CHECK_CUDA(cudaMemcpyAsync(hPhi, phi, HS * (size_t) nC, cudaMemcpyHostToDevice, si));
+    if (nB > 0) CG_CHECK_CUDA(cudaMemcpyAsync(hPb, phiB, HS * (size_t) nB, cudaMemcpyHostToDevice, si));
+    CG_CHECK_CUDA(cudaEventRecord(m->inEv[0], si));
+    CG_CHECK_CUDA(cudaStreamWaitEvent(st, m->inEv[0], 0));
     if (f64) {
         k_gather<H, double><<<gC, BLK, 0, st>>>(nC, 1, m->cellN2O, hPhi, 0, (double *) phiI, 0);
         if (nB > 0) {
@@ -983,17 +993,21 @@ int forward_adjoint_t(cupcfd_gpu_mesh *m, int32_t precision, const H *phi, const
     CG_TRY(launch_adj_part(m, f64, gradI, 2.0, nullptr, nullptr, pbI, pbbI, nullptr, st));
     CG_CHECK_CUDA(cudaEventRecord(m->pipeEv[0], st));
     // state in, mass flux
-    CG_CHECK_CUDA(cudaMemcpyAsync(hR, den, HS * (size_t) nC, cudaMemcpyHostToDevice, st));
-    CG_CHECK_CUDA(cudaMemcpyAsync(hU, u, HS * (size_t) nC, cudaMemcpyHostToDevice, st));
-    CG_CHECK_CUDA(cudaMemcpyAsync(hV, v, HS * (size_t) nC, cudaMemcpyHostToDevice, st));
-    CG_CHECK_CUDA(cudaMemcpyAsync(hW, w, HS * (size_t) nC, cudaMemcpyHostToDevice, st));
+    CG_CHECK_CUDA(cudaMemcpyAsync(hR, den, HS * (size_t) nC, cudaMemcpyHostToDevice, si));
+    CG_CHECK_CUDA(cudaMemcpyAsync(hU, u, HS * (size_t) nC, cudaMemcpyHostToDevice, si));
+    CG_CHECK_CUDA(cudaMemcpyAsync(hV, v, HS * (size_t) nC, cudaMemcpyHostToDevice, si));
+    CG_CHECK_CUDA(cudaMemcpyAsync(hW, w, HS * (size_t) nC, cudaMemcpyHostToDevice, si));
+    CG_CHECK_CUDA(cudaEventRecord(m->inEv[1], si));
+    CG_CHECK_CUDA(cudaStreamWaitEvent(st, m->inEv[1], 0));
     if (f64) k_gather<H, double><<<gC, BLK, 0, st>>>(nC, 4, m->cellN2O, hR, nC, (double *) stI, ldc);
     else k_state_to_f4<H><<<gC, BLK, 0, st>>>(nC, m->cellN2O, hR, hU, hV, hW, (float4 *) stI);
     CG_LAUNCHED();
     CG_TRY(cupcfd_gpu_dev_mass_plain(m, precision, stI, mfI, st));
     CG_CHECK_CUDA(cudaEventRecord(m->pipeEv[1], st));
     // gface in, loss and adjoint
-    CG_CHECK_CUDA(cudaMemcpyAsync(hG, gface, HS * (size_t) nF, cudaMemcpyHostToDevice, st));
+    CG_CHECK_CUDA(cudaMemcpyAsync(hG, gface, HS * (size_t) nF, cudaMemcpyHostToDevice, si));
+    CG_CHECK_CUDA(cudaEventRecord(m->inEv[2], si));
+    CG_CHECK_CUDA(cudaStreamWaitEvent(st, m->inEv[2], 0));
     if (f64) k_gather<H, double><<<gF, BLK, 0, st>>>(nF, 1, m->faceN2O, hG, 0, (double *) gI, 0);
     else k_gather<H, float><<<gF, BLK, 0, st>>>(nF, 1, m->faceN2O, hG, 0, (float *) gI, 0);
     CG_LAUNCHED();

@@ -84,10 +84,12 @@ struct Sell {
 struct cupcfd_gpu_mesh {
     int device = 0;
     cudaStream_t stream = nullptr;  // used by the host-buffer calls
-    // the host forward+adjoint's copies back run on outStream after pipeEv[i]
+    // the host forward+adjoint's copies back run on outStream after pipeEv[i],
+    // its copies in on inStream, each input set's arrival inEv[i]
     // (created on first use)
-    cudaStream_t outStream = nullptr;
+    cudaStream_t outStream = nullptr, inStream = nullptr;
     cudaEvent_t pipeEv[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t inEv[3] = {nullptr, nullptr, nullptr};
     int nC = 0, nF = 0, nB = 0, nFi = 0, nR = 0;
     int nInc = 0, maxDeg = 0;
     int order = 0, precisions = 0;

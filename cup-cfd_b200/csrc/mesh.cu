@@ -823,12 +823,16 @@ extern "C" int cupcfd_gpu_mesh_destroy(cupcfd_gpu_mesh *m) {
     cudaSetDevice(m->device);
     if (m->stream) cudaStreamSynchronize(m->stream);
     if (m->outStream) cudaStreamSynchronize(m->outStream);
+    if (m->inStream) cudaStreamSynchronize(m->inStream);
     for (auto &b : m->owned) cudaFree(b.p);
     for (auto &b : m->scratch)
         if (b.p) cudaFree(b.p);
     for (cudaEvent_t e : m->pipeEv)
         if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : m->inEv)
+        if (e) cudaEventDestroy(e);
     if (m->outStream) cudaStreamDestroy(m->outStream);
+    if (m->inStream) cudaStreamDestroy(m->inStream);
     if (m->stream) cudaStreamDestroy(m->stream);
     delete m;
     return CUPCFD_E_SUCCESS;
