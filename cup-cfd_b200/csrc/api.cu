@@ -65,11 +65,12 @@ inline SellView sell(const cupcfd_gpu_mesh *m) { return SellView{m->sell.slicePt
 // (all hexahedral meshes), else 0 (the general kernels).
 inline int full_width(const cupcfd_gpu_mesh *m) { return m->fullWidth; }
 // launches the L2-prefetch kernel template K at the mesh's full width
-#define CG_LAUNCH_PF(m, K, grid, st, ...)                                      \
-    do {                                                                       \
-        if (full_width(m) == 6) K<6><<<(grid), BLK, 0, (st)>>>(__VA_ARGS__);   \
-        else K<0><<<(grid), BLK, 0, (st)>>>(__VA_ARGS__);                      \
+#define CG_LAUNCH_PF_BLOCK(m, K, grid, block, st, ...)                          \
+    do {                                                                        \
+        if (full_width(m) == 6) K<6><<<(grid), (block), 0, (st)>>>(__VA_ARGS__); \
+        else K<0><<<(grid), (block), 0, (st)>>>(__VA_ARGS__);                   \
     } while (0)
+#define CG_LAUNCH_PF(m, K, grid, st, ...) CG_LAUNCH_PF_BLOCK(m, K, grid, BLK, st, __VA_ARGS__)
 
 // ---------------------------------------------------------------------------
 // device timers (cupcfd_gpu_timing_*): a KTIMER scope records one event
@@ -157,10 +158,12 @@ int tiles_setup(cupcfd_gpu_mesh *m, cudaStream_t st) {
         w6 ? (const void *) k_adj_f64_pf<6> : (const void *) k_adj_f64_pf<0>,
         w6 ? (const void *) k_fwd_madj_f32_pf<6> : (const void *) k_fwd_madj_f32_pf<0>,
         w6 ? (const void *) k_gadj_f32_pf<6> : (const void *) k_gadj_f32_pf<0>};
+    // block sizes: 256 threads (one tile) except the forward+mass adjoint's
+    const int pfBlock[6] = {TILE_CELLS, TILE_CELLS, TILE_CELLS, TILE_CELLS, CUPCFD_FWD_MADJ_BLOCK, TILE_CELLS};
     for (int i = 0; i < 6; i++) {
         int nb = 0;
-        CG_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pfKern[i], TILE_CELLS, 0));
-        m->prefetchWave[i] = sms * std::max(1, nb);
+        CG_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pfKern[i], pfBlock[i], 0));
+        m->prefetchWave[i] = sms * std::max(1, nb * pfBlock[i] / TILE_CELLS);  // in tiles
     }
     m->prefetchDist = m->prefetchWave[PF_FWD_F32];
     if (const char *e = std::getenv("CUPCFD_PREFETCH_DIST"))
@@ -521,13 +524,16 @@ extern "C" int cupcfd_gpu_dev_forward_adjoint(cupcfd_gpu_mesh *m, int32_t precis
         CG_RETURN_IF(((uintptr_t) lp) % 8 != 0, CUPCFD_E_CONFIG_INVALID_VALUE, "dev_forward_adjoint: loss not 8-byte aligned");
         cudaStream_t st = as_stream(stream);
         unsigned grid = grid_for(m->nC, BLK);
+        // one loss partial per warp: TILE_CELLS / 32 per tile
+        constexpr int WPT = TILE_CELLS / 32;
         double *part;
-        CG_TRY(scratch(m, S_LOSS, grid, &part));
+        CG_TRY(scratch(m, S_LOSS, (size_t) grid * WPT, &part));
         CG_TRY(pipe_init(m));
         PrefetchArgs pf = prefetch_args(m, PF_FWD_MADJ), pfg = prefetch_args(m, PF_GADJ);
         {
             KTIMER("k_fwd_madj_f32_pf", st);
-            CG_LAUNCH_PF(m, k_fwd_madj_f32_pf, grid, st, m->nC, sell(m), m->fg32, (const float *) phi,
+            CG_LAUNCH_PF_BLOCK(m, k_fwd_madj_f32_pf, grid * (TILE_CELLS / CUPCFD_FWD_MADJ_BLOCK), CUPCFD_FWD_MADJ_BLOCK,
+                         st, m->nC, sell(m), m->fg32, (const float *) phi,
                          (const float *) phiB, m->vol, (const float4 *) state, (const float *) gface, (float *) grad,
                          (float *) massFlux, (float4 *) stateBar, part, m->nC, pf);
             CG_LAUNCHED();
@@ -540,7 +546,7 @@ extern "C" int cupcfd_gpu_dev_forward_adjoint(cupcfd_gpu_mesh *m, int32_t precis
             CG_CHECK_CUDA(cudaEventRecord(m->pipeEv[0], st));
             CG_CHECK_CUDA(cudaStreamWaitEvent(so, m->pipeEv[0], 0));
             KTIMER("k_reduce_partials", so);
-            k_reduce_partials<<<1, 1024, 0, so>>>((int) grid, part, lp);
+            k_reduce_partials<WPT><<<1, 1024, 0, so>>>((int) grid, part, lp);
             CG_LAUNCHED();
         }
         CG_CHECK_CUDA(cudaEventRecord(m->pipeEv[1], m->outStream));

@@ -300,20 +300,41 @@ __global__ void __launch_bounds__(256) k_loss(int nC, SellView sv, const T *__re
 // t adds part[t], part[t + blockDim], ... in that order, then a tree over
 // the block. The loads of each group of 16 are issued before its adds, so
 // they overlap instead of each add waiting on its own load.
+// G > 1: the n block values are given as G partials each, partial k of
+// block i at part[k n + i] (one per warp of a 256-cell tile, G = 8, stored
+// warp-major so that these loads coalesce), summed in order from 0.0 first:
+// the value block_sum_store<32 G> forms, so the result has the same bits.
+template <int G>
+__device__ __forceinline__ double group_value(const double *v) {
+    if (G == 1) return v[0];
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < G; k++) s += v[k];
+    return s;
+}
+
+template <int G = 1>
 __global__ void k_reduce_partials(int n, const double *__restrict__ part, double *__restrict__ out) {
     __shared__ double red[1024];
-    constexpr int U = 16;
+    constexpr int U = G >= 16 ? 1 : 16 / G;
     const int bd = blockDim.x;
     double t = 0.0;
     int i = threadIdx.x;
     for (; i + (U - 1) * bd < n; i += U * bd) {
-        double v[U];
+        double v[U * G];
 #pragma unroll
-        for (int j = 0; j < U; j++) v[j] = __ldg(part + i + j * bd);
+        for (int j = 0; j < U; j++)
 #pragma unroll
-        for (int j = 0; j < U; j++) t += v[j];
+            for (int k = 0; k < G; k++) v[j * G + k] = __ldg(part + (size_t) k * n + i + j * bd);
+#pragma unroll
+        for (int j = 0; j < U; j++) t += group_value<G>(v + j * G);
     }
-    for (; i < n; i += bd) t += part[i];
+    for (; i < n; i += bd) {
+        double v[G];
+#pragma unroll
+        for (int k = 0; k < G; k++) v[k] = part[(size_t) k * n + i];
+        t += group_value<G>(v);
+    }
     red[threadIdx.x] = t;
     __syncthreads();
     for (int k = blockDim.x / 2; k > 0; k >>= 1) {

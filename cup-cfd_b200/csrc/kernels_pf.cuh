@@ -107,22 +107,35 @@ __global__ void __launch_bounds__(TILE_CELLS, CUPCFD_MINB_ADJ_F64)
 // Forward with the mass-flux adjoint (fwd_madj_cell_f32), L2 prefetch as
 // k_fwd_f32_pf. With k_gadj_f32_pf it forms the two-launch forward+adjoint:
 // the state and gface are then read by one pass only.
+//
+// It runs in blocks of CUPCFD_FWD_MADJ_BLOCK = 64 threads, four per tile, at
+// the same registers and warps per SM as 256-thread blocks: a block's slot
+// frees when its two warps end instead of its slowest of eight (measured at
+// 256^3: 0.543 ms against 0.568 ms; 32-thread blocks 0.540). The last block
+// of a tile prefetches for the tile. The loss partials are one per warp,
+// warp k of tile t at lossPart[k nTiles + t]; k_reduce_partials<8> sums each
+// tile's eight in order, which gives the per-tile value of
+// block_sum_store<256> bit for bit.
 #ifndef CUPCFD_FWD_MADJ_CHUNK
 #define CUPCFD_FWD_MADJ_CHUNK 2
 #endif
 #ifndef CUPCFD_MINB_FWD_MADJ
-#define CUPCFD_MINB_FWD_MADJ 4
+#define CUPCFD_MINB_FWD_MADJ 4  // in 256-cell tiles per SM
+#endif
+#ifndef CUPCFD_FWD_MADJ_BLOCK
+#define CUPCFD_FWD_MADJ_BLOCK 64
 #endif
 template <int WF>
-__global__ void __launch_bounds__(TILE_CELLS, CUPCFD_MINB_FWD_MADJ)
+__global__ void __launch_bounds__(CUPCFD_FWD_MADJ_BLOCK, CUPCFD_MINB_FWD_MADJ *TILE_CELLS / CUPCFD_FWD_MADJ_BLOCK)
     k_fwd_madj_f32_pf(int nC, SellView sv, const float4 *__restrict__ fg, const float *__restrict__ phi,
                       const float *__restrict__ phiB, const double *__restrict__ vol, const float4 *__restrict__ st,
                       const float *__restrict__ gface, float *__restrict__ g, float *__restrict__ mflux,
                       float4 *__restrict__ stbar, double *__restrict__ lossPart, int64_t ldc, PrefetchArgs pf) {
-    constexpr int T = TILE_CELLS;
-    int c = blockIdx.x * T + threadIdx.x;
-    const int tp = blockIdx.x + pf.dist;
-    const bool lead = threadIdx.x == T - 32 && tp < pf.nTiles;
+    constexpr int T = TILE_CELLS, B = CUPCFD_FWD_MADJ_BLOCK, P = T / B;
+    static_assert(T % B == 0 && B % 32 == 0, "whole warps, whole tiles");
+    int c = blockIdx.x * B + threadIdx.x;
+    const int tp = blockIdx.x / P + pf.dist;
+    const bool lead = blockIdx.x % P == P - 1 && threadIdx.x == B - 32 && tp < pf.nTiles;
     __shared__ int4 s_rng;
     const void *const cellSrc[3] = {phi, st, vol};
     const int cellBytes[3] = {T * 4, T * 16, T * 8};
@@ -130,7 +143,10 @@ __global__ void __launch_bounds__(TILE_CELLS, CUPCFD_MINB_FWD_MADJ)
     double l = 0.0;
     if (c < nC) l = fwd_madj_cell_f32<CUPCFD_FWD_MADJ_CHUNK, 0, WF>(c, sv, fg, phi, phiB, vol, st, gface, g, mflux, stbar, ldc);
     if (lead) prefetch_tile<3>(pf, tp, ranges_ready(&s_rng), fg, 16, gface, cellSrc, cellBytes);
-    if (lossPart) block_sum_store<T>(l, lossPart);
+    if (lossPart) {
+        for (int k = 16; k > 0; k >>= 1) l += __shfl_xor_sync(0xffffffffu, l, k);
+        if ((threadIdx.x & 31) == 0) lossPart[(size_t) ((c >> 5) % (T / 32)) * (gridDim.x / P) + c / T] = l;
+    }
 }
 
 // Gradient part of the adjoint only (adj_cell_f32 without the mass part):

@@ -373,6 +373,13 @@ __device__ __forceinline__ void uvw_fold(int kind, const T (&t)[10], T (&s)[3], 
 #define UVW_CELL_MINB 2  // resident 256-thread blocks per SM asked of the register allocator (118 registers:
                          // the own-cell values held for the whole cell; 3 blocks at 80 spill them)
 #endif
+// The L2-prefetch launches run 64-thread blocks, four per 256-cell tile, at
+// the same registers and warps per SM: a block's slot frees when its two
+// warps end instead of its slowest of eight (2.007 -> 1.941 ms at 256^3;
+// 128-thread blocks 1.964, 32-thread 1.954).
+#ifndef UVW_PF_BLOCK
+#define UVW_PF_BLOCK 64
+#endif
 #ifndef UVW_CHUNK
 #define UVW_CHUNK 6      // incidence entries loaded ahead (a hexahedral cell in one chunk)
 #endif
@@ -400,14 +407,16 @@ __device__ __forceinline__ void uvw_cell(const UvwArgs<T> &a, int c) {
 // The same with the L2 prefetch of the tile one wave of this kernel's
 // resident blocks ahead (prefetch.cuh): its entries, face records and mass
 // fluxes, and its cells' entries in the twenty cell arrays the loop reads.
-// Needs the owner-sorted face order, 256-thread blocks and 16-byte aligned
-// arrays.
+// Needs the owner-sorted face order and 16-byte aligned arrays; launched as
+// UVW_PF_BLOCK-thread blocks, TILE_CELLS / UVW_PF_BLOCK per tile (the last
+// block of a tile prefetches for the tile).
 template <class T>
 __device__ __forceinline__ void uvw_cell_pf(const UvwArgs<T> &a, const PrefetchArgs &pf) {
-    constexpr int TC = TILE_CELLS;
-    const int c = blockIdx.x * TC + threadIdx.x;
-    const int tp = blockIdx.x + pf.dist;
-    const bool lead = threadIdx.x == TC - 32 && tp < pf.nTiles;
+    constexpr int TC = TILE_CELLS, B = UVW_PF_BLOCK, P = TC / B;
+    static_assert(TC % B == 0 && B % 32 == 0, "whole warps, whole tiles");
+    const int c = blockIdx.x * B + threadIdx.x;
+    const int tp = blockIdx.x / P + pf.dist;
+    const bool lead = blockIdx.x % P == P - 1 && threadIdx.x == B - 32 && tp < pf.nTiles;
     __shared__ int4 s_rng;
     if (lead) fetch_ranges_async(&s_rng, pf.desc + tp);
     if (c < a.nC) uvw_cell(a, c);
@@ -433,7 +442,7 @@ __global__ void __launch_bounds__(256, UVW_CELL_MINB) k_uvw_f64(const __grid_con
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c < a.nC) uvw_cell(a, c);
 }
-__global__ void __launch_bounds__(TILE_CELLS, UVW_CELL_MINB) k_uvw_f64_pf(const __grid_constant__ UvwArgs<double> a,
+__global__ void __launch_bounds__(UVW_PF_BLOCK, UVW_CELL_MINB *TILE_CELLS / UVW_PF_BLOCK) k_uvw_f64_pf(const __grid_constant__ UvwArgs<double> a,
                                                                           PrefetchArgs pf) {
     uvw_cell_pf(a, pf);
 }
@@ -442,7 +451,7 @@ __global__ void __launch_bounds__(256, UVW_CELL_MINB) k_uvw_f32ref(const __grid_
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c < a.nC) uvw_cell(a, c);
 }
-__global__ void __launch_bounds__(TILE_CELLS, UVW_CELL_MINB) k_uvw_f32ref_pf(const __grid_constant__ UvwArgs<float> a,
+__global__ void __launch_bounds__(UVW_PF_BLOCK, UVW_CELL_MINB *TILE_CELLS / UVW_PF_BLOCK) k_uvw_f32ref_pf(const __grid_constant__ UvwArgs<float> a,
                                                                              PrefetchArgs pf) {
     uvw_cell_pf(a, pf);
 }

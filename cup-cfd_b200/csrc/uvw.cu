@@ -82,8 +82,9 @@ bool prefetch_disabled() {
     return off;
 }
 
-// Prefetch distance of the L2-prefetch kernel `kern`: one wave of its
-// resident blocks (SMs x blocks per SM), the measured optimum for
+// Prefetch distance of the L2-prefetch kernel `kern`, in tiles: one wave of
+// its resident blocks (SMs x tiles' worth of blocks per SM), the measured
+// optimum for
 // k_uvw_f64_pf (2.13 ms at 256^3 against 2.35-2.39 ms for 1/3 to 4/3 of a
 // wave; CUPCFD_PREFETCH_DIST overrides).
 int prefetch_wave(int device, const void *kern) {
@@ -92,10 +93,10 @@ int prefetch_wave(int device, const void *kern) {
     std::lock_guard<std::mutex> g(mu);
     auto it = wave.find({device, kern});
     if (it != wave.end()) return it->second;
-    int sms = 148, blocks = UVW_CELL_MINB;
+    int sms = 148, blocks = UVW_CELL_MINB * TILE_CELLS / UVW_PF_BLOCK;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kern, TILE_CELLS, 0);
-    int d = std::max(1, sms * std::max(1, blocks));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kern, UVW_PF_BLOCK, 0);
+    int d = std::max(1, sms * std::max(1, blocks * UVW_PF_BLOCK / TILE_CELLS));  // in tiles
     if (const char *e = std::getenv("CUPCFD_PREFETCH_DIST")) if (*e) d = std::max(1, std::atoi(e));
     wave[{device, kern}] = d;
     return d;
@@ -144,10 +145,10 @@ int run_face_loop(cupcfd_gpu_mesh *m, T gammaBlend, T small, const T *u, const T
         pf.nTiles = m->nTiles;
         if constexpr (F64) {
             pf.dist = prefetch_wave(m->device, (const void *) k_uvw_f64_pf);
-            k_uvw_f64_pf<<<grid_for(m->nC, TILE_CELLS), TILE_CELLS, 0, st>>>(a, pf);
+            k_uvw_f64_pf<<<grid_for(m->nC, TILE_CELLS) * (TILE_CELLS / UVW_PF_BLOCK), UVW_PF_BLOCK, 0, st>>>(a, pf);
         } else {
             pf.dist = prefetch_wave(m->device, (const void *) k_uvw_f32ref_pf);
-            k_uvw_f32ref_pf<<<grid_for(m->nC, TILE_CELLS), TILE_CELLS, 0, st>>>(a, pf);
+            k_uvw_f32ref_pf<<<grid_for(m->nC, TILE_CELLS) * (TILE_CELLS / UVW_PF_BLOCK), UVW_PF_BLOCK, 0, st>>>(a, pf);
         }
     } else {
         if constexpr (F64)
