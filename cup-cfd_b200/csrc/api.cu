@@ -18,7 +18,7 @@ namespace {
 constexpr int BLK = 256;
 
 // the L2-prefetch kernels, indexing cupcfd_gpu_mesh::prefetchWave
-enum PfKernel { PF_FWD_F32 = 0, PF_ADJ_F32, PF_FWD_F64, PF_ADJ_F64, PF_FWD_MADJ, PF_GADJ };
+enum PfKernel { PF_FWD_F32 = 0, PF_ADJ_F32, PF_FWD_F64, PF_ADJ_F64, PF_FWD_MADJ, PF_GADJ, PF_MADJ, PF_COUNT };
 
 // scratch slots of a mesh (each grows on demand and is reused across calls)
 enum Slot {
@@ -151,16 +151,20 @@ int tiles_setup(cupcfd_gpu_mesh *m, cudaStream_t st) {
     m->fullWidth = m->sell.width == 6 && (int64_t) m->nInc == 6 * (int64_t) m->nC &&
                    !(fw && std::strcmp(fw, "0") == 0) ? 6 : 0;
     const bool w6 = full_width(m) == 6;
-    const void *pfKern[6] = {
+    const void *pfKern[] = {
         w6 ? (const void *) k_fwd_f32_pf<6> : (const void *) k_fwd_f32_pf<0>,
         w6 ? (const void *) k_adj_f32_pf<6> : (const void *) k_adj_f32_pf<0>,
         w6 ? (const void *) k_fwd_f64_pf<6> : (const void *) k_fwd_f64_pf<0>,
         w6 ? (const void *) k_adj_f64_pf<6> : (const void *) k_adj_f64_pf<0>,
         w6 ? (const void *) k_fwd_madj_f32_pf<6> : (const void *) k_fwd_madj_f32_pf<0>,
-        w6 ? (const void *) k_gadj_f32_pf<6> : (const void *) k_gadj_f32_pf<0>};
+        w6 ? (const void *) k_gadj_f32_pf<6> : (const void *) k_gadj_f32_pf<0>,
+        w6 ? (const void *) k_madj_f32_pf<6> : (const void *) k_madj_f32_pf<0>};
+    static_assert(sizeof(pfKern) / sizeof(pfKern[0]) == PF_COUNT, "one kernel per PfKernel");
+    static_assert(PF_COUNT <= (int) (sizeof(m->prefetchWave) / sizeof(m->prefetchWave[0])), "room for every wave");
     // block sizes: 256 threads (one tile) except the forward+mass adjoint's
-    const int pfBlock[6] = {TILE_CELLS, TILE_CELLS, TILE_CELLS, TILE_CELLS, CUPCFD_FWD_MADJ_BLOCK, TILE_CELLS};
-    for (int i = 0; i < 6; i++) {
+    const int pfBlock[PF_COUNT] = {TILE_CELLS, TILE_CELLS, TILE_CELLS,           TILE_CELLS,
+                                   CUPCFD_FWD_MADJ_BLOCK, TILE_CELLS, TILE_CELLS};
+    for (int i = 0; i < PF_COUNT; i++) {
         int nb = 0;
         CG_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pfKern[i], pfBlock[i], 0));
         m->prefetchWave[i] = sms * std::max(1, nb * pfBlock[i] / TILE_CELLS);  // in tiles
@@ -893,13 +897,27 @@ extern "C" int cupcfd_gpu_flux_mass_dolfyn_face_loop_f32(
 
 
 namespace {
-// One part of the benchmark adjoint with the plain adjoint kernels: the
-// gradient part (phibar, phibBar from g, hscale 2) when state and gface are
-// null, the mass part (stateBar) when g is null and hscale 0. Each output's
-// sum is the one the combined kernels form, so the results are theirs.
+// One part of the benchmark adjoint: the gradient part (phibar, phibBar from
+// g, hscale 2) when state and gface are null, the mass part (stateBar) when g
+// is null and hscale 0. FP32 on tiled meshes with 16-byte aligned arrays: the
+// L2-prefetch kernels of each part (k_gadj_f32_pf, k_madj_f32_pf); else the
+// plain adjoint kernels. Each output's sum is the one the combined kernels
+// form, so the results are theirs.
 int launch_adj_part(const cupcfd_gpu_mesh *m, bool f64, const void *g, double hscale, const void *state,
                     const void *gface, void *phiBar, void *phiBBar, void *stateBar, cudaStream_t st) {
     unsigned grid = grid_for(m->nC, BLK);
+    const bool gradPart = gface == nullptr;
+    if (!f64 && m->tiles && m->nC % 4 == 0 &&
+        (gradPart ? hscale == 2.0 && aligned16(g) : hscale == 0.0 && !g && aligned16(state) && aligned16(gface))) {
+        if (gradPart)
+            CG_LAUNCH_PF(m, k_gadj_f32_pf, grid, st, m->nC, sell(m), m->fg32, (const float *) g, 2.f,
+                         (float *) phiBar, (float *) phiBBar, m->nC, prefetch_args(m, PF_GADJ));
+        else
+            CG_LAUNCH_PF(m, k_madj_f32_pf, grid, st, m->nC, sell(m), m->fg32, (const float4 *) state,
+                         (const float *) gface, (float4 *) stateBar, m->nC, prefetch_args(m, PF_MADJ));
+        CG_LAUNCHED();
+        return CUPCFD_E_SUCCESS;
+    }
     if (f64)
         k_adj_f64<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg64, (const double *) g, hscale, (const double *) state,
                                         (const double *) gface, (double *) phiBar, (double *) phiBBar,
@@ -997,6 +1015,26 @@ int forward_adjoint_t(cupcfd_gpu_mesh *m, int32_t precision, const H *phi, const
     CG_LAUNCHED();
     CG_TRY(launch_grad_once(m, precision, false, false, phiI, phibI, nullptr, gradI, nullptr, st));
     CG_TRY(launch_adj_part(m, f64, gradI, 2.0, nullptr, nullptr, pbI, pbbI, nullptr, st));
+    // Each result goes back to reference numbering (host type) on the mesh
+    // stream right after the kernel that makes it, so the copy stream only
+    // copies: its engine does not wait for a conversion between two copies.
+    if (f64) {
+        k_blocks_to_aos<double, H><<<gC, BLK, 0, st>>>(nC, 3, m->cellO2N, (const double *) gradI, ldc, oG);
+        k_gather<double, H><<<gC, BLK, 0, st>>>(nC, 1, m->cellO2N, (const double *) pbI, 0, oPb, 0);
+        if (nB > 0) {
+            k_convert<double, H><<<grid_for(nB, BLK), BLK, 0, st>>>(nB, (const double *) pbbI, oPbb);
+            g_launches.fetch_add(1, std::memory_order_relaxed);
+        }
+    } else {
+        k_blocks_to_aos<float, H><<<gC, BLK, 0, st>>>(nC, 3, m->cellO2N, (const float *) gradI, ldc, oG);
+        k_gather<float, H><<<gC, BLK, 0, st>>>(nC, 1, m->cellO2N, (const float *) pbI, 0, oPb, 0);
+        if (nB > 0) {
+            k_convert<float, H><<<grid_for(nB, BLK), BLK, 0, st>>>(nB, (const float *) pbbI, oPbb);
+            g_launches.fetch_add(1, std::memory_order_relaxed);
+        }
+    }
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    CG_LAUNCHED();
     CG_CHECK_CUDA(cudaEventRecord(m->pipeEv[0], st));
     // state in, mass flux
     CG_CHECK_CUDA(cudaMemcpyAsync(hR, den, HS * (size_t) nC, cudaMemcpyHostToDevice, si));
@@ -1009,6 +1047,9 @@ int forward_adjoint_t(cupcfd_gpu_mesh *m, int32_t precision, const H *phi, const
     else k_state_to_f4<H><<<gC, BLK, 0, st>>>(nC, m->cellN2O, hR, hU, hV, hW, (float4 *) stI);
     CG_LAUNCHED();
     CG_TRY(cupcfd_gpu_dev_mass_plain(m, precision, stI, mfI, st));
+    if (f64) k_faces_to_ref<double, H><<<gF, BLK, 0, st>>>(nF, m->faceO2N, m->faceCells, (const double *) mfI, oMf, 1);
+    else k_faces_to_ref<float, H><<<gF, BLK, 0, st>>>(nF, m->faceO2N, m->faceCells, (const float *) mfI, oMf, 1);
+    CG_LAUNCHED();
     CG_CHECK_CUDA(cudaEventRecord(m->pipeEv[1], st));
     // gface in, loss and adjoint
     CG_CHECK_CUDA(cudaMemcpyAsync(hG, gface, HS * (size_t) nF, cudaMemcpyHostToDevice, si));
@@ -1017,6 +1058,13 @@ int forward_adjoint_t(cupcfd_gpu_mesh *m, int32_t precision, const H *phi, const
     if (f64) k_gather<H, double><<<gF, BLK, 0, st>>>(nF, 1, m->faceN2O, hG, 0, (double *) gI, 0);
     else k_gather<H, float><<<gF, BLK, 0, st>>>(nF, 1, m->faceN2O, hG, 0, (float *) gI, 0);
     CG_LAUNCHED();
+    // the mass part of the adjoint first: its results are the last large set
+    // to go out; the loss (8 bytes) follows it
+    CG_TRY(launch_adj_part(m, f64, nullptr, 0.0, stI, gI, nullptr, nullptr, sbI, st));
+    if (f64) k_gather<double, H><<<gC, BLK, 0, st>>>(nC, 4, m->cellO2N, (const double *) sbI, ldc, oR, nC);
+    else k_f4_to_ref<H><<<gC, BLK, 0, st>>>(nC, m->cellO2N, (const float4 *) sbI, oR, oU, oV, oW);
+    CG_LAUNCHED();
+    CG_CHECK_CUDA(cudaEventRecord(m->pipeEv[2], st));
     if (f64)
         k_loss<double><<<gC, 256, 0, st>>>(nC, sell(m), (const double *) gI, (const double *) mfI,
                                            (const double *) gradI, m->vol, part, ldc);
@@ -1026,45 +1074,20 @@ int forward_adjoint_t(cupcfd_gpu_mesh *m, int32_t precision, const H *phi, const
     CG_LAUNCHED();
     k_reduce_partials<<<1, 1024, 0, st>>>((int) gC, part, dloss);
     CG_LAUNCHED();
-    CG_TRY(launch_adj_part(m, f64, nullptr, 0.0, stI, gI, nullptr, nullptr, sbI, st));
-    CG_CHECK_CUDA(cudaEventRecord(m->pipeEv[2], st));
 
-    // back to reference numbering (host type) and to the host, on the copy stream
+    // to the host, on the copy stream, each set once it exists
     CG_CHECK_CUDA(cudaStreamWaitEvent(so, m->pipeEv[0], 0));
-    if (f64) {
-        k_blocks_to_aos<double, H><<<gC, BLK, 0, so>>>(nC, 3, m->cellO2N, (const double *) gradI, ldc, oG);
-        k_gather<double, H><<<gC, BLK, 0, so>>>(nC, 1, m->cellO2N, (const double *) pbI, 0, oPb, 0);
-        if (nB > 0) {
-            k_convert<double, H><<<grid_for(nB, BLK), BLK, 0, so>>>(nB, (const double *) pbbI, oPbb);
-            g_launches.fetch_add(1, std::memory_order_relaxed);
-        }
-    } else {
-        k_blocks_to_aos<float, H><<<gC, BLK, 0, so>>>(nC, 3, m->cellO2N, (const float *) gradI, ldc, oG);
-        k_gather<float, H><<<gC, BLK, 0, so>>>(nC, 1, m->cellO2N, (const float *) pbI, 0, oPb, 0);
-        if (nB > 0) {
-            k_convert<float, H><<<grid_for(nB, BLK), BLK, 0, so>>>(nB, (const float *) pbbI, oPbb);
-            g_launches.fetch_add(1, std::memory_order_relaxed);
-        }
-    }
-    g_launches.fetch_add(1, std::memory_order_relaxed);
-    CG_LAUNCHED();
     if (grad) CG_CHECK_CUDA(cudaMemcpyAsync(grad, oG, 3 * HS * (size_t) nC, cudaMemcpyDeviceToHost, so));
     if (phiBar) CG_CHECK_CUDA(cudaMemcpyAsync(phiBar, oPb, HS * (size_t) nC, cudaMemcpyDeviceToHost, so));
     if (phiBBar && nB > 0) CG_CHECK_CUDA(cudaMemcpyAsync(phiBBar, oPbb, HS * (size_t) nB, cudaMemcpyDeviceToHost, so));
     CG_CHECK_CUDA(cudaStreamWaitEvent(so, m->pipeEv[1], 0));
-    if (f64) k_faces_to_ref<double, H><<<gF, BLK, 0, so>>>(nF, m->faceO2N, m->faceCells, (const double *) mfI, oMf, 1);
-    else k_faces_to_ref<float, H><<<gF, BLK, 0, so>>>(nF, m->faceO2N, m->faceCells, (const float *) mfI, oMf, 1);
-    CG_LAUNCHED();
     if (massFlux) CG_CHECK_CUDA(cudaMemcpyAsync(massFlux, oMf, HS * (size_t) nF, cudaMemcpyDeviceToHost, so));
     CG_CHECK_CUDA(cudaStreamWaitEvent(so, m->pipeEv[2], 0));
-    if (f64) k_gather<double, H><<<gC, BLK, 0, so>>>(nC, 4, m->cellO2N, (const double *) sbI, ldc, oR, nC);
-    else k_f4_to_ref<H><<<gC, BLK, 0, so>>>(nC, m->cellO2N, (const float4 *) sbI, oR, oU, oV, oW);
-    CG_LAUNCHED();
     if (denBar) CG_CHECK_CUDA(cudaMemcpyAsync(denBar, oR, HS * (size_t) nC, cudaMemcpyDeviceToHost, so));
     if (uBar) CG_CHECK_CUDA(cudaMemcpyAsync(uBar, oU, HS * (size_t) nC, cudaMemcpyDeviceToHost, so));
     if (vBar) CG_CHECK_CUDA(cudaMemcpyAsync(vBar, oV, HS * (size_t) nC, cudaMemcpyDeviceToHost, so));
     if (wBar) CG_CHECK_CUDA(cudaMemcpyAsync(wBar, oW, HS * (size_t) nC, cudaMemcpyDeviceToHost, so));
-    if (loss) CG_CHECK_CUDA(cudaMemcpyAsync(loss, dloss, 8, cudaMemcpyDeviceToHost, so));
+    if (loss) CG_CHECK_CUDA(cudaMemcpyAsync(loss, dloss, 8, cudaMemcpyDeviceToHost, st));
     CG_CHECK_CUDA(cudaStreamSynchronize(so));
     CG_CHECK_CUDA(cudaStreamSynchronize(st));
     return CUPCFD_E_SUCCESS;

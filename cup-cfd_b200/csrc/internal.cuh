@@ -147,7 +147,7 @@ struct cupcfd_gpu_mesh {
     int nTiles = 0;
     bool tiles = false;
     int prefetchDist = 0;         // tiles ahead for the L2 prefetch
-    int prefetchWave[6] = {0, 0, 0, 0, 0, 0};  // per prefetch kernel (PfKernel in api.cu): one wave of its blocks
+    int prefetchWave[8] = {};  // per prefetch kernel (PfKernel in api.cu): one wave of its blocks, in tiles
 
     std::vector<cupcfd_gpu::DevBuf> owned;  // everything above, freed by destroy
     std::vector<cupcfd_gpu::DevBuf> scratch; // reusable buffers for host-buffer calls

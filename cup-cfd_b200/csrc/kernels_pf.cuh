@@ -177,6 +177,27 @@ __global__ void __launch_bounds__(TILE_CELLS, CUPCFD_MINB_GADJ)
     if (lead) prefetch_tile<3>(pf, tp, ranges_ready(&s_rng), fg, 16, (const float *) nullptr, cellSrc, cellBytes);
 }
 
+// Mass-flux part of the adjoint only (adj_cell_f32 with hscale 0): stbar
+// from the state and gface, with the L2 prefetch of their tile ranges. The
+// host forward+adjoint call runs it once gface is in; with k_gadj_f32_pf for
+// the gradient part it forms the same sums as k_adj_f32_pf, so the same bits.
+template <int WF>
+__global__ void __launch_bounds__(TILE_CELLS, CUPCFD_MINB_F32)
+    k_madj_f32_pf(int nC, SellView sv, const float4 *__restrict__ fg, const float4 *__restrict__ st,
+                  const float *__restrict__ gface, float4 *__restrict__ stbar, int64_t ldc, PrefetchArgs pf) {
+    constexpr int T = TILE_CELLS;
+    int c = blockIdx.x * T + threadIdx.x;
+    const int tp = blockIdx.x + pf.dist;
+    const bool lead = threadIdx.x == T - 32 && tp < pf.nTiles;
+    __shared__ int4 s_rng;
+    const void *const cellSrc[1] = {st};
+    const int cellBytes[1] = {T * 16};
+    if (lead) fetch_ranges_async(&s_rng, pf.desc + tp);
+    if (c < nC)
+        adj_cell_f32<false, CUPCFD_ADJ_CHUNK, 0, WF>(c, sv, fg, nullptr, 0.f, st, gface, nullptr, nullptr, stbar, ldc);
+    if (lead) prefetch_tile<1>(pf, tp, ranges_ready(&s_rng), fg, 16, gface, cellSrc, cellBytes);
+}
+
 // Largest |c - neighbour| over the incidence lists (the numbering's bandwidth).
 // Launched with whole warps (blockDim a multiple of 32), no early return.
 __global__ void k_bandwidth(int nC, SellView sv, int *__restrict__ out) {
