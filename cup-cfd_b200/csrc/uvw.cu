@@ -82,8 +82,10 @@ bool prefetch_disabled() {
     return off;
 }
 
-// Prefetch distance of the L2-prefetch kernel `kern`, in tiles: one wave of
-// its resident blocks (SMs x tiles' worth of blocks per SM), the measured
+// Prefetch distance of the L2-prefetch kernel `kern`, in tiles: 1.25 waves
+// of its resident blocks (SMs x tiles' worth of blocks per SM): with
+// 64-thread blocks 1.87 ms at 256^3 against 1.94 at 1 wave, 1.95 at 1.5,
+// 2.08 at 0.75, 2.21 at 2. In 256-thread blocks one wave was the measured
 // optimum for
 // k_uvw_f64_pf (2.13 ms at 256^3 against 2.35-2.39 ms for 1/3 to 4/3 of a
 // wave; CUPCFD_PREFETCH_DIST overrides).
@@ -96,7 +98,7 @@ int prefetch_wave(int device, const void *kern) {
     int sms = 148, blocks = UVW_CELL_MINB * TILE_CELLS / UVW_PF_BLOCK;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kern, UVW_PF_BLOCK, 0);
-    int d = std::max(1, sms * std::max(1, blocks * UVW_PF_BLOCK / TILE_CELLS));  // in tiles
+    int d = std::max(1, sms * std::max(1, blocks * UVW_PF_BLOCK / TILE_CELLS) * 5 / 4);  // in tiles
     if (const char *e = std::getenv("CUPCFD_PREFETCH_DIST")) if (*e) d = std::max(1, std::atoi(e));
     wave[{device, kern}] = d;
     return d;
