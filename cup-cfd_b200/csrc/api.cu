@@ -164,10 +164,17 @@ int tiles_setup(cupcfd_gpu_mesh *m, cudaStream_t st) {
     // block sizes: 256 threads (one tile) except the forward+mass adjoint's
     const int pfBlock[PF_COUNT] = {TILE_CELLS, TILE_CELLS, TILE_CELLS,           TILE_CELLS,
                                    CUPCFD_FWD_MADJ_BLOCK, TILE_CELLS, TILE_CELLS};
-    // prefetch distance in waves, in quarters: 1 wave, except 1.25 for the
-    // forward+mass adjoint (0.536 ms at 256^3 against 0.545 at 1 wave, 0.540
-    // at 1.5, 0.572 at 2, 0.584 at 0.75)
-    const int pfQuarters[PF_COUNT] = {4, 4, 4, 4, 5, 4, 4};
+    // prefetch distance in waves, in quarters, measured at 256^3 (same box):
+    // 1.25 waves for the forward+mass adjoint (0.538 ms against 0.546 at 1
+    // wave, 0.541 at 1.5, 0.581 at 0.75), the separate FP32 forward and
+    // adjoint (0.491 / 0.528 against 0.492 / 0.531), the FP64 forward (0.706
+    // against 0.720) and the mass-only adjoint; 1 wave for the gradient
+    // adjoint (equal) and the FP64 adjoint (0.84 against 0.81 ms)
+    int pfQuarters[PF_COUNT] = {5, 5, 5, 4, 5, 4, 5};
+    // CUPCFD_PREFETCH_QUARTERS=q sets every kernel's distance to q/4 waves
+    if (const char *e = std::getenv("CUPCFD_PREFETCH_QUARTERS"))
+        if (*e)
+            for (int &q : pfQuarters) q = std::max(1, std::atoi(e));
     for (int i = 0; i < PF_COUNT; i++) {
         int nb = 0;
         CG_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pfKern[i], pfBlock[i], 0));
