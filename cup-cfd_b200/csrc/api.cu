@@ -918,8 +918,10 @@ int launch_adj_part(const cupcfd_gpu_mesh *m, bool f64, const void *g, double hs
                     const void *gface, void *phiBar, void *phiBBar, void *stateBar, cudaStream_t st) {
     unsigned grid = grid_for(m->nC, BLK);
     const bool gradPart = gface == nullptr;
+    KernelTimer kt(nullptr, st);
     if (!f64 && m->tiles && m->nC % 4 == 0 &&
         (gradPart ? hscale == 2.0 && aligned16(g) : hscale == 0.0 && !g && aligned16(state) && aligned16(gface))) {
+        kt.set_name(gradPart ? "k_gadj_f32_pf" : "k_madj_f32_pf");
         if (gradPart)
             CG_LAUNCH_PF(m, k_gadj_f32_pf, grid, st, m->nC, sell(m), m->fg32, (const float *) g, 2.f,
                          (float *) phiBar, (float *) phiBBar, m->nC, prefetch_args(m, PF_GADJ));
@@ -929,6 +931,7 @@ int launch_adj_part(const cupcfd_gpu_mesh *m, bool f64, const void *g, double hs
         CG_LAUNCHED();
         return CUPCFD_E_SUCCESS;
     }
+    kt.set_name(f64 ? "k_adj_f64" : "k_adj_f32");
     if (f64)
         k_adj_f64<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg64, (const double *) g, hscale, (const double *) state,
                                         (const double *) gface, (double *) phiBar, (double *) phiBBar,

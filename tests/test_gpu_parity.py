@@ -538,7 +538,20 @@ def test_host_call_equals_device_call(cg, gpu, order, prec, mk):
     mesh = cg.Mesh.from_arrays(ref, order=order)
     f = O.fields(ref, 25)
     gface = np.random.Generator(np.random.Philox(key=26)).standard_normal(ref["nFaces"])
-    host = cg.forward_adjoint(mesh, prec, f["phi"], f["phiB"], f["den"], f["u"], f["v"], f["w"], gface)
+    cg.timing_read()
+    cg.timing_enable(True)
+    try:
+        host = cg.forward_adjoint(mesh, prec, f["phi"], f["phiB"], f["den"], f["u"], f["v"], f["w"], gface)
+        ran = set(cg.timing_read())
+    finally:
+        cg.timing_enable(False)
+    # the adjoint's two parts: the L2-prefetch kernels in FP32 on a tiled mesh
+    # whose cell count allows whole 16-byte state ranges, else the plain
+    # adjoint kernel
+    if prec == cg.PREC_F32C and mesh.tiles and mesh.nCells % 4 == 0:
+        assert {"k_gadj_f32_pf", "k_madj_f32_pf"} <= ran, sorted(ran)
+    else:
+        assert ("k_adj_f64" if prec == cg.PREC_F64 else "k_adj_f32") in ran, sorted(ran)
     c2o, f2o = mesh.numbering()
     nC, nF, nB = mesh.nCells, mesh.nFaces, mesh.nBoundaries
     dt = torch.float64 if prec == cg.PREC_F64 else torch.float32
