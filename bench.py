@@ -121,7 +121,11 @@ def profile_traffic():
 
 
 class Clocks:
-    """nvidia-smi sampler for the timed region (SM clock, throttle reasons)."""
+    """nvidia-smi sampler for the timed region, every 20 ms (SM and memory
+    clocks, board power, throttle reasons). A sustained forward+adjoint loop
+    reaches the board's power limit within 100-200 ms (sw_power_cap, SM clock
+    down to about 1.56 GHz, memory clock unchanged), so the samples must be
+    dense enough to see a timed region of a few hundred milliseconds."""
 
     def __init__(self, index):
         self.index = index
@@ -134,9 +138,9 @@ class Clocks:
             os.close(fd)
             q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                  "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,clocks.mem")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -149,7 +153,8 @@ class Clocks:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
-        sm, mx, reasons = [], None, set()
+        sm, mem, pw, mx, reasons = [], [], [], None, set()
+        capped = 0
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         with open(self.path) as fh:
             for line in fh:
@@ -161,12 +166,62 @@ class Clocks:
                     mx = float(p[2])
                 except ValueError:
                     continue
+                for conv, dst, i in ((float, pw, 3), (float, mem, 9)):
+                    try:
+                        dst.append(conv(p[i]))
+                    except (ValueError, IndexError):
+                        pass
                 for nm, v in zip(names, p[5:9]):
                     if v.lower() == "active":
                         reasons.add(nm)
+                        capped += nm == "sw_power_cap"
         os.unlink(self.path)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        out = {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+               "samples": len(sm)}
+        if sm:
+            out["sm_mhz_min"] = min(sm)
+        if mem:
+            out["mem_mhz"] = statistics.median(mem)
+        if pw:
+            out["power_w_max"] = max(pw)
+        if "sw_power_cap" in reasons:
+            out["sw_power_cap_samples"] = capped
+        return out
+
+
+def sustained_run(step, st, seconds, ms_guess, nF, world, index):
+    """The step back to back for about `seconds`, with the clocks sampled:
+    device time per step in 100 ms bins of device time. The board's power
+    limit engages 100-200 ms into a sustained loop (sw_power_cap: the SM clock
+    falls, the memory clock does not), so a long run settles at the rate of
+    the last bins, below the first."""
+    import torch
+    n = max(10, int(seconds * 1e3 / max(ms_guess, 1e-3)))
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
+    torch.cuda.synchronize()
+    time.sleep(1.0)  # let the board cool back from the measurements before
+    clocks = Clocks(index)
+    clocks.start()
+    time.sleep(0.1)
+    for k in range(n):
+        ev[k][0].record(st)
+        step()
+        ev[k][1].record(st)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    time.sleep(1.0)  # and again before the measurements after
+    t = [a.elapsed_time(b) for a, b in ev]
+    starts = [ev[0][0].elapsed_time(a) for a, _ in ev]
+    span = starts[-1] + t[-1]
+    bins = {}
+    for s0, x in zip(starts, t):
+        bins.setdefault(int(s0 // 100), []).append(x)
+    per = [sum(v) / len(v) for _, v in sorted(bins.items())]
+    last = [x for s0, x in zip(starts, t) if s0 >= span - 500.0]
+    ms_last = sum(last) / len(last)
+    return {"seconds": span / 1e3, "steps": n, "ms_per_step_per_100ms": [round(x, 4) for x in per],
+            "ms_per_step_first_100ms": per[0], "ms_per_step_last_500ms": ms_last,
+            "value_last_500ms": world * nF / (ms_last * 1e-3) / 1e9, "unit": "Gfaces/s", "clocks": clk}
 
 
 # ---------------------------------------------------------------------------
@@ -633,6 +688,10 @@ def run_gpu(a):
     total_ms = max_over_ranks(total_ms, dist, dev)
     ms_step = total_ms / K
     value = job_gfaces(world, nF, ms_step * 1e-3)
+    sus = None
+    if a.sustained_s > 0:
+        # the same step for longer, after the timed region: the power-capped rate
+        sus = sustained_run(step, st, a.sustained_s, ms_step, nF, world, vis[local] if local < len(vis) else local)
 
     # ---- the same work as the separate dev_forward and dev_adjoint calls, for comparison
     e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
@@ -843,6 +902,7 @@ def run_gpu(a):
             "next_rows": rows,
             "gpu_launches": launches,
             "clocks": clk,
+            "sustained": sus,
             "mesh_build_s": t_build,
         }
         print(json.dumps(line), flush=True)
@@ -868,6 +928,9 @@ def main():
     ap.add_argument("--cpu-reps", type=int, default=10)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-uvw", action="store_true", help="skip the momentum face loop measurement")
+    ap.add_argument("--sustained-s", type=float, default=1.5,
+                    help="after the timed region, run the step back to back this long and report its rate per "
+                         "100 ms with the clocks (0: skip)")
     ap.add_argument("--no-rows", action="store_true",
                     help="skip the boundary-loop, halo and mesh-file measurements")
     a = ap.parse_args()
