@@ -92,6 +92,10 @@ struct Acc2 {
     }
     __device__ __forceinline__ void sub_prod(float a, float b) { add_prod(-a, b); }
     __device__ __forceinline__ double value() const { return (double) s + (double) e; }
+    // (float) value(), in one FP32 add and with the same bits: the double sum
+    // of two floats is exact unless their exponents differ by more than 29,
+    // and then |e| < 2^-29 |s| and both forms give s
+    __device__ __forceinline__ float value_f() const { return __fadd_rn(s, e); }
 };
 
 // Two Acc2 sums advanced together by the sm_100 packed FP32x2 operations
@@ -139,6 +143,9 @@ struct Acc2x2 {
     }
     __device__ __forceinline__ double x() const { return (double) s.x + (double) e.x; }
     __device__ __forceinline__ double y() const { return (double) s.y + (double) e.y; }
+    // (float) x(), (float) y() in FP32, the same bits (Acc2::value_f)
+    __device__ __forceinline__ float xf() const { return __fadd_rn(s.x, e.x); }
+    __device__ __forceinline__ float yf() const { return __fadd_rn(s.y, e.y); }
 };
 
 // ---------------------------------------------------------------------------

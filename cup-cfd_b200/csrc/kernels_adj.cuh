@@ -233,7 +233,7 @@ __device__ __forceinline__ double fwd_madj_cell_f32(int c, const SellView &sv, c
     double fact = 1.0 / V;
     float rx = (float) (axy.x() * fact), ry = (float) (axy.y() * fact), rz = (float) (azr.x() * fact);
     g[c] = rx; g[ldc + c] = ry; g[2 * ldc + c] = rz;
-    stbar[c] = make_float4((float) azr.y(), (float) uvb.x(), (float) uvb.y(), (float) wb.value());
+    stbar[c] = make_float4(azr.yf(), uvb.xf(), uvb.yf(), wb.value_f());
     return __fma_rn(V, __fma_rn((double) rx, (double) rx, __fma_rn((double) ry, (double) ry, __dmul_rn((double) rz, (double) rz))),
                     lsum);
 }
@@ -484,8 +484,8 @@ __device__ __forceinline__ void adj_cell_f32(int c, const SellView &sv, const fl
         }
         next_entries<PIPE>(e, k0 + CH, w, en, nx);
     }
-    if (doG) phibar[c] = (float) pb.value();
-    if (doM) stbar[c] = make_float4((float) rb.value(), (float) uvb.x(), (float) uvb.y(), (float) wb.value());
+    if (doG) phibar[c] = pb.value_f();
+    if (doM) stbar[c] = make_float4(rb.value_f(), uvb.xf(), uvb.yf(), wb.value_f());
 }
 
 __global__ void __launch_bounds__(256, CUPCFD_MINB_ADJ_F64) k_adj_f64(int nC, SellView sv, const double4 *__restrict__ fg,
