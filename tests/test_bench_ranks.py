@@ -70,3 +70,48 @@ def test_two_gloo_ranks_time_max_and_reference_arm_on_rank0():
     import bench
     assert line["config"] == bench.workload_config(6, 2, 2)
     assert line["steps"] == 3 and line["warmup"] == 3
+
+
+class _DoneProc:
+    def terminate(self):
+        pass
+
+    def wait(self, timeout=None):
+        return 0
+
+
+def test_clock_sampler_reads_power_cap_and_memory_clock(tmp_path):
+    """bench.Clocks parses nvidia-smi rows in the order it asks for them
+    (index, SM clock, SM max, power, active mask, hw_slowdown,
+    hw_thermal_slowdown, sw_thermal_slowdown, sw_power_cap, memory clock):
+    the SM clock's median and minimum, the memory clock, the highest power
+    and every throttle reason seen, with the samples that had the power cap;
+    unreadable rows are skipped."""
+    sys.path.insert(0, ROOT)
+    import bench
+    rows = ["0, 1965, 1965, 268.4, 0x0000000000000000, Not Active, Not Active, Not Active, Not Active, 3996",
+            "0, 1965, 1965, 730.1, 0x0000000000000000, Not Active, Not Active, Not Active, Not Active, 3996",
+            "0, 1612, 1965, 995.8, 0x0000000000000004, Not Active, Not Active, Not Active, Active, 3996",
+            "0, 1567, 1965, 1014.0, 0x0000000000000004, Not Active, Not Active, Not Active, Active, 3996",
+            "0, 1560, 1965, 997.1, 0x0000000000000004, Not Active, Not Active, Not Active, Active, 3996",
+            "0, [N/A], 1965, 990.0, 0x0, Not Active, Not Active, Not Active, Not Active, 3996",
+            "garbage"]
+    c = bench.Clocks(0)
+    c.path = str(tmp_path / "clocks.csv")
+    with open(c.path, "w") as fh:
+        fh.write("\n".join(rows) + "\n")
+    c.proc = _DoneProc()
+    out = c.stop()
+    assert out["samples"] == 5
+    assert out["sm_mhz"] == 1612.0 and out["sm_mhz_min"] == 1560.0 and out["sm_max_mhz"] == 1965.0
+    assert out["mem_mhz"] == 3996.0 and out["power_w_max"] == 1014.0
+    assert out["reasons"] == ["sw_power_cap"] and out["sw_power_cap_samples"] == 3
+    assert not os.path.exists(c.path)
+
+
+def test_clock_sampler_without_nvidia_smi():
+    """No sampler process: the line says so instead of inventing clocks."""
+    sys.path.insert(0, ROOT)
+    import bench
+    c = bench.Clocks(0)
+    assert c.stop() == {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
