@@ -161,9 +161,10 @@ int tiles_setup(cupcfd_gpu_mesh *m, cudaStream_t st) {
         w6 ? (const void *) k_madj_f32_pf<6> : (const void *) k_madj_f32_pf<0>};
     static_assert(sizeof(pfKern) / sizeof(pfKern[0]) == PF_COUNT, "one kernel per PfKernel");
     static_assert(PF_COUNT <= (int) (sizeof(m->prefetchWave) / sizeof(m->prefetchWave[0])), "room for every wave");
-    // block sizes: 256 threads (one tile) except the forward+mass adjoint's
-    const int pfBlock[PF_COUNT] = {TILE_CELLS, TILE_CELLS, TILE_CELLS,           TILE_CELLS,
-                                   CUPCFD_FWD_MADJ_BLOCK, TILE_CELLS, TILE_CELLS};
+    // block sizes: 64 threads (TileBlock) for the forward kernels and the
+    // FP32 adjoint, 256 (one tile) for the FP64 adjoint and the adjoint parts
+    const int pfBlock[PF_COUNT] = {CUPCFD_FWD_BLOCK,      CUPCFD_FWD_BLOCK, CUPCFD_FWD_BLOCK, TILE_CELLS,
+                                   CUPCFD_FWD_MADJ_BLOCK, TILE_CELLS,       TILE_CELLS};
     // prefetch distance in waves, in quarters, measured at 256^3 (same box):
     // 1.25 waves for the forward+mass adjoint (0.538 ms against 0.546 at 1
     // wave, 0.541 at 1.5, 0.581 at 0.75), the separate FP32 forward and
@@ -422,14 +423,20 @@ extern "C" int cupcfd_gpu_dev_mass_plain_adjoint(cupcfd_gpu_mesh *m, int32_t pre
 namespace {
 // FP32 forward: the L2-prefetch kernel when the mesh has tile ranges and the
 // arrays start on 16-byte boundaries, else the plain one (identical results).
-// One launch either way; the caller checks it. part: per-256-cell loss
-// partials, or null.
+// One launch either way; the caller checks it. part: the loss partials, or
+// null: one per warp (TILE_CELLS / 32 per tile, warp-major; *group set to
+// that) from the L2-prefetch kernel, one per 256-cell tile (*group 1) from
+// the plain one; room for TILE_CELLS / 32 per tile either way.
 const char *launch_fwd_f32(const cupcfd_gpu_mesh *m, const void *phi, const void *phiB, const void *state,
-                           const void *gface, void *grad, void *massFlux, double *part, cudaStream_t st) {
+                           const void *gface, void *grad, void *massFlux, double *part, cudaStream_t st,
+                           int *group) {
+    *group = 1;
     if (m->tiles && aligned16(phi) && aligned16(state) && (!gface || aligned16(gface))) {
-        CG_LAUNCH_PF(m, k_fwd_f32_pf, grid_for(m->nC, BLK), st, m->nC, sell(m), m->fg32, (const float *) phi,
-                     (const float *) phiB, m->vol, (const float4 *) state, (const float *) gface, (float *) grad,
-                     (float *) massFlux, part, m->nC, prefetch_args(m, PF_FWD_F32));
+        CG_LAUNCH_PF_BLOCK(m, k_fwd_f32_pf, grid_for(m->nC, BLK) * (TILE_CELLS / CUPCFD_FWD_BLOCK), CUPCFD_FWD_BLOCK,
+                           st, m->nC, sell(m), m->fg32, (const float *) phi, (const float *) phiB, m->vol,
+                           (const float4 *) state, (const float *) gface, (float *) grad, (float *) massFlux, part,
+                           m->nC, prefetch_args(m, PF_FWD_F32));
+        *group = TILE_CELLS / 32;
         return "k_fwd_f32_pf";
     }
     k_fwd_f32<BLK><<<grid_for(m->nC, BLK), BLK, 0, st>>>(m->nC, sell(m), m->fg32, (const float *) phi,
@@ -443,12 +450,16 @@ const char *launch_fwd_f32(const cupcfd_gpu_mesh *m, const void *phi, const void
 // arrays allow whole 16-byte ranges (state blocks of an even cell count),
 // else the plain one. Identical results.
 const char *launch_fwd_f64(const cupcfd_gpu_mesh *m, const void *phi, const void *phiB, const void *state,
-                           const void *gface, void *grad, void *massFlux, double *part, cudaStream_t st) {
+                           const void *gface, void *grad, void *massFlux, double *part, cudaStream_t st,
+                           int *group) {
+    *group = 1;
     if (m->tiles && aligned16(phi) && aligned16(state) && (!gface || aligned16(gface)) &&
         m->nC % 2 == 0) {
-        CG_LAUNCH_PF(m, k_fwd_f64_pf, grid_for(m->nC, BLK), st, m->nC, sell(m), m->fg64, (const double *) phi,
-                     (const double *) phiB, m->vol, (const double *) state, (const double *) gface, (double *) grad,
-                     (double *) massFlux, part, m->nC, prefetch_args(m, PF_FWD_F64));
+        CG_LAUNCH_PF_BLOCK(m, k_fwd_f64_pf, grid_for(m->nC, BLK) * (TILE_CELLS / CUPCFD_FWD_BLOCK), CUPCFD_FWD_BLOCK,
+                           st, m->nC, sell(m), m->fg64, (const double *) phi, (const double *) phiB, m->vol,
+                           (const double *) state, (const double *) gface, (double *) grad, (double *) massFlux,
+                           part, m->nC, prefetch_args(m, PF_FWD_F64));
+        *group = TILE_CELLS / 32;
         return "k_fwd_f64_pf";
     }
     k_fwd_f64<BLK><<<grid_for(m->nC, BLK), BLK, 0, st>>>(m->nC, sell(m), m->fg64, (const double *) phi,
@@ -472,14 +483,23 @@ extern "C" int cupcfd_gpu_dev_forward(cupcfd_gpu_mesh *m, int32_t precision, con
     cudaStream_t st = as_stream(stream);
     unsigned grid = grid_for(m->nC, BLK);
     double *part = nullptr;
-    if (loss) CG_TRY(scratch(m, S_LOSS, grid, &part));
+    if (loss) CG_TRY(scratch(m, S_LOSS, (size_t) grid * (TILE_CELLS / 32), &part));
+    int group = 1;
     {
         KernelTimer kt(nullptr, st);
-        kt.set_name(precision == CUPCFD_PREC_F64 ? launch_fwd_f64(m, phi, phiB, state, gface, grad, massFlux, part, st)
-                                                 : launch_fwd_f32(m, phi, phiB, state, gface, grad, massFlux, part, st));
+        kt.set_name(precision == CUPCFD_PREC_F64
+                        ? launch_fwd_f64(m, phi, phiB, state, gface, grad, massFlux, part, st, &group)
+                        : launch_fwd_f32(m, phi, phiB, state, gface, grad, massFlux, part, st, &group));
         CG_LAUNCHED();
     }
     if (loss) {
+        // per-warp partials: each tile's value first (many blocks), then the
+        // fixed-order sum over tiles; the same bits as per-tile partials
+        if (group > 1) {
+            KTIMER("k_group_partials", st);
+            k_group_partials<TILE_CELLS / 32><<<grid_for(grid, BLK), BLK, 0, st>>>((int) grid, part);
+            CG_LAUNCHED();
+        }
         KTIMER("k_reduce_partials", st);
         k_reduce_partials<<<1, 1024, 0, st>>>((int) grid, part, loss);
         CG_LAUNCHED();
@@ -509,9 +529,10 @@ extern "C" int cupcfd_gpu_dev_adjoint(cupcfd_gpu_mesh *m, int32_t precision, con
                                         (const double *) gface, (double *) phiBar, (double *) phiBBar, (double *) stateBar, m->nC);
     } else if (m->tiles && aligned16(grad) && aligned16(state) && aligned16(gface) && m->nC % 4 == 0) {
         kt.set_name("k_adj_f32_pf");
-        CG_LAUNCH_PF(m, k_adj_f32_pf, grid, st, m->nC, sell(m), m->fg32, (const float *) grad, 2.f,
-                     (const float4 *) state, (const float *) gface, (float *) phiBar, (float *) phiBBar,
-                     (float4 *) stateBar, m->nC, prefetch_args(m, PF_ADJ_F32));
+        CG_LAUNCH_PF_BLOCK(m, k_adj_f32_pf, grid * (TILE_CELLS / CUPCFD_FWD_BLOCK), CUPCFD_FWD_BLOCK, st, m->nC,
+                           sell(m), m->fg32, (const float *) grad, 2.f, (const float4 *) state, (const float *) gface,
+                           (float *) phiBar, (float *) phiBBar, (float4 *) stateBar, m->nC,
+                           prefetch_args(m, PF_ADJ_F32));
     } else {
         kt.set_name("k_adj_f32");
         k_adj_f32<<<grid, BLK, 0, st>>>(m->nC, sell(m), m->fg32, (const float *) grad, 2.f, (const float4 *) state,
@@ -1141,10 +1162,10 @@ extern "C" int cupcfd_gpu_forward_adjoint_f32(cupcfd_gpu_mesh *m, int32_t precis
 // (which also synchronises the device). This variant runs the same kernels
 // with the partials in a fixed array compiled into the library instead.
 //
-// Limits: the array holds NOALLOC_MAX_PARTIALS doubles (512 KiB, one per
-// 256-cell block), so a loss can be reduced for meshes of up to 16,777,216
-// cells; larger meshes are rejected with CUPCFD_E_ARRAY_SIZE_MISMATCH before
-// anything runs. Every GPU that loads the library holds the array until the
+// Limits: the array holds NOALLOC_MAX_PARTIALS doubles (4 MiB: one per warp,
+// eight per 256-cell tile, for NOALLOC_MAX_TILES tiles), so a loss can be
+// reduced for meshes of up to 16,777,216 cells; larger meshes are rejected
+// with CUPCFD_E_ARRAY_SIZE_MISMATCH before anything runs. Every GPU that loads the library holds the array until the
 // process exits. All calls share it: each call writes every slot it reads
 // before reading it (nothing needs clearing), but calls whose kernels
 // overlap on the GPU (different streams, no ordering between them) race on
@@ -1153,7 +1174,8 @@ extern "C" int cupcfd_gpu_forward_adjoint_f32(cupcfd_gpu_mesh *m, int32_t precis
 // before any stream capture. No error message is recorded (recording one
 // allocates host memory); the status code says what failed.
 namespace {
-constexpr int NOALLOC_MAX_PARTIALS = 65536;
+constexpr int NOALLOC_MAX_TILES = 65536;
+constexpr int NOALLOC_MAX_PARTIALS = NOALLOC_MAX_TILES * (TILE_CELLS / 32);
 constexpr int NOALLOC_MAX_DEVICES = 64;
 static __device__ __align__(256) double g_noalloc_partials[NOALLOC_MAX_PARTIALS];
 // Per device, the array's device address once looked up (null until then).
@@ -1190,7 +1212,7 @@ extern "C" int cupcfd_gpu_dev_forward_noalloc(cupcfd_gpu_mesh *m, int32_t precis
         if (((uintptr_t) state) % sa != 0 || ((uintptr_t) loss) % 8 != 0) return CUPCFD_E_CONFIG_INVALID_VALUE;
     }
     unsigned grid = grid_for(m->nC, BLK);
-    if (loss && grid > (unsigned) NOALLOC_MAX_PARTIALS) return CUPCFD_E_ARRAY_SIZE_MISMATCH;
+    if (loss && grid > (unsigned) NOALLOC_MAX_TILES) return CUPCFD_E_ARRAY_SIZE_MISMATCH;
     int dev = m->device;
     if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return CUPCFD_E_NOT_IMPLEMENTED;
     DeviceGuard guard(dev);
@@ -1207,13 +1229,19 @@ extern "C" int cupcfd_gpu_dev_forward_noalloc(cupcfd_gpu_mesh *m, int32_t precis
         }
     }
     cudaStream_t st = as_stream(stream);
+    int group = 1;
     if (precision == CUPCFD_PREC_F64)
-        launch_fwd_f64(m, phi, phiB, state, gface, grad, massFlux, part, st);
+        launch_fwd_f64(m, phi, phiB, state, gface, grad, massFlux, part, st, &group);
     else
-        launch_fwd_f32(m, phi, phiB, state, gface, grad, massFlux, part, st);
+        launch_fwd_f32(m, phi, phiB, state, gface, grad, massFlux, part, st, &group);
     g_launches.fetch_add(1, std::memory_order_relaxed);
     if (cudaGetLastError() != cudaSuccess) return CUPCFD_E_ERROR;
     if (loss) {
+        if (group > 1) {
+            k_group_partials<TILE_CELLS / 32><<<grid_for(grid, BLK), BLK, 0, st>>>((int) grid, part);
+            g_launches.fetch_add(1, std::memory_order_relaxed);
+            if (cudaGetLastError() != cudaSuccess) return CUPCFD_E_ERROR;
+        }
         k_reduce_partials<<<1, 1024, 0, st>>>((int) grid, part, loss);
         g_launches.fetch_add(1, std::memory_order_relaxed);
         if (cudaGetLastError() != cudaSuccess) return CUPCFD_E_ERROR;

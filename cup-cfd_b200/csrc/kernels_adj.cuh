@@ -313,6 +313,22 @@ __device__ __forceinline__ double group_value(const double *v) {
     return s;
 }
 
+// In place: part[t] becomes block t's value from its G partials (part[k n +
+// t], k < G) summed in order from 0.0, the value k_reduce_partials<G> forms
+// for it, so k_reduce_partials<1> over part[0, n) then gives k_reduce_partials
+// <G>'s result bit for bit (each thread accumulates the same values in the
+// same order). One thread per block value, reading and writing only its own
+// column; many blocks, where k_reduce_partials<G> is one.
+template <int G>
+__global__ void __launch_bounds__(256) k_group_partials(int n, double *__restrict__ part) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    double v[G];
+#pragma unroll
+    for (int k = 0; k < G; k++) v[k] = part[(size_t) k * n + t];
+    part[t] = group_value<G>(v);
+}
+
 template <int G = 1>
 __global__ void k_reduce_partials(int n, const double *__restrict__ part, double *__restrict__ out) {
     __shared__ double red[1024];

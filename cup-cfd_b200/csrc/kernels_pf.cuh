@@ -27,63 +27,70 @@ namespace cupcfd_gpu {
 // same order, so the same bits).
 // ---------------------------------------------------------------------------
 
+// The separate forward and FP32 adjoint kernels run in blocks of
+// CUPCFD_FWD_BLOCK = 64 threads (TileBlock), the forwards with one loss
+// partial per warp, folded per tile by k_group_partials before the fixed-
+// order sum. At 256^3 on one box: FP32 forward 0.477-0.485 ms against
+// 0.503-0.533 in 256-thread blocks, FP32 adjoint 0.518-0.529 against
+// 0.543-0.583, FP64 forward 0.698-0.704 against 0.707-0.717. The FP64
+// adjoint keeps 256-thread blocks (slower in 64: 0.835 against 0.81 ms).
+#ifndef CUPCFD_FWD_BLOCK
+#define CUPCFD_FWD_BLOCK 64
+#endif
 template <int WF>
-__global__ void __launch_bounds__(TILE_CELLS, CUPCFD_MINB_F32)
+__global__ void __launch_bounds__(CUPCFD_FWD_BLOCK, CUPCFD_MINB_F32 *TILE_CELLS / CUPCFD_FWD_BLOCK)
     k_fwd_f32_pf(int nC, SellView sv, const float4 *__restrict__ fg, const float *__restrict__ phi,
                  const float *__restrict__ phiB, const double *__restrict__ vol, const float4 *__restrict__ st,
                  const float *__restrict__ gface, float *__restrict__ g, float *__restrict__ mflux,
                  double *__restrict__ lossPart, int64_t ldc, PrefetchArgs pf) {
     constexpr int T = TILE_CELLS;
-    int c = blockIdx.x * T + threadIdx.x;
-    const int tp = blockIdx.x + pf.dist;
-    const bool lead = threadIdx.x == T - 32 && tp < pf.nTiles;
+    const TileBlock<CUPCFD_FWD_BLOCK> tb(pf);
+    const int c = tb.c;
     __shared__ int4 s_rng;
     const void *const cellSrc[3] = {phi, st, vol};
     const int cellBytes[3] = {T * 4, T * 16, T * 8};
-    if (lead) fetch_ranges_async(&s_rng, pf.desc + tp);
+    if (tb.lead) fetch_ranges_async(&s_rng, pf.desc + tb.tp);
     double l = 0.0;
     if (c < nC) l = fwd_cell_f32<CUPCFD_FWD_CHUNK, WF>(c, sv, fg, phi, phiB, vol, st, gface, g, mflux, ldc);
-    if (lead) prefetch_tile<3>(pf, tp, ranges_ready(&s_rng), fg, 16, gface, cellSrc, cellBytes);
-    if (lossPart) block_sum_store<T>(l, lossPart);
+    if (tb.lead) prefetch_tile<3>(pf, tb.tp, ranges_ready(&s_rng), fg, 16, gface, cellSrc, cellBytes);
+    if (lossPart) warp_partial_store<CUPCFD_FWD_BLOCK>(l, c, lossPart);
 }
 
 template <int WF>
-__global__ void __launch_bounds__(TILE_CELLS, CUPCFD_MINB_F32)
+__global__ void __launch_bounds__(CUPCFD_FWD_BLOCK, CUPCFD_MINB_F32 *TILE_CELLS / CUPCFD_FWD_BLOCK)
     k_adj_f32_pf(int nC, SellView sv, const float4 *__restrict__ fg, const float *__restrict__ g, float hscale,
                  const float4 *__restrict__ st, const float *__restrict__ gface, float *__restrict__ phibar,
                  float *__restrict__ phibBar, float4 *__restrict__ stbar, int64_t ldc, PrefetchArgs pf) {
     constexpr int T = TILE_CELLS;
-    int c = blockIdx.x * T + threadIdx.x;
-    const int tp = blockIdx.x + pf.dist;
-    const bool lead = threadIdx.x == T - 32 && tp < pf.nTiles;
+    const TileBlock<CUPCFD_FWD_BLOCK> tb(pf);
+    const int c = tb.c;
     __shared__ int4 s_rng;
     const void *const cellSrc[4] = {g, g + ldc, g + 2 * ldc, st};
     const int cellBytes[4] = {T * 4, T * 4, T * 4, T * 16};
-    if (lead) fetch_ranges_async(&s_rng, pf.desc + tp);
+    if (tb.lead) fetch_ranges_async(&s_rng, pf.desc + tb.tp);
     if (c < nC) adj_cell_f32<false, CUPCFD_ADJ_CHUNK, 0, WF>(c, sv, fg, g, hscale, st, gface, phibar, phibBar, stbar, ldc);
-    if (lead) prefetch_tile<4>(pf, tp, ranges_ready(&s_rng), fg, 16, gface, cellSrc, cellBytes);
+    if (tb.lead) prefetch_tile<4>(pf, tb.tp, ranges_ready(&s_rng), fg, 16, gface, cellSrc, cellBytes);
 }
 
 // FP64 forward (fwd_cell_f64, exact reference arithmetic) with the same L2
 // prefetch; the state's four component blocks are prefetched one by one.
 template <int WF>
-__global__ void __launch_bounds__(TILE_CELLS, CUPCFD_MINB_FWD_F64)
+__global__ void __launch_bounds__(CUPCFD_FWD_BLOCK, CUPCFD_MINB_FWD_F64 *TILE_CELLS / CUPCFD_FWD_BLOCK)
     k_fwd_f64_pf(int nC, SellView sv, const double4 *__restrict__ fg, const double *__restrict__ phi,
                  const double *__restrict__ phiB, const double *__restrict__ vol, const double *__restrict__ st,
                  const double *__restrict__ gface, double *__restrict__ g, double *__restrict__ mflux,
                  double *__restrict__ lossPart, int64_t ldc, PrefetchArgs pf) {
     constexpr int T = TILE_CELLS;
-    int c = blockIdx.x * T + threadIdx.x;
-    const int tp = blockIdx.x + pf.dist;
-    const bool lead = threadIdx.x == T - 32 && tp < pf.nTiles;
+    const TileBlock<CUPCFD_FWD_BLOCK> tb(pf);
+    const int c = tb.c;
     __shared__ int4 s_rng;
     const void *const cellSrc[6] = {phi, vol, st, st + ldc, st + 2 * ldc, st + 3 * ldc};
     const int cellBytes[6] = {T * 8, T * 8, T * 8, T * 8, T * 8, T * 8};
-    if (lead) fetch_ranges_async(&s_rng, pf.desc + tp);
+    if (tb.lead) fetch_ranges_async(&s_rng, pf.desc + tb.tp);
     double l = 0.0;
     if (c < nC) l = fwd_cell_f64<CUPCFD_FWD_CHUNK_F64, WF>(c, sv, fg, phi, phiB, vol, st, gface, g, mflux, ldc);
-    if (lead) prefetch_tile<6>(pf, tp, ranges_ready(&s_rng), fg, 32, gface, cellSrc, cellBytes);
-    if (lossPart) block_sum_store<T>(l, lossPart);
+    if (tb.lead) prefetch_tile<6>(pf, tb.tp, ranges_ready(&s_rng), fg, 32, gface, cellSrc, cellBytes);
+    if (lossPart) warp_partial_store<CUPCFD_FWD_BLOCK>(l, c, lossPart);
 }
 
 // FP64 adjoint (adj_cell_f64) with the same L2 prefetch.
@@ -131,22 +138,17 @@ __global__ void __launch_bounds__(CUPCFD_FWD_MADJ_BLOCK, CUPCFD_MINB_FWD_MADJ *T
                       const float *__restrict__ phiB, const double *__restrict__ vol, const float4 *__restrict__ st,
                       const float *__restrict__ gface, float *__restrict__ g, float *__restrict__ mflux,
                       float4 *__restrict__ stbar, double *__restrict__ lossPart, int64_t ldc, PrefetchArgs pf) {
-    constexpr int T = TILE_CELLS, B = CUPCFD_FWD_MADJ_BLOCK, P = T / B;
-    static_assert(T % B == 0 && B % 32 == 0, "whole warps, whole tiles");
-    int c = blockIdx.x * B + threadIdx.x;
-    const int tp = blockIdx.x / P + pf.dist;
-    const bool lead = blockIdx.x % P == P - 1 && threadIdx.x == B - 32 && tp < pf.nTiles;
+    constexpr int T = TILE_CELLS;
+    const TileBlock<CUPCFD_FWD_MADJ_BLOCK> tb(pf);
+    const int c = tb.c;
     __shared__ int4 s_rng;
     const void *const cellSrc[3] = {phi, st, vol};
     const int cellBytes[3] = {T * 4, T * 16, T * 8};
-    if (lead) fetch_ranges_async(&s_rng, pf.desc + tp);
+    if (tb.lead) fetch_ranges_async(&s_rng, pf.desc + tb.tp);
     double l = 0.0;
     if (c < nC) l = fwd_madj_cell_f32<CUPCFD_FWD_MADJ_CHUNK, 0, WF>(c, sv, fg, phi, phiB, vol, st, gface, g, mflux, stbar, ldc);
-    if (lead) prefetch_tile<3>(pf, tp, ranges_ready(&s_rng), fg, 16, gface, cellSrc, cellBytes);
-    if (lossPart) {
-        for (int k = 16; k > 0; k >>= 1) l += __shfl_xor_sync(0xffffffffu, l, k);
-        if ((threadIdx.x & 31) == 0) lossPart[(size_t) ((c >> 5) % (T / 32)) * (gridDim.x / P) + c / T] = l;
-    }
+    if (tb.lead) prefetch_tile<3>(pf, tb.tp, ranges_ready(&s_rng), fg, 16, gface, cellSrc, cellBytes);
+    if (lossPart) warp_partial_store<CUPCFD_FWD_MADJ_BLOCK>(l, c, lossPart);
 }
 
 // Gradient part of the adjoint only (adj_cell_f32 without the mass part):

@@ -6,7 +6,7 @@
 // order is one contiguous range of device memory: its incidence entries,
 // the records of the faces its cells own, and its cells' entries in every
 // cell array. TileDesc holds those ranges, built once per mesh. In the
-// prefetch kernels one lane per 256-cell block asks L2 to fetch the ranges
+// prefetch kernels one lane per 256-cell tile asks L2 to fetch the ranges
 // of the tile `dist` blocks ahead (cp.async.bulk.prefetch.L2), so the
 // streamed loads of later blocks become L2 hits; shared memory and L1 are
 // untouched and the per-cell arithmetic is that of the plain kernels.
@@ -50,6 +50,35 @@ __device__ __forceinline__ void fetch_ranges_async(int4 *dst, const TileDesc *d)
 __device__ __forceinline__ int4 ranges_ready(const int4 *src) {
     asm volatile("cp.async.wait_group 0;" ::: "memory");
     return *src;
+}
+
+// Blocks smaller than a tile: TILE_CELLS / B blocks of B threads per tile,
+// at the registers and warps per SM of 256-thread blocks. A block's slot
+// frees when its own warps end instead of the slowest of eight. The last
+// block of a tile prefetches for the tile (the lead lane: its last warp's
+// first lane).
+template <int B>
+struct TileBlock {
+    static_assert(TILE_CELLS % B == 0 && B % 32 == 0, "whole warps, whole tiles");
+    static constexpr int P = TILE_CELLS / B;
+    int c, tp;
+    bool lead;
+    __device__ __forceinline__ explicit TileBlock(const PrefetchArgs &pf) {
+        c = blockIdx.x * B + threadIdx.x;
+        tp = blockIdx.x / P + pf.dist;
+        lead = blockIdx.x % P == P - 1 && threadIdx.x == B - 32 && tp < pf.nTiles;
+    }
+};
+
+// One loss partial per warp, warp k of tile t at part[k nTiles + t] (stored
+// warp-major, so that the loads which fold them coalesce); summed per tile in
+// order from 0.0 (k_group_partials, k_reduce_partials<8>) they give the value
+// a 256-thread block's reduction forms. Every lane takes part.
+template <int B>
+__device__ __forceinline__ void warp_partial_store(double l, int c, double *part) {
+    for (int k = 16; k > 0; k >>= 1) l += __shfl_xor_sync(0xffffffffu, l, k);
+    if ((threadIdx.x & 31) == 0)
+        part[(size_t) ((c >> 5) % (TILE_CELLS / 32)) * (gridDim.x / TileBlock<B>::P) + c / TILE_CELLS] = l;
 }
 
 // Prefetches a tile's ranges: its entries, its owned faces' records (fgSize

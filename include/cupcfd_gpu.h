@@ -513,8 +513,8 @@ int cupcfd_gpu_dev_adjoint(cupcfd_gpu_mesh *mesh, int32_t precision, const void 
  * the loss partials live in a fixed array inside the library instead of the
  * mesh's scratch pool, and the call makes no cudaMalloc/cudaFree or other
  * allocating call. Same arguments and results as cupcfd_gpu_dev_forward.
- * Limits: the array holds 65,536 partials (512 KiB per GPU that loads the
- * library, held until exit), so with a loss the mesh may have at most
+ * Limits: the array holds 524,288 partials (one per warp: 4 MiB per GPU that
+ * loads the library, held until exit), so with a loss the mesh may have at most
  * 16,777,216 cells; larger meshes return CUPCFD_E_ARRAY_SIZE_MISMATCH. All
  * calls share the array: calls whose kernels overlap on the GPU race. The
  * first call on a device sets up the array's address with that device

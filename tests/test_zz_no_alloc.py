@@ -62,8 +62,9 @@ def test_noalloc_forward_equals_forward_twice(cg, gpu, prec):
 
 def test_noalloc_rejects_meshes_beyond_its_limit(cg, gpu):
     import torch
-    # 257 x 256 x 256 = 16,842,752 cells: one 256-cell block more than the
-    # 65,536 loss partials the fixed array holds
+    # 257 x 256 x 256 = 16,842,752 cells: 65,792 tiles of 256 cells, beyond the
+    # 65,536 tiles (eight loss partials each, one per warp) the fixed array
+    # holds
     mesh = cg.Mesh.structgen(257, 256, 256, order=cg.ORDER_OWNER, precisions=1 << cg.PREC_F32C)
     phi, phiB, st, gface = _fields(torch, mesh, 1, 3)
     g, m, l = _outputs(torch, mesh, torch.float32)
