@@ -412,11 +412,10 @@ __device__ __forceinline__ void uvw_cell(const UvwArgs<T> &a, int c) {
 // block of a tile prefetches for the tile).
 template <class T>
 __device__ __forceinline__ void uvw_cell_pf(const UvwArgs<T> &a, const PrefetchArgs &pf) {
-    constexpr int TC = TILE_CELLS, B = UVW_PF_BLOCK, P = TC / B;
-    static_assert(TC % B == 0 && B % 32 == 0, "whole warps, whole tiles");
-    const int c = blockIdx.x * B + threadIdx.x;
-    const int tp = blockIdx.x / P + pf.dist;
-    const bool lead = blockIdx.x % P == P - 1 && threadIdx.x == B - 32 && tp < pf.nTiles;
+    constexpr int TC = TILE_CELLS;
+    const TileBlock<UVW_PF_BLOCK> tb(pf);
+    const int c = tb.c, tp = tb.tp;
+    const bool lead = tb.lead;
     __shared__ int4 s_rng;
     if (lead) fetch_ranges_async(&s_rng, pf.desc + tp);
     if (c < a.nC) uvw_cell(a, c);
