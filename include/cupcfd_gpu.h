@@ -375,10 +375,11 @@ int cupcfd_gpu_flux_mass_dolfyn_face_loop_f32(cupcfd_gpu_mesh *mesh,
  * with m_f = rho_f (u_f . S_f). Outputs (host, FP64, any may be NULL):
  * grad[3*nCells] (xyz interleaved), massFlux[nFaces] (boundary entries 0),
  * phiBar[nCells], phiBBar[nBoundaries], denBar/uBar/vBar/wBar[nCells],
- * loss[1]. nGradient is 1. Results are copied back on a second stream of the
- * mesh while later inputs are still being copied in (gradient and phiBar once
- * phi is in, mass fluxes once the state is in, the state adjoint and the loss
- * once gface is in); they equal cupcfd_gpu_dev_forward_adjoint's bit for bit.
+ * loss[1]. nGradient is 1. The inputs go in on a copy-in stream of the mesh
+ * and the results come back on a copy-out stream while later inputs are
+ * still being copied in (gradient and phiBar once phi is in, mass fluxes once
+ * the state is in, the state adjoint and then the loss once gface is in);
+ * they equal cupcfd_gpu_dev_forward_adjoint's bit for bit.
  * Pinned host buffers let the copies in both directions overlap. Returns when
  * every output is in host memory. */
 int cupcfd_gpu_forward_adjoint(cupcfd_gpu_mesh *mesh, int32_t precision,
